@@ -1,0 +1,60 @@
+"""Builds the native libraries in-tree.
+
+libfdmap_gpu.so   CUDA engine (sm_100a) + host-side domain initialisation,
+                  the C ABI of include/fdmap_gpu.h and include/fdmap_host.h.
+
+The shared object is written next to this file so that it travels with the
+source tree; it is rebuilt when any source or header is newer than it.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+LIB = PKG / "libfdmap_gpu.so"
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _sources() -> list[Path]:
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
+
+
+def _deps() -> list[Path]:
+    return _sources() + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + sorted(INCLUDE.glob("*.h"))
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build_library(force: bool = False, verbose: bool = False) -> Path:
+    """Compile libfdmap_gpu.so for sm_100a (cross-compiles without a GPU)."""
+    if not force and not _stale(LIB, _deps()):
+        return LIB
+    cmd = [
+        NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo",
+        f"-I{INCLUDE}", f"-I{CSRC}",
+        "-Xcompiler", "-fPIC,-O3", "-shared",
+        *[str(s) for s in _sources()],
+        "-o", str(LIB) + ".tmp",
+    ]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(str(LIB) + ".tmp", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build_library(force="--force" in sys.argv, verbose=True))

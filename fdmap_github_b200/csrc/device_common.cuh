@@ -1,0 +1,145 @@
+// Device-side data layout and the point-wise physics shared by the kernels:
+// rotations (geometry.f90:285-336), characteristic boundary conditions
+// (boundaries.f90:155-377), locked and frictional interface solves
+// (interfaces.f90:676-1012) and friction laws (friction.f90:555-1506).
+//
+// HBM layout.  Each block is stored separately with a row pitch that is a
+// multiple of 32 doubles (256 B), so every row starts on a 256-byte boundary
+// and a warp reading 32 consecutive nodes touches exactly two 128-byte lines:
+//   field l, block-local node (i, j):  base + l*plane + j*pitch + i,
+//   plane = pitch*ny.
+// Fields are ping-ponged (F[0], F[1]) between RK stages because the fused
+// stencil reads neighbours of a node while other CTAs already write the
+// updated state; rates DF are updated in place (only the node itself reads
+// its own rate).
+#pragma once
+
+#include <cstdint>
+
+#include "fdmap_desc.h"
+
+namespace fdmap {
+
+constexpr int MAX_BLOCKS = 16;
+constexpr int MAX_IFACES = 32;
+
+struct DevSide {
+  int bc, n;
+  int cov_lo, cov_hi;  // side-local nodes [cov_lo, cov_hi) whose hat variables come from an interface
+  double* M;           // (n,5)
+  double* F0;          // (n,nF)
+  double* nrm;         // (n,2)
+  double* Fhat;        // (n,nF)
+};
+
+struct DevBlock {
+  int nx, ny, pitch;
+  long long plane;
+  double* F[2];
+  double* DF;
+  double *xq, *xr, *yq, *yr, *Ji;      // (pitch, ny)
+  double *rho, *G, *M, *gamma, *nu;    // heterogeneous only
+  double rho_b, G_b, M_b, gamma_b, nu_b;
+  double coef[4][3];                   // homogeneous interior weights DI(s)/rho, DI(s)*G, DI(s)*M
+                                       // (a, b, c of rates_interior_mode2, rates.f90:400-405)
+  double F0v[9];
+  DevSide side[4];
+  int src_ok, src_i0, src_j0;          // block-local source indices
+  double src_wx[5], src_wy[5];         // singular_source weights d for i0-2..i0+2
+  int tile_begin;                      // first stencil tile of this block
+  int tiles_x;
+};
+
+// per-interface friction storage: st[f*n + k] for the 18 FDMAP_FAULT_* fields,
+// par[p*n + k] for the per-node parameters below
+enum { PAR_A = 0, PAR_B, PAR_V0, PAR_F0, PAR_L, PAR_FW, PAR_VW, PAR_C0, PAR_FS, PAR_FD, PAR_DC, PAR_BSS0, PAR_BSN0, PAR_N };
+
+struct DevFriction {
+  int law, reg, rup_field, force, ld_shape, tp_use, has_bsS0, has_bsN0;
+  double rup_threshold, angle, xlockm, xlockp, flock, skempton;
+  double kn_c0, kn_fd, kn_dfdx, kn_vL, kn_vR, kn_xL, kn_xR, kn_tmax;
+  double ld_S, ld_N, ld_T, ld_R, ld_x0, ld_y0, tp_p0;
+  double* st;
+  double* par;
+};
+
+struct DevIface {
+  int direction, im, ip, m, p, n, coupling;
+  int offm, offp;  // side-local index of global node m on the minus / plus side
+  double* nhat;    // (n,2)
+  double *x, *y;   // (n)
+  DevFriction fr;
+};
+
+struct DevDomain {
+  int mode, nF, nblocks, nifaces, het;
+  int nbst, nbnd, pI;
+  double DI[4];     // DI[s], s = 1..pI (fd_coeff.f90)
+  double DL[6][9];  // DL[r][s]: weight of point s for the derivative at boundary node r
+  DevBlock blk[MAX_BLOCKS];
+  DevIface ifc[MAX_IFACES];
+  // edge work segments: BC sides first, then interfaces
+  int nseg;
+  int seg_kind[4 * MAX_BLOCKS + MAX_IFACES];   // 0 = BC side, 1 = interface
+  int seg_a[4 * MAX_BLOCKS + MAX_IFACES];      // block (BC) or interface index
+  int seg_b[4 * MAX_BLOCKS + MAX_IFACES];      // side (BC)
+  int seg_start[4 * MAX_BLOCKS + MAX_IFACES + 1];
+  fdmap_source src;
+  unsigned long long* status;  // [0] Newton failures, [1] nonfinite flags
+};
+
+struct StageArgs {
+  double A;      // RK coefficient A(stage): rates are scaled by it first
+  double Bdt;    // B(stage)*dt: state update weight
+  double t;      // stage time
+  int in, out;   // F buffer read / written
+  int scale;     // scale rates by A (0 for the initial edge solve)
+  int update;    // update the state (0 on the final step and the initial solve)
+};
+
+// ---------------------------------------------------------------------------
+// rotations (geometry.f90:285-336; fields.f90:1297-1356)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void xy2nt_vec(double wx, double wy, double& wt, double& wn, double n0, double n1) {
+  wt = n1 * wx - n0 * wy;
+  wn = n0 * wx + n1 * wy;
+}
+__device__ __forceinline__ void nt2xy_vec(double& wx, double& wy, double wt, double wn, double n0, double n1) {
+  wx = n1 * wt + n0 * wn;
+  wy = -n0 * wt + n1 * wn;
+}
+__device__ __forceinline__ void xy2nt_mat(double wxx, double wxy, double wyy, double& wtt, double& wnt, double& wnn,
+                                          double n0, double n1) {
+  wtt = -(2.0 * n0 * n1 * wxy) + (n1 * n1) * wxx + (n0 * n0) * wyy;
+  wnt = n0 * n1 * (wxx - wyy) + ((n1 * n1) - (n0 * n0)) * wxy;
+  wnn = 2.0 * n0 * n1 * wxy + (n0 * n0) * wxx + (n1 * n1) * wyy;
+}
+__device__ __forceinline__ void nt2xy_mat(double& wxx, double& wxy, double& wyy, double wtt, double wnt, double wnn,
+                                          double n0, double n1) {
+  wxx = 2.0 * n0 * n1 * wnt + (n1 * n1) * wtt + (n0 * n0) * wnn;
+  wxy = -(n0 * n1 * (wtt - wnn)) + ((n1 * n1) - (n0 * n0)) * wnt;
+  wyy = -(2.0 * n0 * n1 * wnt) + (n0 * n0) * wtt + (n1 * n1) * wnn;
+}
+__device__ __forceinline__ void rot2_xy2nt(const double* F, double n0, double n1, double* o) {
+  xy2nt_vec(F[0], F[1], o[0], o[1], n0, n1);
+  xy2nt_mat(F[2], F[3], F[4], o[2], o[3], o[4], n0, n1);
+  o[5] = F[5];
+}
+__device__ __forceinline__ void rot2_nt2xy(double* F, double n0, double n1, double vt, double vn, double stt,
+                                           double snt, double snn, double szz) {
+  nt2xy_vec(F[0], F[1], vt, vn, n0, n1);
+  nt2xy_mat(F[2], F[3], F[4], stt, snt, snn, n0, n1);
+  F[5] = szz;
+}
+__device__ __forceinline__ void rot3_xy2nt(const double* F, double n0, double n1, double* o) {
+  o[0] = F[0];
+  xy2nt_vec(F[1], F[2], o[1], o[2], n0, n1);
+}
+__device__ __forceinline__ void rot3_nt2xy(double* F, double n0, double n1, double vz, double stz, double snz) {
+  F[0] = vz;
+  nt2xy_vec(F[1], F[2], stz, snz, n0, n1);
+}
+
+__device__ __forceinline__ double fsign(double a, double b) { return copysign(fabs(a), b); }
+
+}  // namespace fdmap

@@ -1,0 +1,562 @@
+// Host side of the B200 engine: device allocation and layout conversion,
+// the RK stage loop (time_step_LS, time_step.f90:71-167) and the C ABI
+// declared in include/fdmap_gpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "edge_kernel.cuh"
+#include "fdmap_gpu.h"
+#include "sbp_tables.h"
+#include "stencil_kernel.cuh"
+
+using namespace fdmap;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return set_err(FDMAP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+  } while (0)
+
+struct BlockGeom {
+  int mgx, mgy, nx, ny, pitch;
+  long long plane;
+};
+
+// singular_source weights (source.f90:327-406) for the 5 nodes i0-2..i0+2
+void source_weights(double h, double a, double* w) {
+  double beta = (1.0 - 2.0 * a) / 4.0 + 0.25;
+  double gam = (2.0 * a - 1.0) / 16.0;
+  double gap = (2.0 * a + 1.0) / 16.0;
+  w[0] = (-gam) / h;
+  w[1] = (beta + 3.0 * gam - gap) / h;
+  w[2] = (1.0 - a - 2.0 * beta - 3.0 * gam + 3.0 * gap) / h;
+  w[3] = (a + beta + gam - 3.0 * gap) / h;
+  w[4] = (gap) / h;
+}
+
+}  // namespace
+
+struct fdmap_gpu {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevDomain hdom{};
+  DevDomain* ddom = nullptr;
+  std::vector<void*> allocs;
+  long long bytes = 0;
+  int cur = 0;
+  int mode = 2, nF = 6, pI = 2, het = 0;
+  RkTable rk{};
+  int nx_g = 0, ny_g = 0;
+  std::vector<BlockGeom> geom;
+  std::vector<int> iface_n;
+  std::vector<int> iface_fric;
+  int total_tiles = 0, edge_threads = 0;
+  double* h_stage = nullptr;  // pinned staging buffer for layout conversion
+  size_t stage_doubles = 0;
+  unsigned long long* d_status = nullptr;
+  long long launches = 0;
+  double* dev_fhat[MAX_BLOCKS][4] = {};
+  int side_n[MAX_BLOCKS][4] = {};
+
+  template <typename T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    size_t bytes_ = count * sizeof(T);
+    if (bytes_ == 0) bytes_ = 16;
+    cudaError_t e = cudaMalloc(&q, bytes_);
+    if (e != cudaSuccess) return set_err(FDMAP_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(q);
+    bytes += (long long)bytes_;
+    *p = (T*)q;
+    return FDMAP_OK;
+  }
+  int upload(double** dst, const double* src, size_t count) {
+    int rc = alloc(dst, count);
+    if (rc) return rc;
+    if (src) CUDA_TRY(cudaMemcpy(*dst, src, count * sizeof(double), cudaMemcpyHostToDevice));
+    return FDMAP_OK;
+  }
+  // global (nx_g, ny_g) plane -> padded block plane on the device
+  int upload_plane(double* dst, const double* src, const BlockGeom& g) {
+    std::vector<double> tmp((size_t)g.plane, 0.0);
+    for (int j = 0; j < g.ny; ++j)
+      for (int i = 0; i < g.nx; ++i)
+        tmp[(size_t)j * g.pitch + i] = src[(size_t)(g.mgx - 1 + i) + (size_t)nx_g * (size_t)(g.mgy - 1 + j)];
+    CUDA_TRY(cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return FDMAP_OK;
+  }
+  ~fdmap_gpu() {
+    if (device >= 0) cudaSetDevice(device);
+    for (void* p : allocs) cudaFree(p);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+int launch_edges(fdmap_gpu* h, const StageArgs& a) {
+  if (h->edge_threads == 0) return FDMAP_OK;
+  int tpb = 128;
+  int nb = (h->edge_threads + tpb - 1) / tpb;
+  if (h->mode == 2) edge_kernel<2><<<nb, tpb, 0, h->stream>>>(h->ddom, a);
+  else edge_kernel<3><<<nb, tpb, 0, h->stream>>>(h->ddom, a);
+  h->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return FDMAP_OK;
+}
+
+template <int MODE>
+void launch_stencil_mode(fdmap_gpu* h, const StageArgs& a) {
+  dim3 grid(h->total_tiles), block(TX * TY);
+  if (h->het) {
+    if (h->pI == 1) stencil_kernel<MODE, 1, true><<<grid, block, 0, h->stream>>>(h->ddom, a);
+    else if (h->pI == 2) stencil_kernel<MODE, 2, true><<<grid, block, 0, h->stream>>>(h->ddom, a);
+    else stencil_kernel<MODE, 3, true><<<grid, block, 0, h->stream>>>(h->ddom, a);
+  } else {
+    if (h->pI == 1) stencil_kernel<MODE, 1, false><<<grid, block, 0, h->stream>>>(h->ddom, a);
+    else if (h->pI == 2) stencil_kernel<MODE, 2, false><<<grid, block, 0, h->stream>>>(h->ddom, a);
+    else stencil_kernel<MODE, 3, false><<<grid, block, 0, h->stream>>>(h->ddom, a);
+  }
+}
+
+int launch_stencil(fdmap_gpu* h, const StageArgs& a) {
+  if (h->mode == 2) launch_stencil_mode<2>(h, a);
+  else launch_stencil_mode<3>(h, a);
+  h->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return FDMAP_OK;
+}
+
+int validate(const fdmap_desc* d) {
+  if (!d) return set_err(FDMAP_ERR_INVALID_ARG, "null descriptor");
+  if (d->mode != 2 && d->mode != 3) return set_err(FDMAP_ERR_INVALID_ARG, "mode must be 2 or 3");
+  if (d->nF != (d->mode == 2 ? 6 : 3)) return set_err(FDMAP_ERR_INVALID_ARG, "nF does not match mode");
+  if (d->nblocks < 1 || d->nblocks > MAX_BLOCKS) return set_err(FDMAP_ERR_UNSUPPORTED, "1..16 blocks supported");
+  if (d->nifaces < 0 || d->nifaces > MAX_IFACES) return set_err(FDMAP_ERR_UNSUPPORTED, "at most 32 interfaces supported");
+  if (!d->F || !d->DF || !d->xq || !d->xr || !d->yq || !d->yr || !d->Ji)
+    return set_err(FDMAP_ERR_INVALID_ARG, "missing body arrays");
+  if (d->heterogeneous && (!d->rho || !d->G || (d->mode == 2 && (!d->M || !d->gamma || !d->nu))))
+    return set_err(FDMAP_ERR_INVALID_ARG, "missing heterogeneous material arrays");
+  fdmap::SbpOperator op;
+  if (!fdmap::sbp_operator(d->fd_method, &op)) return set_err(FDMAP_ERR_UNSUPPORTED, "unknown FD method");
+  for (int b = 0; b < d->nblocks; ++b) {
+    const fdmap_block& B = d->blocks[b];
+    int nx = B.pgx - B.mgx + 1, ny = B.pgy - B.mgy + 1;
+    if (B.mgx < 1 || B.mgy < 1 || B.pgx > d->nx || B.pgy > d->ny)
+      return set_err(FDMAP_ERR_INVALID_ARG, "block index limits outside the domain");
+    if (nx < 2 * op.nbst || ny < 2 * op.nbst || nx < op.nbnd || ny < op.nbnd)
+      return set_err(FDMAP_ERR_UNSUPPORTED, "block too small for the SBP boundary closures");
+    for (int s = 0; s < 4; ++s) {
+      const fdmap_side& S = B.side[s];
+      if (S.n != (s < 2 ? ny : nx)) return set_err(FDMAP_ERR_INVALID_ARG, "side length mismatch");
+      if (!S.M || !S.F0 || !S.normal) return set_err(FDMAP_ERR_INVALID_ARG, "missing side arrays");
+      if (d->mode == 3 && S.bc != FDMAP_BC_NONE && S.bc != FDMAP_BC_ABSORBING && S.bc != FDMAP_BC_FREE &&
+          S.bc != FDMAP_BC_RIGID)
+        return set_err(FDMAP_ERR_UNSUPPORTED, "boundary condition not available in mode III");
+    }
+  }
+  for (int k = 0; k < d->nifaces; ++k) {
+    const fdmap_iface& I = d->ifaces[k];
+    if (I.iblockm < 0 || I.iblockm >= d->nblocks || I.iblockp < 0 || I.iblockp >= d->nblocks || I.p < I.m)
+      return set_err(FDMAP_ERR_INVALID_ARG, "bad interface description");
+    if (I.coupling == FDMAP_COUPLING_FRICTION) {
+      const fdmap_friction& fr = I.fr;
+      if (!fr.V || !fr.O || !fr.S || !fr.N || !fr.S0 || !fr.N0 || !fr.Ds || !fr.Dn || !fr.DDs || !fr.DDn ||
+          !fr.Psi || !fr.DPsi || !fr.D || !fr.trup || !fr.W || !fr.DW || !fr.Nreg || !fr.DNreg)
+        return set_err(FDMAP_ERR_INVALID_ARG, "missing friction state arrays");
+      if (fr.law >= FDMAP_FR_SL && (!fr.a || !fr.b || !fr.V0 || !fr.f0 || !fr.L || !fr.fw || !fr.Vw))
+        return set_err(FDMAP_ERR_INVALID_ARG, "missing rate-and-state parameters");
+      if (fr.law == FDMAP_FR_SW && (!fr.c0 || !fr.fs || !fr.fd || !fr.Dc))
+        return set_err(FDMAP_ERR_INVALID_ARG, "missing slip-weakening parameters");
+    }
+  }
+  return FDMAP_OK;
+}
+
+int build(fdmap_gpu* h, const fdmap_desc* d) {
+  DevDomain& D = h->hdom;
+  std::memset(&D, 0, sizeof(D));
+  fdmap::SbpOperator op;
+  fdmap::sbp_operator(d->fd_method, &op);
+  fdmap::rk_table(d->rk_order, &h->rk);
+  if (h->rk.nstage == 0) return set_err(FDMAP_ERR_INVALID_ARG, "Invalid Runge-Kutta order");
+  h->mode = d->mode; h->nF = d->nF; h->pI = op.pI; h->het = d->heterogeneous;
+  h->nx_g = d->nx; h->ny_g = d->ny;
+  D.mode = d->mode; D.nF = d->nF; D.nblocks = d->nblocks; D.nifaces = d->nifaces; D.het = d->heterogeneous;
+  D.nbst = op.nbst; D.nbnd = op.nbnd; D.pI = op.pI;
+  for (int s = 0; s <= op.pI; ++s) D.DI[s] = op.DI[s];
+  for (int r = 0; r < op.nbst; ++r)
+    for (int s = 0; s < op.nbnd; ++s) D.DL[r][s] = op.DL[r][s];
+  D.src = d->src;
+  const int nF = d->nF;
+  int tiles = 0;
+  h->geom.resize(d->nblocks);
+  for (int b = 0; b < d->nblocks; ++b) {
+    const fdmap_block& fb = d->blocks[b];
+    DevBlock& B = D.blk[b];
+    BlockGeom& g = h->geom[b];
+    g.mgx = fb.mgx; g.mgy = fb.mgy;
+    g.nx = fb.pgx - fb.mgx + 1; g.ny = fb.pgy - fb.mgy + 1;
+    g.pitch = (g.nx + 31) / 32 * 32;
+    g.plane = (long long)g.pitch * g.ny;
+    B.nx = g.nx; B.ny = g.ny; B.pitch = g.pitch; B.plane = g.plane;
+    int rc;
+    for (int q = 0; q < 2; ++q)
+      if ((rc = h->alloc(&B.F[q], (size_t)g.plane * nF))) return rc;
+    if ((rc = h->alloc(&B.DF, (size_t)g.plane * nF))) return rc;
+    double** met[5] = {&B.xq, &B.xr, &B.yq, &B.yr, &B.Ji};
+    const double* msrc[5] = {d->xq, d->xr, d->yq, d->yr, d->Ji};
+    for (int q = 0; q < 5; ++q) {
+      if ((rc = h->alloc(met[q], (size_t)g.plane))) return rc;
+      if ((rc = h->upload_plane(*met[q], msrc[q], g))) return rc;
+    }
+    if (d->heterogeneous) {
+      double** hm[5] = {&B.rho, &B.G, &B.M, &B.gamma, &B.nu};
+      const double* hs[5] = {d->rho, d->G, d->M, d->gamma, d->nu};
+      for (int q = 0; q < 5; ++q) {
+        if (!hs[q]) continue;
+        if ((rc = h->alloc(hm[q], (size_t)g.plane))) return rc;
+        if ((rc = h->upload_plane(*hm[q], hs[q], g))) return rc;
+      }
+    }
+    B.rho_b = fb.rho; B.G_b = fb.G; B.M_b = fb.M; B.gamma_b = fb.gamma; B.nu_b = fb.nu;
+    for (int s = 1; s <= op.pI; ++s) {
+      B.coef[s][0] = op.DI[s] / fb.rho;
+      B.coef[s][1] = op.DI[s] * fb.G;
+      B.coef[s][2] = op.DI[s] * fb.M;
+    }
+    for (int q = 0; q < 9; ++q) B.F0v[q] = fb.F0[q];
+    for (int s = 0; s < 4; ++s) {
+      const fdmap_side& fs = fb.side[s];
+      DevSide& S = B.side[s];
+      S.bc = fs.bc; S.n = fs.n; S.cov_lo = 0; S.cov_hi = 0;
+      if ((rc = h->upload(&S.M, fs.M, (size_t)fs.n * 5))) return rc;
+      if ((rc = h->upload(&S.F0, fs.F0, (size_t)fs.n * nF))) return rc;
+      if ((rc = h->upload(&S.nrm, fs.normal, (size_t)fs.n * 2))) return rc;
+      if ((rc = h->alloc(&S.Fhat, (size_t)fs.n * nF))) return rc;
+      std::vector<double> big((size_t)fs.n * nF, 1e40);  // fields.f90:850 sentinel
+      CUDA_TRY(cudaMemcpy(S.Fhat, big.data(), big.size() * sizeof(double), cudaMemcpyHostToDevice));
+      h->dev_fhat[b][s] = S.Fhat;
+      h->side_n[b][s] = fs.n;
+    }
+    B.src_ok = 0;
+    if (d->src.use_singular && fb.src_ok) {
+      B.src_ok = 1;
+      B.src_i0 = fb.src_i0 - fb.mgx;
+      B.src_j0 = fb.src_j0 - fb.mgy;
+      source_weights(fb.src_hx, fb.src_ax, B.src_wx);
+      source_weights(fb.src_hy, fb.src_ay, B.src_wy);
+    }
+    B.tiles_x = (g.nx + TX - 1) / TX;
+    int tiles_y = (g.ny + TY - 1) / TY;
+    B.tile_begin = tiles;
+    tiles += B.tiles_x * tiles_y;
+  }
+  h->total_tiles = tiles;
+
+  // interfaces
+  h->iface_n.resize(d->nifaces);
+  h->iface_fric.resize(d->nifaces);
+  for (int k = 0; k < d->nifaces; ++k) {
+    const fdmap_iface& fi = d->ifaces[k];
+    DevIface& I = D.ifc[k];
+    I.direction = fi.direction; I.im = fi.iblockm; I.ip = fi.iblockp; I.m = fi.m; I.p = fi.p;
+    I.n = fi.p - fi.m + 1; I.coupling = fi.coupling;
+    h->iface_n[k] = I.n;
+    h->iface_fric[k] = fi.coupling == FDMAP_COUPLING_FRICTION;
+    const fdmap_block& Bm = d->blocks[fi.iblockm];
+    const fdmap_block& Bp = d->blocks[fi.iblockp];
+    I.offm = fi.m - (fi.direction == 0 ? Bm.mgy : Bm.mgx);
+    I.offp = fi.m - (fi.direction == 0 ? Bp.mgy : Bp.mgx);
+    // sides whose hat variables come from this interface
+    DevSide& Sm = D.blk[fi.iblockm].side[fi.direction == 0 ? 1 : 3];
+    DevSide& Sp = D.blk[fi.iblockp].side[fi.direction == 0 ? 0 : 2];
+    Sm.cov_lo = I.offm; Sm.cov_hi = I.offm + I.n;
+    Sp.cov_lo = I.offp; Sp.cov_hi = I.offp + I.n;
+    int rc;
+    if ((rc = h->upload(&I.nhat, fi.nhat, 2 * (size_t)I.n))) return rc;
+    if ((rc = h->upload(&I.x, fi.x, (size_t)I.n))) return rc;
+    if ((rc = h->upload(&I.y, fi.y, (size_t)I.n))) return rc;
+    if (fi.coupling != FDMAP_COUPLING_FRICTION) continue;
+    const fdmap_friction& ff = fi.fr;
+    DevFriction& FR = I.fr;
+    FR.law = ff.law; FR.reg = ff.reg; FR.rup_field = ff.rup_field; FR.force = ff.force;
+    FR.ld_shape = ff.ld_shape; FR.tp_use = ff.tp_use;
+    FR.has_bsS0 = ff.bsS0 != nullptr; FR.has_bsN0 = ff.bsN0 != nullptr;
+    FR.rup_threshold = ff.rup_threshold; FR.angle = ff.angle; FR.xlockm = ff.xlockm; FR.xlockp = ff.xlockp;
+    FR.flock = ff.flock; FR.skempton = ff.skempton;
+    FR.kn_c0 = ff.kn_c0; FR.kn_fd = ff.kn_fd; FR.kn_dfdx = ff.kn_dfdx; FR.kn_vL = ff.kn_vL; FR.kn_vR = ff.kn_vR;
+    FR.kn_xL = ff.kn_xL; FR.kn_xR = ff.kn_xR; FR.kn_tmax = ff.kn_tmax;
+    FR.ld_S = ff.ld_S; FR.ld_N = ff.ld_N; FR.ld_T = ff.ld_T; FR.ld_R = ff.ld_R; FR.ld_x0 = ff.ld_x0;
+    FR.ld_y0 = ff.ld_y0; FR.tp_p0 = ff.tp_p0;
+    const int n = I.n;
+    std::vector<double> st((size_t)FDMAP_FAULT_NFIELDS * n), par((size_t)PAR_N * n, 0.0);
+    const double* sp[FDMAP_FAULT_NFIELDS] = {ff.D, ff.Psi, ff.DPsi, ff.trup, ff.V, ff.O, ff.S, ff.N, ff.S0,
+                                             ff.N0, ff.Ds, ff.Dn, ff.DDs, ff.DDn, ff.W, ff.DW, ff.Nreg, ff.DNreg};
+    for (int f = 0; f < FDMAP_FAULT_NFIELDS; ++f) std::memcpy(&st[(size_t)f * n], sp[f], n * sizeof(double));
+    const double* pp[PAR_N] = {ff.a, ff.b, ff.V0, ff.f0, ff.L, ff.fw, ff.Vw, ff.c0, ff.fs, ff.fd, ff.Dc, ff.bsS0, ff.bsN0};
+    for (int q = 0; q < PAR_N; ++q)
+      if (pp[q]) std::memcpy(&par[(size_t)q * n], pp[q], n * sizeof(double));
+    if ((rc = h->upload(&FR.st, st.data(), st.size()))) return rc;
+    if ((rc = h->upload(&FR.par, par.data(), par.size()))) return rc;
+  }
+
+  // edge work segments: BC sides, then interfaces
+  int nseg = 0, start = 0;
+  for (int b = 0; b < d->nblocks; ++b)
+    for (int s = 0; s < 4; ++s) {
+      if (D.blk[b].side[s].bc == FDMAP_BC_NONE) continue;
+      D.seg_kind[nseg] = 0; D.seg_a[nseg] = b; D.seg_b[nseg] = s; D.seg_start[nseg] = start;
+      start += D.blk[b].side[s].n;
+      ++nseg;
+    }
+  for (int k = 0; k < d->nifaces; ++k) {
+    D.seg_kind[nseg] = 1; D.seg_a[nseg] = k; D.seg_b[nseg] = 0; D.seg_start[nseg] = start;
+    start += D.ifc[k].n;
+    ++nseg;
+  }
+  D.seg_start[nseg] = start;
+  D.nseg = nseg;
+  h->edge_threads = start;
+
+  int rc;
+  if ((rc = h->alloc(&h->d_status, 4))) return rc;
+  CUDA_TRY(cudaMemset(h->d_status, 0, 4 * sizeof(unsigned long long)));
+  D.status = h->d_status;
+  if ((rc = h->alloc(&h->ddom, 1))) return rc;
+  CUDA_TRY(cudaMemcpy(h->ddom, &D, sizeof(DevDomain), cudaMemcpyHostToDevice));
+
+  // staging buffer and initial fields
+  size_t total = 0;
+  for (auto& g : h->geom) total += (size_t)g.plane * nF;
+  h->stage_doubles = total;
+  CUDA_TRY(cudaMallocHost(&h->h_stage, total * sizeof(double)));
+  h->cur = 0;
+  return fdmap_gpu_set_fields(h, d->F, d->DF);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu** out) {
+  if (!out) return set_err(FDMAP_ERR_INVALID_ARG, "null handle pointer");
+  *out = nullptr;
+  int rc = validate(d);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_err(FDMAP_ERR_CUDA, "no CUDA device available");
+  if (device < 0 || device >= ndev) return set_err(FDMAP_ERR_INVALID_ARG, "bad device index");
+  fdmap_gpu* h = new (std::nothrow) fdmap_gpu();
+  if (!h) return set_err(FDMAP_ERR_NOMEM, "out of host memory");
+  h->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return set_err(FDMAP_ERR_CUDA, "cannot initialise device");
+  }
+  rc = build(h, d);
+  if (rc == FDMAP_OK && init_edges) rc = fdmap_gpu_init_edges(h, d->t0);
+  if (rc == FDMAP_OK) rc = fdmap_gpu_synchronize(h);
+  if (rc) {
+    std::string keep = g_err;
+    delete h;
+    g_err = keep;
+    return rc;
+  }
+  *out = h;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_init_edges(fdmap_gpu* h, double t) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  StageArgs a{};
+  a.A = 0.0; a.Bdt = 0.0; a.t = t; a.in = h->cur; a.out = 1 - h->cur; a.scale = 0; a.update = 0;
+  return launch_edges(h, a);
+}
+
+int fdmap_gpu_time_step(fdmap_gpu* h, double t0, double dt, int final_step) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  for (int s = 0; s < h->rk.nstage; ++s) {
+    StageArgs a{};
+    a.A = h->rk.A[s];
+    a.Bdt = h->rk.B[s] * dt;
+    a.t = t0 + h->rk.C[s] * dt;
+    a.in = h->cur;
+    a.out = 1 - h->cur;
+    a.scale = 1;
+    a.update = final_step ? 0 : 1;
+    int rc = launch_edges(h, a);
+    if (rc) return rc;
+    rc = launch_stencil(h, a);
+    if (rc) return rc;
+    if (final_step) return FDMAP_OK;
+    h->cur = 1 - h->cur;
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_run(fdmap_gpu* h, double t_start, double dt, int n_first, int n_last, int nt) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  h->launches = 0;
+  for (int n = n_first; n <= n_last; ++n) {
+    int rc = fdmap_gpu_time_step(h, t_start + (double)(n - 1) * dt, dt, n == nt);
+    if (rc) return rc;
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_synchronize(fdmap_gpu* h) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_fields(fdmap_gpu* h, double* F, double* DF) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  const int nF = h->nF;
+  for (int which = 0; which < 2; ++which) {
+    double* dst = which == 0 ? F : DF;
+    if (!dst) continue;
+    size_t off = 0;
+    for (int b = 0; b < h->hdom.nblocks; ++b) {
+      const BlockGeom& g = h->geom[b];
+      const double* src = which == 0 ? h->hdom.blk[b].F[h->cur] : h->hdom.blk[b].DF;
+      CUDA_TRY(cudaMemcpyAsync(h->h_stage + off, src, (size_t)g.plane * nF * sizeof(double), cudaMemcpyDeviceToHost,
+                               h->stream));
+      off += (size_t)g.plane * nF;
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    off = 0;
+    const size_t NN = (size_t)h->nx_g * h->ny_g;
+    for (int b = 0; b < h->hdom.nblocks; ++b) {
+      const BlockGeom& g = h->geom[b];
+      for (int l = 0; l < nF; ++l)
+        for (int j = 0; j < g.ny; ++j) {
+          const double* s = h->h_stage + off + (size_t)l * g.plane + (size_t)j * g.pitch;
+          double* t = dst + (size_t)l * NN + (size_t)(g.mgy - 1 + j) * h->nx_g + (g.mgx - 1);
+          std::memcpy(t, s, g.nx * sizeof(double));
+        }
+      off += (size_t)g.plane * nF;
+    }
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_fields(fdmap_gpu* h, const double* F, const double* DF) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  const int nF = h->nF;
+  const size_t NN = (size_t)h->nx_g * h->ny_g;
+  for (int which = 0; which < 2; ++which) {
+    const double* src = which == 0 ? F : DF;
+    if (!src) continue;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));  // staging buffer reuse
+    size_t off = 0;
+    for (int b = 0; b < h->hdom.nblocks; ++b) {
+      const BlockGeom& g = h->geom[b];
+      for (int l = 0; l < nF; ++l)
+        for (int j = 0; j < g.ny; ++j) {
+          double* t = h->h_stage + off + (size_t)l * g.plane + (size_t)j * g.pitch;
+          const double* s = src + (size_t)l * NN + (size_t)(g.mgy - 1 + j) * h->nx_g + (g.mgx - 1);
+          std::memcpy(t, s, g.nx * sizeof(double));
+          for (int i = g.nx; i < g.pitch; ++i) t[i] = 0.0;
+        }
+      double* dst = which == 0 ? h->hdom.blk[b].F[h->cur] : h->hdom.blk[b].DF;
+      CUDA_TRY(cudaMemcpyAsync(dst, h->h_stage + off, (size_t)g.plane * nF * sizeof(double), cudaMemcpyHostToDevice,
+                               h->stream));
+      off += (size_t)g.plane * nF;
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_fault(fdmap_gpu* h, int iface, int field, double* out) {
+  if (!h || !out || iface < 0 || iface >= h->hdom.nifaces || field < 0 || field >= FDMAP_FAULT_NFIELDS)
+    return set_err(FDMAP_ERR_INVALID_ARG, "bad get_fault arguments");
+  if (!h->iface_fric[iface]) return set_err(FDMAP_ERR_INVALID_ARG, "interface is not frictional");
+  CUDA_TRY(cudaSetDevice(h->device));
+  int n = h->iface_n[iface];
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(out, h->hdom.ifc[iface].fr.st + (size_t)field * n, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_fault(fdmap_gpu* h, int iface, int field, const double* in) {
+  if (!h || !in || iface < 0 || iface >= h->hdom.nifaces || field < 0 || field >= FDMAP_FAULT_NFIELDS)
+    return set_err(FDMAP_ERR_INVALID_ARG, "bad set_fault arguments");
+  if (!h->iface_fric[iface]) return set_err(FDMAP_ERR_INVALID_ARG, "interface is not frictional");
+  CUDA_TRY(cudaSetDevice(h->device));
+  int n = h->iface_n[iface];
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(h->hdom.ifc[iface].fr.st + (size_t)field * n, in, n * sizeof(double), cudaMemcpyHostToDevice));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_fhat(fdmap_gpu* h, int b, int s, double* out) {
+  if (!h || !out || b < 0 || b >= h->hdom.nblocks || s < 0 || s > 3)
+    return set_err(FDMAP_ERR_INVALID_ARG, "bad get_fhat arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(out, h->dev_fhat[b][s], (size_t)h->side_n[b][s] * h->nF * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  unsigned long long st[4];
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+  if (newton_failures) *newton_failures = (long long)st[0];
+  return st[0] ? FDMAP_ERR_NEWTON_NOCONV : FDMAP_OK;
+}
+
+long long fdmap_gpu_launch_count(fdmap_gpu* h) { return h ? h->launches : -1; }
+
+long long fdmap_gpu_device_bytes(fdmap_gpu* h) { return h ? h->bytes : -1; }
+
+void fdmap_gpu_destroy(fdmap_gpu* h) { delete h; }
+
+const char* fdmap_gpu_strerror(int code) {
+  switch (code) {
+    case FDMAP_OK: return "ok";
+    case FDMAP_ERR_INVALID_ARG: return "invalid argument";
+    case FDMAP_ERR_CUDA: return "CUDA error";
+    case FDMAP_ERR_NONFINITE: return "non-finite value detected";
+    case FDMAP_ERR_NEWTON_NOCONV: return "friction Newton solver did not converge";
+    case FDMAP_ERR_TIMEOUT: return "device wait timed out";
+    case FDMAP_ERR_UNSUPPORTED: return "unsupported configuration";
+    case FDMAP_ERR_IO: return "I/O error";
+    case FDMAP_ERR_NOMEM: return "out of memory";
+  }
+  return "unknown error";
+}
+
+const char* fdmap_gpu_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

@@ -1,0 +1,343 @@
+// Fused stage kernel: for every node of every block, in one pass over HBM,
+//   DF <- A*DF                                   (scale_rates_interior, fields.f90:1061)
+//   DF += SAT penalty (sides L, R, B, T)         (set_rates_SAT, time_step.f90:754-851)
+//   DF += SBP split-form rates                   (rates.f90 / rates_heterogeneous.f90)
+//   DF6 <- nu*(DF3+DF5)  (mode II, plane strain) (rates_szz, rates.f90:920-936)
+//   DF += point source / gravity                 (set_source, source.f90:147-252)
+//   F_out <- F_in + (B*dt)*DF                    (update_fields_interior, fields.f90:1167)
+// Interior nodes read their cross-shaped neighbourhood from a shared-memory
+// tile loaded once per CTA; nodes inside the SBP boundary closures (within
+// nbst of a block edge) take a slower path through L1/L2 that applies the
+// one-sided DL/DR rows exactly like rates_boundary_mode2/3.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace fdmap {
+
+// Rate components as flat sums of metric-average x field products
+// (rates.f90:30-49, 407-444): the Y-metric term uses field fa, the X-metric
+// term field fb, optionally times gamma; coef 0: DI/rho, 1: DI*G, 2: DI*M.
+template <int MODE> struct RDef;
+template <> struct RDef<2> {
+  static constexpr int NR = 5;
+  __host__ __device__ static constexpr int fa(int r) { return r == 0 ? 2 : r == 1 ? 3 : r == 2 ? 0 : r == 3 ? 1 : 0; }
+  __host__ __device__ static constexpr int fb(int r) { return r == 0 ? 3 : r == 1 ? 4 : r == 2 ? 1 : r == 3 ? 0 : 1; }
+  __host__ __device__ static constexpr bool ga(int r) { return r == 4; }
+  __host__ __device__ static constexpr bool gb(int r) { return r == 2; }
+  __host__ __device__ static constexpr int coef(int r) { return r < 2 ? 0 : (r == 3 ? 1 : 2); }
+};
+template <> struct RDef<3> {
+  static constexpr int NR = 3;
+  __host__ __device__ static constexpr int fa(int r) { return r == 0 ? 1 : r == 1 ? 0 : -1; }
+  __host__ __device__ static constexpr int fb(int r) { return r == 0 ? 2 : r == 1 ? -1 : 0; }
+  __host__ __device__ static constexpr bool ga(int) { return false; }
+  __host__ __device__ static constexpr bool gb(int) { return false; }
+  __host__ __device__ static constexpr int coef(int r) { return r == 0 ? 0 : 1; }
+};
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+
+struct NodeMat {
+  double rho, G, M, gamma, nu;
+};
+
+__device__ __forceinline__ double mat_coef(const NodeMat& m, int kind, double w) {
+  // w/rho, w*G, w*M
+  return kind == 0 ? w / m.rho : (kind == 1 ? w * m.G : w * m.M);
+}
+
+// flux of rate r at point k: q direction +t1 - t2 (Yr, Xr), r direction -t1 + t2 (Yq, Xq);
+// r is a compile-time constant after unrolling, so the table lookups fold away
+template <int MODE>
+__device__ __forceinline__ double flux(int r, double Ym, double Xm, const double* Fk, double g, bool qdir) {
+  using RD = RDef<MODE>;
+  double v = 0.0;
+  if (RD::fa(r) >= 0) {
+    double t = Ym * Fk[RD::fa(r)];
+    if (RD::ga(r)) t *= g;
+    v = qdir ? t : -t;
+  }
+  if (RD::fb(r) >= 0) {
+    double t = Xm * Fk[RD::fb(r)];
+    if (RD::gb(r)) t *= g;
+    v = qdir ? v - t : v + t;
+  }
+  return v;
+}
+
+// Closure-region rates for node (i, j) read through the cache hierarchy
+// (rates_boundary_mode2/3 and the heterogeneous variants).
+template <int MODE, int PI_>
+__device__ void closure_rates(const DevDomain& D, const DevBlock& B, const double* __restrict__ Fin, int i, int j,
+                              const NodeMat& m, double Ji, double* acc) {
+  using RD = RDef<MODE>;
+  constexpr int NR = RD::NR;
+  const int nx = B.nx, ny = B.ny, nbst = D.nbst, nbnd = D.nbnd;
+  const long long pitch = B.pitch, plane = B.plane;
+  const long long c = (long long)j * pitch + i;
+  const int qreg = i < nbst ? 0 : (i > nx - 1 - nbst ? 1 : -1);
+  const int rreg = j < nbst ? 0 : (j > ny - 1 - nbst ? 1 : -1);
+  const double yrc = B.yr[c], xrc = B.xr[c], yqc = B.yq[c], xqc = B.xq[c];
+  auto loadF = [&](long long k, double* Fk) {
+#pragma unroll
+    for (int l = 0; l < (MODE == 2 ? 5 : 3); ++l) Fk[l] = Fin[l * plane + k];
+  };
+  auto qterm = [&](long long k, double w, int sgn) {
+    double Fk[5];
+    loadF(k, Fk);
+    double Y = 0.5 * (B.yr[k] + yrc), X = 0.5 * (B.xr[k] + xrc);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      double f = flux<MODE>(r, Y, X, Fk, m.gamma, true);
+      acc[r] += (sgn * f) * mat_coef(m, RD::coef(r), w) * Ji;
+    }
+  };
+  auto rterm = [&](long long k, double w, int sgn) {
+    double Fk[5];
+    loadF(k, Fk);
+    double Y = 0.5 * (B.yq[k] + yqc), X = 0.5 * (B.xq[k] + xqc);
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+      double f = flux<MODE>(r, Y, X, Fk, m.gamma, false);
+      acc[r] += (sgn * f) * mat_coef(m, RD::coef(r), w) * Ji;
+    }
+  };
+  auto qone = [&](int s, double& w, long long& k) {
+    if (qreg == 0) { w = D.DL[i][s]; k = (long long)j * pitch + s; }
+    else { w = -D.DL[nx - 1 - i][s]; k = (long long)j * pitch + (nx - 1 - s); }
+  };
+  auto rone = [&](int s, double& w, long long& k) {
+    if (rreg == 0) { w = D.DL[j][s]; k = (long long)s * pitch + i; }
+    else { w = -D.DL[ny - 1 - j][s]; k = (long long)(ny - 1 - s) * pitch + i; }
+  };
+  if (qreg >= 0 && rreg >= 0) {
+    for (int s = 0; s < nbnd; ++s) {
+      double w; long long k;
+      qone(s, w, k);
+      qterm(k, w, 1);
+      rone(s, w, k);
+      rterm(k, w, 1);
+    }
+  } else if (qreg >= 0) {
+    for (int s = 0; s < nbnd; ++s) {
+      double w; long long k;
+      qone(s, w, k);
+      qterm(k, w, 1);
+    }
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      rterm(c + s * pitch, D.DI[s], 1);
+      rterm(c - s * pitch, D.DI[s], -1);
+    }
+  } else {
+    for (int s = 0; s < nbnd; ++s) {
+      double w; long long k;
+      rone(s, w, k);
+      rterm(k, w, 1);
+    }
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      qterm(c + s, D.DI[s], 1);
+      qterm(c - s, D.DI[s], -1);
+    }
+  }
+}
+
+// SAT penalty of side s at side-local index k for the node whose fields are F
+// (SAT_term / split_sp, time_step.f90:813-851)
+template <int MODE>
+__device__ __forceinline__ void sat_term(const DevSide& S, int k, const double* F, double* acc) {
+  constexpr int NF = MODE == 2 ? 6 : 3;
+  double Ks = S.M[k + 3 * S.n], Kp = S.M[k + 4 * S.n];
+  double d[6];
+#pragma unroll
+  for (int l = 0; l < NF; ++l) d[l] = S.Fhat[k + S.n * l] - F[l];
+  if (MODE == 3) {
+#pragma unroll
+    for (int l = 0; l < 3; ++l) acc[l] += Ks * d[l];
+  } else {
+    double n0 = S.nrm[k], n1 = S.nrm[k + S.n];
+    double r[6], Fs[6], Fp[6];
+    rot2_xy2nt(d, n0, n1, r);
+    rot2_nt2xy(Fs, n0, n1, r[0], 0.0, 0.0, r[3], 0.0, 0.0);
+    rot2_nt2xy(Fp, n0, n1, 0.0, r[1], r[2], 0.0, r[4], r[5]);
+#pragma unroll
+    for (int l = 0; l < 6; ++l) acc[l] += Ks * Fs[l];
+#pragma unroll
+    for (int l = 0; l < 6; ++l) acc[l] += Kp * Fp[l];
+  }
+}
+
+// singular source amplitude (source.f90:208-223)
+__device__ __forceinline__ double stf_amp(const fdmap_source& S, double t) {
+  const double pi = 3.14159265358979323846264338327950288;
+  double tc = t - S.t_center;
+  switch (S.stf) {
+    case FDMAP_STF_RAMP: return fmax(fmin(tc / S.t_duration, 1.0), 0.0);
+    case FDMAP_STF_SINUSOID: return sin(2.0 * pi * tc / S.t_duration);
+    case FDMAP_STF_GAUSSIAN: return exp(-0.5 * (tc * tc) / (S.t_duration * S.t_duration));
+    default:
+      return (1.0 - 2.0 * (pi * pi) * (tc * tc) / (S.t_duration * S.t_duration)) *
+             exp(-(pi * pi) * (tc * tc) / (S.t_duration * S.t_duration));
+  }
+}
+
+template <int MODE, int PI_, bool HET>
+__global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __restrict__ Dp, StageArgs a) {
+  using RD = RDef<MODE>;
+  constexpr int NR = RD::NR;
+  constexpr int NF = MODE == 2 ? 6 : 3;
+  constexpr int H = PI_;
+  constexpr int WX = TX + 2 * H, WY = TY + 2 * H;
+  __shared__ double sF[NR][WY][WX];
+  __shared__ double s_yr[TY][WX], s_xr[TY][WX];
+  __shared__ double s_yq[WY][TX], s_xq[WY][TX];
+
+  const DevDomain& D = *Dp;
+  int b = 0;
+  while (b + 1 < D.nblocks && (int)blockIdx.x >= D.blk[b + 1].tile_begin) ++b;
+  const DevBlock& B = D.blk[b];
+  const int tile = blockIdx.x - B.tile_begin;
+  const int i0 = (tile % B.tiles_x) * TX, j0 = (tile / B.tiles_x) * TY;
+  const int nx = B.nx, ny = B.ny;
+  const long long pitch = B.pitch, plane = B.plane;
+  const double* __restrict__ Fin = B.F[a.in];
+  const int tid = threadIdx.x;
+
+  // cooperative tile loads (cross-shaped halo; corners loaded but unused)
+  for (int idx = tid; idx < WX * WY; idx += TX * TY) {
+    int ty = idx / WX, tx = idx % WX;
+    int gi = i0 + tx - H, gj = j0 + ty - H;
+    if (gi >= 0 && gi < nx && gj >= 0 && gj < ny) {
+      long long g = (long long)gj * pitch + gi;
+#pragma unroll
+      for (int l = 0; l < NR; ++l) sF[l][ty][tx] = Fin[l * plane + g];
+    }
+  }
+  for (int idx = tid; idx < WX * TY; idx += TX * TY) {
+    int ty = idx / WX, tx = idx % WX;
+    int gi = i0 + tx - H, gj = j0 + ty;
+    if (gi >= 0 && gi < nx && gj < ny) {
+      long long g = (long long)gj * pitch + gi;
+      s_yr[ty][tx] = B.yr[g];
+      s_xr[ty][tx] = B.xr[g];
+    }
+  }
+  for (int idx = tid; idx < TX * WY; idx += TX * TY) {
+    int ty = idx / TX, tx = idx % TX;
+    int gi = i0 + tx, gj = j0 + ty - H;
+    if (gi < nx && gj >= 0 && gj < ny) {
+      long long g = (long long)gj * pitch + gi;
+      s_yq[ty][tx] = B.yq[g];
+      s_xq[ty][tx] = B.xq[g];
+    }
+  }
+  __syncthreads();
+
+  const int tx = tid % TX, ty = tid / TX;
+  const int i = i0 + tx, j = j0 + ty;
+  if (i >= nx || j >= ny) return;
+  const long long c = (long long)j * pitch + i;
+
+  double acc[NF];
+#pragma unroll
+  for (int l = 0; l < NF; ++l) acc[l] = a.A * B.DF[l * plane + c];
+
+  double Fc[NF];
+#pragma unroll
+  for (int l = 0; l < NR; ++l) Fc[l] = sF[l][ty + H][tx + H];
+  if (MODE == 2) Fc[5] = Fin[5 * plane + c];
+
+  // SAT on the block edges, in the reference's side order L, R, B, T
+  if (i == 0) sat_term<MODE>(B.side[0], j, Fc, acc);
+  if (i == nx - 1) sat_term<MODE>(B.side[1], j, Fc, acc);
+  if (j == 0) sat_term<MODE>(B.side[2], i, Fc, acc);
+  if (j == ny - 1) sat_term<MODE>(B.side[3], i, Fc, acc);
+
+  NodeMat m;
+  if (HET) {
+    m.rho = B.rho[c]; m.G = B.G[c];
+    if (MODE == 2) { m.M = B.M[c]; m.gamma = B.gamma[c]; m.nu = B.nu[c]; }
+    else { m.M = 0.0; m.gamma = 0.0; m.nu = 0.0; }
+  } else {
+    m.rho = B.rho_b; m.G = B.G_b; m.M = B.M_b; m.gamma = B.gamma_b; m.nu = B.nu_b;
+  }
+  const double Ji = B.Ji[c];
+  const int nbst = D.nbst;
+  const bool interior = (i >= nbst && i <= nx - 1 - nbst && j >= nbst && j <= ny - 1 - nbst);
+
+  if (interior) {
+    const int cx = tx + H, cy = ty + H;
+    const double yrc = s_yr[ty][cx], xrc = s_xr[ty][cx];
+    const double yqc = s_yq[cy][tx], xqc = s_xq[cy][tx];
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      const double Yrp = 0.5 * (s_yr[ty][cx + s] + yrc), Xrp = 0.5 * (s_xr[ty][cx + s] + xrc);
+      const double Yrm = 0.5 * (s_yr[ty][cx - s] + yrc), Xrm = 0.5 * (s_xr[ty][cx - s] + xrc);
+      const double Yqp = 0.5 * (s_yq[cy + s][tx] + yqc), Xqp = 0.5 * (s_xq[cy + s][tx] + xqc);
+      const double Yqm = 0.5 * (s_yq[cy - s][tx] + yqc), Xqm = 0.5 * (s_xq[cy - s][tx] + xqc);
+      const double w = HET ? D.DI[s] : 0.0;
+#pragma unroll
+      for (int r = 0; r < NR; ++r) {
+        double sum = 0.0;
+        if (RD::fa(r) >= 0) {
+          const int f = RD::fa(r);
+          double t = Yrp * sF[f][cy][cx + s] - Yrm * sF[f][cy][cx - s] - Yqp * sF[f][cy + s][cx] +
+                     Yqm * sF[f][cy - s][cx];
+          if (RD::ga(r)) t *= m.gamma;
+          sum += t;
+        }
+        if (RD::fb(r) >= 0) {
+          const int f = RD::fb(r);
+          double t = -Xrp * sF[f][cy][cx + s] + Xrm * sF[f][cy][cx - s] + Xqp * sF[f][cy + s][cx] -
+                     Xqm * sF[f][cy - s][cx];
+          if (RD::gb(r)) t *= m.gamma;
+          sum += t;
+        }
+        const double cf = HET ? mat_coef(m, RD::coef(r), w) : B.coef[s][RD::coef(r)];
+        acc[r] += sum * cf * Ji;
+      }
+    }
+  } else {
+    closure_rates<MODE, PI_>(D, B, Fin, i, j, m, Ji, acc);
+  }
+
+  if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
+
+  // body forces (set_source, source.f90:147-252)
+  if (D.src.use_gravity) {
+    if (MODE == 2) { acc[0] += D.src.gx; acc[1] += D.src.gy; }
+    else acc[0] += D.src.gz;
+  }
+  if (D.src.use_singular && B.src_ok) {
+    int di = i - B.src_i0, dj = j - B.src_j0;
+    if (di >= -2 && di <= 2 && dj >= -2 && dj <= 2) {
+      double A = stf_amp(D.src, a.t);
+      double dx = B.src_wx[di + 2], dy = B.src_wy[dj + 2];
+      if (MODE == 2) {
+        acc[0] += A * D.src.Fx * dx * dy / B.rho_b;
+        acc[1] += A * D.src.Fy * dx * dy / B.rho_b;
+        acc[2] -= A * D.src.Mxx * dx * dy;
+        acc[3] -= A * D.src.Mxy * dx * dy;
+        acc[4] -= A * D.src.Myy * dx * dy;
+      } else {
+        acc[0] += A * D.src.Fz * dx * dy / B.rho_b;
+        acc[1] -= A * D.src.Mzx * dx * dy;
+        acc[2] -= A * D.src.Mzy * dx * dy;
+      }
+    }
+  }
+
+  double* __restrict__ DF = B.DF;
+#pragma unroll
+  for (int l = 0; l < NF; ++l) DF[l * plane + c] = acc[l];
+  if (a.update) {
+    double* __restrict__ Fout = B.F[a.out];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fout[l * plane + c] = Fc[l] + a.Bdt * acc[l];
+  }
+}
+
+}  // namespace fdmap

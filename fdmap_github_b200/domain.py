@@ -1,0 +1,151 @@
+"""Python mirror of FDMAP's host interface for the time-stepping path.
+
+The names follow the reference's Fortran routines:
+
+  init_domain(input_text, base_dir)   -> HostDomain   (domain.f90:45-378 + main.f90:57-116)
+  GpuDomain(host).time_step_LS(t, dt, final_step)     (time_step.f90:71-167)
+  GpuDomain(host).run(n_first, n_last)                (main.f90:168-231 loop body)
+
+Errors raise FdmapError where the reference would call error() / stop.
+The arrays returned use FDMAP's global layout F(i, j, l) (Fortran order),
+exposed as numpy arrays of shape (nF, ny, nx).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from . import native
+from .native import FAULT_INDEX, check_gpu, check_host, dptr, lib
+
+
+class HostDomain:
+    """An initialised FDMAP domain held in host memory (the Fortran driver's state)."""
+
+    def __init__(self, input_text: str, base_dir: str | Path | None = None):
+        self._h = C.c_void_p()
+        base = str(base_dir).encode() if base_dir is not None else None
+        check_host(lib().fdmap_host_init(input_text.encode(), base, C.byref(self._h)), "init_domain")
+        ints = (C.c_int * 8)()
+        dbls = (C.c_double * 5)()
+        check_host(lib().fdmap_host_info(self._h, ints, dbls), "fdmap_host_info")
+        (self.mode, self.nF, self.nx, self.ny, self.nblocks, self.nifaces, self.nt, self.rk_order) = list(ints)
+        (self.t0, self.dt, self.CFL, self.hmin, self.hmax) = list(dbls)
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def desc(self) -> C.c_void_p:
+        return C.c_void_p(lib().fdmap_host_desc(self._h))
+
+    def array(self, name: str) -> np.ndarray:
+        """View of a body array ("F", "DF", "x", "y", "xq", ...), shape (k, ny, nx)."""
+        n = C.c_longlong()
+        p = lib().fdmap_host_array(self._h, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        a = np.ctypeslib.as_array(p, shape=(n.value,))
+        k = n.value // (self.nx * self.ny)
+        return a.reshape(k, self.ny, self.nx)
+
+    def iface_n(self, iface: int) -> int:
+        n = lib().fdmap_host_iface_n(self._h, iface)
+        if n < 0:
+            check_host(n, "fdmap_host_iface_n")
+        return n
+
+    def block_limits(self, b: int) -> tuple[int, int, int, int]:
+        lim = (C.c_int * 4)()
+        check_host(lib().fdmap_host_block_limits(self._h, b, lim), "fdmap_host_block_limits")
+        return tuple(lim)
+
+    def close(self) -> None:
+        if self._h:
+            lib().fdmap_host_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def init_domain(input_text: str, base_dir: str | Path | None = None) -> HostDomain:
+    """Parse an FDMAP .in text and initialise the domain on the host."""
+    return HostDomain(input_text, base_dir)
+
+
+class GpuDomain:
+    """Device-resident copy of a domain, advanced by the sm_100a kernels."""
+
+    def __init__(self, host: HostDomain, device: int = 0, init_edges: bool = True):
+        self.host = host
+        self.nx, self.ny, self.nF = host.nx, host.ny, host.nF
+        self._g = C.c_void_p()
+        check_gpu(lib().fdmap_gpu_create(host.desc, device, int(init_edges), C.byref(self._g)), "fdmap_gpu_create")
+
+    def time_step_LS(self, t0: float, dt: float, final_step: bool = False) -> None:
+        check_gpu(lib().fdmap_gpu_time_step(self._g, t0, dt, int(final_step)), "time_step_LS")
+
+    def run(self, n_first: int, n_last: int, t_start: float | None = None, dt: float | None = None,
+            nt: int | None = None) -> None:
+        h = self.host
+        check_gpu(lib().fdmap_gpu_run(self._g, h.t0 if t_start is None else t_start, h.dt if dt is None else dt,
+                                      n_first, n_last, h.nt if nt is None else nt), "fdmap_gpu_run")
+
+    def synchronize(self) -> None:
+        check_gpu(lib().fdmap_gpu_synchronize(self._g), "fdmap_gpu_synchronize")
+
+    def get_fields(self, want_F: bool = True, want_DF: bool = False):
+        F = np.empty((self.nF, self.ny, self.nx)) if want_F else None
+        DF = np.empty((self.nF, self.ny, self.nx)) if want_DF else None
+        check_gpu(lib().fdmap_gpu_get_fields(self._g, dptr(F), dptr(DF)), "fdmap_gpu_get_fields")
+        return F, DF
+
+    def set_fields(self, F=None, DF=None) -> None:
+        F = None if F is None else np.ascontiguousarray(F, dtype=np.float64)
+        DF = None if DF is None else np.ascontiguousarray(DF, dtype=np.float64)
+        check_gpu(lib().fdmap_gpu_set_fields(self._g, dptr(F), dptr(DF)), "fdmap_gpu_set_fields")
+
+    def get_fault(self, iface: int, field: str) -> np.ndarray:
+        out = np.empty(self.host.iface_n(iface))
+        check_gpu(lib().fdmap_gpu_get_fault(self._g, iface, FAULT_INDEX[field], dptr(out)), "fdmap_gpu_get_fault")
+        return out
+
+    def set_fault(self, iface: int, field: str, values) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        check_gpu(lib().fdmap_gpu_set_fault(self._g, iface, FAULT_INDEX[field], dptr(v)), "fdmap_gpu_set_fault")
+
+    def get_fhat(self, b: int, s: int) -> np.ndarray:
+        mgx, pgx, mgy, pgy = self.host.block_limits(b)
+        n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+        out = np.empty(n * self.nF)
+        check_gpu(lib().fdmap_gpu_get_fhat(self._g, b, s, dptr(out)), "fdmap_gpu_get_fhat")
+        return out.reshape(self.nF, n)
+
+    def newton_failures(self) -> int:
+        n = C.c_longlong()
+        lib().fdmap_gpu_status(self._g, C.byref(n))
+        return n.value
+
+    def launch_count(self) -> int:
+        return lib().fdmap_gpu_launch_count(self._g)
+
+    def device_bytes(self) -> int:
+        return lib().fdmap_gpu_device_bytes(self._g)
+
+    def close(self) -> None:
+        if self._g:
+            lib().fdmap_gpu_destroy(self._g)
+            self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

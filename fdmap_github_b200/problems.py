@@ -1,0 +1,182 @@
+"""FDMAP input files (.in namelists + binary side files) for the benchmark
+configurations.  The texts use only FDMAP's own input vocabulary, so the same
+files drive FDMAP itself, the host initialisation here and the CPU oracle.
+
+Units follow FDMAP: km, s, m/s, MPa, g/cm^3, km/s (2670 kg/m^3 -> 2.67,
+3464 m/s -> 3.464, 25 m -> 0.025).
+
+  antiplane_pulse      mode III SH pulse, one Cartesian block          (config "c1")
+  rupture_sw           mode II slip-weakening rupture, two blocks      (config "c2")
+  rough_fault_rs       mode II rate-and-state on a rough fault         (config "c3")
+  heterogeneous_ricker mode III heterogeneous medium, Ricker point force (config "c5")
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+
+def _f(x: float) -> str:
+    """Fortran double literal."""
+    return repr(float(x)).replace("e", "d") if "e" in repr(float(x)) else repr(float(x)) + "d0"
+
+
+def antiplane_pulse(n: int = 201, L: float = 10.0, nt: int = 501, rk: int = 4, cfl: float = 0.5,
+                    fd: str = "SBP4", sigma: float = 0.5, amp: float = 1.0) -> str:
+    """Mode III SH wave from a Gaussian velocity pulse at the centre of an L x L km
+    block of n x n nodes, absorbing SAT boundaries on all sides."""
+    c = 0.5 * L
+    return f"""&problem_list name='antiplane_pulse', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
+&domain_list mode=3, FDmethod='{fd}', nblocks_x=1, nblocks_y=1 /
+!---BLOCK1---
+&grid_list nx={n}, ny={n}, LB=0d0,0d0, LT=0d0,{_f(L)}, RB={_f(L)},0d0, RT={_f(L)},{_f(L)} /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='absorbing' /
+&material_list rho=2.67d0, cs=3.464d0 /
+&fields_list P5%shape='gaussian', P5%x0={_f(c)}, P5%y0={_f(c)}, P5%Lx={_f(sigma)}, P5%Ly={_f(sigma)}, P5%vz={_f(amp)} /
+"""
+
+
+def rupture_sw(nx: int = 1601, ny: int = 801, h: float = 0.025, nt: int = 4001, rk: int = 4, cfl: float = 0.5,
+               fd: str = "SBP4", patch_half_width: float = 1.5) -> str:
+    """Mode II dynamic rupture on a planar fault y = 0 between two blocks of
+    nx x ny nodes (spacing h km), linear slip-weakening friction, uniform
+    prestress syy = -110 MPa, sxy = 65 MPa, and an 80 MPa nucleation patch."""
+    Lx = (nx - 1) * h
+    Ly = (ny - 1) * h
+    x0, x1 = -0.5 * Lx, 0.5 * Lx
+    blk = """&material_list rho=2.67d0, cs=3.464d0, cp=6d0 /
+&fields_list syy0=-110d0, sxy0=65d0 /
+"""
+    return f"""&problem_list name='rupture_sw', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
+&domain_list mode=2, FDmethod='{fd}', nblocks_x=1, nblocks_y=2 /
+!---BLOCK1---
+&grid_list nx={nx}, ny={ny}, LB={_f(x0)},{_f(-Ly)}, LT={_f(x0)},0d0, RB={_f(x1)},{_f(-Ly)}, RT={_f(x1)},0d0 /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='none' /
+{blk}!---BLOCK2---
+&grid_list nx={nx}, ny={ny}, LB={_f(x0)},0d0, LT={_f(x0)},{_f(Ly)}, RB={_f(x1)},0d0, RT={_f(x1)},{_f(Ly)} /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='none', bcT='absorbing' /
+{blk}!---IFACE1---
+&interface_list coupling='friction' /
+&friction_list friction_law='SW', sw%fs=0.68d0, sw%fd=0.52d0, sw%Dc=0.4d0,
+  ld%shape='boxcar', ld%R={_f(patch_half_width)}, ld%S=15d0, ld%x0=0d0,
+  rup_field='V', rup_threshold=1d-3 /
+"""
+
+
+def fractal_profile(x: np.ndarray, alpha: float, lambda_min: float, seed: int) -> tuple[np.ndarray, np.ndarray]:
+    """Seeded band-limited self-similar profile y(x) (power spectral density
+    proportional to k^-3, i.e. Hurst exponent 1) with rms amplitude alpha*L and
+    wavelengths between lambda_min and the profile length L; returns (y, dy/dx)."""
+    rng = np.random.default_rng(seed)
+    n = x.size
+    L = x[-1] - x[0]
+    m = 4 * n
+    k = np.fft.rfftfreq(m, d=(x[1] - x[0]))
+    amp = np.zeros_like(k)
+    band = (k >= 1.0 / L) & (k <= 1.0 / lambda_min)
+    amp[band] = k[band] ** -1.5
+    spec = amp * np.exp(2j * np.pi * rng.random(k.size))
+    y = np.fft.irfft(spec, n=m)[:n]
+    dy = np.fft.irfft(spec * 2j * np.pi * k, n=m)[:n]
+    scale = alpha * L / np.sqrt(np.mean(y ** 2))
+    y = y * scale
+    dy = dy * scale
+    y = y - y[0]  # anchor the left end at y = 0
+    return y, dy
+
+
+def _write(path: Path, *arrays) -> None:
+    np.concatenate([np.asarray(a, dtype=np.float64).ravel() for a in arrays]).tofile(path)
+
+
+def rough_fault_rs(outdir: str | Path, nx: int = 2001, ny: int = 1001, h: float = 0.02, nt: int = 6001, rk: int = 4,
+                   cfl: float = 0.5, fd: str = "SBP4", seed: int = 0, alpha: float = 1e-3, Vinit: float = 1e-12,
+                   tp: bool = False) -> str:
+    """Mode II regularised rate-and-state (flash-heating slip law 'RFL') on a
+    rough fault between two curvilinear blocks.  Writes the fault curve, the
+    background-stress file and the initial-state file into outdir and returns
+    the input text (file names relative to outdir)."""
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    Lx, Ly = (nx - 1) * h, (ny - 1) * h
+    x = np.linspace(-0.5 * Lx, 0.5 * Lx, nx)
+    y, dy = fractal_profile(x, alpha, 20 * h, seed)
+    nrm = np.sqrt(1.0 + dy ** 2)
+    # curve file (grid.f90:683-695): x, y, n1, n2; the stored normal points out of
+    # the upper block (downwards); the lower block's T side flips it (grid.f90:453)
+    _write(out / "fault.curve", x, y, dy / nrm, -1.0 / nrm)
+    # depth-dependent effective normal stress capped at 120 MPa, shear at 0.6 N
+    depth = x - x[0]
+    N0 = np.minimum(120.0, 20.0 + 10.0 * depth)
+    a, b, V0, f0, L, fw, Vw = 0.01, 0.014, 1e-6, 0.6, 0.4, 0.2, 0.1
+    fss = f0 - (b - a) * np.log(Vinit / V0)
+    S0 = 0.6 * N0
+    _write(out / "stress.dat", S0, N0)
+    # state giving slip velocity Vinit under the background stress (strength()
+    # of friction.f90:1066-1071 inverted for Psi)
+    Psi = a * np.log(2.0 * V0 / Vinit * np.sinh(S0 / (a * N0)))
+    _write(out / "state.dat", Psi)
+    del fss
+    xa, xb = x[0], x[-1]
+    ya, yb = y[0], y[-1]
+    tp_list = "&thermpres_list n=64, p0=0d0 /\n" if tp else ""
+    blk = """&material_list rho=2.67d0, cs=3.464d0, cp=6d0 /
+"""
+    return f"""&problem_list name='rough_fault_rs', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
+&domain_list mode=2, FDmethod='{fd}', nblocks_x=1, nblocks_y=2 /
+!---BLOCK1---
+&grid_list nx={nx}, ny={ny}, LB={_f(xa)},{_f(-Ly)}, LT={_f(xa)},{_f(ya)}, RB={_f(xb)},{_f(-Ly)}, RT={_f(xb)},{_f(yb)},
+  bndTfile='fault.curve' /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='none' /
+{blk}!---BLOCK2---
+&grid_list nx={nx}, ny={ny}, LB={_f(xa)},{_f(ya)}, LT={_f(xa)},{_f(Ly)}, RB={_f(xb)},{_f(yb)}, RT={_f(xb)},{_f(Ly)},
+  bndBfile='fault.curve' /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='none', bcT='absorbing' /
+{blk}!---IFACE1---
+&interface_list coupling='friction' /
+&friction_list friction_law='RFL', rs%a={_f(a)}, rs%b={_f(b)}, rs%V0={_f(V0)}, rs%f0={_f(f0)}, rs%L={_f(L)},
+  rs%fw={_f(fw)}, rs%Vw={_f(Vw)}, stress_file=T, stress_filename='stress.dat',
+  state_file=T, state_filename='state.dat',
+  ld%shape='gaussian', ld%R=1.5d0, ld%S=25d0, ld%x0={_f(0.25 * Lx * 0 + x[nx // 2])},
+  rup_field='V', rup_threshold=1d-3 /
+{tp_list}"""
+
+
+def heterogeneous_ricker(outdir: str | Path, n: int = 801, h: float = 0.02, nt: int = 2001, rk: int = 4,
+                         cfl: float = 0.5, fd: str = "SBP4", seed: int = 0, std: float = 0.1, corr: float = 0.4,
+                         f_peak: float = 5.0, rho_scale: float = 1.0) -> str:
+    """Mode III wave in a heterogeneous block: shear modulus and density are
+    seeded Gaussian random fields (relative std `std`, correlation length
+    `corr` km) about 32 GPa and 2.67 g/cm^3; Ricker point force at a seeded node."""
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    L = (n - 1) * h
+
+    def grf(r):
+        w = r.standard_normal((n, n))
+        k = np.fft.fftfreq(n, d=h)
+        kx, ky = np.meshgrid(k, k, indexing="ij")
+        filt = np.exp(-0.5 * (2 * np.pi) ** 2 * (kx ** 2 + ky ** 2) * (corr / 2) ** 2)
+        g = np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
+        return g / g.std()
+
+    rho = 2.67 * rho_scale * (1.0 + std * grf(rng))
+    G = 32.0 * (1.0 + std * grf(rng))
+    cs = np.sqrt(G / rho)
+    cp = np.sqrt(3.0) * cs
+    # medium file (material.f90:278-321): rho, cs, cp over the global grid, i fastest
+    _write(out / "medium.dat", rho.T, cs.T, cp.T)
+    i0, j0 = rng.integers(n // 4, 3 * n // 4, size=2)
+    x0, y0 = i0 * h + 0.37 * h, j0 * h + 0.61 * h
+    T = 1.0 / f_peak
+    return f"""&problem_list name='heterogeneous_ricker', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
+&domain_list mode=3, FDmethod='{fd}', nblocks_x=1, nblocks_y=1 /
+!---BLOCK1---
+&grid_list nx={n}, ny={n}, LB=0d0,0d0, LT=0d0,{_f(L)}, RB={_f(L)},0d0, RT={_f(L)},{_f(L)} /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='free' /
+&material_list heterogeneous=T, filename='medium.dat', rho=2.67d0, cs=3.464d0 /
+!---END---
+&source_list x0={_f(x0)}, y0={_f(y0)}, Fz=1d0, source_time_function='Ricker', t_center={_f(1.2 * T)}, t_duration={_f(T)} /
+"""

@@ -1,0 +1,83 @@
+/*
+ * fdmap_gpu.h -- C ABI of the B200 time-stepping engine for FDMAP.
+ *
+ * Drop-in boundary: a Fortran driver that has run init_domain keeps its time
+ * loop (main.f90:168-231) and replaces the body of time_step_LS
+ * (time_step.f90:96-165: scale_rates_all, prepare_edges,
+ * enforce_edge_conditions, set_rates_all, update_fields_all, exchange_fields)
+ * by one call per step.  Plain C types only; fortran/fdmap_gpu_mod.f90 holds
+ * the matching bind(C) interfaces.
+ *
+ * Conventions
+ *  - every entry point returns FDMAP_OK (0) or a negative FDMAP_ERR_* code; the
+ *    library never aborts or traps (the reference's error() -> MPI_Abort and
+ *    Newton double failure -> stop become error codes);
+ *  - host arrays are only borrowed for the duration of a call; all state lives
+ *    on the device, owned by the handle;
+ *  - one handle per host thread; step calls are asynchronous on the handle's
+ *    stream, fdmap_gpu_get_* and fdmap_gpu_synchronize block.
+ */
+#ifndef FDMAP_GPU_H
+#define FDMAP_GPU_H
+
+#include "fdmap_desc.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fdmap_gpu fdmap_gpu;
+
+/* Copies the domain to device `device` and, when `init_edges` is non-zero,
+ * runs enforce_edge_conditions(D, 0) at d->t0 as init_domain does
+ * (domain.f90:346-356): initial hat variables, slip velocity and Nreg.
+ * Replaces: the device-resident half of init_domain (domain.f90:45-378). */
+int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu** h);
+
+/* enforce_edge_conditions(D, 0d0) at time t (domain.f90:442-471 with dt = 0). */
+int fdmap_gpu_init_edges(fdmap_gpu* h, double t);
+
+/* One low-storage RK step from t0 (time_step_LS, time_step.f90:71-167).
+ * final_step != 0 evaluates stage-1 rates and fault solve only, as the
+ * reference does on its last loop index (time_step.f90:133). */
+int fdmap_gpu_time_step(fdmap_gpu* h, double t0, double dt, int final_step);
+
+/* The main-loop body for n = n_first..n_last: t = t_start + (n-1)*dt, final
+ * step when n == nt (main.f90:168-187).  Steps are issued as CUDA graphs. */
+int fdmap_gpu_run(fdmap_gpu* h, double t_start, double dt, int n_first, int n_last, int nt);
+
+int fdmap_gpu_synchronize(fdmap_gpu* h);
+
+/* Body fields F(nx,ny,nF) and rates DF(nx,ny,nF) in FDMAP's global
+ * column-major layout; either pointer may be NULL.  Blocks the host. */
+int fdmap_gpu_get_fields(fdmap_gpu* h, double* F, double* DF);
+int fdmap_gpu_set_fields(fdmap_gpu* h, const double* F, const double* DF);
+
+/* One FDMAP_FAULT_* field of interface `iface` (0-based), p-m+1 values. */
+int fdmap_gpu_get_fault(fdmap_gpu* h, int iface, int field, double* out);
+int fdmap_gpu_set_fault(fdmap_gpu* h, int iface, int field, const double* in);
+
+/* Hat variables Fhat(n,nF) of side s (0..3 = L,R,B,T) of block b. */
+int fdmap_gpu_get_fhat(fdmap_gpu* h, int b, int s, double* out);
+
+/* Device status: Newton failures so far (the reference stops on the first). */
+int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
+
+/* Kernel launches issued by the last fdmap_gpu_run / time_step call. */
+long long fdmap_gpu_launch_count(fdmap_gpu* h);
+
+/* Device bytes held by the handle. */
+long long fdmap_gpu_device_bytes(fdmap_gpu* h);
+
+void fdmap_gpu_destroy(fdmap_gpu* h);
+
+const char* fdmap_gpu_strerror(int code);
+
+/* Last CUDA / validation message on this thread. */
+const char* fdmap_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDMAP_GPU_H */

@@ -1,0 +1,65 @@
+/*
+ * fdmap_host.h -- host-side domain initialisation.
+ *
+ * In a production FDMAP run the Fortran driver performs init_domain
+ * (domain.f90:45-378) itself and passes the resulting arrays to the GPU engine
+ * through fdmap_desc.  This library ships a C++ restatement of that
+ * initialisation so that FDMAP's own namelist input files (the `.in` format read
+ * by main.f90:29-78 and the per-block/per-interface lists) can drive the GPU
+ * engine without the Fortran toolchain.  It reads:
+ *   problem_list, domain_list, and per '!---BLOCKn---' grid_list,
+ *   boundaries_list, material_list, fields_list, operator_list; per
+ *   '!---IFACEn---' interface_list, friction_list, thermpres_list; source_list;
+ * plus the binary side files FDMAP reads (curve files, heterogeneous medium,
+ * friction / stress / state files), all real*8 in native byte order.
+ */
+#ifndef FDMAP_HOST_H
+#define FDMAP_HOST_H
+
+#include "fdmap_desc.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fdmap_domain fdmap_domain; /* owns every array the descriptor points to */
+
+/* Parse `input_text` (contents of an FDMAP .in file) and initialise the domain.
+ * Relative file names inside the input are resolved against `base_dir`
+ * (may be NULL = current directory).  Replaces init_domain + the time-loop
+ * setup of main.f90:57-116.  Returns FDMAP_OK or a negative FDMAP_ERR_*;
+ * fdmap_host_last_error() then describes the failure. */
+int fdmap_host_init(const char* input_text, const char* base_dir, fdmap_domain** out);
+
+/* The descriptor of an initialised domain (owned by the domain). */
+const fdmap_desc* fdmap_host_desc(const fdmap_domain* dom);
+
+/* Mutable access for callers that seed states before handing the domain over. */
+fdmap_desc* fdmap_host_desc_mut(fdmap_domain* dom);
+
+void fdmap_host_free(fdmap_domain* dom);
+
+/* Scalar summary for bindings without struct support:
+ * ints[8]  = mode, nF, nx, ny, nblocks, nifaces, nt, rk_order
+ * dbls[5]  = t0, dt, CFL, hmin, hmax */
+int fdmap_host_info(const fdmap_domain* dom, int* ints, double* dbls);
+
+/* Number of nodes p-m+1 of interface `iface` (0-based), or a negative code. */
+int fdmap_host_iface_n(const fdmap_domain* dom, int iface);
+
+/* Block index limits: lim[4] = mgx, pgx, mgy, pgy (1-based). */
+int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim);
+
+/* Pointer to a body array owned by the domain ("F", "DF", "x", "y", "xq", "xr",
+ * "yq", "yr", "J", "Ji", "rho", "cs", "cp", "G", "M", "gamma", "nu"); *count
+ * receives its length.  NULL if the name is unknown or the array is absent. */
+double* fdmap_host_array(fdmap_domain* dom, const char* name, long long* count);
+
+/* Human-readable description of the last error on this thread. */
+const char* fdmap_host_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FDMAP_HOST_H */

@@ -1,0 +1,108 @@
+"""ctypes binding of the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg.  It
+consumes the same fdmap_desc a HostDomain produces.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .build import LIB, build_oracle
+
+FAULT_FIELDS = ["D", "Psi", "DPsi", "trup", "V", "O", "S", "N", "S0", "N0",
+                "Ds", "Dn", "DDs", "DDn", "W", "DW", "Nreg", "DNreg"]
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build_oracle()
+        L = C.CDLL(str(LIB))
+        _DP = C.POINTER(C.c_double)
+        L.oracle_create.restype = C.c_void_p
+        L.oracle_create.argtypes = [C.c_void_p]
+        L.oracle_destroy.argtypes = [C.c_void_p]
+        L.oracle_init_edges.argtypes = [C.c_void_p, C.c_double]
+        L.oracle_time_step.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int]
+        L.oracle_run.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]
+        L.oracle_get_fields.argtypes = [C.c_void_p, _DP, _DP]
+        L.oracle_set_fields.argtypes = [C.c_void_p, _DP, _DP]
+        L.oracle_get_fault.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
+        L.oracle_get_fhat.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
+        L.oracle_newton_failures.restype = C.c_longlong
+        L.oracle_newton_failures.argtypes = [C.c_void_p]
+        L.oracle_num_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class OracleDomain:
+    """CPU restatement of FDMAP's time stepping on a copy of a HostDomain."""
+
+    def __init__(self, host, init_edges: bool = True):
+        self.host = host
+        self.nx, self.ny, self.nF = host.nx, host.ny, host.nF
+        self._o = lib().oracle_create(host.desc)
+        if not self._o:
+            raise RuntimeError("oracle_create rejected the descriptor")
+        if init_edges:
+            lib().oracle_init_edges(self._o, host.t0)
+
+    def time_step_LS(self, t0: float, dt: float, final_step: bool = False) -> None:
+        lib().oracle_time_step(self._o, t0, dt, int(final_step))
+
+    def run(self, n_first: int, n_last: int, t_start=None, dt=None, nt=None) -> None:
+        h = self.host
+        lib().oracle_run(self._o, h.t0 if t_start is None else t_start, h.dt if dt is None else dt,
+                         n_first, n_last, h.nt if nt is None else nt)
+
+    def get_fields(self, want_F: bool = True, want_DF: bool = False):
+        F = np.empty((self.nF, self.ny, self.nx)) if want_F else None
+        DF = np.empty((self.nF, self.ny, self.nx)) if want_DF else None
+        lib().oracle_get_fields(self._o, _p(F), _p(DF))
+        return F, DF
+
+    def set_fields(self, F=None, DF=None) -> None:
+        F = None if F is None else np.ascontiguousarray(F, dtype=np.float64)
+        DF = None if DF is None else np.ascontiguousarray(DF, dtype=np.float64)
+        lib().oracle_set_fields(self._o, _p(F), _p(DF))
+
+    def get_fault(self, iface: int, field: str) -> np.ndarray:
+        out = np.empty(self.host.iface_n(iface))
+        rc = lib().oracle_get_fault(self._o, iface, FAULT_FIELDS.index(field), _p(out))
+        if rc != 0:
+            raise RuntimeError(f"oracle_get_fault failed ({rc})")
+        return out
+
+    def get_fhat(self, b: int, s: int) -> np.ndarray:
+        mgx, pgx, mgy, pgy = self.host.block_limits(b)
+        n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+        out = np.empty(n * self.nF)
+        lib().oracle_get_fhat(self._o, b, s, _p(out))
+        return out.reshape(self.nF, n)
+
+    def newton_failures(self) -> int:
+        return lib().oracle_newton_failures(self._o)
+
+    def close(self) -> None:
+        if self._o:
+            lib().oracle_destroy(self._o)
+            self._o = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def num_threads() -> int:
+    return lib().oracle_num_threads()

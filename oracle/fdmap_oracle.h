@@ -1,0 +1,72 @@
+/*
+ * fdmap_oracle.h -- CPU restatement of FDMAP's explicit time step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the parity oracle the GPU engine is
+ * checked against, and the timed CPU baseline of bench.py.  Nothing in the
+ * product (fdmap_github_b200/) links, imports or calls it.
+ *
+ * It restates, routine by routine and in the same floating-point evaluation
+ * order, FDMAP's time_step_LS (time_step.f90:71-167) and everything it calls
+ * for the elastic + interface configurations: scale/update of rates
+ * (fields.f90:1061-1242), prepare_edges (domain.f90:420-439, 1325-1346),
+ * boundary conditions (boundaries.f90:74-377), locked and frictional
+ * interfaces (interfaces.f90:520-1012), friction (friction.f90:555-1506),
+ * SAT penalties (time_step.f90:754-851), SBP rates (rates.f90:8-936,
+ * rates_heterogeneous.f90:8-917) and point sources (source.f90:147-406).
+ *
+ * Parity status: the reference (Fortran 90 + MPI) cannot be compiled or run
+ * in this environment and ships no golden vectors or test fixtures, so this
+ * restatement is "parity unpinned" against reference outputs.  It is pinned
+ * instead against known answers that follow from the reference's own
+ * definitions: SBP identities of the literal coefficient tables, exactness of
+ * the operators on low-order polynomials, manufactured-solution convergence,
+ * discrete energy decay, Newton residuals below the reference's atolR, and
+ * closed-form characteristic boundary solutions.
+ */
+#ifndef FDMAP_ORACLE_H
+#define FDMAP_ORACLE_H
+
+#include "../include/fdmap_desc.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct oracle_domain oracle_domain;
+
+/* Deep-copies the descriptor.  Returns NULL on invalid input. */
+oracle_domain* oracle_create(const fdmap_desc* d);
+void oracle_destroy(oracle_domain* o);
+
+/* enforce_edge_conditions(D, 0d0) at time t, as init_domain does
+ * (domain.f90:346-356): sets Fhat, initial slip velocity, Nreg. */
+int oracle_init_edges(oracle_domain* o, double t);
+
+/* One time_step_LS call at time t0 with step dt (time_step.f90:71-167). */
+int oracle_time_step(oracle_domain* o, double t0, double dt, int final_step);
+
+/* main.f90 time loop for n = n_first..n_last: t = t_start + (n-1)*dt,
+ * final step when n == nt. */
+int oracle_run(oracle_domain* o, double t_start, double dt, int n_first, int n_last, int nt);
+
+/* (nx,ny,nF) body fields and rates; either pointer may be NULL. */
+int oracle_get_fields(const oracle_domain* o, double* F, double* DF);
+int oracle_set_fields(oracle_domain* o, const double* F, const double* DF);
+
+/* Fault field `field` (FDMAP_FAULT_* in fdmap_gpu.h order) of interface iface. */
+int oracle_get_fault(const oracle_domain* o, int iface, int field, double* out);
+
+/* Hat variables of side s (0..3) of block b: (n, nF). */
+int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out);
+
+/* Number of Newton failures seen so far (the reference warns and retries). */
+long long oracle_newton_failures(const oracle_domain* o);
+
+/* Number of OpenMP threads the oracle uses (1 when built without OpenMP). */
+int oracle_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
