@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the FDMAP time-stepping hot path on B200.
+
+Workload (default "rupture"): mode II dynamic rupture, two blocks of
+1601 x 801 nodes (dx = 25 m) joined at a planar slip-weakening fault, LS-RK4
+at CFL 0.5 -- the configuration the headline metric is quoted on.  A step is
+one full low-storage RK4 time step (5 stages) over all 2,564,802 nodes.
+
+  value   FP64 node-updates/s of the whole job (all ranks), device-resident state,
+          K steps timed with CUDA events on the engine's stream
+  e2e     the same metric through the public C ABI with host buffers: the
+          initial state upload, the per-step fault output read-back (slip,
+          slip rate, shear stress, rupture time) and the final field
+          download are inside the timed region
+  roofline  the fused stencil kernel's achieved HBM bandwidth (algorithmic
+          bytes per launch / its mean CUDA-event duration) against the measured
+          copy bandwidth
+
+Multi-GPU: one replica per rank (weak scaling), no data-path collective.
+`--impl reference` times the CPU restatement of the reference (the Fortran/MPI
+reference cannot be built in this image) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from fdmap_github_b200 import GpuDomain, init_domain, problems  # noqa: E402
+from fdmap_github_b200.native import FAULT_INDEX  # noqa: E402
+
+METRIC = "FP64 node-updates/s"
+UNIT = "node-updates/s"
+
+# Algorithmic HBM bytes per node per RK stage of the fused stencil kernel
+# (compulsory reads and writes of one stage; see DESIGN.md "Roofline"):
+#   mode II: F 6 read + 6 write, DF 5 read + 6 write, metrics xq,xr,yq,yr,Ji 5 read
+#   mode III: F 3+3, DF 3+3, metrics 5;  heterogeneous adds rho,G (III) / 5 arrays (II)
+BYTES_PER_NODE_STAGE = {(2, False): 28 * 8, (2, True): 33 * 8, (3, False): 17 * 8, (3, True): 19 * 8}
+
+
+def workload(name: str, tmpdir: Path):
+    if name == "rupture":
+        return problems.rupture_sw(), None, {"workload": "mode II slip-weakening rupture, 2 blocks x 1601x801, dx 25 m, LS-RK4 CFL 0.5",
+                                             "nodes": 1601 * 1602, "fault_nodes": 1601}
+    if name == "pulse":
+        return problems.antiplane_pulse(), None, {"workload": "mode III SH pulse, 1 block 201x201, LS-RK4 CFL 0.5", "nodes": 201 * 201}
+    if name == "roughfault":
+        text = problems.rough_fault_rs(tmpdir)
+        return text, tmpdir, {"workload": "mode II rate-and-state (RFL) rough fault, 2 curvilinear blocks x 2001x1001",
+                              "nodes": 2001 * 2002, "fault_nodes": 2001}
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(config_key: str):
+    """DRAM bytes per stencil launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "stencil_kernel_ncu.md"
+    if not p.exists():
+        return None
+    m = re.search(rf"traffic_bytes_per_launch\[{config_key}\]\s*=\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def barrier_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_gpu(args) -> None:
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    tmp = ROOT / "_bench_tmp" / f"rank{rank}"
+    text, base, info = workload(args.workload, tmp)
+    host = init_domain(text, base)
+    nodes = host.nx * host.ny
+    het = host.heterogeneous
+    stream = torch.cuda.current_stream()
+
+    # ---- device-resident throughput (value)
+    g = GpuDomain(host, device=local)
+    lib_set_stream(g, stream)
+    nt_inf = 1 << 30
+    g.run(1, args.warmup, nt=nt_inf)
+    g.synchronize()
+    barrier(world)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier(world)
+        start.record(stream)
+        g.run(args.warmup + 1, args.warmup + args.steps, nt=nt_inf)
+        stop.record(stream)
+        stop.synchronize()
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(stop)
+    ms_max = barrier_max(ms, world)
+    launches = g.launch_count()
+    value = world * nodes * args.steps / (ms_max * 1e-3)
+
+    # ---- per-kernel durations for the roofline (same kernels, event-bracketed)
+    from fdmap_github_b200.native import lib
+    import ctypes as C
+
+    lib().fdmap_gpu_profile(g._g, 1)
+    g.run(args.warmup + args.steps + 1, args.warmup + 2 * args.steps, nt=nt_inf)
+    kms = (C.c_double * 3)()
+    kn = (C.c_longlong * 3)()
+    lib().fdmap_gpu_profile_read(g._g, kms, kn)
+    lib().fdmap_gpu_profile(g._g, 0)
+    stencil_ms = kms[0] / max(kn[0], 1)
+    closure_ms = kms[1] / max(kn[1], 1)
+    edge_ms = kms[2] / max(kn[2], 1)
+    bps = BYTES_PER_NODE_STAGE[(host.mode, het)]
+    alg_bytes = bps * interior_nodes(host)
+    achieved = alg_bytes / (stencil_ms * 1e-3) / 1e9
+    peaks = measured_peaks()
+    newton_fail = g.newton_failures()
+    g.close()
+
+    # ---- end to end through the public API with host buffers
+    g2 = GpuDomain(host, device=local, init_edges=False)
+    lib_set_stream(g2, stream)
+    F0 = np.ascontiguousarray(host.array("F"))
+    DF0 = np.ascontiguousarray(host.array("DF"))
+    pin_F = torch.from_numpy(F0).pin_memory()
+    pin_DF = torch.from_numpy(DF0).pin_memory()
+    nf = info.get("fault_nodes", 0)
+    out_fault = torch.empty((4, max(nf, 1)), dtype=torch.float64).pin_memory()
+    Fout = torch.empty_like(pin_F).pin_memory()
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    g2.set_fields(pin_F.numpy(), pin_DF.numpy())
+    lib().fdmap_gpu_init_edges(g2._g, host.t0)
+    for n in range(1, args.steps + 1):
+        g2.run(n, n, nt=nt_inf)
+        if nf:
+            for k, f in enumerate(("D", "V", "S", "trup")):
+                lib().fdmap_gpu_get_fault(g2._g, 0, FAULT_INDEX[f],
+                                          out_fault[k].numpy().ctypes.data_as(C.POINTER(C.c_double)))
+    F_final, _ = g2.get_fields()
+    e_stop.record(stream)
+    e_stop.synchronize()
+    e_ms = max(e_start.elapsed_time(e_stop), (time.perf_counter() - t0) * 1e3)
+    e_ms = barrier_max(e_ms, world)
+    e2e = world * nodes * args.steps / (e_ms * 1e-3)
+    h2d = (F0.nbytes + DF0.nbytes) / args.steps
+    d2h = (4 * nf * 8) + F0.nbytes / args.steps
+    g2.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(host, args)
+
+    if rank == 0:
+        ck = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {**info, "parallelism": f"replicas{world}", "rk_stages_per_step": 5,
+                       "l2": "inputs larger than L2 (state ~0.5 GB)", "nt_reference": host.nt},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload),
+                         "kernel": "stencil_kernel", "alg_bytes_per_launch": alg_bytes,
+                         "mean_launch_ms": stencil_ms, "closure_kernel_mean_ms": closure_ms,
+                         "interface_kernel_mean_ms": edge_ms,
+                         "peak_source": peaks["source"]},
+            "clocks": ck,
+            "gpu_launches": launches,
+            "newton_failures": newton_fail,
+        }
+        if cpu is not None:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def interior_nodes(host) -> int:
+    """Nodes handled by the interior kernel: all but the SBP closure strips."""
+    nbst = {2: 1, 4: 4, 6: 6}
+    fd = host.fd_method
+    n = 0
+    for b in range(host.nblocks):
+        mgx, pgx, mgy, pgy = host.block_limits(b)
+        nx, ny = pgx - mgx + 1, pgy - mgy + 1
+        n += max(nx - 2 * nbst[fd], 0) * max(ny - 2 * nbst[fd], 0)
+    return n
+
+
+def lib_set_stream(g, stream) -> None:
+    from fdmap_github_b200.native import check_gpu, lib
+
+    check_gpu(lib().fdmap_gpu_set_stream(g._g, stream.cuda_stream), "fdmap_gpu_set_stream")
+
+
+def cpu_baseline(host, args, seconds: float = 15.0) -> dict:
+    """The oracle (CPU restatement of the reference's time step) on the host
+    cores, timed on a bounded number of steps of the same workload."""
+    from oracle.binding import OracleDomain, num_threads
+
+    o = OracleDomain(host)
+    o.run(1, 1, nt=1 << 30)  # warm-up step
+    n, t0 = 0, time.perf_counter()
+    while True:
+        n += 1
+        o.run(1 + n, 1 + n, nt=1 << 30)
+        el = time.perf_counter() - t0
+        if el > seconds or n >= 200:
+            break
+    nodes = host.nx * host.ny
+    return {"value": nodes * n / el, "unit": UNIT, "cores": num_threads(), "kind": "port",
+            "sample": f"{n} full LS-RK4 steps of the same {host.nx}x{host.ny}-node workload ({el:.1f} s)"}
+
+
+def run_reference(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    tmp = ROOT / "_bench_tmp" / "ref"
+    text, base, info = workload(args.workload, tmp)
+    host = init_domain(text, base)
+    from oracle.binding import OracleDomain, num_threads
+
+    o = OracleDomain(host)
+    nodes = host.nx * host.ny
+    o.run(1, min(args.warmup, 1), nt=1 << 30)
+    t0 = time.perf_counter()
+    steps = max(1, min(args.steps, 8))
+    o.run(2, 1 + steps, nt=1 << 30)
+    el = time.perf_counter() - t0
+    v = nodes * steps / el
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": 1,
+            "ms_per_step": el / steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {**info, "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": num_threads(), "kind": "port",
+                             "sample": f"{steps} LS-RK4 steps of the full workload on the host cores"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--workload", default="rupture", choices=["rupture", "pulse", "roughfault"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

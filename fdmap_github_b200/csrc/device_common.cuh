@@ -48,6 +48,7 @@ struct DevBlock {
   double src_wx[5], src_wy[5];         // singular_source weights d for i0-2..i0+2
   int tile_begin;                      // first stencil tile of this block
   int tiles_x;
+  long long march_unit_begin;          // first row-group unit of this block (march kernel)
 };
 
 // per-interface friction storage: st[f*n + k] for the 18 FDMAP_FAULT_* fields,
@@ -78,7 +79,9 @@ struct DevDomain {
   double DL[6][9];  // DL[r][s]: weight of point s for the derivative at boundary node r
   DevBlock blk[MAX_BLOCKS];
   DevIface ifc[MAX_IFACES];
-  // edge work segments: BC sides first, then interfaces
+  // closure strips of every block (bottom, top, left, right): thread offsets
+  long long cstart[4 * MAX_BLOCKS + 1];
+  // interface work segments (one thread per interface node)
   int nseg;
   int seg_kind[4 * MAX_BLOCKS + MAX_IFACES];   // 0 = BC side, 1 = interface
   int seg_a[4 * MAX_BLOCKS + MAX_IFACES];      // block (BC) or interface index

@@ -1,4 +1,4 @@
-// Edge kernel: one thread per boundary node or interface node.
+// Interface kernel: one thread per interface node.
 //
 // Replaces, for one RK stage, prepare_edges (domain.f90:420-439; the edge rows
 // are read straight from the block's field array -- on one GPU the MPI edge
@@ -455,32 +455,16 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
   }
 }
 
+// One thread per interface node: the locked / frictional solve of this stage,
+// hat variables of both sides, and the fault register life cycle.
 template <int MODE>
 __global__ void __launch_bounds__(128) edge_kernel(const DevDomain* __restrict__ Dp, StageArgs a) {
-  constexpr int NF = MODE == 2 ? 6 : 3;
   const DevDomain& D = *Dp;
   int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.seg_start[D.nseg]) return;
   int sg = 0;
   while (tid >= D.seg_start[sg + 1]) ++sg;
-  int k = tid - D.seg_start[sg];
-  if (D.seg_kind[sg] == 0) {
-    const DevBlock& B = D.blk[D.seg_a[sg]];
-    int s = D.seg_b[sg];
-    const DevSide& S = B.side[s];
-    if (k >= S.cov_lo && k < S.cov_hi) return;  // hat variables set by the interface
-    int i, j;
-    side_node_local(s, k, B.nx, B.ny, i, j);
-    const double* f = B.F[a.in] + (long long)j * B.pitch + i;
-    double F[6], F0[6], Fh[6];
-#pragma unroll
-    for (int l = 0; l < NF; ++l) { F[l] = f[l * B.plane]; F0[l] = S.F0[k + S.n * l]; }
-    d_set_bc<MODE>(Fh, F, F0, S.nrm[k], S.nrm[k + S.n], S.bc, S.M[k], S.M[k + S.n], S.M[k + 2 * S.n]);
-#pragma unroll
-    for (int l = 0; l < NF; ++l) S.Fhat[k + S.n * l] = Fh[l];
-  } else {
-    d_iface_node<MODE>(D, D.ifc[D.seg_a[sg]], k, a);
-  }
+  d_iface_node<MODE>(D, D.ifc[D.seg_a[sg]], tid - D.seg_start[sg], a);
 }
 
 }  // namespace fdmap

@@ -8,12 +8,15 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <cstdlib>
+#include <type_traits>
 #include <string>
 #include <vector>
 
 #include "edge_kernel.cuh"
 #include "fdmap_gpu.h"
 #include "sbp_tables.h"
+#include "march_kernel.cuh"
 #include "stencil_kernel.cuh"
 
 using namespace fdmap;
@@ -68,12 +71,26 @@ struct fdmap_gpu {
   std::vector<int> iface_n;
   std::vector<int> iface_fric;
   int total_tiles = 0, edge_threads = 0;
+  long long closure_threads = 0;
+  long long march_units = 0;
+  int march_grid = 0;
+  int use_march = 1;
+  double* met_base[MAX_BLOCKS] = {};
+  double* het_base[MAX_BLOCKS] = {};
+  TmapSet* tmaps = nullptr;  // host copy, passed by value to the march kernel
   double* h_stage = nullptr;  // pinned staging buffer for layout conversion
   size_t stage_doubles = 0;
   unsigned long long* d_status = nullptr;
   long long launches = 0;
   double* dev_fhat[MAX_BLOCKS][4] = {};
   int side_n[MAX_BLOCKS][4] = {};
+  cudaStream_t own_stream = nullptr;
+  // per-kernel event timing (fdmap_gpu_profile)
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;  // kind, (start, stop)
+  double prof_ms[3] = {0, 0, 0};
+  long long prof_n[3] = {0, 0, 0};
 
   template <typename T>
   int alloc(T** p, size_t count) {
@@ -85,6 +102,16 @@ struct fdmap_gpu {
     allocs.push_back(q);
     bytes += (long long)bytes_;
     *p = (T*)q;
+    return FDMAP_OK;
+  }
+  // field arrays: PADL doubles of front padding so halo bulk copies may start
+  // before column 0; every plane carries PADTAIL doubles of slack after its last row
+  int alloc_planes(double** base, int nplanes, long long plane) {
+    double* raw = nullptr;
+    int rc = alloc(&raw, (size_t)PADL + (size_t)nplanes * plane);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemset(raw, 0, ((size_t)PADL + (size_t)nplanes * plane) * sizeof(double)));
+    *base = raw + PADL;
     return FDMAP_OK;
   }
   int upload(double** dst, const double* src, size_t count) {
@@ -102,20 +129,56 @@ struct fdmap_gpu {
     CUDA_TRY(cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(double), cudaMemcpyHostToDevice));
     return FDMAP_OK;
   }
+  cudaEvent_t take_event() {
+    cudaEvent_t e;
+    if (!ev_pool.empty()) { e = ev_pool.back(); ev_pool.pop_back(); }
+    else cudaEventCreate(&e);
+    return e;
+  }
+  // folds finished event pairs into the totals (blocking on the last one)
+  void drain_events() {
+    for (auto& p : ev_pending) {
+      cudaEventSynchronize(p.second.second);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+      prof_ms[p.first] += ms;
+      prof_n[p.first] += 1;
+      ev_pool.push_back(p.second.first);
+      ev_pool.push_back(p.second.second);
+    }
+    ev_pending.clear();
+  }
   ~fdmap_gpu() {
     if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+    for (auto e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
     if (h_stage) cudaFreeHost(h_stage);
-    if (stream) cudaStreamDestroy(stream);
+    if (own_stream) cudaStreamDestroy(own_stream);
+    delete tmaps;
   }
 };
 
 namespace {
 
+struct ProfScope {
+  fdmap_gpu* h;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(fdmap_gpu* h_, int kind_) : h(h_), kind(kind_) {
+    if (h->profiling) { a = h->take_event(); b = h->take_event(); cudaEventRecord(a, h->stream); }
+  }
+  ~ProfScope() {
+    if (a) { cudaEventRecord(b, h->stream); h->ev_pending.push_back({kind, {a, b}}); }
+  }
+};
+
 int launch_edges(fdmap_gpu* h, const StageArgs& a) {
   if (h->edge_threads == 0) return FDMAP_OK;
   int tpb = 128;
   int nb = (h->edge_threads + tpb - 1) / tpb;
+  ProfScope ps(h, 2);
   if (h->mode == 2) edge_kernel<2><<<nb, tpb, 0, h->stream>>>(h->ddom, a);
   else edge_kernel<3><<<nb, tpb, 0, h->stream>>>(h->ddom, a);
   h->launches++;
@@ -137,8 +200,127 @@ void launch_stencil_mode(fdmap_gpu* h, const StageArgs& a) {
   }
 }
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// 3-D FP64 tensor map over `nplanes` consecutive planes of a block array
+int encode_map(EncodeTiledFn enc, CUtensorMap* map, double* base, const BlockGeom& g, int nplanes, int box_x, int box_z) {
+  cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
+  cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8};
+  cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)MR, (cuuint32_t)box_z};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_err(FDMAP_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  return FDMAP_OK;
+}
+
+template <int MODE, int PI_, bool HET>
+int march_maps(fdmap_gpu* h) {
+  using L = MarchLayout<MODE, PI_, HET>;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult qr;
+  CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr));
+  if (!fn || qr != cudaDriverEntryPointSuccess) return set_err(FDMAP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  EncodeTiledFn enc = (EncodeTiledFn)fn;
+  if (!h->tmaps) h->tmaps = new (std::nothrow) TmapSet();
+  if (!h->tmaps) return set_err(FDMAP_ERR_NOMEM, "out of host memory");
+  std::memset(h->tmaps, 0, sizeof(TmapSet));
+  int rc;
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const BlockGeom& g = h->geom[b];
+    DevBlock& B = h->hdom.blk[b];
+    for (int q = 0; q < 2; ++q) {
+      if ((rc = encode_map(enc, &h->tmaps->F[b][q], B.F[q], g, h->nF, L::WH, L::NR))) return rc;
+      if ((rc = encode_map(enc, &h->tmaps->F6[b][q], B.F[q], g, h->nF, MW, 1))) return rc;
+    }
+    if ((rc = encode_map(enc, &h->tmaps->DF[b], B.DF, g, h->nF, MW, L::NR))) return rc;
+    if ((rc = encode_map(enc, &h->tmaps->MH[b], h->met_base[b], g, 5, L::WH, 2))) return rc;
+    if ((rc = encode_map(enc, &h->tmaps->MC[b], h->met_base[b], g, 5, MW, 3))) return rc;
+    if (HET && (rc = encode_map(enc, &h->tmaps->HT[b], h->het_base[b], g, 5, MW, L::NH))) return rc;
+  }
+  return FDMAP_OK;
+}
+
+template <int MODE, int PI_, bool HET>
+int march_setup(fdmap_gpu* h) {
+  size_t smem = MarchLayout<MODE, PI_, HET>::BYTES;
+  int optin = 0;
+  CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
+  if (smem > (size_t)optin) {  // the ring does not fit: this variant uses the tiled kernel
+    h->use_march = 0;
+    return FDMAP_OK;
+  }
+  int rc0 = march_maps<MODE, PI_, HET>(h);
+  if (rc0) return rc0;
+  auto k = march_kernel<MODE, PI_, HET>;
+  CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0, sms = 0;
+  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, MTHREADS, smem));
+  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
+  if (per_sm < 1) return set_err(FDMAP_ERR_CUDA, "march kernel does not fit on an SM");
+  long long g = (long long)sms * per_sm;
+  h->march_grid = (int)std::min<long long>(g, h->march_units);
+  return FDMAP_OK;
+}
+
+template <int MODE, int PI_, bool HET>
+void march_launch(fdmap_gpu* h, const StageArgs& a) {
+  MarchPlan plan{h->march_grid, h->march_units};
+  march_kernel<MODE, PI_, HET><<<h->march_grid, MTHREADS, MarchLayout<MODE, PI_, HET>::BYTES, h->stream>>>(h->ddom, a, plan, *h->tmaps);
+}
+
+template <int MODE, bool HET, typename Fn>
+int dispatch_pi(int pI, Fn&& fn) {
+  if (pI == 1) return fn(std::integral_constant<int, 1>{});
+  if (pI == 2) return fn(std::integral_constant<int, 2>{});
+  return fn(std::integral_constant<int, 3>{});
+}
+
+int march_dispatch(fdmap_gpu* h, const StageArgs* a) {
+  auto go = [&](auto mode_c, auto het_c) {
+    constexpr int MODE = decltype(mode_c)::value;
+    constexpr bool HET = decltype(het_c)::value;
+    return dispatch_pi<MODE, HET>(h->pI, [&](auto pi_c) {
+      constexpr int PI_ = decltype(pi_c)::value;
+      if (a) { march_launch<MODE, PI_, HET>(h, *a); return (int)FDMAP_OK; }
+      return march_setup<MODE, PI_, HET>(h);
+    });
+  };
+  if (h->mode == 2) return h->het ? go(std::integral_constant<int, 2>{}, std::true_type{}) : go(std::integral_constant<int, 2>{}, std::false_type{});
+  return h->het ? go(std::integral_constant<int, 3>{}, std::true_type{}) : go(std::integral_constant<int, 3>{}, std::false_type{});
+}
+
+template <int MODE>
+void launch_closure_mode(fdmap_gpu* h, const StageArgs& a) {
+  int nb = (int)((h->closure_threads + 127) / 128);
+  if (h->het) {
+    if (h->pI == 1) closure_kernel<MODE, 1, true><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+    else if (h->pI == 2) closure_kernel<MODE, 2, true><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+    else closure_kernel<MODE, 3, true><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+  } else {
+    if (h->pI == 1) closure_kernel<MODE, 1, false><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+    else if (h->pI == 2) closure_kernel<MODE, 2, false><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+    else closure_kernel<MODE, 3, false><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+  }
+}
+
+// one stage: interface solves, then closure strips (which read the interface
+// hat variables), then the interior; all read F[in] and write disjoint nodes
 int launch_stencil(fdmap_gpu* h, const StageArgs& a) {
-  if (h->mode == 2) launch_stencil_mode<2>(h, a);
+  {
+    ProfScope pc(h, 1);
+    if (h->mode == 2) launch_closure_mode<2>(h, a);
+    else launch_closure_mode<3>(h, a);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+  }
+  ProfScope ps(h, 0);
+  if (h->use_march) {
+    int rc = march_dispatch(h, &a);
+    if (rc) return rc;
+  } else if (h->mode == 2) launch_stencil_mode<2>(h, a);
   else launch_stencil_mode<3>(h, a);
   h->launches++;
   CUDA_TRY(cudaGetLastError());
@@ -216,26 +398,32 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     g.mgx = fb.mgx; g.mgy = fb.mgy;
     g.nx = fb.pgx - fb.mgx + 1; g.ny = fb.pgy - fb.mgy + 1;
     g.pitch = (g.nx + 31) / 32 * 32;
-    g.plane = (long long)g.pitch * g.ny;
+    g.plane = ((long long)g.pitch * g.ny + PADTAIL + 31) / 32 * 32;
     B.nx = g.nx; B.ny = g.ny; B.pitch = g.pitch; B.plane = g.plane;
     int rc;
     for (int q = 0; q < 2; ++q)
-      if ((rc = h->alloc(&B.F[q], (size_t)g.plane * nF))) return rc;
-    if ((rc = h->alloc(&B.DF, (size_t)g.plane * nF))) return rc;
-    double** met[5] = {&B.xq, &B.xr, &B.yq, &B.yr, &B.Ji};
-    const double* msrc[5] = {d->xq, d->xr, d->yq, d->yr, d->Ji};
+      if ((rc = h->alloc_planes(&B.F[q], nF, g.plane))) return rc;
+    if ((rc = h->alloc_planes(&B.DF, nF, g.plane))) return rc;
+    // metric terms as 5 consecutive planes yr, xr, yq, xq, Ji (one TMA tensor)
+    double* met_base = nullptr;
+    if ((rc = h->alloc_planes(&met_base, 5, g.plane))) return rc;
+    double** met[5] = {&B.yr, &B.xr, &B.yq, &B.xq, &B.Ji};
+    const double* msrc[5] = {d->yr, d->xr, d->yq, d->xq, d->Ji};
     for (int q = 0; q < 5; ++q) {
-      if ((rc = h->alloc(met[q], (size_t)g.plane))) return rc;
+      *met[q] = met_base + (size_t)q * g.plane;
       if ((rc = h->upload_plane(*met[q], msrc[q], g))) return rc;
     }
+    h->met_base[b] = met_base;
     if (d->heterogeneous) {
+      double* het_base = nullptr;
+      if ((rc = h->alloc_planes(&het_base, 5, g.plane))) return rc;
       double** hm[5] = {&B.rho, &B.G, &B.M, &B.gamma, &B.nu};
       const double* hs[5] = {d->rho, d->G, d->M, d->gamma, d->nu};
       for (int q = 0; q < 5; ++q) {
-        if (!hs[q]) continue;
-        if ((rc = h->alloc(hm[q], (size_t)g.plane))) return rc;
-        if ((rc = h->upload_plane(*hm[q], hs[q], g))) return rc;
+        *hm[q] = het_base + (size_t)q * g.plane;
+        if (hs[q] && (rc = h->upload_plane(*hm[q], hs[q], g))) return rc;
       }
+      h->het_base[b] = het_base;
     }
     B.rho_b = fb.rho; B.G_b = fb.G; B.M_b = fb.M; B.gamma_b = fb.gamma; B.nu_b = fb.nu;
     for (int s = 1; s <= op.pI; ++s) {
@@ -269,6 +457,8 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     int tiles_y = (g.ny + TY - 1) / TY;
     B.tile_begin = tiles;
     tiles += B.tiles_x * tiles_y;
+    B.march_unit_begin = h->march_units;
+    h->march_units += (long long)((g.nx + MW - 1) / MW) * ((g.ny + MR - 1) / MR);
   }
   h->total_tiles = tiles;
 
@@ -319,25 +509,34 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     if ((rc = h->upload(&FR.par, par.data(), par.size()))) return rc;
   }
 
-  // edge work segments: BC sides, then interfaces
+  // interface work segments; closure strips per block
   int nseg = 0, start = 0;
-  for (int b = 0; b < d->nblocks; ++b)
-    for (int s = 0; s < 4; ++s) {
-      if (D.blk[b].side[s].bc == FDMAP_BC_NONE) continue;
-      D.seg_kind[nseg] = 0; D.seg_a[nseg] = b; D.seg_b[nseg] = s; D.seg_start[nseg] = start;
-      start += D.blk[b].side[s].n;
-      ++nseg;
-    }
   for (int k = 0; k < d->nifaces; ++k) {
     D.seg_kind[nseg] = 1; D.seg_a[nseg] = k; D.seg_b[nseg] = 0; D.seg_start[nseg] = start;
     start += D.ifc[k].n;
     ++nseg;
+  }
+  {
+    long long cs = 0;
+    for (int b = 0; b < d->nblocks; ++b) {
+      const BlockGeom& g = h->geom[b];
+      long long strip[4] = {(long long)op.nbst * g.nx, (long long)op.nbst * g.nx,
+                            (long long)(g.ny - 2 * op.nbst) * op.nbst, (long long)(g.ny - 2 * op.nbst) * op.nbst};
+      for (int q = 0; q < 4; ++q) { D.cstart[4 * b + q] = cs; cs += strip[q]; }
+    }
+    D.cstart[4 * d->nblocks] = cs;
+    h->closure_threads = cs;
   }
   D.seg_start[nseg] = start;
   D.nseg = nseg;
   h->edge_threads = start;
 
   int rc;
+  {
+    const char* ek = getenv("FDMAP_STENCIL");
+    h->use_march = !(ek && std::string(ek) == "tile");
+    if (h->use_march && (rc = march_dispatch(h, nullptr))) return rc;
+  }
   if ((rc = h->alloc(&h->d_status, 4))) return rc;
   CUDA_TRY(cudaMemset(h->d_status, 0, 4 * sizeof(unsigned long long)));
   D.status = h->d_status;
@@ -369,10 +568,12 @@ int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu*
   fdmap_gpu* h = new (std::nothrow) fdmap_gpu();
   if (!h) return set_err(FDMAP_ERR_NOMEM, "out of host memory");
   h->device = device;
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaSetDevice(device) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     delete h;
     return set_err(FDMAP_ERR_CUDA, "cannot initialise device");
   }
+  h->stream = h->own_stream;
   rc = build(h, d);
   if (rc == FDMAP_OK && init_edges) rc = fdmap_gpu_init_edges(h, d->t0);
   if (rc == FDMAP_OK) rc = fdmap_gpu_synchronize(h);
@@ -534,6 +735,34 @@ int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures) {
   CUDA_TRY(cudaMemcpy(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost));
   if (newton_failures) *newton_failures = (long long)st[0];
   return st[0] ? FDMAP_ERR_NEWTON_NOCONV : FDMAP_OK;
+}
+
+int fdmap_gpu_set_stream(fdmap_gpu* h, void* stream) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->stream = stream ? (cudaStream_t)stream : h->own_stream;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_profile(fdmap_gpu* h, int enable) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  h->drain_events();
+  h->profiling = enable != 0;
+  for (int k = 0; k < 3; ++k) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_profile_read(fdmap_gpu* h, double* ms, long long* count) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  h->drain_events();
+  for (int k = 0; k < 3; ++k) {
+    if (ms) ms[k] = h->prof_ms[k];
+    if (count) count[k] = h->prof_n[k];
+  }
+  return FDMAP_OK;
 }
 
 long long fdmap_gpu_launch_count(fdmap_gpu* h) { return h ? h->launches : -1; }

@@ -1099,6 +1099,7 @@ extern "C" int fdmap_host_info(const fdmap_domain* dom, int* ints, double* dbls)
   if (ints) {
     ints[0] = d.mode; ints[1] = d.nF; ints[2] = d.nx; ints[3] = d.ny;
     ints[4] = d.nblocks; ints[5] = d.nifaces; ints[6] = d.nt; ints[7] = d.rk_order;
+    ints[8] = d.fd_method; ints[9] = d.heterogeneous;
   }
   if (dbls) {
     dbls[0] = d.t0; dbls[1] = d.dt; dbls[2] = d.CFL; dbls[3] = d.hmin; dbls[4] = d.hmax;

@@ -1,0 +1,324 @@
+// Persistent "march" stage kernel: the same per-node work as stencil_kernel
+// (fused scale + SAT + SBP rates + szz + sources + RK update), organised for
+// HBM streaming on sm_100a.
+//
+// Work: every block is cut into strips of W = 64 columns; the strip-rows of
+// all blocks form one sequence of row groups (R = 4 rows) that is split into
+// equal contiguous ranges, one per resident CTA (grid = SMs x CTAs per SM), so
+// every CTA streams the same amount of data and consecutive CTAs hold
+// vertically adjacent rows (their halo rows are shared through L2).
+//
+// Data movement: the rows a CTA needs -- fields used by the rates and the
+// metric terms -- arrive in a shared-memory ring of NS = 2R + 2H row slots
+// through 1-D TMA bulk copies (cp.async.bulk ... mbarrier::complete_tx) issued
+// by one thread two row groups ahead; each slot has its own mbarrier.
+// Neighbours along i come from the slot's halo columns, neighbours along j
+// from the adjacent slots.  Per-node data that no neighbour needs (rates DF,
+// szz, 1/J, heterogeneous material) is read by the owning thread with plain
+// coalesced loads one row group ahead.
+#pragma once
+
+#include <cuda.h>
+
+#include "stencil_kernel.cuh"
+
+namespace fdmap {
+
+constexpr int MW = 128;         // strip width (columns)
+constexpr int MR = 4;           // rows per row group
+constexpr int MTHREADS = MW * MR;
+constexpr int PADL = 32;        // doubles of front padding before every field array
+constexpr int PADTAIL = 192;    // slack after the last row of every field plane
+constexpr int NGS = 4;          // neighbour ring: row groups g-1, g, g+1 resident, g+2 in flight
+constexpr int NCS = 2;          // centre ring: group g resident, g+1 in flight
+
+__host__ __device__ constexpr int even_halo(int h) { return (h + 1) & ~1; }
+__host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
+
+template <int MODE, int PI_, bool HET>
+struct MarchLayout {
+  static constexpr int NR = RDef<MODE>::NR;
+  static constexpr int HP = even_halo(PI_);
+  static constexpr int WH = MW + 2 * HP;                       // halo row length (doubles)
+  static constexpr int NH = HET ? (MODE == 2 ? 5 : 2) : 0;     // heterogeneous material planes
+  // neighbour group slot: rate fields [NR][MR][WH], yr,xr [2][MR][WH], yq,xq,Ji [3][MR][MW]
+  static constexpr size_t F_OFF = 0;
+  static constexpr size_t MH_OFF = align128(F_OFF + (size_t)NR * MR * WH * 8);
+  static constexpr size_t MC_OFF = align128(MH_OFF + (size_t)2 * MR * WH * 8);
+  static constexpr size_t GSLOT = align128(MC_OFF + (size_t)3 * MR * MW * 8);
+  // centre group slot: DF [NR][MR][MW], szz [1][MR][MW] (mode II), material [NH][MR][MW]
+  static constexpr size_t DF_OFF = 0;
+  static constexpr size_t F6_OFF = align128(DF_OFF + (size_t)NR * MR * MW * 8);
+  static constexpr size_t HT_OFF = align128(F6_OFF + (MODE == 2 ? (size_t)MR * MW * 8 : 0));
+  static constexpr size_t CSLOT = align128(HT_OFF + (size_t)NH * MR * MW * 8);
+  static constexpr size_t BARS_OFF = NGS * GSLOT + NCS * CSLOT;
+  static constexpr size_t BYTES = BARS_OFF + (NGS + NCS) * 8 + 128;  // + alignment slack
+  static constexpr unsigned NB_BYTES = (unsigned)(((size_t)(NR + 2) * WH + 3 * MW) * MR * 8);
+};
+
+struct MarchPlan {
+  int grid;          // CTAs launched
+  long long units;   // total row groups over all strips of all blocks
+};
+
+// TMA descriptors of every block, passed by value as a __grid_constant__ parameter
+struct TmapSet {
+  CUtensorMap F[MAX_BLOCKS][2];    // rate fields, box {WH, MR, NR}
+  CUtensorMap F6[MAX_BLOCKS][2];   // szz plane (mode II), box {MW, MR, 1}
+  CUtensorMap DF[MAX_BLOCKS];      // rates, box {MW, MR, NR}
+  CUtensorMap MH[MAX_BLOCKS];      // yr, xr, box {WH, MR, 2}
+  CUtensorMap MC[MAX_BLOCKS];      // yq, xq, Ji, box {MW, MR, 3}
+  CUtensorMap HT[MAX_BLOCKS];      // heterogeneous material, box {MW, MR, NH}
+};
+
+// ---------------------------------------------------------------------------
+// PTX helpers: mbarrier and 1-D bulk copy global -> shared
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 3-D tiled TMA load (no multicast) of one box into shared memory
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Bounded wait: gives up after ~2^28 polls (seconds) and records the event in
+// the status word instead of spinning forever.
+__device__ __forceinline__ void mbar_wait_bounded(unsigned long long* bar, unsigned parity, unsigned long long* status) {
+  for (unsigned it = 0; it < (1u << 28); ++it)
+    if (mbar_try_wait(bar, parity)) return;
+  atomicOr(&status[1], 2ull);
+}
+
+// Row-group unit u -> (block, strip, first row)
+struct UnitPos {
+  int b, sx, j0;
+};
+
+__device__ __forceinline__ UnitPos unit_pos(const DevDomain& D, long long u) {
+  UnitPos p{0, 0, 0};
+  int b = 0;
+  while (b + 1 < D.nblocks && u >= D.blk[b + 1].march_unit_begin) ++b;
+  const DevBlock& B = D.blk[b];
+  long long local = u - B.march_unit_begin;
+  int groups = (B.ny + MR - 1) / MR;
+  p.b = b;
+  p.sx = (int)(local / groups);
+  p.j0 = (int)(local % groups) * MR;
+  return p;
+}
+
+template <int MODE, int PI_, bool HET>
+__global__ void __launch_bounds__(MTHREADS, 1)
+    march_kernel(const DevDomain* __restrict__ Dp, StageArgs a, MarchPlan plan, const __grid_constant__ TmapSet tm) {
+  using L = MarchLayout<MODE, PI_, HET>;
+  using RD = RDef<MODE>;
+  constexpr int NR = RD::NR;
+  constexpr int NF = MODE == 2 ? 6 : 3;
+  constexpr int H = PI_;
+  constexpr int HP = L::HP;
+  constexpr int WH = L::WH;
+  extern __shared__ unsigned char smem_dyn[];
+  unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
+  unsigned long long* nbar = reinterpret_cast<unsigned long long*>(smem + L::BARS_OFF);
+  unsigned long long* cbar = nbar + NGS;
+
+  const DevDomain& D = *Dp;
+  const int tid = threadIdx.x;
+  const int cx = tid % MW, ry = tid / MW;
+  const long long ubeg = plan.units * blockIdx.x / gridDim.x;
+  const long long uend = plan.units * (blockIdx.x + 1) / gridDim.x;
+  const bool load_df = a.scale && a.A != 0.0;  // A = 0 (first stage): A*DF = 0, DF is not read
+  const unsigned cbytes = (unsigned)((load_df ? (size_t)NR * MR * MW * 8 : 0) + (MODE == 2 ? (size_t)MR * MW * 8 : 0) +
+                                     (size_t)L::NH * MR * MW * 8);
+
+  long long u = ubeg;
+  while (u < uend) {
+    // segment: consecutive row groups of one strip
+    const UnitPos p0 = unit_pos(D, u);
+    const int b = p0.b;
+    const DevBlock& B = D.blk[b];
+    const int groups = (B.ny + MR - 1) / MR;
+    const long long strip_end = B.march_unit_begin + (long long)(p0.sx + 1) * groups;
+    const long long seg_end = uend < strip_end ? uend : strip_end;
+    const int jr0 = p0.j0;
+    const int jr1 = min(B.ny, (int)(jr0 + (seg_end - u) * MR));
+    const int i0 = p0.sx * MW;
+    const int nx = B.nx, ny = B.ny;
+    const long long pitch = B.pitch, plane = B.plane;
+    const double* __restrict__ Fin = B.F[a.in];
+    const int ngroups = (jr1 - jr0 + MR - 1) / MR;
+    // neighbour groups needed: k = gmin .. gmax (group k holds rows jr0 + k*MR ..)
+    const int gmin = jr0 >= MR ? -1 : 0;
+    const int gmax = ngroups - 1 + (jr1 < ny ? 1 : 0);
+    const CUtensorMap* mF = &tm.F[b][a.in];
+    const CUtensorMap* mF6 = &tm.F6[b][a.in];
+
+    if (tid == 0) {
+      for (int s = 0; s < NGS + NCS; ++s) mbar_init(&nbar[s], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    auto fill_nb = [&](int k) {  // neighbour group k -> slot (k - gmin) % NGS
+      const int sl = (k - gmin) % NGS;
+      unsigned char* g = smem + (size_t)sl * L::GSLOT;
+      const int row = jr0 + k * MR;
+      mbar_arrive_tx(&nbar[sl], L::NB_BYTES);
+      tma_load_3d(g + L::F_OFF, mF, i0 - HP, row, 0, &nbar[sl]);
+      tma_load_3d(g + L::MH_OFF, &tm.MH[b], i0 - HP, row, 0, &nbar[sl]);
+      tma_load_3d(g + L::MC_OFF, &tm.MC[b], i0, row, 2, &nbar[sl]);
+    };
+    auto fill_c = [&](int k) {  // centre group k -> slot k % NCS
+      const int sl = k % NCS;
+      unsigned char* g = smem + (size_t)NGS * L::GSLOT + (size_t)sl * L::CSLOT;
+      const int row = jr0 + k * MR;
+      mbar_arrive_tx(&cbar[sl], cbytes);
+      if (load_df) tma_load_3d(g + L::DF_OFF, &tm.DF[b], i0, row, 0, &cbar[sl]);
+      if (MODE == 2) tma_load_3d(g + L::F6_OFF, mF6, i0, row, 5, &cbar[sl]);
+      if (HET) tma_load_3d(g + L::HT_OFF, &tm.HT[b], i0, row, 0, &cbar[sl]);
+    };
+    if (tid == 0) {
+      fence_proxy_async();
+      for (int k = gmin; k <= min(gmax, gmin + NGS - 1); ++k) fill_nb(k);
+      for (int k = 0; k < min(ngroups, NCS); ++k) fill_c(k);
+    }
+
+    // per-CTA constants for the interior fast path
+    double cf[PI_ + 1][3];
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s)
+#pragma unroll
+      for (int q = 0; q < 3; ++q) cf[s][q] = B.coef[s][q];
+    const double rho_b = B.rho_b, G_b = B.G_b, M_b = B.M_b, gamma_b = B.gamma_b, nu_b = B.nu_b;
+    double* __restrict__ DFp = B.DF;
+    double* __restrict__ Fout = B.F[a.out];
+
+    const int nbst = D.nbst;
+    const int i = i0 + cx;
+    for (int g = 0; g < ngroups; ++g) {
+      // wait for groups g-1, g, g+1 (neighbours) and centre group g
+      // neighbour group k lives in slot (k - gmin) % NGS as that slot's fill (k - gmin) / NGS
+      for (int k = max(gmin, g - 1); k <= min(gmax, g + 1); ++k)
+        mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status);
+      mbar_wait_bounded(&cbar[g % NCS], (unsigned)((g / NCS) & 1), D.status);
+      const int j = jr0 + g * MR + ry;
+      if (j < jr1 && i >= nbst && i <= nx - 1 - nbst && j >= nbst && j <= ny - 1 - nbst) {
+        const long long c = (long long)j * pitch + i;
+        // row j lives in group g, row ry; rows j +- s in group g + (ry +- s) div MR
+        auto nrow = [&](int dr, size_t off, int q, int width) -> const double* {
+          int rr = ry + dr;
+          int k = g + (rr >= 0 ? rr / MR : -1);
+          int r = rr - (k - g) * MR;
+          return reinterpret_cast<const double*>(smem + (size_t)((k - gmin) % NGS) * L::GSLOT + off) + ((size_t)q * MR + r) * width;
+        };
+        const unsigned char* cslot = smem + (size_t)NGS * L::GSLOT + (size_t)(g % NCS) * L::CSLOT;
+        double acc[NF];
+        if (load_df) {
+          const double* dfc = reinterpret_cast<const double*>(cslot + L::DF_OFF) + (size_t)ry * MW + cx;
+#pragma unroll
+          for (int l = 0; l < NR; ++l) acc[l] = a.A * dfc[(size_t)l * MR * MW];
+        } else {
+#pragma unroll
+          for (int l = 0; l < NR; ++l) acc[l] = 0.0;
+        }
+        if (MODE == 2) acc[5] = 0.0;  // DF6 is overwritten by rates_szz below
+        double Fc[NF];
+#pragma unroll
+        for (int l = 0; l < NR; ++l) Fc[l] = nrow(0, L::F_OFF, l, WH)[cx + HP];
+        if (MODE == 2) Fc[5] = reinterpret_cast<const double*>(cslot + L::F6_OFF)[(size_t)ry * MW + cx];
+        const double Ji = nrow(0, L::MC_OFF, 2, MW)[cx];
+        NodeMat m;
+        if (HET) {
+          const double* ht = reinterpret_cast<const double*>(cslot + L::HT_OFF) + (size_t)ry * MW + cx;
+          m.rho = ht[0]; m.G = ht[(size_t)MR * MW];
+          if (MODE == 2) { m.M = ht[(size_t)2 * MR * MW]; m.gamma = ht[(size_t)3 * MR * MW]; m.nu = ht[(size_t)4 * MR * MW]; }
+          else { m.M = 0.0; m.gamma = 0.0; m.nu = 0.0; }
+        } else {
+          m.rho = rho_b; m.G = G_b; m.M = M_b; m.gamma = gamma_b; m.nu = nu_b;
+        }
+        {
+          const double* hy = nrow(0, L::MH_OFF, 0, WH) + cx + HP;  // yr, centred on the node
+          const double* hx = nrow(0, L::MH_OFF, 1, WH) + cx + HP;  // xr
+          const double yrc = hy[0], xrc = hx[0];
+          const double yqc = nrow(0, L::MC_OFF, 0, MW)[cx], xqc = nrow(0, L::MC_OFF, 1, MW)[cx];
+#pragma unroll
+          for (int s = 1; s <= PI_; ++s) {
+            const double Yrp = 0.5 * (hy[s] + yrc), Xrp = 0.5 * (hx[s] + xrc);
+            const double Yrm = 0.5 * (hy[-s] + yrc), Xrm = 0.5 * (hx[-s] + xrc);
+            const double Yqp = 0.5 * (nrow(s, L::MC_OFF, 0, MW)[cx] + yqc), Xqp = 0.5 * (nrow(s, L::MC_OFF, 1, MW)[cx] + xqc);
+            const double Yqm = 0.5 * (nrow(-s, L::MC_OFF, 0, MW)[cx] + yqc), Xqm = 0.5 * (nrow(-s, L::MC_OFF, 1, MW)[cx] + xqc);
+            const double w = HET ? D.DI[s] : 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+              double sum = 0.0;
+              if (RD::fa(r) >= 0) {
+                const int f = RD::fa(r);
+                const double* fr = nrow(0, L::F_OFF, f, WH) + cx + HP;
+                double t = Yrp * fr[s] - Yrm * fr[-s] - Yqp * nrow(s, L::F_OFF, f, WH)[cx + HP] +
+                           Yqm * nrow(-s, L::F_OFF, f, WH)[cx + HP];
+                if (RD::ga(r)) t *= m.gamma;
+                sum += t;
+              }
+              if (RD::fb(r) >= 0) {
+                const int f = RD::fb(r);
+                const double* fr = nrow(0, L::F_OFF, f, WH) + cx + HP;
+                double t = -Xrp * fr[s] + Xrm * fr[-s] + Xqp * nrow(s, L::F_OFF, f, WH)[cx + HP] -
+                           Xqm * nrow(-s, L::F_OFF, f, WH)[cx + HP];
+                if (RD::gb(r)) t *= m.gamma;
+                sum += t;
+              }
+              const double cfr = HET ? mat_coef(m, RD::coef(r), w) : cf[s][RD::coef(r)];
+              acc[r] += sum * cfr * Ji;
+            }
+          }
+        }
+        if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
+        body_forces<MODE>(D, B, i, j, a.t, acc);
+#pragma unroll
+        for (int l = 0; l < NF; ++l) DFp[l * plane + c] = acc[l];
+        if (a.update) {
+#pragma unroll
+          for (int l = 0; l < NF; ++l) Fout[l * plane + c] = Fc[l] + a.Bdt * acc[l];
+        }
+      }
+      __syncthreads();
+      // group g-1 is no longer needed: its slot takes group g-1+NGS; centre slot g%NCS takes g+NCS
+      if (tid == 0) {
+        fence_proxy_async();
+        if (g - 1 >= gmin && g - 1 + NGS <= gmax) fill_nb(g - 1 + NGS);
+        if (g + NCS < ngroups) fill_c(g + NCS);
+      }
+    }
+    __syncthreads();
+    u = seg_end;
+  }
+}
+
+}  // namespace fdmap

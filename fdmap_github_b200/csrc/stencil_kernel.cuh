@@ -11,7 +11,7 @@
 // one-sided DL/DR rows exactly like rates_boundary_mode2/3.
 #pragma once
 
-#include "device_common.cuh"
+#include "edge_kernel.cuh"
 
 namespace fdmap {
 
@@ -70,7 +70,7 @@ __device__ __forceinline__ double flux(int r, double Ym, double Xm, const double
 // Closure-region rates for node (i, j) read through the cache hierarchy
 // (rates_boundary_mode2/3 and the heterogeneous variants).
 template <int MODE, int PI_>
-__device__ void closure_rates(const DevDomain& D, const DevBlock& B, const double* __restrict__ Fin, int i, int j,
+__device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock& B, const double* __restrict__ Fin, int i, int j,
                               const NodeMat& m, double Ji, double* acc) {
   using RD = RDef<MODE>;
   constexpr int NR = RD::NR;
@@ -146,14 +146,29 @@ __device__ void closure_rates(const DevDomain& D, const DevBlock& B, const doubl
 }
 
 // SAT penalty of side s at side-local index k for the node whose fields are F
-// (SAT_term / split_sp, time_step.f90:813-851)
+// (SAT_term / split_sp, time_step.f90:813-851).  On an outer boundary the hat
+// variables depend only on this node's fields (set_bc, boundaries.f90:132-377),
+// so they are evaluated here and stored for inspection; on an interface they
+// were written by the interface kernel of this stage.
 template <int MODE>
 __device__ __forceinline__ void sat_term(const DevSide& S, int k, const double* F, double* acc) {
   constexpr int NF = MODE == 2 ? 6 : 3;
   double Ks = S.M[k + 3 * S.n], Kp = S.M[k + 4 * S.n];
+  double Fh[6];
+  if (S.bc != FDMAP_BC_NONE && !(k >= S.cov_lo && k < S.cov_hi)) {
+    double F0[6];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) F0[l] = S.F0[k + S.n * l];
+    d_set_bc<MODE>(Fh, F, F0, S.nrm[k], S.nrm[k + S.n], S.bc, S.M[k], S.M[k + S.n], S.M[k + 2 * S.n]);
+#pragma unroll
+    for (int l = 0; l < NF; ++l) S.Fhat[k + S.n * l] = Fh[l];
+  } else {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fh[l] = S.Fhat[k + S.n * l];
+  }
   double d[6];
 #pragma unroll
-  for (int l = 0; l < NF; ++l) d[l] = S.Fhat[k + S.n * l] - F[l];
+  for (int l = 0; l < NF; ++l) d[l] = Fh[l] - F[l];
   if (MODE == 3) {
 #pragma unroll
     for (int l = 0; l < 3; ++l) acc[l] += Ks * d[l];
@@ -181,6 +196,93 @@ __device__ __forceinline__ double stf_amp(const fdmap_source& S, double t) {
     default:
       return (1.0 - 2.0 * (pi * pi) * (tc * tc) / (S.t_duration * S.t_duration)) *
              exp(-(pi * pi) * (tc * tc) / (S.t_duration * S.t_duration));
+  }
+}
+
+// point source and gravity (set_source, source.f90:147-252) at block-local node (i, j)
+template <int MODE>
+__device__ __forceinline__ void body_forces(const DevDomain& D, const DevBlock& B, int i, int j, double t, double* acc) {
+  if (D.src.use_gravity) {
+    if (MODE == 2) { acc[0] += D.src.gx; acc[1] += D.src.gy; }
+    else acc[0] += D.src.gz;
+  }
+  if (D.src.use_singular && B.src_ok) {
+    int di = i - B.src_i0, dj = j - B.src_j0;
+    if (di >= -2 && di <= 2 && dj >= -2 && dj <= 2) {
+      double A = stf_amp(D.src, t);
+      double dx = B.src_wx[di + 2], dy = B.src_wy[dj + 2];
+      if (MODE == 2) {
+        acc[0] += A * D.src.Fx * dx * dy / B.rho_b;
+        acc[1] += A * D.src.Fy * dx * dy / B.rho_b;
+        acc[2] -= A * D.src.Mxx * dx * dy;
+        acc[3] -= A * D.src.Mxy * dx * dy;
+        acc[4] -= A * D.src.Myy * dx * dy;
+      } else {
+        acc[0] += A * D.src.Fz * dx * dy / B.rho_b;
+        acc[1] -= A * D.src.Mzx * dx * dy;
+        acc[2] -= A * D.src.Mzy * dx * dy;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ bool interior_node(const DevDomain& D, const DevBlock& B, int i, int j) {
+  return i >= D.nbst && i <= B.nx - 1 - D.nbst && j >= D.nbst && j <= B.ny - 1 - D.nbst;
+}
+
+// Boundary kernel: every node within nbst of a block edge (the SBP closure
+// strips) -- scale, SAT (with boundary hat variables evaluated in place),
+// one-sided closure rates (rates_boundary_mode2/3), szz, sources, update.
+// Thread -> (block, strip, node) through the per-block strip offsets.
+template <int MODE, int PI_, bool HET>
+__global__ void __launch_bounds__(128) closure_kernel(const DevDomain* __restrict__ Dp, StageArgs a) {
+  constexpr int NF = MODE == 2 ? 6 : 3;
+  const DevDomain& D = *Dp;
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= D.cstart[4 * D.nblocks]) return;
+  int sg = 0;
+  while (tid >= D.cstart[sg + 1]) ++sg;
+  const int b = sg >> 2, strip = sg & 3;
+  const DevBlock& B = D.blk[b];
+  const int nbst = D.nbst, nx = B.nx, ny = B.ny;
+  long long k = tid - D.cstart[sg];
+  int i, j;
+  if (strip == 0) { j = (int)(k / nx); i = (int)(k % nx); }                      // bottom rows
+  else if (strip == 1) { j = ny - nbst + (int)(k / nx); i = (int)(k % nx); }     // top rows
+  else if (strip == 2) { j = nbst + (int)(k / nbst); i = (int)(k % nbst); }       // left columns
+  else { j = nbst + (int)(k / nbst); i = nx - nbst + (int)(k % nbst); }           // right columns
+  const long long pitch = B.pitch, plane = B.plane;
+  const long long c = (long long)j * pitch + i;
+  const double* __restrict__ Fin = B.F[a.in];
+  double acc[NF];
+  const bool load_df = a.scale && a.A != 0.0;
+#pragma unroll
+  for (int l = 0; l < NF; ++l) acc[l] = load_df ? a.A * B.DF[l * plane + c] : 0.0;
+  if (MODE == 2) acc[5] = 0.0;
+  double Fc[NF];
+#pragma unroll
+  for (int l = 0; l < NF; ++l) Fc[l] = Fin[l * plane + c];
+  if (i == 0) sat_term<MODE>(B.side[0], j, Fc, acc);
+  if (i == nx - 1) sat_term<MODE>(B.side[1], j, Fc, acc);
+  if (j == 0) sat_term<MODE>(B.side[2], i, Fc, acc);
+  if (j == ny - 1) sat_term<MODE>(B.side[3], i, Fc, acc);
+  NodeMat m;
+  if (HET) {
+    m.rho = B.rho[c]; m.G = B.G[c];
+    if (MODE == 2) { m.M = B.M[c]; m.gamma = B.gamma[c]; m.nu = B.nu[c]; }
+    else { m.M = 0.0; m.gamma = 0.0; m.nu = 0.0; }
+  } else {
+    m.rho = B.rho_b; m.G = B.G_b; m.M = B.M_b; m.gamma = B.gamma_b; m.nu = B.nu_b;
+  }
+  closure_rates<MODE, PI_>(D, B, Fin, i, j, m, B.Ji[c], acc);
+  if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
+  body_forces<MODE>(D, B, i, j, a.t, acc);
+#pragma unroll
+  for (int l = 0; l < NF; ++l) B.DF[l * plane + c] = acc[l];
+  if (a.update) {
+    double* __restrict__ Fout = B.F[a.out];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fout[l * plane + c] = Fc[l] + a.Bdt * acc[l];
   }
 }
 
@@ -241,20 +343,17 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
   if (i >= nx || j >= ny) return;
   const long long c = (long long)j * pitch + i;
 
+  if (!interior_node(D, B, i, j)) return;  // closure strips: closure_kernel
   double acc[NF];
+  const bool load_df = a.scale && a.A != 0.0;
 #pragma unroll
-  for (int l = 0; l < NF; ++l) acc[l] = a.A * B.DF[l * plane + c];
+  for (int l = 0; l < NF; ++l) acc[l] = load_df ? a.A * B.DF[l * plane + c] : 0.0;
+  if (MODE == 2) acc[5] = 0.0;
 
   double Fc[NF];
 #pragma unroll
   for (int l = 0; l < NR; ++l) Fc[l] = sF[l][ty + H][tx + H];
   if (MODE == 2) Fc[5] = Fin[5 * plane + c];
-
-  // SAT on the block edges, in the reference's side order L, R, B, T
-  if (i == 0) sat_term<MODE>(B.side[0], j, Fc, acc);
-  if (i == nx - 1) sat_term<MODE>(B.side[1], j, Fc, acc);
-  if (j == 0) sat_term<MODE>(B.side[2], i, Fc, acc);
-  if (j == ny - 1) sat_term<MODE>(B.side[3], i, Fc, acc);
 
   NodeMat m;
   if (HET) {
@@ -265,10 +364,7 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
     m.rho = B.rho_b; m.G = B.G_b; m.M = B.M_b; m.gamma = B.gamma_b; m.nu = B.nu_b;
   }
   const double Ji = B.Ji[c];
-  const int nbst = D.nbst;
-  const bool interior = (i >= nbst && i <= nx - 1 - nbst && j >= nbst && j <= ny - 1 - nbst);
-
-  if (interior) {
+  {
     const int cx = tx + H, cy = ty + H;
     const double yrc = s_yr[ty][cx], xrc = s_xr[ty][cx];
     const double yqc = s_yq[cy][tx], xqc = s_xq[cy][tx];
@@ -300,35 +396,10 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
         acc[r] += sum * cf * Ji;
       }
     }
-  } else {
-    closure_rates<MODE, PI_>(D, B, Fin, i, j, m, Ji, acc);
   }
 
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-
-  // body forces (set_source, source.f90:147-252)
-  if (D.src.use_gravity) {
-    if (MODE == 2) { acc[0] += D.src.gx; acc[1] += D.src.gy; }
-    else acc[0] += D.src.gz;
-  }
-  if (D.src.use_singular && B.src_ok) {
-    int di = i - B.src_i0, dj = j - B.src_j0;
-    if (di >= -2 && di <= 2 && dj >= -2 && dj <= 2) {
-      double A = stf_amp(D.src, a.t);
-      double dx = B.src_wx[di + 2], dy = B.src_wy[dj + 2];
-      if (MODE == 2) {
-        acc[0] += A * D.src.Fx * dx * dy / B.rho_b;
-        acc[1] += A * D.src.Fy * dx * dy / B.rho_b;
-        acc[2] -= A * D.src.Mxx * dx * dy;
-        acc[3] -= A * D.src.Mxy * dx * dy;
-        acc[4] -= A * D.src.Myy * dx * dy;
-      } else {
-        acc[0] += A * D.src.Fz * dx * dy / B.rho_b;
-        acc[1] -= A * D.src.Mzx * dx * dy;
-        acc[2] -= A * D.src.Mzy * dx * dy;
-      }
-    }
-  }
+  body_forces<MODE>(D, B, i, j, a.t, acc);
 
   double* __restrict__ DF = B.DF;
 #pragma unroll

@@ -28,10 +28,12 @@ class HostDomain:
         self._h = C.c_void_p()
         base = str(base_dir).encode() if base_dir is not None else None
         check_host(lib().fdmap_host_init(input_text.encode(), base, C.byref(self._h)), "init_domain")
-        ints = (C.c_int * 8)()
+        ints = (C.c_int * 10)()
         dbls = (C.c_double * 5)()
         check_host(lib().fdmap_host_info(self._h, ints, dbls), "fdmap_host_info")
-        (self.mode, self.nF, self.nx, self.ny, self.nblocks, self.nifaces, self.nt, self.rk_order) = list(ints)
+        (self.mode, self.nF, self.nx, self.ny, self.nblocks, self.nifaces, self.nt, self.rk_order, self.fd_method,
+         het) = list(ints)
+        self.heterogeneous = bool(het)
         (self.t0, self.dt, self.CFL, self.hmin, self.hmax) = list(dbls)
 
     @property

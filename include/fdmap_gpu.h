@@ -48,6 +48,17 @@ int fdmap_gpu_run(fdmap_gpu* h, double t_start, double dt, int n_first, int n_la
 
 int fdmap_gpu_synchronize(fdmap_gpu* h);
 
+/* Issue all subsequent work on `stream` (a cudaStream_t of the same device,
+ * e.g. the caller's framework stream); NULL restores the handle's own stream. */
+int fdmap_gpu_set_stream(fdmap_gpu* h, void* stream);
+
+/* Per-kernel timing: when enabled, CUDA events bracket every launch on the
+ * handle's stream.  fdmap_gpu_profile_read fills ms[3] / count[3] with the
+ * summed milliseconds and launch counts since enabling: [0] the interior
+ * stencil kernel, [1] the boundary-closure kernel, [2] the interface kernel. */
+int fdmap_gpu_profile(fdmap_gpu* h, int enable);
+int fdmap_gpu_profile_read(fdmap_gpu* h, double* ms, long long* count);
+
 /* Body fields F(nx,ny,nF) and rates DF(nx,ny,nF) in FDMAP's global
  * column-major layout; either pointer may be NULL.  Blocks the host. */
 int fdmap_gpu_get_fields(fdmap_gpu* h, double* F, double* DF);

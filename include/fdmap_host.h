@@ -40,7 +40,7 @@ fdmap_desc* fdmap_host_desc_mut(fdmap_domain* dom);
 void fdmap_host_free(fdmap_domain* dom);
 
 /* Scalar summary for bindings without struct support:
- * ints[8]  = mode, nF, nx, ny, nblocks, nifaces, nt, rk_order
+ * ints[10] = mode, nF, nx, ny, nblocks, nifaces, nt, rk_order, fd_method, heterogeneous
  * dbls[5]  = t0, dt, CFL, hmin, hmax */
 int fdmap_host_info(const fdmap_domain* dom, int* ints, double* dbls);
 
