@@ -177,7 +177,9 @@ def run_gpu(args) -> None:
     host = init_domain(text, base)
     nodes = host.nx * host.ny
     het = host.heterogeneous
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the engine's kernels and the timing events share it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
 
     # ---- device-resident throughput (value)
     g = GpuDomain(host, device=local)

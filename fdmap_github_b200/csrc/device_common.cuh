@@ -40,6 +40,7 @@ struct DevBlock {
   double *xq, *xr, *yq, *yr, *Ji;      // (pitch, ny)
   double *rho, *G, *M, *gamma, *nu;    // heterogeneous only
   double rho_b, G_b, M_b, gamma_b, nu_b;
+  double rinv_b;                       // 1/rho_b
   double coef[4][3];                   // homogeneous interior weights DI(s)/rho, DI(s)*G, DI(s)*M
                                        // (a, b, c of rates_interior_mode2, rates.f90:400-405)
   double F0v[9];
@@ -58,15 +59,22 @@ enum { PAR_A = 0, PAR_B, PAR_V0, PAR_F0, PAR_L, PAR_FW, PAR_VW, PAR_C0, PAR_FS, 
 struct DevFriction {
   int law, reg, rup_field, force, ld_shape, tp_use, has_bsS0, has_bsN0;
   double rup_threshold, angle, xlockm, xlockp, flock, skempton;
+  double cos_angle, sin_angle;  // cos/sin of the fault angle, evaluated once on the host
   double kn_c0, kn_fd, kn_dfdx, kn_vL, kn_vR, kn_xL, kn_xR, kn_tmax;
   double ld_S, ld_N, ld_T, ld_R, ld_x0, ld_y0, tp_p0;
   double* st;
   double* par;
 };
 
+// per-interface-node impedance terms, evaluated once on the host (each is a
+// correctly rounded division, so the values equal the in-kernel ones):
+// 1/Zs-, 1/Zs+, 1/Zp-, 1/Zp+, etas = 1/(1/Zs+ + 1/Zs-), etap = 1/(1/Zp+ + 1/Zp-)
+enum { IC_ZSIM = 0, IC_ZSIP, IC_ZPIM, IC_ZPIP, IC_ETAS, IC_ETAP, IC_N };
+
 struct DevIface {
   int direction, im, ip, m, p, n, coupling;
   int offm, offp;  // side-local index of global node m on the minus / plus side
+  double* icoef;   // (n, IC_N)
   double* nhat;    // (n,2)
   double *x, *y;   // (n)
   DevFriction fr;
@@ -91,14 +99,31 @@ struct DevDomain {
   unsigned long long* status;  // [0] Newton failures, [1] nonfinite flags
 };
 
+// Step clock kept on the device so that a captured CUDA graph can be replayed
+// step after step: step n starts at t0 = t_start + (n-1)*dt (main.f90:176).
+struct TimeState {
+  double t_start, dt;
+  long long n;
+};
+
 struct StageArgs {
   double A;      // RK coefficient A(stage): rates are scaled by it first
   double Bdt;    // B(stage)*dt: state update weight
-  double t;      // stage time
+  double t;      // stage time (when ts == nullptr)
   int in, out;   // F buffer read / written
   int scale;     // scale rates by A (0 for the initial edge solve)
   int update;    // update the state (0 on the final step and the initial solve)
+  const TimeState* ts;  // device step clock (graph replays), or nullptr
+  double C;      // RK C(stage-1): stage time = t0 + C*dt
 };
+
+// Stage time t0 + C*dt with t0 = t_start + (n-1)*dt, rounded exactly as the
+// host (and the reference) evaluate it: no fused multiply-add.
+__device__ __forceinline__ double stage_time(const StageArgs& a) {
+  if (!a.ts) return a.t;
+  const double t0 = __dadd_rn(a.ts->t_start, __dmul_rn((double)(a.ts->n - 1), a.ts->dt));
+  return __dadd_rn(t0, __dmul_rn(a.C, a.ts->dt));
+}
 
 // ---------------------------------------------------------------------------
 // rotations (geometry.f90:285-336; fields.f90:1297-1356)

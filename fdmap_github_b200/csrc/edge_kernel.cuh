@@ -35,7 +35,7 @@ __device__ __forceinline__ double d_boxcar(double r, double w, double fin, doubl
 // load_stress default branch + load_ramp (friction.f90:1317-1374, 1455-1484)
 __device__ void d_load_stress(const DevFriction& FR, int n, int k, double x, double y, double t, double& S0,
                               double& N0) {
-  double xx = x * cos(FR.angle) + y * sin(FR.angle);
+  double xx = x * FR.cos_angle + y * FR.sin_angle;
   double r = fabs((xx - FR.ld_x0) / FR.ld_R);
   S0 = FR.has_bsS0 ? FR.par[PAR_BSS0 * n + k] : 0.0;
   N0 = FR.has_bsN0 ? FR.par[PAR_BSN0 * n + k] : 0.0;
@@ -191,7 +191,7 @@ __device__ void d_solve_friction(const DevFriction& FR, int n, int k, NodeState&
   }
   if (dt == 0.0) st.Nreg = st.N;
   if (!FR.reg) st.Nreg = st.N;
-  double xx = x * cos(FR.angle) + y * sin(FR.angle);
+  double xx = x * FR.cos_angle + y * FR.sin_angle;
   if (xx < FR.xlockm || xx > FR.xlockp) {
     st.S = FR.flock * st.Nreg;
     if (fabs(Slock) >= st.S) { st.S = fsign(st.S, Slock); st.V = (Slock - st.S) / eta; }
@@ -294,7 +294,8 @@ __device__ __forceinline__ void side_node_local(int s, int k, int nx, int ny, in
 // interface node (interfaces.f90:676-1012 + friction register life cycle)
 // ---------------------------------------------------------------------------
 template <int MODE>
-__device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const StageArgs& a) {
+__device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const StageArgs& a, double* Fhm_out = nullptr,
+                             double* Fhp_out = nullptr) {
   constexpr int NF = MODE == 2 ? 6 : 3;
   const DevBlock& Bm = D.blk[I.im];
   const DevBlock& Bp = D.blk[I.ip];
@@ -324,14 +325,15 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
       double rp[6], rm[6];
       rot2_xy2nt(Fp, n0, n1, rp);
       rot2_xy2nt(Fm, n0, n1, rm);
-      double Zsip = 1.0 / Zsp, Zsim = 1.0 / Zsm, Zpip = 1.0 / Zpp, Zpim = 1.0 / Zpm;
-      double etap = 1.0 / (Zpip + Zpim);
+      const double Zsip = I.icoef[IC_ZSIP * I.n + k], Zsim = I.icoef[IC_ZSIM * I.n + k];
+      const double Zpip = I.icoef[IC_ZPIP * I.n + k], Zpim = I.icoef[IC_ZPIM * I.n + k];
+      double etap = I.icoef[IC_ETAP * I.n + k];
       double phip = etap * (rp[4] * Zpip + rm[4] * Zpim + rp[1] - rm[1]);
       double vnp = rp[1] + Zpip * (rp[4] - phip);
       double vnm = rm[1] - Zpim * (rm[4] - phip);
       double sttp = rp[2] - gp * (rp[4] - phip), sttm = rm[2] - gm * (rm[4] - phip);
       double szzp = rp[5] - gp * (rp[4] - phip), szzm = rm[5] - gm * (rm[4] - phip);
-      double etas = 1.0 / (Zsip + Zsim);
+      double etas = I.icoef[IC_ETAS * I.n + k];
       double phis = etas * (rp[3] * Zsip + rm[3] * Zsim + rp[0] - rm[0]);
       double vtp = rp[0] + Zsip * (rp[3] - phis);
       double vtm = rm[0] - Zsim * (rm[3] - phis);
@@ -341,8 +343,8 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
       double rp[3], rm[3];
       rot3_xy2nt(Fp, n0, n1, rp);
       rot3_xy2nt(Fm, n0, n1, rm);
-      double Zsip = 1.0 / Zsp, Zsim = 1.0 / Zsm;
-      double etas = 1.0 / (Zsip + Zsim);
+      const double Zsip = I.icoef[IC_ZSIP * I.n + k], Zsim = I.icoef[IC_ZSIM * I.n + k];
+      double etas = I.icoef[IC_ETAS * I.n + k];
       double phis = etas * (rp[2] * Zsip + rm[2] * Zsim + rp[0] - rm[0]);
       double vzp = rp[0] + Zsip * (rp[2] - phis);
       double vzm = rm[0] - Zsim * (rm[2] - phis);
@@ -376,14 +378,15 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
       for (int l = 0; l < 6; ++l) { dp[l] = Fp[l] - dF0p[l]; dm[l] = Fm[l] - dF0m[l]; }
       rot2_xy2nt(dp, n0, n1, rp);
       rot2_xy2nt(dm, n0, n1, rm);
-      double Zsip = 1.0 / Zsp, Zsim = 1.0 / Zsm, Zpip = 1.0 / Zpp, Zpim = 1.0 / Zpm;
-      double etas = 1.0 / (Zsip + Zsim);
+      const double Zsip = I.icoef[IC_ZSIP * I.n + k], Zsim = I.icoef[IC_ZSIM * I.n + k];
+      const double Zpip = I.icoef[IC_ZPIP * I.n + k], Zpim = I.icoef[IC_ZPIM * I.n + k];
+      double etas = I.icoef[IC_ETAS * I.n + k];
       double phis = etas * (rp[3] * Zsip + rm[3] * Zsim + rp[0] - rm[0]);
-      double etap = 1.0 / (Zpip + Zpim);
+      double etap = I.icoef[IC_ETAP * I.n + k];
       double phip = etap * (rp[4] * Zpip + rm[4] * Zpim + rp[1] - rm[1]);
       double S0 = r0p[3];
       double N0 = -r0p[4] - p;
-      d_solve_friction(FR, n, k, ns, S0, N0, phip, phis, etas, x, y, a.t, a.Bdt, D.status);
+      d_solve_friction(FR, n, k, ns, S0, N0, phip, phis, etas, x, y, stage_time(a), a.Bdt, D.status);
       double snn = -(ns.N - ns.N0) / (1.0 - FR.skempton);
       double vnp = rp[1] + Zpip * (rp[4] - snn);
       double vnm = rm[1] - Zpim * (rm[4] - snn);
@@ -403,14 +406,14 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
       double rp[3], rm[3];
       rot3_xy2nt(dp, n0, n1, rp);
       rot3_xy2nt(dm, n0, n1, rm);
-      double Zsip = 1.0 / Zsp, Zsim = 1.0 / Zsm;
-      double etas = 1.0 / (Zsip + Zsim);
+      const double Zsip = I.icoef[IC_ZSIP * I.n + k], Zsim = I.icoef[IC_ZSIM * I.n + k];
+      double etas = I.icoef[IC_ETAS * I.n + k];
       double phis = etas * (rp[2] * Zsip + rm[2] * Zsim + rp[0] - rm[0]);
       double S0 = r0p[2];
       double stt, snt, snn;
       xy2nt_mat(Bp.F0v[3], Bp.F0v[4], Bp.F0v[6], stt, snt, snn, n0, n1);
       double N0 = -snn - p;
-      d_solve_friction(FR, n, k, ns, S0, N0, 0.0, phis, etas, x, y, a.t, a.Bdt, D.status);
+      d_solve_friction(FR, n, k, ns, S0, N0, 0.0, phis, etas, x, y, stage_time(a), a.Bdt, D.status);
       double snz = ns.S - ns.S0;
       double vzp = rp[0] + Zsip * (rp[2] - snz);
       double vzm = rm[0] - Zsim * (rm[2] - snz);
@@ -430,7 +433,7 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
     DW = DW + ns.S * ns.V;
     double trup = st[ST_TRUP * n + k];
     bool rup = FR.rup_field == 1 ? (ns.D > FR.rup_threshold) : (fabs(ns.V) > FR.rup_threshold);
-    if (rup) trup = fmin(trup, a.t);
+    if (rup) trup = fmin(trup, stage_time(a));
     st[ST_TRUP * n + k] = trup;
     st[ST_V * n + k] = ns.V; st[ST_O * n + k] = ns.O; st[ST_S * n + k] = ns.S; st[ST_N * n + k] = ns.N;
     st[ST_S0 * n + k] = ns.S0; st[ST_N0 * n + k] = ns.N0;
@@ -453,13 +456,16 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
     Sm.Fhat[km + Sm.n * l] = Fhm[l];
     Sp.Fhat[kp + Sp.n * l] = Fhp[l];
   }
+  if (Fhm_out) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) { Fhm_out[l] = Fhm[l]; Fhp_out[l] = Fhp[l]; }
+  }
 }
 
 // One thread per interface node: the locked / frictional solve of this stage,
 // hat variables of both sides, and the fault register life cycle.
 template <int MODE>
-__global__ void __launch_bounds__(128) edge_kernel(const DevDomain* __restrict__ Dp, StageArgs a) {
-  const DevDomain& D = *Dp;
+__global__ void __launch_bounds__(128) edge_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
   int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.seg_start[D.nseg]) return;
   int sg = 0;

@@ -56,6 +56,17 @@ void source_weights(double h, double a, double* w) {
 
 }  // namespace
 
+namespace fdmap {
+// end of a replayed step: advance the device step clock
+__global__ void advance_step(TimeState* ts) { ts->n += 1; }
+// start of a replayed sequence: set the step clock (by value, no host buffer to keep alive)
+__global__ void set_step_clock(TimeState* ts, double t_start, double dt, long long n) {
+  ts->t_start = t_start;
+  ts->dt = dt;
+  ts->n = n;
+}
+}  // namespace fdmap
+
 struct fdmap_gpu {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -75,6 +86,13 @@ struct fdmap_gpu {
   long long march_units = 0;
   int march_grid = 0;
   int use_march = 1;
+  int fused = 0;  // boundary kernel handles interface solves and closure strips in one launch
+  // CUDA graphs of one full step, one per starting F buffer, replayed by fdmap_gpu_run
+  TimeState* d_time = nullptr;
+  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+  double graph_dt = 0.0;
+  long long graph_launches = 0;
+  bool use_graphs = true;
   double* met_base[MAX_BLOCKS] = {};
   double* het_base[MAX_BLOCKS] = {};
   TmapSet* tmaps = nullptr;  // host copy, passed by value to the march kernel
@@ -157,6 +175,8 @@ struct fdmap_gpu {
     if (h_stage) cudaFreeHost(h_stage);
     if (own_stream) cudaStreamDestroy(own_stream);
     delete tmaps;
+    for (auto& ge : step_graph)
+      if (ge) cudaGraphExecDestroy(ge);
   }
 };
 
@@ -179,8 +199,8 @@ int launch_edges(fdmap_gpu* h, const StageArgs& a) {
   int tpb = 128;
   int nb = (h->edge_threads + tpb - 1) / tpb;
   ProfScope ps(h, 2);
-  if (h->mode == 2) edge_kernel<2><<<nb, tpb, 0, h->stream>>>(h->ddom, a);
-  else edge_kernel<3><<<nb, tpb, 0, h->stream>>>(h->ddom, a);
+  if (h->mode == 2) edge_kernel<2><<<nb, tpb, 0, h->stream>>>(h->hdom, a);
+  else edge_kernel<3><<<nb, tpb, 0, h->stream>>>(h->hdom, a);
   h->launches++;
   CUDA_TRY(cudaGetLastError());
   return FDMAP_OK;
@@ -296,20 +316,46 @@ template <int MODE>
 void launch_closure_mode(fdmap_gpu* h, const StageArgs& a) {
   int nb = (int)((h->closure_threads + 127) / 128);
   if (h->het) {
-    if (h->pI == 1) closure_kernel<MODE, 1, true><<<nb, 128, 0, h->stream>>>(h->ddom, a);
-    else if (h->pI == 2) closure_kernel<MODE, 2, true><<<nb, 128, 0, h->stream>>>(h->ddom, a);
-    else closure_kernel<MODE, 3, true><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+    if (h->pI == 1) closure_kernel<MODE, 1, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else if (h->pI == 2) closure_kernel<MODE, 2, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else closure_kernel<MODE, 3, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
   } else {
-    if (h->pI == 1) closure_kernel<MODE, 1, false><<<nb, 128, 0, h->stream>>>(h->ddom, a);
-    else if (h->pI == 2) closure_kernel<MODE, 2, false><<<nb, 128, 0, h->stream>>>(h->ddom, a);
-    else closure_kernel<MODE, 3, false><<<nb, 128, 0, h->stream>>>(h->ddom, a);
+    if (h->pI == 1) closure_kernel<MODE, 1, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else if (h->pI == 2) closure_kernel<MODE, 2, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else closure_kernel<MODE, 3, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
   }
 }
 
-// one stage: interface solves, then closure strips (which read the interface
-// hat variables), then the interior; all read F[in] and write disjoint nodes
-int launch_stencil(fdmap_gpu* h, const StageArgs& a) {
-  {
+template <int MODE>
+void launch_boundary_mode(fdmap_gpu* h, const StageArgs& a) {
+  long long items = h->edge_threads + h->closure_threads;
+  int nb = (int)((items + 127) / 128);
+  if (h->het) {
+    if (h->pI == 1) boundary_kernel<MODE, 1, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else if (h->pI == 2) boundary_kernel<MODE, 2, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else boundary_kernel<MODE, 3, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+  } else {
+    if (h->pI == 1) boundary_kernel<MODE, 1, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else if (h->pI == 2) boundary_kernel<MODE, 2, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    else boundary_kernel<MODE, 3, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+  }
+}
+
+// one stage.  Boundary work first -- with no multi-interface junction nodes a
+// single boundary kernel (interface solves and closure strips are
+// independent items); otherwise interface solves, then closure strips (which
+// read the interface hat variables) -- then the interior.  All of them read
+// F[in] and write disjoint nodes.
+int launch_stage(fdmap_gpu* h, const StageArgs& a) {
+  if (h->fused) {
+    ProfScope pc(h, 1);
+    if (h->mode == 2) launch_boundary_mode<2>(h, a);
+    else launch_boundary_mode<3>(h, a);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+  } else {
+    int rc = launch_edges(h, a);
+    if (rc) return rc;
     ProfScope pc(h, 1);
     if (h->mode == 2) launch_closure_mode<2>(h, a);
     else launch_closure_mode<3>(h, a);
@@ -426,6 +472,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       h->het_base[b] = het_base;
     }
     B.rho_b = fb.rho; B.G_b = fb.G; B.M_b = fb.M; B.gamma_b = fb.gamma; B.nu_b = fb.nu;
+    B.rinv_b = 1.0 / fb.rho;
     for (int s = 1; s <= op.pI; ++s) {
       B.coef[s][0] = op.DI[s] / fb.rho;
       B.coef[s][1] = op.DI[s] * fb.G;
@@ -482,6 +529,24 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     Sm.cov_lo = I.offm; Sm.cov_hi = I.offm + I.n;
     Sp.cov_lo = I.offp; Sp.cov_hi = I.offp + I.n;
     int rc;
+    {
+      // impedance terms of both sides (interfaces.f90:696-699, 735-760, 851-855, 956-965)
+      const fdmap_side& fsm = Bm.side[fi.direction == 0 ? 1 : 3];
+      const fdmap_side& fsp = Bp.side[fi.direction == 0 ? 0 : 2];
+      std::vector<double> ic((size_t)IC_N * I.n);
+      for (int q = 0; q < I.n; ++q) {
+        double Zsm = fsm.M[I.offm + q], Zsp = fsp.M[I.offp + q];
+        double Zpm = fsm.M[I.offm + q + fsm.n], Zpp = fsp.M[I.offp + q + fsp.n];
+        double Zsim = 1.0 / Zsm, Zsip = 1.0 / Zsp, Zpim = 1.0 / Zpm, Zpip = 1.0 / Zpp;
+        ic[(size_t)IC_ZSIM * I.n + q] = Zsim;
+        ic[(size_t)IC_ZSIP * I.n + q] = Zsip;
+        ic[(size_t)IC_ZPIM * I.n + q] = Zpim;
+        ic[(size_t)IC_ZPIP * I.n + q] = Zpip;
+        ic[(size_t)IC_ETAS * I.n + q] = 1.0 / (Zsip + Zsim);
+        ic[(size_t)IC_ETAP * I.n + q] = 1.0 / (Zpip + Zpim);
+      }
+      if ((rc = h->upload(&I.icoef, ic.data(), ic.size()))) return rc;
+    }
     if ((rc = h->upload(&I.nhat, fi.nhat, 2 * (size_t)I.n))) return rc;
     if ((rc = h->upload(&I.x, fi.x, (size_t)I.n))) return rc;
     if ((rc = h->upload(&I.y, fi.y, (size_t)I.n))) return rc;
@@ -492,6 +557,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     FR.ld_shape = ff.ld_shape; FR.tp_use = ff.tp_use;
     FR.has_bsS0 = ff.bsS0 != nullptr; FR.has_bsN0 = ff.bsN0 != nullptr;
     FR.rup_threshold = ff.rup_threshold; FR.angle = ff.angle; FR.xlockm = ff.xlockm; FR.xlockp = ff.xlockp;
+    FR.cos_angle = std::cos(ff.angle); FR.sin_angle = std::sin(ff.angle);
     FR.flock = ff.flock; FR.skempton = ff.skempton;
     FR.kn_c0 = ff.kn_c0; FR.kn_fd = ff.kn_fd; FR.kn_dfdx = ff.kn_dfdx; FR.kn_vL = ff.kn_vL; FR.kn_vR = ff.kn_vR;
     FR.kn_xL = ff.kn_xL; FR.kn_xR = ff.kn_xR; FR.kn_tmax = ff.kn_tmax;
@@ -536,8 +602,25 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     const char* ek = getenv("FDMAP_STENCIL");
     h->use_march = !(ek && std::string(ek) == "tile");
     if (h->use_march && (rc = march_dispatch(h, nullptr))) return rc;
+    // fused stage launches need every interface-side node to sit on one interface only
+    bool junction = false;
+    for (int b = 0; b < d->nblocks; ++b) {
+      const DevBlock& B = D.blk[b];
+      bool cov[4];
+      for (int q = 0; q < 4; ++q) cov[q] = B.side[q].cov_hi > B.side[q].cov_lo;
+      // a corner node shared by two interface sides
+      if ((cov[0] || cov[1]) && (cov[2] || cov[3])) junction = true;
+    }
+    // one merged boundary launch is opt-in: the two separate launches measure faster
+    const char* ef = getenv("FDMAP_FUSED");
+    h->fused = !junction && (ef && std::string(ef) == "1");
   }
   if ((rc = h->alloc(&h->d_status, 4))) return rc;
+  if ((rc = h->alloc(&h->d_time, 1))) return rc;
+  {
+    const char* eg = getenv("FDMAP_GRAPHS");
+    h->use_graphs = !(eg && std::string(eg) == "0");
+  }
   CUDA_TRY(cudaMemset(h->d_status, 0, 4 * sizeof(unsigned long long)));
   D.status = h->d_status;
   if ((rc = h->alloc(&h->ddom, 1))) return rc;
@@ -550,6 +633,60 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   CUDA_TRY(cudaMallocHost(&h->h_stage, total * sizeof(double)));
   h->cur = 0;
   return fdmap_gpu_set_fields(h, d->F, d->DF);
+}
+
+// all stages of one step starting from buffer `cur`; final = stage 1 only
+int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, const TimeState* ts) {
+  for (int s = 0; s < h->rk.nstage; ++s) {
+    StageArgs a{};
+    a.A = h->rk.A[s];
+    a.Bdt = h->rk.B[s] * dt;
+    a.t = t0 + h->rk.C[s] * dt;
+    a.C = h->rk.C[s];
+    a.ts = ts;
+    a.in = cur;
+    a.out = 1 - cur;
+    a.scale = 1;
+    a.update = final_step ? 0 : 1;
+    int rc = launch_stage(h, a);
+    if (rc) return rc;
+    if (final_step) return FDMAP_OK;
+    cur = 1 - cur;
+  }
+  return FDMAP_OK;
+}
+
+// capture one step per starting buffer; kernels read the step clock from d_time
+int build_step_graphs(fdmap_gpu* h, double dt) {
+  for (auto& ge : h->step_graph)
+    if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  bool prof = h->profiling;
+  h->profiling = false;
+  cudaStream_t keep = h->stream;
+  h->stream = h->own_stream;
+  long long before = h->launches;
+  int rc = FDMAP_OK;
+  for (int c = 0; c < 2 && rc == FDMAP_OK; ++c) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { rc = set_err(FDMAP_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(e)); break; }
+    long long l0 = h->launches;
+    rc = issue_step(h, c, 0.0, dt, false, h->d_time);
+    if (rc == FDMAP_OK) advance_step<<<1, 1, 0, h->stream>>>(h->d_time);
+    h->graph_launches = h->launches - l0 + 1;
+    e = cudaStreamEndCapture(h->stream, &g);
+    if (rc == FDMAP_OK && e != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
+    if (rc == FDMAP_OK) {
+      e = cudaGraphInstantiate(&h->step_graph[c], g, 0);
+      if (e != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    }
+    if (g) cudaGraphDestroy(g);
+  }
+  h->launches = before;
+  h->stream = keep;
+  h->profiling = prof;
+  if (rc == FDMAP_OK) h->graph_dt = dt;
+  return rc;
 }
 
 }  // namespace
@@ -598,28 +735,32 @@ int fdmap_gpu_init_edges(fdmap_gpu* h, double t) {
 int fdmap_gpu_time_step(fdmap_gpu* h, double t0, double dt, int final_step) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
   CUDA_TRY(cudaSetDevice(h->device));
-  for (int s = 0; s < h->rk.nstage; ++s) {
-    StageArgs a{};
-    a.A = h->rk.A[s];
-    a.Bdt = h->rk.B[s] * dt;
-    a.t = t0 + h->rk.C[s] * dt;
-    a.in = h->cur;
-    a.out = 1 - h->cur;
-    a.scale = 1;
-    a.update = final_step ? 0 : 1;
-    int rc = launch_edges(h, a);
-    if (rc) return rc;
-    rc = launch_stencil(h, a);
-    if (rc) return rc;
-    if (final_step) return FDMAP_OK;
-    h->cur = 1 - h->cur;
-  }
+  int rc = issue_step(h, h->cur, t0, dt, final_step != 0, nullptr);
+  if (rc) return rc;
+  if (!final_step && (h->rk.nstage & 1)) h->cur = 1 - h->cur;
   return FDMAP_OK;
 }
 
 int fdmap_gpu_run(fdmap_gpu* h, double t_start, double dt, int n_first, int n_last, int nt) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
   h->launches = 0;
+  int n_graph_last = std::min(n_last, nt - 1);  // the final step (n == nt) is issued directly
+  if (h->use_graphs && !h->profiling && n_graph_last >= n_first) {
+    if (h->graph_dt != dt || !h->step_graph[0]) {
+      int rc = build_step_graphs(h, dt);
+      if (rc) return rc;
+    }
+    set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, t_start, dt, (long long)n_first);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    for (int n = n_first; n <= n_graph_last; ++n) {
+      CUDA_TRY(cudaGraphLaunch(h->step_graph[h->cur], h->stream));
+      h->launches += h->graph_launches;
+      if (h->rk.nstage & 1) h->cur = 1 - h->cur;
+    }
+    n_first = n_graph_last + 1;
+  }
   for (int n = n_first; n <= n_last; ++n) {
     int rc = fdmap_gpu_time_step(h, t_start + (double)(n - 1) * dt, dt, n == nt);
     if (rc) return rc;

@@ -61,6 +61,47 @@ struct MarchPlan {
   long long units;   // total row groups over all strips of all blocks
 };
 
+// Interface node k of interface I, then the whole stage for the two edge nodes
+// it couples (minus side, plus side), using the hat variables just solved.
+template <int MODE, int PI_, bool HET>
+__device__ __forceinline__ void iface_item(const DevDomain& D, const DevIface& I, int k, const StageArgs& a) {
+  double Fhm[6], Fhp[6];
+  d_iface_node<MODE>(D, I, k, a, Fhm, Fhp);
+  const DevBlock& Bm = D.blk[I.im];
+  const DevBlock& Bp = D.blk[I.ip];
+  const int sm = I.direction == 0 ? 1 : 3, sp = I.direction == 0 ? 0 : 2;
+  int im_, jm_, ip_, jp_;
+  side_node_local(sm, I.offm + k, Bm.nx, Bm.ny, im_, jm_);
+  side_node_local(sp, I.offp + k, Bp.nx, Bp.ny, ip_, jp_);
+  closure_node<MODE, PI_, HET>(D, Bm, im_, jm_, a, sm, Fhm);
+  closure_node<MODE, PI_, HET>(D, Bp, ip_, jp_, a, sp, Fhp);
+}
+
+template <int MODE, int PI_, bool HET>
+__device__ __forceinline__ void closure_work(const DevDomain& D, long long it, const StageArgs& a) {
+  int i, j;
+  const int b = closure_item(D, it, i, j);
+  const DevBlock& B = D.blk[b];
+  if (on_interface_side(B, i, j)) return;  // done by the interface item of that node
+  closure_node<MODE, PI_, HET>(D, B, i, j, a, -1, nullptr);
+}
+
+// Boundary kernel: one thread per interface node (solve + its two edge nodes),
+// then one thread per remaining node of the SBP closure strips.  No item
+// depends on another, and none depends on the interior kernel of the stage.
+template <int MODE, int PI_, bool HET>
+__global__ void __launch_bounds__(128) boundary_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
+  const long long nif = D.seg_start[D.nseg];
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid < nif) {
+    int sg = 0;
+    while (tid >= D.seg_start[sg + 1]) ++sg;
+    iface_item<MODE, PI_, HET>(D, D.ifc[D.seg_a[sg]], (int)(tid - D.seg_start[sg]), a);
+  } else if (tid - nif < D.cstart[4 * D.nblocks]) {
+    closure_work<MODE, PI_, HET>(D, tid - nif, a);
+  }
+}
+
 // TMA descriptors of every block, passed by value as a __grid_constant__ parameter
 struct TmapSet {
   CUtensorMap F[MAX_BLOCKS][2];    // rate fields, box {WH, MR, NR}
@@ -155,6 +196,7 @@ __global__ void __launch_bounds__(MTHREADS, 1)
   const long long ubeg = plan.units * blockIdx.x / gridDim.x;
   const long long uend = plan.units * (blockIdx.x + 1) / gridDim.x;
   const bool load_df = a.scale && a.A != 0.0;  // A = 0 (first stage): A*DF = 0, DF is not read
+
   const unsigned cbytes = (unsigned)((load_df ? (size_t)NR * MR * MW * 8 : 0) + (MODE == 2 ? (size_t)MR * MW * 8 : 0) +
                                      (size_t)L::NH * MR * MW * 8);
 
@@ -263,6 +305,7 @@ __global__ void __launch_bounds__(MTHREADS, 1)
         } else {
           m.rho = rho_b; m.G = G_b; m.M = M_b; m.gamma = gamma_b; m.nu = nu_b;
         }
+        m.rinv = HET ? 1.0 / m.rho : 0.0;
         {
           const double* hy = nrow(0, L::MH_OFF, 0, WH) + cx + HP;  // yr, centred on the node
           const double* hx = nrow(0, L::MH_OFF, 1, WH) + cx + HP;  // xr
@@ -300,7 +343,7 @@ __global__ void __launch_bounds__(MTHREADS, 1)
           }
         }
         if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-        body_forces<MODE>(D, B, i, j, a.t, acc);
+        body_forces<MODE>(D, B, i, j, stage_time(a), acc);
 #pragma unroll
         for (int l = 0; l < NF; ++l) DFp[l * plane + c] = acc[l];
         if (a.update) {

@@ -41,11 +41,12 @@ constexpr int TY = 8;
 
 struct NodeMat {
   double rho, G, M, gamma, nu;
+  double rinv;  // 1/rho
 };
 
 __device__ __forceinline__ double mat_coef(const NodeMat& m, int kind, double w) {
-  // w/rho, w*G, w*M
-  return kind == 0 ? w / m.rho : (kind == 1 ? w * m.G : w * m.M);
+  // w/rho, w*G, w*M (the division is taken once per node through rinv)
+  return kind == 0 ? w * m.rinv : (kind == 1 ? w * m.G : w * m.M);
 }
 
 // flux of rate r at point k: q direction +t1 - t2 (Yr, Xr), r direction -t1 + t2 (Yq, Xq);
@@ -69,12 +70,15 @@ __device__ __forceinline__ double flux(int r, double Ym, double Xm, const double
 
 // Closure-region rates for node (i, j) read through the cache hierarchy
 // (rates_boundary_mode2/3 and the heterogeneous variants).
+__host__ __device__ constexpr int nbnd_of(int pI) { return pI == 1 ? 2 : (pI == 2 ? 6 : 9); }
+
 template <int MODE, int PI_>
 __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock& B, const double* __restrict__ Fin, int i, int j,
                               const NodeMat& m, double Ji, double* acc) {
   using RD = RDef<MODE>;
   constexpr int NR = RD::NR;
-  const int nx = B.nx, ny = B.ny, nbst = D.nbst, nbnd = D.nbnd;
+  constexpr int nbnd = nbnd_of(PI_);  // one-sided stencil width (fd_coeff.f90:57-70)
+  const int nx = B.nx, ny = B.ny, nbst = D.nbst;
   const long long pitch = B.pitch, plane = B.plane;
   const long long c = (long long)j * pitch + i;
   const int qreg = i < nbst ? 0 : (i > nx - 1 - nbst ? 1 : -1);
@@ -113,6 +117,7 @@ __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock
     else { w = -D.DL[ny - 1 - j][s]; k = (long long)(ny - 1 - s) * pitch + i; }
   };
   if (qreg >= 0 && rreg >= 0) {
+#pragma unroll
     for (int s = 0; s < nbnd; ++s) {
       double w; long long k;
       qone(s, w, k);
@@ -121,6 +126,7 @@ __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock
       rterm(k, w, 1);
     }
   } else if (qreg >= 0) {
+#pragma unroll
     for (int s = 0; s < nbnd; ++s) {
       double w; long long k;
       qone(s, w, k);
@@ -132,6 +138,7 @@ __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock
       rterm(c - s * pitch, D.DI[s], -1);
     }
   } else {
+#pragma unroll
     for (int s = 0; s < nbnd; ++s) {
       double w; long long k;
       rone(s, w, k);
@@ -145,27 +152,25 @@ __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock
   }
 }
 
-// SAT penalty of side s at side-local index k for the node whose fields are F
-// (SAT_term / split_sp, time_step.f90:813-851).  On an outer boundary the hat
-// variables depend only on this node's fields (set_bc, boundaries.f90:132-377),
-// so they are evaluated here and stored for inspection; on an interface they
-// were written by the interface kernel of this stage.
+// Hat variables of an outer-boundary node depend only on the node's own fields
+// (set_bc, boundaries.f90:132-377), so they are evaluated where they are used
+// and stored for inspection.
 template <int MODE>
-__device__ __forceinline__ void sat_term(const DevSide& S, int k, const double* F, double* acc) {
+__device__ __forceinline__ void bc_hat(const DevSide& S, int k, const double* F, double* Fh) {
+  constexpr int NF = MODE == 2 ? 6 : 3;
+  double F0[6];
+#pragma unroll
+  for (int l = 0; l < NF; ++l) F0[l] = S.F0[k + S.n * l];
+  d_set_bc<MODE>(Fh, F, F0, S.nrm[k], S.nrm[k + S.n], S.bc, S.M[k], S.M[k + S.n], S.M[k + 2 * S.n]);
+#pragma unroll
+  for (int l = 0; l < NF; ++l) S.Fhat[k + S.n * l] = Fh[l];
+}
+
+// SAT penalty (SAT_term / split_sp, time_step.f90:813-851) with hat variables Fh
+template <int MODE>
+__device__ __forceinline__ void sat_apply(const DevSide& S, int k, const double* F, const double* Fh, double* acc) {
   constexpr int NF = MODE == 2 ? 6 : 3;
   double Ks = S.M[k + 3 * S.n], Kp = S.M[k + 4 * S.n];
-  double Fh[6];
-  if (S.bc != FDMAP_BC_NONE && !(k >= S.cov_lo && k < S.cov_hi)) {
-    double F0[6];
-#pragma unroll
-    for (int l = 0; l < NF; ++l) F0[l] = S.F0[k + S.n * l];
-    d_set_bc<MODE>(Fh, F, F0, S.nrm[k], S.nrm[k + S.n], S.bc, S.M[k], S.M[k + S.n], S.M[k + 2 * S.n]);
-#pragma unroll
-    for (int l = 0; l < NF; ++l) S.Fhat[k + S.n * l] = Fh[l];
-  } else {
-#pragma unroll
-    for (int l = 0; l < NF; ++l) Fh[l] = S.Fhat[k + S.n * l];
-  }
   double d[6];
 #pragma unroll
   for (int l = 0; l < NF; ++l) d[l] = Fh[l] - F[l];
@@ -183,6 +188,26 @@ __device__ __forceinline__ void sat_term(const DevSide& S, int k, const double* 
 #pragma unroll
     for (int l = 0; l < 6; ++l) acc[l] += Kp * Fp[l];
   }
+}
+
+// SAT of side s for the node with fields F: hat variables from `Fh_given` when
+// s == iside (an interface solve done by the caller), evaluated in place on
+// an outer boundary, or read back from the interface kernel's output.
+template <int MODE>
+__device__ __forceinline__ void sat_term(const DevSide& S, int s, int k, const double* F, double* acc, int iside,
+                                         const double* Fh_given) {
+  constexpr int NF = MODE == 2 ? 6 : 3;
+  double Fh[6];
+  if (s == iside) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fh[l] = Fh_given[l];
+  } else if (S.bc != FDMAP_BC_NONE && !(k >= S.cov_lo && k < S.cov_hi)) {
+    bc_hat<MODE>(S, k, F, Fh);
+  } else {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fh[l] = S.Fhat[k + S.n * l];
+  }
+  sat_apply<MODE>(S, k, F, Fh, acc);
 }
 
 // singular source amplitude (source.f90:208-223)
@@ -230,27 +255,14 @@ __device__ __forceinline__ bool interior_node(const DevDomain& D, const DevBlock
   return i >= D.nbst && i <= B.nx - 1 - D.nbst && j >= D.nbst && j <= B.ny - 1 - D.nbst;
 }
 
-// Boundary kernel: every node within nbst of a block edge (the SBP closure
-// strips) -- scale, SAT (with boundary hat variables evaluated in place),
-// one-sided closure rates (rates_boundary_mode2/3), szz, sources, update.
-// Thread -> (block, strip, node) through the per-block strip offsets.
+// Whole stage for one node of the SBP closure strips: scale, SAT (sides in the
+// reference's order L, R, B, T), one-sided closure rates (rates_boundary_mode2/3),
+// szz, sources, update.  Side `iside` takes the caller's hat variables.
 template <int MODE, int PI_, bool HET>
-__global__ void __launch_bounds__(128) closure_kernel(const DevDomain* __restrict__ Dp, StageArgs a) {
+__device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock& B, int i, int j, const StageArgs& a,
+                                             int iside, const double* Fh_given) {
   constexpr int NF = MODE == 2 ? 6 : 3;
-  const DevDomain& D = *Dp;
-  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= D.cstart[4 * D.nblocks]) return;
-  int sg = 0;
-  while (tid >= D.cstart[sg + 1]) ++sg;
-  const int b = sg >> 2, strip = sg & 3;
-  const DevBlock& B = D.blk[b];
-  const int nbst = D.nbst, nx = B.nx, ny = B.ny;
-  long long k = tid - D.cstart[sg];
-  int i, j;
-  if (strip == 0) { j = (int)(k / nx); i = (int)(k % nx); }                      // bottom rows
-  else if (strip == 1) { j = ny - nbst + (int)(k / nx); i = (int)(k % nx); }     // top rows
-  else if (strip == 2) { j = nbst + (int)(k / nbst); i = (int)(k % nbst); }       // left columns
-  else { j = nbst + (int)(k / nbst); i = nx - nbst + (int)(k % nbst); }           // right columns
+  const int nx = B.nx, ny = B.ny;
   const long long pitch = B.pitch, plane = B.plane;
   const long long c = (long long)j * pitch + i;
   const double* __restrict__ Fin = B.F[a.in];
@@ -262,10 +274,10 @@ __global__ void __launch_bounds__(128) closure_kernel(const DevDomain* __restric
   double Fc[NF];
 #pragma unroll
   for (int l = 0; l < NF; ++l) Fc[l] = Fin[l * plane + c];
-  if (i == 0) sat_term<MODE>(B.side[0], j, Fc, acc);
-  if (i == nx - 1) sat_term<MODE>(B.side[1], j, Fc, acc);
-  if (j == 0) sat_term<MODE>(B.side[2], i, Fc, acc);
-  if (j == ny - 1) sat_term<MODE>(B.side[3], i, Fc, acc);
+  if (i == 0) sat_term<MODE>(B.side[0], 0, j, Fc, acc, iside, Fh_given);
+  if (i == nx - 1) sat_term<MODE>(B.side[1], 1, j, Fc, acc, iside, Fh_given);
+  if (j == 0) sat_term<MODE>(B.side[2], 2, i, Fc, acc, iside, Fh_given);
+  if (j == ny - 1) sat_term<MODE>(B.side[3], 3, i, Fc, acc, iside, Fh_given);
   NodeMat m;
   if (HET) {
     m.rho = B.rho[c]; m.G = B.G[c];
@@ -274,9 +286,10 @@ __global__ void __launch_bounds__(128) closure_kernel(const DevDomain* __restric
   } else {
     m.rho = B.rho_b; m.G = B.G_b; m.M = B.M_b; m.gamma = B.gamma_b; m.nu = B.nu_b;
   }
+  m.rinv = HET ? 1.0 / m.rho : B.rinv_b;
   closure_rates<MODE, PI_>(D, B, Fin, i, j, m, B.Ji[c], acc);
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-  body_forces<MODE>(D, B, i, j, a.t, acc);
+  body_forces<MODE>(D, B, i, j, stage_time(a), acc);
 #pragma unroll
   for (int l = 0; l < NF; ++l) B.DF[l * plane + c] = acc[l];
   if (a.update) {
@@ -284,6 +297,40 @@ __global__ void __launch_bounds__(128) closure_kernel(const DevDomain* __restric
 #pragma unroll
     for (int l = 0; l < NF; ++l) Fout[l * plane + c] = Fc[l] + a.Bdt * acc[l];
   }
+}
+
+// closure strip item -> block-local node; returns the block
+__device__ __forceinline__ int closure_item(const DevDomain& D, long long tid, int& i, int& j) {
+  int sg = 0;
+  while (tid >= D.cstart[sg + 1]) ++sg;
+  const int b = sg >> 2, strip = sg & 3;
+  const DevBlock& B = D.blk[b];
+  const int nbst = D.nbst, nx = B.nx, ny = B.ny;
+  long long k = tid - D.cstart[sg];
+  if (strip == 0) { j = (int)(k / nx); i = (int)(k % nx); }                      // bottom rows
+  else if (strip == 1) { j = ny - nbst + (int)(k / nx); i = (int)(k % nx); }     // top rows
+  else if (strip == 2) { j = nbst + (int)(k / nbst); i = (int)(k % nbst); }       // left columns
+  else { j = nbst + (int)(k / nbst); i = nx - nbst + (int)(k % nbst); }           // right columns
+  return b;
+}
+
+// true if node (i, j) lies on a block side whose hat variables come from an interface
+__device__ __forceinline__ bool on_interface_side(const DevBlock& B, int i, int j) {
+  if (i == 0 && j >= B.side[0].cov_lo && j < B.side[0].cov_hi) return true;
+  if (i == B.nx - 1 && j >= B.side[1].cov_lo && j < B.side[1].cov_hi) return true;
+  if (j == 0 && i >= B.side[2].cov_lo && i < B.side[2].cov_hi) return true;
+  if (j == B.ny - 1 && i >= B.side[3].cov_lo && i < B.side[3].cov_hi) return true;
+  return false;
+}
+
+// Boundary kernel: every node within nbst of a block edge (the SBP closure strips).
+template <int MODE, int PI_, bool HET>
+__global__ void __launch_bounds__(128) closure_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
+  long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (tid >= D.cstart[4 * D.nblocks]) return;
+  int i, j;
+  const int b = closure_item(D, tid, i, j);
+  closure_node<MODE, PI_, HET>(D, D.blk[b], i, j, a, -1, nullptr);
 }
 
 template <int MODE, int PI_, bool HET>
@@ -363,6 +410,7 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
   } else {
     m.rho = B.rho_b; m.G = B.G_b; m.M = B.M_b; m.gamma = B.gamma_b; m.nu = B.nu_b;
   }
+  m.rinv = HET ? 1.0 / m.rho : B.rinv_b;
   const double Ji = B.Ji[c];
   {
     const int cx = tx + H, cy = ty + H;
@@ -399,7 +447,7 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
   }
 
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-  body_forces<MODE>(D, B, i, j, a.t, acc);
+  body_forces<MODE>(D, B, i, j, stage_time(a), acc);
 
   double* __restrict__ DF = B.DF;
 #pragma unroll

@@ -110,14 +110,12 @@ def rough_fault_rs(outdir: str | Path, nx: int = 2001, ny: int = 1001, h: float 
     depth = x - x[0]
     N0 = np.minimum(120.0, 20.0 + 10.0 * depth)
     a, b, V0, f0, L, fw, Vw = 0.01, 0.014, 1e-6, 0.6, 0.4, 0.2, 0.1
-    fss = f0 - (b - a) * np.log(Vinit / V0)
     S0 = 0.6 * N0
     _write(out / "stress.dat", S0, N0)
     # state giving slip velocity Vinit under the background stress (strength()
     # of friction.f90:1066-1071 inverted for Psi)
     Psi = a * np.log(2.0 * V0 / Vinit * np.sinh(S0 / (a * N0)))
     _write(out / "state.dat", Psi)
-    del fss
     xa, xb = x[0], x[-1]
     ya, yb = y[0], y[-1]
     tp_list = "&thermpres_list n=64, p0=0d0 /\n" if tp else ""
@@ -138,7 +136,7 @@ def rough_fault_rs(outdir: str | Path, nx: int = 2001, ny: int = 1001, h: float 
 &friction_list friction_law='RFL', rs%a={_f(a)}, rs%b={_f(b)}, rs%V0={_f(V0)}, rs%f0={_f(f0)}, rs%L={_f(L)},
   rs%fw={_f(fw)}, rs%Vw={_f(Vw)}, stress_file=T, stress_filename='stress.dat',
   state_file=T, state_filename='state.dat',
-  ld%shape='gaussian', ld%R=1.5d0, ld%S=25d0, ld%x0={_f(0.25 * Lx * 0 + x[nx // 2])},
+  ld%shape='gaussian', ld%R=1.5d0, ld%S=25d0, ld%x0={_f(x[nx // 2])},
   rup_field='V', rup_threshold=1d-3 /
 {tp_list}"""
 

@@ -1,0 +1,172 @@
+! fdmap_gpu_mod -- ISO_C_BINDING interfaces to the B200 time-stepping engine
+! (include/fdmap_gpu.h, include/fdmap_host.h).
+!
+! A Fortran driver keeps its own init_domain and time loop (main.f90) and
+! hands the domain to the engine once; fdmap_gpu_time_step then replaces the
+! body of time_step_LS (time_step.f90:96-165) for one step.  The descriptor
+! (type(fdmap_desc_t) below mirrors struct fdmap_desc field by field) holds
+! plain values and c_loc() pointers to the driver's own arrays:
+!   F(C%mx:C%px, C%my:C%py, nF) -> F      (no ghost layers: pass F(mx:px,my:py,:)
+!                                          through a contiguous copy when the
+!                                          driver keeps ghosts)
+!   G%xq, G%xr, G%yq, G%yr, G%J, G%Ji -> metric pointers, same layout
+!   BF%bndFL%M(:,1:5), %F0, B%bndL%n  -> fdmap_side_t of each block side
+!   I%nhat, I%x, I%y, I%FR%...        -> fdmap_iface_t / fdmap_friction_t
+! Every routine returns 0 or a negative FDMAP_ERR_* code; none aborts.
+module fdmap_gpu_mod
+
+  use, intrinsic :: iso_c_binding, only : c_int, c_double, c_ptr, c_char, c_long_long, c_null_ptr
+
+  implicit none
+
+  integer(c_int), parameter :: FDMAP_OK = 0, FDMAP_ERR_INVALID_ARG = -1, FDMAP_ERR_CUDA = -2, &
+       FDMAP_ERR_NONFINITE = -3, FDMAP_ERR_NEWTON_NOCONV = -4, FDMAP_ERR_TIMEOUT = -5, &
+       FDMAP_ERR_UNSUPPORTED = -6, FDMAP_ERR_IO = -7, FDMAP_ERR_NOMEM = -8
+
+  ! fault fields, in checkpoint_friction order (friction.f90:528-546)
+  integer(c_int), parameter :: FDMAP_FAULT_D = 0, FDMAP_FAULT_PSI = 1, FDMAP_FAULT_DPSI = 2, &
+       FDMAP_FAULT_TRUP = 3, FDMAP_FAULT_V = 4, FDMAP_FAULT_O = 5, FDMAP_FAULT_S = 6, &
+       FDMAP_FAULT_N = 7, FDMAP_FAULT_S0 = 8, FDMAP_FAULT_N0 = 9, FDMAP_FAULT_DS = 10, &
+       FDMAP_FAULT_DN = 11, FDMAP_FAULT_DDS = 12, FDMAP_FAULT_DDN = 13, FDMAP_FAULT_W = 14, &
+       FDMAP_FAULT_DW = 15, FDMAP_FAULT_NREG = 16, FDMAP_FAULT_DNREG = 17
+
+  type, bind(C) :: fdmap_side_t
+     integer(c_int) :: bc, n
+     type(c_ptr) :: M, F0, normal, x, y
+  end type fdmap_side_t
+
+  type, bind(C) :: fdmap_block_t
+     integer(c_int) :: mgx, pgx, mgy, pgy
+     real(c_double) :: rho, cs, cp, G, M, gamma, nu
+     real(c_double) :: F0(9)
+     type(fdmap_side_t) :: side(4)
+     integer(c_int) :: src_ok, src_i0, src_j0
+     real(c_double) :: src_hx, src_hy, src_ax, src_ay
+  end type fdmap_block_t
+
+  type, bind(C) :: fdmap_friction_t
+     integer(c_int) :: law, reg, rup_field
+     real(c_double) :: rup_threshold, angle, xlockm, xlockp, flock, skempton
+     integer(c_int) :: force
+     real(c_double) :: kn_c0, kn_fd, kn_dfdx, kn_vL, kn_vR, kn_xL, kn_xR, kn_tmax
+     integer(c_int) :: ld_shape
+     real(c_double) :: ld_S, ld_N, ld_T, ld_R, ld_x0, ld_y0
+     integer(c_int) :: tp_use
+     real(c_double) :: tp_p0
+     type(c_ptr) :: a, b, V0, f0, L, fw, Vw, c0, fs, fd, Dc, bsS0, bsN0
+     type(c_ptr) :: V, O, S, N, S0, N0, Ds, Dn, DDs, DDn, Psi, DPsi, D, trup, W, DW, Nreg, DNreg
+  end type fdmap_friction_t
+
+  type, bind(C) :: fdmap_iface_t
+     integer(c_int) :: direction, iblockm, iblockp, m, p, coupling
+     type(c_ptr) :: nhat, x, y
+     type(fdmap_friction_t) :: fr
+  end type fdmap_iface_t
+
+  type, bind(C) :: fdmap_source_t
+     integer(c_int) :: use_singular, use_gravity, stf
+     real(c_double) :: x0, y0, t_center, t_duration, Fx, Fy, Fz, Mxx, Mxy, Myy, Mzx, Mzy, gx, gy, gz
+  end type fdmap_source_t
+
+  type, bind(C) :: fdmap_desc_t
+     integer(c_int) :: mode, nF, fd_method, rk_order, nx, ny, nblocks, nifaces
+     type(c_ptr) :: blocks, ifaces
+     integer(c_int) :: heterogeneous
+     type(c_ptr) :: F, DF, x, y, xq, xr, yq, yr, J, Ji
+     type(c_ptr) :: rho, cs, cp, G, M, gamma, nu
+     type(fdmap_source_t) :: src
+     real(c_double) :: t0, dt, CFL
+     integer(c_int) :: nt
+     real(c_double) :: hmin, hmax
+  end type fdmap_desc_t
+
+  interface
+
+     ! ---- engine (include/fdmap_gpu.h)
+     integer(c_int) function fdmap_gpu_create(d, device, init_edges, h) bind(C, name='fdmap_gpu_create')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: d
+       integer(c_int), value :: device, init_edges
+       type(c_ptr), intent(out) :: h
+     end function fdmap_gpu_create
+
+     integer(c_int) function fdmap_gpu_init_edges(h, t) bind(C, name='fdmap_gpu_init_edges')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: t
+     end function fdmap_gpu_init_edges
+
+     integer(c_int) function fdmap_gpu_time_step(h, t0, dt, final_step) bind(C, name='fdmap_gpu_time_step')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: t0, dt
+       integer(c_int), value :: final_step
+     end function fdmap_gpu_time_step
+
+     integer(c_int) function fdmap_gpu_run(h, t_start, dt, n_first, n_last, nt) bind(C, name='fdmap_gpu_run')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: t_start, dt
+       integer(c_int), value :: n_first, n_last, nt
+     end function fdmap_gpu_run
+
+     integer(c_int) function fdmap_gpu_synchronize(h) bind(C, name='fdmap_gpu_synchronize')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function fdmap_gpu_synchronize
+
+     integer(c_int) function fdmap_gpu_get_fields(h, F, DF) bind(C, name='fdmap_gpu_get_fields')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, F, DF
+     end function fdmap_gpu_get_fields
+
+     integer(c_int) function fdmap_gpu_set_fields(h, F, DF) bind(C, name='fdmap_gpu_set_fields')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, F, DF
+     end function fdmap_gpu_set_fields
+
+     integer(c_int) function fdmap_gpu_get_fault(h, iface, field, out) bind(C, name='fdmap_gpu_get_fault')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: iface, field
+       real(c_double), intent(out) :: out(*)
+     end function fdmap_gpu_get_fault
+
+     integer(c_int) function fdmap_gpu_set_fault(h, iface, field, in) bind(C, name='fdmap_gpu_set_fault')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: iface, field
+       real(c_double), intent(in) :: in(*)
+     end function fdmap_gpu_set_fault
+
+     integer(c_int) function fdmap_gpu_status(h, newton_failures) bind(C, name='fdmap_gpu_status')
+       import :: c_int, c_ptr, c_long_long
+       type(c_ptr), value :: h
+       integer(c_long_long), intent(out) :: newton_failures
+     end function fdmap_gpu_status
+
+     subroutine fdmap_gpu_destroy(h) bind(C, name='fdmap_gpu_destroy')
+       import :: c_ptr
+       type(c_ptr), value :: h
+     end subroutine fdmap_gpu_destroy
+
+     ! ---- host initialisation from an FDMAP input text (include/fdmap_host.h)
+     integer(c_int) function fdmap_host_init(input_text, base_dir, dom) bind(C, name='fdmap_host_init')
+       import :: c_int, c_ptr, c_char
+       character(kind=c_char), intent(in) :: input_text(*), base_dir(*)
+       type(c_ptr), intent(out) :: dom
+     end function fdmap_host_init
+
+     type(c_ptr) function fdmap_host_desc(dom) bind(C, name='fdmap_host_desc')
+       import :: c_ptr
+       type(c_ptr), value :: dom
+     end function fdmap_host_desc
+
+     subroutine fdmap_host_free(dom) bind(C, name='fdmap_host_free')
+       import :: c_ptr
+       type(c_ptr), value :: dom
+     end subroutine fdmap_host_free
+
+  end interface
+
+end module fdmap_gpu_mod

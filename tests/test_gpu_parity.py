@@ -77,3 +77,46 @@ def test_rk_orders(require_gpu, rk):
     o.run(1, h.nt)
     assert_fields_close(g.get_fields()[0], o.get_fields()[0])
     assert_fault_close(g, o, dt=h.dt)
+
+
+def test_graph_replay_matches_direct_steps(require_gpu, tmp_path):
+    """fdmap_gpu_run replays a captured CUDA graph per step with the step clock
+    on the device; it must reproduce per-step fdmap_gpu_time_step bit for bit
+    (stage times enter the rupture times and the source amplitude)."""
+    for text, base in ((problems.rupture_sw(nx=81, ny=41, h=0.5, nt=40), None),
+                       (problems.heterogeneous_ricker(tmp_path, n=61, h=0.05, nt=40), tmp_path)):
+        h = init_domain(text, base)
+        g1, g2 = GpuDomain(h), GpuDomain(h)
+        g1.run(1, h.nt)
+        for n in range(1, h.nt + 1):
+            g2.time_step_LS(h.t0 + (n - 1) * h.dt, h.dt, final_step=(n == h.nt))
+        F1, D1 = g1.get_fields(True, True)
+        F2, D2 = g2.get_fields(True, True)
+        assert np.array_equal(F1, F2) and np.array_equal(D1, D2)
+        if h.nifaces:
+            for f in ("V", "S", "D", "trup", "Psi"):
+                assert np.array_equal(g1.get_fault(0, f), g2.get_fault(0, f)), f
+
+
+def test_heterogeneous_point_source(require_gpu, tmp_path):
+    """Config c5 physics at reduced size: heterogeneous mode III medium, Ricker
+    point force, free top surface."""
+    text = problems.heterogeneous_ricker(tmp_path, n=101, h=0.05, nt=121)
+    h, g, o = _pair(text, tmp_path)
+    g.run(1, h.nt)
+    o.run(1, h.nt)
+    Fo = o.get_fields()[0]
+    assert np.abs(Fo[0]).max() > 0
+    assert_fields_close(g.get_fields()[0], Fo)
+
+
+def test_rough_fault_rate_state(require_gpu, tmp_path):
+    """Config c3 physics at reduced size: curvilinear blocks around a rough
+    fault, regularised rate-and-state friction with flash heating (RFL)."""
+    text = problems.rough_fault_rs(tmp_path, nx=121, ny=61, h=0.25, nt=161)
+    h, g, o = _pair(text, tmp_path)
+    g.run(1, h.nt)
+    o.run(1, h.nt)
+    assert_fields_close(g.get_fields()[0], o.get_fields()[0])
+    assert_fault_close(g, o, dt=h.dt, fields=("V", "S", "N", "D", "Psi"))
+    assert g.newton_failures() == 0 and o.newton_failures() == 0
