@@ -27,7 +27,6 @@ import json
 import os
 import re
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -45,7 +44,7 @@ METRIC = "FP64 node-updates/s"
 UNIT = "node-updates/s"
 
 # Algorithmic HBM bytes per node per RK stage of the fused stencil kernel
-# (compulsory reads and writes of one stage; see DESIGN.md "Roofline"):
+# (compulsory reads and writes of one stage):
 #   mode II: F 6 read + 6 write, DF 5 read + 6 write, metrics xq,xr,yq,yr,Ji 5 read
 #   mode III: F 3+3, DF 3+3, metrics 5;  heterogeneous adds rho,G (III) / 5 arrays (II)
 BYTES_PER_NODE_STAGE = {(2, False): 28 * 8, (2, True): 33 * 8, (3, False): 17 * 8, (3, True): 19 * 8}
@@ -65,57 +64,68 @@ def workload(name: str, tmpdir: Path):
 
 
 class ClockSampler:
-    """Samples nvidia-smi clocks and throttle reasons while running."""
+    """Samples SM clocks and clock-event (throttle) reasons through NVML every
+    few milliseconds while the timed region runs (read-only queries)."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_S = 0.005
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+               "hw_power_brake_slowdown": 0x80, "sw_power_cap": 0x4}
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.lines: list[str] = []
+        self.samples: list[tuple[int, int]] = []
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._t = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-        except FileNotFoundError:
-            self.proc = None
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._sample()
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        except Exception:
+            self._t = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _sample(self):
+        nv = self._nv
+        mhz = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+        try:
+            rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        except AttributeError:
+            rs = nv.nvmlDeviceGetCurrentClocksThrottleReasons(self._h)
+        self.samples.append((mhz, rs))
+
+    def _run(self):
+        while not self._stop.wait(self.PERIOD_S):
+            try:
+                self._sample()
+            except Exception:
+                return
 
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
+        if self._t is not None:
+            self._stop.set()
+            self._t.join(timeout=5)
             try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+                self._sample()
+            except Exception:
+                pass
 
     def summary(self) -> dict:
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            p = [x.strip() for x in ln.split(",")]
-            if len(p) < 9:
-                continue
-            try:
-                sm.append(float(p[1]))
-                mx.append(float(p[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, p[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [m for m, _ in self.samples]
+        reasons = set()
+        for _, rs in self.samples:
+            for name, bit in self.REASONS.items():
+                if rs & bit:
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvml"}
 
 
 def measured_peaks() -> dict:
@@ -355,8 +365,8 @@ def run_reference(args) -> None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="rupture", choices=["rupture", "pulse", "roughfault"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -316,11 +316,9 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
     F0p[l] = Sp.F0[kp + Sp.n * l];
   }
   double n0 = I.nhat[k], n1 = I.nhat[k + I.n];
-  double Zsm = Sm.M[km], Zsp = Sp.M[kp];
   double Fhm[6], Fhp[6];
   if (I.coupling == FDMAP_COUPLING_LOCKED) {
     if (MODE == 2) {
-      double Zpm = Sm.M[km + Sm.n], Zpp = Sp.M[kp + Sp.n];
       double gm = Sm.M[km + 2 * Sm.n], gp = Sp.M[kp + 2 * Sp.n];
       double rp[6], rm[6];
       rot2_xy2nt(Fp, n0, n1, rp);
@@ -370,7 +368,6 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
       // interfaces.f90:795 hands (F0m, F0p) to dummies declared (F0p, F0m)
       const double* dF0p = F0m;
       const double* dF0m = F0p;
-      double Zpm = Sm.M[km + Sm.n], Zpp = Sp.M[kp + Sp.n];
       double gm = Sm.M[km + 2 * Sm.n], gp = Sp.M[kp + 2 * Sp.n];
       double r0p[6];
       rot2_xy2nt(dF0p, n0, n1, r0p);
@@ -465,7 +462,7 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
 // One thread per interface node: the locked / frictional solve of this stage,
 // hat variables of both sides, and the fault register life cycle.
 template <int MODE>
-__global__ void __launch_bounds__(128) edge_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
+__global__ void __launch_bounds__(64) edge_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
   int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.seg_start[D.nseg]) return;
   int sg = 0;

@@ -103,6 +103,11 @@ struct fdmap_gpu {
   double* dev_fhat[MAX_BLOCKS][4] = {};
   int side_n[MAX_BLOCKS][4] = {};
   cudaStream_t own_stream = nullptr;
+  // boundary work (interface solves, closure strips) runs on a low-priority
+  // side stream beside the interior march of the same stage
+  bool overlap = false;
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // per-kernel event timing (fdmap_gpu_profile)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -174,6 +179,9 @@ struct fdmap_gpu {
     for (void* p : allocs) cudaFree(p);
     if (h_stage) cudaFreeHost(h_stage);
     if (own_stream) cudaStreamDestroy(own_stream);
+    if (side_stream) cudaStreamDestroy(side_stream);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     delete tmaps;
     for (auto& ge : step_graph)
       if (ge) cudaGraphExecDestroy(ge);
@@ -196,7 +204,7 @@ struct ProfScope {
 
 int launch_edges(fdmap_gpu* h, const StageArgs& a) {
   if (h->edge_threads == 0) return FDMAP_OK;
-  int tpb = 128;
+  int tpb = 64;
   int nb = (h->edge_threads + tpb - 1) / tpb;
   ProfScope ps(h, 2);
   if (h->mode == 2) edge_kernel<2><<<nb, tpb, 0, h->stream>>>(h->hdom, a);
@@ -346,22 +354,7 @@ void launch_boundary_mode(fdmap_gpu* h, const StageArgs& a) {
 // independent items); otherwise interface solves, then closure strips (which
 // read the interface hat variables) -- then the interior.  All of them read
 // F[in] and write disjoint nodes.
-int launch_stage(fdmap_gpu* h, const StageArgs& a) {
-  if (h->fused) {
-    ProfScope pc(h, 1);
-    if (h->mode == 2) launch_boundary_mode<2>(h, a);
-    else launch_boundary_mode<3>(h, a);
-    h->launches++;
-    CUDA_TRY(cudaGetLastError());
-  } else {
-    int rc = launch_edges(h, a);
-    if (rc) return rc;
-    ProfScope pc(h, 1);
-    if (h->mode == 2) launch_closure_mode<2>(h, a);
-    else launch_closure_mode<3>(h, a);
-    h->launches++;
-    CUDA_TRY(cudaGetLastError());
-  }
+int launch_interior(fdmap_gpu* h, const StageArgs& a) {
   ProfScope ps(h, 0);
   if (h->use_march) {
     int rc = march_dispatch(h, &a);
@@ -371,6 +364,48 @@ int launch_stage(fdmap_gpu* h, const StageArgs& a) {
   h->launches++;
   CUDA_TRY(cudaGetLastError());
   return FDMAP_OK;
+}
+
+int launch_boundary(fdmap_gpu* h, const StageArgs& a) {
+  int rc = launch_edges(h, a);
+  if (rc) return rc;
+  ProfScope pc(h, 1);
+  if (h->mode == 2) launch_closure_mode<2>(h, a);
+  else launch_closure_mode<3>(h, a);
+  h->launches++;
+  CUDA_TRY(cudaGetLastError());
+  return FDMAP_OK;
+}
+
+int launch_stage(fdmap_gpu* h, const StageArgs& a) {
+  if (h->overlap && !h->profiling && !h->fused) {
+    // fork: the interior march is issued first on the (high-priority) main
+    // stream so its persistent CTAs take the SMs; edge + closure follow on
+    // the side stream and fill the registers the march leaves free; join.
+    CUDA_TRY(cudaEventRecord(h->ev_fork, h->stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+    int rc = launch_interior(h, a);
+    if (rc) return rc;
+    cudaStream_t main_stream = h->stream;
+    h->stream = h->side_stream;
+    rc = launch_boundary(h, a);
+    h->stream = main_stream;
+    if (rc) return rc;
+    CUDA_TRY(cudaEventRecord(h->ev_join, h->side_stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+    return FDMAP_OK;
+  }
+  if (h->fused) {
+    ProfScope pc(h, 1);
+    if (h->mode == 2) launch_boundary_mode<2>(h, a);
+    else launch_boundary_mode<3>(h, a);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+  } else {
+    int rc = launch_boundary(h, a);
+    if (rc) return rc;
+  }
+  return launch_interior(h, a);
 }
 
 int validate(const fdmap_desc* d) {
@@ -614,6 +649,10 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     // one merged boundary launch is opt-in: the two separate launches measure faster
     const char* ef = getenv("FDMAP_FUSED");
     h->fused = !junction && (ef && std::string(ef) == "1");
+    // concurrent boundary work needs the interior march (it leaves registers
+    // free); FDMAP_OVERLAP=0 serialises the stage
+    const char* eo = getenv("FDMAP_OVERLAP");
+    h->overlap = h->use_march && !h->fused && !(eo && std::string(eo) == "0");
   }
   if ((rc = h->alloc(&h->d_status, 4))) return rc;
   if ((rc = h->alloc(&h->d_time, 1))) return rc;
@@ -677,7 +716,7 @@ int build_step_graphs(fdmap_gpu* h, double dt) {
     e = cudaStreamEndCapture(h->stream, &g);
     if (rc == FDMAP_OK && e != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
     if (rc == FDMAP_OK) {
-      e = cudaGraphInstantiate(&h->step_graph[c], g, 0);
+      e = cudaGraphInstantiate(&h->step_graph[c], g, cudaGraphInstantiateFlagUseNodePriority);
       if (e != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
     }
     if (g) cudaGraphDestroy(g);
@@ -705,8 +744,12 @@ int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu*
   fdmap_gpu* h = new (std::nothrow) fdmap_gpu();
   if (!h) return set_err(FDMAP_ERR_NOMEM, "out of host memory");
   h->device = device;
-  if (cudaSetDevice(device) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  int prio_low = 0, prio_high = 0;
+  if (cudaSetDevice(device) != cudaSuccess || cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&h->own_stream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&h->side_stream, cudaStreamNonBlocking, prio_low) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
     delete h;
     return set_err(FDMAP_ERR_CUDA, "cannot initialise device");
   }

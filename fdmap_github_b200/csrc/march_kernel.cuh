@@ -175,14 +175,20 @@ __device__ __forceinline__ UnitPos unit_pos(const DevDomain& D, long long u) {
   return p;
 }
 
+// Register budget of the march kernel: 96 per thread (48K of the SM's 64K for
+// the 512-thread CTA) leaves room for one boundary CTA beside it, so the
+// edge and closure kernels of the same stage run concurrently with the
+// interior march.  The SBP6 mode II variant needs more to avoid spills.
+template <int MODE, int PI_>
+constexpr int march_regs() { return (MODE == 2 && PI_ == 3) ? 128 : 96; }
+
 template <int MODE, int PI_, bool HET>
-__global__ void __launch_bounds__(MTHREADS, 1)
+__global__ void __maxnreg__((march_regs<MODE, PI_>()))
     march_kernel(const DevDomain* __restrict__ Dp, StageArgs a, MarchPlan plan, const __grid_constant__ TmapSet tm) {
   using L = MarchLayout<MODE, PI_, HET>;
   using RD = RDef<MODE>;
   constexpr int NR = RD::NR;
   constexpr int NF = MODE == 2 ? 6 : 3;
-  constexpr int H = PI_;
   constexpr int HP = L::HP;
   constexpr int WH = L::WH;
   extern __shared__ unsigned char smem_dyn[];
@@ -214,7 +220,6 @@ __global__ void __launch_bounds__(MTHREADS, 1)
     const int i0 = p0.sx * MW;
     const int nx = B.nx, ny = B.ny;
     const long long pitch = B.pitch, plane = B.plane;
-    const double* __restrict__ Fin = B.F[a.in];
     const int ngroups = (jr1 - jr0 + MR - 1) / MR;
     // neighbour groups needed: k = gmin .. gmax (group k holds rows jr0 + k*MR ..)
     const int gmin = jr0 >= MR ? -1 : 0;
