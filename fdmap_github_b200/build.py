@@ -38,17 +38,33 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build_library(force: bool = False, verbose: bool = False) -> Path:
-    """Compile libfdmap_gpu.so for sm_100a (cross-compiles without a GPU)."""
-    if not force and not _stale(LIB, _deps()):
-        return LIB
+def _compile(src: Path, obj: Path, verbose: bool) -> None:
     cmd = [
         NVCC, "-std=c++17", "-O3", *ARCH, "-lineinfo",
         f"-I{INCLUDE}", f"-I{CSRC}",
-        "-Xcompiler", "-fPIC,-O3", "-shared",
-        *[str(s) for s in _sources()],
-        "-o", str(LIB) + ".tmp",
+        "-Xcompiler", "-fPIC,-O3", "-c", str(src), "-o", str(obj),
     ]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+
+
+def build_library(force: bool = False, verbose: bool = False) -> Path:
+    """Compile libfdmap_gpu.so for sm_100a (cross-compiles without a GPU).
+
+    Each source is compiled to its own object in parallel (objects under
+    csrc/_build), then nvcc links the shared object."""
+    if not force and not _stale(LIB, _deps()):
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    objdir = CSRC / "_build"
+    objdir.mkdir(exist_ok=True)
+    srcs = _sources()
+    objs = [objdir / (s.name + ".o") for s in srcs]
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        list(ex.map(lambda so: _compile(so[0], so[1], verbose), zip(srcs, objs)))
+    cmd = [NVCC, *ARCH, "-shared", *[str(o) for o in objs], "-o", str(LIB) + ".tmp"]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

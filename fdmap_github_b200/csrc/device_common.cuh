@@ -14,6 +14,8 @@
 // its own rate).
 #pragma once
 
+#include <cuda.h>
+
 #include <cstdint>
 
 #include "fdmap_desc.h"
@@ -80,6 +82,12 @@ struct DevIface {
   DevFriction fr;
 };
 
+// Device layout of every field array: PADL doubles of front padding (so that
+// halo boxes may start before column 0) and PADTAIL doubles of slack after
+// the last row of each plane.
+constexpr int PADL = 32;
+constexpr int PADTAIL = 192;
+
 struct DevDomain {
   int mode, nF, nblocks, nifaces, het;
   int nbst, nbnd, pI;
@@ -98,6 +106,29 @@ struct DevDomain {
   fdmap_source src;
   unsigned long long* status;  // [0] Newton failures, [1] nonfinite flags
 };
+
+// TMA descriptors of every block, passed by value as a __grid_constant__ parameter
+// (single domain) or read from device memory (batched instances)
+struct TmapSet {
+  CUtensorMap F[MAX_BLOCKS][2];    // rate fields, box {WH, MR, NR}
+  CUtensorMap F6[MAX_BLOCKS][2];   // szz plane (mode II), box {MW, MR, 1}
+  CUtensorMap DF[MAX_BLOCKS];      // rates, box {MW, MR, NR}
+  CUtensorMap MH[MAX_BLOCKS];      // yr, xr, box {WH, MR, 2}
+  CUtensorMap MC[MAX_BLOCKS];      // yq, xq, Ji, box {MW, MR, 3}
+  CUtensorMap HT[MAX_BLOCKS];      // heterogeneous material, box {MW, MR, NH}
+};
+
+// Batched launches: CTAs [begin[k], begin[k+1]) serve instance k.  Returns
+// the instance of CTA `cta` (binary search, uniform across the CTA).
+__device__ __forceinline__ int batch_instance(const int* __restrict__ begin, int ninst, int cta) {
+  int lo = 0, hi = ninst - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (begin[mid] <= cta) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
 
 // Step clock kept on the device so that a captured CUDA graph can be replayed
 // step after step: step n starts at t0 = t_start + (n-1)*dt (main.f90:176).

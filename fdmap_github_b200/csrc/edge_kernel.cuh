@@ -470,4 +470,17 @@ __global__ void __launch_bounds__(64) edge_kernel(const __grid_constant__ DevDom
   d_iface_node<MODE>(D, D.ifc[D.seg_a[sg]], tid - D.seg_start[sg], a);
 }
 
+// Interface nodes of a batch of independent instances in one launch.
+template <int MODE>
+__global__ void __launch_bounds__(128)
+    edge_kernel_batch(const DevDomain* __restrict__ doms, const int* __restrict__ cta_begin, int ninst, StageArgs a) {
+  const int k = batch_instance(cta_begin, ninst, blockIdx.x);
+  const DevDomain& D = doms[k];
+  const int tid = (blockIdx.x - cta_begin[k]) * blockDim.x + threadIdx.x;
+  if (tid >= D.seg_start[D.nseg]) return;
+  int sg = 0;
+  while (tid >= D.seg_start[sg + 1]) ++sg;
+  d_iface_node<MODE>(D, D.ifc[D.seg_a[sg]], tid - D.seg_start[sg], a);
+}
+
 }  // namespace fdmap

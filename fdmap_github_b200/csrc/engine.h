@@ -1,0 +1,182 @@
+// Internal header of the engine: the handle behind include/fdmap_gpu.h and
+// the launchers that other translation units of the library (ensemble,
+// adjoint) call.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "device_common.cuh"
+#include "fdmap_gpu.h"
+#include "sbp_tables.h"
+
+namespace fdmap {
+
+int set_err(int code, const std::string& msg);
+extern thread_local std::string g_err;
+
+#define CUDA_TRY(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return ::fdmap::set_err(FDMAP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+struct BlockGeom {
+  int mgx, mgy, nx, ny, pitch;
+  long long plane;
+};
+
+__global__ void advance_step(TimeState* ts);
+__global__ void set_step_clock(TimeState* ts, double t_start, double dt, long long n);
+
+}  // namespace fdmap
+
+using namespace fdmap;  // internal header: the handle below is written in the engine's namespace terms
+
+struct fdmap_gpu {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  DevDomain hdom{};
+  DevDomain* ddom = nullptr;
+  std::vector<void*> allocs;
+  long long bytes = 0;
+  int cur = 0;
+  int mode = 2, nF = 6, pI = 2, het = 0;
+  RkTable rk{};
+  int nx_g = 0, ny_g = 0;
+  std::vector<BlockGeom> geom;
+  std::vector<int> iface_n;
+  std::vector<int> iface_fric;
+  int total_tiles = 0, edge_threads = 0;
+  long long closure_threads = 0;
+  long long march_units = 0;
+  int march_grid = 0;
+  int use_march = 1;
+  int fused = 0;  // boundary kernel handles interface solves and closure strips in one launch
+  // CUDA graphs of one full step, one per starting F buffer, replayed by fdmap_gpu_run
+  TimeState* d_time = nullptr;
+  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
+  double graph_dt = 0.0;
+  long long graph_launches = 0;
+  bool use_graphs = true;
+  double* met_base[MAX_BLOCKS] = {};
+  double* het_base[MAX_BLOCKS] = {};
+  TmapSet* tmaps = nullptr;  // host copy, passed by value to the march kernel
+  double* h_stage = nullptr;  // pinned staging buffer for layout conversion
+  size_t stage_doubles = 0;
+  unsigned long long* d_status = nullptr;
+  long long launches = 0;
+  double* dev_fhat[MAX_BLOCKS][4] = {};
+  int side_n[MAX_BLOCKS][4] = {};
+  cudaStream_t own_stream = nullptr;
+  // boundary work (interface solves, closure strips) runs on a low-priority
+  // side stream beside the interior march of the same stage
+  bool overlap = false;
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // per-kernel event timing (fdmap_gpu_profile)
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;  // kind, (start, stop)
+  double prof_ms[3] = {0, 0, 0};
+  long long prof_n[3] = {0, 0, 0};
+
+  template <typename T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    size_t bytes_ = count * sizeof(T);
+    if (bytes_ == 0) bytes_ = 16;
+    cudaError_t e = cudaMalloc(&q, bytes_);
+    if (e != cudaSuccess) return set_err(FDMAP_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    allocs.push_back(q);
+    bytes += (long long)bytes_;
+    *p = (T*)q;
+    return FDMAP_OK;
+  }
+  // field arrays: PADL doubles of front padding so halo bulk copies may start
+  // before column 0; every plane carries PADTAIL doubles of slack after its last row
+  int alloc_planes(double** base, int nplanes, long long plane) {
+    double* raw = nullptr;
+    int rc = alloc(&raw, (size_t)PADL + (size_t)nplanes * plane);
+    if (rc) return rc;
+    CUDA_TRY(cudaMemset(raw, 0, ((size_t)PADL + (size_t)nplanes * plane) * sizeof(double)));
+    *base = raw + PADL;
+    return FDMAP_OK;
+  }
+  int upload(double** dst, const double* src, size_t count) {
+    int rc = alloc(dst, count);
+    if (rc) return rc;
+    if (src) CUDA_TRY(cudaMemcpy(*dst, src, count * sizeof(double), cudaMemcpyHostToDevice));
+    return FDMAP_OK;
+  }
+  // global (nx_g, ny_g) plane -> padded block plane on the device
+  int upload_plane(double* dst, const double* src, const BlockGeom& g) {
+    std::vector<double> tmp((size_t)g.plane, 0.0);
+    for (int j = 0; j < g.ny; ++j)
+      for (int i = 0; i < g.nx; ++i)
+        tmp[(size_t)j * g.pitch + i] = src[(size_t)(g.mgx - 1 + i) + (size_t)nx_g * (size_t)(g.mgy - 1 + j)];
+    CUDA_TRY(cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return FDMAP_OK;
+  }
+  cudaEvent_t take_event() {
+    cudaEvent_t e;
+    if (!ev_pool.empty()) { e = ev_pool.back(); ev_pool.pop_back(); }
+    else cudaEventCreate(&e);
+    return e;
+  }
+  // folds finished event pairs into the totals (blocking on the last one)
+  void drain_events() {
+    for (auto& p : ev_pending) {
+      cudaEventSynchronize(p.second.second);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+      prof_ms[p.first] += ms;
+      prof_n[p.first] += 1;
+      ev_pool.push_back(p.second.first);
+      ev_pool.push_back(p.second.second);
+    }
+    ev_pending.clear();
+  }
+  ~fdmap_gpu() {
+    if (device >= 0) cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+    for (auto e : ev_pool) cudaEventDestroy(e);
+    for (void* p : allocs) cudaFree(p);
+    if (h_stage) cudaFreeHost(h_stage);
+    if (own_stream) cudaStreamDestroy(own_stream);
+    if (side_stream) cudaStreamDestroy(side_stream);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    delete tmaps;
+    for (auto& ge : step_graph)
+      if (ge) cudaGraphExecDestroy(ge);
+  }
+};
+
+namespace fdmap {
+
+// Launchers over a batch of independent domains (one DevDomain per instance,
+// in device memory).  `proto` supplies the compile-time variant (mode, SBP
+// order, heterogeneity); every instance must share it.
+struct BatchPlan {
+  const DevDomain* doms;          // [ninst] device copies of each instance's domain
+  const TmapSet* tmaps;           // [ninst] device copies of each instance's tensor maps
+  const long long* unit_begin;    // [ninst+1] march units, prefix over instances
+  const int* closure_cta_begin;   // [ninst+1] closure CTAs, prefix over instances
+  const int* edge_cta_begin;      // [ninst+1] interface CTAs, prefix over instances
+  int ninst;
+  long long units;
+  int march_grid;
+  int closure_ctas, closure_tpb;
+  int edge_ctas, edge_tpb;
+};
+int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+int batch_closure(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+int batch_edges(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+
+}  // namespace fdmap

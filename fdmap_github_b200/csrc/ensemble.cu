@@ -1,0 +1,429 @@
+// Batched ensemble: many independent FDMAP domains (instances of uneven
+// grid sizes and their own prestress) advanced together.  Every stage is one
+// launch per kernel kind for ALL instances:
+//   - the persistent interior march walks the concatenated row-group units of
+//     every block of every instance (one CTA per SM, balanced partition);
+//   - one interface launch covers every fault node of every instance;
+//   - one closure launch covers every SBP boundary strip of every instance.
+// Per-node arithmetic is the single-domain kernels' own, so every instance
+// reproduces its plain single-domain run bit for bit.  Each step is captured
+// once as a CUDA graph and replayed.  Launch shapes (thread-block sizes of the
+// boundary kernels, boundary/interior overlap) are picked by a timing-based
+// autotuner (fdmap_gpu_ensemble_tune).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+#include "fdmap_gpu.h"
+
+using namespace fdmap;
+
+struct fdmap_ensemble {
+  int device = 0;
+  int ninst = 0;
+  std::vector<fdmap_gpu*> inst;
+  fdmap_gpu* proto = nullptr;  // instance 0: compile-time variant of all
+  cudaStream_t stream = nullptr, side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  DevDomain* d_doms = nullptr;
+  TmapSet* d_tmaps = nullptr;
+  long long* d_unit_begin = nullptr;
+  int* d_closure_begin = nullptr;
+  int* d_edge_begin = nullptr;
+  TimeState* d_time = nullptr;
+  std::vector<long long> closure_threads, edge_threads;
+  BatchPlan plan{};
+  int overlap = 1;
+  int cur = 0;
+  RkTable rk{};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  double graph_dt = 0.0;
+  long long graph_launches = 0;
+  long long launches = 0;
+
+  void free_graphs() {
+    for (auto& g : graph)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  }
+  ~fdmap_ensemble() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    free_graphs();
+    for (fdmap_gpu* h : inst) fdmap_gpu_destroy(h);
+    cudaFree(d_doms);
+    cudaFree(d_tmaps);
+    cudaFree(d_unit_begin);
+    cudaFree(d_closure_begin);
+    cudaFree(d_edge_begin);
+    cudaFree(d_time);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// CTA prefix over instances for a boundary kernel of `tpb` threads per CTA
+int cta_prefix(const std::vector<long long>& threads, int tpb, std::vector<int>& begin) {
+  begin.assign(threads.size() + 1, 0);
+  long long c = 0;
+  for (size_t k = 0; k < threads.size(); ++k) {
+    begin[k] = (int)c;
+    c += (threads[k] + tpb - 1) / tpb;
+  }
+  begin[threads.size()] = (int)c;
+  return (int)c;
+}
+
+int apply_shapes(fdmap_ensemble* e, int closure_tpb, int edge_tpb, int overlap) {
+  if (closure_tpb != 64 && closure_tpb != 128 && closure_tpb != 256)
+    return set_err(FDMAP_ERR_INVALID_ARG, "closure block size must be 64, 128 or 256");
+  if (edge_tpb != 32 && edge_tpb != 64 && edge_tpb != 128)
+    return set_err(FDMAP_ERR_INVALID_ARG, "interface block size must be 32, 64 or 128");
+  std::vector<int> cb, eb;
+  e->plan.closure_ctas = cta_prefix(e->closure_threads, closure_tpb, cb);
+  e->plan.edge_ctas = cta_prefix(e->edge_threads, edge_tpb, eb);
+  e->plan.closure_tpb = closure_tpb;
+  e->plan.edge_tpb = edge_tpb;
+  CUDA_TRY(cudaMemcpy(e->d_closure_begin, cb.data(), cb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(e->d_edge_begin, eb.data(), eb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  e->overlap = overlap != 0;
+  e->free_graphs();
+  return FDMAP_OK;
+}
+
+int ens_stage(fdmap_ensemble* e, const StageArgs& a) {
+  const BatchPlan& p = e->plan;
+  int rc;
+  if (e->overlap) {
+    CUDA_TRY(cudaEventRecord(e->ev_fork, e->stream));
+    CUDA_TRY(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
+    if ((rc = batch_march(e->proto, a, p, e->stream))) return rc;
+    if ((rc = batch_edges(e->proto, a, p, e->side))) return rc;
+    if ((rc = batch_closure(e->proto, a, p, e->side))) return rc;
+    CUDA_TRY(cudaEventRecord(e->ev_join, e->side));
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_join, 0));
+  } else {
+    if ((rc = batch_edges(e->proto, a, p, e->stream))) return rc;
+    if ((rc = batch_closure(e->proto, a, p, e->stream))) return rc;
+    if ((rc = batch_march(e->proto, a, p, e->stream))) return rc;
+  }
+  e->launches += (p.edge_ctas ? 1 : 0) + (p.closure_ctas ? 1 : 0) + 1;
+  return FDMAP_OK;
+}
+
+// all stages of one step of every instance (final step: stage 1 only)
+int ens_issue_step(fdmap_ensemble* e, int cur, double t0, double dt, bool final_step, const TimeState* ts) {
+  for (int s = 0; s < e->rk.nstage; ++s) {
+    StageArgs a{};
+    a.A = e->rk.A[s];
+    a.Bdt = e->rk.B[s] * dt;
+    a.t = t0 + e->rk.C[s] * dt;
+    a.C = e->rk.C[s];
+    a.ts = ts;
+    a.in = cur;
+    a.out = 1 - cur;
+    a.scale = 1;
+    a.update = final_step ? 0 : 1;
+    int rc = ens_stage(e, a);
+    if (rc) return rc;
+    if (final_step) return FDMAP_OK;
+    cur = 1 - cur;
+  }
+  return FDMAP_OK;
+}
+
+int ens_build_graphs(fdmap_ensemble* e, double dt) {
+  e->free_graphs();
+  long long before = e->launches;
+  int rc = FDMAP_OK;
+  for (int c = 0; c < 2 && rc == FDMAP_OK; ++c) {
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+    if (ce != cudaSuccess) return set_err(FDMAP_ERR_CUDA, std::string("capture: ") + cudaGetErrorString(ce));
+    long long l0 = e->launches;
+    rc = ens_issue_step(e, c, 0.0, dt, false, e->d_time);
+    if (rc == FDMAP_OK) advance_step<<<1, 1, 0, e->stream>>>(e->d_time);
+    e->graph_launches = e->launches - l0 + 1;
+    ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc == FDMAP_OK && ce != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ce));
+    if (rc == FDMAP_OK) {
+      ce = cudaGraphInstantiate(&e->graph[c], g, cudaGraphInstantiateFlagUseNodePriority);
+      if (ce != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(ce));
+    }
+    if (g) cudaGraphDestroy(g);
+  }
+  e->launches = before;
+  if (rc == FDMAP_OK) e->graph_dt = dt;
+  return rc;
+}
+
+int ens_check_cur(fdmap_ensemble* e) {
+  for (fdmap_gpu* h : e->inst)
+    if (h->cur != e->cur) return set_err(FDMAP_ERR_INVALID_ARG, "an instance was stepped outside its ensemble");
+  return FDMAP_OK;
+}
+
+void ens_sync_cur(fdmap_ensemble* e) {
+  for (fdmap_gpu* h : e->inst) h->cur = e->cur;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdmap_gpu_ensemble_create(const fdmap_desc* const* descs, int ninst, int device, int init_edges,
+                              fdmap_ensemble** out) {
+  if (!out) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble pointer");
+  *out = nullptr;
+  if (!descs || ninst < 1) return set_err(FDMAP_ERR_INVALID_ARG, "an ensemble needs at least one instance");
+  fdmap_ensemble* e = new (std::nothrow) fdmap_ensemble();
+  if (!e) return set_err(FDMAP_ERR_NOMEM, "out of host memory");
+  e->device = device;
+  e->ninst = ninst;
+  auto fail = [&](int rc) {
+    std::string keep = g_err;
+    delete e;
+    g_err = keep;
+    return rc;
+  };
+  int rc;
+  for (int k = 0; k < ninst; ++k) {
+    fdmap_gpu* h = nullptr;
+    if ((rc = fdmap_gpu_create(descs[k], device, init_edges, &h))) return fail(rc);
+    e->inst.push_back(h);
+  }
+  fdmap_gpu* p = e->inst[0];
+  e->proto = p;
+  for (fdmap_gpu* h : e->inst) {
+    if (h->mode != p->mode || h->pI != p->pI || h->het != p->het || h->rk.nstage != p->rk.nstage)
+      return fail(set_err(FDMAP_ERR_INVALID_ARG, "ensemble instances must share mode, FD method, RK order and material kind"));
+    for (int s = 0; s < h->rk.nstage; ++s)
+      if (h->rk.A[s] != p->rk.A[s] || h->rk.B[s] != p->rk.B[s] || h->rk.C[s] != p->rk.C[s])
+        return fail(set_err(FDMAP_ERR_INVALID_ARG, "ensemble instances must share the RK table"));
+    if (!h->use_march)
+      return fail(set_err(FDMAP_ERR_UNSUPPORTED, "ensembles need the marching interior kernel (homogeneous mode II or any mode III)"));
+    if (h->cur != 0) return fail(set_err(FDMAP_ERR_INVALID_ARG, "instance buffer state"));
+  }
+  e->rk = p->rk;
+  if ((rc = [&]() -> int {
+        CUDA_TRY(cudaSetDevice(device));
+        int lo = 0, hi = 0;
+        CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        CUDA_TRY(cudaStreamCreateWithPriority(&e->stream, cudaStreamNonBlocking, hi));
+        CUDA_TRY(cudaStreamCreateWithPriority(&e->side, cudaStreamNonBlocking, lo));
+        CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
+        // per-instance device descriptors and tensor maps, unit prefix
+        std::vector<DevDomain> doms(ninst);
+        std::vector<TmapSet> maps(ninst);
+        std::vector<long long> ub(ninst + 1, 0);
+        long long units = 0;
+        int grid = 0;
+        for (int k = 0; k < ninst; ++k) {
+          fdmap_gpu* h = e->inst[k];
+          doms[k] = h->hdom;
+          maps[k] = *h->tmaps;
+          ub[k] = units;
+          units += h->march_units;
+          grid = std::max(grid, h->march_grid);
+          e->closure_threads.push_back(h->closure_threads);
+          e->edge_threads.push_back(h->edge_threads);
+        }
+        ub[ninst] = units;
+        CUDA_TRY(cudaMalloc(&e->d_doms, sizeof(DevDomain) * ninst));
+        CUDA_TRY(cudaMalloc(&e->d_tmaps, sizeof(TmapSet) * ninst));
+        CUDA_TRY(cudaMalloc(&e->d_unit_begin, sizeof(long long) * (ninst + 1)));
+        CUDA_TRY(cudaMalloc(&e->d_closure_begin, sizeof(int) * (ninst + 1)));
+        CUDA_TRY(cudaMalloc(&e->d_edge_begin, sizeof(int) * (ninst + 1)));
+        CUDA_TRY(cudaMalloc(&e->d_time, sizeof(TimeState)));
+        CUDA_TRY(cudaMemcpy(e->d_doms, doms.data(), sizeof(DevDomain) * ninst, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(e->d_tmaps, maps.data(), sizeof(TmapSet) * ninst, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(e->d_unit_begin, ub.data(), sizeof(long long) * (ninst + 1), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemset(e->d_time, 0, sizeof(TimeState)));
+        e->plan.doms = e->d_doms;
+        e->plan.tmaps = e->d_tmaps;
+        e->plan.unit_begin = e->d_unit_begin;
+        e->plan.closure_cta_begin = e->d_closure_begin;
+        e->plan.edge_cta_begin = e->d_edge_begin;
+        e->plan.ninst = ninst;
+        e->plan.units = units;
+        // one CTA per SM (the ring fills shared memory), never more CTAs than units
+        e->plan.march_grid = (int)std::min<long long>(grid, units);
+        // instances read and write through the ensemble stream
+        for (fdmap_gpu* h : e->inst) {
+          CUDA_TRY(cudaStreamSynchronize(h->stream));
+          h->stream = e->stream;
+        }
+        return FDMAP_OK;
+      }()))
+    return fail(rc);
+  if ((rc = apply_shapes(e, 128, 64, 1))) return fail(rc);
+  *out = e;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_instance(fdmap_ensemble* e, int k, fdmap_gpu** h) {
+  if (!e || !h) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  if (k < 0 || k >= e->ninst) return set_err(FDMAP_ERR_INVALID_ARG, "instance index out of range");
+  *h = e->inst[k];
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_size(fdmap_ensemble* e) { return e ? e->ninst : -1; }
+
+int fdmap_gpu_ensemble_time_step(fdmap_ensemble* e, double t0, double dt, int final_step) {
+  if (!e) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble");
+  CUDA_TRY(cudaSetDevice(e->device));
+  int rc = ens_check_cur(e);
+  if (rc) return rc;
+  if ((rc = ens_issue_step(e, e->cur, t0, dt, final_step != 0, nullptr))) return rc;
+  if (!final_step && (e->rk.nstage & 1)) e->cur = 1 - e->cur;
+  ens_sync_cur(e);
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_run(fdmap_ensemble* e, double t_start, double dt, int n_first, int n_last, int nt) {
+  if (!e) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble");
+  CUDA_TRY(cudaSetDevice(e->device));
+  int rc = ens_check_cur(e);
+  if (rc) return rc;
+  e->launches = 0;
+  const int n_graph_last = std::min(n_last, nt - 1);  // the final step (n == nt) is issued directly
+  if (n_graph_last >= n_first) {
+    if (e->graph_dt != dt || !e->graph[0]) {
+      if ((rc = ens_build_graphs(e, dt))) return rc;
+    }
+    set_step_clock<<<1, 1, 0, e->stream>>>(e->d_time, t_start, dt, (long long)n_first);
+    e->launches++;
+    CUDA_TRY(cudaGetLastError());
+    for (int n = n_first; n <= n_graph_last; ++n) {
+      CUDA_TRY(cudaGraphLaunch(e->graph[e->cur], e->stream));
+      e->launches += e->graph_launches;
+      if (e->rk.nstage & 1) e->cur = 1 - e->cur;
+    }
+    n_first = n_graph_last + 1;
+  }
+  ens_sync_cur(e);
+  for (int n = n_first; n <= n_last; ++n)
+    if ((rc = fdmap_gpu_ensemble_time_step(e, t_start + (double)(n - 1) * dt, dt, n == nt))) return rc;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_synchronize(fdmap_ensemble* e) {
+  if (!e) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_set_shape(fdmap_ensemble* e, const int* shape) {
+  if (!e || !shape) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return apply_shapes(e, shape[0], shape[1], shape[2]);
+}
+
+int fdmap_gpu_ensemble_get_shape(fdmap_ensemble* e, int* shape) {
+  if (!e || !shape) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  shape[0] = e->plan.closure_tpb;
+  shape[1] = e->plan.edge_tpb;
+  shape[2] = e->overlap;
+  return FDMAP_OK;
+}
+
+// Autotuner: times `steps` graph-replayed steps (best of two repetitions) for every launch shape
+// (closure block size x interface block size x boundary/interior overlap),
+// keeps the fastest and leaves it applied.  The instances' state is saved
+// before and restored after, so tuning does not advance the ensemble.
+int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_shape, double* best_ms) {
+  if (!e) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble");
+  if (steps < 1) return set_err(FDMAP_ERR_INVALID_ARG, "steps must be positive");
+  CUDA_TRY(cudaSetDevice(e->device));
+  int rc = ens_check_cur(e);
+  if (rc) return rc;
+  // snapshot of every instance's state (both F buffers, DF, fault state) on the device
+  struct Saved { void* dst; const void* src; size_t bytes; };
+  std::vector<Saved> saved;
+  std::vector<void*> bufs;
+  auto cleanup = [&]() { for (void* b : bufs) cudaFree(b); };
+  auto snap = [&](const void* src, size_t bytes) -> int {
+    void* d = nullptr;
+    if (cudaMalloc(&d, bytes) != cudaSuccess) return set_err(FDMAP_ERR_NOMEM, "no device memory for the tuning snapshot");
+    bufs.push_back(d);
+    saved.push_back({d, src, bytes});
+    CUDA_TRY(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, e->stream));
+    return FDMAP_OK;
+  };
+  for (fdmap_gpu* h : e->inst) {
+    for (int b = 0; b < h->hdom.nblocks && rc == FDMAP_OK; ++b) {
+      const DevBlock& B = h->hdom.blk[b];
+      const size_t bytes = (size_t)B.plane * h->nF * sizeof(double);
+      for (int q = 0; q < 2 && rc == FDMAP_OK; ++q) rc = snap(B.F[q], bytes);
+      if (rc == FDMAP_OK) rc = snap(B.DF, bytes);
+    }
+    for (int k = 0; k < h->hdom.nifaces && rc == FDMAP_OK; ++k) {
+      const DevIface& I = h->hdom.ifc[k];
+      if (I.fr.st) rc = snap(I.fr.st, (size_t)FDMAP_FAULT_NFIELDS * I.n * sizeof(double));
+    }
+    if (rc) break;
+  }
+  if (rc) { cleanup(); return rc; }
+  const int cur0 = e->cur;
+  const int ctpb[3] = {64, 128, 256}, etpb[3] = {32, 64, 128};
+  int best[3] = {e->plan.closure_tpb, e->plan.edge_tpb, e->overlap};
+  float best_t = -1.f;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  for (int ov = 0; ov < 2 && rc == FDMAP_OK; ++ov)
+    for (int ci = 0; ci < 3 && rc == FDMAP_OK; ++ci)
+      for (int ei = 0; ei < 3 && rc == FDMAP_OK; ++ei) {
+        if ((rc = apply_shapes(e, ctpb[ci], etpb[ei], ov))) break;
+        // warm-up step (also builds the graphs), then two timed repetitions; the faster counts
+        if ((rc = fdmap_gpu_ensemble_run(e, 0.0, dt, 1, 1, 1 << 30))) break;
+        float ms = -1.f;
+        for (int rep = 0; rep < 2 && rc == FDMAP_OK; ++rep) {
+          cudaEventRecord(t0, e->stream);
+          if ((rc = fdmap_gpu_ensemble_run(e, 0.0, dt, 2, 1 + steps, 1 << 30))) break;
+          cudaEventRecord(t1, e->stream);
+          if (cudaEventSynchronize(t1) != cudaSuccess) { rc = set_err(FDMAP_ERR_CUDA, "tuning run failed"); break; }
+          float m = 0.f;
+          cudaEventElapsedTime(&m, t0, t1);
+          if (ms < 0.f || m < ms) ms = m;
+        }
+        if (rc) break;
+        if (best_t < 0.f || ms < best_t) {
+          best_t = ms;
+          best[0] = ctpb[ci]; best[1] = etpb[ei]; best[2] = ov;
+        }
+      }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  // restore the state and the buffer parity
+  for (const Saved& s : saved)
+    if (cudaMemcpyAsync(const_cast<void*>(s.src), s.dst, s.bytes, cudaMemcpyDeviceToDevice, e->stream) != cudaSuccess && !rc)
+      rc = set_err(FDMAP_ERR_CUDA, "restoring the tuning snapshot failed");
+  if (cudaStreamSynchronize(e->stream) != cudaSuccess && !rc) rc = set_err(FDMAP_ERR_CUDA, "tuning restore failed");
+  cleanup();
+  e->cur = cur0;
+  ens_sync_cur(e);
+  if (rc) return rc;
+  if ((rc = apply_shapes(e, best[0], best[1], best[2]))) return rc;
+  if (best_shape) { best_shape[0] = best[0]; best_shape[1] = best[1]; best_shape[2] = best[2]; }
+  if (best_ms) *best_ms = best_t / steps;
+  return FDMAP_OK;
+}
+
+long long fdmap_gpu_ensemble_launch_count(fdmap_ensemble* e) { return e ? e->launches : -1; }
+
+void fdmap_gpu_ensemble_destroy(fdmap_ensemble* e) { delete e; }
+
+}  // extern "C"

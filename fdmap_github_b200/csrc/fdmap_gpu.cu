@@ -14,33 +14,23 @@
 #include <vector>
 
 #include "edge_kernel.cuh"
-#include "fdmap_gpu.h"
-#include "sbp_tables.h"
+#include "engine.h"
 #include "march_kernel.cuh"
+#include "sbp_tables.h"
 #include "stencil_kernel.cuh"
 
 using namespace fdmap;
 
-namespace {
-
+namespace fdmap {
 thread_local std::string g_err;
 
 int set_err(int code, const std::string& msg) {
   g_err = msg;
   return code;
 }
+}  // namespace fdmap
 
-#define CUDA_TRY(call)                                                                      \
-  do {                                                                                      \
-    cudaError_t e_ = (call);                                                                \
-    if (e_ != cudaSuccess)                                                                  \
-      return set_err(FDMAP_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
-  } while (0)
-
-struct BlockGeom {
-  int mgx, mgy, nx, ny, pitch;
-  long long plane;
-};
+namespace {
 
 // singular_source weights (source.f90:327-406) for the 5 nodes i0-2..i0+2
 void source_weights(double h, double a, double* w) {
@@ -67,126 +57,6 @@ __global__ void set_step_clock(TimeState* ts, double t_start, double dt, long lo
 }
 }  // namespace fdmap
 
-struct fdmap_gpu {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  DevDomain hdom{};
-  DevDomain* ddom = nullptr;
-  std::vector<void*> allocs;
-  long long bytes = 0;
-  int cur = 0;
-  int mode = 2, nF = 6, pI = 2, het = 0;
-  RkTable rk{};
-  int nx_g = 0, ny_g = 0;
-  std::vector<BlockGeom> geom;
-  std::vector<int> iface_n;
-  std::vector<int> iface_fric;
-  int total_tiles = 0, edge_threads = 0;
-  long long closure_threads = 0;
-  long long march_units = 0;
-  int march_grid = 0;
-  int use_march = 1;
-  int fused = 0;  // boundary kernel handles interface solves and closure strips in one launch
-  // CUDA graphs of one full step, one per starting F buffer, replayed by fdmap_gpu_run
-  TimeState* d_time = nullptr;
-  cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
-  double graph_dt = 0.0;
-  long long graph_launches = 0;
-  bool use_graphs = true;
-  double* met_base[MAX_BLOCKS] = {};
-  double* het_base[MAX_BLOCKS] = {};
-  TmapSet* tmaps = nullptr;  // host copy, passed by value to the march kernel
-  double* h_stage = nullptr;  // pinned staging buffer for layout conversion
-  size_t stage_doubles = 0;
-  unsigned long long* d_status = nullptr;
-  long long launches = 0;
-  double* dev_fhat[MAX_BLOCKS][4] = {};
-  int side_n[MAX_BLOCKS][4] = {};
-  cudaStream_t own_stream = nullptr;
-  // boundary work (interface solves, closure strips) runs on a low-priority
-  // side stream beside the interior march of the same stage
-  bool overlap = false;
-  cudaStream_t side_stream = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  // per-kernel event timing (fdmap_gpu_profile)
-  bool profiling = false;
-  std::vector<cudaEvent_t> ev_pool;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;  // kind, (start, stop)
-  double prof_ms[3] = {0, 0, 0};
-  long long prof_n[3] = {0, 0, 0};
-
-  template <typename T>
-  int alloc(T** p, size_t count) {
-    void* q = nullptr;
-    size_t bytes_ = count * sizeof(T);
-    if (bytes_ == 0) bytes_ = 16;
-    cudaError_t e = cudaMalloc(&q, bytes_);
-    if (e != cudaSuccess) return set_err(FDMAP_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    allocs.push_back(q);
-    bytes += (long long)bytes_;
-    *p = (T*)q;
-    return FDMAP_OK;
-  }
-  // field arrays: PADL doubles of front padding so halo bulk copies may start
-  // before column 0; every plane carries PADTAIL doubles of slack after its last row
-  int alloc_planes(double** base, int nplanes, long long plane) {
-    double* raw = nullptr;
-    int rc = alloc(&raw, (size_t)PADL + (size_t)nplanes * plane);
-    if (rc) return rc;
-    CUDA_TRY(cudaMemset(raw, 0, ((size_t)PADL + (size_t)nplanes * plane) * sizeof(double)));
-    *base = raw + PADL;
-    return FDMAP_OK;
-  }
-  int upload(double** dst, const double* src, size_t count) {
-    int rc = alloc(dst, count);
-    if (rc) return rc;
-    if (src) CUDA_TRY(cudaMemcpy(*dst, src, count * sizeof(double), cudaMemcpyHostToDevice));
-    return FDMAP_OK;
-  }
-  // global (nx_g, ny_g) plane -> padded block plane on the device
-  int upload_plane(double* dst, const double* src, const BlockGeom& g) {
-    std::vector<double> tmp((size_t)g.plane, 0.0);
-    for (int j = 0; j < g.ny; ++j)
-      for (int i = 0; i < g.nx; ++i)
-        tmp[(size_t)j * g.pitch + i] = src[(size_t)(g.mgx - 1 + i) + (size_t)nx_g * (size_t)(g.mgy - 1 + j)];
-    CUDA_TRY(cudaMemcpy(dst, tmp.data(), tmp.size() * sizeof(double), cudaMemcpyHostToDevice));
-    return FDMAP_OK;
-  }
-  cudaEvent_t take_event() {
-    cudaEvent_t e;
-    if (!ev_pool.empty()) { e = ev_pool.back(); ev_pool.pop_back(); }
-    else cudaEventCreate(&e);
-    return e;
-  }
-  // folds finished event pairs into the totals (blocking on the last one)
-  void drain_events() {
-    for (auto& p : ev_pending) {
-      cudaEventSynchronize(p.second.second);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, p.second.first, p.second.second);
-      prof_ms[p.first] += ms;
-      prof_n[p.first] += 1;
-      ev_pool.push_back(p.second.first);
-      ev_pool.push_back(p.second.second);
-    }
-    ev_pending.clear();
-  }
-  ~fdmap_gpu() {
-    if (device >= 0) cudaSetDevice(device);
-    if (stream) cudaStreamSynchronize(stream);
-    for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
-    for (auto e : ev_pool) cudaEventDestroy(e);
-    for (void* p : allocs) cudaFree(p);
-    if (h_stage) cudaFreeHost(h_stage);
-    if (own_stream) cudaStreamDestroy(own_stream);
-    if (side_stream) cudaStreamDestroy(side_stream);
-    if (ev_fork) cudaEventDestroy(ev_fork);
-    if (ev_join) cudaEventDestroy(ev_join);
-    delete tmaps;
-    for (auto& ge : step_graph)
-      if (ge) cudaGraphExecDestroy(ge);
-  }
-};
 
 namespace {
 
@@ -295,7 +165,7 @@ int march_setup(fdmap_gpu* h) {
 
 template <int MODE, int PI_, bool HET>
 void march_launch(fdmap_gpu* h, const StageArgs& a) {
-  MarchPlan plan{h->march_grid, h->march_units};
+  MarchPlan plan{h->march_grid, h->march_units, nullptr, nullptr, 1};
   march_kernel<MODE, PI_, HET><<<h->march_grid, MTHREADS, MarchLayout<MODE, PI_, HET>::BYTES, h->stream>>>(h->ddom, a, plan, *h->tmaps);
 }
 
@@ -319,6 +189,58 @@ int march_dispatch(fdmap_gpu* h, const StageArgs* a) {
   if (h->mode == 2) return h->het ? go(std::integral_constant<int, 2>{}, std::true_type{}) : go(std::integral_constant<int, 2>{}, std::false_type{});
   return h->het ? go(std::integral_constant<int, 3>{}, std::true_type{}) : go(std::integral_constant<int, 3>{}, std::false_type{});
 }
+
+// (mode, SBP half-width, heterogeneity) of a handle as compile-time constants
+template <typename Fn>
+int dispatch_variant(const fdmap_gpu* h, Fn&& fn) {
+  auto go = [&](auto mode_c, auto het_c) {
+    return dispatch_pi<decltype(mode_c)::value, decltype(het_c)::value>(
+        h->pI, [&](auto pi_c) { return fn(mode_c, pi_c, het_c); });
+  };
+  if (h->mode == 2) return h->het ? go(std::integral_constant<int, 2>{}, std::true_type{}) : go(std::integral_constant<int, 2>{}, std::false_type{});
+  return h->het ? go(std::integral_constant<int, 3>{}, std::true_type{}) : go(std::integral_constant<int, 3>{}, std::false_type{});
+}
+
+}  // namespace
+
+namespace fdmap {
+
+int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s) {
+  return dispatch_variant(proto, [&](auto mode_c, auto pi_c, auto het_c) {
+    constexpr int MODE = decltype(mode_c)::value;
+    constexpr int PI_ = decltype(pi_c)::value;
+    constexpr bool HET = decltype(het_c)::value;
+    MarchPlan plan{p.march_grid, p.units, p.tmaps, p.unit_begin, p.ninst};
+    march_kernel<MODE, PI_, HET><<<p.march_grid, MTHREADS, MarchLayout<MODE, PI_, HET>::BYTES, s>>>(p.doms, a, plan,
+                                                                                                    *proto->tmaps);
+    CUDA_TRY(cudaGetLastError());
+    return (int)FDMAP_OK;
+  });
+}
+
+int batch_closure(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s) {
+  if (p.closure_ctas == 0) return FDMAP_OK;
+  return dispatch_variant(proto, [&](auto mode_c, auto pi_c, auto het_c) {
+    constexpr int MODE = decltype(mode_c)::value;
+    constexpr int PI_ = decltype(pi_c)::value;
+    constexpr bool HET = decltype(het_c)::value;
+    closure_kernel_batch<MODE, PI_, HET><<<p.closure_ctas, p.closure_tpb, 0, s>>>(p.doms, p.closure_cta_begin, p.ninst, a);
+    CUDA_TRY(cudaGetLastError());
+    return (int)FDMAP_OK;
+  });
+}
+
+int batch_edges(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s) {
+  if (p.edge_ctas == 0) return FDMAP_OK;
+  if (proto->mode == 2) edge_kernel_batch<2><<<p.edge_ctas, p.edge_tpb, 0, s>>>(p.doms, p.edge_cta_begin, p.ninst, a);
+  else edge_kernel_batch<3><<<p.edge_ctas, p.edge_tpb, 0, s>>>(p.doms, p.edge_cta_begin, p.ninst, a);
+  CUDA_TRY(cudaGetLastError());
+  return FDMAP_OK;
+}
+
+}  // namespace fdmap
+
+namespace {
 
 template <int MODE>
 void launch_closure_mode(fdmap_gpu* h, const StageArgs& a) {

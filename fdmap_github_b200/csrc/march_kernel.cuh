@@ -27,8 +27,6 @@ namespace fdmap {
 constexpr int MW = 128;         // strip width (columns)
 constexpr int MR = 4;           // rows per row group
 constexpr int MTHREADS = MW * MR;
-constexpr int PADL = 32;        // doubles of front padding before every field array
-constexpr int PADTAIL = 192;    // slack after the last row of every field plane
 constexpr int NGS = 4;          // neighbour ring: row groups g-1, g, g+1 resident, g+2 in flight
 constexpr int NCS = 2;          // centre ring: group g resident, g+1 in flight
 
@@ -58,7 +56,12 @@ struct MarchLayout {
 
 struct MarchPlan {
   int grid;          // CTAs launched
-  long long units;   // total row groups over all strips of all blocks
+  long long units;   // total row groups over all strips of all blocks (of all instances)
+  // batched instances: per-instance tensor maps in device memory and the
+  // prefix of march units over instances; ninst == 1 uses the by-value maps
+  const TmapSet* tms;
+  const long long* unit_begin;
+  int ninst;
 };
 
 // Interface node k of interface I, then the whole stage for the two edge nodes
@@ -102,15 +105,6 @@ __global__ void __launch_bounds__(128) boundary_kernel(const __grid_constant__ D
   }
 }
 
-// TMA descriptors of every block, passed by value as a __grid_constant__ parameter
-struct TmapSet {
-  CUtensorMap F[MAX_BLOCKS][2];    // rate fields, box {WH, MR, NR}
-  CUtensorMap F6[MAX_BLOCKS][2];   // szz plane (mode II), box {MW, MR, 1}
-  CUtensorMap DF[MAX_BLOCKS];      // rates, box {MW, MR, NR}
-  CUtensorMap MH[MAX_BLOCKS];      // yr, xr, box {WH, MR, 2}
-  CUtensorMap MC[MAX_BLOCKS];      // yq, xq, Ji, box {MW, MR, 3}
-  CUtensorMap HT[MAX_BLOCKS];      // heterogeneous material, box {MW, MR, NH}
-};
 
 // ---------------------------------------------------------------------------
 // PTX helpers: mbarrier and 1-D bulk copy global -> shared
@@ -184,7 +178,7 @@ constexpr int march_regs() { return (MODE == 2 && PI_ == 3) ? 128 : 96; }
 
 template <int MODE, int PI_, bool HET>
 __global__ void __maxnreg__((march_regs<MODE, PI_>()))
-    march_kernel(const DevDomain* __restrict__ Dp, StageArgs a, MarchPlan plan, const __grid_constant__ TmapSet tm) {
+    march_kernel(const DevDomain* __restrict__ doms, StageArgs a, MarchPlan plan, const __grid_constant__ TmapSet tm) {
   using L = MarchLayout<MODE, PI_, HET>;
   using RD = RDef<MODE>;
   constexpr int NR = RD::NR;
@@ -196,7 +190,6 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
   unsigned long long* nbar = reinterpret_cast<unsigned long long*>(smem + L::BARS_OFF);
   unsigned long long* cbar = nbar + NGS;
 
-  const DevDomain& D = *Dp;
   const int tid = threadIdx.x;
   const int cx = tid % MW, ry = tid / MW;
   const long long ubeg = plan.units * blockIdx.x / gridDim.x;
@@ -208,12 +201,27 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
 
   long long u = ubeg;
   while (u < uend) {
+    // instance owning unit u (the last one whose first unit is <= u)
+    int inst = 0;
+    long long base = 0;
+    if (plan.ninst > 1) {
+      int lo = 0, hi = plan.ninst - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (plan.unit_begin[mid] <= u) lo = mid;
+        else hi = mid - 1;
+      }
+      inst = lo;
+      base = plan.unit_begin[inst];
+    }
+    const DevDomain& D = doms[inst];
+    const TmapSet& tmi = plan.tms ? plan.tms[inst] : tm;
     // segment: consecutive row groups of one strip
-    const UnitPos p0 = unit_pos(D, u);
+    const UnitPos p0 = unit_pos(D, u - base);
     const int b = p0.b;
     const DevBlock& B = D.blk[b];
     const int groups = (B.ny + MR - 1) / MR;
-    const long long strip_end = B.march_unit_begin + (long long)(p0.sx + 1) * groups;
+    const long long strip_end = base + B.march_unit_begin + (long long)(p0.sx + 1) * groups;
     const long long seg_end = uend < strip_end ? uend : strip_end;
     const int jr0 = p0.j0;
     const int jr1 = min(B.ny, (int)(jr0 + (seg_end - u) * MR));
@@ -224,8 +232,8 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
     // neighbour groups needed: k = gmin .. gmax (group k holds rows jr0 + k*MR ..)
     const int gmin = jr0 >= MR ? -1 : 0;
     const int gmax = ngroups - 1 + (jr1 < ny ? 1 : 0);
-    const CUtensorMap* mF = &tm.F[b][a.in];
-    const CUtensorMap* mF6 = &tm.F6[b][a.in];
+    const CUtensorMap* mF = &tmi.F[b][a.in];
+    const CUtensorMap* mF6 = &tmi.F6[b][a.in];
 
     if (tid == 0) {
       for (int s = 0; s < NGS + NCS; ++s) mbar_init(&nbar[s], 1);
@@ -239,17 +247,17 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
       const int row = jr0 + k * MR;
       mbar_arrive_tx(&nbar[sl], L::NB_BYTES);
       tma_load_3d(g + L::F_OFF, mF, i0 - HP, row, 0, &nbar[sl]);
-      tma_load_3d(g + L::MH_OFF, &tm.MH[b], i0 - HP, row, 0, &nbar[sl]);
-      tma_load_3d(g + L::MC_OFF, &tm.MC[b], i0, row, 2, &nbar[sl]);
+      tma_load_3d(g + L::MH_OFF, &tmi.MH[b], i0 - HP, row, 0, &nbar[sl]);
+      tma_load_3d(g + L::MC_OFF, &tmi.MC[b], i0, row, 2, &nbar[sl]);
     };
     auto fill_c = [&](int k) {  // centre group k -> slot k % NCS
       const int sl = k % NCS;
       unsigned char* g = smem + (size_t)NGS * L::GSLOT + (size_t)sl * L::CSLOT;
       const int row = jr0 + k * MR;
       mbar_arrive_tx(&cbar[sl], cbytes);
-      if (load_df) tma_load_3d(g + L::DF_OFF, &tm.DF[b], i0, row, 0, &cbar[sl]);
+      if (load_df) tma_load_3d(g + L::DF_OFF, &tmi.DF[b], i0, row, 0, &cbar[sl]);
       if (MODE == 2) tma_load_3d(g + L::F6_OFF, mF6, i0, row, 5, &cbar[sl]);
-      if (HET) tma_load_3d(g + L::HT_OFF, &tm.HT[b], i0, row, 0, &cbar[sl]);
+      if (HET) tma_load_3d(g + L::HT_OFF, &tmi.HT[b], i0, row, 0, &cbar[sl]);
     };
     if (tid == 0) {
       fence_proxy_async();

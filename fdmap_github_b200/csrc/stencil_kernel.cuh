@@ -333,6 +333,19 @@ __global__ void __launch_bounds__(128) closure_kernel(const __grid_constant__ De
   closure_node<MODE, PI_, HET>(D, D.blk[b], i, j, a, -1, nullptr);
 }
 
+// Closure strips of a batch of independent instances in one launch.
+template <int MODE, int PI_, bool HET>
+__global__ void __launch_bounds__(256)
+    closure_kernel_batch(const DevDomain* __restrict__ doms, const int* __restrict__ cta_begin, int ninst, StageArgs a) {
+  const int k = batch_instance(cta_begin, ninst, blockIdx.x);
+  const DevDomain& D = doms[k];
+  const long long tid = (long long)(blockIdx.x - cta_begin[k]) * blockDim.x + threadIdx.x;
+  if (tid >= D.cstart[4 * D.nblocks]) return;
+  int i, j;
+  const int b = closure_item(D, tid, i, j);
+  closure_node<MODE, PI_, HET>(D, D.blk[b], i, j, a, -1, nullptr);
+}
+
 template <int MODE, int PI_, bool HET>
 __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __restrict__ Dp, StageArgs a) {
   using RD = RDef<MODE>;

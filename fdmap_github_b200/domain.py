@@ -85,9 +85,13 @@ def init_domain(input_text: str, base_dir: str | Path | None = None) -> HostDoma
 class GpuDomain:
     """Device-resident copy of a domain, advanced by the sm_100a kernels."""
 
-    def __init__(self, host: HostDomain, device: int = 0, init_edges: bool = True):
+    def __init__(self, host: HostDomain, device: int = 0, init_edges: bool = True, _handle=None, _owner=None):
         self.host = host
         self.nx, self.ny, self.nF = host.nx, host.ny, host.nF
+        self._owner = _owner  # an instance handle is owned (and freed) by its ensemble
+        if _handle is not None:
+            self._g = _handle
+            return
         self._g = C.c_void_p()
         check_gpu(lib().fdmap_gpu_create(host.desc, device, int(init_edges), C.byref(self._g)), "fdmap_gpu_create")
 
@@ -142,9 +146,86 @@ class GpuDomain:
         return lib().fdmap_gpu_device_bytes(self._g)
 
     def close(self) -> None:
-        if self._g:
+        if self._g and self._owner is None:
             lib().fdmap_gpu_destroy(self._g)
-            self._g = C.c_void_p()
+        self._g = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GpuEnsemble:
+    """Independent domains advanced together by batched launches
+    (fdmap_gpu_ensemble_*): one interior march, one interface and one closure
+    launch per stage for all instances, one CUDA graph per step."""
+
+    def __init__(self, hosts: list[HostDomain], device: int = 0, init_edges: bool = True):
+        self.hosts = list(hosts)
+        arr = (C.c_void_p * len(self.hosts))(*[h.desc.value for h in self.hosts])
+        self._e = C.c_void_p()
+        check_gpu(lib().fdmap_gpu_ensemble_create(arr, len(self.hosts), device, int(init_edges), C.byref(self._e)),
+                  "fdmap_gpu_ensemble_create")
+        self.instances = []
+        for k, h in enumerate(self.hosts):
+            g = C.c_void_p()
+            check_gpu(lib().fdmap_gpu_ensemble_instance(self._e, k, C.byref(g)), "fdmap_gpu_ensemble_instance")
+            self.instances.append(GpuDomain(h, _handle=g, _owner=self))
+
+    def __len__(self) -> int:
+        return len(self.hosts)
+
+    def __getitem__(self, k: int) -> GpuDomain:
+        return self.instances[k]
+
+    def time_step_LS(self, t0: float, dt: float, final_step: bool = False) -> None:
+        check_gpu(lib().fdmap_gpu_ensemble_time_step(self._e, t0, dt, int(final_step)), "ensemble time_step_LS")
+
+    @property
+    def dt(self) -> float:
+        """Common time step: the smallest of the instances' stable steps."""
+        return min(h.dt for h in self.hosts)
+
+    def run(self, n_first: int, n_last: int, t_start: float | None = None, dt: float | None = None,
+            nt: int | None = None) -> None:
+        h = self.hosts[0]
+        check_gpu(lib().fdmap_gpu_ensemble_run(self._e, h.t0 if t_start is None else t_start,
+                                               self.dt if dt is None else dt, n_first, n_last,
+                                               h.nt if nt is None else nt), "fdmap_gpu_ensemble_run")
+
+    def synchronize(self) -> None:
+        check_gpu(lib().fdmap_gpu_ensemble_synchronize(self._e), "fdmap_gpu_ensemble_synchronize")
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        s = (C.c_int * 3)()
+        check_gpu(lib().fdmap_gpu_ensemble_get_shape(self._e, s), "fdmap_gpu_ensemble_get_shape")
+        return tuple(s)
+
+    @shape.setter
+    def shape(self, v) -> None:
+        s = (C.c_int * 3)(*v)
+        check_gpu(lib().fdmap_gpu_ensemble_set_shape(self._e, s), "fdmap_gpu_ensemble_set_shape")
+
+    def tune(self, steps: int = 5, dt: float | None = None) -> tuple[tuple[int, int, int], float]:
+        """Autotune the launch shape; returns (shape, ms per step of the best)."""
+        s = (C.c_int * 3)()
+        ms = C.c_double()
+        check_gpu(lib().fdmap_gpu_ensemble_tune(self._e, self.dt if dt is None else dt, steps, s,
+                                                C.byref(ms)), "fdmap_gpu_ensemble_tune")
+        return tuple(s), ms.value
+
+    def launch_count(self) -> int:
+        return lib().fdmap_gpu_ensemble_launch_count(self._e)
+
+    def close(self) -> None:
+        for g in self.instances:
+            g._g = C.c_void_p()
+        if self._e:
+            lib().fdmap_gpu_ensemble_destroy(self._e)
+            self._e = C.c_void_p()
 
     def __del__(self):
         try:

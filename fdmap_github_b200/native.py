@@ -61,6 +61,18 @@ SIGNATURES = {
     "fdmap_gpu_destroy": (None, [_VP]),
     "fdmap_gpu_strerror": (C.c_char_p, [C.c_int]),
     "fdmap_gpu_last_error": (C.c_char_p, []),
+    # fdmap_gpu.h: batched ensemble
+    "fdmap_gpu_ensemble_create": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_int, C.c_int, C.POINTER(_VP)]),
+    "fdmap_gpu_ensemble_size": (C.c_int, [_VP]),
+    "fdmap_gpu_ensemble_instance": (C.c_int, [_VP, C.c_int, C.POINTER(_VP)]),
+    "fdmap_gpu_ensemble_time_step": (C.c_int, [_VP, C.c_double, C.c_double, C.c_int]),
+    "fdmap_gpu_ensemble_run": (C.c_int, [_VP, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int]),
+    "fdmap_gpu_ensemble_synchronize": (C.c_int, [_VP]),
+    "fdmap_gpu_ensemble_set_shape": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "fdmap_gpu_ensemble_get_shape": (C.c_int, [_VP, C.POINTER(C.c_int)]),
+    "fdmap_gpu_ensemble_tune": (C.c_int, [_VP, C.c_double, C.c_int, C.POINTER(C.c_int), _DP]),
+    "fdmap_gpu_ensemble_launch_count": (C.c_longlong, [_VP]),
+    "fdmap_gpu_ensemble_destroy": (None, [_VP]),
 }
 
 _lib = None

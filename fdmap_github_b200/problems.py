@@ -9,6 +9,7 @@ Units follow FDMAP: km, s, m/s, MPa, g/cm^3, km/s (2670 kg/m^3 -> 2.67,
   rupture_sw           mode II slip-weakening rupture, two blocks      (config "c2")
   rough_fault_rs       mode II rate-and-state on a rough fault         (config "c3")
   heterogeneous_ricker mode III heterogeneous medium, Ricker point force (config "c5")
+  ensemble_instance    mode II rate-and-state, planar fault, von Karman prestress (config "c4")
 """
 from __future__ import annotations
 
@@ -177,4 +178,73 @@ def heterogeneous_ricker(outdir: str | Path, n: int = 801, h: float = 0.02, nt: 
 &material_list heterogeneous=T, filename='medium.dat', rho=2.67d0, cs=3.464d0 /
 !---END---
 &source_list x0={_f(x0)}, y0={_f(y0)}, Fz=1d0, source_time_function='Ricker', t_center={_f(1.2 * T)}, t_duration={_f(T)} /
+"""
+
+
+def von_karman_1d(n: int, h: float, hurst: float, corr: float, seed: int) -> np.ndarray:
+    """Seeded 1-D von Karman random field on n points of spacing h: power
+    spectral density proportional to (1 + (k a)^2)^-(H + 1/2) with k the
+    angular wavenumber and a the correlation length; zero mean, unit std."""
+    rng = np.random.default_rng(seed)
+    m = 2 * n
+    k = 2.0 * np.pi * np.fft.rfftfreq(m, d=h)
+    psd = (1.0 + (k * corr) ** 2) ** (-(hurst + 0.5))
+    w = np.fft.rfft(rng.standard_normal(m)) * np.sqrt(psd)
+    w[0] = 0.0
+    f = np.fft.irfft(w, n=m)[:n]
+    f = f - f.mean()
+    return f / f.std()
+
+
+ENSEMBLE_GRIDS = ((401, 401), (801, 401), (801, 801), (1601, 801))
+
+
+def ensemble_grid(seed: int) -> tuple[int, int]:
+    """Per-block grid of ensemble instance `seed`: a seeded uniform draw from
+    401x401, 801x401, 801x801 and 1601x801 (nx x ny)."""
+    return ENSEMBLE_GRIDS[int(np.random.default_rng(1000 + seed).integers(len(ENSEMBLE_GRIDS)))]
+
+
+def ensemble_instance(outdir: str | Path, seed: int, nx: int | None = None, ny: int | None = None,
+                      h: float = 0.025, nt: int = 1001, rk: int = 4, cfl: float = 0.5, fd: str = "SBP4",
+                      N0: float = 120.0, Vinit: float = 1e-12, hurst: float = 0.8, corr: float = 2.0,
+                      std: float = 0.1, strength_frac: float = 0.6) -> str:
+    """One instance of the rupture ensemble: mode II regularised rate-and-state
+    (slip law with flash heating, 'RFL', the rough-fault friction parameters)
+    on a planar fault y = 0 between two blocks of nx x ny nodes (spacing h km).
+    Initial shear stress S0 = strength_frac * f0 * N0 * (1 + std * z) with z a
+    seeded von Karman field (Hurst `hurst`, correlation length `corr` km);
+    the state gives slip velocity Vinit under it; a Gaussian overstress at
+    the fault centre nucleates rupture.  Writes stress and state files into
+    outdir and returns the input text (file names relative to outdir)."""
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    if nx is None or ny is None:
+        nx, ny = ensemble_grid(seed)
+    Lx, Ly = (nx - 1) * h, (ny - 1) * h
+    a, b, V0, f0, L, fw, Vw = 0.01, 0.014, 1e-6, 0.6, 0.4, 0.2, 0.1
+    z = von_karman_1d(nx, h, hurst, corr, seed)
+    N0a = np.full(nx, N0)
+    S0 = strength_frac * f0 * N0a * (1.0 + std * z)
+    _write(out / f"stress_{seed}.dat", S0, N0a)
+    Psi = a * np.log(2.0 * V0 / Vinit * np.sinh(S0 / (a * N0a)))
+    _write(out / f"state_{seed}.dat", Psi)
+    x0, x1 = -0.5 * Lx, 0.5 * Lx
+    blk = """&material_list rho=2.67d0, cs=3.464d0, cp=6d0 /
+"""
+    return f"""&problem_list name='ensemble_{seed}', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
+&domain_list mode=2, FDmethod='{fd}', nblocks_x=1, nblocks_y=2 /
+!---BLOCK1---
+&grid_list nx={nx}, ny={ny}, LB={_f(x0)},{_f(-Ly)}, LT={_f(x0)},0d0, RB={_f(x1)},{_f(-Ly)}, RT={_f(x1)},0d0 /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='none' /
+{blk}!---BLOCK2---
+&grid_list nx={nx}, ny={ny}, LB={_f(x0)},0d0, LT={_f(x0)},{_f(Ly)}, RB={_f(x1)},0d0, RT={_f(x1)},{_f(Ly)} /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='none', bcT='absorbing' /
+{blk}!---IFACE1---
+&interface_list coupling='friction' /
+&friction_list friction_law='RFL', rs%a={_f(a)}, rs%b={_f(b)}, rs%V0={_f(V0)}, rs%f0={_f(f0)}, rs%L={_f(L)},
+  rs%fw={_f(fw)}, rs%Vw={_f(Vw)}, stress_file=T, stress_filename='stress_{seed}.dat',
+  state_file=T, state_filename='state_{seed}.dat',
+  ld%shape='gaussian', ld%R=1.5d0, ld%S=25d0, ld%x0=0d0,
+  rup_field='V', rup_threshold=1d-3 /
 """

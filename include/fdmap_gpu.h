@@ -87,6 +87,47 @@ const char* fdmap_gpu_strerror(int code);
 /* Last CUDA / validation message on this thread. */
 const char* fdmap_gpu_last_error(void);
 
+/* ------------------------------------------------------------------------
+ * Batched ensemble: `ninst` independent domains (uneven grid sizes, their own
+ * prestress and friction state) advanced together, each stage one launch per
+ * kernel kind for all instances, each step a replayed CUDA graph.  The
+ * reference runs such an ensemble as separate main.f90 jobs, one per input
+ * file; there is no single reference routine this replaces.  Instances must
+ * share mode, FD method, RK order and material kind (homogeneous mode II or
+ * any mode III) and step with one dt.  Every instance reproduces its plain
+ * single-domain run bit for bit.
+ * ---------------------------------------------------------------------- */
+typedef struct fdmap_ensemble fdmap_ensemble;
+
+/* descs[k]: descriptor of instance k (as for fdmap_gpu_create). */
+int fdmap_gpu_ensemble_create(const fdmap_desc* const* descs, int ninst, int device, int init_edges,
+                              fdmap_ensemble** e);
+int fdmap_gpu_ensemble_size(fdmap_ensemble* e);
+
+/* Handle of instance k for fdmap_gpu_get_* / set_* / status (ordered after
+ * the ensemble's work).  Owned by the ensemble; stepping it on its own is an
+ * error for the next ensemble step. */
+int fdmap_gpu_ensemble_instance(fdmap_ensemble* e, int k, fdmap_gpu** h);
+
+/* As fdmap_gpu_time_step / fdmap_gpu_run, for every instance at once. */
+int fdmap_gpu_ensemble_time_step(fdmap_ensemble* e, double t0, double dt, int final_step);
+int fdmap_gpu_ensemble_run(fdmap_ensemble* e, double t_start, double dt, int n_first, int n_last, int nt);
+int fdmap_gpu_ensemble_synchronize(fdmap_ensemble* e);
+
+/* Launch shape: shape[0] closure-kernel block size (64, 128, 256),
+ * shape[1] interface-kernel block size (32, 64, 128), shape[2] 1 = boundary
+ * kernels run beside the interior march, 0 = serialised. */
+int fdmap_gpu_ensemble_set_shape(fdmap_ensemble* e, const int* shape);
+int fdmap_gpu_ensemble_get_shape(fdmap_ensemble* e, int* shape);
+
+/* Autotuner: times `steps` replayed steps of every launch shape, applies the
+ * fastest and returns it (best_shape[3], best_ms per step; either may be
+ * NULL).  The ensemble's state is restored afterwards. */
+int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_shape, double* best_ms);
+
+long long fdmap_gpu_ensemble_launch_count(fdmap_ensemble* e);
+void fdmap_gpu_ensemble_destroy(fdmap_ensemble* e);
+
 #ifdef __cplusplus
 }
 #endif
