@@ -4,9 +4,10 @@ frictional faults), behind a C ABI that FDMAP's Fortran driver can call.
 Public Python surface (a mirror of the reference's host interface):
   init_domain, HostDomain, GpuDomain  -- fdmap_github_b200.domain
   GpuEnsemble                         -- batched independent instances
+  GpuAdjoint                          -- misfit gradient (forward/backward pair)
   FdmapError                          -- raised on any non-zero status
 """
-from .domain import GpuDomain, GpuEnsemble, HostDomain, init_domain  # noqa: F401
+from .domain import GpuAdjoint, GpuDomain, GpuEnsemble, HostDomain, init_domain  # noqa: F401
 from .native import FAULT_FIELDS, FdmapError  # noqa: F401
 
-__all__ = ["init_domain", "HostDomain", "GpuDomain", "GpuEnsemble", "FdmapError", "FAULT_FIELDS"]
+__all__ = ["init_domain", "HostDomain", "GpuDomain", "GpuEnsemble", "GpuAdjoint", "FdmapError", "FAULT_FIELDS"]

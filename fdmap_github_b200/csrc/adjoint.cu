@@ -1,0 +1,455 @@
+// Forward/backward pair for gradients of a receiver-seismogram misfit with
+// respect to the density and shear-modulus fields of a heterogeneous mode III
+// block (SBP-SAT wave solve, LS-RK time stepping).  The reference has no
+// adjoint; the forward pass is the engine's own time step (time_step_LS,
+// time_step.f90:71-167), so the misfit is that of the production path.
+//
+//   forward : steps 1..nt-1 as replayed graphs; vz sampled at the receivers at
+//             every step start (n = 1..nt, the reference's stage-1 output
+//             point, time_step.f90:129); the fields are checkpointed every
+//             `checkpoint_every` steps.
+//   backward: segments in reverse; each is recomputed from its checkpoint with
+//             every stage input stored, then reversed stage by stage with the
+//             discrete adjoint (adjoint_kernel.cuh), injecting the receiver
+//             residuals dJ/dU^n = vz - d at every step start.
+// J = 1/2 sum_n sum_r (vz_r(U^n) - d_r^n)^2.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "adjoint_kernel.cuh"
+#include "engine.h"
+#include "fdmap_gpu.h"
+
+using namespace fdmap;
+
+struct fdmap_adjoint {
+  fdmap_gpu* h = nullptr;
+  int K = 45;                        // steps per checkpoint segment
+  int nrec = 0;
+  int N = 0;                         // samples of the last forward (nt)
+  double t_start = 0.0, dt = 0.0;
+  std::vector<long long> rec_host;   // block-local linear node index of each receiver
+  long long* rec = nullptr;
+  double* init_F = nullptr;          // initial fields (3 planes)
+  double* init_DF = nullptr;
+  double* ckpt = nullptr;            // checkpoints, 3 planes each
+  int nckpt_alloc = 0;
+  double* store = nullptr;           // stage inputs of one segment: K*nstage slots of 3 planes
+  double* ub[2] = {nullptr, nullptr};
+  double* qp[2] = {nullptr, nullptr};
+  double* grho = nullptr;
+  double* gG = nullptr;
+  double* geo[4] = {nullptr, nullptr, nullptr, nullptr};
+  double* traces = nullptr;          // N*nrec
+  double* resid = nullptr;           // N*nrec
+  int trace_alloc = 0;
+  AdjClock* clock = nullptr;
+  bool have_resid = false;
+  // graphs: forward step (by F parity), recompute step (by F parity), adjoint step (by ubar parity)
+  cudaGraphExec_t g_fwd[2] = {nullptr, nullptr}, g_rec[2] = {nullptr, nullptr}, g_adj[2] = {nullptr, nullptr};
+  double graph_dt = -1.0;
+  std::vector<void*> mem;
+
+  long long stride() const { return 3 * h->hdom.blk[0].plane; }
+  void free_graphs() {
+    for (auto* set : {g_fwd, g_rec, g_adj})
+      for (int q = 0; q < 2; ++q)
+        if (set[q]) { cudaGraphExecDestroy(set[q]); set[q] = nullptr; }
+    graph_dt = -1.0;
+  }
+  ~fdmap_adjoint() {
+    if (h) {
+      cudaSetDevice(h->device);
+      cudaStreamSynchronize(h->stream);
+    }
+    free_graphs();
+    for (void* p : mem) cudaFree(p);
+    if (h) fdmap_gpu_destroy(h);
+  }
+  template <typename T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, std::max<size_t>(count * sizeof(T), 16)) != cudaSuccess)
+      return set_err(FDMAP_ERR_NOMEM, "adjoint: out of device memory");
+    mem.push_back(q);
+    *p = (T*)q;
+    return FDMAP_OK;
+  }
+  void release(void* p) {
+    if (!p) return;
+    auto it = std::find(mem.begin(), mem.end(), p);
+    if (it != mem.end()) mem.erase(it);
+    cudaFree(p);
+  }
+};
+
+namespace {
+
+int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p) {
+  fdmap_gpu* h = a->h;
+  const DevBlock& B = h->hdom.blk[0];
+  dim3 blk(ATX * ATY), grid((B.nx + ATX - 1) / ATX, (B.ny + ATY - 1) / ATY);
+  // interior tiles and edge tiles write disjoint nodes from the same inputs
+  if (h->pI == 1) {
+    adj_stage_kernel<1><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_edge_kernel<1><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+  } else if (h->pI == 2) {
+    adj_stage_kernel<2><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_edge_kernel<2><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+  } else {
+    adj_stage_kernel<3><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_edge_kernel<3><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return FDMAP_OK;
+}
+
+// forward stage sequence of one step from buffer `cur` (the engine's time_step_LS body)
+int forward_step_stages(fdmap_adjoint* a, int cur, double dt, bool stash) {
+  fdmap_gpu* h = a->h;
+  const DevBlock& B = h->hdom.blk[0];
+  for (int s = 0; s < h->rk.nstage; ++s) {
+    if (stash) {
+      adj_stash<<<296, 256, 0, h->stream>>>(B.F[cur], a->store, a->stride(), &a->clock->rel, s, h->rk.nstage,
+                                            a->stride());
+      CUDA_TRY(cudaGetLastError());
+    }
+    StageArgs st{};
+    st.A = h->rk.A[s];
+    st.Bdt = h->rk.B[s] * dt;
+    st.C = h->rk.C[s];
+    st.ts = h->d_time;
+    st.in = cur;
+    st.out = 1 - cur;
+    st.scale = 1;
+    st.update = 1;
+    int rc = engine_stage(h, st);
+    if (rc) return rc;
+    cur = 1 - cur;
+  }
+  return FDMAP_OK;
+}
+
+int capture(fdmap_adjoint* a, cudaGraphExec_t* out, const std::function<int()>& body) {
+  cudaStream_t s = a->h->stream;
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int rc = body();
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (rc == FDMAP_OK && e != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("adjoint capture: ") + cudaGetErrorString(e));
+  if (rc == FDMAP_OK) {
+    e = cudaGraphInstantiate(out, g, cudaGraphInstantiateFlagUseNodePriority);
+    if (e != cudaSuccess) rc = set_err(FDMAP_ERR_CUDA, std::string("adjoint instantiate: ") + cudaGetErrorString(e));
+  }
+  if (g) cudaGraphDestroy(g);
+  return rc;
+}
+
+int build_graphs(fdmap_adjoint* a, double dt) {
+  a->free_graphs();
+  fdmap_gpu* h = a->h;
+  const long long saved = h->launches;
+  const DevBlock& B = h->hdom.blk[0];
+  int rc = FDMAP_OK;
+  for (int c = 0; c < 2 && rc == FDMAP_OK; ++c) {
+    // forward step: sample vz at the receivers at the step start, then the stages
+    rc = capture(a, &a->g_fwd[c], [&]() -> int {
+      adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[c], a->rec, a->nrec, h->d_time, a->traces, a->trace_alloc);
+      int r = forward_step_stages(a, c, dt, false);
+      if (r) return r;
+      advance_step<<<1, 1, 0, h->stream>>>(h->d_time);
+      return (int)FDMAP_OK;
+    });
+    if (rc) break;
+    // recomputed step: every stage input goes to the segment store
+    rc = capture(a, &a->g_rec[c], [&]() -> int {
+      int r = forward_step_stages(a, c, dt, true);
+      if (r) return r;
+      adj_forward_advance<<<1, 1, 0, h->stream>>>(h->d_time, a->clock);
+      return (int)FDMAP_OK;
+    });
+    if (rc) break;
+    // adjoint step: stages in reverse from ubar parity c, then the residual at this step start
+    rc = capture(a, &a->g_adj[c], [&]() -> int {
+      int q = c;
+      for (int s = h->rk.nstage - 1; s >= 0; --s) {
+        AdjStage p{};
+        p.A = h->rk.A[s];
+        p.Bdt = h->rk.B[s] * dt;
+        p.s = s;
+        p.nstage = h->rk.nstage;
+        p.ub_in = a->ub[q];
+        p.qp_in = a->qp[q];
+        p.ub_out = a->ub[1 - q];
+        p.qp_out = a->qp[1 - q];
+        p.store = a->store;
+        p.stride = a->stride();
+        p.rel = &a->clock->rel;
+        p.grho = a->grho;
+        p.gG = a->gG;
+        int r = adj_stage_launch(a, p);
+        if (r) return r;
+        q = 1 - q;
+      }
+      adj_inject<<<1, 32, 0, h->stream>>>(a->ub[q], a->rec, a->nrec, a->resid, a->clock, 1);
+      return (int)FDMAP_OK;
+    });
+  }
+  h->launches = saved;
+  if (rc == FDMAP_OK) a->graph_dt = dt;
+  return rc;
+}
+
+// global (nx, ny) plane -> device block plane and back
+int to_block(fdmap_adjoint* a, double* dst, const double* src) {
+  fdmap_gpu* h = a->h;
+  return h->upload_plane(dst, src, h->geom[0]);
+}
+
+int from_block(fdmap_adjoint* a, double* dst, const double* src) {
+  fdmap_gpu* h = a->h;
+  const BlockGeom& g = h->geom[0];
+  std::vector<double> tmp((size_t)g.plane);
+  CUDA_TRY(cudaMemcpy(tmp.data(), src, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int j = 0; j < g.ny; ++j)
+    std::memcpy(dst + (size_t)(g.mgy - 1 + j) * h->nx_g + (g.mgx - 1), tmp.data() + (size_t)j * g.pitch,
+                g.nx * sizeof(double));
+  return FDMAP_OK;
+}
+
+int ensure_trace_buffers(fdmap_adjoint* a, int N) {
+  if (N <= a->trace_alloc) return FDMAP_OK;
+  a->release(a->traces);
+  a->release(a->resid);
+  a->traces = a->resid = nullptr;
+  int rc;
+  if ((rc = a->alloc(&a->traces, (size_t)N * a->nrec))) return rc;
+  if ((rc = a->alloc(&a->resid, (size_t)N * a->nrec))) return rc;
+  a->trace_alloc = N;
+  a->free_graphs();  // graphs hold the buffer pointers
+  return FDMAP_OK;
+}
+
+int ensure_checkpoints(fdmap_adjoint* a, int nck) {
+  if (nck <= a->nckpt_alloc) return FDMAP_OK;
+  a->release(a->ckpt);
+  a->ckpt = nullptr;
+  int rc = a->alloc(&a->ckpt, (size_t)nck * a->stride());
+  if (rc) return rc;
+  a->nckpt_alloc = nck;
+  return FDMAP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const int* rec_i, const int* rec_j,
+                             int checkpoint_every, fdmap_adjoint** out) {
+  if (!out) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint pointer");
+  *out = nullptr;
+  if (!d) return set_err(FDMAP_ERR_INVALID_ARG, "null descriptor");
+  if (d->mode != 3 || d->nblocks != 1 || d->nifaces != 0 || !d->heterogeneous)
+    return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers one heterogeneous mode III block without interfaces");
+  for (int s = 0; s < 4; ++s) {
+    int bc = d->blocks[0].side[s].bc;
+    if (bc != FDMAP_BC_ABSORBING && bc != FDMAP_BC_FREE && bc != FDMAP_BC_RIGID)
+      return set_err(FDMAP_ERR_UNSUPPORTED, "adjoint sides must be absorbing, free or rigid");
+  }
+  if (nrec < 1 || !rec_i || !rec_j) return set_err(FDMAP_ERR_INVALID_ARG, "receivers required");
+  if (checkpoint_every < 1) return set_err(FDMAP_ERR_INVALID_ARG, "checkpoint interval must be positive");
+  fdmap_adjoint* a = new (std::nothrow) fdmap_adjoint();
+  if (!a) return set_err(FDMAP_ERR_NOMEM, "out of host memory");
+  auto fail = [&](int rc) {
+    std::string keep = g_err;
+    delete a;
+    g_err = keep;
+    return rc;
+  };
+  int rc = fdmap_gpu_create(d, device, 1, &a->h);
+  if (rc) return fail(rc);
+  fdmap_gpu* h = a->h;
+  a->K = checkpoint_every;
+  a->nrec = nrec;
+  const BlockGeom& g = h->geom[0];
+  for (int r = 0; r < nrec; ++r) {
+    int i = rec_i[r] - g.mgx, j = rec_j[r] - g.mgy;
+    if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) return fail(set_err(FDMAP_ERR_INVALID_ARG, "receiver outside the block"));
+    a->rec_host.push_back((long long)j * g.pitch + i);
+  }
+  const long long S = a->stride();
+  if ((rc = a->alloc(&a->rec, nrec)) || (rc = a->alloc(&a->init_F, S)) || (rc = a->alloc(&a->init_DF, S)) ||
+      (rc = a->alloc(&a->store, (size_t)a->K * h->rk.nstage * S)) || (rc = a->alloc(&a->ub[0], S)) ||
+      (rc = a->alloc(&a->ub[1], S)) || (rc = a->alloc(&a->qp[0], S)) || (rc = a->alloc(&a->qp[1], S)) ||
+      (rc = a->alloc(&a->grho, g.plane)) || (rc = a->alloc(&a->gG, g.plane)) || (rc = a->alloc(&a->clock, 1)))
+    return fail(rc);
+  if (cudaMemcpy(a->rec, a->rec_host.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(set_err(FDMAP_ERR_CUDA, "receiver upload"));
+  const DevBlock& B = h->hdom.blk[0];
+  if (cudaMemcpy(a->init_F, B.F[h->cur], S * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess ||
+      cudaMemcpy(a->init_DF, B.DF, S * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess)
+    return fail(set_err(FDMAP_ERR_CUDA, "initial state copy"));
+  // edge geometry factors H00i*|grad|/J (init_edges, domain.f90:1349-1459)
+  SbpOperator op;
+  sbp_operator(d->fd_method, &op);
+  const fdmap_block& fb = d->blocks[0];
+  for (int s = 0; s < 4; ++s) {
+    const int n = (s < 2) ? g.ny : g.nx;
+    std::vector<double> geo(n);
+    for (int k = 0; k < n; ++k) {
+      int i, j;
+      if (s == 0) { i = fb.mgx; j = fb.mgy + k; }
+      else if (s == 1) { i = fb.pgx; j = fb.mgy + k; }
+      else if (s == 2) { i = fb.mgx + k; j = fb.mgy; }
+      else { i = fb.mgx + k; j = fb.pgy; }
+      const size_t q = (size_t)(i - 1) + (size_t)d->nx * (size_t)(j - 1);
+      const double mag = (s < 2) ? std::sqrt(d->xr[q] * d->xr[q] + d->yr[q] * d->yr[q])
+                                 : std::sqrt(d->xq[q] * d->xq[q] + d->yq[q] * d->yq[q]);
+      geo[k] = op.H00i * mag / d->J[q];
+    }
+    if ((rc = a->alloc(&a->geo[s], n))) return fail(rc);
+    if (cudaMemcpy(a->geo[s], geo.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(set_err(FDMAP_ERR_CUDA, "geometry upload"));
+  }
+  *out = a;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_adjoint_set_material(fdmap_adjoint* a, const double* rho, const double* G) {
+  if (!a || !rho || !G) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  fdmap_gpu* h = a->h;
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const BlockGeom& g = h->geom[0];
+  for (size_t q = 0; q < (size_t)h->nx_g * h->ny_g; ++q)
+    if (!(rho[q] > 0.0) || !(G[q] > 0.0)) return set_err(FDMAP_ERR_INVALID_ARG, "density and shear modulus must be positive");
+  DevBlock& B = h->hdom.blk[0];
+  int rc;
+  if ((rc = to_block(a, B.rho, rho))) return rc;
+  if ((rc = to_block(a, B.G, G))) return rc;
+  for (int s = 0; s < 4; ++s) {
+    const DevSide& S = B.side[s];
+    adj_edge_material<<<(S.n + 127) / 128, 128, 0, h->stream>>>(S, B.rho, B.G, a->geo[s], s, g.nx, g.ny, g.pitch);
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int nt, const double* data, double* traces,
+                              double* misfit) {
+  if (!a) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint");
+  if (nt < 2) return set_err(FDMAP_ERR_INVALID_ARG, "nt must be at least 2");
+  fdmap_gpu* h = a->h;
+  CUDA_TRY(cudaSetDevice(h->device));
+  int rc;
+  if ((rc = ensure_trace_buffers(a, nt))) return rc;
+  const int nck = (nt - 1 + a->K - 1) / a->K;
+  if ((rc = ensure_checkpoints(a, nck))) return rc;
+  a->N = nt;
+  a->t_start = t_start;
+  a->dt = dt;
+  a->have_resid = false;
+  if (a->graph_dt != dt || !a->g_fwd[0]) {
+    if ((rc = build_graphs(a, dt))) return rc;
+  }
+  // reset to the initial state
+  DevBlock& B = h->hdom.blk[0];
+  const long long S = a->stride();
+  h->cur = 0;
+  CUDA_TRY(cudaMemcpyAsync(B.F[0], a->init_F, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(B.DF, a->init_DF, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, t_start, dt, 1);
+  CUDA_TRY(cudaGetLastError());
+  for (int n = 1; n <= nt - 1; ++n) {
+    if ((n - 1) % a->K == 0)
+      CUDA_TRY(cudaMemcpyAsync(a->ckpt + (size_t)((n - 1) / a->K) * S, B.F[h->cur], S * sizeof(double),
+                               cudaMemcpyDeviceToDevice, h->stream));
+    CUDA_TRY(cudaGraphLaunch(a->g_fwd[h->cur], h->stream));
+    if (h->rk.nstage & 1) h->cur = 1 - h->cur;
+  }
+  // last sample: the state the final step starts from (clock n == nt)
+  adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[h->cur], a->rec, a->nrec, h->d_time, a->traces, nt);
+  CUDA_TRY(cudaGetLastError());
+  std::vector<double> tr((size_t)nt * a->nrec);
+  CUDA_TRY(cudaMemcpyAsync(tr.data(), a->traces, tr.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (traces) std::memcpy(traces, tr.data(), tr.size() * sizeof(double));
+  if (data) {
+    double J = 0.0;
+    for (size_t q = 0; q < tr.size(); ++q) {
+      const double r = tr[q] - data[q];
+      tr[q] = r;
+      J += 0.5 * r * r;
+    }
+    if (misfit) *misfit = J;
+    CUDA_TRY(cudaMemcpy(a->resid, tr.data(), tr.size() * sizeof(double), cudaMemcpyHostToDevice));
+    a->have_resid = true;
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_G) {
+  if (!a) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint");
+  if (!a->have_resid) return set_err(FDMAP_ERR_INVALID_ARG, "backward needs a forward run with data");
+  fdmap_gpu* h = a->h;
+  CUDA_TRY(cudaSetDevice(h->device));
+  DevBlock& B = h->hdom.blk[0];
+  const long long S = a->stride();
+  const int N = a->N;
+  const size_t plane_bytes = (size_t)B.plane * sizeof(double);
+  for (int q = 0; q < 2; ++q) {
+    CUDA_TRY(cudaMemsetAsync(a->ub[q], 0, S * sizeof(double), h->stream));
+    CUDA_TRY(cudaMemsetAsync(a->qp[q], 0, S * sizeof(double), h->stream));
+  }
+  CUDA_TRY(cudaMemsetAsync(a->grho, 0, plane_bytes, h->stream));
+  CUDA_TRY(cudaMemsetAsync(a->gG, 0, plane_bytes, h->stream));
+  // dJ/dU^N at the receivers
+  AdjClock ck{0, N};
+  CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
+  adj_inject<<<1, 32, 0, h->stream>>>(a->ub[0], a->rec, a->nrec, a->resid, a->clock, 0);
+  CUDA_TRY(cudaGetLastError());
+  int p = 0;  // ubar parity
+  const int nseg = (N - 1 + a->K - 1) / a->K;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int n0 = seg * a->K + 1, n1 = std::min(n0 + a->K, N);  // steps n0 .. n1-1
+    h->cur = 0;
+    CUDA_TRY(cudaMemcpyAsync(B.F[0], a->ckpt + (size_t)seg * S, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, a->t_start, a->dt, n0);
+    ck.rel = 0;
+    ck.n = N;  // unused while recomputing
+    CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
+    for (int n = n0; n < n1; ++n) {
+      CUDA_TRY(cudaGraphLaunch(a->g_rec[h->cur], h->stream));
+      if (h->rk.nstage & 1) h->cur = 1 - h->cur;
+    }
+    ck.rel = n1 - 1 - n0;
+    ck.n = n1 - 1;
+    CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
+    for (int n = n1 - 1; n >= n0; --n) {
+      CUDA_TRY(cudaGraphLaunch(a->g_adj[p], h->stream));
+      if (h->rk.nstage & 1) p = 1 - p;
+    }
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  int rc;
+  if (grad_rho && (rc = from_block(a, grad_rho, a->grho))) return rc;
+  if (grad_G && (rc = from_block(a, grad_G, a->gG))) return rc;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_adjoint_fields(fdmap_adjoint* a, double* F) {
+  if (!a) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint");
+  return fdmap_gpu_get_fields(a->h, F, nullptr);
+}
+
+void fdmap_gpu_adjoint_destroy(fdmap_adjoint* a) { delete a; }
+
+}  // extern "C"

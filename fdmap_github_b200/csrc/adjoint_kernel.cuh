@@ -1,0 +1,379 @@
+// Discrete adjoint of one low-storage RK stage of the mode III heterogeneous
+// SBP-SAT update (rates_h_interior_mode3 / rates_h_boundary_mode3,
+// rates_heterogeneous.f90:8-372, with set_rates_SAT / set_bc_mode3,
+// time_step.f90:754-851, boundaries.f90:155-235).
+//
+// Forward stage s (forward numbering, u = fields, q = rate register):
+//   q_s = A_s q_{s-1} + R(u_{s-1}, t_s),   u_s = u_{s-1} + B_s dt q_s,
+// with R(u) = L(rho, G) u + f(t) linear in u.  Its adjoint, run for
+// s = nstage..1 with qbar' = A_{s+1} qbar_{s+1} carried between stages:
+//   qs   = qbar' + B_s dt ubar            (adjoint of the update)
+//   ubar = ubar + L^T qs                  (adjoint of the rates)
+//   grad += (dR/dm)(u_{s-1})^T qs         (material gradient, rho and G)
+//   qbar' = A_s qs
+//
+// L^T is applied as a gather: input node (i, j) collects, from every output
+// node whose stencil holds it, that node's weight times its adjoint rate.  An
+// output node's q-direction stencil depends only on its column (one-sided DL
+// rows within nbst of the left/right side, DR = -reverse(DL) on the right,
+// central DI elsewhere) and its r-direction stencil only on its row, so the
+// candidate output nodes of an input node are enumerated per direction.
+#pragma once
+
+#include "stencil_kernel.cuh"
+
+namespace fdmap {
+
+struct AdjStage {
+  double A, Bdt;                  // RK A(s), B(s)*dt of the forward stage
+  int s, nstage;                  // forward stage index (0-based), stages per step
+  const double* ub_in;            // ubar (3 planes, block layout)
+  const double* qp_in;            // qbar' carried from the later stage
+  double* ub_out;
+  double* qp_out;
+  const double* store;            // forward stage inputs u_{s-1}: store + (rel*nstage + s)*stride
+  long long stride;
+  const long long* rel;           // device: step index within the recomputed segment
+  double* grho;                   // dJ/drho, dJ/dG (1 plane each), accumulated
+  double* gG;
+};
+
+// material-free volume rates phi_r(c) = Ji(c) * sum of stencil terms, so that
+// R_0 = phi_0 / rho(c) and R_{1,2} = G(c) * phi_{1,2} (rates_heterogeneous.f90:8-48 and closures)
+template <int PI_>
+__device__ __forceinline__ void phi_volume(const DevDomain& D, const DevBlock& B, const double* __restrict__ u, int i,
+                                           int j, double* phi) {
+  constexpr int nbnd = nbnd_of(PI_);
+  const int nx = B.nx, ny = B.ny, nbst = D.nbst;
+  const long long pitch = B.pitch, plane = B.plane;
+  const long long c = (long long)j * pitch + i;
+  const double yrc = B.yr[c], xrc = B.xr[c], yqc = B.yq[c], xqc = B.xq[c];
+  phi[0] = phi[1] = phi[2] = 0.0;
+  auto qterm = [&](long long k, double W) {
+    const double Y = 0.5 * (B.yr[k] + yrc), X = 0.5 * (B.xr[k] + xrc);
+    const double f0 = u[k], f1 = u[plane + k], f2 = u[2 * plane + k];
+    phi[0] += W * (Y * f1 - X * f2);
+    phi[1] += W * (Y * f0);
+    phi[2] += W * (-X * f0);
+  };
+  auto rterm = [&](long long k, double W) {
+    const double Y = 0.5 * (B.yq[k] + yqc), X = 0.5 * (B.xq[k] + xqc);
+    const double f0 = u[k], f1 = u[plane + k], f2 = u[2 * plane + k];
+    phi[0] += W * (-Y * f1 + X * f2);
+    phi[1] += W * (-Y * f0);
+    phi[2] += W * (X * f0);
+  };
+  if (i < nbst) {
+#pragma unroll
+    for (int s = 0; s < nbnd; ++s) qterm((long long)j * pitch + s, D.DL[i][s]);
+  } else if (i > nx - 1 - nbst) {
+#pragma unroll
+    for (int s = 0; s < nbnd; ++s) qterm((long long)j * pitch + (nx - 1 - s), -D.DL[nx - 1 - i][s]);
+  } else {
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) { qterm(c + s, D.DI[s]); qterm(c - s, -D.DI[s]); }
+  }
+  if (j < nbst) {
+#pragma unroll
+    for (int s = 0; s < nbnd; ++s) rterm((long long)s * pitch + i, D.DL[j][s]);
+  } else if (j > ny - 1 - nbst) {
+#pragma unroll
+    for (int s = 0; s < nbnd; ++s) rterm((long long)(ny - 1 - s) * pitch + i, -D.DL[ny - 1 - j][s]);
+  } else {
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) { rterm(c + s * pitch, D.DI[s]); rterm(c - s * pitch, -D.DI[s]); }
+  }
+  const double Ji = B.Ji[c];
+  phi[0] *= Ji; phi[1] *= Ji; phi[2] *= Ji;
+}
+
+// SAT of one outer side at an edge node in mode III (set_bc_mode3 + SAT_term):
+//   r0 = vz - vz0,  r2 = n0 (sxz - sxz0) + n1 (syz - syz0),
+//   e = E(Zs) (r0, r2),   DF += Ks * (e0, n0 e2, n1 e2).
+// E (absorbing) = -1/2 [[1, 1/Zs], [Zs, 1]], (free) [[0, -1/Zs], [0, -1]],
+// (rigid) [[-1, 0], [-Zs, 0]].  Adds the transposed action on lam to ubar and
+// the derivatives through Zs = rho*cs, Ks = cs*geo (cs = sqrt(G/rho)) to the gradient.
+__device__ __forceinline__ void sat_adjoint(int bc, double Zs, double Ks, double n0, double n1, const double* lam,
+                                            const double* ust, const double* F0, double rho, double G, double* ub,
+                                            double* grho, double* gG) {
+  const double a0 = Ks * lam[0], a2 = Ks * (n0 * lam[1] + n1 * lam[2]);
+  const double r0 = ust[0] - F0[0], r2 = n0 * (ust[1] - F0[1]) + n1 * (ust[2] - F0[2]);
+  double p0, p2, e0, e2, de0, de2;  // E^T a;  E r;  dE/dZs r
+  if (bc == FDMAP_BC_ABSORBING) {
+    p0 = -0.5 * a0 - 0.5 * Zs * a2;
+    p2 = -0.5 * a0 / Zs - 0.5 * a2;
+    e0 = -0.5 * r0 - 0.5 * r2 / Zs;
+    e2 = -0.5 * Zs * r0 - 0.5 * r2;
+    de0 = 0.5 * r2 / (Zs * Zs);
+    de2 = -0.5 * r0;
+  } else if (bc == FDMAP_BC_FREE) {
+    p0 = 0.0;
+    p2 = -a0 / Zs - a2;
+    e0 = -r2 / Zs;
+    e2 = -r2;
+    de0 = r2 / (Zs * Zs);
+    de2 = 0.0;
+  } else {  // rigid
+    p0 = -a0 - Zs * a2;
+    p2 = 0.0;
+    e0 = -r0;
+    e2 = -Zs * r0;
+    de0 = 0.0;
+    de2 = -r0;
+  }
+  ub[0] += p0;
+  ub[1] += n0 * p2;
+  ub[2] += n1 * p2;
+  const double lt = n0 * lam[1] + n1 * lam[2];
+  const double gK = lam[0] * e0 + lt * e2;          // d/dKs of lam . SAT
+  const double gZ = Ks * (lam[0] * de0 + lt * de2);  // d/dZs
+  // Zs = sqrt(rho G), Ks = geo sqrt(G / rho)
+  *grho += 0.5 * (gZ * Zs - gK * Ks) / rho;
+  *gG += 0.5 * (gZ * Zs + gK * Ks) / G;
+}
+
+// One node of the adjoint stage through the cache hierarchy: every node, any
+// position (closures, corners, sides).
+template <int PI_>
+__device__ __forceinline__ void adj_node_generic(const DevDomain& D, const AdjStage& p, int i, int j) {
+  constexpr int nbnd = nbnd_of(PI_);
+  const DevBlock& B = D.blk[0];
+  const int nx = B.nx, ny = B.ny, nbst = D.nbst;
+  const long long pitch = B.pitch, plane = B.plane;
+  const long long c = (long long)j * pitch + i;
+  const double* __restrict__ ub = p.ub_in;
+  const double* __restrict__ qp = p.qp_in;
+  auto qs = [&](long long k, int f) { return qp[f * plane + k] + p.Bdt * ub[f * plane + k]; };
+
+  double acc[3] = {0.0, 0.0, 0.0};
+  const double yrc = B.yr[c], xrc = B.xr[c], yqc = B.yq[c], xqc = B.xq[c];
+  // output node k (same row) whose q-stencil weights this node by W
+  auto gather_q = [&](int ic, double W) {
+    const long long k = (long long)j * pitch + ic;
+    const double Y = 0.5 * (B.yr[k] + yrc), X = 0.5 * (B.xr[k] + xrc);
+    const double wj = W * B.Ji[k], g = B.G[k];
+    const double l0 = qs(k, 0) * (wj / B.rho[k]), l1 = qs(k, 1) * (wj * g), l2 = qs(k, 2) * (wj * g);
+    acc[1] += Y * l0;
+    acc[2] -= X * l0;
+    acc[0] += Y * l1 - X * l2;
+  };
+  auto gather_r = [&](int jc, double W) {
+    const long long k = (long long)jc * pitch + i;
+    const double Y = 0.5 * (B.yq[k] + yqc), X = 0.5 * (B.xq[k] + xqc);
+    const double wj = W * B.Ji[k], g = B.G[k];
+    const double l0 = qs(k, 0) * (wj / B.rho[k]), l1 = qs(k, 1) * (wj * g), l2 = qs(k, 2) * (wj * g);
+    acc[1] -= Y * l0;
+    acc[2] += X * l0;
+    acc[0] += -Y * l1 + X * l2;
+  };
+#pragma unroll
+  for (int s = 1; s <= PI_; ++s) {
+    const int a = i - s, b = i + s;  // output columns with this node at +s / -s
+    if (a >= nbst && a <= nx - 1 - nbst) gather_q(a, D.DI[s]);
+    if (b >= nbst && b <= nx - 1 - nbst) gather_q(b, -D.DI[s]);
+    const int ar = j - s, br = j + s;
+    if (ar >= nbst && ar <= ny - 1 - nbst) gather_r(ar, D.DI[s]);
+    if (br >= nbst && br <= ny - 1 - nbst) gather_r(br, -D.DI[s]);
+  }
+  if (i < nbnd)
+    for (int ic = 0; ic < nbst; ++ic) gather_q(ic, D.DL[ic][i]);
+  if (nx - 1 - i < nbnd)
+    for (int ic = nx - nbst; ic < nx; ++ic) gather_q(ic, -D.DL[nx - 1 - ic][nx - 1 - i]);
+  if (j < nbnd)
+    for (int jc = 0; jc < nbst; ++jc) gather_r(jc, D.DL[jc][j]);
+  if (ny - 1 - j < nbnd)
+    for (int jc = ny - nbst; jc < ny; ++jc) gather_r(jc, -D.DL[ny - 1 - jc][ny - 1 - j]);
+
+  // adjoint rates and stage input of this node
+  const double lam[3] = {qs(c, 0), qs(c, 1), qs(c, 2)};
+  const double* __restrict__ ust = p.store + ((*p.rel) * p.nstage + p.s) * p.stride;
+  const double rho = B.rho[c], G = B.G[c];
+  double grho = 0.0, gG = 0.0;
+  // SAT of the outer sides through this node, in the forward's side order
+  auto side = [&](int sd, int k) {
+    const DevSide& S = B.side[sd];
+    const double us[3] = {ust[c], ust[plane + c], ust[2 * plane + c]};
+    const double F0[3] = {S.F0[k], S.F0[k + S.n], S.F0[k + 2 * S.n]};
+    sat_adjoint(S.bc, S.M[k], S.M[k + 3 * S.n], S.nrm[k], S.nrm[k + S.n], lam, us, F0, rho, G, acc, &grho, &gG);
+  };
+  if (i == 0) side(0, j);
+  if (i == nx - 1) side(1, j);
+  if (j == 0) side(2, i);
+  if (j == ny - 1) side(3, i);
+
+  // volume part of dR/dm at this node
+  double phi[3];
+  phi_volume<PI_>(D, B, ust, i, j, phi);
+  const double rinv = 1.0 / rho;
+  grho -= lam[0] * phi[0] * (rinv * rinv);
+  gG += lam[1] * phi[1] + lam[2] * phi[2];
+  p.grho[c] += grho;
+  p.gG[c] += gG;
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    p.ub_out[f * plane + c] = ub[f * plane + c] + acc[f];
+    p.qp_out[f * plane + c] = p.A * lam[f];
+  }
+}
+
+constexpr int ATX = 32, ATY = 8;
+
+// Adjoint stage, 32 x 8 nodes per CTA.  Tiles whose nodes are all at least
+// nbnd from every side (so every output node they gather from, and their own
+// volume rates, use the central stencil) stage the weighted adjoint rates
+// l_r = qs_r * Ji * (1/rho | G), the metrics and the stage input in shared
+// memory with a PI_-wide halo; adj_edge_kernel takes the other tiles.
+// tiles whose nodes are all at least nbnd from every side
+__device__ __forceinline__ bool adj_tile_interior(int i0, int j0, int nx, int ny, int nbnd) {
+  return i0 >= nbnd && i0 + ATX - 1 <= nx - 1 - nbnd && j0 >= nbnd && j0 + ATY - 1 <= ny - 1 - nbnd;
+}
+
+// the other tiles (closures, sides, corners): generic per-node path
+template <int PI_>
+__global__ void __launch_bounds__(ATX* ATY) adj_edge_kernel(const __grid_constant__ DevDomain D, AdjStage p) {
+  const DevBlock& B = D.blk[0];
+  const int i0 = blockIdx.x * ATX, j0 = blockIdx.y * ATY;
+  if (adj_tile_interior(i0, j0, B.nx, B.ny, nbnd_of(PI_))) return;
+  const int i = i0 + threadIdx.x % ATX, j = j0 + threadIdx.x / ATX;
+  if (i < B.nx && j < B.ny) adj_node_generic<PI_>(D, p, i, j);
+}
+
+template <int PI_>
+__global__ void __launch_bounds__(ATX* ATY, 4) adj_stage_kernel(const __grid_constant__ DevDomain D, AdjStage p) {
+  constexpr int H = PI_, WX = ATX + 2 * H, WY = ATY + 2 * H;
+  __shared__ double sL[3][WY][WX];  // weighted adjoint rates
+  __shared__ double sM[4][WY][WX];  // yr, xr, yq, xq
+  __shared__ double sU[3][WY][WX];  // stage input u_{s-1}
+  const DevBlock& B = D.blk[0];
+  const int i0 = blockIdx.x * ATX, j0 = blockIdx.y * ATY;
+  const int tx = threadIdx.x % ATX, ty = threadIdx.x / ATX;
+  if (!adj_tile_interior(i0, j0, B.nx, B.ny, nbnd_of(PI_))) return;  // adj_edge_kernel's tile
+  const long long pitch = B.pitch, plane = B.plane;
+  const double* __restrict__ ust = p.store + ((*p.rel) * p.nstage + p.s) * p.stride;
+  for (int q = threadIdx.x; q < WX * WY; q += ATX * ATY) {
+    const int yy = q / WX, xx = q % WX;
+    const long long k = (long long)(j0 - H + yy) * pitch + (i0 - H + xx);  // inside the block: the tile is interior
+    const double Jk = B.Ji[k], wv = Jk / B.rho[k], ws = Jk * B.G[k];
+    sL[0][yy][xx] = (p.qp_in[k] + p.Bdt * p.ub_in[k]) * wv;
+    sL[1][yy][xx] = (p.qp_in[plane + k] + p.Bdt * p.ub_in[plane + k]) * ws;
+    sL[2][yy][xx] = (p.qp_in[2 * plane + k] + p.Bdt * p.ub_in[2 * plane + k]) * ws;
+    sM[0][yy][xx] = B.yr[k];
+    sM[1][yy][xx] = B.xr[k];
+    sM[2][yy][xx] = B.yq[k];
+    sM[3][yy][xx] = B.xq[k];
+    sU[0][yy][xx] = ust[k];
+    sU[1][yy][xx] = ust[plane + k];
+    sU[2][yy][xx] = ust[2 * plane + k];
+  }
+  __syncthreads();
+  const int X0 = tx + H, Y0 = ty + H;
+  const double yrc = sM[0][Y0][X0], xrc = sM[1][Y0][X0], yqc = sM[2][Y0][X0], xqc = sM[3][Y0][X0];
+  double acc[3] = {0.0, 0.0, 0.0};
+  double phi[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int s = 1; s <= PI_; ++s) {
+    const double w = D.DI[s];
+#pragma unroll
+    for (int side = -1; side <= 1; side += 2) {
+      // q direction: output node X0 + side*s; this node sits at -side*s in its stencil
+      const int xa = X0 + side * s;
+      const double W = -side * w;  // left output (side -1): +DI, right output: -DI
+      const double Y = 0.5 * (sM[0][Y0][xa] + yrc), X = 0.5 * (sM[1][Y0][xa] + xrc);
+      const double l0 = sL[0][Y0][xa], l1 = sL[1][Y0][xa], l2 = sL[2][Y0][xa];
+      acc[1] += W * (Y * l0);
+      acc[2] -= W * (X * l0);
+      acc[0] += W * (Y * l1 - X * l2);
+      // own volume rate: neighbour at side*s with weight side*DI
+      const double u0 = sU[0][Y0][xa], u1 = sU[1][Y0][xa], u2 = sU[2][Y0][xa];
+      const double Wf = side * w;
+      phi[0] += Wf * (Y * u1 - X * u2);
+      phi[1] += Wf * (Y * u0);
+      phi[2] += Wf * (-X * u0);
+      // r direction
+      const int ya = Y0 + side * s;
+      const double Yr = 0.5 * (sM[2][ya][X0] + yqc), Xr = 0.5 * (sM[3][ya][X0] + xqc);
+      const double m0 = sL[0][ya][X0], m1 = sL[1][ya][X0], m2 = sL[2][ya][X0];
+      acc[1] -= W * (Yr * m0);
+      acc[2] += W * (Xr * m0);
+      acc[0] += W * (-Yr * m1 + Xr * m2);
+      const double v0 = sU[0][ya][X0], v1 = sU[1][ya][X0], v2 = sU[2][ya][X0];
+      phi[0] += Wf * (-Yr * v1 + Xr * v2);
+      phi[1] += Wf * (-Yr * v0);
+      phi[2] += Wf * (Xr * v0);
+    }
+  }
+  const int i = i0 + tx, j = j0 + ty;
+  const long long c = (long long)j * pitch + i;
+  double lam[3], ubc[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    ubc[f] = p.ub_in[f * plane + c];
+    lam[f] = p.qp_in[f * plane + c] + p.Bdt * ubc[f];
+  }
+  const double Ji = B.Ji[c], rinv = 1.0 / B.rho[c];
+  p.grho[c] += -lam[0] * (phi[0] * Ji) * (rinv * rinv);
+  p.gG[c] += lam[1] * (phi[1] * Ji) + lam[2] * (phi[2] * Ji);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    p.ub_out[f * plane + c] = ubc[f] + acc[f];
+    p.qp_out[f * plane + c] = p.A * lam[f];
+  }
+}
+
+// Edge impedance and penalty of a heterogeneous mode III side from the node's
+// (rho, G): Zs = rho*cs, Ks = cs*geo with cs = sqrt(G/rho) (init_edges,
+// domain.f90:1349-1459, with the material given as rho and G)
+__global__ void adj_edge_material(DevSide S, const double* __restrict__ rho, const double* __restrict__ G,
+                                  const double* __restrict__ geo, int side, int nx, int ny, long long pitch) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= S.n) return;
+  int i, j;
+  side_node_local(side, k, nx, ny, i, j);
+  const long long c = (long long)j * pitch + i;
+  const double cs = sqrt(G[c] / rho[c]);
+  S.M[k] = rho[c] * cs;
+  S.M[k + 3 * S.n] = cs * geo[k];
+}
+
+// vz at the receivers of state u for sample n = ts->n (1-based)
+__global__ void adj_sample(const double* __restrict__ u, const long long* __restrict__ rec, int nrec,
+                           const TimeState* ts, double* traces, int nsamples) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long n = ts->n;
+  if (r >= nrec || n < 1 || n > nsamples) return;
+  traces[(n - 1) * nrec + r] = u[rec[r]];
+}
+
+// stage input u_{s-1} -> stage store slot (rel*nstage + s)
+__global__ void adj_stash(const double* __restrict__ u, double* store, long long stride, const long long* rel, int s,
+                          int nstage, long long count) {
+  double* dst = store + ((*rel) * nstage + s) * stride;
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < count; k += (long long)gridDim.x * blockDim.x)
+    dst[k] = u[k];
+}
+
+struct AdjClock {
+  long long rel;   // step within the current segment
+  long long n;     // global step whose adjoint runs next (backward) / sample index
+};
+
+// end of a recomputed step: advance the forward clock and the segment index
+__global__ void adj_forward_advance(TimeState* ts, AdjClock* ck) {
+  ts->n += 1;
+  ck->rel += 1;
+}
+
+// end of an adjoint step n: ubar += dJ/dU^n at the receivers, then step back
+__global__ void adj_inject(double* ub, const long long* __restrict__ rec, int nrec, const double* __restrict__ resid,
+                           AdjClock* ck, int back) {
+  if (threadIdx.x != 0) return;
+  const long long n = ck->n;
+  // serial: two receivers may share a node
+  for (int r = 0; r < nrec; ++r) ub[rec[r]] += resid[(n - 1) * nrec + r];
+  if (back) {
+    ck->n -= 1;
+    ck->rel -= 1;
+  }
+}
+
+}  // namespace fdmap

@@ -33,7 +33,7 @@ __device__ __forceinline__ double d_boxcar(double r, double w, double fin, doubl
 }
 
 // load_stress default branch + load_ramp (friction.f90:1317-1374, 1455-1484)
-__device__ void d_load_stress(const DevFriction& FR, int n, int k, double x, double y, double t, double& S0,
+static __device__ void d_load_stress(const DevFriction& FR, int n, int k, double x, double y, double t, double& S0,
                               double& N0) {
   double xx = x * FR.cos_angle + y * FR.sin_angle;
   double r = fabs((xx - FR.ld_x0) / FR.ld_R);
@@ -90,7 +90,7 @@ __device__ __forceinline__ void d_strength(int law, const DRS& rs, double V, dou
 
 // newton_solver (friction.f90:909-1038): bracketed Newton with log-bisection.
 // Returns true on failure (imax iterations without meeting atolR).
-__device__ bool d_newton(int law, const DRS& rs, double& V, double& S, double Slock, double N, double eta, double Psi) {
+static __device__ bool d_newton(int law, const DRS& rs, double& V, double& S, double Slock, double N, double eta, double Psi) {
   const int imax = 99;
   const double atolR = 2.220446049250313e-16 * 1e4;
   double Vmin = fmin(0.0, Slock / eta);
@@ -132,7 +132,7 @@ __device__ __forceinline__ double pow8(double x) {
 }
 
 // state_rate (friction.f90:1147-1264)
-__device__ double d_state_rate(int law, const DRS& rs, double V, double Psi) {
+static __device__ double d_state_rate(int law, const DRS& rs, double V, double Psi) {
   if (law == FDMAP_FR_FRICTIONLESS || law == FDMAP_FR_SW || law == FDMAP_FR_LOCKED) return 0.0;
   if (V == 0.0) return 0.0;
   double absV = fabs(V);
@@ -174,7 +174,7 @@ struct NodeState {
   double V, O, S, N, S0, N0, Nreg, D, Psi;
 };
 
-__device__ void d_solve_friction(const DevFriction& FR, int n, int k, NodeState& st, double S0, double N0, double phip,
+static __device__ void d_solve_friction(const DevFriction& FR, int n, int k, NodeState& st, double S0, double N0, double phip,
                                  double phis, double eta, double x, double y, double t, double dt,
                                  unsigned long long* status) {
   d_load_stress(FR, n, k, x, y, t, st.S0, st.N0);

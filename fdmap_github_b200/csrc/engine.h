@@ -175,6 +175,9 @@ struct BatchPlan {
   int closure_ctas, closure_tpb;
   int edge_ctas, edge_tpb;
 };
+// One RK stage of a single domain (boundary + interior kernels) on h->stream.
+int engine_stage(fdmap_gpu* h, const StageArgs& a);
+
 int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 int batch_closure(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 int batch_edges(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);

@@ -190,6 +190,8 @@ int march_dispatch(fdmap_gpu* h, const StageArgs* a) {
   return h->het ? go(std::integral_constant<int, 3>{}, std::true_type{}) : go(std::integral_constant<int, 3>{}, std::false_type{});
 }
 
+int launch_stage(fdmap_gpu* h, const StageArgs& a);
+
 // (mode, SBP half-width, heterogeneity) of a handle as compile-time constants
 template <typename Fn>
 int dispatch_variant(const fdmap_gpu* h, Fn&& fn) {
@@ -204,6 +206,8 @@ int dispatch_variant(const fdmap_gpu* h, Fn&& fn) {
 }  // namespace
 
 namespace fdmap {
+
+int engine_stage(fdmap_gpu* h, const StageArgs& a) { return launch_stage(h, a); }
 
 int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s) {
   return dispatch_variant(proto, [&](auto mode_c, auto pi_c, auto het_c) {

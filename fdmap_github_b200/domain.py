@@ -232,3 +232,64 @@ class GpuEnsemble:
             self.close()
         except Exception:
             pass
+
+
+class GpuAdjoint:
+    """Forward/backward pair (fdmap_gpu_adjoint_*): receiver misfit of a
+    heterogeneous mode III block and its gradient with respect to the density
+    and shear-modulus fields, by the discrete adjoint with checkpoints."""
+
+    def __init__(self, host: HostDomain, receivers, checkpoint_every: int = 45, device: int = 0):
+        self.host = host
+        rec = np.asarray(receivers, dtype=np.int32).reshape(-1, 2)  # 1-based (i, j)
+        self.nrec = rec.shape[0]
+        ri = np.ascontiguousarray(rec[:, 0])
+        rj = np.ascontiguousarray(rec[:, 1])
+        self._a = C.c_void_p()
+        ip = C.POINTER(C.c_int)
+        check_gpu(lib().fdmap_gpu_adjoint_create(host.desc, device, self.nrec, ri.ctypes.data_as(ip),
+                                                 rj.ctypes.data_as(ip), checkpoint_every, C.byref(self._a)),
+                  "fdmap_gpu_adjoint_create")
+
+    def set_material(self, rho: np.ndarray, G: np.ndarray) -> None:
+        r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)
+        g = np.ascontiguousarray(G, dtype=np.float64).reshape(-1)
+        check_gpu(lib().fdmap_gpu_adjoint_set_material(self._a, dptr(r), dptr(g)), "fdmap_gpu_adjoint_set_material")
+
+    def forward(self, nt: int | None = None, data: np.ndarray | None = None, dt: float | None = None,
+                t_start: float | None = None):
+        """Returns (traces[nt, nrec], misfit or None)."""
+        h = self.host
+        nt = h.nt if nt is None else nt
+        tr = np.empty((nt, self.nrec))
+        J = C.c_double(0.0)
+        d = None if data is None else np.ascontiguousarray(data, dtype=np.float64)
+        check_gpu(lib().fdmap_gpu_adjoint_forward(self._a, h.t0 if t_start is None else t_start,
+                                                  h.dt if dt is None else dt, nt, dptr(d), dptr(tr), C.byref(J)),
+                  "fdmap_gpu_adjoint_forward")
+        return tr, (J.value if d is not None else None)
+
+    def backward(self):
+        """Returns (dJ/drho, dJ/dG), each shaped (ny, nx)."""
+        h = self.host
+        gr = np.empty((h.ny, h.nx))
+        gg = np.empty((h.ny, h.nx))
+        check_gpu(lib().fdmap_gpu_adjoint_backward(self._a, dptr(gr), dptr(gg)), "fdmap_gpu_adjoint_backward")
+        return gr, gg
+
+    def fields(self) -> np.ndarray:
+        h = self.host
+        F = np.empty((h.nF, h.ny, h.nx))
+        check_gpu(lib().fdmap_gpu_adjoint_fields(self._a, dptr(F)), "fdmap_gpu_adjoint_fields")
+        return F
+
+    def close(self) -> None:
+        if self._a:
+            lib().fdmap_gpu_adjoint_destroy(self._a)
+            self._a = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -73,6 +73,14 @@ SIGNATURES = {
     "fdmap_gpu_ensemble_tune": (C.c_int, [_VP, C.c_double, C.c_int, C.POINTER(C.c_int), _DP]),
     "fdmap_gpu_ensemble_launch_count": (C.c_longlong, [_VP]),
     "fdmap_gpu_ensemble_destroy": (None, [_VP]),
+    # fdmap_gpu.h: forward/backward pair
+    "fdmap_gpu_adjoint_create": (C.c_int, [_VP, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int,
+                                           C.POINTER(_VP)]),
+    "fdmap_gpu_adjoint_set_material": (C.c_int, [_VP, _DP, _DP]),
+    "fdmap_gpu_adjoint_forward": (C.c_int, [_VP, C.c_double, C.c_double, C.c_int, _DP, _DP, _DP]),
+    "fdmap_gpu_adjoint_backward": (C.c_int, [_VP, _DP, _DP]),
+    "fdmap_gpu_adjoint_fields": (C.c_int, [_VP, _DP]),
+    "fdmap_gpu_adjoint_destroy": (None, [_VP]),
 }
 
 _lib = None

@@ -128,6 +128,45 @@ int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_s
 long long fdmap_gpu_ensemble_launch_count(fdmap_ensemble* e);
 void fdmap_gpu_ensemble_destroy(fdmap_ensemble* e);
 
+/* ------------------------------------------------------------------------
+ * Forward/backward pair: gradient of the receiver misfit
+ *   J = 1/2 sum_{n=1..nt} sum_r (vz(x_r, t_n) - data[n-1][r])^2
+ * (vz sampled at every step start, where the reference writes its output,
+ * time_step.f90:129) with respect to the density rho(x) and shear modulus
+ * G(x) of one heterogeneous mode III block with absorbing / free / rigid
+ * sides and no interfaces.  The forward pass is fdmap_gpu_time_step itself;
+ * the backward pass is the discrete adjoint of those LS-RK stages
+ * (SBP-SAT rates and the edge impedances Zs = rho*cs, Ks = cs*H00i*|grad|/J
+ * with cs = sqrt(G/rho)), with the fields checkpointed every
+ * `checkpoint_every` steps and each segment recomputed once.  The reference
+ * has no adjoint; there is no routine this replaces.
+ * ---------------------------------------------------------------------- */
+typedef struct fdmap_adjoint fdmap_adjoint;
+
+/* rec_i, rec_j: 1-based global node indices of the nrec receivers. */
+int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const int* rec_i, const int* rec_j,
+                             int checkpoint_every, fdmap_adjoint** a);
+
+/* Replace the material by rho(nx,ny), G(nx,ny) (global layout); the edge
+ * impedances follow.  The point source keeps the block density, as in
+ * set_source (source.f90:147-252). */
+int fdmap_gpu_adjoint_set_material(fdmap_adjoint* a, const double* rho, const double* G);
+
+/* Steps 1..nt-1 from the initial state given at creation.  traces (nt*nrec,
+ * sample-major) receives vz at the receivers; with data (nt*nrec) the misfit
+ * is returned and the residuals are kept for fdmap_gpu_adjoint_backward.
+ * Either pointer may be NULL. */
+int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int nt, const double* data, double* traces,
+                              double* misfit);
+
+/* dJ/drho and dJ/dG in the global (nx,ny) layout (either may be NULL). */
+int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_G);
+
+/* Body fields F(nx,ny,3) after the last forward pass. */
+int fdmap_gpu_adjoint_fields(fdmap_adjoint* a, double* F);
+
+void fdmap_gpu_adjoint_destroy(fdmap_adjoint* a);
+
 #ifdef __cplusplus
 }
 #endif
