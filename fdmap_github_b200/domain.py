@@ -134,6 +134,13 @@ class GpuDomain:
         check_gpu(lib().fdmap_gpu_get_fhat(self._g, b, s, dptr(out)), "fdmap_gpu_get_fhat")
         return out.reshape(self.nF, n)
 
+    def fault_max_noalloc(self, iface: int, field: str) -> float:
+        """max |field| along interface `iface`, reduced on the device without allocating."""
+        out = C.c_double()
+        check_gpu(lib().fdmap_gpu_fault_max_noalloc(self._g, iface, FAULT_INDEX[field], C.byref(out)),
+                  "fdmap_gpu_fault_max_noalloc")
+        return out.value
+
     def newton_failures(self) -> int:
         n = C.c_longlong()
         lib().fdmap_gpu_status(self._g, C.byref(n))

@@ -56,6 +56,7 @@ SIGNATURES = {
     "fdmap_gpu_set_fault": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_get_fhat": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_status": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_fault_max_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_launch_count": (C.c_longlong, [_VP]),
     "fdmap_gpu_device_bytes": (C.c_longlong, [_VP]),
     "fdmap_gpu_destroy": (None, [_VP]),

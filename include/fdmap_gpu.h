@@ -74,6 +74,16 @@ int fdmap_gpu_get_fhat(fdmap_gpu* h, int b, int s, double* out);
 /* Device status: Newton failures so far (the reference stops on the first). */
 int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
 
+/* max |field| over the nodes of interface `iface` (a friction interface),
+ * reduced on the device into *out.  No counterpart in the reference (its
+ * drivers scan the Fortran arrays).  Allocates nothing during the call: for
+ * drivers that check the fault every step and cannot allocate inside their
+ * time loop.  Its scratch is a static device array shared by all handles of a
+ * device, so calls on one device must not overlap; faults longer than
+ * 1,048,576 nodes are rejected (FDMAP_ERR_UNSUPPORTED).  The first call on a
+ * device looks up that scratch and should come before any stream capture. */
+int fdmap_gpu_fault_max_noalloc(fdmap_gpu* h, int iface, int field, double* out);
+
 /* Kernel launches issued by the last fdmap_gpu_run / time_step call. */
 long long fdmap_gpu_launch_count(fdmap_gpu* h);
 
