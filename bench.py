@@ -137,8 +137,8 @@ def measured_peaks() -> dict:
 
 
 def profiled_traffic(config_key: str):
-    """DRAM bytes per stencil launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "stencil_kernel_ncu.md"
+    """DRAM bytes per interior-kernel launch from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / "march_kernel_rupture_2x1601x801.md"
     if not p.exists():
         return None
     m = re.search(rf"traffic_bytes_per_launch\[{config_key}\]\s*=\s*([0-9.eE+]+)", p.read_text())
@@ -280,7 +280,7 @@ def run_gpu(args) -> None:
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload),
-                         "kernel": "stencil_kernel", "alg_bytes_per_launch": alg_bytes,
+                         "kernel": "march_kernel", "alg_bytes_per_launch": alg_bytes,
                          "mean_launch_ms": stencil_ms, "closure_kernel_mean_ms": closure_ms,
                          "interface_kernel_mean_ms": edge_ms,
                          "peak_source": peaks["source"]},

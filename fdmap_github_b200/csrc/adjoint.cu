@@ -37,6 +37,14 @@ struct fdmap_adjoint {
   double t_start = 0.0, dt = 0.0;
   std::vector<long long> rec_host;   // block-local linear node index of each receiver
   long long* rec = nullptr;
+  // distinct receiver nodes and the receivers on each (CSR), for the residual injection
+  int nnode = 0;
+  long long* node = nullptr;
+  int* rstart = nullptr;
+  int* rlist = nullptr;
+  long long nband = 0;                // nodes within nbnd of a side
+  cudaStream_t side = nullptr;        // band kernel beside the interior adjoint kernel
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   double* init_F = nullptr;          // initial fields (3 planes)
   double* init_DF = nullptr;
   double* ckpt = nullptr;            // checkpoints, 3 planes each
@@ -71,6 +79,9 @@ struct fdmap_adjoint {
     }
     free_graphs();
     for (void* p : mem) cudaFree(p);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (h) fdmap_gpu_destroy(h);
   }
   template <typename T>
@@ -92,22 +103,28 @@ struct fdmap_adjoint {
 
 namespace {
 
+// interior tiles on the main stream, the band on the side stream (disjoint
+// nodes, same inputs), joined before the next stage
 int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p) {
   fdmap_gpu* h = a->h;
   const DevBlock& B = h->hdom.blk[0];
   dim3 blk(ATX * ATY), grid((B.nx + ATX - 1) / ATX, (B.ny + ATY - 1) / ATY);
-  // interior tiles and edge tiles write disjoint nodes from the same inputs
+  const int bgrid = (int)((a->nband + 255) / 256);
+  CUDA_TRY(cudaEventRecord(a->ev_fork, h->stream));
+  CUDA_TRY(cudaStreamWaitEvent(a->side, a->ev_fork, 0));
   if (h->pI == 1) {
     adj_stage_kernel<1><<<grid, blk, 0, h->stream>>>(h->hdom, p);
-    adj_edge_kernel<1><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_band_kernel<1><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
   } else if (h->pI == 2) {
     adj_stage_kernel<2><<<grid, blk, 0, h->stream>>>(h->hdom, p);
-    adj_edge_kernel<2><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_band_kernel<2><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
   } else {
     adj_stage_kernel<3><<<grid, blk, 0, h->stream>>>(h->hdom, p);
-    adj_edge_kernel<3><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_band_kernel<3><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
   }
   CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaEventRecord(a->ev_join, a->side));
+  CUDA_TRY(cudaStreamWaitEvent(h->stream, a->ev_join, 0));
   return FDMAP_OK;
 }
 
@@ -161,10 +178,10 @@ int build_graphs(fdmap_adjoint* a, double dt) {
   for (int c = 0; c < 2 && rc == FDMAP_OK; ++c) {
     // forward step: sample vz at the receivers at the step start, then the stages
     rc = capture(a, &a->g_fwd[c], [&]() -> int {
-      adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[c], a->rec, a->nrec, h->d_time, a->traces, a->trace_alloc);
       int r = forward_step_stages(a, c, dt, false);
       if (r) return r;
-      advance_step<<<1, 1, 0, h->stream>>>(h->d_time);
+      const int last = (h->rk.nstage & 1) ? 1 - c : c;  // buffer holding the new state
+      adj_sample_advance<<<1, 128, 0, h->stream>>>(B.F[last], a->rec, a->nrec, h->d_time, a->traces, a->trace_alloc);
       return (int)FDMAP_OK;
     });
     if (rc) break;
@@ -198,7 +215,8 @@ int build_graphs(fdmap_adjoint* a, double dt) {
         if (r) return r;
         q = 1 - q;
       }
-      adj_inject<<<1, 32, 0, h->stream>>>(a->ub[q], a->rec, a->nrec, a->resid, a->clock, 1);
+      adj_inject<<<1, 128, 0, h->stream>>>(a->ub[q], a->node, a->rstart, a->rlist, a->nnode, a->nrec, a->resid,
+                                           a->clock, 1);
       return (int)FDMAP_OK;
     });
   }
@@ -279,6 +297,18 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
   a->K = checkpoint_every;
   a->nrec = nrec;
   const BlockGeom& g = h->geom[0];
+  const int nbnd = h->hdom.nbnd;
+  if (g.nx < 2 * nbnd + 1 || g.ny < 2 * nbnd + 1)
+    return fail(set_err(FDMAP_ERR_UNSUPPORTED, "block too small for the adjoint band decomposition"));
+  a->nband = 2LL * nbnd * g.nx + 2LL * nbnd * (g.ny - 2 * nbnd);
+  {
+    int lo = 0, hi = 0;
+    if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&a->side, cudaStreamNonBlocking, lo) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a->ev_join, cudaEventDisableTiming) != cudaSuccess)
+      return fail(set_err(FDMAP_ERR_CUDA, "adjoint stream setup"));
+  }
   for (int r = 0; r < nrec; ++r) {
     int i = rec_i[r] - g.mgx, j = rec_j[r] - g.mgy;
     if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) return fail(set_err(FDMAP_ERR_INVALID_ARG, "receiver outside the block"));
@@ -292,6 +322,29 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
     return fail(rc);
   if (cudaMemcpy(a->rec, a->rec_host.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(set_err(FDMAP_ERR_CUDA, "receiver upload"));
+  {
+    // distinct receiver nodes in first-appearance order, receivers listed per node
+    std::vector<long long> nodes;
+    std::vector<std::vector<int>> members;
+    for (int r = 0; r < nrec; ++r) {
+      auto it = std::find(nodes.begin(), nodes.end(), a->rec_host[r]);
+      if (it == nodes.end()) { nodes.push_back(a->rec_host[r]); members.push_back({r}); }
+      else members[it - nodes.begin()].push_back(r);
+    }
+    std::vector<int> rstart(1, 0), rlist;
+    for (auto& m : members) {
+      rlist.insert(rlist.end(), m.begin(), m.end());
+      rstart.push_back((int)rlist.size());
+    }
+    a->nnode = (int)nodes.size();
+    if ((rc = a->alloc(&a->node, nodes.size())) || (rc = a->alloc(&a->rstart, rstart.size())) ||
+        (rc = a->alloc(&a->rlist, rlist.size())))
+      return fail(rc);
+    if (cudaMemcpy(a->node, nodes.data(), nodes.size() * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(a->rstart, rstart.data(), rstart.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(a->rlist, rlist.data(), rlist.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(set_err(FDMAP_ERR_CUDA, "receiver upload"));
+  }
   const DevBlock& B = h->hdom.blk[0];
   if (cudaMemcpy(a->init_F, B.F[h->cur], S * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess ||
       cudaMemcpy(a->init_DF, B.DF, S * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess)
@@ -367,6 +420,8 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
   CUDA_TRY(cudaMemcpyAsync(B.F[0], a->init_F, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   CUDA_TRY(cudaMemcpyAsync(B.DF, a->init_DF, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, t_start, dt, 1);
+  // sample 1: the initial state; each replayed step samples the state it produces
+  adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[0], a->rec, a->nrec, h->d_time, a->traces, nt);
   CUDA_TRY(cudaGetLastError());
   for (int n = 1; n <= nt - 1; ++n) {
     if ((n - 1) % a->K == 0)
@@ -375,9 +430,6 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
     CUDA_TRY(cudaGraphLaunch(a->g_fwd[h->cur], h->stream));
     if (h->rk.nstage & 1) h->cur = 1 - h->cur;
   }
-  // last sample: the state the final step starts from (clock n == nt)
-  adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[h->cur], a->rec, a->nrec, h->d_time, a->traces, nt);
-  CUDA_TRY(cudaGetLastError());
   std::vector<double> tr((size_t)nt * a->nrec);
   CUDA_TRY(cudaMemcpyAsync(tr.data(), a->traces, tr.size() * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -414,7 +466,8 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
   // dJ/dU^N at the receivers
   AdjClock ck{0, N};
   CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
-  adj_inject<<<1, 32, 0, h->stream>>>(a->ub[0], a->rec, a->nrec, a->resid, a->clock, 0);
+  adj_inject<<<1, 128, 0, h->stream>>>(a->ub[0], a->node, a->rstart, a->rlist, a->nnode, a->nrec, a->resid, a->clock,
+                                       0);
   CUDA_TRY(cudaGetLastError());
   int p = 0;  // ubar parity
   const int nseg = (N - 1 + a->K - 1) / a->K;

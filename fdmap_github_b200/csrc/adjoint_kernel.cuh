@@ -218,24 +218,40 @@ __device__ __forceinline__ void adj_node_generic(const DevDomain& D, const AdjSt
 
 constexpr int ATX = 32, ATY = 8;
 
-// Adjoint stage, 32 x 8 nodes per CTA.  Tiles whose nodes are all at least
-// nbnd from every side (so every output node they gather from, and their own
-// volume rates, use the central stencil) stage the weighted adjoint rates
+// Adjoint stage, 32 x 8 nodes per CTA, for nodes at least nbnd from every side
+// (every output node they gather from, and their own volume rates, use the
+// central stencil).  The tile stages the weighted adjoint rates
 // l_r = qs_r * Ji * (1/rho | G), the metrics and the stage input in shared
-// memory with a PI_-wide halo; adj_edge_kernel takes the other tiles.
-// tiles whose nodes are all at least nbnd from every side
-__device__ __forceinline__ bool adj_tile_interior(int i0, int j0, int nx, int ny, int nbnd) {
-  return i0 >= nbnd && i0 + ATX - 1 <= nx - 1 - nbnd && j0 >= nbnd && j0 + ATY - 1 <= ny - 1 - nbnd;
+// memory with a PI_-wide halo.  Nodes within nbnd of a side (the band) are
+// left to adj_band_kernel, which runs concurrently on the same inputs.
+// nodes within nbnd of a side use closure rows somewhere in their gather or
+// their own rates: the band handled by adj_band_kernel
+__device__ __forceinline__ bool adj_node_interior(int i, int j, int nx, int ny, int nbnd) {
+  return i >= nbnd && i <= nx - 1 - nbnd && j >= nbnd && j <= ny - 1 - nbnd;
 }
 
-// the other tiles (closures, sides, corners): generic per-node path
+// band node q -> (i, j): nbnd full rows at the bottom, nbnd at the top, then
+// nbnd columns on the left and right of the rows between
+__device__ __forceinline__ void band_node(long long q, int nx, int ny, int nbnd, int& i, int& j) {
+  const long long rows = (long long)nbnd * nx;
+  if (q < rows) { j = (int)(q / nx); i = (int)(q % nx); return; }
+  q -= rows;
+  if (q < rows) { j = ny - nbnd + (int)(q / nx); i = (int)(q % nx); return; }
+  q -= rows;
+  const int k = (int)(q % (2 * nbnd));
+  j = nbnd + (int)(q / (2 * nbnd));
+  i = k < nbnd ? k : nx - 2 * nbnd + k;
+}
+
+// the band (closures, sides, corners): generic per-node path
 template <int PI_>
-__global__ void __launch_bounds__(ATX* ATY) adj_edge_kernel(const __grid_constant__ DevDomain D, AdjStage p) {
+__global__ void __launch_bounds__(256) adj_band_kernel(const __grid_constant__ DevDomain D, AdjStage p, long long nband) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nband) return;
   const DevBlock& B = D.blk[0];
-  const int i0 = blockIdx.x * ATX, j0 = blockIdx.y * ATY;
-  if (adj_tile_interior(i0, j0, B.nx, B.ny, nbnd_of(PI_))) return;
-  const int i = i0 + threadIdx.x % ATX, j = j0 + threadIdx.x / ATX;
-  if (i < B.nx && j < B.ny) adj_node_generic<PI_>(D, p, i, j);
+  int i, j;
+  band_node(q, B.nx, B.ny, nbnd_of(PI_), i, j);
+  adj_node_generic<PI_>(D, p, i, j);
 }
 
 template <int PI_>
@@ -244,15 +260,22 @@ __global__ void __launch_bounds__(ATX* ATY, 4) adj_stage_kernel(const __grid_con
   __shared__ double sL[3][WY][WX];  // weighted adjoint rates
   __shared__ double sM[4][WY][WX];  // yr, xr, yq, xq
   __shared__ double sU[3][WY][WX];  // stage input u_{s-1}
+  constexpr int nbnd = nbnd_of(PI_);
   const DevBlock& B = D.blk[0];
+  const int nx = B.nx, ny = B.ny;
   const int i0 = blockIdx.x * ATX, j0 = blockIdx.y * ATY;
   const int tx = threadIdx.x % ATX, ty = threadIdx.x / ATX;
-  if (!adj_tile_interior(i0, j0, B.nx, B.ny, nbnd_of(PI_))) return;  // adj_edge_kernel's tile
+  // tiles entirely inside the band have no work here
+  if (i0 + ATX - 1 < nbnd || i0 > nx - 1 - nbnd || j0 + ATY - 1 < nbnd || j0 > ny - 1 - nbnd) return;
   const long long pitch = B.pitch, plane = B.plane;
   const double* __restrict__ ust = p.store + ((*p.rel) * p.nstage + p.s) * p.stride;
   for (int q = threadIdx.x; q < WX * WY; q += ATX * ATY) {
     const int yy = q / WX, xx = q % WX;
-    const long long k = (long long)(j0 - H + yy) * pitch + (i0 - H + xx);  // inside the block: the tile is interior
+    const int gi = i0 - H + xx, gj = j0 - H + yy;
+    // positions outside the block are never read: an interior node's
+    // neighbours lie within PI_ <= nbnd of it
+    if (gi < 0 || gi >= nx || gj < 0 || gj >= ny) continue;
+    const long long k = (long long)gj * pitch + gi;
     const double Jk = B.Ji[k], wv = Jk / B.rho[k], ws = Jk * B.G[k];
     sL[0][yy][xx] = (p.qp_in[k] + p.Bdt * p.ub_in[k]) * wv;
     sL[1][yy][xx] = (p.qp_in[plane + k] + p.Bdt * p.ub_in[plane + k]) * ws;
@@ -266,6 +289,7 @@ __global__ void __launch_bounds__(ATX* ATY, 4) adj_stage_kernel(const __grid_con
     sU[2][yy][xx] = ust[2 * plane + k];
   }
   __syncthreads();
+  if (!adj_node_interior(i0 + tx, j0 + ty, nx, ny, nbnd)) return;  // band node (adj_band_kernel)
   const int X0 = tx + H, Y0 = ty + H;
   const double yrc = sM[0][Y0][X0], xrc = sM[1][Y0][X0], yqc = sM[2][Y0][X0], xqc = sM[3][Y0][X0];
   double acc[3] = {0.0, 0.0, 0.0};
@@ -363,17 +387,33 @@ __global__ void adj_forward_advance(TimeState* ts, AdjClock* ck) {
   ck->rel += 1;
 }
 
-// end of an adjoint step n: ubar += dJ/dU^n at the receivers, then step back
-__global__ void adj_inject(double* ub, const long long* __restrict__ rec, int nrec, const double* __restrict__ resid,
+// end of an adjoint step n: ubar += dJ/dU^n at the receivers, then step back.
+// One thread per distinct receiver node; receivers sharing a node (rlist
+// entries rstart[t]..rstart[t+1]) are summed in a fixed order.
+__global__ void adj_inject(double* ub, const long long* __restrict__ node, const int* __restrict__ rstart,
+                           const int* __restrict__ rlist, int nnode, int nrec, const double* __restrict__ resid,
                            AdjClock* ck, int back) {
-  if (threadIdx.x != 0) return;
   const long long n = ck->n;
-  // serial: two receivers may share a node
-  for (int r = 0; r < nrec; ++r) ub[rec[r]] += resid[(n - 1) * nrec + r];
-  if (back) {
+  for (int t = threadIdx.x; t < nnode; t += blockDim.x) {
+    double sum = 0.0;
+    for (int q = rstart[t]; q < rstart[t + 1]; ++q) sum += resid[(n - 1) * nrec + rlist[q]];
+    ub[node[t]] += sum;
+  }
+  __syncthreads();
+  if (back && threadIdx.x == 0) {
     ck->n -= 1;
     ck->rel -= 1;
   }
+}
+
+// end of a forward step: vz at the receivers of the new state (sample n+1), then n += 1
+__global__ void adj_sample_advance(const double* __restrict__ u, const long long* __restrict__ rec, int nrec,
+                                   TimeState* ts, double* traces, int nsamples) {
+  const long long n = ts->n + 1;
+  for (int r = threadIdx.x; r < nrec; r += blockDim.x)
+    if (n >= 1 && n <= nsamples) traces[(n - 1) * nrec + r] = u[rec[r]];
+  __syncthreads();
+  if (threadIdx.x == 0) ts->n = n;
 }
 
 }  // namespace fdmap

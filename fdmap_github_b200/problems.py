@@ -107,11 +107,11 @@ def rough_fault_rs(outdir: str | Path, nx: int = 2001, ny: int = 1001, h: float 
     # curve file (grid.f90:683-695): x, y, n1, n2; the stored normal points out of
     # the upper block (downwards); the lower block's T side flips it (grid.f90:453)
     _write(out / "fault.curve", x, y, dy / nrm, -1.0 / nrm)
-    # depth-dependent effective normal stress capped at 120 MPa, shear at 0.6 N
+    # depth-dependent effective normal stress capped at 120 MPa, shear at 0.4 N
     depth = x - x[0]
     N0 = np.minimum(120.0, 20.0 + 10.0 * depth)
     a, b, V0, f0, L, fw, Vw = 0.01, 0.014, 1e-6, 0.6, 0.4, 0.2, 0.1
-    S0 = 0.6 * N0
+    S0 = 0.4 * N0
     _write(out / "stress.dat", S0, N0)
     # state giving slip velocity Vinit under the background stress (strength()
     # of friction.f90:1066-1071 inverted for Psi)
@@ -137,7 +137,7 @@ def rough_fault_rs(outdir: str | Path, nx: int = 2001, ny: int = 1001, h: float 
 &friction_list friction_law='RFL', rs%a={_f(a)}, rs%b={_f(b)}, rs%V0={_f(V0)}, rs%f0={_f(f0)}, rs%L={_f(L)},
   rs%fw={_f(fw)}, rs%Vw={_f(Vw)}, stress_file=T, stress_filename='stress.dat',
   state_file=T, state_filename='state.dat',
-  ld%shape='gaussian', ld%R=1.5d0, ld%S=25d0, ld%x0={_f(x[nx // 2])},
+  ld%shape='gaussian', ld%R=3d0, ld%S=45d0, ld%x0={_f(x[nx // 2])},
   rup_field='V', rup_threshold=1d-3 /
 {tp_list}"""
 
@@ -245,6 +245,6 @@ def ensemble_instance(outdir: str | Path, seed: int, nx: int | None = None, ny: 
 &friction_list friction_law='RFL', rs%a={_f(a)}, rs%b={_f(b)}, rs%V0={_f(V0)}, rs%f0={_f(f0)}, rs%L={_f(L)},
   rs%fw={_f(fw)}, rs%Vw={_f(Vw)}, stress_file=T, stress_filename='stress_{seed}.dat',
   state_file=T, state_filename='state_{seed}.dat',
-  ld%shape='gaussian', ld%R=1.5d0, ld%S=25d0, ld%x0=0d0,
+  ld%shape='gaussian', ld%R=3d0, ld%S=45d0, ld%x0=0d0,
   rup_field='V', rup_threshold=1d-3 /
 """
