@@ -9,9 +9,10 @@ one full low-storage RK4 time step (5 stages) over all 2,564,802 nodes.
   value   FP64 node-updates/s of the whole job (all ranks), device-resident state,
           K steps timed with CUDA events on the engine's stream
   e2e     the same metric through the public C ABI with host buffers: the
-          initial state upload, the per-step fault output read-back (slip,
-          slip rate, shear stress, rupture time) and the final field
-          download are inside the timed region
+          initial state upload, the fault output of every step (slip, slip
+          rate, shear stress, rupture time as float32 time series, gathered
+          on the device and written to files) and the final field download
+          are inside the timed region
   roofline  the fused stencil kernel's achieved HBM bandwidth (algorithmic
           bytes per launch / its mean CUDA-event duration) against the measured
           copy bandwidth
@@ -28,6 +29,7 @@ import os
 import re
 import statistics
 import sys
+import tempfile
 import threading
 import time
 from pathlib import Path
@@ -182,7 +184,7 @@ def run_gpu(args) -> None:
 
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
-    tmp = ROOT / "_bench_tmp" / f"rank{rank}"
+    tmp = Path(tempfile.mkdtemp(prefix=f"fdmap_bench_r{rank}_"))
     text, base, info = workload(args.workload, tmp)
     host = init_domain(text, base)
     nodes = host.nx * host.ny
@@ -240,8 +242,14 @@ def run_gpu(args) -> None:
     pin_F = torch.from_numpy(F0).pin_memory()
     pin_DF = torch.from_numpy(DF0).pin_memory()
     nf = info.get("fault_nodes", 0)
-    out_fault = torch.empty((4, max(nf, 1)), dtype=torch.float64).pin_memory()
-    Fout = torch.empty_like(pin_F).pin_memory()
+    # fault time series of every step (slip, slip rate, shear stress, rupture
+    # time) through the device-side output: gathered into the device ring at
+    # the reference's stage-1 output point, drained to float32 files
+    out_dir = Path(tempfile.mkdtemp(prefix=f"fdmap_bench_out_r{rank}_"))
+    if nf:
+        for f in ("D", "V", "S", "trup"):
+            g2.output_add(f"fault_{f}", 0, 0, FAULT_INDEX[f], 1, nf, 1, nmin=0, nmax=1 << 62, stride=1)
+        g2.output_open(str(out_dir / "bench"), ring_steps=256)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -249,12 +257,9 @@ def run_gpu(args) -> None:
     e_start.record(stream)
     g2.set_fields(pin_F.numpy(), pin_DF.numpy())
     lib().fdmap_gpu_init_edges(g2._g, host.t0)
-    for n in range(1, args.steps + 1):
-        g2.run(n, n, nt=nt_inf)
-        if nf:
-            for k, f in enumerate(("D", "V", "S", "trup")):
-                lib().fdmap_gpu_get_fault(g2._g, 0, FAULT_INDEX[f],
-                                          out_fault[k].numpy().ctypes.data_as(C.POINTER(C.c_double)))
+    g2.run(1, args.steps, nt=nt_inf)
+    if nf:
+        g2.output_flush()
     F_final, _ = g2.get_fields()
     e_stop.record(stream)
     e_stop.synchronize()
@@ -262,7 +267,9 @@ def run_gpu(args) -> None:
     e_ms = barrier_max(e_ms, world)
     e2e = world * nodes * args.steps / (e_ms * 1e-3)
     h2d = (F0.nbytes + DF0.nbytes) / args.steps
-    d2h = (4 * nf * 8) + F0.nbytes / args.steps
+    d2h = (4 * nf * 4) + F0.nbytes / args.steps
+    if nf:
+        g2.output_close()
     g2.close()
 
     cpu = None
@@ -339,7 +346,7 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    tmp = ROOT / "_bench_tmp" / "ref"
+    tmp = Path(tempfile.mkdtemp(prefix="fdmap_bench_ref_"))
     text, base, info = workload(args.workload, tmp)
     host = init_domain(text, base)
     from oracle.binding import OracleDomain, num_threads
@@ -362,19 +369,154 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_ensemble(args) -> None:
+    """Batched ensemble (64 mode II rate-and-state instances of seeded grid
+    sizes and von Karman prestress): runs/s of the ensemble against the same
+    instances advanced one after another by the plain single-domain path.  A
+    run is 1000 steps; both arms are timed on `--steps` steps after warm-up
+    and scaled to the run length."""
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    from fdmap_github_b200 import GpuEnsemble
+
+    tmp = Path(tempfile.mkdtemp(prefix=f"fdmap_bench_ens_r{rank}_"))
+    n = args.instances
+    hosts = [init_domain(problems.ensemble_instance(tmp, s), tmp) for s in range(n)]
+    nodes = sum(h.nx * h.ny for h in hosts)
+    dt = min(h.dt for h in hosts)
+    run_steps = 1000
+    ens = GpuEnsemble(hosts, device=local)
+    shape, tune_ms = ens.tune(steps=5, dt=dt)
+    ens.run(1, args.warmup, dt=dt, nt=1 << 30)
+    ens.synchronize()
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        ens.run(args.warmup + 1, args.warmup + args.steps, dt=dt, nt=1 << 30)
+        ens.synchronize()
+        el = time.perf_counter() - t0
+    launches = ens.launch_count()
+    ens.close()
+    el = barrier_max(el, world)
+    # sequential arm: the same instances through the plain path, one at a time
+    seq = 0.0
+    for h in hosts:
+        g = GpuDomain(h, device=local)
+        g.run(1, args.warmup, dt=dt, nt=1 << 30)
+        g.synchronize()
+        t0 = time.perf_counter()
+        g.run(args.warmup + 1, args.warmup + args.steps, dt=dt, nt=1 << 30)
+        g.synchronize()
+        seq += time.perf_counter() - t0
+        g.close()
+    per_step = el / args.steps
+    runs = world * n / (per_step * run_steps)
+    if rank == 0:
+        line = {"metric": "ensemble runs/s", "value": runs, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"{n} mode II rate-and-state instances (RFL), 2 blocks each of "
+                                       "401x401 / 801x401 / 801x801 / 1601x801 (seeded), von Karman prestress",
+                           "instances": n, "nodes": nodes, "run_steps": run_steps, "shape": list(shape),
+                           "tuned_ms_per_step": tune_ms},
+                "node_updates_per_s": world * nodes / per_step,
+                "sequential_plain": {"runs_per_s": n / (seq / args.steps * run_steps),
+                                     "ms_per_step": seq / args.steps * 1e3},
+                "speedup_vs_sequential": seq / el, "clocks": clocks.summary(), "gpu_launches": launches}
+        print(json.dumps(line), flush=True)
+
+
+def run_adjoint(args) -> None:
+    """Forward/backward pair on the heterogeneous mode III block (801x801,
+    2000 steps, 32 receivers on the top row, checkpoints every 45 steps):
+    backward/forward time ratio and 16 random-direction central-difference
+    checks of the gradient (h = 1e-6 relative)."""
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    from fdmap_github_b200 import GpuAdjoint
+
+    tmp = Path(tempfile.mkdtemp(prefix=f"fdmap_bench_adj_r{rank}_"))
+    host = init_domain(problems.heterogeneous_ricker(tmp), tmp)
+    n = host.nx
+    rec = [(int(i), host.ny) for i in np.linspace(2, n - 1, 32).round().astype(int)]
+    rho, G = host.array("rho")[0].copy(), host.array("G")[0].copy()
+    # plain forward solve of the same problem (the reference point of the ratio)
+    g = GpuDomain(host, device=local)
+    g.run(1, 3, nt=1 << 30)
+    g.synchronize()
+    t0 = time.perf_counter()
+    g.run(1, host.nt - 1, nt=1 << 30)
+    g.synchronize()
+    t_fwd = time.perf_counter() - t0
+    g.close()
+    a = GpuAdjoint(host, rec, checkpoint_every=45, device=local)
+    y, x = np.meshgrid(np.linspace(0, 1, host.ny), np.linspace(0, 1, host.nx), indexing="ij")
+    bump = np.exp(-((x - 0.4) ** 2 + (y - 0.7) ** 2) / 0.02)
+    a.set_material(rho * (1 + 0.05 * bump), G * (1 - 0.05 * bump))
+    data, _ = a.forward()  # data: the perturbed model's seismograms
+    a.set_material(rho, G)
+    a.forward(data=data)
+    a.backward()  # warm-up of both passes
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        _, J = a.forward(data=data)
+        t_af = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        g_rho, g_G = a.backward()
+        t_bwd = time.perf_counter() - t0
+    rng = np.random.default_rng(0)
+    eps, errs = 1e-6, []
+    for _ in range(16):
+        d_rho = rng.uniform(-1, 1, rho.shape)
+        d_G = rng.uniform(-1, 1, G.shape)
+        pred = float(np.sum(g_rho * rho * d_rho) + np.sum(g_G * G * d_G))
+        a.set_material(rho * (1 + eps * d_rho), G * (1 + eps * d_G))
+        _, Jp = a.forward(data=data)
+        a.set_material(rho * (1 - eps * d_rho), G * (1 - eps * d_G))
+        _, Jm = a.forward(data=data)
+        fd = (Jp - Jm) / (2 * eps)
+        errs.append(abs(fd - pred) / abs(fd))
+    a.close()
+    if rank == 0:
+        nodes = host.nx * host.ny
+        line = {"metric": "adjoint/forward time", "value": t_bwd / t_fwd, "unit": "ratio", "n_gpus": world,
+                "steps": host.nt - 1, "warmup": 1, "ms_per_step": t_bwd / (host.nt - 1) * 1e3,
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": "mode III heterogeneous 801x801 (dx 20 m), Ricker 5 Hz point force, "
+                                       "32 top-row receivers, LS-RK4, checkpoints every 45 steps",
+                           "nodes": nodes, "steps": host.nt - 1},
+                "forward_s": t_fwd, "forward_node_updates_per_s": nodes * (host.nt - 1) / t_fwd,
+                "forward_with_checkpoints_s": t_af, "backward_s": t_bwd,
+                "forward_plus_backward_over_forward": (t_af + t_bwd) / t_fwd, "misfit": J,
+                "fd_check": {"directions": 16, "h_rel": eps, "max_rel_err": max(errs),
+                             "median_rel_err": float(np.median(errs))},
+                "clocks": clocks.summary()}
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--workload", default="rupture", choices=["rupture", "pulse", "roughfault"])
+    ap.add_argument("--workload", default="rupture", choices=["rupture", "pulse", "roughfault", "ensemble", "adjoint"])
+    ap.add_argument("--instances", type=int, default=64, help="ensemble workload: number of instances")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "ensemble":
+        run_ensemble(args)
+    elif args.workload == "adjoint":
+        run_adjoint(args)
     else:
         run_gpu(args)
 

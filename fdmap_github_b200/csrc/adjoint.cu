@@ -43,8 +43,10 @@ struct fdmap_adjoint {
   int* rstart = nullptr;
   int* rlist = nullptr;
   long long nband = 0;                // nodes within nbnd of a side
-  cudaStream_t side = nullptr;        // band kernel beside the interior adjoint kernel
+  cudaStream_t side = nullptr;        // band kernel beside the interior adjoint kernel (high priority)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t copy = nullptr;        // stage-input copies beside the recomputed stage
+  cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;
   double* init_F = nullptr;          // initial fields (3 planes)
   double* init_DF = nullptr;
   double* ckpt = nullptr;            // checkpoints, 3 planes each
@@ -81,7 +83,10 @@ struct fdmap_adjoint {
     for (void* p : mem) cudaFree(p);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_cfork) cudaEventDestroy(ev_cfork);
+    if (ev_cjoin) cudaEventDestroy(ev_cjoin);
     if (side) cudaStreamDestroy(side);
+    if (copy) cudaStreamDestroy(copy);
     if (h) fdmap_gpu_destroy(h);
   }
   template <typename T>
@@ -103,7 +108,7 @@ struct fdmap_adjoint {
 
 namespace {
 
-// interior tiles on the main stream, the band on the side stream (disjoint
+// interior tiles on the main stream, the band on a side stream (disjoint
 // nodes, same inputs), joined before the next stage
 int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p) {
   fdmap_gpu* h = a->h;
@@ -112,15 +117,17 @@ int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p) {
   const int bgrid = (int)((a->nband + 255) / 256);
   CUDA_TRY(cudaEventRecord(a->ev_fork, h->stream));
   CUDA_TRY(cudaStreamWaitEvent(a->side, a->ev_fork, 0));
+  // the latency-bound band kernel goes first, at high priority, so its few CTAs
+  // are placed before the interior tiles fill the SMs
   if (h->pI == 1) {
-    adj_stage_kernel<1><<<grid, blk, 0, h->stream>>>(h->hdom, p);
     adj_band_kernel<1><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
+    adj_stage_kernel<1><<<grid, blk, 0, h->stream>>>(h->hdom, p);
   } else if (h->pI == 2) {
-    adj_stage_kernel<2><<<grid, blk, 0, h->stream>>>(h->hdom, p);
     adj_band_kernel<2><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
+    adj_stage_kernel<2><<<grid, blk, 0, h->stream>>>(h->hdom, p);
   } else {
-    adj_stage_kernel<3><<<grid, blk, 0, h->stream>>>(h->hdom, p);
     adj_band_kernel<3><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
+    adj_stage_kernel<3><<<grid, blk, 0, h->stream>>>(h->hdom, p);
   }
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaEventRecord(a->ev_join, a->side));
@@ -134,9 +141,15 @@ int forward_step_stages(fdmap_adjoint* a, int cur, double dt, bool stash) {
   const DevBlock& B = h->hdom.blk[0];
   for (int s = 0; s < h->rk.nstage; ++s) {
     if (stash) {
-      adj_stash<<<296, 256, 0, h->stream>>>(B.F[cur], a->store, a->stride(), &a->clock->rel, s, h->rk.nstage,
-                                            a->stride());
+      // the stage only reads F[cur]; the copy of it runs beside the stage and
+      // joins before the next stage overwrites that buffer
+      if (s > 0) CUDA_TRY(cudaStreamWaitEvent(h->stream, a->ev_cjoin, 0));
+      CUDA_TRY(cudaEventRecord(a->ev_cfork, h->stream));
+      CUDA_TRY(cudaStreamWaitEvent(a->copy, a->ev_cfork, 0));
+      adj_stash<<<296, 256, 0, a->copy>>>(B.F[cur], a->store, a->stride(), &a->clock->rel, s, h->rk.nstage,
+                                          a->stride());
       CUDA_TRY(cudaGetLastError());
+      CUDA_TRY(cudaEventRecord(a->ev_cjoin, a->copy));
     }
     StageArgs st{};
     st.A = h->rk.A[s];
@@ -151,6 +164,7 @@ int forward_step_stages(fdmap_adjoint* a, int cur, double dt, bool stash) {
     if (rc) return rc;
     cur = 1 - cur;
   }
+  if (stash) CUDA_TRY(cudaStreamWaitEvent(h->stream, a->ev_cjoin, 0));
   return FDMAP_OK;
 }
 
@@ -304,7 +318,10 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
   {
     int lo = 0, hi = 0;
     if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
-        cudaStreamCreateWithPriority(&a->side, cudaStreamNonBlocking, lo) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&a->side, cudaStreamNonBlocking, hi) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&a->copy, cudaStreamNonBlocking, lo) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a->ev_cfork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&a->ev_cjoin, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&a->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&a->ev_join, cudaEventDisableTiming) != cudaSuccess)
       return fail(set_err(FDMAP_ERR_CUDA, "adjoint stream setup"));

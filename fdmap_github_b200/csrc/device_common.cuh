@@ -66,6 +66,7 @@ struct DevFriction {
   double ld_S, ld_N, ld_T, ld_R, ld_x0, ld_y0, tp_p0;
   double* st;
   double* par;
+  double* st_out;  // stage-1 snapshot of the 18 fields at the output point (outputs open), else null
 };
 
 // per-interface-node impedance terms, evaluated once on the host (each is a
@@ -146,6 +147,7 @@ struct StageArgs {
   int update;    // update the state (0 on the final step and the initial solve)
   const TimeState* ts;  // device step clock (graph replays), or nullptr
   double C;      // RK C(stage-1): stage time = t0 + C*dt
+  int tap;       // stage 1 with outputs open: interface kernels write their output snapshot
 };
 
 // Stage time t0 + C*dt with t0 = t_start + (n-1)*dt, rounded exactly as the

@@ -434,6 +434,16 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
     st[ST_TRUP * n + k] = trup;
     st[ST_V * n + k] = ns.V; st[ST_O * n + k] = ns.O; st[ST_S * n + k] = ns.S; st[ST_N * n + k] = ns.N;
     st[ST_S0 * n + k] = ns.S0; st[ST_N0 * n + k] = ns.N0;
+    if (a.tap && FR.st_out) {
+      // the fields as write_output sees them in stage 1: solved and rates set, not yet updated
+      double* so = FR.st_out;
+      so[ST_D * n + k] = ns.D; so[ST_PSI * n + k] = ns.Psi; so[ST_DPSI * n + k] = DPsi; so[ST_TRUP * n + k] = trup;
+      so[ST_V * n + k] = ns.V; so[ST_O * n + k] = ns.O; so[ST_S * n + k] = ns.S; so[ST_N * n + k] = ns.N;
+      so[ST_S0 * n + k] = ns.S0; so[ST_N0 * n + k] = ns.N0; so[ST_DS * n + k] = st[ST_DS * n + k];
+      so[ST_DN * n + k] = st[ST_DN * n + k]; so[ST_DDS * n + k] = DDs; so[ST_DDN * n + k] = DDn;
+      so[ST_W * n + k] = st[ST_W * n + k]; so[ST_DW * n + k] = DW; so[ST_NREG * n + k] = ns.Nreg;
+      so[ST_DNREG * n + k] = DNreg;
+    }
     double Nreg = ns.Nreg;
     if (a.update) {
       // update_fields_friction (friction.f90:576-590)

@@ -30,6 +30,9 @@ struct BlockGeom {
   long long plane;
 };
 
+struct OutputState;  // device-side output (output.cu)
+void output_destroy(fdmap_gpu* h);
+
 __global__ void advance_step(TimeState* ts);
 __global__ void set_step_clock(TimeState* ts, double t_start, double dt, long long n);
 
@@ -73,6 +76,9 @@ struct fdmap_gpu {
   double* dev_fhat[MAX_BLOCKS][4] = {};
   int side_n[MAX_BLOCKS][4] = {};
   cudaStream_t own_stream = nullptr;
+  // device-side output (fdmap_gpu_output_*): open state and the next step index
+  OutputState* out = nullptr;
+  long long out_next_n = 1;
   // boundary work (interface solves, closure strips) runs on a low-priority
   // side stream beside the interior march of the same stage
   bool overlap = false;
@@ -152,6 +158,7 @@ struct fdmap_gpu {
     if (side_stream) cudaStreamDestroy(side_stream);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    output_destroy(this);
     delete tmaps;
     for (auto& ge : step_graph)
       if (ge) cudaGraphExecDestroy(ge);
@@ -159,6 +166,11 @@ struct fdmap_gpu {
 };
 
 namespace fdmap {
+
+// device-side output hooks (output.cu)
+bool output_is_open(const fdmap_gpu* h);
+int output_before_step(fdmap_gpu* h, long long n, double t);
+int output_gather(fdmap_gpu* h, const TimeState* ts, long long n, int cur);
 
 // Launchers over a batch of independent domains (one DevDomain per instance,
 // in device memory).  `proto` supplies the compile-time variant (mode, SBP

@@ -600,10 +600,15 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   return fdmap_gpu_set_fields(h, d->F, d->DF);
 }
 
-// all stages of one step starting from buffer `cur`; final = stage 1 only
-int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, const TimeState* ts) {
+// all stages of one step starting from buffer `cur`; final = stage 1 only.
+// With outputs open, stage 1 taps the interface state and the output gather
+// follows it (step index from the device clock `ts`, else `n`).
+int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, const TimeState* ts, long long n = 0) {
+  const bool outputs = output_is_open(h);
+  const int cur0 = cur;
   for (int s = 0; s < h->rk.nstage; ++s) {
     StageArgs a{};
+    a.tap = (s == 0 && outputs) ? 1 : 0;
     a.A = h->rk.A[s];
     a.Bdt = h->rk.B[s] * dt;
     a.t = t0 + h->rk.C[s] * dt;
@@ -615,6 +620,7 @@ int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, con
     a.update = final_step ? 0 : 1;
     int rc = launch_stage(h, a);
     if (rc) return rc;
+    if (s == 0 && outputs && (rc = output_gather(h, ts, n, cur0))) return rc;
     if (final_step) return FDMAP_OK;
     cur = 1 - cur;
   }
@@ -704,8 +710,11 @@ int fdmap_gpu_init_edges(fdmap_gpu* h, double t) {
 int fdmap_gpu_time_step(fdmap_gpu* h, double t0, double dt, int final_step) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
   CUDA_TRY(cudaSetDevice(h->device));
-  int rc = issue_step(h, h->cur, t0, dt, final_step != 0, nullptr);
+  int rc = output_before_step(h, h->out_next_n, t0);
   if (rc) return rc;
+  rc = issue_step(h, h->cur, t0, dt, final_step != 0, nullptr, h->out_next_n);
+  if (rc) return rc;
+  h->out_next_n += 1;
   if (!final_step && (h->rk.nstage & 1)) h->cur = 1 - h->cur;
   return FDMAP_OK;
 }
@@ -724,16 +733,20 @@ int fdmap_gpu_run(fdmap_gpu* h, double t_start, double dt, int n_first, int n_la
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     for (int n = n_first; n <= n_graph_last; ++n) {
+      int rc = output_before_step(h, n, t_start + (double)(n - 1) * dt);
+      if (rc) return rc;
       CUDA_TRY(cudaGraphLaunch(h->step_graph[h->cur], h->stream));
       h->launches += h->graph_launches;
       if (h->rk.nstage & 1) h->cur = 1 - h->cur;
     }
     n_first = n_graph_last + 1;
   }
+  h->out_next_n = n_first;
   for (int n = n_first; n <= n_last; ++n) {
     int rc = fdmap_gpu_time_step(h, t_start + (double)(n - 1) * dt, dt, n == nt);
     if (rc) return rc;
   }
+  h->out_next_n = (long long)n_last + 1;
   return FDMAP_OK;
 }
 

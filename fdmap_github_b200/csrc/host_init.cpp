@@ -1112,6 +1112,19 @@ extern "C" int fdmap_host_iface_n(const fdmap_domain* dom, int iface) {
   return dom->desc.ifaces[iface].p - dom->desc.ifaces[iface].m + 1;
 }
 
+extern "C" int fdmap_host_iface_info(const fdmap_domain* dom, int iface, int* info) {
+  if (!dom || !info || iface < 0 || iface >= dom->desc.nifaces) return FDMAP_ERR_INVALID_ARG;
+  const fdmap_iface& I = dom->desc.ifaces[iface];
+  info[0] = I.direction; info[1] = I.m; info[2] = I.p; info[3] = I.coupling;
+  return FDMAP_OK;
+}
+
+extern "C" const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface, int which) {
+  if (!dom || iface < 0 || iface >= dom->desc.nifaces) return nullptr;
+  const fdmap_iface& I = dom->desc.ifaces[iface];
+  return which == 0 ? I.x : I.y;
+}
+
 extern "C" int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim) {
   if (!dom || !lim || block < 0 || block >= dom->desc.nblocks) return FDMAP_ERR_INVALID_ARG;
   const fdmap_block& b = dom->desc.blocks[block];

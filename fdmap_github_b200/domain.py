@@ -60,6 +60,20 @@ class HostDomain:
             check_host(n, "fdmap_host_iface_n")
         return n
 
+    def iface_info(self, iface: int) -> tuple[int, int, int, int]:
+        """(direction 0='x' / 1='y', m, p, coupling) of interface `iface`."""
+        info = (C.c_int * 4)()
+        check_host(lib().fdmap_host_iface_info(self._h, iface, info), "fdmap_host_iface_info")
+        return tuple(info)
+
+    def iface_xy(self, iface: int) -> tuple[np.ndarray, np.ndarray]:
+        n = self.iface_n(iface)
+        out = []
+        for w in (0, 1):
+            p = lib().fdmap_host_iface_xy(self._h, iface, w)
+            out.append(np.ctypeslib.as_array(p, shape=(n,)).copy() if p else np.zeros(n))
+        return out[0], out[1]
+
     def block_limits(self, b: int) -> tuple[int, int, int, int]:
         lim = (C.c_int * 4)()
         check_host(lib().fdmap_host_block_limits(self._h, b, lim), "fdmap_host_block_limits")
@@ -133,6 +147,21 @@ class GpuDomain:
         out = np.empty(n * self.nF)
         check_gpu(lib().fdmap_gpu_get_fhat(self._g, b, s, dptr(out)), "fdmap_gpu_get_fhat")
         return out.reshape(self.nF, n)
+
+    # ---- device-side output (fdmap_gpu_output_*)
+    def output_add(self, name: str, kind: int, index: int, field: int, mx: int, px: int, sx: int = 1,
+                   my: int = 1, py: int = 1, sy: int = 1, nmin: int = 0, nmax: int = 2**62, stride: int = 1) -> None:
+        check_gpu(lib().fdmap_gpu_output_add(self._g, name.encode(), kind, index, field, mx, px, sx, my, py, sy,
+                                             nmin, nmax, stride), "fdmap_gpu_output_add")
+
+    def output_open(self, prefix: str, ring_steps: int = 512) -> None:
+        check_gpu(lib().fdmap_gpu_output_open(self._g, str(prefix).encode(), ring_steps), "fdmap_gpu_output_open")
+
+    def output_flush(self) -> None:
+        check_gpu(lib().fdmap_gpu_output_flush(self._g), "fdmap_gpu_output_flush")
+
+    def output_close(self) -> None:
+        check_gpu(lib().fdmap_gpu_output_close(self._g), "fdmap_gpu_output_close")
 
     def fault_max_noalloc(self, iface: int, field: str) -> float:
         """max |field| along interface `iface`, reduced on the device without allocating."""

@@ -39,6 +39,8 @@ SIGNATURES = {
     "fdmap_host_info": (C.c_int, [_VP, C.POINTER(C.c_int), _DP]),
     "fdmap_host_iface_n": (C.c_int, [_VP, C.c_int]),
     "fdmap_host_block_limits": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
+    "fdmap_host_iface_info": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
+    "fdmap_host_iface_xy": (_DP, [_VP, C.c_int, C.c_int]),
     "fdmap_host_array": (_DP, [_VP, C.c_char_p, C.POINTER(C.c_longlong)]),
     "fdmap_host_last_error": (C.c_char_p, []),
     # fdmap_gpu.h
@@ -57,6 +59,11 @@ SIGNATURES = {
     "fdmap_gpu_get_fhat": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_status": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
     "fdmap_gpu_fault_max_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
+    "fdmap_gpu_output_add": (C.c_int, [_VP, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.c_int]),
+    "fdmap_gpu_output_open": (C.c_int, [_VP, C.c_char_p, C.c_int]),
+    "fdmap_gpu_output_flush": (C.c_int, [_VP]),
+    "fdmap_gpu_output_close": (C.c_int, [_VP]),
     "fdmap_gpu_launch_count": (C.c_longlong, [_VP]),
     "fdmap_gpu_device_bytes": (C.c_longlong, [_VP]),
     "fdmap_gpu_destroy": (None, [_VP]),

@@ -74,6 +74,29 @@ int fdmap_gpu_get_fhat(fdmap_gpu* h, int b, int s, double* out);
 /* Device status: Newton failures so far (the reference stops on the first). */
 int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
 
+/* ------------------------------------------------------------------------
+ * Device-side output (write_output, output.f90:990-1060).  An item samples
+ * one field at each step whose index D%n (= n-1 for loop index n) lies in
+ * [nmin, nmax] with (D%n - nmin) % stride == 0, at the reference's output
+ * point (stage 1 after the interface solve, before the update,
+ * time_step.f90:129).  Values are gathered on the device into float32 rings
+ * of `ring_steps` output steps; the host appends them to
+ * <prefix>_<name>.dat (i fastest) and D%t to <prefix>_<name>.t, as
+ * open_output_file names and lays out its files (output.f90:916-987).
+ *   FDMAP_OUT_FAULT: `index` = interface, `field` = FDMAP_FAULT_*,
+ *                    nodes mx..px (1-based along the interface) step sx;
+ *   FDMAP_OUT_BODY:  `field` = body field component (0..nF-1), global
+ *                    nodes mx..px step sx by my..py step sy.
+ * Items are added before fdmap_gpu_output_open; fdmap_gpu_output_flush
+ * writes everything recorded so far, fdmap_gpu_output_close flushes and
+ * releases the rings. */
+enum { FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1 };
+int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, int field, int mx, int px, int sx,
+                         int my, int py, int sy, long long nmin, long long nmax, int stride);
+int fdmap_gpu_output_open(fdmap_gpu* h, const char* prefix, int ring_steps);
+int fdmap_gpu_output_flush(fdmap_gpu* h);
+int fdmap_gpu_output_close(fdmap_gpu* h);
+
 /* max |field| over the nodes of interface `iface` (a friction interface),
  * reduced on the device into *out.  No counterpart in the reference (its
  * drivers scan the Fortran arrays).  Allocates nothing during the call: for

@@ -47,6 +47,13 @@ int fdmap_host_info(const fdmap_domain* dom, int* ints, double* dbls);
 /* Number of nodes p-m+1 of interface `iface` (0-based), or a negative code. */
 int fdmap_host_iface_n(const fdmap_domain* dom, int iface);
 
+/* Interface layout: info[4] = direction (0 'x', 1 'y'), m, p (1-based global
+ * indices along the interface), coupling. */
+int fdmap_host_iface_info(const fdmap_domain* dom, int iface, int* info);
+
+/* Interface geometry: x[n], y[n] of interface `iface` (NULL if absent). */
+const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface, int which);
+
 /* Block index limits: lim[4] = mgx, pgx, mgy, pgy (1-based). */
 int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim);
 

@@ -1,0 +1,110 @@
+"""Device-side output: the reference's output list, the float32 .dat/.t
+files, the stage-1 output point, and drains of the device ring."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from fdmap_github_b200 import GpuDomain, init_domain, problems
+from fdmap_github_b200.output import configure_outputs, read_output_list
+
+OUT_LIST = """
+!---begin:output_list---
+I
+iface1
+x y
+0d0 0d0 1
+I
+iface1
+D V S trup
+0d0 1d10 1
+B
+body
+vx sxy
+0d0 1d10 4
+P
+point_body
+vy
+0d0 1d10 1
+20 11
+G
+grid_iface1
+V
+0d0 1d10 2
+5 10 25
+!---end:output_list---
+"""
+
+
+def test_read_output_list():
+    items = read_output_list(OUT_LIST)
+    assert [it.name for it in items] == ["I", "I", "B", "P", "G"]
+    assert items[1].fields == ["D", "V", "S", "trup"] and items[1].stride == 1
+    assert items[2].location == "body" and items[2].stride == 4 and items[2].tmax == 1e10
+    assert items[3].index == [20, 11]
+    assert items[4].location == "grid_iface1" and items[4].index == [5, 10, 25]
+
+
+def _problem(nt=31):
+    return problems.rupture_sw(nx=41, ny=21, h=0.5, nt=nt) + OUT_LIST
+
+
+@pytest.mark.gpu
+def test_outputs_match_stage1_state(require_gpu, tmp_path):
+    text = _problem()
+    h = init_domain(text)
+    g = GpuDomain(h)
+    prefix = tmp_path / "rup"
+    names = configure_outputs(g, h, text, prefix, ring_steps=7)  # small ring: several drains
+    assert "I_V" in names and "G_15_V" in names
+    nsteps = 30
+    g.run(1, nsteps, nt=h.nt)  # graph replays
+    g.output_close()
+    # reference trajectory with a stage-1 probe per step (final-step semantics:
+    # solve and rates only, nothing updated)
+    p = GpuDomain(h)
+    nf = h.iface_n(0)
+    D = np.fromfile(f"{prefix}_I_D.dat", dtype=np.float32).reshape(-1, nf)
+    V = np.fromfile(f"{prefix}_I_V.dat", dtype=np.float32).reshape(-1, nf)
+    tr = np.fromfile(f"{prefix}_I_trup.dat", dtype=np.float32).reshape(-1, nf)
+    vx = np.fromfile(f"{prefix}_B_vx.dat", dtype=np.float32).reshape(-1, h.ny, h.nx)
+    vy = np.fromfile(f"{prefix}_P_vy.dat", dtype=np.float32)
+    gv = np.fromfile(f"{prefix}_G_15_V.dat", dtype=np.float32)
+    t = np.fromfile(f"{prefix}_I_V.t", dtype=np.float32)
+    assert D.shape[0] == V.shape[0] == nsteps and vx.shape[0] == (nsteps - 1) // 4 + 1 and gv.size == nsteps // 2
+    np.testing.assert_array_equal(t, (h.t0 + np.arange(nsteps) * h.dt).astype(np.float32))
+    for n in range(1, nsteps + 1):
+        t0 = h.t0 + (n - 1) * h.dt
+        F, _ = p.get_fields()
+        Dn = p.get_fault(0, "D")  # before the probe: the step-start slip
+        p.time_step_LS(t0, h.dt, final_step=True)
+        np.testing.assert_array_equal(D[n - 1], Dn.astype(np.float32))
+        np.testing.assert_array_equal(V[n - 1], p.get_fault(0, "V").astype(np.float32))
+        np.testing.assert_array_equal(tr[n - 1], p.get_fault(0, "trup").astype(np.float32))
+        assert vy[n - 1] == np.float32(F[1, 10, 19])
+        if (n - 1) % 4 == 0:
+            np.testing.assert_array_equal(vx[(n - 1) // 4], F[0].astype(np.float32))
+        if (n - 1) % 2 == 0:
+            assert gv[(n - 1) // 2] == np.float32(p.get_fault(0, "V")[14])
+        p.time_step_LS(t0, h.dt)
+    # static items are written once
+    x = np.fromfile(f"{prefix}_I_x.dat", dtype=np.float32)
+    assert x.size == nf
+
+
+@pytest.mark.gpu
+def test_outputs_eager_steps_equal_graph_steps(require_gpu, tmp_path):
+    text = _problem(nt=13)
+    h = init_domain(text)
+    a, b = GpuDomain(h), GpuDomain(h)
+    configure_outputs(a, h, text, tmp_path / "a", ring_steps=4)
+    configure_outputs(b, h, text, tmp_path / "b", ring_steps=100)
+    a.run(1, h.nt)  # graphs + final step
+    for n in range(1, h.nt + 1):
+        b.time_step_LS(h.t0 + (n - 1) * h.dt, h.dt, final_step=(n == h.nt))
+    a.output_close()
+    b.output_close()
+    for nm in ("I_D", "I_V", "I_S", "B_vx", "P_vy"):
+        x = np.fromfile(tmp_path / f"a_{nm}.dat", dtype=np.float32)
+        y = np.fromfile(tmp_path / f"b_{nm}.dat", dtype=np.float32)
+        assert x.size > 0 and np.array_equal(x, y), nm
