@@ -69,8 +69,7 @@ struct fdmap_gpu {
   double* met_base[MAX_BLOCKS] = {};
   double* het_base[MAX_BLOCKS] = {};
   TmapSet* tmaps = nullptr;  // host copy, passed by value to the march kernel
-  double* h_stage = nullptr;  // pinned staging buffer for layout conversion
-  size_t stage_doubles = 0;
+  double* d_global = nullptr;  // one field set in FDMAP's global layout: get/set_fields staging
   unsigned long long* d_status = nullptr;
   long long launches = 0;
   double* dev_fhat[MAX_BLOCKS][4] = {};
@@ -153,7 +152,6 @@ struct fdmap_gpu {
     for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
     for (auto e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
-    if (h_stage) cudaFreeHost(h_stage);
     if (own_stream) cudaStreamDestroy(own_stream);
     if (side_stream) cudaStreamDestroy(side_stream);
     if (ev_fork) cudaEventDestroy(ev_fork);

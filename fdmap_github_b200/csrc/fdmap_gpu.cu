@@ -47,6 +47,24 @@ void source_weights(double h, double a, double* w) {
 }  // namespace
 
 namespace fdmap {
+// global (i fastest, j, field) array <-> padded block planes of one block
+__global__ void scatter_block(const double* __restrict__ g, double* __restrict__ dst, int nxg, long long NN, int mgx,
+                              int mgy, int nx, int ny, int pitch, long long plane, int nF) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= pitch || j >= ny) return;
+  for (int l = 0; l < nF; ++l)
+    dst[l * plane + (long long)j * pitch + i] =
+        i < nx ? g[l * NN + (long long)(mgy - 1 + j) * nxg + (mgx - 1 + i)] : 0.0;
+}
+__global__ void gather_block(const double* __restrict__ src, double* __restrict__ g, int nxg, long long NN, int mgx,
+                             int mgy, int nx, int ny, int pitch, long long plane, int nF) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= nx || j >= ny) return;
+  for (int l = 0; l < nF; ++l)
+    g[l * NN + (long long)(mgy - 1 + j) * nxg + (mgx - 1 + i)] = src[l * plane + (long long)j * pitch + i];
+}
 // end of a replayed step: advance the device step clock
 __global__ void advance_step(TimeState* ts) { ts->n += 1; }
 // start of a replayed sequence: set the step clock (by value, no host buffer to keep alive)
@@ -591,11 +609,8 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   if ((rc = h->alloc(&h->ddom, 1))) return rc;
   CUDA_TRY(cudaMemcpy(h->ddom, &D, sizeof(DevDomain), cudaMemcpyHostToDevice));
 
-  // staging buffer and initial fields
-  size_t total = 0;
-  for (auto& g : h->geom) total += (size_t)g.plane * nF;
-  h->stage_doubles = total;
-  CUDA_TRY(cudaMallocHost(&h->h_stage, total * sizeof(double)));
+  // global-layout staging buffer and initial fields
+  if ((rc = h->alloc(&h->d_global, (size_t)d->nx * d->ny * nF))) return rc;
   h->cur = 0;
   return fdmap_gpu_set_fields(h, d->F, d->DF);
 }
@@ -761,30 +776,21 @@ int fdmap_gpu_get_fields(fdmap_gpu* h, double* F, double* DF) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
   CUDA_TRY(cudaSetDevice(h->device));
   const int nF = h->nF;
+  const long long NN = (long long)h->nx_g * h->ny_g;
   for (int which = 0; which < 2; ++which) {
     double* dst = which == 0 ? F : DF;
     if (!dst) continue;
-    size_t off = 0;
+    // padded block planes -> one contiguous global array on the device -> one copy
     for (int b = 0; b < h->hdom.nblocks; ++b) {
       const BlockGeom& g = h->geom[b];
       const double* src = which == 0 ? h->hdom.blk[b].F[h->cur] : h->hdom.blk[b].DF;
-      CUDA_TRY(cudaMemcpyAsync(h->h_stage + off, src, (size_t)g.plane * nF * sizeof(double), cudaMemcpyDeviceToHost,
-                               h->stream));
-      off += (size_t)g.plane * nF;
+      dim3 grid((g.nx + 255) / 256, g.ny);
+      gather_block<<<grid, 256, 0, h->stream>>>(src, h->d_global, h->nx_g, NN, g.mgx, g.mgy, g.nx, g.ny, g.pitch,
+                                               g.plane, nF);
+      CUDA_TRY(cudaGetLastError());
     }
+    CUDA_TRY(cudaMemcpyAsync(dst, h->d_global, (size_t)NN * nF * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    off = 0;
-    const size_t NN = (size_t)h->nx_g * h->ny_g;
-    for (int b = 0; b < h->hdom.nblocks; ++b) {
-      const BlockGeom& g = h->geom[b];
-      for (int l = 0; l < nF; ++l)
-        for (int j = 0; j < g.ny; ++j) {
-          const double* s = h->h_stage + off + (size_t)l * g.plane + (size_t)j * g.pitch;
-          double* t = dst + (size_t)l * NN + (size_t)(g.mgy - 1 + j) * h->nx_g + (g.mgx - 1);
-          std::memcpy(t, s, g.nx * sizeof(double));
-        }
-      off += (size_t)g.plane * nF;
-    }
   }
   return FDMAP_OK;
 }
@@ -793,25 +799,19 @@ int fdmap_gpu_set_fields(fdmap_gpu* h, const double* F, const double* DF) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
   CUDA_TRY(cudaSetDevice(h->device));
   const int nF = h->nF;
-  const size_t NN = (size_t)h->nx_g * h->ny_g;
+  const long long NN = (long long)h->nx_g * h->ny_g;
   for (int which = 0; which < 2; ++which) {
     const double* src = which == 0 ? F : DF;
     if (!src) continue;
-    CUDA_TRY(cudaStreamSynchronize(h->stream));  // staging buffer reuse
-    size_t off = 0;
+    // one copy of the global array, then scattered into the padded block planes
+    CUDA_TRY(cudaMemcpyAsync(h->d_global, src, (size_t)NN * nF * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     for (int b = 0; b < h->hdom.nblocks; ++b) {
       const BlockGeom& g = h->geom[b];
-      for (int l = 0; l < nF; ++l)
-        for (int j = 0; j < g.ny; ++j) {
-          double* t = h->h_stage + off + (size_t)l * g.plane + (size_t)j * g.pitch;
-          const double* s = src + (size_t)l * NN + (size_t)(g.mgy - 1 + j) * h->nx_g + (g.mgx - 1);
-          std::memcpy(t, s, g.nx * sizeof(double));
-          for (int i = g.nx; i < g.pitch; ++i) t[i] = 0.0;
-        }
       double* dst = which == 0 ? h->hdom.blk[b].F[h->cur] : h->hdom.blk[b].DF;
-      CUDA_TRY(cudaMemcpyAsync(dst, h->h_stage + off, (size_t)g.plane * nF * sizeof(double), cudaMemcpyHostToDevice,
-                               h->stream));
-      off += (size_t)g.plane * nF;
+      dim3 grid((g.pitch + 255) / 256, g.ny);
+      scatter_block<<<grid, 256, 0, h->stream>>>(h->d_global, dst, h->nx_g, NN, g.mgx, g.mgy, g.nx, g.ny, g.pitch,
+                                                g.plane, nF);
+      CUDA_TRY(cudaGetLastError());
     }
   }
   CUDA_TRY(cudaStreamSynchronize(h->stream));

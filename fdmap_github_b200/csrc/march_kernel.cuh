@@ -276,6 +276,9 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
     double* __restrict__ Fout = B.F[a.out];
 
     const int nbst = D.nbst;
+    // body forces of this block (point source / gravity), evaluated once per segment
+    const bool forces = D.src.use_gravity || (D.src.use_singular && B.src_ok);
+    const double t_stage = forces ? stage_time(a) : 0.0;
     const int i = i0 + cx;
     for (int g = 0; g < ngroups; ++g) {
       // wait for groups g-1, g, g+1 (neighbours) and centre group g
@@ -356,7 +359,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
           }
         }
         if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-        body_forces<MODE>(D, B, i, j, stage_time(a), acc);
+        if (forces) body_forces<MODE>(D, B, i, j, t_stage, acc);
 #pragma unroll
         for (int l = 0; l < NF; ++l) DFp[l * plane + c] = acc[l];
         if (a.update) {
