@@ -1,0 +1,100 @@
+"""Checkpoint / resume of the device state in FDMAP's FP64 checkpoint files.
+
+The files follow checkpoint_op (checkpoint.f90:254-288) for a single-process
+run: native-endian float64, Fortran column-major arrays, no headers.
+
+  <name>F.ckpt<n>                 F(:,:,l) for l = 1..nF over the global grid,
+                                  then DF(:,:,l)          (fields.f90:335-429)
+  <name>block<b><S>.ckpt<n>       for S = L, R, B, T: per field l the side's
+                                  edge values F(:,l), hat variables Fhat(:,l),
+                                  prestress F0(:,l); then the boundary energy
+                                  E(:) and its rate DE(:)  (fields.f90:432-644)
+  <name>iface<i>side<s>.ckpt<n>   for s = 1, 2: the 18 friction fields in
+                                  checkpoint_friction order D, Psi, DPsi, trup,
+                                  V, O, S, N, S0, N0, Ds, Dn, DDs, DDn, W, DW,
+                                  Nreg, DNreg          (friction.f90:491-552)
+  <name>.ckpt                     the number of the last checkpoint written
+
+The engine does not track the boundary energy, so E and DE are written as
+zeros and ignored on reading.  A resume needs F, DF and the friction fields;
+edge values and hat variables are recomputed in stage 1 of the next step,
+exactly as the reference recomputes them after checkpoint_read.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+
+from .native import FAULT_FIELDS
+
+SIDES = "LRBT"
+COUPLING_FRICTION = 1  # FDMAP_COUPLING_FRICTION
+
+
+def _edge_values(F: np.ndarray, host, b: int, s: int) -> np.ndarray:
+    """Edge row/column of the global fields F (nF, ny, nx) on side s of block b, shape (nF, n)."""
+    mgx, pgx, mgy, pgy = host.block_limits(b)
+    if s == 0:
+        return F[:, mgy - 1:pgy, mgx - 1]
+    if s == 1:
+        return F[:, mgy - 1:pgy, pgx - 1]
+    if s == 2:
+        return F[:, mgy - 1, mgx - 1:pgx]
+    return F[:, pgy - 1, mgx - 1:pgx]
+
+
+def checkpoint_write(gpu, host, name: str | Path, number: int) -> list[Path]:
+    """Write checkpoint `number` of the device state; returns the files written."""
+    name = str(name)
+    F, DF = gpu.get_fields(True, True)
+    files = []
+    p = Path(f"{name}F.ckpt{number}")
+    np.concatenate([F.reshape(-1), DF.reshape(-1)]).astype(np.float64).tofile(p)
+    files.append(p)
+    for b in range(host.nblocks):
+        for s in range(4):
+            F0 = host.side_array(b, s, "F0")
+            Fh = gpu.get_fhat(b, s)
+            Fe = _edge_values(F, host, b, s)
+            n = F0.shape[1]
+            parts = []
+            for l in range(host.nF):
+                parts += [Fe[l], Fh[l], F0[l]]
+            parts += [np.zeros(n), np.zeros(n)]  # boundary energy E, DE (not tracked)
+            p = Path(f"{name}block{b + 1}{SIDES[s]}.ckpt{number}")
+            np.concatenate(parts).astype(np.float64).tofile(p)
+            files.append(p)
+    for i in range(host.nifaces):
+        if host.iface_info(i)[3] != COUPLING_FRICTION:  # only frictional interfaces carry state
+            continue
+        data = np.concatenate([gpu.get_fault(i, f) for f in FAULT_FIELDS]).astype(np.float64)
+        for side in (1, 2):
+            p = Path(f"{name}iface{i + 1}side{side}.ckpt{number}")
+            data.tofile(p)
+            files.append(p)
+    Path(f"{name}.ckpt").write_text(f"{number}\n")
+    return files
+
+
+def checkpoint_read(gpu, host, name: str | Path, number: int | None = None) -> int:
+    """Load checkpoint `number` (default: the last one recorded) into the device
+    state; returns the checkpoint number (the step the run resumes after)."""
+    name = str(name)
+    if number is None:
+        number = int(Path(f"{name}.ckpt").read_text().split()[0])
+    nn = host.nF * host.ny * host.nx
+    a = np.fromfile(f"{name}F.ckpt{number}", dtype=np.float64)
+    if a.size != 2 * nn:
+        raise ValueError(f"{name}F.ckpt{number}: {a.size} values, expected {2 * nn}")
+    gpu.set_fields(a[:nn].reshape(host.nF, host.ny, host.nx), a[nn:].reshape(host.nF, host.ny, host.nx))
+    for i in range(host.nifaces):
+        if host.iface_info(i)[3] != COUPLING_FRICTION:
+            continue
+        n = host.iface_n(i)
+        d = np.fromfile(f"{name}iface{i + 1}side1.ckpt{number}", dtype=np.float64)
+        if d.size != len(FAULT_FIELDS) * n:
+            raise ValueError(f"interface {i + 1} checkpoint: {d.size} values, expected {len(FAULT_FIELDS) * n}")
+        for k, f in enumerate(FAULT_FIELDS):
+            gpu.set_fault(i, f, d[k * n:(k + 1) * n])
+    return number

@@ -1125,6 +1125,20 @@ extern "C" const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface,
   return which == 0 ? I.x : I.y;
 }
 
+extern "C" const double* fdmap_host_side_array(const fdmap_domain* dom, int block, int side, const char* name,
+                                               long long* count) {
+  if (!dom || !name || block < 0 || block >= dom->desc.nblocks || side < 0 || side > 3) return nullptr;
+  const fdmap_side& S = dom->desc.blocks[block].side[side];
+  const std::string n = name;
+  const double* p = nullptr;
+  long long len = 0;
+  if (n == "F0") { p = S.F0; len = (long long)S.n * dom->desc.nF; }
+  else if (n == "M") { p = S.M; len = (long long)S.n * 5; }
+  else if (n == "normal") { p = S.normal; len = (long long)S.n * 2; }
+  if (p && count) *count = len;
+  return p;
+}
+
 extern "C" int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim) {
   if (!dom || !lim || block < 0 || block >= dom->desc.nblocks) return FDMAP_ERR_INVALID_ARG;
   const fdmap_block& b = dom->desc.blocks[block];

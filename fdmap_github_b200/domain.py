@@ -74,6 +74,17 @@ class HostDomain:
             out.append(np.ctypeslib.as_array(p, shape=(n,)).copy() if p else np.zeros(n))
         return out[0], out[1]
 
+    def side_array(self, b: int, s: int, name: str) -> np.ndarray:
+        """Side array of block b, side s (0..3 = L, R, B, T): "F0" -> (nF, n), "M" -> (5, n), "normal" -> (2, n)."""
+        n = C.c_longlong()
+        p = lib().fdmap_host_side_array(self._h, b, s, name.encode(), C.byref(n))
+        if not p:
+            raise KeyError(name)
+        a = np.ctypeslib.as_array(p, shape=(n.value,)).copy()
+        mgx, pgx, mgy, pgy = self.block_limits(b)
+        side_n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+        return a.reshape(-1, side_n)
+
     def block_limits(self, b: int) -> tuple[int, int, int, int]:
         lim = (C.c_int * 4)()
         check_host(lib().fdmap_host_block_limits(self._h, b, lim), "fdmap_host_block_limits")

@@ -41,6 +41,7 @@ SIGNATURES = {
     "fdmap_host_block_limits": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
     "fdmap_host_iface_info": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
     "fdmap_host_iface_xy": (_DP, [_VP, C.c_int, C.c_int]),
+    "fdmap_host_side_array": (_DP, [_VP, C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_longlong)]),
     "fdmap_host_array": (_DP, [_VP, C.c_char_p, C.POINTER(C.c_longlong)]),
     "fdmap_host_last_error": (C.c_char_p, []),
     # fdmap_gpu.h

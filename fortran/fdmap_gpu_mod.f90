@@ -24,6 +24,8 @@ module fdmap_gpu_mod
        FDMAP_ERR_UNSUPPORTED = -6, FDMAP_ERR_IO = -7, FDMAP_ERR_NOMEM = -8
 
   ! fault fields, in checkpoint_friction order (friction.f90:528-546)
+  integer(c_int), parameter :: FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1
+
   integer(c_int), parameter :: FDMAP_FAULT_D = 0, FDMAP_FAULT_PSI = 1, FDMAP_FAULT_DPSI = 2, &
        FDMAP_FAULT_TRUP = 3, FDMAP_FAULT_V = 4, FDMAP_FAULT_O = 5, FDMAP_FAULT_S = 6, &
        FDMAP_FAULT_N = 7, FDMAP_FAULT_S0 = 8, FDMAP_FAULT_N0 = 9, FDMAP_FAULT_DS = 10, &
@@ -149,6 +151,127 @@ module fdmap_gpu_mod
        import :: c_ptr
        type(c_ptr), value :: h
      end subroutine fdmap_gpu_destroy
+
+     integer(c_int) function fdmap_gpu_set_stream(h, stream) bind(C, name='fdmap_gpu_set_stream')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, stream
+     end function fdmap_gpu_set_stream
+
+     integer(c_int) function fdmap_gpu_get_fhat(h, b, s, out) bind(C, name='fdmap_gpu_get_fhat')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: b, s
+       real(c_double), intent(out) :: out(*)
+     end function fdmap_gpu_get_fhat
+
+     integer(c_int) function fdmap_gpu_fault_max_noalloc(h, iface, field, out) bind(C, name='fdmap_gpu_fault_max_noalloc')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: iface, field
+       real(c_double), intent(out) :: out
+     end function fdmap_gpu_fault_max_noalloc
+
+     ! ---- device-side output (write_output replacement)
+     integer(c_int) function fdmap_gpu_output_add(h, name, kind, index, field, mx, px, sx, my, py, sy, &
+          nmin, nmax, stride) bind(C, name='fdmap_gpu_output_add')
+       import :: c_int, c_ptr, c_char, c_long_long
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: name(*)
+       integer(c_int), value :: kind, index, field, mx, px, sx, my, py, sy, stride
+       integer(c_long_long), value :: nmin, nmax
+     end function fdmap_gpu_output_add
+
+     integer(c_int) function fdmap_gpu_output_open(h, prefix, ring_steps) bind(C, name='fdmap_gpu_output_open')
+       import :: c_int, c_ptr, c_char
+       type(c_ptr), value :: h
+       character(kind=c_char), intent(in) :: prefix(*)
+       integer(c_int), value :: ring_steps
+     end function fdmap_gpu_output_open
+
+     integer(c_int) function fdmap_gpu_output_flush(h) bind(C, name='fdmap_gpu_output_flush')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function fdmap_gpu_output_flush
+
+     integer(c_int) function fdmap_gpu_output_close(h) bind(C, name='fdmap_gpu_output_close')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function fdmap_gpu_output_close
+
+     ! ---- batched ensemble
+     integer(c_int) function fdmap_gpu_ensemble_create(descs, ninst, device, init_edges, e) &
+          bind(C, name='fdmap_gpu_ensemble_create')
+       import :: c_int, c_ptr
+       type(c_ptr), intent(in) :: descs(*)
+       integer(c_int), value :: ninst, device, init_edges
+       type(c_ptr), intent(out) :: e
+     end function fdmap_gpu_ensemble_create
+
+     integer(c_int) function fdmap_gpu_ensemble_instance(e, k, h) bind(C, name='fdmap_gpu_ensemble_instance')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: e
+       integer(c_int), value :: k
+       type(c_ptr), intent(out) :: h
+     end function fdmap_gpu_ensemble_instance
+
+     integer(c_int) function fdmap_gpu_ensemble_run(e, t_start, dt, n_first, n_last, nt) &
+          bind(C, name='fdmap_gpu_ensemble_run')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: e
+       real(c_double), value :: t_start, dt
+       integer(c_int), value :: n_first, n_last, nt
+     end function fdmap_gpu_ensemble_run
+
+     integer(c_int) function fdmap_gpu_ensemble_tune(e, dt, steps, best_shape, best_ms) &
+          bind(C, name='fdmap_gpu_ensemble_tune')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: e
+       real(c_double), value :: dt
+       integer(c_int), value :: steps
+       integer(c_int), intent(out) :: best_shape(3)
+       real(c_double), intent(out) :: best_ms
+     end function fdmap_gpu_ensemble_tune
+
+     subroutine fdmap_gpu_ensemble_destroy(e) bind(C, name='fdmap_gpu_ensemble_destroy')
+       import :: c_ptr
+       type(c_ptr), value :: e
+     end subroutine fdmap_gpu_ensemble_destroy
+
+     ! ---- forward/backward pair (misfit gradient)
+     integer(c_int) function fdmap_gpu_adjoint_create(d, device, nrec, rec_i, rec_j, checkpoint_every, a) &
+          bind(C, name='fdmap_gpu_adjoint_create')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: d
+       integer(c_int), value :: device, nrec, checkpoint_every
+       integer(c_int), intent(in) :: rec_i(*), rec_j(*)
+       type(c_ptr), intent(out) :: a
+     end function fdmap_gpu_adjoint_create
+
+     integer(c_int) function fdmap_gpu_adjoint_set_material(a, rho, G) bind(C, name='fdmap_gpu_adjoint_set_material')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a
+       real(c_double), intent(in) :: rho(*), G(*)
+     end function fdmap_gpu_adjoint_set_material
+
+     integer(c_int) function fdmap_gpu_adjoint_forward(a, t_start, dt, nt, data, traces, misfit) &
+          bind(C, name='fdmap_gpu_adjoint_forward')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a, data, traces
+       real(c_double), value :: t_start, dt
+       integer(c_int), value :: nt
+       real(c_double), intent(out) :: misfit
+     end function fdmap_gpu_adjoint_forward
+
+     integer(c_int) function fdmap_gpu_adjoint_backward(a, grad_rho, grad_G) bind(C, name='fdmap_gpu_adjoint_backward')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a
+       real(c_double), intent(out) :: grad_rho(*), grad_G(*)
+     end function fdmap_gpu_adjoint_backward
+
+     subroutine fdmap_gpu_adjoint_destroy(a) bind(C, name='fdmap_gpu_adjoint_destroy')
+       import :: c_ptr
+       type(c_ptr), value :: a
+     end subroutine fdmap_gpu_adjoint_destroy
 
      ! ---- host initialisation from an FDMAP input text (include/fdmap_host.h)
      integer(c_int) function fdmap_host_init(input_text, base_dir, dom) bind(C, name='fdmap_host_init')

@@ -54,6 +54,10 @@ int fdmap_host_iface_info(const fdmap_domain* dom, int iface, int* info);
 /* Interface geometry: x[n], y[n] of interface `iface` (NULL if absent). */
 const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface, int which);
 
+/* Side arrays of block `block`, side `side` (0..3 = L, R, B, T): "F0" (n, nF),
+ * "M" (n, 5) or "normal" (n, 2); *count receives the length.  NULL if absent. */
+const double* fdmap_host_side_array(const fdmap_domain* dom, int block, int side, const char* name, long long* count);
+
 /* Block index limits: lim[4] = mgx, pgx, mgy, pgy (1-based). */
 int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim);
 
