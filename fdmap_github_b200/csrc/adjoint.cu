@@ -47,6 +47,7 @@ struct fdmap_adjoint {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t copy = nullptr;        // stage-input copies beside the recomputed stage
   cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;
+  AdjMaps maps{};                     // TMA descriptors of the interior adjoint tiles
   double* init_F = nullptr;          // initial fields (3 planes)
   double* init_DF = nullptr;
   double* ckpt = nullptr;            // checkpoints, 3 planes each
@@ -108,9 +109,54 @@ struct fdmap_adjoint {
 
 namespace {
 
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// 3-D FP64 map over `nplanes` planes of the block layout, box {bx, by, bz}
+int adj_encode(EncodeTiledFn enc, CUtensorMap* map, const double* base, const BlockGeom& g, long long nplanes, int bx,
+               int by, int bz) {
+  cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
+  cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_err(FDMAP_ERR_CUDA, "adjoint tensor map (" + std::to_string((int)r) + ")");
+  return FDMAP_OK;
+}
+
+template <int PI_>
+int adj_maps_for(fdmap_adjoint* a) {
+  using T = AdjTile<PI_>;
+  fdmap_gpu* h = a->h;
+  const BlockGeom& g = h->geom[0];
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult qr;
+  CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr));
+  if (!fn || qr != cudaDriverEntryPointSuccess) return set_err(FDMAP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  EncodeTiledFn enc = (EncodeTiledFn)fn;
+  int rc;
+  for (int q = 0; q < 2; ++q) {
+    if ((rc = adj_encode(enc, &a->maps.ub[q], a->ub[q], g, 3, T::WX, T::WY, 3))) return rc;
+    if ((rc = adj_encode(enc, &a->maps.qp[q], a->qp[q], g, 3, T::WX, T::WY, 3))) return rc;
+  }
+  if ((rc = adj_encode(enc, &a->maps.st, a->store, g, 3LL * a->K * h->rk.nstage, T::WX, T::WY, 3))) return rc;
+  if ((rc = adj_encode(enc, &a->maps.met, h->met_base[0], g, 5, T::WX, T::WY, 5))) return rc;
+  if ((rc = adj_encode(enc, &a->maps.het, h->het_base[0], g, 2, T::WX, T::WY, 2))) return rc;
+  CUDA_TRY(cudaFuncSetAttribute(adj_stage_tma<PI_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM + 128));
+  return FDMAP_OK;
+}
+
+int adj_maps(fdmap_adjoint* a) {
+  const int pI = a->h->pI;
+  return pI == 1 ? adj_maps_for<1>(a) : (pI == 2 ? adj_maps_for<2>(a) : adj_maps_for<3>(a));
+}
+
 // interior tiles on the main stream, the band on a side stream (disjoint
-// nodes, same inputs), joined before the next stage
-int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p) {
+// nodes, same inputs), joined before the next stage; q = ubar / qbar' parity
+int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p, int q) {
   fdmap_gpu* h = a->h;
   const DevBlock& B = h->hdom.blk[0];
   dim3 blk(ATX * ATY), grid((B.nx + ATX - 1) / ATX, (B.ny + ATY - 1) / ATY);
@@ -121,13 +167,13 @@ int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p) {
   // are placed before the interior tiles fill the SMs
   if (h->pI == 1) {
     adj_band_kernel<1><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
-    adj_stage_kernel<1><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_stage_tma<1><<<grid, blk, AdjTile<1>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
   } else if (h->pI == 2) {
     adj_band_kernel<2><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
-    adj_stage_kernel<2><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_stage_tma<2><<<grid, blk, AdjTile<2>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
   } else {
     adj_band_kernel<3><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
-    adj_stage_kernel<3><<<grid, blk, 0, h->stream>>>(h->hdom, p);
+    adj_stage_tma<3><<<grid, blk, AdjTile<3>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
   }
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaEventRecord(a->ev_join, a->side));
@@ -225,7 +271,7 @@ int build_graphs(fdmap_adjoint* a, double dt) {
         p.rel = &a->clock->rel;
         p.grho = a->grho;
         p.gG = a->gG;
-        int r = adj_stage_launch(a, p);
+        int r = adj_stage_launch(a, p, q);
         if (r) return r;
         q = 1 - q;
       }
@@ -388,6 +434,7 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
     if (cudaMemcpy(a->geo[s], geo.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(set_err(FDMAP_ERR_CUDA, "geometry upload"));
   }
+  if ((rc = adj_maps(a))) return fail(rc);
   *out = a;
   return FDMAP_OK;
 }

@@ -20,6 +20,7 @@
 // candidate output nodes of an input node are enumerated per direction.
 #pragma once
 
+#include "march_kernel.cuh"
 #include "stencil_kernel.cuh"
 
 namespace fdmap {
@@ -218,12 +219,7 @@ __device__ __forceinline__ void adj_node_generic(const DevDomain& D, const AdjSt
 
 constexpr int ATX = 32, ATY = 8;
 
-// Adjoint stage, 32 x 8 nodes per CTA, for nodes at least nbnd from every side
-// (every output node they gather from, and their own volume rates, use the
-// central stencil).  The tile stages the weighted adjoint rates
-// l_r = qs_r * Ji * (1/rho | G), the metrics and the stage input in shared
-// memory with a PI_-wide halo.  Nodes within nbnd of a side (the band) are
-// left to adj_band_kernel, which runs concurrently on the same inputs.
+
 // nodes within nbnd of a side use closure rows somewhere in their gather or
 // their own rates: the band handled by adj_band_kernel
 __device__ __forceinline__ bool adj_node_interior(int i, int j, int nx, int ny, int nbnd) {
@@ -252,96 +248,6 @@ __global__ void __launch_bounds__(256) adj_band_kernel(const __grid_constant__ D
   int i, j;
   band_node(q, B.nx, B.ny, nbnd_of(PI_), i, j);
   adj_node_generic<PI_>(D, p, i, j);
-}
-
-template <int PI_>
-__global__ void __launch_bounds__(ATX* ATY, 4) adj_stage_kernel(const __grid_constant__ DevDomain D, AdjStage p) {
-  constexpr int H = PI_, WX = ATX + 2 * H, WY = ATY + 2 * H;
-  __shared__ double sL[3][WY][WX];  // weighted adjoint rates
-  __shared__ double sM[4][WY][WX];  // yr, xr, yq, xq
-  __shared__ double sU[3][WY][WX];  // stage input u_{s-1}
-  constexpr int nbnd = nbnd_of(PI_);
-  const DevBlock& B = D.blk[0];
-  const int nx = B.nx, ny = B.ny;
-  const int i0 = blockIdx.x * ATX, j0 = blockIdx.y * ATY;
-  const int tx = threadIdx.x % ATX, ty = threadIdx.x / ATX;
-  // tiles entirely inside the band have no work here
-  if (i0 + ATX - 1 < nbnd || i0 > nx - 1 - nbnd || j0 + ATY - 1 < nbnd || j0 > ny - 1 - nbnd) return;
-  const long long pitch = B.pitch, plane = B.plane;
-  const double* __restrict__ ust = p.store + ((*p.rel) * p.nstage + p.s) * p.stride;
-  for (int q = threadIdx.x; q < WX * WY; q += ATX * ATY) {
-    const int yy = q / WX, xx = q % WX;
-    const int gi = i0 - H + xx, gj = j0 - H + yy;
-    // positions outside the block are never read: an interior node's
-    // neighbours lie within PI_ <= nbnd of it
-    if (gi < 0 || gi >= nx || gj < 0 || gj >= ny) continue;
-    const long long k = (long long)gj * pitch + gi;
-    const double Jk = B.Ji[k], wv = Jk / B.rho[k], ws = Jk * B.G[k];
-    sL[0][yy][xx] = (p.qp_in[k] + p.Bdt * p.ub_in[k]) * wv;
-    sL[1][yy][xx] = (p.qp_in[plane + k] + p.Bdt * p.ub_in[plane + k]) * ws;
-    sL[2][yy][xx] = (p.qp_in[2 * plane + k] + p.Bdt * p.ub_in[2 * plane + k]) * ws;
-    sM[0][yy][xx] = B.yr[k];
-    sM[1][yy][xx] = B.xr[k];
-    sM[2][yy][xx] = B.yq[k];
-    sM[3][yy][xx] = B.xq[k];
-    sU[0][yy][xx] = ust[k];
-    sU[1][yy][xx] = ust[plane + k];
-    sU[2][yy][xx] = ust[2 * plane + k];
-  }
-  __syncthreads();
-  if (!adj_node_interior(i0 + tx, j0 + ty, nx, ny, nbnd)) return;  // band node (adj_band_kernel)
-  const int X0 = tx + H, Y0 = ty + H;
-  const double yrc = sM[0][Y0][X0], xrc = sM[1][Y0][X0], yqc = sM[2][Y0][X0], xqc = sM[3][Y0][X0];
-  double acc[3] = {0.0, 0.0, 0.0};
-  double phi[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-  for (int s = 1; s <= PI_; ++s) {
-    const double w = D.DI[s];
-#pragma unroll
-    for (int side = -1; side <= 1; side += 2) {
-      // q direction: output node X0 + side*s; this node sits at -side*s in its stencil
-      const int xa = X0 + side * s;
-      const double W = -side * w;  // left output (side -1): +DI, right output: -DI
-      const double Y = 0.5 * (sM[0][Y0][xa] + yrc), X = 0.5 * (sM[1][Y0][xa] + xrc);
-      const double l0 = sL[0][Y0][xa], l1 = sL[1][Y0][xa], l2 = sL[2][Y0][xa];
-      acc[1] += W * (Y * l0);
-      acc[2] -= W * (X * l0);
-      acc[0] += W * (Y * l1 - X * l2);
-      // own volume rate: neighbour at side*s with weight side*DI
-      const double u0 = sU[0][Y0][xa], u1 = sU[1][Y0][xa], u2 = sU[2][Y0][xa];
-      const double Wf = side * w;
-      phi[0] += Wf * (Y * u1 - X * u2);
-      phi[1] += Wf * (Y * u0);
-      phi[2] += Wf * (-X * u0);
-      // r direction
-      const int ya = Y0 + side * s;
-      const double Yr = 0.5 * (sM[2][ya][X0] + yqc), Xr = 0.5 * (sM[3][ya][X0] + xqc);
-      const double m0 = sL[0][ya][X0], m1 = sL[1][ya][X0], m2 = sL[2][ya][X0];
-      acc[1] -= W * (Yr * m0);
-      acc[2] += W * (Xr * m0);
-      acc[0] += W * (-Yr * m1 + Xr * m2);
-      const double v0 = sU[0][ya][X0], v1 = sU[1][ya][X0], v2 = sU[2][ya][X0];
-      phi[0] += Wf * (-Yr * v1 + Xr * v2);
-      phi[1] += Wf * (-Yr * v0);
-      phi[2] += Wf * (Xr * v0);
-    }
-  }
-  const int i = i0 + tx, j = j0 + ty;
-  const long long c = (long long)j * pitch + i;
-  double lam[3], ubc[3];
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    ubc[f] = p.ub_in[f * plane + c];
-    lam[f] = p.qp_in[f * plane + c] + p.Bdt * ubc[f];
-  }
-  const double Ji = B.Ji[c], rinv = 1.0 / B.rho[c];
-  p.grho[c] += -lam[0] * (phi[0] * Ji) * (rinv * rinv);
-  p.gG[c] += lam[1] * (phi[1] * Ji) + lam[2] * (phi[2] * Ji);
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    p.ub_out[f * plane + c] = ubc[f] + acc[f];
-    p.qp_out[f * plane + c] = p.A * lam[f];
-  }
 }
 
 // Edge impedance and penalty of a heterogeneous mode III side from the node's
@@ -385,6 +291,133 @@ struct AdjClock {
 __global__ void adj_forward_advance(TimeState* ts, AdjClock* ck) {
   ts->n += 1;
   ck->rel += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Interior adjoint stage, 32 x 8 nodes per CTA, for nodes at least nbnd from
+// every side (every output node they gather from, and their own volume
+// rates, use the central stencil); the band is adj_band_kernel's.  The tile
+// is delivered by TMA: five 3-D boxes
+// (qbar' 3 planes, ubar 3, stage input 3, metrics yr xr yq xq Ji 5, rho G 2)
+// land in shared memory on one mbarrier; the box starts HX = PI_ rounded up
+// to even columns left of the tile so every box starts on a 16-byte boundary.
+// ---------------------------------------------------------------------------
+struct AdjMaps {
+  CUtensorMap ub[2];  // ubar buffers, box {WX, WY, 3}
+  CUtensorMap qp[2];  // qbar' buffers, box {WX, WY, 3}
+  CUtensorMap st;     // stage-input store (3 planes per slot), box {WX, WY, 3}
+  CUtensorMap met;    // yr, xr, yq, xq, Ji, box {WX, WY, 5}
+  CUtensorMap het;    // rho, G, box {WX, WY, 2}
+};
+
+template <int PI_>
+struct AdjTile {
+  static constexpr int HX = (PI_ + 1) & ~1;
+  static constexpr int HY = PI_;
+  static constexpr int WX = ATX + 2 * HX;
+  static constexpr int WY = ATY + 2 * HY;
+  static constexpr int PL = WX * WY;                 // doubles per plane of the tile
+  static constexpr int NPL = 16;                     // qp 3, ub 3, st 3, met 5, het 2
+  static constexpr unsigned BYTES = (unsigned)NPL * PL * 8;  // bytes the five boxes deliver
+  // each box lands on a 128-byte aligned group (offsets in doubles)
+  static constexpr int grp(int planes) { return (planes * PL * 8 + 127) / 128 * 16; }
+  static constexpr int QP = 0, UB = QP + grp(3), ST = UB + grp(3), MET = ST + grp(3), HET = MET + grp(5);
+  static constexpr unsigned SMEM = (unsigned)(HET + grp(2)) * 8;
+};
+
+template <int PI_>
+__global__ void __launch_bounds__(ATX* ATY) adj_stage_tma(const __grid_constant__ DevDomain D, AdjStage p,
+                                                           const __grid_constant__ AdjMaps maps, int q) {
+  using T = AdjTile<PI_>;
+  constexpr int nbnd = nbnd_of(PI_);
+  extern __shared__ unsigned char adj_smem_raw[];
+  double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(adj_smem_raw) + 127) & ~uintptr_t(127));
+  __shared__ unsigned long long bar;
+  const DevBlock& B = D.blk[0];
+  const int nx = B.nx, ny = B.ny;
+  const int i0 = blockIdx.x * ATX, j0 = blockIdx.y * ATY;
+  const int tx = threadIdx.x % ATX, ty = threadIdx.x / ATX;
+  if (i0 + ATX - 1 < nbnd || i0 > nx - 1 - nbnd || j0 + ATY - 1 < nbnd || j0 > ny - 1 - nbnd) return;
+  // P(group, plane, yy, xx): plane `plane` of a box group, tile row yy, column xx
+  auto P = [&](int grp, int plane, int yy, int xx) -> double& { return sm[grp + (plane * T::WY + yy) * T::WX + xx]; };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_proxy_async();
+    const int x = i0 - T::HX, y = j0 - T::HY;
+    const int slot = (int)((*p.rel) * p.nstage + p.s) * 3;
+    mbar_arrive_tx(&bar, T::BYTES);
+    tma_load_3d(&P(T::QP, 0, 0, 0), &maps.qp[q], x, y, 0, &bar);
+    tma_load_3d(&P(T::UB, 0, 0, 0), &maps.ub[q], x, y, 0, &bar);
+    tma_load_3d(&P(T::ST, 0, 0, 0), &maps.st, x, y, slot, &bar);
+    tma_load_3d(&P(T::MET, 0, 0, 0), &maps.met, x, y, 0, &bar);
+    tma_load_3d(&P(T::HET, 0, 0, 0), &maps.het, x, y, 0, &bar);
+  }
+  __syncthreads();
+  mbar_wait_bounded(&bar, 0, D.status);
+  const int X0 = tx + T::HX, Y0 = ty + T::HY;
+  const bool mine = adj_node_interior(i0 + tx, j0 + ty, nx, ny, nbnd);
+  double lam[3], ubc[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    ubc[f] = P(T::UB, f, Y0, X0);
+    lam[f] = P(T::QP, f, Y0, X0) + p.Bdt * ubc[f];
+  }
+  const double Jc = P(T::MET, 4, Y0, X0), rho_c = P(T::HET, 0, Y0, X0);
+  __syncthreads();
+  // weighted adjoint rates l_r = qs_r * Ji * (1/rho | G), in place of qbar'
+  for (int k = threadIdx.x; k < T::PL; k += ATX * ATY) {
+    const int yy = k / T::WX, xx = k % T::WX;
+    const double Jk = P(T::MET, 4, yy, xx), wv = Jk / P(T::HET, 0, yy, xx), ws = Jk * P(T::HET, 1, yy, xx);
+    P(T::QP, 0, yy, xx) = (P(T::QP, 0, yy, xx) + p.Bdt * P(T::UB, 0, yy, xx)) * wv;
+    P(T::QP, 1, yy, xx) = (P(T::QP, 1, yy, xx) + p.Bdt * P(T::UB, 1, yy, xx)) * ws;
+    P(T::QP, 2, yy, xx) = (P(T::QP, 2, yy, xx) + p.Bdt * P(T::UB, 2, yy, xx)) * ws;
+  }
+  __syncthreads();
+  if (!mine) return;  // band node (adj_band_kernel)
+  const double yrc = P(T::MET, 0, Y0, X0), xrc = P(T::MET, 1, Y0, X0), yqc = P(T::MET, 2, Y0, X0),
+               xqc = P(T::MET, 3, Y0, X0);
+  double acc[3] = {0.0, 0.0, 0.0};
+  double phi[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int s = 1; s <= PI_; ++s) {
+    const double w = D.DI[s];
+#pragma unroll
+    for (int side = -1; side <= 1; side += 2) {
+      const int xa = X0 + side * s;
+      const double W = -side * w;  // left output (side -1): +DI, right output: -DI
+      const double Y = 0.5 * (P(T::MET, 0, Y0, xa) + yrc), X = 0.5 * (P(T::MET, 1, Y0, xa) + xrc);
+      const double l0 = P(T::QP, 0, Y0, xa), l1 = P(T::QP, 1, Y0, xa), l2 = P(T::QP, 2, Y0, xa);
+      acc[1] += W * (Y * l0);
+      acc[2] -= W * (X * l0);
+      acc[0] += W * (Y * l1 - X * l2);
+      const double u0 = P(T::ST, 0, Y0, xa), u1 = P(T::ST, 1, Y0, xa), u2 = P(T::ST, 2, Y0, xa);
+      const double Wf = side * w;
+      phi[0] += Wf * (Y * u1 - X * u2);
+      phi[1] += Wf * (Y * u0);
+      phi[2] += Wf * (-X * u0);
+      const int ya = Y0 + side * s;
+      const double Yr = 0.5 * (P(T::MET, 2, ya, X0) + yqc), Xr = 0.5 * (P(T::MET, 3, ya, X0) + xqc);
+      const double m0 = P(T::QP, 0, ya, X0), m1 = P(T::QP, 1, ya, X0), m2 = P(T::QP, 2, ya, X0);
+      acc[1] -= W * (Yr * m0);
+      acc[2] += W * (Xr * m0);
+      acc[0] += W * (-Yr * m1 + Xr * m2);
+      const double v0 = P(T::ST, 0, ya, X0), v1 = P(T::ST, 1, ya, X0), v2 = P(T::ST, 2, ya, X0);
+      phi[0] += Wf * (-Yr * v1 + Xr * v2);
+      phi[1] += Wf * (-Yr * v0);
+      phi[2] += Wf * (Xr * v0);
+    }
+  }
+  const long long pitch = B.pitch, plane = B.plane;
+  const long long c = (long long)(j0 + ty) * pitch + (i0 + tx);
+  const double rinv = 1.0 / rho_c;
+  p.grho[c] += -lam[0] * (phi[0] * Jc) * (rinv * rinv);
+  p.gG[c] += lam[1] * (phi[1] * Jc) + lam[2] * (phi[2] * Jc);
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    p.ub_out[f * plane + c] = ubc[f] + acc[f];
+    p.qp_out[f * plane + c] = p.A * lam[f];
+  }
 }
 
 // end of an adjoint step n: ubar += dJ/dU^n at the receivers, then step back.
