@@ -386,11 +386,18 @@ def run_ensemble(args) -> None:
 
     tmp = Path(tempfile.mkdtemp(prefix=f"fdmap_bench_ens_r{rank}_"))
     n = args.instances
-    hosts = [init_domain(problems.ensemble_instance(tmp, s), tmp) for s in range(n)]
+    from fdmap_github_b200 import init_domains
+
+    t_init = time.perf_counter()
+    hosts = init_domains([problems.ensemble_instance(tmp, s) for s in range(n)], tmp)
+    t_init = time.perf_counter() - t_init
+    t_create = time.perf_counter()
     nodes = sum(h.nx * h.ny for h in hosts)
     dt = min(h.dt for h in hosts)
     run_steps = 1000
     ens = GpuEnsemble(hosts, device=local)
+    ens.synchronize()
+    t_create = time.perf_counter() - t_create
     shape, tune_ms = ens.tune(steps=5, dt=dt)
     ens.run(1, args.warmup, dt=dt, nt=1 << 30)
     ens.synchronize()
@@ -427,7 +434,8 @@ def run_ensemble(args) -> None:
                 "node_updates_per_s": world * nodes / per_step,
                 "sequential_plain": {"runs_per_s": n / (seq / args.steps * run_steps),
                                      "ms_per_step": seq / args.steps * 1e3},
-                "speedup_vs_sequential": seq / el, "clocks": clocks.summary(), "gpu_launches": launches}
+                "speedup_vs_sequential": seq / el, "host_init_s": t_init, "ensemble_create_s": t_create,
+                "clocks": clocks.summary(), "gpu_launches": launches}
         print(json.dumps(line), flush=True)
 
 

@@ -7,7 +7,7 @@ Public Python surface (a mirror of the reference's host interface):
   GpuAdjoint                          -- misfit gradient (forward/backward pair)
   FdmapError                          -- raised on any non-zero status
 """
-from .domain import GpuAdjoint, GpuDomain, GpuEnsemble, HostDomain, init_domain  # noqa: F401
+from .domain import GpuAdjoint, GpuDomain, GpuEnsemble, HostDomain, init_domain, init_domains  # noqa: F401
 from .native import FAULT_FIELDS, FdmapError  # noqa: F401
 
-__all__ = ["init_domain", "HostDomain", "GpuDomain", "GpuEnsemble", "GpuAdjoint", "FdmapError", "FAULT_FIELDS"]
+__all__ = ["init_domain", "init_domains", "HostDomain", "GpuDomain", "GpuEnsemble", "GpuAdjoint", "FdmapError", "FAULT_FIELDS"]

@@ -107,6 +107,17 @@ def init_domain(input_text: str, base_dir: str | Path | None = None) -> HostDoma
     return HostDomain(input_text, base_dir)
 
 
+def init_domains(input_texts: list[str], base_dir: str | Path | None = None, threads: int | None = None) -> list[HostDomain]:
+    """Initialise many independent domains (an ensemble's instances) on a pool
+    of host threads; the native initialisation releases the interpreter lock."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+
+    n = threads or min(len(input_texts), os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=max(1, n)) as ex:
+        return list(ex.map(lambda t: HostDomain(t, base_dir), input_texts))
+
+
 class GpuDomain:
     """Device-resident copy of a domain, advanced by the sm_100a kernels."""
 
