@@ -49,6 +49,8 @@ struct DevBlock {
   DevSide side[4];
   int src_ok, src_i0, src_j0;          // block-local source indices
   double src_wx[5], src_wy[5];         // singular_source weights d for i0-2..i0+2
+  double Cdiss;                        // scaled artificial dissipation (0: none)
+  double* J;                           // Jacobian plane (dissipative blocks only)
   int tile_begin;                      // first stencil tile of this block
   int tiles_x;
   long long march_unit_begin;          // first row-group unit of this block (march kernel)
@@ -94,6 +96,8 @@ struct DevDomain {
   int nbst, nbnd, pI;
   double DI[4];     // DI[s], s = 1..pI (fd_coeff.f90)
   double DL[6][9];  // DL[r][s]: weight of point s for the derivative at boundary node r
+  double AI[4];     // artificial dissipation AI(s), s = 0..pI (fd_coeff.f90)
+  double AL[6][9];  // AL[r][s]: dissipation weight of point s at boundary node r (AR mirrors it)
   DevBlock blk[MAX_BLOCKS];
   DevIface ifc[MAX_IFACES];
   // closure strips of every block (bottom, top, left, right): thread offsets

@@ -59,6 +59,7 @@ struct fdmap_gpu {
   long long march_units = 0;
   int march_grid = 0;
   int use_march = 1;
+  bool dissipation = false;  // some block has Cdiss > 0 (tiled interior kernel)
   int fused = 0;  // boundary kernel handles interface solves and closure strips in one launch
   // CUDA graphs of one full step, one per starting F buffer, replayed by fdmap_gpu_run
   TimeState* d_time = nullptr;

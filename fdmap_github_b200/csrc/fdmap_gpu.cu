@@ -369,6 +369,10 @@ int validate(const fdmap_desc* d) {
     int nx = B.pgx - B.mgx + 1, ny = B.pgy - B.mgy + 1;
     if (B.mgx < 1 || B.mgy < 1 || B.pgx > d->nx || B.pgy > d->ny)
       return set_err(FDMAP_ERR_INVALID_ARG, "block index limits outside the domain");
+    if (B.Cdiss > 0.0 && (!d->J || d->heterogeneous))
+      return set_err(d->J ? FDMAP_ERR_UNSUPPORTED : FDMAP_ERR_INVALID_ARG,
+                     d->J ? "artificial dissipation in heterogeneous blocks is not supported"
+                          : "artificial dissipation needs the Jacobian array J");
     if (nx < 2 * op.nbst || ny < 2 * op.nbst || nx < op.nbnd || ny < op.nbnd)
       return set_err(FDMAP_ERR_UNSUPPORTED, "block too small for the SBP boundary closures");
     for (int s = 0; s < 4; ++s) {
@@ -412,6 +416,9 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   for (int s = 0; s <= op.pI; ++s) D.DI[s] = op.DI[s];
   for (int r = 0; r < op.nbst; ++r)
     for (int s = 0; s < op.nbnd; ++s) D.DL[r][s] = op.DL[r][s];
+  for (int s = 0; s <= op.pI; ++s) D.AI[s] = op.AI[s];
+  for (int r = 0; r < op.nbst; ++r)
+    for (int s = 0; s < op.nbnd; ++s) D.AL[r][s] = op.AL[r][s];
   D.src = d->src;
   const int nF = d->nF;
   int tiles = 0;
@@ -451,6 +458,13 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       h->het_base[b] = het_base;
     }
     B.rho_b = fb.rho; B.G_b = fb.G; B.M_b = fb.M; B.gamma_b = fb.gamma; B.nu_b = fb.nu;
+    B.Cdiss = fb.Cdiss;
+    B.J = nullptr;
+    if (fb.Cdiss > 0.0) {  // the dissipation term weights neighbours by J itself
+      if ((rc = h->alloc_planes(&B.J, 1, g.plane))) return rc;
+      if ((rc = h->upload_plane(B.J, d->J, g))) return rc;
+      h->dissipation = true;
+    }
     B.rinv_b = 1.0 / fb.rho;
     for (int s = 1; s <= op.pI; ++s) {
       B.coef[s][0] = op.DI[s] / fb.rho;
@@ -579,7 +593,8 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   int rc;
   {
     const char* ek = getenv("FDMAP_STENCIL");
-    h->use_march = !(ek && std::string(ek) == "tile");
+    // dissipative blocks need J at the neighbours, which the march ring does not carry
+    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation;
     if (h->use_march && (rc = march_dispatch(h, nullptr))) return rc;
     // fused stage launches need every interface-side node to sit on one interface only
     bool junction = false;

@@ -312,6 +312,7 @@ struct BlockIn {
   std::string medium_file;
   double rho = 0, G = 0, cs = 0, cp = 0, M = 0, gamma = 0, nu = 0, Zs = 0, Zp = 0;
   double F0v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double Cdiss = 0;  // operator_list (domain.f90:172-180), scaled by CFL/dt after set_dt
   Curve curve[4];
   SideStore side[4];
 };
@@ -557,7 +558,7 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     size_t mk = seek_marker(text, "!---BLOCK" + std::to_string(b + 1) + "---");
     if (mk == std::string::npos) fail(FDMAP_ERR_INVALID_ARG, "String '!---BLOCK" + std::to_string(b + 1) + "---' not found in file");
     Namelist ol = read_nml(text, mk, "operator_list");
-    if (get_real(ol, "cdiss", 0.0) > 0.0) fail(FDMAP_ERR_UNSUPPORTED, "artificial dissipation (Cdiss>0) is not supported");
+    B.Cdiss = get_real(ol, "cdiss", 0.0);
     Namelist gl = read_nml(text, mk, "grid_list");
     B.nx = get_int(gl, "nx", 1);
     B.ny = get_int(gl, "ny", 1);
@@ -847,6 +848,7 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     fdmap_block& fb = dom.blocks[b];
     fb.mgx = B.mgx; fb.pgx = B.pgx; fb.mgy = B.mgy; fb.pgy = B.pgy;
     fb.rho = B.rho; fb.cs = B.cs; fb.cp = B.cp; fb.G = B.G; fb.M = B.M; fb.gamma = B.gamma; fb.nu = B.nu;
+    fb.Cdiss = B.Cdiss;
     for (int q = 0; q < 9; ++q) fb.F0[q] = B.F0v[q];
     for (int s = 0; s < 4; ++s) {
       fdmap_side& fs = fb.side[s];
@@ -900,6 +902,14 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
   if (nt == 0) nt = (int)std::ceil(tend / dt);
   else nt = (int)std::ceil((double)(nt - 1) * refine) + 1;
   d.t0 = t0; d.dt = dt; d.CFL = CFL; d.nt = nt; d.hmin = hmin; d.hmax = hmax;
+  // artificial dissipation scaled as (wave speed)/(grid spacing) (domain.f90:317-320)
+  for (int b = 0; b < nblocks; ++b) {
+    BlockIn& B = dom.bin[b];
+    if (B.Cdiss > 0.0 && B.heterogeneous)
+      fail(FDMAP_ERR_UNSUPPORTED, "artificial dissipation in a heterogeneous block is not supported");
+    B.Cdiss = B.Cdiss * CFL / dt;
+    dom.blocks[b].Cdiss = B.Cdiss;
+  }
 
   // ---- interfaces (get_iface_neighbors, init_iface, init_iface_blocks, init_friction,
   //      init_thermpres; domain.f90:1648-1682, interfaces.f90:26-278, friction.f90:55-317)
@@ -1137,6 +1147,11 @@ extern "C" const double* fdmap_host_side_array(const fdmap_domain* dom, int bloc
   else if (n == "normal") { p = S.normal; len = (long long)S.n * 2; }
   if (p && count) *count = len;
   return p;
+}
+
+extern "C" double fdmap_host_block_cdiss(const fdmap_domain* dom, int block) {
+  if (!dom || block < 0 || block >= dom->desc.nblocks) return FDMAP_ERR_INVALID_ARG;
+  return dom->desc.blocks[block].Cdiss;
 }
 
 extern "C" int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim) {

@@ -150,6 +150,36 @@ __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock
       qterm(c - s, D.DI[s], -1);
     }
   }
+  if (B.Cdiss > 0.0) {
+    // artificial dissipation (rates_dissipation_boundary_mode2/3, rates.f90:1002-1394,
+    // 1485-2021): J-weighted AL rows (AR mirrors AL without a sign change) in a
+    // one-sided direction, AI in a central one, and AI(0)*F once per central direction
+    const double Cd = B.Cdiss;
+    auto diss = [&](long long k, double wa) {
+      const double Jk = B.J[k];
+#pragma unroll
+      for (int l = 0; l < NR; ++l) acc[l] += Jk * Fin[l * plane + k] * wa * Ji * Cd;
+    };
+    if (qreg >= 0) {
+#pragma unroll
+      for (int s = 0; s < nbnd; ++s)
+        diss((long long)j * pitch + (qreg == 0 ? s : nx - 1 - s), qreg == 0 ? D.AL[i][s] : D.AL[nx - 1 - i][s]);
+    } else {
+#pragma unroll
+      for (int s = 1; s <= PI_; ++s) { diss(c + s, D.AI[s]); diss(c - s, D.AI[s]); }
+    }
+    if (rreg >= 0) {
+#pragma unroll
+      for (int s = 0; s < nbnd; ++s)
+        diss((long long)(rreg == 0 ? s : ny - 1 - s) * pitch + i, rreg == 0 ? D.AL[j][s] : D.AL[ny - 1 - j][s]);
+    } else {
+#pragma unroll
+      for (int s = 1; s <= PI_; ++s) { diss(c + s * pitch, D.AI[s]); diss(c - s * pitch, D.AI[s]); }
+    }
+    const double ncentral = (qreg < 0 ? 1.0 : 0.0) + (rreg < 0 ? 1.0 : 0.0);
+#pragma unroll
+    for (int l = 0; l < NR; ++l) acc[l] += ncentral * D.AI[0] * Cd * Fin[l * plane + c];
+  }
 }
 
 // Hat variables of an outer-boundary node depend only on the node's own fields
@@ -356,6 +386,7 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
   __shared__ double sF[NR][WY][WX];
   __shared__ double s_yr[TY][WX], s_xr[TY][WX];
   __shared__ double s_yq[WY][TX], s_xq[WY][TX];
+  __shared__ double s_Jr[TY][WX], s_Jq[WY][TX];  // Jacobian halos (dissipative blocks)
 
   const DevDomain& D = *Dp;
   int b = 0;
@@ -394,6 +425,19 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
       long long g = (long long)gj * pitch + gi;
       s_yq[ty][tx] = B.yq[g];
       s_xq[ty][tx] = B.xq[g];
+    }
+  }
+  const bool diss = B.Cdiss > 0.0;
+  if (diss) {
+    for (int idx = tid; idx < WX * TY; idx += TX * TY) {
+      int ty = idx / WX, tx = idx % WX;
+      int gi = i0 + tx - H, gj = j0 + ty;
+      if (gi >= 0 && gi < nx && gj < ny) s_Jr[ty][tx] = B.J[(long long)gj * pitch + gi];
+    }
+    for (int idx = tid; idx < TX * WY; idx += TX * TY) {
+      int ty = idx / TX, tx = idx % TX;
+      int gi = i0 + tx, gj = j0 + ty - H;
+      if (gi < nx && gj >= 0 && gj < ny) s_Jq[ty][tx] = B.J[(long long)gj * pitch + gi];
     }
   }
   __syncthreads();
@@ -455,6 +499,21 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
         }
         const double cf = HET ? mat_coef(m, RD::coef(r), w) : B.coef[s][RD::coef(r)];
         acc[r] += sum * cf * Ji;
+      }
+    }
+    if (diss) {
+      // artificial dissipation (rates_dissipation_interior_mode2/3, rates.f90:939-999,
+      // 1397-1482): 2*AI(0)*F + sum_s AI(s)*Ji*(J F at the four neighbours at distance s)
+      const double Cd = B.Cdiss;
+#pragma unroll
+      for (int l = 0; l < NR; ++l) {
+        double sum = 2.0 * D.AI[0] * Cd * sF[l][cy][cx];
+#pragma unroll
+        for (int s = 1; s <= PI_; ++s)
+          sum += D.AI[s] * Cd * Ji *
+                 (s_Jr[ty][cx + s] * sF[l][cy][cx + s] + s_Jr[ty][cx - s] * sF[l][cy][cx - s] +
+                  s_Jq[cy + s][tx] * sF[l][cy + s][cx] + s_Jq[cy - s][tx] * sF[l][cy - s][cx]);
+        acc[l] += sum;
       }
     }
   }

@@ -85,6 +85,13 @@ class HostDomain:
         side_n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
         return a.reshape(-1, side_n)
 
+    def block_cdiss(self, b: int) -> float:
+        """Artificial dissipation coefficient of block b, scaled by CFL/dt (0 = none)."""
+        v = lib().fdmap_host_block_cdiss(self._h, b)
+        if v < 0:
+            check_host(int(v), "fdmap_host_block_cdiss")
+        return v
+
     def block_limits(self, b: int) -> tuple[int, int, int, int]:
         lim = (C.c_int * 4)()
         check_host(lib().fdmap_host_block_limits(self._h, b, lim), "fdmap_host_block_limits")

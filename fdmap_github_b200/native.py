@@ -39,6 +39,7 @@ SIGNATURES = {
     "fdmap_host_info": (C.c_int, [_VP, C.POINTER(C.c_int), _DP]),
     "fdmap_host_iface_n": (C.c_int, [_VP, C.c_int]),
     "fdmap_host_block_limits": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
+    "fdmap_host_block_cdiss": (C.c_double, [_VP, C.c_int]),
     "fdmap_host_iface_info": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
     "fdmap_host_iface_xy": (_DP, [_VP, C.c_int, C.c_int]),
     "fdmap_host_side_array": (_DP, [_VP, C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_longlong)]),

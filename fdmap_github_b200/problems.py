@@ -23,30 +23,36 @@ def _f(x: float) -> str:
     return repr(float(x)).replace("e", "d") if "e" in repr(float(x)) else repr(float(x)) + "d0"
 
 
+def _operator(cdiss: float) -> str:
+    """operator_list of a block: artificial dissipation coefficient (domain.f90:89)."""
+    return f"&operator_list Cdiss={_f(cdiss)} /\n" if cdiss > 0 else ""
+
+
 def antiplane_pulse(n: int = 201, L: float = 10.0, nt: int = 501, rk: int = 4, cfl: float = 0.5,
-                    fd: str = "SBP4", sigma: float = 0.5, amp: float = 1.0) -> str:
+                    fd: str = "SBP4", sigma: float = 0.5, amp: float = 1.0, cdiss: float = 0.0) -> str:
     """Mode III SH wave from a Gaussian velocity pulse at the centre of an L x L km
-    block of n x n nodes, absorbing SAT boundaries on all sides."""
+    block of n x n nodes, absorbing SAT boundaries on all sides; optional
+    artificial dissipation `cdiss`."""
     c = 0.5 * L
     return f"""&problem_list name='antiplane_pulse', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
 &domain_list mode=3, FDmethod='{fd}', nblocks_x=1, nblocks_y=1 /
 !---BLOCK1---
 &grid_list nx={n}, ny={n}, LB=0d0,0d0, LT=0d0,{_f(L)}, RB={_f(L)},0d0, RT={_f(L)},{_f(L)} /
 &boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='absorbing' /
-&material_list rho=2.67d0, cs=3.464d0 /
+{_operator(cdiss)}&material_list rho=2.67d0, cs=3.464d0 /
 &fields_list P5%shape='gaussian', P5%x0={_f(c)}, P5%y0={_f(c)}, P5%Lx={_f(sigma)}, P5%Ly={_f(sigma)}, P5%vz={_f(amp)} /
 """
 
 
 def rupture_sw(nx: int = 1601, ny: int = 801, h: float = 0.025, nt: int = 4001, rk: int = 4, cfl: float = 0.5,
-               fd: str = "SBP4", patch_half_width: float = 1.5) -> str:
+               fd: str = "SBP4", patch_half_width: float = 1.5, cdiss: float = 0.0) -> str:
     """Mode II dynamic rupture on a planar fault y = 0 between two blocks of
     nx x ny nodes (spacing h km), linear slip-weakening friction, uniform
     prestress syy = -110 MPa, sxy = 65 MPa, and an 80 MPa nucleation patch."""
     Lx = (nx - 1) * h
     Ly = (ny - 1) * h
     x0, x1 = -0.5 * Lx, 0.5 * Lx
-    blk = """&material_list rho=2.67d0, cs=3.464d0, cp=6d0 /
+    blk = _operator(cdiss) + """&material_list rho=2.67d0, cs=3.464d0, cp=6d0 /
 &fields_list syy0=-110d0, sxy0=65d0 /
 """
     return f"""&problem_list name='rupture_sw', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /

@@ -44,6 +44,7 @@ module fdmap_gpu_mod
      type(fdmap_side_t) :: side(4)
      integer(c_int) :: src_ok, src_i0, src_j0
      real(c_double) :: src_hx, src_hy, src_ax, src_ay
+     real(c_double) :: Cdiss
   end type fdmap_block_t
 
   type, bind(C) :: fdmap_friction_t

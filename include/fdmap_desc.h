@@ -132,6 +132,9 @@ typedef struct fdmap_block {
    * search results; src_ok=0 when the source point lies outside this block */
   int src_ok, src_i0, src_j0;
   double src_hx, src_hy, src_ax, src_ay;
+  /* artificial dissipation coefficient of the block, already scaled by CFL/dt
+   * (operator_list Cdiss, domain.f90:172-180, 319); 0 = no dissipation */
+  double Cdiss;
 } fdmap_block;
 
 /* friction state and parameters of one interface (fr_type, friction.f90:38-49) */

@@ -58,6 +58,10 @@ const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface, int which)
  * "M" (n, 5) or "normal" (n, 2); *count receives the length.  NULL if absent. */
 const double* fdmap_host_side_array(const fdmap_domain* dom, int block, int side, const char* name, long long* count);
 
+/* Scaled artificial dissipation coefficient of block `block` (Cdiss*CFL/dt,
+ * domain.f90:317-320), or a negative code for a bad index. */
+double fdmap_host_block_cdiss(const fdmap_domain* dom, int block);
+
 /* Block index limits: lim[4] = mgx, pgx, mgy, pgy (1-based). */
 int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim);
 

@@ -27,6 +27,8 @@ struct Ops {
   int nbnd, nbst, pI;
   double DI[4];     // DI(s), s = 1..pI
   double DL[6][9];  // DL(s,r) at [r][s]
+  double AI[4];     // AI(s), s = 0..pI (artificial dissipation, symmetric)
+  double AL[6][9];  // AL(s,r) at [r][s]; AR(-s,-r) = AL(s,r) (fd_coeff.f90:244)
 };
 
 bool make_ops(int method, Ops* o) {
@@ -35,6 +37,8 @@ bool make_ops(int method, Ops* o) {
     o->nbnd = 2; o->nbst = 1; o->pI = 1;
     o->DI[1] = 0.5;
     o->DL[0][0] = -1.0; o->DL[0][1] = 1.0;
+    o->AI[0] = -1.0; o->AI[1] = 0.5;
+    o->AL[0][0] = -1.0; o->AL[0][1] = 1.0;
     return true;
   }
   if (method == FDMAP_SBP4) {
@@ -45,6 +49,12 @@ bool make_ops(int method, Ops* o) {
                       {0.093023255813953, -0.686046511627907, 0.0, 0.686046511627907, -0.093023255813953, 0.0},
                       {0.030612244897959, 0.0, -0.602040816326531, 0.0, 0.653061224489796, -0.081632653061224}};
     for (int r = 0; r < 4; ++r) for (int s = 0; s < 6; ++s) o->DL[r][s] = t[r][s];
+    o->AI[0] = -0.500000000000000; o->AI[1] = 0.333333333333333; o->AI[2] = -0.083333333333333;
+    double a[4][6] = {{-0.470588235294118, 0.941176470588235, -0.470588235294118, 0.0, 0.0, 0.0},
+                      {0.271186440677966, -0.610169491525424, 0.406779661016949, -0.067796610169492, 0.0, 0.0},
+                      {-0.186046511627907, 0.558139534883721, -0.651162790697674, 0.372093023255814, -0.093023255813953, 0.0},
+                      {0.0, -0.081632653061224, 0.326530612244898, -0.489795918367347, 0.326530612244898, -0.081632653061224}};
+    for (int r = 0; r < 4; ++r) for (int s = 0; s < 6; ++s) o->AL[r][s] = a[r][s];
     return true;
   }
   if (method == FDMAP_SBP6) {
@@ -58,6 +68,15 @@ bool make_ops(int method, Ops* o) {
         {-0.036210680656541, 0.105400944933782, 0.015764336127392, -0.707905442575989, 0.0, 0.769199413962647, -0.164529643265203, 0.018281071473911, 0},
         {-0.011398193015050, 0.020437334208704, 0.011220896474665, 0.063183694641876, -0.691649024426814, 0.0, 0.739709139060752, -0.147941827812150, 0.016437980868017}};
     for (int r = 0; r < 6; ++r) for (int s = 0; s < 9; ++s) o->DL[r][s] = t[r][s];
+    o->AI[0] = -0.333333333333333; o->AI[1] = 0.25; o->AI[2] = -0.1; o->AI[3] = 0.016666666666667;
+    double a[6][9] = {
+        {-0.105502234595941, 0.316506703787823, -0.316506703787823, 0.105502234595941, 0, 0, 0, 0, 0},
+        {0.071922084408557, -0.227753267293765, 0.251727295429951, -0.107883126612836, 0.011987014068093, 0, 0, 0, 0},
+        {-0.159350793065290, 0.557727775728513, -0.743637034304685, 0.478052379195869, -0.159350793065290, 0.026558465510882, 0, 0, 0},
+        {0.026870684829259, -0.120918081731666, 0.241836163463333, -0.282142190707221, 0.201530136219444, -0.080612054487778, 0.013435342414630, 0, 0},
+        {0.0, 0.018281071473911, -0.109686428843468, 0.274216072108671, -0.365621429478228, 0.274216072108671, -0.109686428843468, 0.018281071473911, 0},
+        {0.0, 0.0, 0.016437980868017, -0.098627885208100, 0.246569713020251, -0.328759617360334, 0.246569713020251, -0.098627885208100, 0.016437980868017}};
+    for (int r = 0; r < 6; ++r) for (int s = 0; s < 9; ++s) o->AL[r][s] = a[r][s];
     return true;
   }
   return false;
@@ -128,6 +147,7 @@ struct Blk {
   Side side[4];
   int src_ok, src_i0, src_j0;
   double src_hx, src_hy, src_ax, src_ay;
+  double Cdiss;  // scaled artificial dissipation (0: set_rates, >0: set_rates_dissipation)
 };
 
 struct Fric {
@@ -151,7 +171,7 @@ struct oracle_domain {
   RK rk;
   std::vector<Blk> blk;
   std::vector<Ifc> ifc;
-  vec F, DF, x, y, xq, xr, yq, yr, Ji;
+  vec F, DF, x, y, xq, xr, yq, yr, J, Ji;
   vec rho, G, M, gamma, nu;
   fdmap_source src;
   double t;
@@ -923,20 +943,147 @@ void rates_boundary(Ctx& c, const Blk& B, int mx, int px, int my, int py, int qs
     }
 }
 
+// ---------------------------------------------------------------------------
+// Rates with artificial dissipation (set_rates_dissipation, time_step.f90:555-751;
+// rates_dissipation_*_mode2/3, rates.f90:939-2021), homogeneous blocks.
+// ---------------------------------------------------------------------------
+// interior (rates.f90:939-999 mode III, 1397-1482 mode II)
+void rates_dissipation_interior(Ctx& c, const Blk& B, int mx, int px, int my, int py) {
+  oracle_domain& D = *c.D;
+  const Ops& op = D.op;
+  const double Cd = B.Cdiss;
+  double dco[4] = {0.0, 0.0, 0.0, 0.0};  // c(s) / d(s): AI(s)*Cdiss; zero beyond pI
+  for (int s = 1; s <= op.pI; ++s) dco[s] = op.AI[s] * Cd;
+  dco[0] = 2.0 * op.AI[0] * Cd;  // used for both the q and the r derivative
+  const int nf = c.nr;             // mode II: fields 1..5 (szz is set by rates_szz)
+#pragma omp parallel for schedule(static)
+  for (int j = my; j <= py; ++j)
+    for (int i = mx; i <= px; ++i) {
+      size_t g = G2(D, i, j);
+      double gmm = gam(c, B, g);
+      for (int l = 0; l < nf; ++l) D.DF[g + c.NN * l] = D.DF[g + c.NN * l] + dco[0] * D.F[g + c.NN * l];
+      for (int s = 1; s <= op.pI; ++s) {
+        size_t qp = G2(D, i + s, j), qm = G2(D, i - s, j), rp = G2(D, i, j + s), rm = G2(D, i, j - s);
+        for (int r = 0; r < c.nr; ++r) {
+          const RateDef& rd = c.defs[r];
+          double T = 0;
+          bool first = true;
+          add_flux(c, rd, true, +1, g, qp, gmm, T, first);
+          add_flux(c, rd, true, -1, g, qm, gmm, T, first);
+          add_flux(c, rd, false, +1, g, rp, gmm, T, first);
+          add_flux(c, rd, false, -1, g, rm, gmm, T, first);
+          double a = rd.coef == 0 ? op.DI[s] / B.rho : (rd.coef == 1 ? op.DI[s] * B.G : op.DI[s] * B.M);
+          size_t off = c.NN * r;
+          double S = D.J[qp] * D.F[qp + off] + D.J[qm] * D.F[qm + off] + D.J[rp] * D.F[rp + off] +
+                     D.J[rm] * D.F[rm + off];
+          double Ji = D.Ji[g];
+          if (D.mode == 3) D.DF[g + off] = D.DF[g + off] + T * a * Ji + dco[s] * Ji * S;
+          else D.DF[g + off] = D.DF[g + off] + (a * T + dco[s] * S) * Ji;
+        }
+      }
+    }
+}
+
+// one-sided dissipation weight at node idx: AL(s, idx-m) at the minus end,
+// AR(-s, idx-p) = AL(s, p-idx) at the plus end
+inline double onesided_diss(const Ops& op, int side, int idx, int m, int p, int s) {
+  return side == 0 ? op.AL[idx - m][s] : op.AL[p - idx][s];
+}
+
+// boundary strips and corners (rates.f90:1002-1394 mode III, 1485-2021 mode II)
+void rates_dissipation_boundary(Ctx& c, const Blk& B, int mx, int px, int my, int py, int qside, int rside) {
+  oracle_domain& D = *c.D;
+  const Ops& op = D.op;
+  const double Cd = B.Cdiss;
+  const int nF = D.nF;  // DF(i,j,:) covers every field (szz is overwritten by rates_szz)
+#pragma omp parallel for schedule(static)
+  for (int j = my; j <= py; ++j)
+    for (int i = mx; i <= px; ++i) {
+      size_t g = G2(D, i, j);
+      double gmm = gam(c, B, g);
+      const double Ji = D.Ji[g];
+      auto rates_at = [&](bool qdir, size_t k, double w) {
+        for (int r = 0; r < c.nr; ++r) {
+          const RateDef& rd = c.defs[r];
+          double acc = 0; bool first = true;
+          add_flux(c, rd, qdir, +1, g, k, gmm, acc, first);
+          D.DF[g + c.NN * r] = D.DF[g + c.NN * r] + bscale(c, B, g, rd.coef, acc, w);
+        }
+      };
+      auto diss_at = [&](size_t k, double wa) {
+        for (int l = 0; l < nF; ++l)
+          D.DF[g + c.NN * l] = D.DF[g + c.NN * l] + D.J[k] * D.F[k + c.NN * l] * wa * Ji * Cd;
+      };
+      if (qside >= 0 && rside >= 0) {
+        // corners: per s, q rates + dissipation, then r rates + dissipation; no AI(0) term
+        for (int s = 0; s < op.nbnd; ++s) {
+          double wq, wr;
+          int pq, pr;
+          onesided(op, qside, i, B.mgx, B.pgx, s, wq, pq);
+          onesided(op, rside, j, B.mgy, B.pgy, s, wr, pr);
+          size_t kq = G2(D, pq, j), kr = G2(D, i, pr);
+          rates_at(true, kq, wq);
+          diss_at(kq, onesided_diss(op, qside, i, B.mgx, B.pgx, s));
+          rates_at(false, kr, wr);
+          diss_at(kr, onesided_diss(op, rside, j, B.mgy, B.pgy, s));
+        }
+        continue;
+      }
+      bool qone = qside >= 0;
+      for (int s = 0; s < op.nbnd; ++s) {
+        double w; int pt;
+        double wa;
+        if (qone) { onesided(op, qside, i, B.mgx, B.pgx, s, w, pt); wa = onesided_diss(op, qside, i, B.mgx, B.pgx, s); }
+        else { onesided(op, rside, j, B.mgy, B.pgy, s, w, pt); wa = onesided_diss(op, rside, j, B.mgy, B.pgy, s); }
+        size_t k = qone ? G2(D, pt, j) : G2(D, i, pt);
+        rates_at(qone, k, w);
+        diss_at(k, wa);
+      }
+      for (int l = 0; l < nF; ++l) D.DF[g + c.NN * l] = D.DF[g + c.NN * l] + D.F[g + c.NN * l] * op.AI[0] * Cd;
+      for (int s = 1; s <= op.pI; ++s) {
+        size_t kp = qone ? G2(D, i, j + s) : G2(D, i + s, j);
+        size_t km = qone ? G2(D, i, j - s) : G2(D, i - s, j);
+        for (int r = 0; r < c.nr; ++r) {
+          const RateDef& rd = c.defs[r];
+          double acc = 0; bool first = true;
+          add_flux(c, rd, !qone, +1, g, kp, gmm, acc, first);
+          add_flux(c, rd, !qone, -1, g, km, gmm, acc, first);
+          D.DF[g + c.NN * r] = D.DF[g + c.NN * r] + bscale(c, B, g, rd.coef, acc, op.DI[s]);
+        }
+        for (int l = 0; l < nF; ++l)
+          D.DF[g + c.NN * l] =
+              D.DF[g + c.NN * l] + (D.J[kp] * D.F[kp + c.NN * l] + D.J[km] * D.F[km + c.NN * l]) * op.AI[s] * Ji * Cd;
+      }
+    }
+}
+
 // set_rates (time_step.f90:318-552) for one block
 void set_rates(oracle_domain& D, const Blk& B) {
   Ctx c{&D, D.mode == 2 ? kMode2 : kMode3, D.mode == 2 ? 5 : 3, (size_t)D.nx * D.ny};
   int nbst = D.op.nbst;
   int mix = B.mgx + nbst, pix = B.pgx - nbst, miy = B.mgy + nbst, piy = B.pgy - nbst;
-  rates_interior(c, B, mix, pix, miy, piy);
-  rates_boundary(c, B, B.mgx, mix - 1, miy, piy, 0, -1);        // L
-  rates_boundary(c, B, pix + 1, B.pgx, miy, piy, 1, -1);        // R
-  rates_boundary(c, B, mix, pix, B.mgy, miy - 1, -1, 0);        // B
-  rates_boundary(c, B, mix, pix, piy + 1, B.pgy, -1, 1);        // T
-  rates_boundary(c, B, B.mgx, mix - 1, B.mgy, miy - 1, 0, 0);   // LB
-  rates_boundary(c, B, pix + 1, B.pgx, B.mgy, miy - 1, 1, 0);   // RB
-  rates_boundary(c, B, B.mgx, mix - 1, piy + 1, B.pgy, 0, 1);   // LT
-  rates_boundary(c, B, pix + 1, B.pgx, piy + 1, B.pgy, 1, 1);   // RT
+  if (B.Cdiss > 0.0) {
+    // set_rates_dissipation: the same regions, dissipative rate routines
+    rates_dissipation_interior(c, B, mix, pix, miy, piy);
+    rates_dissipation_boundary(c, B, B.mgx, mix - 1, miy, piy, 0, -1);        // L
+    rates_dissipation_boundary(c, B, pix + 1, B.pgx, miy, piy, 1, -1);        // R
+    rates_dissipation_boundary(c, B, mix, pix, B.mgy, miy - 1, -1, 0);        // B
+    rates_dissipation_boundary(c, B, mix, pix, piy + 1, B.pgy, -1, 1);        // T
+    rates_dissipation_boundary(c, B, B.mgx, mix - 1, B.mgy, miy - 1, 0, 0);   // LB
+    rates_dissipation_boundary(c, B, pix + 1, B.pgx, B.mgy, miy - 1, 1, 0);   // RB
+    rates_dissipation_boundary(c, B, B.mgx, mix - 1, piy + 1, B.pgy, 0, 1);   // LT
+    rates_dissipation_boundary(c, B, pix + 1, B.pgx, piy + 1, B.pgy, 1, 1);   // RT
+  } else {
+    rates_interior(c, B, mix, pix, miy, piy);
+    rates_boundary(c, B, B.mgx, mix - 1, miy, piy, 0, -1);        // L
+    rates_boundary(c, B, pix + 1, B.pgx, miy, piy, 1, -1);        // R
+    rates_boundary(c, B, mix, pix, B.mgy, miy - 1, -1, 0);        // B
+    rates_boundary(c, B, mix, pix, piy + 1, B.pgy, -1, 1);        // T
+    rates_boundary(c, B, B.mgx, mix - 1, B.mgy, miy - 1, 0, 0);   // LB
+    rates_boundary(c, B, pix + 1, B.pgx, B.mgy, miy - 1, 1, 0);   // RB
+    rates_boundary(c, B, B.mgx, mix - 1, piy + 1, B.pgy, 0, 1);   // LT
+    rates_boundary(c, B, pix + 1, B.pgx, piy + 1, B.pgy, 1, 1);   // RT
+  }
   if (D.mode == 2) {
     // rates_szz / rates_h_szz (rates.f90:920-936, rates_heterogeneous.f90:901-917)
     size_t NN = c.NN;
@@ -1053,6 +1200,7 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
   o->x = copyv(d->x, NN); o->y = copyv(d->y, NN);
   o->xq = copyv(d->xq, NN); o->xr = copyv(d->xr, NN); o->yq = copyv(d->yq, NN); o->yr = copyv(d->yr, NN);
   o->Ji = copyv(d->Ji, NN);
+  if (d->J) o->J = copyv(d->J, NN);
   if (o->het) {
     o->rho = copyv(d->rho, NN); o->G = copyv(d->G, NN); o->M = copyv(d->M, NN);
     o->gamma = copyv(d->gamma, NN); o->nu = copyv(d->nu, NN);
@@ -1067,6 +1215,8 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
     for (int q = 0; q < 9; ++q) B.F0[q] = fb.F0[q];
     B.src_ok = fb.src_ok; B.src_i0 = fb.src_i0; B.src_j0 = fb.src_j0;
     B.src_hx = fb.src_hx; B.src_hy = fb.src_hy; B.src_ax = fb.src_ax; B.src_ay = fb.src_ay;
+    B.Cdiss = fb.Cdiss;
+    if (B.Cdiss > 0.0 && !d->J) { delete o; return nullptr; }
     for (int s = 0; s < 4; ++s) {
       const fdmap_side& fs = fb.side[s];
       Side& S = B.side[s];

@@ -120,3 +120,46 @@ def test_rough_fault_rate_state(require_gpu, tmp_path):
     assert_fields_close(g.get_fields()[0], o.get_fields()[0])
     assert_fault_close(g, o, dt=h.dt, fields=("V", "S", "N", "D", "Psi"))
     assert g.newton_failures() == 0 and o.newton_failures() == 0
+
+
+def _random_fields(h, seed):
+    rng = np.random.default_rng(seed)
+    F = h.array("F")
+    F[:] = rng.standard_normal(F.shape)
+
+
+@pytest.mark.parametrize("fd", ["SBP2", "SBP4", "SBP6"])
+def test_dissipation_stage_rates_mode3(require_gpu, fd):
+    """One stage of the dissipative rates (set_rates_dissipation) on a random
+    field, so every AI / AL weight and every closure row is exercised."""
+    h = init_domain(problems.antiplane_pulse(n=41, L=4.0, nt=2, fd=fd, cdiss=0.4))
+    _random_fields(h, 1)
+    g, o = GpuDomain(h), OracleDomain(h)
+    g.time_step_LS(h.t0, h.dt, final_step=True)
+    o.time_step_LS(h.t0, h.dt, final_step=True)
+    assert_fields_close(g.get_fields(False, True)[1], o.get_fields(False, True)[1], rtol=1e-12, what="DF")
+
+
+def test_dissipation_stage_rates_mode2(require_gpu):
+    h = init_domain(problems.rupture_sw(nx=41, ny=21, h=0.5, nt=2, cdiss=0.3))
+    _random_fields(h, 2)
+    g, o = GpuDomain(h), OracleDomain(h)
+    g.time_step_LS(h.t0, h.dt, final_step=True)
+    o.time_step_LS(h.t0, h.dt, final_step=True)
+    assert_fields_close(g.get_fields(False, True)[1], o.get_fields(False, True)[1], rtol=1e-12, what="DF")
+
+
+@pytest.mark.parametrize("fd", ["SBP2", "SBP4", "SBP6"])
+def test_dissipation_pulse_run(require_gpu, fd):
+    h, g, o = _pair(problems.antiplane_pulse(n=61, L=6.0, nt=61, fd=fd, cdiss=0.5))
+    g.run(1, h.nt)
+    o.run(1, h.nt)
+    assert_fields_close(g.get_fields()[0], o.get_fields()[0])
+
+
+def test_dissipation_rupture_run(require_gpu):
+    h, g, o = _pair(problems.rupture_sw(nx=121, ny=61, h=0.25, nt=121, cdiss=0.3))
+    g.run(1, h.nt)
+    o.run(1, h.nt)
+    assert_fields_close(g.get_fields()[0], o.get_fields()[0])
+    assert_fault_close(g, o, dt=h.dt, fields=("V", "S", "N", "D"))

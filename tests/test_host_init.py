@@ -70,7 +70,7 @@ def test_namelist_forms():
 
 
 def test_rejects_unsupported_features():
-    bad = problems.antiplane_pulse(n=21, L=2.0, nt=3).replace("&material_list", "&operator_list Cdiss=0.5d0 /\n&material_list")
+    bad = problems.antiplane_pulse(n=21, L=2.0, nt=3).replace("&fields_list", "&fields_list prestress_from_file=T,")
     with pytest.raises(FdmapError) as e:
         init_domain(bad)
     assert e.value.code == -6
@@ -94,3 +94,13 @@ def test_rough_fault_files(tmp_path):
     assert np.abs(y[40, :]).max() > 0
     J = h.array("J")[0]
     assert np.all(J > 0)
+
+
+def test_dissipation_coefficient_scaled_by_cfl_over_dt():
+    """operator_list Cdiss is read per block and scaled by CFL/dt after set_dt
+    (domain.f90:172-180, 317-320)."""
+    h = init_domain(problems.antiplane_pulse(n=21, L=2.0, nt=3, cdiss=0.3))
+    assert h.block_cdiss(0) == pytest.approx(0.3 * h.CFL / h.dt, rel=1e-15)
+    h2 = init_domain(problems.rupture_sw(nx=41, ny=21, h=0.5, nt=3, cdiss=0.2))
+    assert h2.block_cdiss(0) == h2.block_cdiss(1) == pytest.approx(0.2 * h2.CFL / h2.dt, rel=1e-15)
+    assert init_domain(problems.antiplane_pulse(n=21, L=2.0, nt=3)).block_cdiss(0) == 0.0

@@ -144,3 +144,50 @@ def test_locked_interface_energy():
     assert Es[-1] > 0.98 * E0
     F = o.get_fields()[0]
     assert np.abs(F[0][21:]).max() > 0.05  # the pulse crossed into block 2
+
+
+def _stage_rates(text, F):
+    h = init_domain(text)
+    h.array("F")[:] = F
+    o = OracleDomain(h)
+    o.time_step_LS(h.t0, h.dt, final_step=True)
+    return h, o.get_fields(False, True)[1]
+
+
+@pytest.mark.parametrize("fd", ["SBP2", "SBP4", "SBP6"])
+def test_dissipation_annihilates_constants_and_interior_linears(fd):
+    """The artificial dissipation (AI interior / AL closure rows, J-weighted,
+    rates.f90:939-1394) vanishes on constant fields everywhere and on linear
+    fields away from the closures: the rates with and without it agree."""
+    n, L, cd = 41, 4.0, 0.5
+    base = problems.antiplane_pulse(n=n, L=L, nt=2, fd=fd, amp=0.0)
+    h0 = init_domain(base)
+    x, y = h0.array("x")[0], h0.array("y")[0]
+    scale = h0.CFL / h0.dt * cd
+    for F in (np.stack([np.full_like(x, 0.3), np.full_like(x, 0.2), np.full_like(x, -0.1)]),
+              np.stack([0.1 * x + 0.2 * y, 0.3 * x - 0.1 * y, -0.2 * x + 0.05 * y])):
+        _, DF0 = _stage_rates(base, F)
+        h1, DF1 = _stage_rates(problems.antiplane_pulse(n=n, L=L, nt=2, fd=fd, amp=0.0, cdiss=cd), F)
+        assert h1.block_cdiss(0) == pytest.approx(scale)
+        nb = {"SBP2": 2, "SBP4": 6, "SBP6": 9}[fd]
+        region = (slice(None), slice(None), slice(None)) if np.ptp(F[0]) == 0 else \
+            (slice(None), slice(nb, -nb), slice(nb, -nb))
+        d = np.abs(DF1 - DF0)[region].max()
+        assert d <= 1e-12 * scale * (1 + np.abs(F).max() * L), (fd, d)
+
+
+def test_dissipation_removes_energy():
+    """With energy-conserving free boundaries the dissipative run loses energy
+    monotonically, and more than the run without dissipation."""
+    def run(cd):
+        h = init_domain(problems.antiplane_pulse(n=61, L=6.0, nt=201, sigma=0.3, cdiss=cd).replace("'absorbing'", "'free'"))
+        o = OracleDomain(h)
+        E = [energy_mode3(h, o.get_fields()[0])]
+        for n in range(1, 201):
+            o.time_step_LS(h.t0 + (n - 1) * h.dt, h.dt)
+            if n % 20 == 0:
+                E.append(energy_mode3(h, o.get_fields()[0]))
+        return np.array(E)
+    E0, E1 = run(0.0), run(0.5)
+    assert np.all(np.diff(E1) <= 1e-12 * E1[0])
+    assert E1[-1] < E0[-1] * (1 - 1e-4), (E1[-1] / E0[-1])
