@@ -160,19 +160,19 @@ int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p, int q) {
   fdmap_gpu* h = a->h;
   const DevBlock& B = h->hdom.blk[0];
   dim3 blk(ATX * ATY), grid((B.nx + ATX - 1) / ATX, (B.ny + ATY - 1) / ATY);
-  const int bgrid = (int)((a->nband + 255) / 256);
+  const int bgrid = (int)((a->nband + BAND_NODES - 1) / BAND_NODES);
   CUDA_TRY(cudaEventRecord(a->ev_fork, h->stream));
   CUDA_TRY(cudaStreamWaitEvent(a->side, a->ev_fork, 0));
   // the latency-bound band kernel goes first, at high priority, so its few CTAs
   // are placed before the interior tiles fill the SMs
   if (h->pI == 1) {
-    adj_band_kernel<1><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
+    adj_band_kernel<1><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, a->nband);
     adj_stage_tma<1><<<grid, blk, AdjTile<1>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
   } else if (h->pI == 2) {
-    adj_band_kernel<2><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
+    adj_band_kernel<2><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, a->nband);
     adj_stage_tma<2><<<grid, blk, AdjTile<2>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
   } else {
-    adj_band_kernel<3><<<bgrid, 256, 0, a->side>>>(h->hdom, p, a->nband);
+    adj_band_kernel<3><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, a->nband);
     adj_stage_tma<3><<<grid, blk, AdjTile<3>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
   }
   CUDA_TRY(cudaGetLastError());

@@ -39,55 +39,6 @@ struct AdjStage {
   double* gG;
 };
 
-// material-free volume rates phi_r(c) = Ji(c) * sum of stencil terms, so that
-// R_0 = phi_0 / rho(c) and R_{1,2} = G(c) * phi_{1,2} (rates_heterogeneous.f90:8-48 and closures)
-template <int PI_>
-__device__ __forceinline__ void phi_volume(const DevDomain& D, const DevBlock& B, const double* __restrict__ u, int i,
-                                           int j, double* phi) {
-  constexpr int nbnd = nbnd_of(PI_);
-  const int nx = B.nx, ny = B.ny, nbst = D.nbst;
-  const long long pitch = B.pitch, plane = B.plane;
-  const long long c = (long long)j * pitch + i;
-  const double yrc = B.yr[c], xrc = B.xr[c], yqc = B.yq[c], xqc = B.xq[c];
-  phi[0] = phi[1] = phi[2] = 0.0;
-  auto qterm = [&](long long k, double W) {
-    const double Y = 0.5 * (B.yr[k] + yrc), X = 0.5 * (B.xr[k] + xrc);
-    const double f0 = u[k], f1 = u[plane + k], f2 = u[2 * plane + k];
-    phi[0] += W * (Y * f1 - X * f2);
-    phi[1] += W * (Y * f0);
-    phi[2] += W * (-X * f0);
-  };
-  auto rterm = [&](long long k, double W) {
-    const double Y = 0.5 * (B.yq[k] + yqc), X = 0.5 * (B.xq[k] + xqc);
-    const double f0 = u[k], f1 = u[plane + k], f2 = u[2 * plane + k];
-    phi[0] += W * (-Y * f1 + X * f2);
-    phi[1] += W * (-Y * f0);
-    phi[2] += W * (X * f0);
-  };
-  if (i < nbst) {
-#pragma unroll
-    for (int s = 0; s < nbnd; ++s) qterm((long long)j * pitch + s, D.DL[i][s]);
-  } else if (i > nx - 1 - nbst) {
-#pragma unroll
-    for (int s = 0; s < nbnd; ++s) qterm((long long)j * pitch + (nx - 1 - s), -D.DL[nx - 1 - i][s]);
-  } else {
-#pragma unroll
-    for (int s = 1; s <= PI_; ++s) { qterm(c + s, D.DI[s]); qterm(c - s, -D.DI[s]); }
-  }
-  if (j < nbst) {
-#pragma unroll
-    for (int s = 0; s < nbnd; ++s) rterm((long long)s * pitch + i, D.DL[j][s]);
-  } else if (j > ny - 1 - nbst) {
-#pragma unroll
-    for (int s = 0; s < nbnd; ++s) rterm((long long)(ny - 1 - s) * pitch + i, -D.DL[ny - 1 - j][s]);
-  } else {
-#pragma unroll
-    for (int s = 1; s <= PI_; ++s) { rterm(c + s * pitch, D.DI[s]); rterm(c - s * pitch, -D.DI[s]); }
-  }
-  const double Ji = B.Ji[c];
-  phi[0] *= Ji; phi[1] *= Ji; phi[2] *= Ji;
-}
-
 // SAT of one outer side at an edge node in mode III (set_bc_mode3 + SAT_term):
 //   r0 = vz - vz0,  r2 = n0 (sxz - sxz0) + n1 (syz - syz0),
 //   e = E(Zs) (r0, r2),   DF += Ks * (e0, n0 e2, n1 e2).
@@ -133,10 +84,14 @@ __device__ __forceinline__ void sat_adjoint(int bc, double Zs, double Ks, double
   *gG += 0.5 * (gZ * Zs + gK * Ks) / G;
 }
 
-// One node of the adjoint stage through the cache hierarchy: every node, any
-// position (closures, corners, sides).
+// One direction of one node of the adjoint stage through the cache hierarchy
+// (closures, sides, corners): part 0 gathers the q direction, the q half of
+// the node's own volume rates and the SAT of the L / R sides; part 1 the r
+// direction, its half of the volume rates and the SAT of the B / T sides.
+// The two partial sums are added by the caller.
 template <int PI_>
-__device__ __forceinline__ void adj_node_generic(const DevDomain& D, const AdjStage& p, int i, int j) {
+__device__ __forceinline__ void adj_node_part(const DevDomain& D, const AdjStage& p, int i, int j, int part,
+                                              double* acc, double* phi, double& grho, double& gG) {
   constexpr int nbnd = nbnd_of(PI_);
   const DevBlock& B = D.blk[0];
   const int nx = B.nx, ny = B.ny, nbst = D.nbst;
@@ -145,75 +100,104 @@ __device__ __forceinline__ void adj_node_generic(const DevDomain& D, const AdjSt
   const double* __restrict__ ub = p.ub_in;
   const double* __restrict__ qp = p.qp_in;
   auto qs = [&](long long k, int f) { return qp[f * plane + k] + p.Bdt * ub[f * plane + k]; };
-
-  double acc[3] = {0.0, 0.0, 0.0};
-  const double yrc = B.yr[c], xrc = B.xr[c], yqc = B.yq[c], xqc = B.xq[c];
-  // output node k (same row) whose q-stencil weights this node by W
-  auto gather_q = [&](int ic, double W) {
-    const long long k = (long long)j * pitch + ic;
-    const double Y = 0.5 * (B.yr[k] + yrc), X = 0.5 * (B.xr[k] + xrc);
-    const double wj = W * B.Ji[k], g = B.G[k];
-    const double l0 = qs(k, 0) * (wj / B.rho[k]), l1 = qs(k, 1) * (wj * g), l2 = qs(k, 2) * (wj * g);
-    acc[1] += Y * l0;
-    acc[2] -= X * l0;
-    acc[0] += Y * l1 - X * l2;
-  };
-  auto gather_r = [&](int jc, double W) {
-    const long long k = (long long)jc * pitch + i;
-    const double Y = 0.5 * (B.yq[k] + yqc), X = 0.5 * (B.xq[k] + xqc);
-    const double wj = W * B.Ji[k], g = B.G[k];
-    const double l0 = qs(k, 0) * (wj / B.rho[k]), l1 = qs(k, 1) * (wj * g), l2 = qs(k, 2) * (wj * g);
-    acc[1] -= Y * l0;
-    acc[2] += X * l0;
-    acc[0] += -Y * l1 + X * l2;
-  };
-#pragma unroll
-  for (int s = 1; s <= PI_; ++s) {
-    const int a = i - s, b = i + s;  // output columns with this node at +s / -s
-    if (a >= nbst && a <= nx - 1 - nbst) gather_q(a, D.DI[s]);
-    if (b >= nbst && b <= nx - 1 - nbst) gather_q(b, -D.DI[s]);
-    const int ar = j - s, br = j + s;
-    if (ar >= nbst && ar <= ny - 1 - nbst) gather_r(ar, D.DI[s]);
-    if (br >= nbst && br <= ny - 1 - nbst) gather_r(br, -D.DI[s]);
-  }
-  if (i < nbnd)
-    for (int ic = 0; ic < nbst; ++ic) gather_q(ic, D.DL[ic][i]);
-  if (nx - 1 - i < nbnd)
-    for (int ic = nx - nbst; ic < nx; ++ic) gather_q(ic, -D.DL[nx - 1 - ic][nx - 1 - i]);
-  if (j < nbnd)
-    for (int jc = 0; jc < nbst; ++jc) gather_r(jc, D.DL[jc][j]);
-  if (ny - 1 - j < nbnd)
-    for (int jc = ny - nbst; jc < ny; ++jc) gather_r(jc, -D.DL[ny - 1 - jc][ny - 1 - j]);
-
-  // adjoint rates and stage input of this node
-  const double lam[3] = {qs(c, 0), qs(c, 1), qs(c, 2)};
+  acc[0] = acc[1] = acc[2] = 0.0;
+  phi[0] = phi[1] = phi[2] = 0.0;
+  grho = gG = 0.0;
   const double* __restrict__ ust = p.store + ((*p.rel) * p.nstage + p.s) * p.stride;
+  if (part == 0) {
+    const double yrc = B.yr[c], xrc = B.xr[c];
+    // output node k (same row) whose q-stencil weights this node by W
+    auto gather_q = [&](int ic, double W) {
+      const long long k = (long long)j * pitch + ic;
+      const double Y = 0.5 * (B.yr[k] + yrc), X = 0.5 * (B.xr[k] + xrc);
+      const double wj = W * B.Ji[k], g = B.G[k];
+      const double l0 = qs(k, 0) * (wj / B.rho[k]), l1 = qs(k, 1) * (wj * g), l2 = qs(k, 2) * (wj * g);
+      acc[1] += Y * l0;
+      acc[2] -= X * l0;
+      acc[0] += Y * l1 - X * l2;
+    };
+    // this node's q-direction volume term from neighbour k with weight W
+    auto phi_q = [&](long long k, double W) {
+      const double Y = 0.5 * (B.yr[k] + yrc), X = 0.5 * (B.xr[k] + xrc);
+      const double f0 = ust[k], f1 = ust[plane + k], f2 = ust[2 * plane + k];
+      phi[0] += W * (Y * f1 - X * f2);
+      phi[1] += W * (Y * f0);
+      phi[2] += W * (-X * f0);
+    };
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      const int a = i - s, b = i + s;  // output columns with this node at +s / -s
+      if (a >= nbst && a <= nx - 1 - nbst) gather_q(a, D.DI[s]);
+      if (b >= nbst && b <= nx - 1 - nbst) gather_q(b, -D.DI[s]);
+    }
+    if (i < nbnd)
+      for (int ic = 0; ic < nbst; ++ic) gather_q(ic, D.DL[ic][i]);
+    if (nx - 1 - i < nbnd)
+      for (int ic = nx - nbst; ic < nx; ++ic) gather_q(ic, -D.DL[nx - 1 - ic][nx - 1 - i]);
+    if (i < nbst) {
+#pragma unroll
+      for (int s = 0; s < nbnd; ++s) phi_q((long long)j * pitch + s, D.DL[i][s]);
+    } else if (i > nx - 1 - nbst) {
+#pragma unroll
+      for (int s = 0; s < nbnd; ++s) phi_q((long long)j * pitch + (nx - 1 - s), -D.DL[nx - 1 - i][s]);
+    } else {
+#pragma unroll
+      for (int s = 1; s <= PI_; ++s) { phi_q(c + s, D.DI[s]); phi_q(c - s, -D.DI[s]); }
+    }
+  } else {
+    const double yqc = B.yq[c], xqc = B.xq[c];
+    auto gather_r = [&](int jc, double W) {
+      const long long k = (long long)jc * pitch + i;
+      const double Y = 0.5 * (B.yq[k] + yqc), X = 0.5 * (B.xq[k] + xqc);
+      const double wj = W * B.Ji[k], g = B.G[k];
+      const double l0 = qs(k, 0) * (wj / B.rho[k]), l1 = qs(k, 1) * (wj * g), l2 = qs(k, 2) * (wj * g);
+      acc[1] -= Y * l0;
+      acc[2] += X * l0;
+      acc[0] += -Y * l1 + X * l2;
+    };
+    auto phi_r = [&](long long k, double W) {
+      const double Y = 0.5 * (B.yq[k] + yqc), X = 0.5 * (B.xq[k] + xqc);
+      const double f0 = ust[k], f1 = ust[plane + k], f2 = ust[2 * plane + k];
+      phi[0] += W * (-Y * f1 + X * f2);
+      phi[1] += W * (-Y * f0);
+      phi[2] += W * (X * f0);
+    };
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      const int ar = j - s, br = j + s;
+      if (ar >= nbst && ar <= ny - 1 - nbst) gather_r(ar, D.DI[s]);
+      if (br >= nbst && br <= ny - 1 - nbst) gather_r(br, -D.DI[s]);
+    }
+    if (j < nbnd)
+      for (int jc = 0; jc < nbst; ++jc) gather_r(jc, D.DL[jc][j]);
+    if (ny - 1 - j < nbnd)
+      for (int jc = ny - nbst; jc < ny; ++jc) gather_r(jc, -D.DL[ny - 1 - jc][ny - 1 - j]);
+    if (j < nbst) {
+#pragma unroll
+      for (int s = 0; s < nbnd; ++s) phi_r((long long)s * pitch + i, D.DL[j][s]);
+    } else if (j > ny - 1 - nbst) {
+#pragma unroll
+      for (int s = 0; s < nbnd; ++s) phi_r((long long)(ny - 1 - s) * pitch + i, -D.DL[ny - 1 - j][s]);
+    } else {
+#pragma unroll
+      for (int s = 1; s <= PI_; ++s) { phi_r(c + s * pitch, D.DI[s]); phi_r(c - s * pitch, -D.DI[s]); }
+    }
+  }
+  // SAT of the outer sides through this node (L, R on part 0; B, T on part 1)
+  const double lam[3] = {qs(c, 0), qs(c, 1), qs(c, 2)};
   const double rho = B.rho[c], G = B.G[c];
-  double grho = 0.0, gG = 0.0;
-  // SAT of the outer sides through this node, in the forward's side order
   auto side = [&](int sd, int k) {
     const DevSide& S = B.side[sd];
     const double us[3] = {ust[c], ust[plane + c], ust[2 * plane + c]};
     const double F0[3] = {S.F0[k], S.F0[k + S.n], S.F0[k + 2 * S.n]};
     sat_adjoint(S.bc, S.M[k], S.M[k + 3 * S.n], S.nrm[k], S.nrm[k + S.n], lam, us, F0, rho, G, acc, &grho, &gG);
   };
-  if (i == 0) side(0, j);
-  if (i == nx - 1) side(1, j);
-  if (j == 0) side(2, i);
-  if (j == ny - 1) side(3, i);
-
-  // volume part of dR/dm at this node
-  double phi[3];
-  phi_volume<PI_>(D, B, ust, i, j, phi);
-  const double rinv = 1.0 / rho;
-  grho -= lam[0] * phi[0] * (rinv * rinv);
-  gG += lam[1] * phi[1] + lam[2] * phi[2];
-  p.grho[c] += grho;
-  p.gG[c] += gG;
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    p.ub_out[f * plane + c] = ub[f * plane + c] + acc[f];
-    p.qp_out[f * plane + c] = p.A * lam[f];
+  if (part == 0) {
+    if (i == 0) side(0, j);
+    if (i == nx - 1) side(1, j);
+  } else {
+    if (j == 0) side(2, i);
+    if (j == ny - 1) side(3, i);
   }
 }
 
@@ -239,15 +223,56 @@ __device__ __forceinline__ void band_node(long long q, int nx, int ny, int nbnd,
   i = k < nbnd ? k : nx - 2 * nbnd + k;
 }
 
-// the band (closures, sides, corners): generic per-node path
+// the band (closures, sides, corners): 128 nodes per 256-thread CTA; threads
+// 0..127 take the q direction of their node, threads 128..255 the r direction
+// of the same node (whole warps per direction, so the branches do not
+// diverge), and the partial sums meet in shared memory
+constexpr int BAND_NODES = 128;
+
 template <int PI_>
-__global__ void __launch_bounds__(256) adj_band_kernel(const __grid_constant__ DevDomain D, AdjStage p, long long nband) {
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= nband) return;
+__global__ void __launch_bounds__(2 * BAND_NODES) adj_band_kernel(const __grid_constant__ DevDomain D, AdjStage p,
+                                                                   long long nband) {
+  __shared__ double part1[8][BAND_NODES];  // acc 3, phi 3, grho, gG of the r direction
+  const int part = threadIdx.x / BAND_NODES, slot = threadIdx.x % BAND_NODES;
+  const long long q = (long long)blockIdx.x * BAND_NODES + slot;
+  const bool valid = q < nband;
   const DevBlock& B = D.blk[0];
-  int i, j;
-  band_node(q, B.nx, B.ny, nbnd_of(PI_), i, j);
-  adj_node_generic<PI_>(D, p, i, j);
+  int i = 0, j = 0;
+  double acc[3], phi[3], grho = 0.0, gG = 0.0;
+  if (valid) {
+    band_node(q, B.nx, B.ny, nbnd_of(PI_), i, j);
+    adj_node_part<PI_>(D, p, i, j, part, acc, phi, grho, gG);
+    if (part == 1) {
+#pragma unroll
+      for (int f = 0; f < 3; ++f) { part1[f][slot] = acc[f]; part1[3 + f][slot] = phi[f]; }
+      part1[6][slot] = grho;
+      part1[7][slot] = gG;
+    }
+  }
+  __syncthreads();
+  if (!valid || part != 0) return;
+#pragma unroll
+  for (int f = 0; f < 3; ++f) { acc[f] += part1[f][slot]; phi[f] += part1[3 + f][slot]; }
+  grho += part1[6][slot];
+  gG += part1[7][slot];
+  const long long pitch = B.pitch, plane = B.plane;
+  const long long c = (long long)j * pitch + i;
+  double lam[3], ubc[3];
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    ubc[f] = p.ub_in[f * plane + c];
+    lam[f] = p.qp_in[f * plane + c] + p.Bdt * ubc[f];
+  }
+  const double Ji = B.Ji[c], rinv = 1.0 / B.rho[c];
+  grho -= lam[0] * (phi[0] * Ji) * (rinv * rinv);
+  gG += lam[1] * (phi[1] * Ji) + lam[2] * (phi[2] * Ji);
+  p.grho[c] += grho;
+  p.gG[c] += gG;
+#pragma unroll
+  for (int f = 0; f < 3; ++f) {
+    p.ub_out[f * plane + c] = ubc[f] + acc[f];
+    p.qp_out[f * plane + c] = p.A * lam[f];
+  }
 }
 
 // Edge impedance and penalty of a heterogeneous mode III side from the node's
