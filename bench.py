@@ -421,6 +421,16 @@ def run_ensemble(args) -> None:
         g.synchronize()
         seq += time.perf_counter() - t0
         g.close()
+    # the same instances with their bodies built on the device (on-device init)
+    t_init_dev = time.perf_counter()
+    devs = init_domains([problems.ensemble_instance(tmp, s) for s in range(n)], tmp, body_on_device=True)
+    t_init_dev = time.perf_counter() - t_init_dev
+    t_create_dev = time.perf_counter()
+    ens_dev = GpuEnsemble(devs, device=local)
+    ens_dev.synchronize()
+    t_create_dev = time.perf_counter() - t_create_dev
+    same_dt = all(a.dt == b.dt for a, b in zip(devs, hosts))
+    ens_dev.close()
     per_step = el / args.steps
     runs = world * n / (per_step * run_steps)
     if rank == 0:
@@ -435,6 +445,8 @@ def run_ensemble(args) -> None:
                 "sequential_plain": {"runs_per_s": n / (seq / args.steps * run_steps),
                                      "ms_per_step": seq / args.steps * 1e3},
                 "speedup_vs_sequential": seq / el, "host_init_s": t_init, "ensemble_create_s": t_create,
+                "device_body_init": {"host_init_s": t_init_dev, "ensemble_create_s": t_create_dev,
+                                     "same_dt_as_host_body": same_dt},
                 "clocks": clocks.summary(), "gpu_launches": launches}
         print(json.dumps(line), flush=True)
 

@@ -23,6 +23,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
+# sources whose device arithmetic must round exactly like the host restatement
+NO_FMA = {"body_init.cu"}
+
+
 def _sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
@@ -44,6 +48,8 @@ def _compile(src: Path, obj: Path, verbose: bool) -> None:
         f"-I{INCLUDE}", f"-I{CSRC}",
         "-Xcompiler", "-fPIC,-O3", "-c", str(src), "-o", str(obj),
     ]
+    if src.name in NO_FMA:
+        cmd.insert(3, "-fmad=false")
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -60,6 +60,9 @@ struct fdmap_gpu {
   int march_grid = 0;
   int use_march = 1;
   bool dissipation = false;  // some block has Cdiss > 0 (tiled interior kernel)
+  bool body_on_device = false;  // body built by build_body (fdmap_desc.body)
+  double tp[5] = {0, 0, 0, 0, 0};  // t0, dt, CFL, hmin, hmax (set_dt)
+  int tp_nt = 0;
   int fused = 0;  // boundary kernel handles interface solves and closure strips in one launch
   // CUDA graphs of one full step, one per starting F buffer, replayed by fdmap_gpu_run
   TimeState* d_time = nullptr;
@@ -186,6 +189,11 @@ struct BatchPlan {
   int closure_ctas, closure_tpb;
   int edge_ctas, edge_tpb;
 };
+// Builds the body of a domain whose descriptor carries fdmap_desc.body
+// (body_init.cu) into the already allocated block planes and side arrays, and
+// finishes set_dt into h->tp / h->tp_nt and each block's scaled Cdiss.
+int build_body(fdmap_gpu* h, const fdmap_desc* d, const SbpOperator& op);
+
 // One RK stage of a single domain (boundary + interior kernels) on h->stream.
 int engine_stage(fdmap_gpu* h, const StageArgs& a);
 

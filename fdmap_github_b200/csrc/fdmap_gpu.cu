@@ -358,8 +358,10 @@ int validate(const fdmap_desc* d) {
   if (d->nF != (d->mode == 2 ? 6 : 3)) return set_err(FDMAP_ERR_INVALID_ARG, "nF does not match mode");
   if (d->nblocks < 1 || d->nblocks > MAX_BLOCKS) return set_err(FDMAP_ERR_UNSUPPORTED, "1..16 blocks supported");
   if (d->nifaces < 0 || d->nifaces > MAX_IFACES) return set_err(FDMAP_ERR_UNSUPPORTED, "at most 32 interfaces supported");
-  if (!d->F || !d->DF || !d->xq || !d->xr || !d->yq || !d->yr || !d->Ji)
+  const bool dev_body = d->body != nullptr;
+  if (!dev_body && (!d->F || !d->DF || !d->xq || !d->xr || !d->yq || !d->yr || !d->Ji))
     return set_err(FDMAP_ERR_INVALID_ARG, "missing body arrays");
+  if (dev_body && !d->body->blocks) return set_err(FDMAP_ERR_INVALID_ARG, "missing block body recipes");
   if (d->heterogeneous && (!d->rho || !d->G || (d->mode == 2 && (!d->M || !d->gamma || !d->nu))))
     return set_err(FDMAP_ERR_INVALID_ARG, "missing heterogeneous material arrays");
   fdmap::SbpOperator op;
@@ -369,7 +371,7 @@ int validate(const fdmap_desc* d) {
     int nx = B.pgx - B.mgx + 1, ny = B.pgy - B.mgy + 1;
     if (B.mgx < 1 || B.mgy < 1 || B.pgx > d->nx || B.pgy > d->ny)
       return set_err(FDMAP_ERR_INVALID_ARG, "block index limits outside the domain");
-    if (B.Cdiss > 0.0 && (!d->J || d->heterogeneous))
+    if (!dev_body && B.Cdiss > 0.0 && (!d->J || d->heterogeneous))
       return set_err(d->J ? FDMAP_ERR_UNSUPPORTED : FDMAP_ERR_INVALID_ARG,
                      d->J ? "artificial dissipation in heterogeneous blocks is not supported"
                           : "artificial dissipation needs the Jacobian array J");
@@ -378,7 +380,8 @@ int validate(const fdmap_desc* d) {
     for (int s = 0; s < 4; ++s) {
       const fdmap_side& S = B.side[s];
       if (S.n != (s < 2 ? ny : nx)) return set_err(FDMAP_ERR_INVALID_ARG, "side length mismatch");
-      if (!S.M || !S.F0 || !S.normal) return set_err(FDMAP_ERR_INVALID_ARG, "missing side arrays");
+      if ((!S.M && !dev_body) || !S.F0 || !S.normal) return set_err(FDMAP_ERR_INVALID_ARG, "missing side arrays");
+      if (dev_body && (!S.x || !S.y)) return set_err(FDMAP_ERR_INVALID_ARG, "missing side coordinates");
       if (d->mode == 3 && S.bc != FDMAP_BC_NONE && S.bc != FDMAP_BC_ABSORBING && S.bc != FDMAP_BC_FREE &&
           S.bc != FDMAP_BC_RIGID)
         return set_err(FDMAP_ERR_UNSUPPORTED, "boundary condition not available in mode III");
@@ -443,7 +446,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     const double* msrc[5] = {d->yr, d->xr, d->yq, d->xq, d->Ji};
     for (int q = 0; q < 5; ++q) {
       *met[q] = met_base + (size_t)q * g.plane;
-      if ((rc = h->upload_plane(*met[q], msrc[q], g))) return rc;
+      if (!d->body && (rc = h->upload_plane(*met[q], msrc[q], g))) return rc;
     }
     h->met_base[b] = met_base;
     if (d->heterogeneous) {
@@ -458,11 +461,12 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       h->het_base[b] = het_base;
     }
     B.rho_b = fb.rho; B.G_b = fb.G; B.M_b = fb.M; B.gamma_b = fb.gamma; B.nu_b = fb.nu;
-    B.Cdiss = fb.Cdiss;
+    B.Cdiss = fb.Cdiss;  // on-device body: scaled by build_body once dt is known
     B.J = nullptr;
-    if (fb.Cdiss > 0.0) {  // the dissipation term weights neighbours by J itself
+    const double cdiss_in = d->body ? d->body->blocks[b].Cdiss : fb.Cdiss;
+    if (cdiss_in > 0.0) {  // the dissipation term weights neighbours by J itself
       if ((rc = h->alloc_planes(&B.J, 1, g.plane))) return rc;
-      if ((rc = h->upload_plane(B.J, d->J, g))) return rc;
+      if (!d->body && (rc = h->upload_plane(B.J, d->J, g))) return rc;
       h->dissipation = true;
     }
     B.rinv_b = 1.0 / fb.rho;
@@ -476,7 +480,11 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       const fdmap_side& fs = fb.side[s];
       DevSide& S = B.side[s];
       S.bc = fs.bc; S.n = fs.n; S.cov_lo = 0; S.cov_hi = 0;
-      if ((rc = h->upload(&S.M, fs.M, (size_t)fs.n * 5))) return rc;
+      if (d->body) {
+        if ((rc = h->alloc(&S.M, (size_t)fs.n * 5))) return rc;
+      } else if ((rc = h->upload(&S.M, fs.M, (size_t)fs.n * 5))) {
+        return rc;
+      }
       if ((rc = h->upload(&S.F0, fs.F0, (size_t)fs.n * nF))) return rc;
       if ((rc = h->upload(&S.nrm, fs.normal, (size_t)fs.n * 2))) return rc;
       if ((rc = h->alloc(&S.Fhat, (size_t)fs.n * nF))) return rc;
@@ -501,6 +509,15 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     h->march_units += (long long)((g.nx + MW - 1) / MW) * ((g.ny + MR - 1) / MR);
   }
   h->total_tiles = tiles;
+  h->body_on_device = d->body != nullptr;
+  if (h->body_on_device) {
+    h->cur = 0;
+    int rcb = build_body(h, d, op);
+    if (rcb) return rcb;
+  } else {
+    h->tp[0] = d->t0; h->tp[1] = d->dt; h->tp[2] = d->CFL; h->tp[3] = d->hmin; h->tp[4] = d->hmax;
+    h->tp_nt = d->nt;
+  }
 
   // interfaces
   h->iface_n.resize(d->nifaces);
@@ -524,12 +541,21 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     int rc;
     {
       // impedance terms of both sides (interfaces.f90:696-699, 735-760, 851-855, 956-965)
-      const fdmap_side& fsm = Bm.side[fi.direction == 0 ? 1 : 3];
-      const fdmap_side& fsp = Bp.side[fi.direction == 0 ? 0 : 2];
+      const int sm = fi.direction == 0 ? 1 : 3, sp = fi.direction == 0 ? 0 : 2;
+      const fdmap_side& fsm = Bm.side[sm];
+      const fdmap_side& fsp = Bp.side[sp];
+      // Zs = rho*cs and Zp = rho*cp (side impedance columns 0 and 1); with the
+      // body built on the device they are formed here from the same material
+      auto Z = [&](const fdmap_block& fb, const fdmap_side& fs, int blk, int side, int k, int c) {
+        if (!d->body) return fs.M[k + (size_t)c * fs.n];
+        const double* mat = d->body->blocks[blk].side_mat[side];
+        if (!mat) return fb.rho * (c == 0 ? fb.cs : fb.cp);
+        return mat[k] * mat[k + (size_t)(c == 0 ? 1 : 2) * fs.n];
+      };
       std::vector<double> ic((size_t)IC_N * I.n);
       for (int q = 0; q < I.n; ++q) {
-        double Zsm = fsm.M[I.offm + q], Zsp = fsp.M[I.offp + q];
-        double Zpm = fsm.M[I.offm + q + fsm.n], Zpp = fsp.M[I.offp + q + fsp.n];
+        double Zsm = Z(Bm, fsm, fi.iblockm, sm, I.offm + q, 0), Zsp = Z(Bp, fsp, fi.iblockp, sp, I.offp + q, 0);
+        double Zpm = Z(Bm, fsm, fi.iblockm, sm, I.offm + q, 1), Zpp = Z(Bp, fsp, fi.iblockp, sp, I.offp + q, 1);
         double Zsim = 1.0 / Zsm, Zsip = 1.0 / Zsp, Zpim = 1.0 / Zpm, Zpip = 1.0 / Zpp;
         ic[(size_t)IC_ZSIM * I.n + q] = Zsim;
         ic[(size_t)IC_ZSIP * I.n + q] = Zsip;
@@ -626,6 +652,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
 
   // global-layout staging buffer and initial fields
   if ((rc = h->alloc(&h->d_global, (size_t)d->nx * d->ny * nF))) return rc;
+  if (h->body_on_device) return FDMAP_OK;  // fields already built in F[0], DF
   h->cur = 0;
   return fdmap_gpu_set_fields(h, d->F, d->DF);
 }
@@ -830,6 +857,49 @@ int fdmap_gpu_set_fields(fdmap_gpu* h, const double* F, const double* DF) {
     }
   }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_time_params(fdmap_gpu* h, double* params, int* nt) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  if (params)
+    for (int q = 0; q < 5; ++q) params[q] = h->tp[q];
+  if (nt) *nt = h->tp_nt;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out) {
+  if (!h || !out || which < FDMAP_METRIC_XQ || which > FDMAP_METRIC_J)
+    return set_err(FDMAP_ERR_INVALID_ARG, "bad get_metric arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    const double* planes[6] = {B.xq, B.xr, B.yq, B.yr, B.Ji, B.J};
+    if (!planes[which]) return set_err(FDMAP_ERR_INVALID_ARG, "the Jacobian plane is kept for dissipative blocks only");
+  }
+  const long long NN = (long long)h->nx_g * h->ny_g;
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    const double* planes[6] = {B.xq, B.xr, B.yq, B.yr, B.Ji, B.J};
+    const BlockGeom& g = h->geom[b];
+    dim3 grid((g.pitch + 255) / 256, g.ny);
+    gather_block<<<grid, 256, 0, h->stream>>>(planes[which], h->d_global, h->nx_g, NN, g.mgx, g.mgy, g.nx, g.ny,
+                                              g.pitch, g.plane, 1);
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaMemcpyAsync(out, h->d_global, (size_t)NN * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_side_impedance(fdmap_gpu* h, int b, int s, double* out) {
+  if (!h || !out || b < 0 || b >= h->hdom.nblocks || s < 0 || s > 3)
+    return set_err(FDMAP_ERR_INVALID_ARG, "bad get_side_impedance arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const DevSide& S = h->hdom.blk[b].side[s];
+  CUDA_TRY(cudaMemcpy(out, S.M, (size_t)S.n * 5 * sizeof(double), cudaMemcpyDeviceToHost));
   return FDMAP_OK;
 }
 

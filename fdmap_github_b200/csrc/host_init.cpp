@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "body_formulas.h"
 #include "sbp_tables.h"
 
 namespace {
@@ -251,28 +252,9 @@ std::vector<double> read_binary_doubles(const std::string& path, size_t count, s
 }
 
 // ---------------------------------------------------------------------------
-// utilities.f90 shape functions (utilities.f90:303-420) and search_binary
-// (utilities.f90:13-157, floor mode without initial guess).
+// search_binary (utilities.f90:13-157, floor mode without initial guess); the
+// shape functions of utilities.f90:303-420 are in body_formulas.h.
 // ---------------------------------------------------------------------------
-const double kTol = 100.0 * 2.220446049250313e-16;  // 100d0*epsilon(r)
-
-double u_boxcar(double r, double w, double fin, double fout) {
-  if (-w + kTol < r && r < w - kTol) return fin;
-  if (std::fabs(-w - r) <= kTol || std::fabs(r - w) <= kTol) return 0.5 * (fin + fout);
-  return fout;
-}
-double u_gaussian(double r, double w, double fin, double fout) {
-  return fout + (fin - fout) * std::exp(-0.5 * ((r / w) * (r / w)));
-}
-double u_smooth(double r, double w, double fin, double fout) {
-  if (r >= w - kTol) return fout;
-  return fout + (fin - fout) * std::exp((r * r) / ((r * r) - (w * w)));
-}
-double u_triangle(double r, double w, double fin, double fout) {
-  if (-w < r && r < w) return fout + (fin - fout) * (1.0 - r / w);
-  return fout;
-}
-
 int search_floor(const double* x, int n, double y, bool* out) {
   // returns a 1-based index i with x(i) <= y < x(i+1)
   if (n == 1) {
@@ -315,6 +297,7 @@ struct BlockIn {
   double Cdiss = 0;  // operator_list (domain.f90:172-180), scaled by CFL/dt after set_dt
   Curve curve[4];
   SideStore side[4];
+  std::vector<double> side_mat[4];  // on-device body of a heterogeneous block: rho, cs, cp at side nodes
 };
 
 struct FrictionStore {
@@ -337,6 +320,10 @@ struct fdmap_domain {
   std::vector<IfaceStore> istore;
   std::vector<double> F, DF, x, y, xq, xr, yq, yr, J, Ji;
   std::vector<double> rho, cs, cp, G, M, gamma, nu;
+  // on-device initialisation: the recipe the engine builds the body from
+  bool dev_body = false;
+  fdmap_body body{};
+  std::vector<fdmap_block_body> bbody;
 };
 
 namespace {
@@ -460,8 +447,24 @@ void sbp_diff(const fdmap::SbpOperator& op, const std::vector<double>& f, std::v
   }
 }
 
+// one coordinate (c = 0: x, 1: y) of node (i, j) of block B, interpolated
+// from its four edge curves (transfinite_interp, geometry.f90:153-200)
+double node_coord(const BlockIn& B, int i, int j, int c) {
+  double qmin = B.mgx, qmax = B.pgx, rmin = B.mgy, rmax = B.pgy;
+  double Wq = qmax - qmin, Wr = rmax - rmin;
+  if (Wq == 0.0) Wq = 1.0;
+  if (Wr == 0.0) Wr = 1.0;
+  const std::vector<double>& cL = c ? B.curve[0].y : B.curve[0].x;
+  const std::vector<double>& cR = c ? B.curve[1].y : B.curve[1].x;
+  const std::vector<double>& cB = c ? B.curve[2].y : B.curve[2].x;
+  const std::vector<double>& cT = c ? B.curve[3].y : B.curve[3].x;
+  return fdmap::transfinite((double)i, (double)j, qmin, qmax, rmin, rmax, Wq, Wr, cL[j - B.mgy], cR[j - B.mgy],
+                            cB[i - B.mgx], cT[i - B.mgx], B.LB[c], B.LT[c], B.RB[c], B.RT[c]);
+}
+
 struct Perturb {
   std::string shape;
+  int code = FDMAP_PERTURB_NONE;
   double x0 = 0, y0 = 0, Lx = 1, Ly = 1;
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};  // vx vy vz sxx sxy sxz syy syz szz
 };
@@ -475,20 +478,19 @@ Perturb read_perturb(const Namelist& nl, const std::string& name) {
   P.Ly = get_real(nl, name, 1, "fields_perturb", "ly");
   const char* comps[9] = {"vx", "vy", "vz", "sxx", "sxy", "sxz", "syy", "syz", "szz"};
   for (int c = 0; c < 9; ++c) P.v[c] = get_real(nl, name, 0, "fields_perturb", comps[c]);
+  if (P.shape == "") P.code = FDMAP_PERTURB_NONE;
+  else if (P.shape == "linear") P.code = FDMAP_PERTURB_LINEAR;
+  else if (P.shape == "boxcar") P.code = FDMAP_PERTURB_BOXCAR;
+  else if (P.shape == "triangle") P.code = FDMAP_PERTURB_TRIANGLE;
+  else if (P.shape == "smooth") P.code = FDMAP_PERTURB_SMOOTH;
+  else if (P.shape == "gaussian") P.code = FDMAP_PERTURB_GAUSSIAN;
+  else fail(FDMAP_ERR_UNSUPPORTED, "perturbation shape '" + P.shape + "' is not supported");
   return P;
 }
 
 // perturb_fields (fields.f90:900-934)
 double perturb_amp(double x, double y, const Perturb& P) {
-  double a = (x - P.x0) / P.Lx, b = (y - P.y0) / P.Ly;
-  double r = std::sqrt(a * a + b * b);
-  if (P.shape == "") return 0.0;
-  if (P.shape == "linear") return (x - P.x0) / P.Lx + (y - P.y0) / P.Ly;
-  if (P.shape == "boxcar") return u_boxcar(r, 1.0, 1.0, 0.0);
-  if (P.shape == "triangle") return u_triangle(r, 1.0, 1.0, 0.0);
-  if (P.shape == "smooth") return u_smooth(r, 1.0, 1.0, 0.0);
-  if (P.shape == "gaussian") return u_gaussian(r, 1.0, 1.0, 0.0);
-  fail(FDMAP_ERR_UNSUPPORTED, "perturbation shape '" + P.shape + "' is not supported");
+  return fdmap::perturb_amp(P.code, x, y, P.x0, P.y0, P.Lx, P.Ly);
 }
 
 // field vector of a perturbation in the mode's field order
@@ -502,7 +504,7 @@ void perturb_vector(const Perturb& P, int mode, double* out) {
   }
 }
 
-void build(fdmap_domain& dom, const std::string& text, const std::string& base) {
+void build(fdmap_domain& dom, const std::string& text, const std::string& base, bool dev_body) {
   fdmap_desc& d = dom.desc;
 
   // ---- problem_list (main.f90:57-78)
@@ -624,9 +626,11 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
 
   // ---- grids (init_grid + interp_block, grid.f90:188-462)
   int minpts = op.nbst == 1 ? 3 : (op.nbst == 4 ? 8 : 12);
-  dom.x.assign(NN, 1e40); dom.y.assign(NN, 1e40);
-  dom.xq.assign(NN, 1.0); dom.xr.assign(NN, 0.0); dom.yq.assign(NN, 0.0); dom.yr.assign(NN, 1.0);
-  dom.J.assign(NN, 1.0); dom.Ji.assign(NN, 1.0);
+  if (!dev_body) {
+    dom.x.assign(NN, 1e40); dom.y.assign(NN, 1e40);
+    dom.xq.assign(NN, 1.0); dom.xr.assign(NN, 0.0); dom.yq.assign(NN, 0.0); dom.yr.assign(NN, 1.0);
+    dom.J.assign(NN, 1.0); dom.Ji.assign(NN, 1.0);
+  }
   for (int b = 0; b < nblocks; ++b) {
     BlockIn& B = dom.bin[b];
     if (B.nx < minpts || B.ny < minpts)
@@ -644,35 +648,18 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     if (B.bndfile[3].empty()) line_map(B.curve[3], B.LT, B.RT, B.mgx, B.pgx, qmin, qmax, B.bndmap[3]);
     else read_curve(B.curve[3], join_path(base, B.bndfile[3]), B.nx);
     for (int k = 0; k < B.nx; ++k) { B.curve[3].n1[k] = -B.curve[3].n1[k]; B.curve[3].n2[k] = -B.curve[3].n2[k]; }
-    // transfinite_interp (geometry.f90:153-200)
-    double Wq = qmax - qmin, Wr = rmax - rmin;
-    if (Wq == 0.0) Wq = 1.0;
-    if (Wr == 0.0) Wr = 1.0;
-    const Curve &cL = B.curve[0], &cR = B.curve[1], &cB = B.curve[2], &cT = B.curve[3];
+    // transfinite_interp (geometry.f90:153-200); left to the device when it builds the body
+    if (dev_body) continue;
     for (int j = B.mgy; j <= B.pgy; ++j)
       for (int i = B.mgx; i <= B.pgx; ++i) {
-        double q = i, r = j;
-        int kj = j - B.mgy, ki = i - B.mgx;
-        double xv = (qmax - q) * cL.x[kj] / Wq + (q - qmin) * cR.x[kj] / Wq +
-                    (rmax - r) * cB.x[ki] / Wr + (r - rmin) * cT.x[ki] / Wr -
-                    (qmax - q) * (rmax - r) * B.LB[0] / (Wq * Wr) -
-                    (qmax - q) * (r - rmin) * B.LT[0] / (Wq * Wr) -
-                    (q - qmin) * (rmax - r) * B.RB[0] / (Wq * Wr) -
-                    (q - qmin) * (r - rmin) * B.RT[0] / (Wq * Wr);
-        double yv = (qmax - q) * cL.y[kj] / Wq + (q - qmin) * cR.y[kj] / Wq +
-                    (rmax - r) * cB.y[ki] / Wr + (r - rmin) * cT.y[ki] / Wr -
-                    (qmax - q) * (rmax - r) * B.LB[1] / (Wq * Wr) -
-                    (qmax - q) * (r - rmin) * B.LT[1] / (Wq * Wr) -
-                    (q - qmin) * (rmax - r) * B.RB[1] / (Wq * Wr) -
-                    (q - qmin) * (r - rmin) * B.RT[1] / (Wq * Wr);
-        dom.x[gidx(d, i, j)] = xv;
-        dom.y[gidx(d, i, j)] = yv;
+        dom.x[gidx(d, i, j)] = node_coord(B, i, j, 0);
+        dom.y[gidx(d, i, j)] = node_coord(B, i, j, 1);
       }
   }
 
   // ---- metrics (init_grid_partials, grid.f90:465-618)
   double hmin = 1e40, hmax = 0.0;
-  for (int b = 0; b < nblocks; ++b) {
+  for (int b = 0; b < nblocks && !dev_body; ++b) {
     BlockIn& B = dom.bin[b];
     std::vector<double> f, Df;
     for (int j = B.mgy; j <= B.pgy; ++j) {
@@ -702,8 +689,8 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     for (int j = B.mgy; j <= B.pgy; ++j)
       for (int i = B.mgx; i <= B.pgx; ++i) {
         size_t g = gidx(d, i, j);
-        double dxv = std::fabs(dom.J[g] / std::sqrt(dom.xr[g] * dom.xr[g] + dom.yr[g] * dom.yr[g]));
-        double dyv = std::fabs(dom.J[g] / std::sqrt(dom.xq[g] * dom.xq[g] + dom.yq[g] * dom.yq[g]));
+        double dxv = fdmap::spacing_q(dom.J[g], dom.xr[g], dom.yr[g]);
+        double dyv = fdmap::spacing_r(dom.J[g], dom.xq[g], dom.yq[g]);
         hmin = std::min(hmin, std::min(dxv, dyv));
         hmax = std::max(hmax, std::max(dxv, dyv));
       }
@@ -741,8 +728,12 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
   }
 
   // ---- fields (init_fields, fields.f90:57-278, 774-897)
-  dom.F.assign(NN * nF, 1e40);
-  dom.DF.assign(NN * nF, 1e40);
+  if (!dev_body) {
+    dom.F.assign(NN * nF, 1e40);
+    dom.DF.assign(NN * nF, 1e40);
+  } else {
+    dom.bbody.assign(nblocks, fdmap_block_body{});
+  }
   for (int b = 0; b < nblocks; ++b) {
     BlockIn& B = dom.bin[b];
     size_t mk = seek_marker(text, "!---BLOCK" + std::to_string(b + 1) + "---");
@@ -769,6 +760,15 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     if (mode == 2) { F0[0] = vx0; F0[1] = vy0; F0[2] = sxx0; F0[3] = sxy0; F0[4] = syy0; F0[5] = szz0; }
     else { F0[0] = vz0; F0[1] = sxz0; F0[2] = syz0; }
     for (int k = 0; k < 5; ++k) perturb_vector(P[k], mode, Pv[k]);
+    if (dev_body) {
+      fdmap_block_body& bb = dom.bbody[b];
+      for (int l = 0; l < nF; ++l) bb.F0[l] = F0[l];
+      for (int k = 0; k < 5; ++k) {
+        bb.p[k].shape = P[k].code;
+        bb.p[k].x0 = P[k].x0; bb.p[k].y0 = P[k].y0; bb.p[k].Lx = P[k].Lx; bb.p[k].Ly = P[k].Ly;
+        for (int l = 0; l < nF; ++l) bb.p[k].v[l] = Pv[k][l];
+      }
+    }
     // sides (P1..P4 only)
     for (int s = 0; s < 4; ++s) {
       const Curve& c = B.curve[s];
@@ -782,7 +782,8 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
           S.F0[k + (size_t)n * l] = F0[l] + A[0] * Pv[0][l] + A[1] * Pv[1][l] + A[2] * Pv[2][l] + A[3] * Pv[3][l];
       }
     }
-    // interior (P1..P5)
+    // interior (P1..P5); left to the device when it builds the body
+    if (dev_body) continue;
     for (int j = B.mgy; j <= B.pgy; ++j)
       for (int i = B.mgx; i <= B.pgx; ++i) {
         size_t g = gidx(d, i, j);
@@ -798,10 +799,29 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     for (int s = 0; s < 4; ++s) {
       int n = (s < 2) ? B.ny : B.nx;
       SideStore& S = B.side[s];
-      S.M.assign((size_t)n * 5, 1e40);
       S.normal.resize((size_t)n * 2);
       S.x = B.curve[s].x;
       S.y = B.curve[s].y;
+      if (dev_body) {
+        // the device derives M from its own metrics; it needs the side material
+        for (int k = 0; k < n; ++k) {
+          S.normal[k] = B.curve[s].n1[k];
+          S.normal[k + n] = B.curve[s].n2[k];
+        }
+        if (B.heterogeneous) {
+          B.side_mat[s].resize((size_t)n * 3);
+          for (int k = 0; k < n; ++k) {
+            int i = s == 0 ? B.mgx : (s == 1 ? B.pgx : B.mgx + k);
+            int j = s == 2 ? B.mgy : (s == 3 ? B.pgy : B.mgy + k);
+            size_t g = gidx(d, i, j);
+            B.side_mat[s][k] = dom.rho[g];
+            B.side_mat[s][k + n] = dom.cs[g];
+            B.side_mat[s][k + 2 * (size_t)n] = dom.cp[g];
+          }
+        }
+        continue;
+      }
+      S.M.assign((size_t)n * 5, 1e40);
       for (int k = 0; k < n; ++k) {
         S.normal[k] = B.curve[s].n1[k];
         S.normal[k + n] = B.curve[s].n2[k];
@@ -816,11 +836,7 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
         else { rho = B.rho; cs = B.cs; cp = B.cp; }
         double mag = (s < 2) ? std::sqrt(dom.xr[g] * dom.xr[g] + dom.yr[g] * dom.yr[g])
                              : std::sqrt(dom.xq[g] * dom.xq[g] + dom.yq[g] * dom.yq[g]);
-        S.M[k + 0 * (size_t)n] = rho * cs;
-        S.M[k + 1 * (size_t)n] = rho * cp;
-        S.M[k + 2 * (size_t)n] = 1.0 - 2.0 * ((cs / cp) * (cs / cp));
-        S.M[k + 3 * (size_t)n] = op.H00i * cs * mag / dom.J[g];
-        S.M[k + 4 * (size_t)n] = op.H00i * cp * mag / dom.J[g];
+        fdmap::edge_impedances(rho, cs, cp, mag, dom.J[g], op.H00i, &S.M[k], n);
       }
     }
   }
@@ -862,26 +878,28 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     }
     fb.src_ok = 0;
     if (src.use_singular) {
+      // the search reads the bottom row of x and the left column of y only
+      // (interpolated here when the device builds the body)
       std::vector<double> xs(B.nx), ys(B.ny);
-      for (int i = B.mgx; i <= B.pgx; ++i) xs[i - B.mgx] = dom.x[gidx(d, i, B.mgy)];
-      for (int j = B.mgy; j <= B.pgy; ++j) ys[j - B.mgy] = dom.y[gidx(d, B.mgx, j)];
+      for (int i = B.mgx; i <= B.pgx; ++i) xs[i - B.mgx] = dev_body ? node_coord(B, i, B.mgy, 0) : dom.x[gidx(d, i, B.mgy)];
+      for (int j = B.mgy; j <= B.pgy; ++j) ys[j - B.mgy] = dev_body ? node_coord(B, B.mgx, j, 1) : dom.y[gidx(d, B.mgx, j)];
       bool outx, outy;
       int i0 = search_floor(xs.data(), B.nx, src.x0, &outx) + B.mgx - 1;
       int j0 = search_floor(ys.data(), B.ny, src.y0, &outy) + B.mgy - 1;
       if (!outx && !outy) {
         fb.src_ok = 1;
         fb.src_i0 = i0; fb.src_j0 = j0;
-        fb.src_hx = dom.x[gidx(d, B.mgx + 1, B.mgy)] - dom.x[gidx(d, B.mgx, B.mgy)];
-        fb.src_hy = dom.y[gidx(d, B.mgx, B.mgy + 1)] - dom.y[gidx(d, B.mgx, B.mgy)];
-        fb.src_ax = (src.x0 - dom.x[gidx(d, i0, B.mgy)]) / fb.src_hx;
-        fb.src_ay = (src.y0 - dom.y[gidx(d, B.mgx, j0)]) / fb.src_hy;
+        fb.src_hx = xs[1] - xs[0];
+        fb.src_hy = ys[1] - ys[0];
+        fb.src_ax = (src.x0 - xs[i0 - B.mgx]) / fb.src_hx;
+        fb.src_ay = (src.y0 - ys[j0 - B.mgy]) / fb.src_hy;
       }
     }
   }
 
   // ---- time step (set_dt, domain.f90:1462-1535)
+  double cmax;
   {
-    if (hmin <= 0.0) fail(FDMAP_ERR_INVALID_ARG, "Minimum grid spacing must be positive");
     double cs = 0, cp = 0;
     if (any_het) {
       cs = -HUGE_VAL; cp = -HUGE_VAL;
@@ -889,26 +907,30 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
     } else {
       for (auto& B : dom.bin) { cs = std::max(cs, B.cs); cp = std::max(cp, B.cp); }
     }
-    double c = std::sqrt(cs * cs + cp * cp);
-    dt = dt / refine;
-    if (CFL == 0.0) {
-      if (dt == 0.0) { CFL = 0.5; dt = CFL * hmin / c; }
-      else CFL = c * dt / hmin;
-    } else {
-      if (dt == 0.0) dt = CFL * hmin / c;
-      else CFL = c * dt / hmin;
-    }
+    cmax = std::sqrt(cs * cs + cp * cp);
   }
-  if (nt == 0) nt = (int)std::ceil(tend / dt);
-  else nt = (int)std::ceil((double)(nt - 1) * refine) + 1;
-  d.t0 = t0; d.dt = dt; d.CFL = CFL; d.nt = nt; d.hmin = hmin; d.hmax = hmax;
-  // artificial dissipation scaled as (wave speed)/(grid spacing) (domain.f90:317-320)
-  for (int b = 0; b < nblocks; ++b) {
-    BlockIn& B = dom.bin[b];
-    if (B.Cdiss > 0.0 && B.heterogeneous)
+  for (int b = 0; b < nblocks; ++b)
+    if (dom.bin[b].Cdiss > 0.0 && dom.bin[b].heterogeneous)
       fail(FDMAP_ERR_UNSUPPORTED, "artificial dissipation in a heterogeneous block is not supported");
-    B.Cdiss = B.Cdiss * CFL / dt;
-    dom.blocks[b].Cdiss = B.Cdiss;
+  d.t0 = t0;
+  if (dev_body) {
+    // finished by fdmap_host_set_spacing once the device has reduced hmin, hmax
+    dom.body.dt_in = dt; dom.body.CFL_in = CFL; dom.body.refine = refine; dom.body.tend = tend;
+    dom.body.nt_in = nt; dom.body.c = cmax;
+    for (int b = 0; b < nblocks; ++b) dom.bbody[b].Cdiss = dom.bin[b].Cdiss;
+    dom.body.blocks = dom.bbody.data();
+    d.dt = NAN; d.CFL = NAN; d.nt = 0; d.hmin = NAN; d.hmax = NAN;
+    for (int b = 0; b < nblocks; ++b) dom.blocks[b].Cdiss = 0.0;
+  } else {
+    if (hmin <= 0.0) fail(FDMAP_ERR_INVALID_ARG, "Minimum grid spacing must be positive");
+    fdmap::finish_time_step(dt, CFL, refine, tend, nt, cmax, hmin, &dt, &CFL, &nt);
+    d.dt = dt; d.CFL = CFL; d.nt = nt; d.hmin = hmin; d.hmax = hmax;
+    // artificial dissipation scaled as (wave speed)/(grid spacing) (domain.f90:317-320)
+    for (int b = 0; b < nblocks; ++b) {
+      BlockIn& B = dom.bin[b];
+      B.Cdiss = B.Cdiss * CFL / dt;
+      dom.blocks[b].Cdiss = B.Cdiss;
+    }
   }
 
   // ---- interfaces (get_iface_neighbors, init_iface, init_iface_blocks, init_friction,
@@ -1064,10 +1086,26 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
   d.blocks = dom.blocks.data();
   d.ifaces = dom.ifaces.data();
   d.heterogeneous = any_het ? 1 : 0;
-  d.F = dom.F.data(); d.DF = dom.DF.data();
-  d.x = dom.x.data(); d.y = dom.y.data();
-  d.xq = dom.xq.data(); d.xr = dom.xr.data(); d.yq = dom.yq.data(); d.yr = dom.yr.data();
-  d.J = dom.J.data(); d.Ji = dom.Ji.data();
+  dom.dev_body = dev_body;
+  if (dev_body) {
+    // body arrays and side impedances come from the device
+    for (int b = 0; b < nblocks; ++b)
+      for (int s = 0; s < 4; ++s) {
+        dom.blocks[b].side[s].M = nullptr;
+        dom.bbody[b].side_mat[s] = dom.bin[b].side_mat[s].empty() ? nullptr : dom.bin[b].side_mat[s].data();
+      }
+    for (int b = 0; b < nblocks; ++b)
+      for (int c = 0; c < 2; ++c) {
+        dom.bbody[b].LB[c] = dom.bin[b].LB[c]; dom.bbody[b].LT[c] = dom.bin[b].LT[c];
+        dom.bbody[b].RB[c] = dom.bin[b].RB[c]; dom.bbody[b].RT[c] = dom.bin[b].RT[c];
+      }
+    d.body = &dom.body;
+  } else {
+    d.F = dom.F.data(); d.DF = dom.DF.data();
+    d.x = dom.x.data(); d.y = dom.y.data();
+    d.xq = dom.xq.data(); d.xr = dom.xr.data(); d.yq = dom.yq.data(); d.yr = dom.yr.data();
+    d.J = dom.J.data(); d.Ji = dom.Ji.data();
+  }
   if (any_het) {
     d.rho = dom.rho.data(); d.cs = dom.cs.data(); d.cp = dom.cp.data(); d.G = dom.G.data();
     d.M = dom.M.data(); d.gamma = dom.gamma.data(); d.nu = dom.nu.data();
@@ -1077,12 +1115,18 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base) 
 }  // namespace
 
 extern "C" int fdmap_host_init(const char* input_text, const char* base_dir, fdmap_domain** out) {
+  return fdmap_host_init_ex(input_text, base_dir, 0, out);
+}
+
+extern "C" int fdmap_host_init_ex(const char* input_text, const char* base_dir, int flags, fdmap_domain** out) {
   if (!input_text || !out) { g_last_error = "null argument"; return FDMAP_ERR_INVALID_ARG; }
+  if (flags & ~FDMAP_INIT_BODY_ON_DEVICE) { g_last_error = "unknown initialisation flags"; return FDMAP_ERR_INVALID_ARG; }
   *out = nullptr;
   std::unique_ptr<fdmap_domain> dom(new (std::nothrow) fdmap_domain());
   if (!dom) { g_last_error = "out of memory"; return FDMAP_ERR_NOMEM; }
   try {
-    build(*dom, std::string(input_text), base_dir ? std::string(base_dir) : std::string());
+    build(*dom, std::string(input_text), base_dir ? std::string(base_dir) : std::string(),
+          (flags & FDMAP_INIT_BODY_ON_DEVICE) != 0);
   } catch (const InitError& e) {
     g_last_error = e.msg;
     return e.code;
@@ -1095,6 +1139,19 @@ extern "C" int fdmap_host_init(const char* input_text, const char* base_dir, fdm
   }
   g_last_error.clear();
   *out = dom.release();
+  return FDMAP_OK;
+}
+
+extern "C" int fdmap_host_set_spacing(fdmap_domain* dom, double hmin, double hmax) {
+  if (!dom || !dom->dev_body) { g_last_error = "the domain's body was not left to the device"; return FDMAP_ERR_INVALID_ARG; }
+  if (!(hmin > 0.0)) { g_last_error = "Minimum grid spacing must be positive"; return FDMAP_ERR_INVALID_ARG; }
+  fdmap_desc& d = dom->desc;
+  const fdmap_body& bd = dom->body;
+  double dt, CFL;
+  int nt;
+  fdmap::finish_time_step(bd.dt_in, bd.CFL_in, bd.refine, bd.tend, bd.nt_in, bd.c, hmin, &dt, &CFL, &nt);
+  d.dt = dt; d.CFL = CFL; d.nt = nt; d.hmin = hmin; d.hmax = hmax;
+  for (int b = 0; b < d.nblocks; ++b) dom->blocks[b].Cdiss = dom->bbody[b].Cdiss * CFL / dt;
   return FDMAP_OK;
 }
 

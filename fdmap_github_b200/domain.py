@@ -3,6 +3,7 @@
 The names follow the reference's Fortran routines:
 
   init_domain(input_text, base_dir)   -> HostDomain   (domain.f90:45-378 + main.f90:57-116)
+  init_domain(..., body_on_device=True)                the O(nx*ny) body left to the device
   GpuDomain(host).time_step_LS(t, dt, final_step)     (time_step.f90:71-167)
   GpuDomain(host).run(n_first, n_last)                (main.f90:168-231 loop body)
 
@@ -24,10 +25,15 @@ from .native import FAULT_INDEX, check_gpu, check_host, dptr, lib
 class HostDomain:
     """An initialised FDMAP domain held in host memory (the Fortran driver's state)."""
 
-    def __init__(self, input_text: str, base_dir: str | Path | None = None):
+    def __init__(self, input_text: str, base_dir: str | Path | None = None, body_on_device: bool = False):
         self._h = C.c_void_p()
         base = str(base_dir).encode() if base_dir is not None else None
-        check_host(lib().fdmap_host_init(input_text.encode(), base, C.byref(self._h)), "init_domain")
+        self.body_on_device = bool(body_on_device)
+        flags = native.INIT_BODY_ON_DEVICE if self.body_on_device else 0
+        check_host(lib().fdmap_host_init_ex(input_text.encode(), base, flags, C.byref(self._h)), "init_domain")
+        self._info()
+
+    def _info(self) -> None:
         ints = (C.c_int * 10)()
         dbls = (C.c_double * 5)()
         check_host(lib().fdmap_host_info(self._h, ints, dbls), "fdmap_host_info")
@@ -35,6 +41,17 @@ class HostDomain:
          het) = list(ints)
         self.heterogeneous = bool(het)
         (self.t0, self.dt, self.CFL, self.hmin, self.hmax) = list(dbls)
+
+    @property
+    def spacing_pending(self) -> bool:
+        """True while a domain whose body is left to the device waits for the
+        grid spacings (dt, CFL, nt are not known before)."""
+        return self.body_on_device and not (self.hmin > 0)
+
+    def set_spacing(self, hmin: float, hmax: float) -> None:
+        """Finish set_dt from the grid spacings the device reduced (fdmap_host_set_spacing)."""
+        check_host(lib().fdmap_host_set_spacing(self._h, hmin, hmax), "fdmap_host_set_spacing")
+        self._info()
 
     @property
     def handle(self) -> C.c_void_p:
@@ -109,12 +126,16 @@ class HostDomain:
             pass
 
 
-def init_domain(input_text: str, base_dir: str | Path | None = None) -> HostDomain:
-    """Parse an FDMAP .in text and initialise the domain on the host."""
-    return HostDomain(input_text, base_dir)
+def init_domain(input_text: str, base_dir: str | Path | None = None, body_on_device: bool = False) -> HostDomain:
+    """Parse an FDMAP .in text and initialise the domain on the host.  With
+    body_on_device the grid, metrics, initial body fields and side impedances
+    are built by the engine on the device instead (GpuDomain / GpuEnsemble
+    finish the time step from the spacings it reduces)."""
+    return HostDomain(input_text, base_dir, body_on_device)
 
 
-def init_domains(input_texts: list[str], base_dir: str | Path | None = None, threads: int | None = None) -> list[HostDomain]:
+def init_domains(input_texts: list[str], base_dir: str | Path | None = None, threads: int | None = None,
+                 body_on_device: bool = False) -> list[HostDomain]:
     """Initialise many independent domains (an ensemble's instances) on a pool
     of host threads; the native initialisation releases the interpreter lock."""
     import os
@@ -122,7 +143,7 @@ def init_domains(input_texts: list[str], base_dir: str | Path | None = None, thr
 
     n = threads or min(len(input_texts), os.cpu_count() or 1)
     with ThreadPoolExecutor(max_workers=max(1, n)) as ex:
-        return list(ex.map(lambda t: HostDomain(t, base_dir), input_texts))
+        return list(ex.map(lambda t: HostDomain(t, base_dir, body_on_device), input_texts))
 
 
 class GpuDomain:
@@ -137,6 +158,28 @@ class GpuDomain:
             return
         self._g = C.c_void_p()
         check_gpu(lib().fdmap_gpu_create(host.desc, device, int(init_edges), C.byref(self._g)), "fdmap_gpu_create")
+        _finish_host(host, self)
+
+    def time_params(self) -> tuple[float, float, float, float, float, int]:
+        """(t0, dt, CFL, hmin, hmax, nt) as the engine holds them."""
+        p = (C.c_double * 5)()
+        nt = C.c_int()
+        check_gpu(lib().fdmap_gpu_time_params(self._g, p, C.byref(nt)), "fdmap_gpu_time_params")
+        return (*list(p), nt.value)
+
+    def get_metric(self, name: str) -> np.ndarray:
+        """Metric plane "xq", "xr", "yq", "yr", "Ji" or "J" (dissipative blocks), shape (ny, nx)."""
+        out = np.empty((self.ny, self.nx))
+        check_gpu(lib().fdmap_gpu_get_metric(self._g, native.METRIC_INDEX[name], dptr(out)), "fdmap_gpu_get_metric")
+        return out
+
+    def get_side_impedance(self, b: int, s: int) -> np.ndarray:
+        """Edge impedances (Zs, Zp, gamma, Ks, Kp) of block b, side s: shape (5, n)."""
+        mgx, pgx, mgy, pgy = self.host.block_limits(b)
+        n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+        out = np.empty(5 * n)
+        check_gpu(lib().fdmap_gpu_get_side_impedance(self._g, b, s, dptr(out)), "fdmap_gpu_get_side_impedance")
+        return out.reshape(5, n)
 
     def time_step_LS(self, t0: float, dt: float, final_step: bool = False) -> None:
         check_gpu(lib().fdmap_gpu_time_step(self._g, t0, dt, int(final_step)), "time_step_LS")
@@ -222,6 +265,14 @@ class GpuDomain:
             pass
 
 
+def _finish_host(host: HostDomain, g: GpuDomain) -> None:
+    """A host domain whose body the device built learns its time step from
+    the spacings the engine reduced."""
+    if host.spacing_pending:
+        _, _, _, hmin, hmax, _ = g.time_params()
+        host.set_spacing(hmin, hmax)
+
+
 class GpuEnsemble:
     """Independent domains advanced together by batched launches
     (fdmap_gpu_ensemble_*): one interior march, one interface and one closure
@@ -238,6 +289,7 @@ class GpuEnsemble:
             g = C.c_void_p()
             check_gpu(lib().fdmap_gpu_ensemble_instance(self._e, k, C.byref(g)), "fdmap_gpu_ensemble_instance")
             self.instances.append(GpuDomain(h, _handle=g, _owner=self))
+            _finish_host(h, self.instances[-1])
 
     def __len__(self) -> int:
         return len(self.hosts)

@@ -27,12 +27,20 @@ FAULT_FIELDS = ["D", "Psi", "DPsi", "trup", "V", "O", "S", "N", "S0", "N0",
                 "Ds", "Dn", "DDs", "DDn", "W", "DW", "Nreg", "DNreg"]
 FAULT_INDEX = {n: i for i, n in enumerate(FAULT_FIELDS)}
 
+# FDMAP_INIT_BODY_ON_DEVICE (include/fdmap_host.h)
+INIT_BODY_ON_DEVICE = 1
+
+# FDMAP_METRIC_* (include/fdmap_gpu.h)
+METRIC_INDEX = {"xq": 0, "xr": 1, "yq": 2, "yr": 3, "Ji": 4, "J": 5}
+
 # every exported entry point with (restype, argtypes)
 _DP = C.POINTER(C.c_double)
 _VP = C.c_void_p
 SIGNATURES = {
     # fdmap_host.h
     "fdmap_host_init": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(_VP)]),
+    "fdmap_host_init_ex": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(_VP)]),
+    "fdmap_host_set_spacing": (C.c_int, [_VP, C.c_double, C.c_double]),
     "fdmap_host_desc": (_VP, [_VP]),
     "fdmap_host_desc_mut": (_VP, [_VP]),
     "fdmap_host_free": (None, [_VP]),
@@ -60,6 +68,9 @@ SIGNATURES = {
     "fdmap_gpu_set_fault": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_get_fhat": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_status": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_time_params": (C.c_int, [_VP, _DP, C.POINTER(C.c_int)]),
+    "fdmap_gpu_get_metric": (C.c_int, [_VP, C.c_int, _DP]),
+    "fdmap_gpu_get_side_impedance": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_fault_max_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_output_add": (C.c_int, [_VP, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.c_int]),

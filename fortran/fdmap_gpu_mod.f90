@@ -81,7 +81,30 @@ module fdmap_gpu_mod
      real(c_double) :: t0, dt, CFL
      integer(c_int) :: nt
      real(c_double) :: hmin, hmax
+     type(c_ptr) :: body          ! fdmap_body_t, or c_null_ptr: body arrays given by the host
   end type fdmap_desc_t
+
+  ! on-device initialisation (fdmap_desc.h: fdmap_perturb, fdmap_block_body, fdmap_body)
+  type, bind(C) :: fdmap_perturb_t
+     integer(c_int) :: shape
+     real(c_double) :: x0, y0, Lx, Ly
+     real(c_double) :: v(6)
+  end type fdmap_perturb_t
+
+  type, bind(C) :: fdmap_block_body_t
+     real(c_double) :: LB(2), LT(2), RB(2), RT(2)
+     real(c_double) :: F0(6)
+     type(fdmap_perturb_t) :: p(5)
+     real(c_double) :: Cdiss
+     type(c_ptr) :: side_mat(4)
+  end type fdmap_block_body_t
+
+  type, bind(C) :: fdmap_body_t
+     type(c_ptr) :: blocks
+     real(c_double) :: dt_in, CFL_in, refine, tend
+     integer(c_int) :: nt_in
+     real(c_double) :: c
+  end type fdmap_body_t
 
   interface
 
@@ -147,6 +170,27 @@ module fdmap_gpu_mod
        type(c_ptr), value :: h
        integer(c_long_long), intent(out) :: newton_failures
      end function fdmap_gpu_status
+
+     integer(c_int) function fdmap_gpu_time_params(h, params, nt) bind(C, name='fdmap_gpu_time_params')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: params(5)   ! t0, dt, CFL, hmin, hmax
+       integer(c_int), intent(out) :: nt
+     end function fdmap_gpu_time_params
+
+     integer(c_int) function fdmap_gpu_get_metric(h, which, out) bind(C, name='fdmap_gpu_get_metric')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: which              ! 0 xq, 1 xr, 2 yq, 3 yr, 4 Ji, 5 J
+       real(c_double), intent(out) :: out(*)
+     end function fdmap_gpu_get_metric
+
+     integer(c_int) function fdmap_gpu_get_side_impedance(h, b, s, out) bind(C, name='fdmap_gpu_get_side_impedance')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: b, s
+       real(c_double), intent(out) :: out(*)
+     end function fdmap_gpu_get_side_impedance
 
      subroutine fdmap_gpu_destroy(h) bind(C, name='fdmap_gpu_destroy')
        import :: c_ptr
@@ -280,6 +324,19 @@ module fdmap_gpu_mod
        character(kind=c_char), intent(in) :: input_text(*), base_dir(*)
        type(c_ptr), intent(out) :: dom
      end function fdmap_host_init
+
+     integer(c_int) function fdmap_host_init_ex(input_text, base_dir, flags, dom) bind(C, name='fdmap_host_init_ex')
+       import :: c_int, c_ptr, c_char
+       character(kind=c_char), intent(in) :: input_text(*), base_dir(*)
+       integer(c_int), value :: flags               ! 1 = FDMAP_INIT_BODY_ON_DEVICE
+       type(c_ptr), intent(out) :: dom
+     end function fdmap_host_init_ex
+
+     integer(c_int) function fdmap_host_set_spacing(dom, hmin, hmax) bind(C, name='fdmap_host_set_spacing')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: dom
+       real(c_double), value :: hmin, hmax
+     end function fdmap_host_set_spacing
 
      type(c_ptr) function fdmap_host_desc(dom) bind(C, name='fdmap_host_desc')
        import :: c_ptr

@@ -181,6 +181,47 @@ typedef struct fdmap_source {
   double gx, gy, gz;
 } fdmap_source;
 
+/* shapes of a fields_perturb item (perturb_fields, fields.f90:900-934) */
+enum {
+  FDMAP_PERTURB_NONE = 0, /* '' */
+  FDMAP_PERTURB_LINEAR = 1,
+  FDMAP_PERTURB_BOXCAR = 2,
+  FDMAP_PERTURB_TRIANGLE = 3,
+  FDMAP_PERTURB_SMOOTH = 4,
+  FDMAP_PERTURB_GAUSSIAN = 5
+};
+
+/* one fields_perturb item (fields.f90:61-67) */
+typedef struct fdmap_perturb {
+  int shape;       /* FDMAP_PERTURB_* */
+  double x0, y0, Lx, Ly;
+  double v[6];     /* perturbation field vector in the mode's field order */
+} fdmap_perturb;
+
+/* What the device needs to build one block's body itself (on-device
+ * initialisation): the grid follows from the side curves (fdmap_side x, y)
+ * and these corners, the initial fields from F0 and the perturbations. */
+typedef struct fdmap_block_body {
+  double LB[2], LT[2], RB[2], RT[2]; /* block corners (block_list, grid.f90:120-150) */
+  double F0[6];                      /* initial fields in the mode's field order */
+  fdmap_perturb p[5];                /* fields_list p1..p5 */
+  double Cdiss;                      /* operator_list Cdiss before the CFL/dt scaling */
+  double* side_mat[4];               /* heterogeneous blocks: (n,3) rho, cs, cp at the
+                                        side nodes; NULL for homogeneous blocks */
+} fdmap_block_body;
+
+/* On-device initialisation: when fdmap_desc.body is set, the body arrays
+ * (F, DF, x, y, metrics, J, Ji) and the side impedances fdmap_side.M are left
+ * NULL by the host and the engine builds them on the device (grid.f90:391-618,
+ * fields.f90:774-897, domain.f90:1349-1459), reducing hmin and hmax there; the
+ * time step is then finished from these set_dt inputs (domain.f90:1462-1535). */
+typedef struct fdmap_body {
+  fdmap_block_body* blocks; /* nblocks */
+  double dt_in, CFL_in, refine, tend;
+  int nt_in;
+  double c;                 /* sqrt(cs_max^2 + cp_max^2) */
+} fdmap_body;
+
 /* the whole domain (domain_type, domain.f90:24-39) */
 typedef struct fdmap_desc {
   int mode;             /* 2 = plane strain (nF=6), 3 = antiplane (nF=3) */
@@ -201,6 +242,9 @@ typedef struct fdmap_desc {
   double t0, dt, CFL;
   int nt;
   double hmin, hmax;
+  /* non-NULL: body built on the device (t0 is final; dt, CFL, nt, hmin, hmax
+   * are finished by the engine, fdmap_gpu_time_params) */
+  const fdmap_body* body;
 } fdmap_desc;
 
 #ifdef __cplusplus

@@ -71,6 +71,25 @@ int fdmap_gpu_set_fault(fdmap_gpu* h, int iface, int field, const double* in);
 /* Hat variables Fhat(n,nF) of side s (0..3 = L,R,B,T) of block b. */
 int fdmap_gpu_get_fhat(fdmap_gpu* h, int b, int s, double* out);
 
+/* Time-loop parameters params[5] = t0, dt, CFL, hmin, hmax and nt.  For a
+ * descriptor with fdmap_desc.body these are the engine's own: hmin and hmax
+ * reduced over the grid it built on the device, dt, CFL and nt finished from
+ * them as set_dt does (domain.f90:1462-1535); hand hmin, hmax to
+ * fdmap_host_set_spacing to finish the host domain identically.  Otherwise
+ * they are the descriptor's. */
+int fdmap_gpu_time_params(fdmap_gpu* h, double* params, int* nt);
+
+/* One metric plane in the global (nx,ny) layout (grid.f90:465-618): the
+ * metric terms as the engine holds them, whether uploaded or built on the
+ * device.  FDMAP_METRIC_J exists for dissipative blocks only. */
+enum { FDMAP_METRIC_XQ = 0, FDMAP_METRIC_XR = 1, FDMAP_METRIC_YQ = 2, FDMAP_METRIC_YR = 3, FDMAP_METRIC_JI = 4,
+       FDMAP_METRIC_J = 5 };
+int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out);
+
+/* Edge impedances M(n,5) = Zs, Zp, gamma, Ks, Kp of side s (0..3 = L,R,B,T)
+ * of block b as the engine holds them (init_edges, domain.f90:1349-1459). */
+int fdmap_gpu_get_side_impedance(fdmap_gpu* h, int b, int s, double* out);
+
 /* Device status: Newton failures so far (the reference stops on the first). */
 int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
 

@@ -31,6 +31,24 @@ typedef struct fdmap_domain fdmap_domain; /* owns every array the descriptor poi
  * fdmap_host_last_error() then describes the failure. */
 int fdmap_host_init(const char* input_text, const char* base_dir, fdmap_domain** out);
 
+/* Flags of fdmap_host_init_ex. */
+enum { FDMAP_INIT_BODY_ON_DEVICE = 1 };
+
+/* As fdmap_host_init.  With FDMAP_INIT_BODY_ON_DEVICE the host does only the
+ * O(nx + ny) part of init_domain (input, edge curves, side initial fields and
+ * normals, interfaces and friction, the source search) and leaves the
+ * O(nx * ny) body -- transfinite grid and metrics (grid.f90:391-618), initial
+ * fields (fields.f90:774-897), side impedances (domain.f90:1349-1459) -- to
+ * the engine, which builds it on the device from fdmap_desc.body.  dt, CFL,
+ * hmin and hmax stay NaN (nt 0) until fdmap_host_set_spacing. */
+int fdmap_host_init_ex(const char* input_text, const char* base_dir, int flags, fdmap_domain** out);
+
+/* Finish set_dt (domain.f90:1462-1535) of a domain initialised with
+ * FDMAP_INIT_BODY_ON_DEVICE from the grid spacings the engine reduced
+ * (fdmap_gpu_time_params): dt, CFL, nt, hmin, hmax and the CFL/dt-scaled Cdiss
+ * of every block, with the arithmetic of fdmap_host_init. */
+int fdmap_host_set_spacing(fdmap_domain* dom, double hmin, double hmax);
+
 /* The descriptor of an initialised domain (owned by the domain). */
 const fdmap_desc* fdmap_host_desc(const fdmap_domain* dom);
 
