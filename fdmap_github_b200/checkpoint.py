@@ -4,7 +4,9 @@ The files follow checkpoint_op (checkpoint.f90:254-288) for a single-process
 run: native-endian float64, Fortran column-major arrays, no headers.
 
   <name>F.ckpt<n>                 F(:,:,l) for l = 1..nF over the global grid,
-                                  then DF(:,:,l)          (fields.f90:335-429)
+                                  then DF(:,:,l), then the perfectly matched
+                                  layer fields Wx(:,:,:) and Wy(:,:,:) when the
+                                  domain has them          (fields.f90:335-429)
   <name>block<b><S>.ckpt<n>       for S = L, R, B, T: per field l the side's
                                   edge values F(:,l), hat variables Fhat(:,l),
                                   prestress F0(:,l); then the boundary energy
@@ -50,7 +52,11 @@ def checkpoint_write(gpu, host, name: str | Path, number: int) -> list[Path]:
     F, DF = gpu.get_fields(True, True)
     files = []
     p = Path(f"{name}F.ckpt{number}")
-    np.concatenate([F.reshape(-1), DF.reshape(-1)]).astype(np.float64).tofile(p)
+    parts = [F.reshape(-1), DF.reshape(-1)]
+    for w, present in zip(("Wx", "Wy"), host.pml_fields()):
+        if present:
+            parts.append(gpu.get_pml(w).reshape(-1))
+    np.concatenate(parts).astype(np.float64).tofile(p)
     files.append(p)
     for b in range(host.nblocks):
         for s in range(4):
@@ -85,9 +91,13 @@ def checkpoint_read(gpu, host, name: str | Path, number: int | None = None) -> i
         number = int(Path(f"{name}.ckpt").read_text().split()[0])
     nn = host.nF * host.ny * host.nx
     a = np.fromfile(f"{name}F.ckpt{number}", dtype=np.float64)
-    if a.size != 2 * nn:
-        raise ValueError(f"{name}F.ckpt{number}: {a.size} values, expected {2 * nn}")
-    gpu.set_fields(a[:nn].reshape(host.nF, host.ny, host.nx), a[nn:].reshape(host.nF, host.ny, host.nx))
+    pml = [w for w, present in zip(("Wx", "Wy"), host.pml_fields()) if present]
+    if a.size != (2 + len(pml)) * nn:
+        raise ValueError(f"{name}F.ckpt{number}: {a.size} values, expected {(2 + len(pml)) * nn}")
+    shape = (host.nF, host.ny, host.nx)
+    gpu.set_fields(a[:nn].reshape(shape), a[nn:2 * nn].reshape(shape))
+    for k, w in enumerate(pml):
+        gpu.set_pml(w, a[(2 + k) * nn:(3 + k) * nn].reshape(shape))
     for i in range(host.nifaces):
         if host.iface_info(i)[3] != COUPLING_FRICTION:
             continue

@@ -51,6 +51,11 @@ struct DevBlock {
   double src_wx[5], src_wy[5];         // singular_source weights d for i0-2..i0+2
   double Cdiss;                        // scaled artificial dissipation (0: none)
   double* J;                           // Jacobian plane (dissipative blocks only)
+  int pml;                             // perfectly matched layer: bit 0 Wx (pmlx), bit 1 Wy (pmly); 0 = none
+  double pml_kappa;                    // frequency shift
+  const double* pml_h;                 // [3][3][2] hxi, hyi of each region (q, r: 0 minus end, 1 plus end, 2 central)
+  const double* pml_s;                 // 2 planes: damping sx, sy at every node
+  double *Wx, *DWx, *Wy, *DWy;         // auxiliary fields and rates, nF planes each (NULL when off)
   int tile_begin;                      // first stencil tile of this block
   int tiles_x;
   long long march_unit_begin;          // first row-group unit of this block (march kernel)

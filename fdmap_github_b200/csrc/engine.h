@@ -60,6 +60,7 @@ struct fdmap_gpu {
   int march_grid = 0;
   int use_march = 1;
   bool dissipation = false;  // some block has Cdiss > 0 (tiled interior kernel)
+  bool pml = false;  // some block has a perfectly matched layer (tiled interior kernel)
   bool body_on_device = false;  // body built by build_body (fdmap_desc.body)
   double tp[5] = {0, 0, 0, 0, 0};  // t0, dt, CFL, hmin, hmax (set_dt)
   int tp_nt = 0;

@@ -375,6 +375,11 @@ int validate(const fdmap_desc* d) {
       return set_err(d->J ? FDMAP_ERR_UNSUPPORTED : FDMAP_ERR_INVALID_ARG,
                      d->J ? "artificial dissipation in heterogeneous blocks is not supported"
                           : "artificial dissipation needs the Jacobian array J");
+    if (d->mode == 2 && (B.pmlx || B.pmly) && B.Cdiss == 0.0 && !(dev_body && d->body->blocks[b].Cdiss > 0.0)) {
+      if (d->heterogeneous) return set_err(FDMAP_ERR_UNSUPPORTED, "a perfectly matched layer needs homogeneous blocks");
+      if (dev_body) return set_err(FDMAP_ERR_UNSUPPORTED, "a perfectly matched layer needs the body arrays on the host");
+      if (B.pml_n > 0.0 && (!d->x || !d->y)) return set_err(FDMAP_ERR_INVALID_ARG, "the PML profile needs x and y");
+    }
     if (nx < 2 * op.nbst || ny < 2 * op.nbst || nx < op.nbnd || ny < op.nbnd)
       return set_err(FDMAP_ERR_UNSUPPORTED, "block too small for the SBP boundary closures");
     for (int s = 0; s < 4; ++s) {
@@ -468,6 +473,49 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       if ((rc = h->alloc_planes(&B.J, 1, g.plane))) return rc;
       if (!d->body && (rc = h->upload_plane(B.J, d->J, g))) return rc;
       h->dissipation = true;
+    }
+    B.pml = 0; B.pml_kappa = 0.0; B.pml_h = nullptr; B.pml_s = nullptr;
+    B.Wx = B.DWx = B.Wy = B.DWy = nullptr;
+    if (d->mode == 2 && (fb.pmlx || fb.pmly) && cdiss_in == 0.0) {
+      // perfectly matched layer (set_rates PML branch, time_step.f90:354-420)
+      B.pml = (fb.pmlx ? 1 : 0) | (fb.pmly ? 2 : 0);
+      B.pml_kappa = fb.pml_kappa;
+      if (fb.pmlx && ((rc = h->alloc_planes(&B.Wx, nF, g.plane)) || (rc = h->alloc_planes(&B.DWx, nF, g.plane))))
+        return rc;
+      if (fb.pmly && ((rc = h->alloc_planes(&B.Wy, nF, g.plane)) || (rc = h->alloc_planes(&B.DWy, nF, g.plane))))
+        return rc;
+      // damping at every node (rates.f90:2065-2068), evaluated once here
+      std::vector<double> damp(2 * (size_t)g.plane, 0.0);
+      for (int j = 0; j < g.ny; ++j)
+        for (int i = 0; i < g.nx; ++i) {
+          double sx = fb.pml_sigma, sy = fb.pml_sigma;
+          if (fb.pml_n > 0.0) {
+            const size_t q = (size_t)(g.mgx - 1 + i) + (size_t)d->nx * (size_t)(g.mgy - 1 + j);
+            const double x = d->x[q], y = d->y[q];
+            sx = fb.pml_sigma * std::pow(std::fabs(std::max(0.0, std::max(fb.pml_mx - x, x - fb.pml_px))), fb.pml_n);
+            sy = fb.pml_sigma * std::pow(std::fabs(std::max(0.0, std::max(fb.pml_my - y, y - fb.pml_py))), fb.pml_n);
+          }
+          damp[(size_t)j * g.pitch + i] = sx;
+          damp[(size_t)g.plane + (size_t)j * g.pitch + i] = sy;
+        }
+      double* ds = nullptr;
+      if ((rc = h->alloc_planes(&ds, 2, g.plane))) return rc;
+      CUDA_TRY(cudaMemcpy(ds, damp.data(), damp.size() * sizeof(double), cudaMemcpyHostToDevice));
+      B.pml_s = ds;
+      // hxi = Ji*yr, hyi = Ji*xq at the first node of each region: q and r
+      // index 0 = minus-end strip, 1 = plus-end strip, 2 = interior
+      double hh[18];
+      const int qi[3] = {0, g.nx - op.nbst, op.nbst}, rj[3] = {0, g.ny - op.nbst, op.nbst};
+      for (int q = 0; q < 3; ++q)
+        for (int r = 0; r < 3; ++r) {
+          const size_t k = (size_t)(g.mgx - 1 + qi[q]) + (size_t)d->nx * (size_t)(g.mgy - 1 + rj[r]);
+          hh[(q * 3 + r) * 2] = d->Ji[k] * d->yr[k];
+          hh[(q * 3 + r) * 2 + 1] = d->Ji[k] * d->xq[k];
+        }
+      double* dh = nullptr;
+      if ((rc = h->upload(&dh, hh, 18))) return rc;
+      B.pml_h = dh;
+      h->pml = true;
     }
     B.rinv_b = 1.0 / fb.rho;
     for (int s = 1; s <= op.pI; ++s) {
@@ -620,7 +668,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   {
     const char* ek = getenv("FDMAP_STENCIL");
     // dissipative blocks need J at the neighbours, which the march ring does not carry
-    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation;
+    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation && !h->pml;
     if (h->use_march && (rc = march_dispatch(h, nullptr))) return rc;
     // fused stage launches need every interface-side node to sit on one interface only
     bool junction = false;
@@ -889,6 +937,46 @@ int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out) {
     CUDA_TRY(cudaGetLastError());
   }
   CUDA_TRY(cudaMemcpyAsync(out, h->d_global, (size_t)NN * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+// PML field Wx (which = 0) or Wy (1) in the global (nx,ny,nF) layout
+int fdmap_gpu_get_pml(fdmap_gpu* h, int which, double* out) {
+  if (!h || !out || which < 0 || which > 1) return set_err(FDMAP_ERR_INVALID_ARG, "bad get_pml arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  const int nF = h->nF;
+  const long long NN = (long long)h->nx_g * h->ny_g;
+  CUDA_TRY(cudaMemsetAsync(h->d_global, 0, (size_t)NN * nF * sizeof(double), h->stream));
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const double* W = which == 0 ? h->hdom.blk[b].Wx : h->hdom.blk[b].Wy;
+    if (!W) continue;
+    const BlockGeom& g = h->geom[b];
+    dim3 grid((g.pitch + 255) / 256, g.ny);
+    gather_block<<<grid, 256, 0, h->stream>>>(W, h->d_global, h->nx_g, NN, g.mgx, g.mgy, g.nx, g.ny, g.pitch, g.plane,
+                                              nF);
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaMemcpyAsync(out, h->d_global, (size_t)NN * nF * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_pml(fdmap_gpu* h, int which, const double* in) {
+  if (!h || !in || which < 0 || which > 1) return set_err(FDMAP_ERR_INVALID_ARG, "bad set_pml arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  const int nF = h->nF;
+  const long long NN = (long long)h->nx_g * h->ny_g;
+  CUDA_TRY(cudaMemcpyAsync(h->d_global, in, (size_t)NN * nF * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    double* W = which == 0 ? h->hdom.blk[b].Wx : h->hdom.blk[b].Wy;
+    if (!W) continue;
+    const BlockGeom& g = h->geom[b];
+    dim3 grid((g.pitch + 255) / 256, g.ny);
+    scatter_block<<<grid, 256, 0, h->stream>>>(h->d_global, W, h->nx_g, NN, g.mgx, g.mgy, g.nx, g.ny, g.pitch, g.plane,
+                                               nF);
+    CUDA_TRY(cudaGetLastError());
+  }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   return FDMAP_OK;
 }

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cctype>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -295,6 +296,9 @@ struct BlockIn {
   double rho = 0, G = 0, cs = 0, cp = 0, M = 0, gamma = 0, nu = 0, Zs = 0, Zp = 0;
   double F0v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   double Cdiss = 0;  // operator_list (domain.f90:172-180), scaled by CFL/dt after set_dt
+  // pml_list (init_pml, material.f90:152-222)
+  bool pmlx = false, pmly = false;
+  double pml_n = 0, pml_sigma = 0, pml_kappa = 0, pml_mx = 0, pml_px = 0, pml_my = 0, pml_py = 0;
   Curve curve[4];
   SideStore side[4];
   std::vector<double> side_mat[4];  // on-device body of a heterogeneous block: rho, cs, cp at side nodes
@@ -561,6 +565,18 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
     if (mk == std::string::npos) fail(FDMAP_ERR_INVALID_ARG, "String '!---BLOCK" + std::to_string(b + 1) + "---' not found in file");
     Namelist ol = read_nml(text, mk, "operator_list");
     B.Cdiss = get_real(ol, "cdiss", 0.0);
+    // pml_list defaults: no layer, sigma = kappa = 0, bounds at -/+huge(0d0).
+    // The reference gives n no default; n = 0 (constant sigma) here.
+    Namelist pml = read_nml(text, mk, "pml_list");
+    B.pmlx = get_bool(pml, "pmlx", false);
+    B.pmly = get_bool(pml, "pmly", false);
+    B.pml_n = get_real(pml, "n", 0.0);
+    B.pml_sigma = get_real(pml, "sigma", 0.0);
+    B.pml_kappa = get_real(pml, "kappa", 0.0);
+    B.pml_mx = get_real(pml, "mx", -DBL_MAX);
+    B.pml_px = get_real(pml, "px", DBL_MAX);
+    B.pml_my = get_real(pml, "my", -DBL_MAX);
+    B.pml_py = get_real(pml, "py", DBL_MAX);
     Namelist gl = read_nml(text, mk, "grid_list");
     B.nx = get_int(gl, "nx", 1);
     B.ny = get_int(gl, "ny", 1);
@@ -865,6 +881,12 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
     fb.mgx = B.mgx; fb.pgx = B.pgx; fb.mgy = B.mgy; fb.pgy = B.pgy;
     fb.rho = B.rho; fb.cs = B.cs; fb.cp = B.cp; fb.G = B.G; fb.M = B.M; fb.gamma = B.gamma; fb.nu = B.nu;
     fb.Cdiss = B.Cdiss;
+    fb.pmlx = B.pmlx ? 1 : 0; fb.pmly = B.pmly ? 1 : 0;
+    fb.pml_n = B.pml_n; fb.pml_sigma = B.pml_sigma; fb.pml_kappa = B.pml_kappa;
+    fb.pml_mx = B.pml_mx; fb.pml_px = B.pml_px; fb.pml_my = B.pml_my; fb.pml_py = B.pml_py;
+    // the PML rates use the block's homogeneous material (rates.f90:2024-2044)
+    if (mode == 2 && (B.pmlx || B.pmly) && B.Cdiss == 0.0 && B.heterogeneous)
+      fail(FDMAP_ERR_UNSUPPORTED, "a perfectly matched layer in a heterogeneous block is not supported");
     for (int q = 0; q < 9; ++q) fb.F0[q] = B.F0v[q];
     for (int s = 0; s < 4; ++s) {
       fdmap_side& fs = fb.side[s];
@@ -1209,6 +1231,17 @@ extern "C" const double* fdmap_host_side_array(const fdmap_domain* dom, int bloc
 extern "C" double fdmap_host_block_cdiss(const fdmap_domain* dom, int block) {
   if (!dom || block < 0 || block >= dom->desc.nblocks) return FDMAP_ERR_INVALID_ARG;
   return dom->desc.blocks[block].Cdiss;
+}
+
+extern "C" int fdmap_host_block_pml(const fdmap_domain* dom, int block, int* flags, double* params) {
+  if (!dom || block < 0 || block >= dom->desc.nblocks) return FDMAP_ERR_INVALID_ARG;
+  const fdmap_block& b = dom->desc.blocks[block];
+  if (flags) { flags[0] = b.pmlx; flags[1] = b.pmly; }
+  if (params) {
+    params[0] = b.pml_n; params[1] = b.pml_sigma; params[2] = b.pml_kappa;
+    params[3] = b.pml_mx; params[4] = b.pml_px; params[5] = b.pml_my; params[6] = b.pml_py;
+  }
+  return FDMAP_OK;
 }
 
 extern "C" int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim) {

@@ -285,6 +285,175 @@ __device__ __forceinline__ bool interior_node(const DevDomain& D, const DevBlock
   return i >= D.nbst && i <= B.nx - 1 - D.nbst && j >= D.nbst && j <= B.ny - 1 - D.nbst;
 }
 
+
+// Perfectly matched layer, mode II (rates_interior_mode2_pml and
+// rates_boundary_mode2_pml, rates.f90:2024-2619): the rates of a PML block at
+// node (i, j), added to acc (the scaled rates plus SAT) in place of the
+// curvilinear split form.  Cartesian differences are scaled by hxi = Ji*yr,
+// hyi = Ji*xq taken at the first node of the node's region; the auxiliary
+// fields Wx, Wy of the node are read, their rates scaled by A, formed here and
+// written back, and on update stages W += Bdt*DW (scale_rates_interior /
+// update_fields_interior, fields.f90:1060-1186).  The reference's interior
+// loop runs to s = 3 with DI(s) = 0 beyond pI; those exact zeros are left out.
+template <int PI_>
+__device__ __forceinline__ void pml_rates(const DevDomain& D, const DevBlock& B, const double* __restrict__ Fin, int i,
+                                          int j, const StageArgs& a, double* acc) {
+  constexpr int NBND = nbnd_of(PI_);
+  constexpr int NF = 6;
+  const int nbst = D.nbst, nx = B.nx, ny = B.ny;
+  const long long pitch = B.pitch, plane = B.plane;
+  const long long c = (long long)j * pitch + i;
+  const int qreg = i < nbst ? 0 : (i > nx - 1 - nbst ? 1 : 2);
+  const int rreg = j < nbst ? 0 : (j > ny - 1 - nbst ? 1 : 2);
+  const double hxi = B.pml_h[(qreg * 3 + rreg) * 2], hyi = B.pml_h[(qreg * 3 + rreg) * 2 + 1];
+  const double sx = B.pml_s[c], sy = B.pml_s[plane + c];
+  const double rho = B.rho_b, G = B.G_b, M = B.M_b, gamma = B.gamma_b;
+  const bool onx = B.pml & 1, ony = (B.pml >> 1) & 1;
+  const bool load = a.scale && a.A != 0.0;
+  double dwx[NF], dwy[NF];
+  if (onx) {
+    double w[NF];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      w[l] = B.Wx[l * plane + c];
+      dwx[l] = load ? a.A * B.DWx[l * plane + c] : 0.0;
+    }
+    acc[0] = acc[0] - w[2] / rho;
+    acc[1] = acc[1] - w[3] / rho;
+    acc[2] = acc[2] - w[0] * M;
+    acc[3] = acc[3] - w[1] * G;
+    acc[4] = acc[4] - w[0] * gamma * M;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] - (sx + B.pml_kappa) * w[l];
+  }
+  if (ony) {
+    double w[NF];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      w[l] = B.Wy[l * plane + c];
+      dwy[l] = load ? a.A * B.DWy[l * plane + c] : 0.0;
+    }
+    acc[0] = acc[0] - w[3] / rho;
+    acc[1] = acc[1] - w[4] / rho;
+    acc[2] = acc[2] - w[1] * gamma * M;
+    acc[3] = acc[3] - w[0] * G;
+    acc[4] = acc[4] - w[1] * M;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] - (sy + B.pml_kappa) * w[l];
+  }
+  double f[NF];
+  auto at = [&](int ii, int jj) {
+    const long long k = (long long)jj * pitch + ii;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) f[l] = Fin[l * plane + k];
+  };
+  auto diff = [&](int ip, int jp, int im, int jm) {
+    const long long kp = (long long)jp * pitch + ip, km = (long long)jm * pitch + im;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) f[l] = Fin[l * plane + kp] - Fin[l * plane + km];
+  };
+  // q- and r-direction contributions of the point values (or differences) f with weight w
+  auto qterm = [&](double w) {
+    if (onx) {
+#pragma unroll
+      for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] + sx * hxi * f[l] * w;
+    }
+    acc[0] = acc[0] + hxi * f[2] * w / rho;
+    acc[1] = acc[1] + hxi * f[3] * w / rho;
+    acc[2] = acc[2] + hxi * f[0] * w * M;
+    acc[3] = acc[3] + hxi * f[1] * w * G;
+    acc[4] = acc[4] + hxi * f[0] * w * M * gamma;
+  };
+  auto rterm = [&](double w) {
+    if (ony) {
+#pragma unroll
+      for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] + sy * hyi * f[l] * w;
+    }
+    acc[0] = acc[0] + hyi * f[3] * w / rho;
+    acc[1] = acc[1] + hyi * f[4] * w / rho;
+    acc[2] = acc[2] + hyi * f[1] * w * M * gamma;
+    acc[3] = acc[3] + hyi * f[0] * w * G;
+    acc[4] = acc[4] + hyi * f[1] * w * M;
+  };
+  if (qreg == 2 && rreg == 2) {
+    // interior (rates.f90:2089-2126)
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      double dq[NF], dr[NF];
+      const long long kqp = c + s, kqm = c - s, krp = c + s * pitch, krm = c - s * pitch;
+#pragma unroll
+      for (int l = 0; l < NF; ++l) {
+        dq[l] = Fin[l * plane + kqp] - Fin[l * plane + kqm];
+        dr[l] = Fin[l * plane + krp] - Fin[l * plane + krm];
+      }
+      const double DIs = D.DI[s];
+      if (onx) {
+#pragma unroll
+        for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] + sx * hxi * dq[l] * DIs;
+      }
+      if (ony) {
+#pragma unroll
+        for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] + sy * hyi * dr[l] * DIs;
+      }
+      const double as = DIs / rho, bs = DIs * G, cs = DIs * M;
+      acc[0] = acc[0] + (hxi * dq[2] + hyi * dr[3]) * as;
+      acc[1] = acc[1] + (hxi * dq[3] + hyi * dr[4]) * as;
+      acc[2] = acc[2] + (hxi * dq[0] + hyi * dr[1] * gamma) * cs;
+      acc[3] = acc[3] + (hxi * dq[1] + hyi * dr[0]) * bs;
+      acc[4] = acc[4] + (hxi * dq[0] * gamma + hyi * dr[1]) * cs;
+    }
+  } else if (qreg < 2 && rreg < 2) {
+    // corners: one-sided in both directions, q then r for each point
+#pragma unroll
+    for (int s = 0; s < NBND; ++s) {
+      const double wq = qreg == 0 ? D.DL[i][s] : -D.DL[nx - 1 - i][s];
+      const double wr = rreg == 0 ? D.DL[j][s] : -D.DL[ny - 1 - j][s];
+      at(qreg == 0 ? s : nx - 1 - s, j);
+      qterm(wq);
+      at(i, rreg == 0 ? s : ny - 1 - s);
+      rterm(wr);
+    }
+  } else if (qreg < 2) {
+    // L / R strips: one-sided in q, then central in r
+#pragma unroll
+    for (int s = 0; s < NBND; ++s) {
+      at(qreg == 0 ? s : nx - 1 - s, j);
+      qterm(qreg == 0 ? D.DL[i][s] : -D.DL[nx - 1 - i][s]);
+    }
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      diff(i, j + s, i, j - s);
+      rterm(D.DI[s]);
+    }
+  } else {
+    // B / T strips: central in q, then one-sided in r
+#pragma unroll
+    for (int s = 1; s <= PI_; ++s) {
+      diff(i + s, j, i - s, j);
+      qterm(D.DI[s]);
+    }
+#pragma unroll
+    for (int s = 0; s < NBND; ++s) {
+      at(i, rreg == 0 ? s : ny - 1 - s);
+      rterm(rreg == 0 ? D.DL[j][s] : -D.DL[ny - 1 - j][s]);
+    }
+  }
+  if (onx) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      B.DWx[l * plane + c] = dwx[l];
+      if (a.update) B.Wx[l * plane + c] = B.Wx[l * plane + c] + a.Bdt * dwx[l];
+    }
+  }
+  if (ony) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      B.DWy[l * plane + c] = dwy[l];
+      if (a.update) B.Wy[l * plane + c] = B.Wy[l * plane + c] + a.Bdt * dwy[l];
+    }
+  }
+}
+
 // Whole stage for one node of the SBP closure strips: scale, SAT (sides in the
 // reference's order L, R, B, T), one-sided closure rates (rates_boundary_mode2/3),
 // szz, sources, update.  Side `iside` takes the caller's hat variables.
@@ -317,7 +486,11 @@ __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock&
     m.rho = B.rho_b; m.G = B.G_b; m.M = B.M_b; m.gamma = B.gamma_b; m.nu = B.nu_b;
   }
   m.rinv = HET ? 1.0 / m.rho : B.rinv_b;
-  closure_rates<MODE, PI_>(D, B, Fin, i, j, m, B.Ji[c], acc);
+  bool pml = false;
+  if constexpr (MODE == 2) {
+    if (B.pml) { pml_rates<PI_>(D, B, Fin, i, j, a, acc); pml = true; }
+  }
+  if (!pml) closure_rates<MODE, PI_>(D, B, Fin, i, j, m, B.Ji[c], acc);
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
   body_forces<MODE>(D, B, i, j, stage_time(a), acc);
 #pragma unroll
@@ -469,7 +642,11 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
   }
   m.rinv = HET ? 1.0 / m.rho : B.rinv_b;
   const double Ji = B.Ji[c];
-  {
+  bool pml = false;
+  if constexpr (MODE == 2) {
+    if (B.pml) { pml_rates<PI_>(D, B, Fin, i, j, a, acc); pml = true; }
+  }
+  if (!pml) {
     const int cx = tx + H, cy = ty + H;
     const double yrc = s_yr[ty][cx], xrc = s_xr[ty][cx];
     const double yqc = s_yq[cy][tx], xqc = s_xq[cy][tx];

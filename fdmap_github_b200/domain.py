@@ -109,6 +109,19 @@ class HostDomain:
             check_host(int(v), "fdmap_host_block_cdiss")
         return v
 
+    def block_pml(self, b: int) -> dict:
+        """pml_list of block b: pmlx, pmly, n, sigma, kappa, mx, px, my, py."""
+        fl = (C.c_int * 2)()
+        pr = (C.c_double * 7)()
+        check_host(lib().fdmap_host_block_pml(self._h, b, fl, pr), "fdmap_host_block_pml")
+        keys = ("n", "sigma", "kappa", "mx", "px", "my", "py")
+        return {"pmlx": bool(fl[0]), "pmly": bool(fl[1]), **dict(zip(keys, list(pr)))}
+
+    def pml_fields(self) -> tuple[bool, bool]:
+        """Whether the domain carries Wx and Wy (some block with pmlx / pmly, fields.f90:203-210)."""
+        p = [self.block_pml(b) for b in range(self.nblocks)]
+        return any(q["pmlx"] for q in p), any(q["pmly"] for q in p)
+
     def block_limits(self, b: int) -> tuple[int, int, int, int]:
         lim = (C.c_int * 4)()
         check_host(lib().fdmap_host_block_limits(self._h, b, lim), "fdmap_host_block_limits")
@@ -172,6 +185,16 @@ class GpuDomain:
         out = np.empty((self.ny, self.nx))
         check_gpu(lib().fdmap_gpu_get_metric(self._g, native.METRIC_INDEX[name], dptr(out)), "fdmap_gpu_get_metric")
         return out
+
+    def get_pml(self, which: str) -> np.ndarray:
+        """Perfectly matched layer field "Wx" or "Wy", shape (nF, ny, nx); zeros outside PML blocks."""
+        out = np.empty((self.nF, self.ny, self.nx))
+        check_gpu(lib().fdmap_gpu_get_pml(self._g, {"Wx": 0, "Wy": 1}[which], dptr(out)), "fdmap_gpu_get_pml")
+        return out
+
+    def set_pml(self, which: str, W) -> None:
+        v = np.ascontiguousarray(W, dtype=np.float64)
+        check_gpu(lib().fdmap_gpu_set_pml(self._g, {"Wx": 0, "Wy": 1}[which], dptr(v)), "fdmap_gpu_set_pml")
 
     def get_side_impedance(self, b: int, s: int) -> np.ndarray:
         """Edge impedances (Zs, Zp, gamma, Ks, Kp) of block b, side s: shape (5, n)."""

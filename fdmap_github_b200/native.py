@@ -47,6 +47,7 @@ SIGNATURES = {
     "fdmap_host_info": (C.c_int, [_VP, C.POINTER(C.c_int), _DP]),
     "fdmap_host_iface_n": (C.c_int, [_VP, C.c_int]),
     "fdmap_host_block_limits": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
+    "fdmap_host_block_pml": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), _DP]),
     "fdmap_host_block_cdiss": (C.c_double, [_VP, C.c_int]),
     "fdmap_host_iface_info": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
     "fdmap_host_iface_xy": (_DP, [_VP, C.c_int, C.c_int]),
@@ -71,6 +72,8 @@ SIGNATURES = {
     "fdmap_gpu_time_params": (C.c_int, [_VP, _DP, C.POINTER(C.c_int)]),
     "fdmap_gpu_get_metric": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_get_side_impedance": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
+    "fdmap_gpu_get_pml": (C.c_int, [_VP, C.c_int, _DP]),
+    "fdmap_gpu_set_pml": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_fault_max_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_output_add": (C.c_int, [_VP, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                        C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_longlong, C.c_int]),

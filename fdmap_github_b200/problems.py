@@ -10,6 +10,7 @@ Units follow FDMAP: km, s, m/s, MPa, g/cm^3, km/s (2670 kg/m^3 -> 2.67,
   rough_fault_rs       mode II rate-and-state on a rough fault         (config "c3")
   heterogeneous_ricker mode III heterogeneous medium, Ricker point force (config "c5")
   ensemble_instance    mode II rate-and-state, planar fault, von Karman prestress (config "c4")
+  pml_pulse            mode II P-SV pulse in a block with a perfectly matched layer
 """
 from __future__ import annotations
 
@@ -42,6 +43,42 @@ def antiplane_pulse(n: int = 201, L: float = 10.0, nt: int = 501, rk: int = 4, c
 {_operator(cdiss)}&material_list rho=2.67d0, cs=3.464d0 /
 &fields_list P5%shape='gaussian', P5%x0={_f(c)}, P5%y0={_f(c)}, P5%Lx={_f(sigma)}, P5%Ly={_f(sigma)}, P5%vz={_f(amp)} /
 """
+
+
+def _pml(pmlx: bool, pmly: bool, npow: float, sigma: float, kappa: float, lo: float, hi: float) -> str:
+    """pml_list of a block (material.f90:152-222): the layer starts at x, y = lo and hi."""
+    t = "T" if pmlx else "F"
+    u = "T" if pmly else "F"
+    return (f"&pml_list pmlx={t}, pmly={u}, n={_f(npow)}, sigma={_f(sigma)}, kappa={_f(kappa)},\n"
+            f"  mx={_f(lo)}, px={_f(hi)}, my={_f(lo)}, py={_f(hi)} /\n")
+
+
+def pml_pulse(n: int = 201, L: float = 10.0, nt: int = 401, rk: int = 4, cfl: float = 0.5, fd: str = "SBP4",
+              width: float = 1.5, npow: float = 2.0, R: float = 1e-3, kappa: float = 0.0, pmlx: bool = True,
+              pmly: bool = True, bc: str = "free", sigma: float | None = None, cdiss: float = 0.0,
+              mode: int = 2) -> str:
+    """Mode II P-SV waves from a Gaussian pulse (vx and sxx) near the centre of an
+    L x L km block of n x n nodes with a perfectly matched layer of `width` km
+    along every side: damping sigma*d^npow at distance d into the layer, sigma
+    chosen for a reflection coefficient R at normal incidence
+    (sigma_max = (npow+1)*cp*ln(1/R)/(2*width)) unless given.  `bc` applies to
+    all four sides ('free' reflects everything the layer lets through)."""
+    cp = 6.0
+    if sigma is None:
+        smax = (npow + 1.0) * cp * np.log(1.0 / R) / (2.0 * width)
+        sigma = smax / width ** npow if npow > 0 else smax
+    c = 0.5 * L
+    f = ("&fields_list P5%shape='gaussian', P5%x0={x0}, P5%y0={y0}, P5%Lx=0.4d0, P5%Ly=0.4d0, "
+         "P5%vx=1d0, P5%sxx=2d0 /\n").format(x0=_f(c - 0.3), y0=_f(c + 0.2))
+    if mode == 3:
+        f = f"&fields_list P5%shape='gaussian', P5%x0={_f(c)}, P5%y0={_f(c)}, P5%Lx=0.4d0, P5%Ly=0.4d0, P5%vz=1d0 /\n"
+    return f"""&problem_list name='pml_pulse', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
+&domain_list mode={mode}, FDmethod='{fd}', nblocks_x=1, nblocks_y=1 /
+!---BLOCK1---
+&grid_list nx={n}, ny={n}, LB=0d0,0d0, LT=0d0,{_f(L)}, RB={_f(L)},0d0, RT={_f(L)},{_f(L)} /
+&boundaries_list bcL='{bc}', bcR='{bc}', bcB='{bc}', bcT='{bc}' /
+{_operator(cdiss)}&material_list rho=2.67d0, cs=3.464d0, cp={_f(cp)} /
+{f}{_pml(pmlx, pmly, npow, sigma, kappa, width, L - width)}"""
 
 
 def rupture_sw(nx: int = 1601, ny: int = 801, h: float = 0.025, nt: int = 4001, rk: int = 4, cfl: float = 0.5,

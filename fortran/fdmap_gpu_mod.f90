@@ -45,6 +45,8 @@ module fdmap_gpu_mod
      integer(c_int) :: src_ok, src_i0, src_j0
      real(c_double) :: src_hx, src_hy, src_ax, src_ay
      real(c_double) :: Cdiss
+     integer(c_int) :: pmlx, pmly                ! pml_list (material.f90:152-222)
+     real(c_double) :: pml_n, pml_sigma, pml_kappa, pml_mx, pml_px, pml_my, pml_py
   end type fdmap_block_t
 
   type, bind(C) :: fdmap_friction_t
@@ -184,6 +186,20 @@ module fdmap_gpu_mod
        integer(c_int), value :: which              ! 0 xq, 1 xr, 2 yq, 3 yr, 4 Ji, 5 J
        real(c_double), intent(out) :: out(*)
      end function fdmap_gpu_get_metric
+
+     integer(c_int) function fdmap_gpu_get_pml(h, which, out) bind(C, name='fdmap_gpu_get_pml')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: which              ! 0 Wx, 1 Wy
+       real(c_double), intent(out) :: out(*)       ! (nx, ny, nF)
+     end function fdmap_gpu_get_pml
+
+     integer(c_int) function fdmap_gpu_set_pml(h, which, in) bind(C, name='fdmap_gpu_set_pml')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       integer(c_int), value :: which
+       real(c_double), intent(in) :: in(*)
+     end function fdmap_gpu_set_pml
 
      integer(c_int) function fdmap_gpu_get_side_impedance(h, b, s, out) bind(C, name='fdmap_gpu_get_side_impedance')
        import :: c_int, c_ptr, c_double

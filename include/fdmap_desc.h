@@ -135,6 +135,13 @@ typedef struct fdmap_block {
   /* artificial dissipation coefficient of the block, already scaled by CFL/dt
    * (operator_list Cdiss, domain.f90:172-180, 319); 0 = no dissipation */
   double Cdiss;
+  /* perfectly matched layer (pml_list, material.f90:152-222): auxiliary fields
+   * Wx (pmlx) / Wy (pmly) with damping sigma*|distance past [mx,px] / [my,py]|^n
+   * (sigma itself when n <= 0) and frequency shift kappa.  Its rates
+   * (rates_*_mode2_pml, rates.f90:2024-2619) replace the block's ordinary ones
+   * in mode II when Cdiss = 0 (time_step.f90:354); mode III ignores it. */
+  int pmlx, pmly;
+  double pml_n, pml_sigma, pml_kappa, pml_mx, pml_px, pml_my, pml_py;
 } fdmap_block;
 
 /* friction state and parameters of one interface (fr_type, friction.f90:38-49) */

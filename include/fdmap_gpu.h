@@ -86,6 +86,12 @@ enum { FDMAP_METRIC_XQ = 0, FDMAP_METRIC_XR = 1, FDMAP_METRIC_YQ = 2, FDMAP_METR
        FDMAP_METRIC_J = 5 };
 int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out);
 
+/* Perfectly matched layer fields (F%Wx, F%Wy, fields.f90:35, 203-210):
+ * which = 0 Wx, 1 Wy, in the global (nx,ny,nF) layout; zeros in blocks
+ * without that layer.  set writes the blocks that have it (resume). */
+int fdmap_gpu_get_pml(fdmap_gpu* h, int which, double* out);
+int fdmap_gpu_set_pml(fdmap_gpu* h, int which, const double* in);
+
 /* Edge impedances M(n,5) = Zs, Zp, gamma, Ks, Kp of side s (0..3 = L,R,B,T)
  * of block b as the engine holds them (init_edges, domain.f90:1349-1459). */
 int fdmap_gpu_get_side_impedance(fdmap_gpu* h, int b, int s, double* out);

@@ -80,6 +80,10 @@ const double* fdmap_host_side_array(const fdmap_domain* dom, int block, int side
  * domain.f90:317-320), or a negative code for a bad index. */
 double fdmap_host_block_cdiss(const fdmap_domain* dom, int block);
 
+/* Perfectly matched layer of block `block` (pml_list, material.f90:152-222):
+ * flags[2] = pmlx, pmly; params[7] = n, sigma, kappa, mx, px, my, py. */
+int fdmap_host_block_pml(const fdmap_domain* dom, int block, int* flags, double* params);
+
 /* Block index limits: lim[4] = mgx, pgx, mgy, pgy (1-based). */
 int fdmap_host_block_limits(const fdmap_domain* dom, int block, int* lim);
 

@@ -33,6 +33,7 @@ def lib() -> C.CDLL:
         L.oracle_set_fields.argtypes = [C.c_void_p, _DP, _DP]
         L.oracle_get_fault.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         L.oracle_get_fhat.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
+        L.oracle_get_pml.argtypes = [C.c_void_p, C.c_int, _DP]
         L.oracle_newton_failures.restype = C.c_longlong
         L.oracle_newton_failures.argtypes = [C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
@@ -88,6 +89,12 @@ class OracleDomain:
         out = np.empty(n * self.nF)
         lib().oracle_get_fhat(self._o, b, s, _p(out))
         return out.reshape(self.nF, n)
+
+    def get_pml(self, which: str) -> np.ndarray:
+        """PML field "Wx" or "Wy", shape (nF, ny, nx); zeros where the domain has none."""
+        out = np.empty((self.nF, self.ny, self.nx))
+        lib().oracle_get_pml(self._o, {"Wx": 0, "Wy": 1}[which], _p(out))
+        return out
 
     def newton_failures(self) -> int:
         return lib().oracle_newton_failures(self._o)

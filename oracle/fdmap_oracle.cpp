@@ -148,6 +148,8 @@ struct Blk {
   int src_ok, src_i0, src_j0;
   double src_hx, src_hy, src_ax, src_ay;
   double Cdiss;  // scaled artificial dissipation (0: set_rates, >0: set_rates_dissipation)
+  bool pmlx, pmly;  // pml_list (material.f90:152-222)
+  double pml_n, pml_sigma, pml_kappa, pml_mx, pml_px, pml_my, pml_py;
 };
 
 struct Fric {
@@ -173,6 +175,7 @@ struct oracle_domain {
   std::vector<Ifc> ifc;
   vec F, DF, x, y, xq, xr, yq, yr, J, Ji;
   vec rho, G, M, gamma, nu;
+  vec Wx, DWx, Wy, DWy;  // PML fields (nx,ny,nF), allocated when some block has pmlx / pmly (fields.f90:203-210)
   fdmap_source src;
   double t;
   long long newton_fail;
@@ -943,6 +946,173 @@ void rates_boundary(Ctx& c, const Blk& B, int mx, int px, int my, int py, int qs
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Perfectly matched layer, mode II (rates_interior_mode2_pml and
+// rates_boundary_mode2_pml, rates.f90:2024-2619).  These replace the
+// curvilinear split-form rates of a block with pmlx or pmly: Cartesian
+// differences scaled by hxi = Ji*yr and hyi = Ji*xq taken at the first node of
+// each region, and the auxiliary fields Wx, Wy.
+// ---------------------------------------------------------------------------
+// damping at a node (rates.f90:2065-2068): sigma, or sigma*|distance past the layer start|^n
+inline void pml_damping(const Blk& B, double x, double y, double& sx, double& sy) {
+  sx = B.pml_sigma;
+  sy = B.pml_sigma;
+  if (B.pml_n > 0.0) {
+    sx = B.pml_sigma * std::pow(std::fabs(std::max(0.0, std::max(B.pml_mx - x, x - B.pml_px))), B.pml_n);
+    sy = B.pml_sigma * std::pow(std::fabs(std::max(0.0, std::max(B.pml_my - y, y - B.pml_py))), B.pml_n);
+  }
+}
+
+// auxiliary-field terms of one node (rates.f90:2070-2088): -W couplings into DF
+// and the decay -(sigma + kappa)*W of DW
+inline void pml_node_terms(oracle_domain& D, const Blk& B, size_t g, double sx, double sy) {
+  const size_t NN = (size_t)D.nx * D.ny;
+  vec& DF = D.DF;
+  const double rho = B.rho, G = B.G, M = B.M, gamma = B.gamma;
+  if (B.pmlx) {
+    const vec& W = D.Wx;
+    DF[g] = DF[g] - W[g + 2 * NN] / rho;
+    DF[g + NN] = DF[g + NN] - W[g + 3 * NN] / rho;
+    DF[g + 2 * NN] = DF[g + 2 * NN] - W[g] * M;
+    DF[g + 3 * NN] = DF[g + 3 * NN] - W[g + NN] * G;
+    DF[g + 4 * NN] = DF[g + 4 * NN] - W[g] * gamma * M;
+    for (int l = 0; l < D.nF; ++l) D.DWx[g + l * NN] = D.DWx[g + l * NN] - (sx + B.pml_kappa) * W[g + l * NN];
+  }
+  if (B.pmly) {
+    const vec& W = D.Wy;
+    DF[g] = DF[g] - W[g + 3 * NN] / rho;
+    DF[g + NN] = DF[g + NN] - W[g + 4 * NN] / rho;
+    DF[g + 2 * NN] = DF[g + 2 * NN] - W[g + NN] * gamma * M;
+    DF[g + 3 * NN] = DF[g + 3 * NN] - W[g] * G;
+    DF[g + 4 * NN] = DF[g + 4 * NN] - W[g + NN] * M;
+    for (int l = 0; l < D.nF; ++l) D.DWy[g + l * NN] = D.DWy[g + l * NN] - (sy + B.pml_kappa) * W[g + l * NN];
+  }
+}
+
+// interior (rates.f90:2024-2129).  The reference runs s = 1..3 with DI(s) = 0
+// beyond pI; those terms add exact zeros and are left out.
+void rates_interior_pml(oracle_domain& D, const Blk& B, int mx, int px, int my, int py) {
+  const size_t NN = (size_t)D.nx * D.ny;
+  const Ops& op = D.op;
+  double a[4], b[4], c[4];
+  for (int s = 1; s <= op.pI; ++s) { a[s] = op.DI[s] / B.rho; b[s] = op.DI[s] * B.G; c[s] = op.DI[s] * B.M; }
+  const double gamma = B.gamma;
+  const size_t g0 = G2(D, mx, my);
+  const double hxi = D.Ji[g0] * D.yr[g0], hyi = D.Ji[g0] * D.xq[g0];
+  vec& DF = D.DF;
+  const vec& F = D.F;
+#pragma omp parallel for schedule(static)
+  for (int j = my; j <= py; ++j)
+    for (int i = mx; i <= px; ++i) {
+      const size_t g = G2(D, i, j);
+      double sx, sy;
+      pml_damping(B, D.x[g], D.y[g], sx, sy);
+      pml_node_terms(D, B, g, sx, sy);
+      for (int s = 1; s <= op.pI; ++s) {
+        const size_t ip = G2(D, i + s, j), im = G2(D, i - s, j), jp = G2(D, i, j + s), jm = G2(D, i, j - s);
+        if (B.pmlx)
+          for (int l = 0; l < D.nF; ++l)
+            D.DWx[g + l * NN] = D.DWx[g + l * NN] + sx * hxi * (F[ip + l * NN] - F[im + l * NN]) * op.DI[s];
+        if (B.pmly)
+          for (int l = 0; l < D.nF; ++l)
+            D.DWy[g + l * NN] = D.DWy[g + l * NN] + sy * hyi * (F[jp + l * NN] - F[jm + l * NN]) * op.DI[s];
+        auto dx = [&](int l) { return F[ip + l * NN] - F[im + l * NN]; };
+        auto dy = [&](int l) { return F[jp + l * NN] - F[jm + l * NN]; };
+        DF[g] = DF[g] + (hxi * dx(2) + hyi * dy(3)) * a[s];
+        DF[g + NN] = DF[g + NN] + (hxi * dx(3) + hyi * dy(4)) * a[s];
+        DF[g + 2 * NN] = DF[g + 2 * NN] + (hxi * dx(0) + hyi * dy(1) * gamma) * c[s];
+        DF[g + 3 * NN] = DF[g + 3 * NN] + (hxi * dx(1) + hyi * dy(0)) * b[s];
+        DF[g + 4 * NN] = DF[g + 4 * NN] + (hxi * dx(0) * gamma + hyi * dy(1)) * c[s];
+      }
+    }
+}
+
+// q-direction (x) contribution of one stencil point: field values at point k
+// with weight w (one-sided) or the difference F(k) - F(km) (central)
+inline void pml_q_term(oracle_domain& D, const Blk& B, size_t g, double sx, double hxi, const double* f, double w) {
+  const size_t NN = (size_t)D.nx * D.ny;
+  vec& DF = D.DF;
+  if (B.pmlx)
+    for (int l = 0; l < D.nF; ++l) D.DWx[g + l * NN] = D.DWx[g + l * NN] + sx * hxi * f[l] * w;
+  DF[g] = DF[g] + hxi * f[2] * w / B.rho;
+  DF[g + NN] = DF[g + NN] + hxi * f[3] * w / B.rho;
+  DF[g + 2 * NN] = DF[g + 2 * NN] + hxi * f[0] * w * B.M;
+  DF[g + 3 * NN] = DF[g + 3 * NN] + hxi * f[1] * w * B.G;
+  DF[g + 4 * NN] = DF[g + 4 * NN] + hxi * f[0] * w * B.M * B.gamma;
+}
+inline void pml_r_term(oracle_domain& D, const Blk& B, size_t g, double sy, double hyi, const double* f, double w) {
+  const size_t NN = (size_t)D.nx * D.ny;
+  vec& DF = D.DF;
+  if (B.pmly)
+    for (int l = 0; l < D.nF; ++l) D.DWy[g + l * NN] = D.DWy[g + l * NN] + sy * hyi * f[l] * w;
+  DF[g] = DF[g] + hyi * f[3] * w / B.rho;
+  DF[g + NN] = DF[g + NN] + hyi * f[4] * w / B.rho;
+  DF[g + 2 * NN] = DF[g + 2 * NN] + hyi * f[1] * w * B.M * B.gamma;
+  DF[g + 3 * NN] = DF[g + 3 * NN] + hyi * f[0] * w * B.G;
+  DF[g + 4 * NN] = DF[g + 4 * NN] + hyi * f[1] * w * B.M;
+}
+
+// boundary regions (rates.f90:2131-2619); qside/rside: -1 central, 0 minus end, 1 plus end
+void rates_boundary_pml(oracle_domain& D, const Blk& B, int mx, int px, int my, int py, int qside, int rside) {
+  const size_t NN = (size_t)D.nx * D.ny;
+  const Ops& op = D.op;
+  const size_t g0 = G2(D, mx, my);
+  const double hxi = D.Ji[g0] * D.yr[g0], hyi = D.Ji[g0] * D.xq[g0];
+  const vec& F = D.F;
+  const int nF = D.nF;
+#pragma omp parallel for schedule(static)
+  for (int j = my; j <= py; ++j)
+    for (int i = mx; i <= px; ++i) {
+      const size_t g = G2(D, i, j);
+      double sx, sy;
+      pml_damping(B, D.x[g], D.y[g], sx, sy);
+      pml_node_terms(D, B, g, sx, sy);
+      double f[6];
+      auto load = [&](size_t k) { for (int l = 0; l < nF; ++l) f[l] = F[k + l * NN]; };
+      auto diff = [&](size_t kp, size_t km) { for (int l = 0; l < nF; ++l) f[l] = F[kp + l * NN] - F[km + l * NN]; };
+      if (qside >= 0 && rside >= 0) {
+        // corners: one-sided in both directions, q then r for each s
+        for (int s = 0; s < op.nbnd; ++s) {
+          double wq, wr;
+          int pq, pr;
+          onesided(op, qside, i, B.mgx, B.pgx, s, wq, pq);
+          onesided(op, rside, j, B.mgy, B.pgy, s, wr, pr);
+          load(G2(D, pq, j));
+          pml_q_term(D, B, g, sx, hxi, f, wq);
+          load(G2(D, i, pr));
+          pml_r_term(D, B, g, sy, hyi, f, wr);
+        }
+      } else if (qside >= 0) {
+        // L / R: one-sided in q, then central in r
+        for (int s = 0; s < op.nbnd; ++s) {
+          double w;
+          int pt;
+          onesided(op, qside, i, B.mgx, B.pgx, s, w, pt);
+          load(G2(D, pt, j));
+          pml_q_term(D, B, g, sx, hxi, f, w);
+        }
+        for (int s = 1; s <= op.pI; ++s) {
+          diff(G2(D, i, j + s), G2(D, i, j - s));
+          pml_r_term(D, B, g, sy, hyi, f, op.DI[s]);
+        }
+      } else {
+        // B / T: central in q, then one-sided in r
+        for (int s = 1; s <= op.pI; ++s) {
+          diff(G2(D, i + s, j), G2(D, i - s, j));
+          pml_q_term(D, B, g, sx, hxi, f, op.DI[s]);
+        }
+        for (int s = 0; s < op.nbnd; ++s) {
+          double w;
+          int pt;
+          onesided(op, rside, j, B.mgy, B.pgy, s, w, pt);
+          load(G2(D, i, pt));
+          pml_r_term(D, B, g, sy, hyi, f, w);
+        }
+      }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Rates with artificial dissipation (set_rates_dissipation, time_step.f90:555-751;
 // rates_dissipation_*_mode2/3, rates.f90:939-2021), homogeneous blocks.
@@ -1073,6 +1243,17 @@ void set_rates(oracle_domain& D, const Blk& B) {
     rates_dissipation_boundary(c, B, pix + 1, B.pgx, B.mgy, miy - 1, 1, 0);   // RB
     rates_dissipation_boundary(c, B, B.mgx, mix - 1, piy + 1, B.pgy, 0, 1);   // LT
     rates_dissipation_boundary(c, B, pix + 1, B.pgx, piy + 1, B.pgy, 1, 1);   // RT
+  } else if (D.mode == 2 && (B.pmlx || B.pmly)) {
+    // set_rates, PML branch (time_step.f90:354-420)
+    rates_interior_pml(D, B, mix, pix, miy, piy);
+    rates_boundary_pml(D, B, B.mgx, mix - 1, miy, piy, 0, -1);        // L
+    rates_boundary_pml(D, B, pix + 1, B.pgx, miy, piy, 1, -1);        // R
+    rates_boundary_pml(D, B, mix, pix, B.mgy, miy - 1, -1, 0);        // B
+    rates_boundary_pml(D, B, mix, pix, piy + 1, B.pgy, -1, 1);        // T
+    rates_boundary_pml(D, B, B.mgx, mix - 1, B.mgy, miy - 1, 0, 0);   // LB
+    rates_boundary_pml(D, B, pix + 1, B.pgx, B.mgy, miy - 1, 1, 0);   // RB
+    rates_boundary_pml(D, B, B.mgx, mix - 1, piy + 1, B.pgy, 0, 1);   // LT
+    rates_boundary_pml(D, B, pix + 1, B.pgx, piy + 1, B.pgy, 1, 1);   // RT
   } else {
     rates_interior(c, B, mix, pix, miy, piy);
     rates_boundary(c, B, B.mgx, mix - 1, miy, piy, 0, -1);        // L
@@ -1164,6 +1345,9 @@ void scale_rates_all(oracle_domain& D, double A) {
   size_t n = D.DF.size();
 #pragma omp parallel for schedule(static)
   for (long long q = 0; q < (long long)n; ++q) D.DF[q] = A * D.DF[q];
+  // scale_rates_interior (fields.f90:1060-1078): the PML rates too
+  for (vec* W : {&D.DWx, &D.DWy})
+    for (double& v : *W) v = A * v;
   for (auto& I : D.ifc)
     if (I.coupling == FDMAP_COUPLING_FRICTION) scale_rates_friction(I.fr, A);
 }
@@ -1172,6 +1356,9 @@ void update_fields_all(oracle_domain& D, double Bdt) {
   size_t n = D.F.size();
 #pragma omp parallel for schedule(static)
   for (long long q = 0; q < (long long)n; ++q) D.F[q] = D.F[q] + Bdt * D.DF[q];
+  // update_fields_interior (fields.f90:1168-1186): the PML fields too
+  for (size_t q = 0; q < D.Wx.size(); ++q) D.Wx[q] = D.Wx[q] + Bdt * D.DWx[q];
+  for (size_t q = 0; q < D.Wy.size(); ++q) D.Wy[q] = D.Wy[q] + Bdt * D.DWy[q];
   for (auto& I : D.ifc)
     if (I.coupling == FDMAP_COUPLING_FRICTION) update_fields_friction(I.fr, Bdt);
 }
@@ -1217,6 +1404,12 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
     B.src_hx = fb.src_hx; B.src_hy = fb.src_hy; B.src_ax = fb.src_ax; B.src_ay = fb.src_ay;
     B.Cdiss = fb.Cdiss;
     if (B.Cdiss > 0.0 && !d->J) { delete o; return nullptr; }
+    B.pmlx = fb.pmlx != 0; B.pmly = fb.pmly != 0;
+    B.pml_n = fb.pml_n; B.pml_sigma = fb.pml_sigma; B.pml_kappa = fb.pml_kappa;
+    B.pml_mx = fb.pml_mx; B.pml_px = fb.pml_px; B.pml_my = fb.pml_my; B.pml_py = fb.pml_py;
+    // Wx / Wy and their rates start at zero (fields.f90:203-210)
+    if (B.pmlx && o->Wx.empty()) { o->Wx.assign(NN * d->nF, 0.0); o->DWx.assign(NN * d->nF, 0.0); }
+    if (B.pmly && o->Wy.empty()) { o->Wy.assign(NN * d->nF, 0.0); o->DWy.assign(NN * d->nF, 0.0); }
     for (int s = 0; s < 4; ++s) {
       const fdmap_side& fs = fb.side[s];
       Side& S = B.side[s];
@@ -1336,6 +1529,16 @@ int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out) {
 }
 
 long long oracle_newton_failures(const oracle_domain* o) { return o ? o->newton_fail : -1; }
+
+// PML field Wx (which = 0) or Wy (1) in the global (nx,ny,nF) layout; zeros when not allocated
+int oracle_get_pml(const oracle_domain* o, int which, double* out) {
+  if (!o || !out || which < 0 || which > 1) return -1;
+  const vec& W = which == 0 ? o->Wx : o->Wy;
+  size_t n = (size_t)o->nx * o->ny * o->nF;
+  if (W.empty()) std::fill(out, out + n, 0.0);
+  else std::copy(W.begin(), W.end(), out);
+  return 0;
+}
 
 int oracle_num_threads(void) {
 #ifdef _OPENMP

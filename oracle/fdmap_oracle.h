@@ -59,6 +59,9 @@ int oracle_get_fault(const oracle_domain* o, int iface, int field, double* out);
 /* Hat variables of side s (0..3) of block b: (n, nF). */
 int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out);
 
+/* PML field Wx (which = 0) or Wy (which = 1), (nx, ny, nF); zeros where none. */
+int oracle_get_pml(const oracle_domain* o, int which, double* out);
+
 /* Number of Newton failures seen so far (the reference warns and retries). */
 long long oracle_newton_failures(const oracle_domain* o);
 

@@ -33,3 +33,31 @@ def test_resume_is_bitwise(require_gpu, tmp_path):
     assert sizes["rupblock1L.ckpt15"] == (3 * h.nF + 2) * 31
     assert sizes["rupblock2T.ckpt15"] == (3 * h.nF + 2) * 61
     assert sizes["rupiface1side1.ckpt15"] == 18 * h.iface_n(0)
+
+
+def test_pml_list_reaches_the_descriptor():
+    h = init_domain(problems.pml_pulse(n=41, L=4.0, width=1.0, pmly=False, kappa=0.25, npow=3.0))
+    p = h.block_pml(0)
+    assert p["pmlx"] and not p["pmly"] and p["n"] == 3.0 and p["kappa"] == 0.25
+    assert (p["mx"], p["px"], p["my"], p["py"]) == (1.0, 3.0, 1.0, 3.0)
+    assert h.pml_fields() == (True, False)
+    q = init_domain(problems.antiplane_pulse(n=21, L=2.0, nt=3)).block_pml(0)
+    assert not q["pmlx"] and q["mx"] == -np.finfo(float).max and q["py"] == np.finfo(float).max
+
+
+@pytest.mark.gpu
+def test_resume_with_pml_is_bitwise(require_gpu, tmp_path):
+    """The F checkpoint carries Wx and Wy after F and DF (fields.f90:406-407)."""
+    h = init_domain(problems.pml_pulse(n=61, L=6.0, width=1.5, nt=200))
+    a = GpuDomain(h)
+    a.run(1, 25)
+    name = tmp_path / "pml"
+    files = checkpoint_write(a, h, name, 25)
+    a.run(26, 45)
+    b = GpuDomain(h)
+    assert checkpoint_read(b, h, name) == 25
+    b.run(26, 45)
+    assert np.array_equal(a.get_fields()[0], b.get_fields()[0])
+    assert np.array_equal(a.get_pml("Wx"), b.get_pml("Wx"))
+    sizes = {p.name: p.stat().st_size // 8 for p in files}
+    assert sizes["pmlF.ckpt25"] == 4 * h.nF * h.nx * h.ny
