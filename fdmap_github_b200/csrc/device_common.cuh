@@ -56,6 +56,9 @@ struct DevBlock {
   const double* pml_h;                 // [3][3][2] hxi, hyi of each region (q, r: 0 minus end, 1 plus end, 2 central)
   const double* pml_s;                 // 2 planes: damping sx, sy at every node
   double *Wx, *DWx, *Wy, *DWy;         // auxiliary fields and rates, nF planes each (NULL when off)
+  const double* gforce;                // tsunami forcing: amp*exp(-(x/sigma)^2/2 - (y/sigma)^2/2) per node, or NULL
+  const double* frc_old;               // forcing from file: frames at the step's start and end,
+  const double* frc_new;               //   nF planes each (NULL when no forcing file)
   int tile_begin;                      // first stencil tile of this block
   int tiles_x;
   long long march_unit_begin;          // first row-group unit of this block (march kernel)
@@ -157,6 +160,7 @@ struct StageArgs {
   const TimeState* ts;  // device step clock (graph replays), or nullptr
   double C;      // RK C(stage-1): stage time = t0 + C*dt
   int tap;       // stage 1 with outputs open: interface kernels write their output snapshot
+  double t0, dt; // step start and length (when ts == nullptr)
 };
 
 // Stage time t0 + C*dt with t0 = t_start + (n-1)*dt, rounded exactly as the
@@ -165,6 +169,17 @@ __device__ __forceinline__ double stage_time(const StageArgs& a) {
   if (!a.ts) return a.t;
   const double t0 = __dadd_rn(a.ts->t_start, __dmul_rn((double)(a.ts->n - 1), a.ts->dt));
   return __dadd_rn(t0, __dmul_rn(a.C, a.ts->dt));
+}
+
+// The step's window [t0, t0 + dt] (load_forcing, source.f90:486-487)
+__device__ __forceinline__ void step_window(const StageArgs& a, double& t_old, double& t_new) {
+  if (!a.ts) {
+    t_old = a.t0;
+    t_new = __dadd_rn(a.t0, a.dt);
+    return;
+  }
+  t_old = __dadd_rn(a.ts->t_start, __dmul_rn((double)(a.ts->n - 1), a.ts->dt));
+  t_new = __dadd_rn(t_old, a.ts->dt);
 }
 
 // ---------------------------------------------------------------------------

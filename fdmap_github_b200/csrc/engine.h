@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <string>
 #include <utility>
 #include <vector>
@@ -61,6 +62,9 @@ struct fdmap_gpu {
   int use_march = 1;
   bool dissipation = false;  // some block has Cdiss > 0 (tiled interior kernel)
   bool pml = false;  // some block has a perfectly matched layer (tiled interior kernel)
+  bool forcing = false;  // tsunami forcing or forcing from file (tiled interior kernel)
+  std::FILE* frc_file = nullptr;  // forcing frames, one (nx,ny,nF) frame per step
+  std::vector<double> frc_host;   // the frame being loaded
   bool body_on_device = false;  // body built by build_body (fdmap_desc.body)
   double tp[5] = {0, 0, 0, 0, 0};  // t0, dt, CFL, hmin, hmax (set_dt)
   int tp_nt = 0;
@@ -154,6 +158,7 @@ struct fdmap_gpu {
   ~fdmap_gpu() {
     if (device >= 0) cudaSetDevice(device);
     if (stream) cudaStreamSynchronize(stream);
+    if (frc_file) std::fclose(frc_file);
     for (auto& p : ev_pending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
     for (auto e : ev_pool) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);

@@ -352,6 +352,39 @@ int launch_stage(fdmap_gpu* h, const StageArgs& a) {
   return launch_interior(h, a);
 }
 
+// reads the next forcing frame into the blocks' new-frame planes (values past
+// the end of the file read as zero)
+int forcing_read_frame(fdmap_gpu* h) {
+  const int nF = h->nF;
+  const long long NN = (long long)h->nx_g * h->ny_g;
+  h->frc_host.assign((size_t)NN * nF, 0.0);
+  size_t got = std::fread(h->frc_host.data(), sizeof(double), h->frc_host.size(), h->frc_file);
+  (void)got;
+  CUDA_TRY(cudaMemcpyAsync(h->d_global, h->frc_host.data(), h->frc_host.size() * sizeof(double),
+                           cudaMemcpyHostToDevice, h->stream));
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const BlockGeom& g = h->geom[b];
+    dim3 grid((g.pitch + 255) / 256, g.ny);
+    scatter_block<<<grid, 256, 0, h->stream>>>(h->d_global, const_cast<double*>(h->hdom.blk[b].frc_new), h->nx_g, NN,
+                                               g.mgx, g.mgy, g.nx, g.ny, g.pitch, g.plane, nF);
+    CUDA_TRY(cudaGetLastError());
+    h->launches++;
+  }
+  return FDMAP_OK;
+}
+
+// load_forcing (source.f90:467-502), at the start of every step: the new frame
+// becomes the old one and the next frame is read
+int forcing_load(fdmap_gpu* h) {
+  if (!h->frc_file) return FDMAP_OK;
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    CUDA_TRY(cudaMemcpyAsync(const_cast<double*>(B.frc_old), B.frc_new, (size_t)h->nF * B.plane * sizeof(double),
+                             cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return forcing_read_frame(h);
+}
+
 int validate(const fdmap_desc* d) {
   if (!d) return set_err(FDMAP_ERR_INVALID_ARG, "null descriptor");
   if (d->mode != 2 && d->mode != 3) return set_err(FDMAP_ERR_INVALID_ARG, "mode must be 2 or 3");
@@ -362,6 +395,9 @@ int validate(const fdmap_desc* d) {
   if (!dev_body && (!d->F || !d->DF || !d->xq || !d->xr || !d->yq || !d->yr || !d->Ji))
     return set_err(FDMAP_ERR_INVALID_ARG, "missing body arrays");
   if (dev_body && !d->body->blocks) return set_err(FDMAP_ERR_INVALID_ARG, "missing block body recipes");
+  if (d->src.gauss_forcing && d->mode == 3 && (!d->x || !d->y))
+    return set_err(dev_body ? FDMAP_ERR_UNSUPPORTED : FDMAP_ERR_INVALID_ARG,
+                   "the tsunami forcing needs the grid coordinates on the host");
   if (d->heterogeneous && (!d->rho || !d->G || (d->mode == 2 && (!d->M || !d->gamma || !d->nu))))
     return set_err(FDMAP_ERR_INVALID_ARG, "missing heterogeneous material arrays");
   fdmap::SbpOperator op;
@@ -517,6 +553,33 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       B.pml_h = dh;
       h->pml = true;
     }
+    B.gforce = nullptr; B.frc_old = nullptr; B.frc_new = nullptr;
+    if (d->src.gauss_forcing && d->mode == 3) {
+      // spatial factor amp*exp(-(x/sigma)^2/2 - (y/sigma)^2/2) of the tsunami forcing (source.f90:308)
+      const fdmap_source& S = d->src;
+      std::vector<double> gf((size_t)g.plane, 0.0);
+      for (int j = 0; j < g.ny; ++j)
+        for (int i = 0; i < g.nx; ++i) {
+          const size_t q = (size_t)(g.mgx - 1 + i) + (size_t)d->nx * (size_t)(g.mgy - 1 + j);
+          const double x = d->x[q], y = d->y[q];
+          gf[(size_t)j * g.pitch + i] =
+              S.gauss_amp * std::exp(-0.5 * ((x / S.gauss_sigma) * (x / S.gauss_sigma)) -
+                                     0.5 * ((y / S.gauss_sigma) * (y / S.gauss_sigma)));
+        }
+      double* dg = nullptr;
+      if ((rc = h->alloc_planes(&dg, 1, g.plane))) return rc;
+      CUDA_TRY(cudaMemcpy(dg, gf.data(), gf.size() * sizeof(double), cudaMemcpyHostToDevice));
+      B.gforce = dg;
+      h->forcing = true;
+    }
+    if (d->src.forcing_filename) {
+      double* fo = nullptr;
+      double* fn = nullptr;
+      if ((rc = h->alloc_planes(&fo, nF, g.plane)) || (rc = h->alloc_planes(&fn, nF, g.plane))) return rc;
+      B.frc_old = fo;
+      B.frc_new = fn;
+      h->forcing = true;
+    }
     B.rinv_b = 1.0 / fb.rho;
     for (int s = 1; s <= op.pI; ++s) {
       B.coef[s][0] = op.DI[s] / fb.rho;
@@ -668,7 +731,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   {
     const char* ek = getenv("FDMAP_STENCIL");
     // dissipative blocks need J at the neighbours, which the march ring does not carry
-    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation && !h->pml;
+    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation && !h->pml && !h->forcing;
     if (h->use_march && (rc = march_dispatch(h, nullptr))) return rc;
     // fused stage launches need every interface-side node to sit on one interface only
     bool junction = false;
@@ -700,6 +763,13 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
 
   // global-layout staging buffer and initial fields
   if ((rc = h->alloc(&h->d_global, (size_t)d->nx * d->ny * nF))) return rc;
+  if (d->src.forcing_filename) {
+    // init_forcing_from_file (source.f90:409-448): frame 0 becomes the new frame
+    h->frc_file = std::fopen(d->src.forcing_filename, "rb");
+    if (!h->frc_file)
+      return set_err(FDMAP_ERR_IO, std::string("cannot open forcing file ") + d->src.forcing_filename);
+    if ((rc = forcing_read_frame(h))) return rc;
+  }
   if (h->body_on_device) return FDMAP_OK;  // fields already built in F[0], DF
   h->cur = 0;
   return fdmap_gpu_set_fields(h, d->F, d->DF);
@@ -718,6 +788,8 @@ int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, con
     a.Bdt = h->rk.B[s] * dt;
     a.t = t0 + h->rk.C[s] * dt;
     a.C = h->rk.C[s];
+    a.t0 = t0;
+    a.dt = dt;
     a.ts = ts;
     a.in = cur;
     a.out = 1 - cur;
@@ -817,6 +889,7 @@ int fdmap_gpu_time_step(fdmap_gpu* h, double t0, double dt, int final_step) {
   CUDA_TRY(cudaSetDevice(h->device));
   int rc = output_before_step(h, h->out_next_n, t0);
   if (rc) return rc;
+  if ((rc = forcing_load(h))) return rc;
   rc = issue_step(h, h->cur, t0, dt, final_step != 0, nullptr, h->out_next_n);
   if (rc) return rc;
   h->out_next_n += 1;
@@ -840,6 +913,7 @@ int fdmap_gpu_run(fdmap_gpu* h, double t_start, double dt, int n_first, int n_la
     for (int n = n_first; n <= n_graph_last; ++n) {
       int rc = output_before_step(h, n, t_start + (double)(n - 1) * dt);
       if (rc) return rc;
+      if ((rc = forcing_load(h))) return rc;
       CUDA_TRY(cudaGraphLaunch(h->step_graph[h->cur], h->stream));
       h->launches += h->graph_launches;
       if (h->rk.nstage & 1) h->cur = 1 - h->cur;

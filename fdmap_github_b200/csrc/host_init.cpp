@@ -327,6 +327,7 @@ struct fdmap_domain {
   // on-device initialisation: the recipe the engine builds the body from
   bool dev_body = false;
   fdmap_body body{};
+  std::string forcing_path;  // source_list forcing_filename, resolved
   std::vector<fdmap_block_body> bbody;
 };
 
@@ -867,8 +868,19 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
   src.Mxx = get_real(sl, "mxx", 0); src.Mxy = get_real(sl, "mxy", 0); src.Myy = get_real(sl, "myy", 0);
   src.Mzx = get_real(sl, "mzx", 0); src.Mzy = get_real(sl, "mzy", 0);
   src.stf = stf_code(get_str(sl, "source_time_function", "gaussian"));
-  if (get_str(sl, "problem", "") != "" || get_bool(sl, "forcing_from_file", false))
-    fail(FDMAP_ERR_UNSUPPORTED, "source problem / forcing from file is not supported");
+  {
+    // tsunami forcing and forcing from file (source.f90:41-115, 299-322)
+    const std::string sproblem = get_str(sl, "problem", "");
+    if (sproblem == "Forcing") src.gauss_forcing = 1;
+    else if (sproblem != "") fail(FDMAP_ERR_UNSUPPORTED, "source problem '" + sproblem + "' is not supported");
+    src.gauss_amp = get_real(sl, "gauss_amp", 0.0);
+    src.gauss_sigma = get_real(sl, "gauss_sigma", 0.0);
+    src.gauss_sigmat = get_real(sl, "gauss_sigmat", 0.0);
+    if (get_bool(sl, "forcing_from_file", false)) {
+      dom.forcing_path = join_path(base, get_str(sl, "forcing_filename", ""));
+      src.forcing_filename = dom.forcing_path.c_str();
+    }
+  }
   src.use_gravity = (src.gx != 0 || src.gy != 0 || src.gz != 0);
   src.use_singular = (src.Fx != 0 || src.Fy != 0 || src.Fz != 0) ||
                      (src.Mxx != 0 || src.Mxy != 0 || src.Myy != 0 || src.Mzx != 0 || src.Mzy != 0);

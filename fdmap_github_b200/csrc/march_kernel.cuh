@@ -359,7 +359,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
           }
         }
         if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-        if (forces) body_forces<MODE>(D, B, i, j, t_stage, acc);
+        if (forces) body_forces<MODE>(D, B, i, j, t_stage, a, acc);
 #pragma unroll
         for (int l = 0; l < NF; ++l) DFp[l * plane + c] = acc[l];
         if (a.update) {

@@ -254,14 +254,18 @@ __device__ __forceinline__ double stf_amp(const fdmap_source& S, double t) {
   }
 }
 
-// point source and gravity (set_source, source.f90:147-252) at block-local node (i, j)
+// body forces (set_source, source.f90:147-324) at block-local node (i, j):
+// gravity, the point source, tsunami forcing and forcing from file, in that order
 template <int MODE>
-__device__ __forceinline__ void body_forces(const DevDomain& D, const DevBlock& B, int i, int j, double t, double* acc) {
+__device__ __forceinline__ void body_forces(const DevDomain& D, const DevBlock& B, int i, int j, double t,
+                                            const StageArgs& a, double* acc) {
   if (D.src.use_gravity) {
     if (MODE == 2) { acc[0] += D.src.gx; acc[1] += D.src.gy; }
     else acc[0] += D.src.gz;
   }
-  if (D.src.use_singular && B.src_ok) {
+  if (D.src.use_singular) {
+    // a point source outside the block ends set_source for it (source.f90:200-206)
+    if (!B.src_ok) return;
     int di = i - B.src_i0, dj = j - B.src_j0;
     if (di >= -2 && di <= 2 && dj >= -2 && dj <= 2) {
       double A = stf_amp(D.src, t);
@@ -278,6 +282,23 @@ __device__ __forceinline__ void body_forces(const DevDomain& D, const DevBlock& 
         acc[2] -= A * D.src.Mzy * dx * dy;
       }
     }
+  }
+  const long long c = (long long)j * B.pitch + i;
+  if (MODE == 3 && B.gforce) {
+    // problem = 'Forcing' (source.f90:299-312); the spatial factor is per node
+    const double pi = 3.14159265358979323846264338327950288;
+    const double u = (t - 4.0 * D.src.gauss_sigmat) / D.src.gauss_sigmat;
+    acc[0] = acc[0] + B.gforce[c] * exp(-0.5 * (u * u)) / (D.src.gauss_sigmat * sqrt(2.0 * pi));
+  }
+  if (B.frc_new) {
+    // forcing from file, interpolated linearly in time (source.f90:315-322)
+    double t_old, t_new;
+    step_window(a, t_old, t_new);
+    const double w_old = (t_new - t) / (t_new - t_old), w_new = 1.0 - w_old;
+    constexpr int NF = MODE == 2 ? 6 : 3;
+#pragma unroll
+    for (int l = 0; l < NF; ++l)
+      acc[l] = acc[l] + w_old * B.frc_old[l * B.plane + c] + w_new * B.frc_new[l * B.plane + c];
   }
 }
 
@@ -492,7 +513,7 @@ __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock&
   }
   if (!pml) closure_rates<MODE, PI_>(D, B, Fin, i, j, m, B.Ji[c], acc);
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-  body_forces<MODE>(D, B, i, j, stage_time(a), acc);
+  body_forces<MODE>(D, B, i, j, stage_time(a), a, acc);
 #pragma unroll
   for (int l = 0; l < NF; ++l) B.DF[l * plane + c] = acc[l];
   if (a.update) {
@@ -696,7 +717,7 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
   }
 
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-  body_forces<MODE>(D, B, i, j, stage_time(a), acc);
+  body_forces<MODE>(D, B, i, j, stage_time(a), a, acc);
 
   double* __restrict__ DF = B.DF;
 #pragma unroll

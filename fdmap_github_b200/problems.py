@@ -11,6 +11,8 @@ Units follow FDMAP: km, s, m/s, MPa, g/cm^3, km/s (2670 kg/m^3 -> 2.67,
   heterogeneous_ricker mode III heterogeneous medium, Ricker point force (config "c5")
   ensemble_instance    mode II rate-and-state, planar fault, von Karman prestress (config "c4")
   pml_pulse            mode II P-SV pulse in a block with a perfectly matched layer
+  gaussian_forcing     mode III long-wave forcing, Gaussian in space and time (problem='Forcing')
+  write_forcing_file   a forcing file sampling the same Gaussian, one frame per step
 """
 from __future__ import annotations
 
@@ -79,6 +81,37 @@ def pml_pulse(n: int = 201, L: float = 10.0, nt: int = 401, rk: int = 4, cfl: fl
 &boundaries_list bcL='{bc}', bcR='{bc}', bcB='{bc}', bcT='{bc}' /
 {_operator(cdiss)}&material_list rho=2.67d0, cs=3.464d0, cp={_f(cp)} /
 {f}{_pml(pmlx, pmly, npow, sigma, kappa, width, L - width)}"""
+
+
+def gaussian_forcing(n: int = 101, L: float = 100.0, nt: int = 101, amp: float = 1.0, sigma: float = 1.25,
+                     sigmat: float = 2.0, cs: float = 0.2, rho: float = 1.0, cfl: float = 0.5, fd: str = "SBP4",
+                     forcing_file: str | None = None) -> str:
+    """Mode III, one block of n x n nodes over [-L/2, L/2]^2 with absorbing
+    sides, driven by the source_list 'Forcing' term (source.f90:299-312):
+    DF(vz) += amp*exp(-(x/sigma)^2/2 - (y/sigma)^2/2) * exp(-((t-4 sigmat)/sigmat)^2/2) / (sigmat*sqrt(2 pi)),
+    or, with `forcing_file`, by that file's frames instead."""
+    h = 0.5 * L
+    src = (f"forcing_from_file=T, forcing_filename='{forcing_file}'" if forcing_file else
+           f"problem='Forcing', gauss_amp={_f(amp)}, gauss_sigma={_f(sigma)}, gauss_sigmat={_f(sigmat)}")
+    return f"""&problem_list name='gaussian_forcing', nt={nt}, CFL={_f(cfl)} , RKorder=4 /
+&domain_list mode=3, FDmethod='{fd}', nblocks_x=1, nblocks_y=1 /
+!---BLOCK1---
+&grid_list nx={n}, ny={n}, LB={_f(-h)},{_f(-h)}, LT={_f(-h)},{_f(h)}, RB={_f(h)},{_f(-h)}, RT={_f(h)},{_f(h)} /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='absorbing' /
+&source_list {src} /
+&material_list rho={_f(rho)}, cs={_f(cs)} /
+"""
+
+
+def write_forcing_file(path: str | Path, x: np.ndarray, y: np.ndarray, times, nF: int, field: int, fn) -> None:
+    """Forcing file (init_forcing_from_file / load_forcing, source.f90:409-502):
+    for each time, nF real*8 planes over the global grid (i fastest), plane
+    `field` = fn(x, y, t) and the others zero.  x, y: node coordinates, shape (ny, nx)."""
+    with open(path, "wb") as f:
+        for t in times:
+            frame = np.zeros((nF,) + x.shape)
+            frame[field] = fn(x, y, t)
+            frame.astype(np.float64).tofile(f)
 
 
 def rupture_sw(nx: int = 1601, ny: int = 801, h: float = 0.025, nt: int = 4001, rk: int = 4, cfl: float = 0.5,

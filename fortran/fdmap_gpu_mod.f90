@@ -71,6 +71,9 @@ module fdmap_gpu_mod
   type, bind(C) :: fdmap_source_t
      integer(c_int) :: use_singular, use_gravity, stf
      real(c_double) :: x0, y0, t_center, t_duration, Fx, Fy, Fz, Mxx, Mxy, Myy, Mzx, Mzy, gx, gy, gz
+     integer(c_int) :: gauss_forcing            ! problem = 'Forcing' (source.f90:299-312)
+     real(c_double) :: gauss_amp, gauss_sigma, gauss_sigmat
+     type(c_ptr) :: forcing_filename            ! C string, or c_null_ptr (source.f90:409-502)
   end type fdmap_source_t
 
   type, bind(C) :: fdmap_desc_t

@@ -186,6 +186,16 @@ typedef struct fdmap_source {
   double x0, y0, t_center, t_duration;
   double Fx, Fy, Fz, Mxx, Mxy, Myy, Mzx, Mzy;
   double gx, gy, gz;
+  /* source_list problem = 'Forcing' (source.f90:299-312), mode III only:
+   * DF(vz) += amp*exp(-(x/sigma)^2/2 - (y/sigma)^2/2)
+   *           * exp(-((t - 4 sigmat)/sigmat)^2/2) / (sigmat*sqrt(2 pi)) */
+  int gauss_forcing;
+  double gauss_amp, gauss_sigma, gauss_sigmat;
+  /* forcing_from_file (source.f90:315-322, 409-502): the file holds one
+   * (nx,ny,nF) real*8 frame per time step, frame 0 at the initial time; each
+   * step reads the next frame and the stage rates add the two frames
+   * interpolated linearly in time.  NULL = no forcing file. */
+  const char* forcing_filename;
 } fdmap_source;
 
 /* shapes of a fields_perturb item (perturb_fields, fields.f90:900-934) */

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <new>
@@ -177,6 +178,13 @@ struct oracle_domain {
   vec rho, G, M, gamma, nu;
   vec Wx, DWx, Wy, DWy;  // PML fields (nx,ny,nF), allocated when some block has pmlx / pmly (fields.f90:203-210)
   fdmap_source src;
+  // forcing from file (source.f90:12-14): the frames of the current step and its window
+  std::FILE* frc = nullptr;
+  vec frc_old, frc_new;
+  double frc_t_old = 0.0, frc_t_new = 0.0;
+  ~oracle_domain() {
+    if (frc) std::fclose(frc);
+  }
   double t;
   long long newton_fail;
 };
@@ -1291,6 +1299,8 @@ void singular_source(int i, int i0, double h, double a, double& d) {
 }
 
 // set_source (source.f90:147-252) for one block; point source and gravity
+void point_source(oracle_domain& D, const Blk& B, double t, double pi);
+
 void set_source(oracle_domain& D, const Blk& B, double t) {
   const fdmap_source& S = D.src;
   size_t NN = (size_t)D.nx * D.ny;
@@ -1302,8 +1312,56 @@ void set_source(oracle_domain& D, const Blk& B, double t) {
         else D.DF[g] = D.DF[g] + S.gz;
       }
   }
-  if (!S.use_singular || !B.src_ok) return;
+  // a point source outside the block ends set_source for it, skipping the
+  // forcing terms below as well (source.f90:200-206)
+  if (S.use_singular && !B.src_ok) return;
   const double pi = 3.14159265358979323846264338327950288;
+  if (S.use_singular) point_source(D, B, t, pi);
+  // problem = 'Forcing': tsunami forcing, mode III only (source.f90:299-312)
+  if (S.gauss_forcing && D.mode == 3) {
+    for (int j = B.mgy; j <= B.pgy; ++j)
+      for (int i = B.mgx; i <= B.pgx; ++i) {
+        size_t g = G2(D, i, j);
+        double x = D.x[g], y = D.y[g];
+        double u = (t - 4.0 * S.gauss_sigmat) / S.gauss_sigmat;
+        D.DF[g] = D.DF[g] + S.gauss_amp *
+                                std::exp(-0.5 * ((x / S.gauss_sigma) * (x / S.gauss_sigma)) -
+                                         0.5 * ((y / S.gauss_sigma) * (y / S.gauss_sigma))) *
+                                std::exp(-0.5 * (u * u)) / (S.gauss_sigmat * std::sqrt(2.0 * pi));
+      }
+  }
+  // forcing from file, interpolated linearly in time (source.f90:315-322)
+  if (D.frc) {
+    double w_old = (D.frc_t_new - t) / (D.frc_t_new - D.frc_t_old);
+    double w_new = 1.0 - w_old;
+    for (int l = 0; l < D.nF; ++l)
+      for (int j = B.mgy; j <= B.pgy; ++j)
+        for (int i = B.mgx; i <= B.pgx; ++i) {
+          size_t g = G2(D, i, j) + NN * l;
+          D.DF[g] = D.DF[g] + w_old * D.frc_old[g] + w_new * D.frc_new[g];
+        }
+  }
+}
+
+// reads the next (nx,ny,nF) forcing frame; values past the end of the file read as zero
+void read_forcing_frame(oracle_domain& D, vec& frame) {
+  frame.assign((size_t)D.nx * D.ny * D.nF, 0.0);
+  size_t got = std::fread(frame.data(), sizeof(double), frame.size(), D.frc);
+  (void)got;
+}
+
+// load_forcing (source.f90:467-502), at the start of every step
+void load_forcing(oracle_domain& D, double t, double dt) {
+  D.frc_t_old = t;
+  D.frc_t_new = t + dt;
+  D.frc_old = D.frc_new;
+  read_forcing_frame(D, D.frc_new);
+}
+
+// singular point force / moment tensor (source.f90:185-252)
+void point_source(oracle_domain& D, const Blk& B, double t, double pi) {
+  const fdmap_source& S = D.src;
+  size_t NN = (size_t)D.nx * D.ny;
   double A;
   double tc = t - S.t_center;
   switch (S.stf) {
@@ -1393,6 +1451,13 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
     o->gamma = copyv(d->gamma, NN); o->nu = copyv(d->nu, NN);
   }
   o->src = d->src;
+  if (d->src.forcing_filename) {
+    // init_forcing_from_file (source.f90:409-448): frame 0 into the new frame
+    o->frc = std::fopen(d->src.forcing_filename, "rb");
+    if (!o->frc) { delete o; return nullptr; }
+    read_forcing_frame(*o, o->frc_new);
+    o->frc_old.assign(o->frc_new.size(), 0.0);
+  }
   o->blk.resize(d->nblocks);
   for (int b = 0; b < d->nblocks; ++b) {
     const fdmap_block& fb = d->blocks[b];
@@ -1477,6 +1542,7 @@ int oracle_time_step(oracle_domain* o, double t0, double dt, int final_step) {
   if (!o) return FDMAP_ERR_INVALID_ARG;
   oracle_domain& D = *o;
   D.t = t0;
+  if (D.frc) load_forcing(D, t0, dt);
   for (int stage = 1; stage <= D.rk.nstage; ++stage) {
     scale_rates_all(D, D.rk.A[stage - 1]);
     prepare_edges(D);
