@@ -536,6 +536,10 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
   if (get_bool(dl, "operator_split", false)) fail(FDMAP_ERR_UNSUPPORTED, "operator_split=T is not supported");
   if (get_bool(dl, "acoustic_gravity_waves", false) || get_bool(dl, "basal_traction_plane_stress", false))
     fail(FDMAP_ERR_UNSUPPORTED, "acoustic gravity / basal traction terms are not supported");
+  // body displacement (set_rates_displacement), peak motion (update_fields_peak)
+  // and the boundary energy balance (set_rates_energy) are not tracked
+  for (const char* flag : {"displacement", "peak", "energy_balance"})
+    if (get_bool(dl, flag, false)) fail(FDMAP_ERR_UNSUPPORTED, std::string(flag) + "=T is not supported");
   std::vector<int> nx_list = get_int_list(dl, "nx_list"), ny_list = get_int_list(dl, "ny_list");
   if (mode != 2 && mode != 3) fail(FDMAP_ERR_INVALID_ARG, "mode must be 2 or 3");
   int method;
