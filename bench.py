@@ -244,6 +244,7 @@ def run_gpu(args) -> None:
     DF0 = np.ascontiguousarray(host.array("DF"))
     pin_F = torch.from_numpy(F0).pin_memory()
     pin_DF = torch.from_numpy(DF0).pin_memory()
+    pin_out = torch.empty(F0.shape, dtype=torch.float64).pin_memory()  # the step's result, read back
     nf = info.get("fault_nodes", 0)
     # fault time series of every step (slip, slip rate, shear stress, rupture
     # time) through the device-side output: gathered into the device ring at
@@ -263,9 +264,11 @@ def run_gpu(args) -> None:
     g2.run(1, args.steps, nt=nt_inf)
     if nf:
         g2.output_flush()
-    F_final, _ = g2.get_fields()
+    rc = lib().fdmap_gpu_get_fields(g2._g, C.cast(pin_out.data_ptr(), C.POINTER(C.c_double)), None)
     e_stop.record(stream)
     e_stop.synchronize()
+    if rc:
+        raise RuntimeError(f"fdmap_gpu_get_fields failed ({rc})")
     e_ms = max(e_start.elapsed_time(e_stop), (time.perf_counter() - t0) * 1e3)
     e_ms = barrier_max(e_ms, world)
     e2e = world * nodes * args.steps / (e_ms * 1e-3)

@@ -8,9 +8,13 @@
 // read from the step-start buffer; fault fields from the stage-1 snapshot the
 // interface kernel writes when outputs are open.  Values are converted to
 // float32 (ps = 4, mpi_routines.f90:12) by one gather launch per step into
-// per-item device rings; the host drains the rings when one would overflow
-// (and on flush) and appends to <prefix>_<name>.dat (the values of each
-// output step, i fastest) and <prefix>_<name>.t (D%t of each output step).
+// per-item device rings of R output steps.  Whenever an item has R/2 output
+// steps not yet copied, the ring is copied to one of two pinned host buffers
+// asynchronously, in stream order behind the gathers; the host writes a copy
+// out (appending to <prefix>_<name>.dat, the values of each output step with
+// i fastest, and <prefix>_<name>.t, D%t of each output step) when it starts
+// the next copy, so the steps keep running while files are written.  Flush
+// and close wait for everything.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -70,8 +74,10 @@ struct OutItemHost {
   std::vector<long long> eoff;
   FILE* dat = nullptr;
   FILE* tf = nullptr;
-  long long issued = 0, drained = 0;  // output steps issued to the device / written to the files
-  std::vector<float> times;           // D%t of issued, undrained output steps
+  long long issued = 0;   // output steps whose gathers are enqueued
+  long long copied = 0;   // output steps covered by an enqueued ring copy
+  long long drained = 0;  // output steps written to the files
+  std::vector<float> times;  // D%t of the issued output steps not yet written
 };
 
 struct OutputState {
@@ -84,14 +90,25 @@ struct OutputState {
   int* d_eb = nullptr;
   long long* d_eoff = nullptr;
   float* d_ring = nullptr;
-  float* h_ring = nullptr;  // pinned copy of the ring
+  float* h_ring[2] = {nullptr, nullptr};  // pinned copies of the ring (one in flight, one being written)
+  int hbuf = 0;                            // buffer the next copy goes to
+  int pbuf = 0;                            // buffer of the copy in flight
+  bool pending = false;                    // a copy is in flight
+  cudaEvent_t ev = nullptr;                // its completion
   long long nelem = 0, ring_floats = 0;
   std::vector<double*> snapshots;  // st_out per friction interface
   void release() {
+    if (ev) cudaEventSynchronize(ev);
     cudaFree(d_items); cudaFree(d_elem_start); cudaFree(d_eb); cudaFree(d_eoff); cudaFree(d_ring);
-    if (h_ring) cudaFreeHost(h_ring);
+    for (float*& hr : h_ring) {
+      if (hr) cudaFreeHost(hr);
+      hr = nullptr;
+    }
+    if (ev) cudaEventDestroy(ev);
+    ev = nullptr;
+    pending = false;
     for (double* p : snapshots) cudaFree(p);
-    d_items = nullptr; d_elem_start = nullptr; d_eb = nullptr; d_eoff = nullptr; d_ring = nullptr; h_ring = nullptr;
+    d_items = nullptr; d_elem_start = nullptr; d_eb = nullptr; d_eoff = nullptr; d_ring = nullptr;
     snapshots.clear();
     for (auto& it : items) {
       if (it.dat) fclose(it.dat);
@@ -105,42 +122,87 @@ static bool active(const DevOutItem& d, long long dn) {
   return dn >= d.nmin && dn <= d.nmax && (dn - d.nmin) % d.stride == 0;
 }
 
-// copy the whole ring back and append every undrained output step to the files
-static int drain(fdmap_gpu* h) {
-  OutputState* o = h->out;
-  bool any = false;
-  for (auto& it : o->items) any = any || it.issued > it.drained;
-  if (!any) return FDMAP_OK;
-  CUDA_TRY(cudaMemcpyAsync(o->h_ring, o->d_ring, o->ring_floats * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(cudaStreamSynchronize(h->stream));
+// append output steps [drained, copied) of every item (all issued ones when
+// `all`) from host copy `hr`
+static int write_records(OutputState* o, const float* hr, bool all) {
   for (auto& it : o->items) {
-    for (long long r = it.drained; r < it.issued; ++r) {
-      const float* src = o->h_ring + it.d.ring0 + (r % o->R) * it.d.size;
+    const long long upto = all ? it.issued : it.copied;
+    for (long long r = it.drained; r < upto; ++r) {
+      const float* src = hr + it.d.ring0 + (r % o->R) * it.d.size;
       if (fwrite(src, sizeof(float), it.d.size, it.dat) != (size_t)it.d.size)
         return set_err(FDMAP_ERR_IO, "cannot write " + o->prefix + "_" + it.name + ".dat");
       const float t = it.times[(size_t)(r - it.drained)];
       if (fwrite(&t, sizeof(float), 1, it.tf) != 1)
         return set_err(FDMAP_ERR_IO, "cannot write " + o->prefix + "_" + it.name + ".t");
     }
-    it.times.clear();
-    it.drained = it.issued;
+    it.times.erase(it.times.begin(), it.times.begin() + (upto - it.drained));
+    it.drained = upto;
+    if (all) it.copied = upto;
+  }
+  return FDMAP_OK;
+}
+
+// wait for the copy in flight (if any) and write what it holds
+static int finish_pending(fdmap_gpu* h) {
+  OutputState* o = h->out;
+  if (!o->pending) return FDMAP_OK;
+  CUDA_TRY(cudaEventSynchronize(o->ev));
+  o->pending = false;
+  return write_records(o, o->h_ring[o->pbuf], false);
+}
+
+// start copying the ring (output steps [copied, issued) of every item) to a
+// pinned buffer behind the gathers already enqueued; the previous copy is
+// written out first
+static int drain_async(fdmap_gpu* h) {
+  OutputState* o = h->out;
+  int rc = finish_pending(h);
+  if (rc) return rc;
+  CUDA_TRY(cudaMemcpyAsync(o->h_ring[o->hbuf], o->d_ring, o->ring_floats * sizeof(float), cudaMemcpyDeviceToHost,
+                           h->stream));
+  CUDA_TRY(cudaEventRecord(o->ev, h->stream));
+  for (auto& it : o->items) it.copied = it.issued;
+  o->pending = true;
+  o->pbuf = o->hbuf;
+  o->hbuf ^= 1;
+  return FDMAP_OK;
+}
+
+// write every output step issued so far (flush / close)
+static int drain(fdmap_gpu* h) {
+  OutputState* o = h->out;
+  int rc = finish_pending(h);
+  if (rc) return rc;
+  bool any = false;
+  for (auto& it : o->items) any = any || it.issued > it.drained;
+  if (any) {
+    CUDA_TRY(cudaMemcpyAsync(o->h_ring[o->hbuf], o->d_ring, o->ring_floats * sizeof(float), cudaMemcpyDeviceToHost,
+                             h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if ((rc = write_records(o, o->h_ring[o->hbuf], true))) return rc;
+  }
+  for (auto& it : o->items) {
     fflush(it.dat);
     fflush(it.tf);
   }
   return FDMAP_OK;
 }
 
-// before step n (loop index) starting at time t: drain if a ring would
-// overflow, then count the output steps this step issues
+// before step n (loop index) starting at time t: start a copy once an item
+// has R/2 output steps not yet copied, then count the output steps this step
+// issues.  A new output step never lands on a ring slot the host has still to
+// read: the copy of that slot precedes it in the stream, and the host reads a
+// pinned buffer before the next copy into it is enqueued.
 int output_before_step(fdmap_gpu* h, long long n, double t) {
   OutputState* o = h->out;
   if (!o || !o->open) return FDMAP_OK;
   const long long dn = n - 1;
-  bool full = false;
+  const long long half = std::max(1, o->R / 2);
+  bool due = false;
   for (auto& it : o->items)
-    if (active(it.d, dn) && it.issued - it.drained >= o->R) full = true;
-  if (full) {
-    int rc = drain(h);
+    if (active(it.d, dn) && it.issued - it.copied >= half) due = true;
+  if (due) {
+    int rc = drain_async(h);
     if (rc) return rc;
   }
   for (auto& it : o->items)
@@ -282,7 +344,7 @@ int fdmap_gpu_output_open(fdmap_gpu* h, const char* prefix, int ring_steps) {
     eoff.insert(eoff.end(), it.eoff.begin(), it.eoff.end());
     ring += (long long)o->R * it.d.size;
     di.push_back(it.d);
-    it.issued = it.drained = 0;
+    it.issued = it.copied = it.drained = 0;
     it.times.clear();
     const std::string base = o->prefix + "_" + it.name;
     it.dat = fopen((base + ".dat").c_str(), "wb");
@@ -304,7 +366,11 @@ int fdmap_gpu_output_open(fdmap_gpu* h, const char* prefix, int ring_steps) {
   if ((e = cudaMalloc(&o->d_eb, std::max<size_t>(eb.size(), 1) * sizeof(int))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&o->d_eoff, std::max<size_t>(eoff.size(), 1) * sizeof(long long))) != cudaSuccess) return fail(e);
   if ((e = cudaMalloc(&o->d_ring, std::max<long long>(ring, 1) * sizeof(float))) != cudaSuccess) return fail(e);
-  if ((e = cudaMallocHost(&o->h_ring, std::max<long long>(ring, 1) * sizeof(float))) != cudaSuccess) return fail(e);
+  for (float*& hr : o->h_ring)
+    if ((e = cudaMallocHost(&hr, std::max<long long>(ring, 1) * sizeof(float))) != cudaSuccess) return fail(e);
+  if ((e = cudaEventCreateWithFlags(&o->ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e);
+  o->hbuf = 0;
+  o->pending = false;
   if ((e = cudaMemcpy(o->d_items, di.data(), di.size() * sizeof(DevOutItem), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMemcpy(o->d_elem_start, start.data(), start.size() * sizeof(long long), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = cudaMemcpy(o->d_eb, eb.data(), eb.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess ||

@@ -108,3 +108,26 @@ def test_outputs_eager_steps_equal_graph_steps(require_gpu, tmp_path):
         x = np.fromfile(tmp_path / f"a_{nm}.dat", dtype=np.float32)
         y = np.fromfile(tmp_path / f"b_{nm}.dat", dtype=np.float32)
         assert x.size > 0 and np.array_equal(x, y), nm
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ring", [1, 2, 3])
+def test_outputs_independent_of_ring_size(require_gpu, tmp_path, ring):
+    """Rings copied to the host asynchronously every R/2 output steps (R = 1:
+    every step) write the same files as one ring that holds the whole run."""
+    text = _problem(nt=21)
+    h = init_domain(text)
+    a, b = GpuDomain(h), GpuDomain(h)
+    configure_outputs(a, h, text, tmp_path / "a", ring_steps=ring)
+    configure_outputs(b, h, text, tmp_path / "b", ring_steps=100)
+    a.run(1, 9)
+    a.output_flush()  # a flush between asynchronous copies
+    a.run(10, h.nt)
+    b.run(1, h.nt)
+    a.output_close()
+    b.output_close()
+    for nm in ("I_D", "I_V", "I_S", "B_vx", "P_vy"):
+        for ext in (".dat", ".t"):
+            x = np.fromfile(tmp_path / f"a_{nm}{ext}", dtype=np.float32)
+            y = np.fromfile(tmp_path / f"b_{nm}{ext}", dtype=np.float32)
+            assert x.size > 0 and np.array_equal(x, y), nm + ext
