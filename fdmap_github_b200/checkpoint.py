@@ -9,18 +9,22 @@ run: native-endian float64, Fortran column-major arrays, no headers.
                                   domain has them          (fields.f90:335-429)
   <name>block<b><S>.ckpt<n>       for S = L, R, B, T: per field l the side's
                                   edge values F(:,l), hat variables Fhat(:,l),
-                                  prestress F0(:,l); then the boundary energy
-                                  E(:) and its rate DE(:)  (fields.f90:432-644)
+                                  prestress F0(:,l); per displacement
+                                  component l the boundary displacement U(:,l)
+                                  and its rate DU(:,l); then the boundary
+                                  energy E(:) and its rate DE(:)
+                                                           (fields.f90:432-644)
   <name>iface<i>side<s>.ckpt<n>   for s = 1, 2: the 18 friction fields in
                                   checkpoint_friction order D, Psi, DPsi, trup,
                                   V, O, S, N, S0, N0, Ds, Dn, DDs, DDn, W, DW,
                                   Nreg, DNreg          (friction.f90:491-552)
   <name>.ckpt                     the number of the last checkpoint written
 
-The engine does not track the boundary energy, so E and DE are written as
-zeros and ignored on reading.  A resume needs F, DF and the friction fields;
-edge values and hat variables are recomputed in stage 1 of the next step,
-exactly as the reference recomputes them after checkpoint_read.
+The engine does not track the boundary energy (energy_balance is off), so E
+and DE are written as the reference leaves them then, 0 and 1e40, and ignored
+on reading.  A resume needs F, DF, the boundary displacement and the friction
+fields; edge values and hat variables are recomputed in stage 1 of the next
+step, exactly as the reference recomputes them after checkpoint_read.
 """
 from __future__ import annotations
 
@@ -64,10 +68,13 @@ def checkpoint_write(gpu, host, name: str | Path, number: int) -> list[Path]:
             Fh = gpu.get_fhat(b, s)
             Fe = _edge_values(F, host, b, s)
             n = F0.shape[1]
+            U, DU = gpu.get_side_displacement(b, s)
             parts = []
             for l in range(host.nF):
                 parts += [Fe[l], Fh[l], F0[l]]
-            parts += [np.zeros(n), np.zeros(n)]  # boundary energy E, DE (not tracked)
+            for l in range(U.shape[0]):
+                parts += [U[l], DU[l]]
+            parts += [np.zeros(n), np.full(n, 1e40)]  # boundary energy E, DE (not tracked)
             p = Path(f"{name}block{b + 1}{SIDES[s]}.ckpt{number}")
             np.concatenate(parts).astype(np.float64).tofile(p)
             files.append(p)
@@ -98,6 +105,19 @@ def checkpoint_read(gpu, host, name: str | Path, number: int | None = None) -> i
     gpu.set_fields(a[:nn].reshape(shape), a[nn:2 * nn].reshape(shape))
     for k, w in enumerate(pml):
         gpu.set_pml(w, a[(2 + k) * nn:(3 + k) * nn].reshape(shape))
+    nU = 2 if host.mode == 2 else 1
+    for b in range(host.nblocks):
+        for s in range(4):
+            mgx, pgx, mgy, pgy = host.block_limits(b)
+            n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+            d = np.fromfile(f"{name}block{b + 1}{SIDES[s]}.ckpt{number}", dtype=np.float64)
+            if d.size != (3 * host.nF + 2 * nU + 2) * n:
+                raise ValueError(f"block {b + 1} side {SIDES[s]} checkpoint: {d.size} values, "
+                                 f"expected {(3 * host.nF + 2 * nU + 2) * n}")
+            base = 3 * host.nF * n
+            U = np.stack([d[base + 2 * l * n:base + (2 * l + 1) * n] for l in range(nU)])
+            DU = np.stack([d[base + (2 * l + 1) * n:base + (2 * l + 2) * n] for l in range(nU)])
+            gpu.set_side_displacement(b, s, U, DU)
     for i in range(host.nifaces):
         if host.iface_info(i)[3] != COUPLING_FRICTION:
             continue

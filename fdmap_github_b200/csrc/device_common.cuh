@@ -32,6 +32,9 @@ struct DevSide {
   double* F0;          // (n,nF)
   double* nrm;         // (n,2)
   double* Fhat;        // (n,nF)
+  double* U;           // (n,nU) boundary displacement (bnd_fields, fields.f90:14-15)
+  double* DU;          // (n,nU) its rate
+  double* Utap;        // (n,nU) U at the start of stage 1 (the output point)
 };
 
 struct DevBlock {

@@ -603,6 +603,12 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       CUDA_TRY(cudaMemcpy(S.Fhat, big.data(), big.size() * sizeof(double), cudaMemcpyHostToDevice));
       h->dev_fhat[b][s] = S.Fhat;
       h->side_n[b][s] = fs.n;
+      // boundary displacement U = 0 and its rate DU = 1e40 (init_fields_side, fields.f90:854-856)
+      const size_t nu = (size_t)fs.n * (d->mode == 2 ? 2 : 1);
+      if ((rc = h->alloc(&S.U, nu)) || (rc = h->alloc(&S.DU, nu)) || (rc = h->alloc(&S.Utap, nu))) return rc;
+      CUDA_TRY(cudaMemset(S.U, 0, nu * sizeof(double)));
+      CUDA_TRY(cudaMemset(S.Utap, 0, nu * sizeof(double)));
+      CUDA_TRY(cudaMemcpy(S.DU, big.data(), nu * sizeof(double), cudaMemcpyHostToDevice));
     }
     B.src_ok = 0;
     if (d->src.use_singular && fb.src_ok) {
@@ -1052,6 +1058,30 @@ int fdmap_gpu_set_pml(fdmap_gpu* h, int which, const double* in) {
     CUDA_TRY(cudaGetLastError());
   }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_side_displacement(fdmap_gpu* h, int b, int s, double* U, double* DU) {
+  if (!h || b < 0 || b >= h->hdom.nblocks || s < 0 || s > 3)
+    return set_err(FDMAP_ERR_INVALID_ARG, "bad get_side_displacement arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const DevSide& S = h->hdom.blk[b].side[s];
+  const size_t nu = (size_t)S.n * (h->mode == 2 ? 2 : 1);
+  if (U) CUDA_TRY(cudaMemcpy(U, S.U, nu * sizeof(double), cudaMemcpyDeviceToHost));
+  if (DU) CUDA_TRY(cudaMemcpy(DU, S.DU, nu * sizeof(double), cudaMemcpyDeviceToHost));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_side_displacement(fdmap_gpu* h, int b, int s, const double* U, const double* DU) {
+  if (!h || b < 0 || b >= h->hdom.nblocks || s < 0 || s > 3)
+    return set_err(FDMAP_ERR_INVALID_ARG, "bad set_side_displacement arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const DevSide& S = h->hdom.blk[b].side[s];
+  const size_t nu = (size_t)S.n * (h->mode == 2 ? 2 : 1);
+  if (U) CUDA_TRY(cudaMemcpy(S.U, U, nu * sizeof(double), cudaMemcpyHostToDevice));
+  if (DU) CUDA_TRY(cudaMemcpy(S.DU, DU, nu * sizeof(double), cudaMemcpyHostToDevice));
   return FDMAP_OK;
 }
 

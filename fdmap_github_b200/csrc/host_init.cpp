@@ -1240,6 +1240,8 @@ extern "C" const double* fdmap_host_side_array(const fdmap_domain* dom, int bloc
   if (n == "F0") { p = S.F0; len = (long long)S.n * dom->desc.nF; }
   else if (n == "M") { p = S.M; len = (long long)S.n * 5; }
   else if (n == "normal") { p = S.normal; len = (long long)S.n * 2; }
+  else if (n == "x") { p = S.x; len = S.n; }
+  else if (n == "y") { p = S.y; len = S.n; }
   if (p && count) *count = len;
   return p;
 }

@@ -30,8 +30,8 @@
 namespace fdmap {
 
 struct DevOutItem {
-  int kind;            // FDMAP_OUT_FAULT or FDMAP_OUT_BODY
-  int index;           // interface (fault) or body field component
+  int kind;            // FDMAP_OUT_FAULT, FDMAP_OUT_BODY or FDMAP_OUT_SIDE
+  int index;           // interface (fault), body field component, or 4*block + side
   int ffield;          // FDMAP_FAULT_* (fault items)
   int stride;
   long long nmin, nmax;
@@ -60,6 +60,10 @@ __global__ void output_gather_kernel(const __grid_constant__ DevDomain D, const 
   if (it.kind == FDMAP_OUT_FAULT) {
     const DevIface& I = D.ifc[it.index];
     v = I.fr.st_out[(long long)it.ffield * I.n + elem_off[e]];
+  } else if (it.kind == FDMAP_OUT_SIDE) {
+    const DevSide& S = D.blk[it.index >> 2].side[it.index & 3];
+    v = it.ffield >= FDMAP_OUT_SIDE_U ? S.Utap[(long long)(it.ffield - FDMAP_OUT_SIDE_U) * S.n + elem_off[e]]
+                                      : S.Fhat[(long long)it.ffield * S.n + elem_off[e]];
   } else {
     const DevBlock& B = D.blk[elem_b[e]];
     v = B.F[cur][(long long)it.index * B.plane + elem_off[e]];
@@ -313,8 +317,19 @@ int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, in
         it.eb.push_back(b);
         it.eoff.push_back((long long)(j - g.mgy) * g.pitch + (i - g.mgx));
       }
+  } else if (kind == FDMAP_OUT_SIDE) {
+    const int b = index >> 2, s = index & 3;
+    if (index < 0 || b >= h->hdom.nblocks) return set_err(FDMAP_ERR_INVALID_ARG, "output: side index out of range");
+    const int nU = h->mode == 2 ? 2 : 1;
+    if (field < 0 || (field >= h->nF && field < FDMAP_OUT_SIDE_U) || field >= FDMAP_OUT_SIDE_U + nU)
+      return set_err(FDMAP_ERR_INVALID_ARG, "output: bad side field");
+    const int n = h->hdom.blk[b].side[s].n;
+    if (mx < 1 || px > n || mx > px) return set_err(FDMAP_ERR_INVALID_ARG, "output: side indices out of range");
+    it.d.index = index;
+    it.d.ffield = field;
+    for (int k = mx; k <= px; k += sx) { it.eb.push_back(b); it.eoff.push_back(k - 1); }
   } else {
-    return set_err(FDMAP_ERR_INVALID_ARG, "output: kind must be FDMAP_OUT_FAULT or FDMAP_OUT_BODY");
+    return set_err(FDMAP_ERR_INVALID_ARG, "output: kind must be FDMAP_OUT_FAULT, FDMAP_OUT_BODY or FDMAP_OUT_SIDE");
   }
   it.d.size = (int)it.eoff.size();
   h->out->items.push_back(std::move(it));

@@ -225,7 +225,7 @@ __device__ __forceinline__ void sat_apply(const DevSide& S, int k, const double*
 // an outer boundary, or read back from the interface kernel's output.
 template <int MODE>
 __device__ __forceinline__ void sat_term(const DevSide& S, int s, int k, const double* F, double* acc, int iside,
-                                         const double* Fh_given) {
+                                         const double* Fh_given, const StageArgs& a) {
   constexpr int NF = MODE == 2 ? 6 : 3;
   double Fh[6];
   if (s == iside) {
@@ -238,6 +238,22 @@ __device__ __forceinline__ void sat_term(const DevSide& S, int s, int k, const d
     for (int l = 0; l < NF; ++l) Fh[l] = S.Fhat[k + S.n * l];
   }
   sat_apply<MODE>(S, k, F, Fh, acc);
+  if (S.U) {
+    // boundary displacement: DU <- A*DU + Fhat(:, 1:nU), U <- U + Bdt*DU
+    // (scale_rates_boundary / set_rates_boundary / update_fields_boundary,
+    // fields.f90:1083-1276); the stage-1 U is kept for the output
+    constexpr int NU = MODE == 2 ? 2 : 1;
+#pragma unroll
+    for (int c = 0; c < NU; ++c) {
+      const long long q = k + (long long)S.n * c;
+      const double u = S.U[q];
+      double du = a.scale ? (a.A != 0.0 ? a.A * S.DU[q] : 0.0) : S.DU[q];
+      du = du + Fh[c];
+      S.DU[q] = du;
+      if (a.tap && S.Utap) S.Utap[q] = u;
+      if (a.update) S.U[q] = u + a.Bdt * du;
+    }
+  }
 }
 
 // singular source amplitude (source.f90:208-223)
@@ -494,10 +510,10 @@ __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock&
   double Fc[NF];
 #pragma unroll
   for (int l = 0; l < NF; ++l) Fc[l] = Fin[l * plane + c];
-  if (i == 0) sat_term<MODE>(B.side[0], 0, j, Fc, acc, iside, Fh_given);
-  if (i == nx - 1) sat_term<MODE>(B.side[1], 1, j, Fc, acc, iside, Fh_given);
-  if (j == 0) sat_term<MODE>(B.side[2], 2, i, Fc, acc, iside, Fh_given);
-  if (j == ny - 1) sat_term<MODE>(B.side[3], 3, i, Fc, acc, iside, Fh_given);
+  if (i == 0) sat_term<MODE>(B.side[0], 0, j, Fc, acc, iside, Fh_given, a);
+  if (i == nx - 1) sat_term<MODE>(B.side[1], 1, j, Fc, acc, iside, Fh_given, a);
+  if (j == 0) sat_term<MODE>(B.side[2], 2, i, Fc, acc, iside, Fh_given, a);
+  if (j == ny - 1) sat_term<MODE>(B.side[3], 3, i, Fc, acc, iside, Fh_given, a);
   NodeMat m;
   if (HET) {
     m.rho = B.rho[c]; m.G = B.G[c];

@@ -92,7 +92,8 @@ class HostDomain:
         return out[0], out[1]
 
     def side_array(self, b: int, s: int, name: str) -> np.ndarray:
-        """Side array of block b, side s (0..3 = L, R, B, T): "F0" -> (nF, n), "M" -> (5, n), "normal" -> (2, n)."""
+        """Side array of block b, side s (0..3 = L, R, B, T): "F0" -> (nF, n), "M" -> (5, n), "normal" -> (2, n),
+        "x" / "y" -> (1, n)."""
         n = C.c_longlong()
         p = lib().fdmap_host_side_array(self._h, b, s, name.encode(), C.byref(n))
         if not p:
@@ -185,6 +186,22 @@ class GpuDomain:
         out = np.empty((self.ny, self.nx))
         check_gpu(lib().fdmap_gpu_get_metric(self._g, native.METRIC_INDEX[name], dptr(out)), "fdmap_gpu_get_metric")
         return out
+
+    def get_side_displacement(self, b: int, s: int):
+        """Boundary displacement U and its rate DU of block b, side s: each (nU, n)."""
+        mgx, pgx, mgy, pgy = self.host.block_limits(b)
+        n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+        nU = 2 if self.host.mode == 2 else 1
+        U, DU = np.empty(nU * n), np.empty(nU * n)
+        check_gpu(lib().fdmap_gpu_get_side_displacement(self._g, b, s, dptr(U), dptr(DU)),
+                  "fdmap_gpu_get_side_displacement")
+        return U.reshape(nU, n), DU.reshape(nU, n)
+
+    def set_side_displacement(self, b: int, s: int, U=None, DU=None) -> None:
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        DU = None if DU is None else np.ascontiguousarray(DU, dtype=np.float64)
+        check_gpu(lib().fdmap_gpu_set_side_displacement(self._g, b, s, dptr(U), dptr(DU)),
+                  "fdmap_gpu_set_side_displacement")
 
     def get_pml(self, which: str) -> np.ndarray:
         """Perfectly matched layer field "Wx" or "Wy", shape (nF, ny, nx); zeros outside PML blocks."""

@@ -73,6 +73,8 @@ SIGNATURES = {
     "fdmap_gpu_get_metric": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_get_side_impedance": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_get_pml": (C.c_int, [_VP, C.c_int, _DP]),
+    "fdmap_gpu_get_side_displacement": (C.c_int, [_VP, C.c_int, C.c_int, _DP, _DP]),
+    "fdmap_gpu_set_side_displacement": (C.c_int, [_VP, C.c_int, C.c_int, _DP, _DP]),
     "fdmap_gpu_set_pml": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_fault_max_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_output_add": (C.c_int, [_VP, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,

@@ -23,7 +23,12 @@ import numpy as np
 
 from .native import FAULT_INDEX
 
-OUT_FAULT, OUT_BODY = 0, 1
+OUT_FAULT, OUT_BODY, OUT_SIDE, OUT_SIDE_U = 0, 1, 2, 8
+# bndX locations (get_field, domain.f90:763-860): the hat variables by position
+# (vx or vz the first, vy the second, sxx, sxy, syy the third to fifth) and the
+# boundary displacement; x, y are static
+SIDE_HAT = {"vx": 0, "vz": 0, "vy": 1, "sxx": 2, "sxy": 3, "syy": 4}
+SIDE_U = {"ux": 0, "uz": 0, "uy": 1}
 
 BODY_FIELDS = {2: ["vx", "vy", "sxx", "sxy", "syy", "szz"], 3: ["vz", "sxz", "syz"]}
 STATIC_BODY = {"x", "y", "xq", "xr", "yq", "yr", "J", "rho", "cs", "cp", "G", "M", "gamma", "nu"}
@@ -33,7 +38,7 @@ STATIC_FAULT = {"x", "y"}
 @dataclass
 class OutputItem:
     name: str
-    location: str          # body, blockN, ifaceN, point_ifaceN, point_body, body_grid, slicex, slicey
+    location: str          # body, blockN, ifaceN, point_ifaceN, point_body, body_grid, slicex, slicey, bndXN
     fields: list[str]
     tmin: float
     tmax: float
@@ -119,6 +124,25 @@ def configure_outputs(gpu, host, text: str, prefix: str | Path, ring_steps: int 
                         gpu.output_add(pn, OUT_FAULT, iface, FAULT_INDEX[f], q, q, 1, nmin=nmin, nmax=nmax,
                                        stride=it.stride)
                         names.append(pn)
+                continue
+            if loc.startswith("bnd"):
+                # bndXN: side X (L, R, B, T) of block N, every side node
+                s = "LRBT".index(loc[3])
+                b = int(loc[4:]) - 1
+                mgx, pgx, mgy, pgy = host.block_limits(b)
+                n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+                if f in ("x", "y"):
+                    static.append((nm, host.side_array(b, s, f)[0], nmin, nmax))
+                    continue
+                nU = 2 if mode == 2 else 1
+                if f in SIDE_U and SIDE_U[f] < nU:
+                    fld = OUT_SIDE_U + SIDE_U[f]
+                elif f in SIDE_HAT and SIDE_HAT[f] < host.nF:
+                    fld = SIDE_HAT[f]
+                else:
+                    raise ValueError(f"output field {f!r} is not available on block boundaries")
+                gpu.output_add(nm, OUT_SIDE, 4 * b + s, fld, 1, n, 1, nmin=nmin, nmax=nmax, stride=it.stride)
+                names.append(nm)
                 continue
             # body locations: index boxes (mx, px, sx, my, py, sy), global 1-based
             boxes: list[tuple[str, tuple[int, int, int, int, int, int]]] = []

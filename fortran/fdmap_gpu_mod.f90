@@ -204,6 +204,22 @@ module fdmap_gpu_mod
        real(c_double), intent(in) :: in(*)
      end function fdmap_gpu_set_pml
 
+     integer(c_int) function fdmap_gpu_get_side_displacement(h, b, s, U, DU) &
+          bind(C, name='fdmap_gpu_get_side_displacement')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: b, s
+       type(c_ptr), value :: U, DU                 ! (n, nU) each, or c_null_ptr
+     end function fdmap_gpu_get_side_displacement
+
+     integer(c_int) function fdmap_gpu_set_side_displacement(h, b, s, U, DU) &
+          bind(C, name='fdmap_gpu_set_side_displacement')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: b, s
+       type(c_ptr), value :: U, DU
+     end function fdmap_gpu_set_side_displacement
+
      integer(c_int) function fdmap_gpu_get_side_impedance(h, b, s, out) bind(C, name='fdmap_gpu_get_side_impedance')
        import :: c_int, c_ptr, c_double
        type(c_ptr), value :: h

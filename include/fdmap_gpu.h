@@ -92,6 +92,14 @@ int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out);
 int fdmap_gpu_get_pml(fdmap_gpu* h, int which, double* out);
 int fdmap_gpu_set_pml(fdmap_gpu* h, int which, const double* in);
 
+/* Boundary displacement U(n,nU) and its rate DU(n,nU) of side s (0..3 =
+ * L,R,B,T) of block b (bndF%U, bndF%DU; nU = 2 in mode II, 1 in mode III):
+ * integrated from the side's hat velocities every stage as the reference
+ * does (scale_rates_boundary / set_rates_boundary / update_fields_boundary,
+ * fields.f90:1083-1276).  Either pointer may be NULL. */
+int fdmap_gpu_get_side_displacement(fdmap_gpu* h, int b, int s, double* U, double* DU);
+int fdmap_gpu_set_side_displacement(fdmap_gpu* h, int b, int s, const double* U, const double* DU);
+
 /* Edge impedances M(n,5) = Zs, Zp, gamma, Ks, Kp of side s (0..3 = L,R,B,T)
  * of block b as the engine holds them (init_edges, domain.f90:1349-1459). */
 int fdmap_gpu_get_side_impedance(fdmap_gpu* h, int b, int s, double* out);
@@ -111,11 +119,16 @@ int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
  *   FDMAP_OUT_FAULT: `index` = interface, `field` = FDMAP_FAULT_*,
  *                    nodes mx..px (1-based along the interface) step sx;
  *   FDMAP_OUT_BODY:  `field` = body field component (0..nF-1), global
- *                    nodes mx..px step sx by my..py step sy.
+ *                    nodes mx..px step sx by my..py step sy;
+ *   FDMAP_OUT_SIDE:  `index` = 4*block + side (0..3 = L,R,B,T), `field` =
+ *                    hat variable component 0..nF-1 or FDMAP_OUT_SIDE_U + c
+ *                    for the boundary displacement component c (the bndX
+ *                    locations, get_field, domain.f90:763-860), side nodes
+ *                    mx..px (1-based along the side) step sx.
  * Items are added before fdmap_gpu_output_open; fdmap_gpu_output_flush
  * writes everything recorded so far, fdmap_gpu_output_close flushes and
  * releases the rings. */
-enum { FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1 };
+enum { FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1, FDMAP_OUT_SIDE = 2, FDMAP_OUT_SIDE_U = 8 };
 int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, int field, int mx, int px, int sx,
                          int my, int py, int sy, long long nmin, long long nmax, int stride);
 int fdmap_gpu_output_open(fdmap_gpu* h, const char* prefix, int ring_steps);

@@ -73,7 +73,8 @@ int fdmap_host_iface_info(const fdmap_domain* dom, int iface, int* info);
 const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface, int which);
 
 /* Side arrays of block `block`, side `side` (0..3 = L, R, B, T): "F0" (n, nF),
- * "M" (n, 5) or "normal" (n, 2); *count receives the length.  NULL if absent. */
+ * "M" (n, 5), "normal" (n, 2), "x" or "y" (n); *count receives the length.
+ * NULL if absent. */
 const double* fdmap_host_side_array(const fdmap_domain* dom, int block, int side, const char* name, long long* count);
 
 /* Scaled artificial dissipation coefficient of block `block` (Cdiss*CFL/dt,

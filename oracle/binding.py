@@ -34,6 +34,7 @@ def lib() -> C.CDLL:
         L.oracle_get_fault.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         L.oracle_get_fhat.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         L.oracle_get_pml.argtypes = [C.c_void_p, C.c_int, _DP]
+        L.oracle_get_side_u.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP, _DP]
         L.oracle_newton_failures.restype = C.c_longlong
         L.oracle_newton_failures.argtypes = [C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
@@ -89,6 +90,15 @@ class OracleDomain:
         out = np.empty(n * self.nF)
         lib().oracle_get_fhat(self._o, b, s, _p(out))
         return out.reshape(self.nF, n)
+
+    def get_side_u(self, b: int, s: int):
+        """Boundary displacement U and its rate DU of block b, side s: each (nU, n)."""
+        mgx, pgx, mgy, pgy = self.host.block_limits(b)
+        n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
+        nU = 2 if self.host.mode == 2 else 1
+        U, DU = np.empty(n * nU), np.empty(n * nU)
+        lib().oracle_get_side_u(self._o, b, s, _p(U), _p(DU))
+        return U.reshape(nU, n), DU.reshape(nU, n)
 
     def get_pml(self, which: str) -> np.ndarray:
         """PML field "Wx" or "Wy", shape (nF, ny, nx); zeros where the domain has none."""

@@ -139,6 +139,7 @@ struct Side {
   int bc, n;
   vec M, F0, normal, x, y;
   vec F, Fhat;  // (n, nF)
+  vec U, DU;    // (n, nU) boundary displacement and its rate (bnd_fields, fields.f90:14-15)
 };
 
 struct Blk {
@@ -1397,6 +1398,15 @@ void set_rates_all(oracle_domain& D) {
   for (auto& B : D.blk) set_rates_SAT(D, B);
   for (auto& B : D.blk) set_rates(D, B);
   for (auto& B : D.blk) set_source(D, B, D.t);
+  // set_rates_boundary (fields.f90:1261-1276): DU += Fhat(:, 1:nU) on every side
+  const int nU = D.mode == 2 ? 2 : 1;
+  for (auto& B : D.blk)
+    for (auto& S : B.side)
+      for (int c = 0; c < nU; ++c)
+        for (int k = 0; k < S.n; ++k) {
+          size_t q = (size_t)k + (size_t)S.n * c;
+          S.DU[q] = S.DU[q] + S.Fhat[q];
+        }
 }
 
 void scale_rates_all(oracle_domain& D, double A) {
@@ -1408,6 +1418,10 @@ void scale_rates_all(oracle_domain& D, double A) {
     for (double& v : *W) v = A * v;
   for (auto& I : D.ifc)
     if (I.coupling == FDMAP_COUPLING_FRICTION) scale_rates_friction(I.fr, A);
+  // scale_rates_boundary (fields.f90:1083-1097): boundary displacement rates
+  for (auto& B : D.blk)
+    for (auto& S : B.side)
+      for (double& v : S.DU) v = A * v;
 }
 
 void update_fields_all(oracle_domain& D, double Bdt) {
@@ -1419,6 +1433,10 @@ void update_fields_all(oracle_domain& D, double Bdt) {
   for (size_t q = 0; q < D.Wy.size(); ++q) D.Wy[q] = D.Wy[q] + Bdt * D.DWy[q];
   for (auto& I : D.ifc)
     if (I.coupling == FDMAP_COUPLING_FRICTION) update_fields_friction(I.fr, Bdt);
+  // update_fields_boundary (fields.f90:1189-1204)
+  for (auto& B : D.blk)
+    for (auto& S : B.side)
+      for (size_t q = 0; q < S.U.size(); ++q) S.U[q] = S.U[q] + Bdt * S.DU[q];
 }
 
 }  // namespace
@@ -1486,6 +1504,10 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
       S.normal = copyv(fs.normal, (size_t)fs.n * 2);
       S.F.assign((size_t)fs.n * d->nF, 1e40);
       S.Fhat.assign((size_t)fs.n * d->nF, 1e40);
+      // init_fields_side (fields.f90:854-856): U = 0, DU = 1e40
+      const int nU = d->mode == 2 ? 2 : 1;
+      S.U.assign((size_t)fs.n * nU, 0.0);
+      S.DU.assign((size_t)fs.n * nU, 1e40);
     }
   }
   o->ifc.resize(d->nifaces);
@@ -1595,6 +1617,15 @@ int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out) {
 }
 
 long long oracle_newton_failures(const oracle_domain* o) { return o ? o->newton_fail : -1; }
+
+// boundary displacement U and its rate DU of side s of block b, (n, nU) each (either may be NULL)
+int oracle_get_side_u(const oracle_domain* o, int b, int s, double* U, double* DU) {
+  if (!o || b < 0 || b >= o->nblocks || s < 0 || s > 3) return -1;
+  const Side& S = o->blk[b].side[s];
+  if (U) std::copy(S.U.begin(), S.U.end(), U);
+  if (DU) std::copy(S.DU.begin(), S.DU.end(), DU);
+  return 0;
+}
 
 // PML field Wx (which = 0) or Wy (1) in the global (nx,ny,nF) layout; zeros when not allocated
 int oracle_get_pml(const oracle_domain* o, int which, double* out) {

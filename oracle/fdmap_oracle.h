@@ -59,6 +59,9 @@ int oracle_get_fault(const oracle_domain* o, int iface, int field, double* out);
 /* Hat variables of side s (0..3) of block b: (n, nF). */
 int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out);
 
+/* Boundary displacement U and rate DU of side s (0..3) of block b: (n, nU) each. */
+int oracle_get_side_u(const oracle_domain* o, int b, int s, double* U, double* DU);
+
 /* PML field Wx (which = 0) or Wy (which = 1), (nx, ny, nF); zeros where none. */
 int oracle_get_pml(const oracle_domain* o, int which, double* out);
 

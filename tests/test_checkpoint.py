@@ -30,9 +30,17 @@ def test_resume_is_bitwise(require_gpu, tmp_path):
     # file sizes as checkpoint_fields / checkpoint_block_fields / checkpoint_friction lay them out
     sizes = {p.name: p.stat().st_size // 8 for p in files}
     assert sizes["rupF.ckpt15"] == 2 * h.nF * h.nx * h.ny
-    assert sizes["rupblock1L.ckpt15"] == (3 * h.nF + 2) * 31
-    assert sizes["rupblock2T.ckpt15"] == (3 * h.nF + 2) * 61
+    # per side: F, Fhat, F0 per field, U and DU per displacement component (nU = 2), E, DE
+    assert sizes["rupblock1L.ckpt15"] == (3 * h.nF + 2 * 2 + 2) * 31
+    assert sizes["rupblock2T.ckpt15"] == (3 * h.nF + 2 * 2 + 2) * 61
     assert sizes["rupiface1side1.ckpt15"] == 18 * h.iface_n(0)
+    # the boundary displacement resumes too
+    for blk in range(2):
+        for s in range(4):
+            Ua, DUa = a.get_side_displacement(blk, s)
+            Ub, DUb = b.get_side_displacement(blk, s)
+            assert np.array_equal(Ua, Ub) and np.array_equal(DUa, DUb), (blk, s)
+    assert np.abs(a.get_side_displacement(0, 3)[0]).max() > 0  # the fault side has slipped
 
 
 def test_pml_list_reaches_the_descriptor():

@@ -163,3 +163,36 @@ def test_dissipation_rupture_run(require_gpu):
     o.run(1, h.nt)
     assert_fields_close(g.get_fields()[0], o.get_fields()[0])
     assert_fault_close(g, o, dt=h.dt, fields=("V", "S", "N", "D"))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [2, 3])
+def test_side_displacement_vs_oracle(require_gpu, mode):
+    """Boundary displacement of every side (integrated from the hat velocities,
+    fields.f90:1083-1276) against the oracle, and the jump across the fault
+    equal to the slip register Ds."""
+    from oracle.binding import OracleDomain
+
+    if mode == 2:
+        h = init_domain(problems.rupture_sw(nx=81, ny=41, h=0.25, nt=200))
+    else:
+        h = init_domain(problems.antiplane_pulse(n=61, L=6.0, nt=200))
+    g, o = GpuDomain(h), OracleDomain(h)
+    g.run(1, 40)
+    o.run(1, 40)
+    sides = [(b, s) for b in range(h.nblocks) for s in range(4)]
+    gpu = {k: g.get_side_displacement(*k) for k in sides}
+    ora = {k: o.get_side_u(*k) for k in sides}
+    # errors relative to the largest displacement (rate) on any side: sides
+    # far from the source carry values at the rounding level of that scale
+    for q in range(2):
+        scale = max(np.abs(ora[k][q]).max() for k in sides)
+        assert scale > 0
+        for k in sides:
+            assert np.abs(gpu[k][q] - ora[k][q]).max() <= 1e-10 * scale, (k, q)
+    if mode == 2:
+        Um, Up = g.get_side_displacement(0, 3)[0], g.get_side_displacement(1, 2)[0]
+        Ds = g.get_fault(0, "Ds")
+        assert np.abs(Ds).max() > 0
+        assert np.abs((Up[0] - Um[0]) - Ds).max() <= 1e-12 * np.abs(Ds).max()
+    g.close()

@@ -131,3 +131,67 @@ def test_outputs_independent_of_ring_size(require_gpu, tmp_path, ring):
             x = np.fromfile(tmp_path / f"a_{nm}{ext}", dtype=np.float32)
             y = np.fromfile(tmp_path / f"b_{nm}{ext}", dtype=np.float32)
             assert x.size > 0 and np.array_equal(x, y), nm + ext
+
+
+BND_LIST = """
+!---begin:output_list---
+S
+bndT2
+ux uy vx vy sxx syy sxy
+0d0 1d10 1
+X
+bndT2
+x y
+0d0 0d0 1
+L
+bndB2
+ux vy
+0d0 1d10 3
+!---end:output_list---
+"""
+
+
+def test_read_boundary_output_list():
+    items = read_output_list(BND_LIST)
+    assert [it.location for it in items] == ["bndT2", "bndT2", "bndB2"]
+    assert items[0].fields == ["ux", "uy", "vx", "vy", "sxx", "syy", "sxy"] and items[2].stride == 3
+
+
+@pytest.mark.gpu
+def test_boundary_outputs_match_stage1_state(require_gpu, tmp_path):
+    """bndX locations: boundary displacement at the step start and the stage-1
+    hat variables (get_field, domain.f90:763-860), here on the free top of the
+    upper block and on the fault side of the same block."""
+    text = problems.rupture_sw(nx=41, ny=21, h=0.5, nt=31) + BND_LIST
+    h = init_domain(text)
+    g = GpuDomain(h)
+    prefix = tmp_path / "bnd"
+    configure_outputs(g, h, text, prefix, ring_steps=5)
+    nsteps = 25
+    g.run(1, nsteps, nt=h.nt)
+    g.output_close()
+    n = 41
+    out = {f: np.fromfile(f"{prefix}_S_{f}.dat", dtype=np.float32).reshape(-1, n)
+           for f in ("ux", "uy", "vx", "vy", "sxx", "syy", "sxy")}
+    lux = np.fromfile(f"{prefix}_L_ux.dat", dtype=np.float32).reshape(-1, n)
+    lvy = np.fromfile(f"{prefix}_L_vy.dat", dtype=np.float32).reshape(-1, n)
+    assert out["ux"].shape[0] == nsteps and lux.shape[0] == (nsteps - 1) // 3 + 1
+    x = np.fromfile(f"{prefix}_X_x.dat", dtype=np.float32)
+    np.testing.assert_array_equal(x, h.side_array(1, 3, "x")[0].astype(np.float32))
+    hat_index = {"vx": 0, "vy": 1, "sxx": 2, "sxy": 3, "syy": 4}
+    p = GpuDomain(h)
+    for step in range(1, nsteps + 1):
+        t0 = h.t0 + (step - 1) * h.dt
+        U, _ = p.get_side_displacement(1, 3)
+        Ub, _ = p.get_side_displacement(1, 2)
+        p.time_step_LS(t0, h.dt, final_step=True)
+        Fh = p.get_fhat(1, 3)
+        np.testing.assert_array_equal(out["ux"][step - 1], U[0].astype(np.float32))
+        np.testing.assert_array_equal(out["uy"][step - 1], U[1].astype(np.float32))
+        for f, l in hat_index.items():
+            np.testing.assert_array_equal(out[f][step - 1], Fh[l].astype(np.float32), err_msg=f)
+        if (step - 1) % 3 == 0:
+            np.testing.assert_array_equal(lux[(step - 1) // 3], Ub[0].astype(np.float32))
+            np.testing.assert_array_equal(lvy[(step - 1) // 3], p.get_fhat(1, 2)[1].astype(np.float32))
+        p.time_step_LS(t0, h.dt)
+    assert np.abs(lux).max() > 0  # the fault side of the upper block moves
