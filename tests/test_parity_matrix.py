@@ -1,0 +1,138 @@
+"""GPU against the oracle across the configuration space of the time step:
+every friction law (friction.f90:700-826, 1147-1264), both interface
+directions, the load shapes (friction.f90:1348-1369), forced rupture,
+thermal-pressurisation p0, regularised normal stress, rupture on slip, a
+rotated fault, and every outer boundary condition (boundaries.f90:155-377),
+in mode II and mode III.  Small two-block problems, 30 steps each."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from fdmap_github_b200 import GpuDomain, init_domain
+from tests.parity import assert_fault_close, assert_fields_close
+
+
+def _f(x: float) -> str:
+    return repr(float(x)).replace("e", "d") if "e" in repr(float(x)) else repr(float(x)) + "d0"
+
+
+def fault_text(mode=2, law="SW", direction="y", ld="gaussian", bc="absorbing", fd="SBP4", n=41, h=0.25,
+               friction_extra="", extra_blocks="", nt=31) -> str:
+    """Two blocks of n x (n//2 + 1) nodes (direction 'y': stacked, fault y = 0;
+    'x': side by side, fault x = 0) with a frictional interface."""
+    m = n // 2 + 1
+    L, W = (n - 1) * h, (m - 1) * h
+    if direction == "y":
+        g1 = f"nx={n}, ny={m}, LB={_f(-L/2)},{_f(-W)}, LT={_f(-L/2)},0d0, RB={_f(L/2)},{_f(-W)}, RT={_f(L/2)},0d0"
+        g2 = f"nx={n}, ny={m}, LB={_f(-L/2)},0d0, LT={_f(-L/2)},{_f(W)}, RB={_f(L/2)},0d0, RT={_f(L/2)},{_f(W)}"
+        b1 = f"bcL='{bc}', bcR='{bc}', bcB='{bc}', bcT='none'"
+        b2 = f"bcL='{bc}', bcR='{bc}', bcB='none', bcT='{bc}'"
+        dom = "nblocks_x=1, nblocks_y=2"
+        stress = "syy0=-100d0, sxy0=58d0, sxx0=-100d0" if mode == 2 else "syy0=-100d0, syz0=58d0"
+    else:
+        g1 = f"nx={m}, ny={n}, LB={_f(-W)},{_f(-L/2)}, LT={_f(-W)},{_f(L/2)}, RB=0d0,{_f(-L/2)}, RT=0d0,{_f(L/2)}"
+        g2 = f"nx={m}, ny={n}, LB=0d0,{_f(-L/2)}, LT=0d0,{_f(L/2)}, RB={_f(W)},{_f(-L/2)}, RT={_f(W)},{_f(L/2)}"
+        b1 = f"bcL='{bc}', bcR='none', bcB='{bc}', bcT='{bc}'"
+        b2 = f"bcL='none', bcR='{bc}', bcB='{bc}', bcT='{bc}'"
+        dom = "nblocks_x=2, nblocks_y=1"
+        # with the normal along +x the fault-tangent direction is -y, so the
+        # shear traction on the fault is -sxy
+        stress = "sxx0=-100d0, sxy0=-58d0, syy0=-100d0" if mode == 2 else "sxx0=-100d0, sxz0=58d0"
+    ldline = f"ld%shape='{ld}', ld%R=1.5d0, ld%S=20d0, ld%x0=0d0, ld%y0=0d0, ld%T=0d0," if ld else ""
+    if law == "SW":
+        params = "sw%fs=0.68d0, sw%fd=0.52d0, sw%Dc=0.2d0,"
+    elif law in ("frictionless", "locked"):
+        params = ""
+    else:
+        params = "rs%a=0.01d0, rs%b=0.014d0, rs%V0=1d-6, rs%f0=0.6d0, rs%L=0.05d0, rs%fw=0.2d0, rs%Vw=0.1d0, Psi0=0.6d0,"
+    blk = f"&material_list rho=2.67d0, cs=3.464d0, cp=6d0 /\n&fields_list {stress} /\n"
+    return f"""&problem_list name='matrix', nt={nt}, CFL=0.5d0, RKorder=4 /
+&domain_list mode={mode}, FDmethod='{fd}', {dom} /
+!---BLOCK1---
+&grid_list {g1} /
+&boundaries_list {b1} /
+{blk}!---BLOCK2---
+&grid_list {g2} /
+&boundaries_list {b2} /
+{blk}{extra_blocks}!---IFACE1---
+&interface_list coupling='friction', direction='{direction}' /
+&friction_list friction_law='{law}', {params} {ldline}
+  rup_field='V', rup_threshold=1d-3 {friction_extra} /
+"""
+
+
+CASES = {
+    # friction laws, mode II, fault y = 0
+    "SW": dict(),
+    "SL": dict(law="SL"),
+    "FL": dict(law="FL"),
+    "RSL": dict(law="RSL"),
+    "RFL": dict(law="RFL"),
+    "RSF": dict(law="RSF"),
+    "RAL": dict(law="RAL"),
+    "frictionless": dict(law="frictionless", ld=""),
+    # mode III
+    "III-SW": dict(mode=3),
+    "III-RAL": dict(mode=3, law="RAL"),
+    "III-x-RSL": dict(mode=3, law="RSL", direction="x"),
+    # fault x = 0
+    "x-SW": dict(direction="x", ld="boxcar"),
+    "x-RFL": dict(direction="x", law="RFL"),
+    # load shapes
+    "ld-uniform": dict(ld="uniform"),
+    "ld-linear": dict(ld="linear"),
+    "ld-smooth_boxcar": dict(ld="smooth_boxcar"),
+    "ld-triangle": dict(ld="triangle"),
+    "ld-smooth": dict(ld="smooth"),
+    "ld-ramp": dict(ld="boxcar", friction_extra=", ld%T=0.1d0"),
+    # forced rupture, thermal pressurisation p0, regularised N, rupture on slip, rotated fault
+    "forced": dict(mode=3, ld="", friction_extra=", force=T, kn%fd=0.52d0, kn%dfdx=0.2d0, kn%vL=-2d0, kn%vR=2d0, "
+                                               "kn%xL=0.2d0, kn%xR=-0.2d0, kn%tmax=4d0"),
+    "tp-p0": dict(law="RSL", extra_blocks="", friction_extra=" /\n&thermpres_list n=64, p0=10d0"),
+    "reg": dict(law="RSL", friction_extra=", reg=T"),
+    "rup-D": dict(friction_extra=", rup_field='D'"),
+    "angle": dict(friction_extra=", angle=10d0"),
+    "lock-window": dict(friction_extra=", xlockm=-2d0, xlockp=2d0, flock=0.8d0"),
+    # outer boundary conditions
+    "bc-free": dict(bc="free"),
+    "bc-rigid": dict(bc="rigid"),
+    "bc-absorbing-0": dict(bc="absorbing-0"),
+    "bc-free-0": dict(bc="free-0"),
+    "bc-rigid-0": dict(bc="rigid-0"),
+    "bc-absorbing-velocity": dict(bc="absorbing-velocity"),
+    "bc-free-velocity": dict(bc="free-velocity"),
+    "III-bc-free": dict(mode=3, bc="free"),
+    "III-bc-rigid": dict(mode=3, bc="rigid"),
+    # operators
+    "SBP2": dict(fd="SBP2"),
+    "SBP6": dict(fd="SBP6", n=49),
+}
+
+
+def test_every_case_initialises_and_runs_on_the_oracle():
+    from oracle.binding import OracleDomain
+
+    for name, kw in CASES.items():
+        h = init_domain(fault_text(**kw))
+        o = OracleDomain(h)
+        o.run(1, 3)
+        F = o.get_fields()[0]
+        assert np.all(np.isfinite(F)), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(CASES))
+def test_gpu_vs_oracle(require_gpu, name):
+    from oracle.binding import OracleDomain
+
+    h = init_domain(fault_text(**CASES[name]))
+    g, o = GpuDomain(h), OracleDomain(h)
+    steps = 30
+    g.run(1, steps)
+    o.run(1, steps)
+    assert_fields_close(g.get_fields()[0], o.get_fields()[0], what=name)
+    assert_fault_close(g, o, dt=h.dt)
+    assert g.newton_failures() == o.newton_failures() == 0
+    assert np.abs(o.get_fault(0, "V")).max() > 1e-3, f"{name}: the fault should slip"
+    g.close()
