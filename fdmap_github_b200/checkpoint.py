@@ -4,9 +4,11 @@ The files follow checkpoint_op (checkpoint.f90:254-288) for a single-process
 run: native-endian float64, Fortran column-major arrays, no headers.
 
   <name>F.ckpt<n>                 F(:,:,l) for l = 1..nF over the global grid,
-                                  then DF(:,:,l), then the perfectly matched
-                                  layer fields Wx(:,:,:) and Wy(:,:,:) when the
-                                  domain has them          (fields.f90:335-429)
+                                  then DF(:,:,l); with displacement = T, per
+                                  component l U(:,:,l) and DU(:,:,l); with
+                                  peak = T, pgv and pga; then the perfectly
+                                  matched layer fields Wx(:,:,:) and Wy(:,:,:)
+                                  when the domain has them (fields.f90:335-429)
   <name>block<b><S>.ckpt<n>       for S = L, R, B, T: per field l the side's
                                   edge values F(:,l), hat variables Fhat(:,l),
                                   prestress F0(:,l); per displacement
@@ -57,6 +59,12 @@ def checkpoint_write(gpu, host, name: str | Path, number: int) -> list[Path]:
     files = []
     p = Path(f"{name}F.ckpt{number}")
     parts = [F.reshape(-1), DF.reshape(-1)]
+    if host.displacement:
+        U, DU = gpu.get_displacement()
+        for l in range(U.shape[0]):
+            parts += [U[l].reshape(-1), DU[l].reshape(-1)]
+    if host.peak:
+        parts += [p.reshape(-1) for p in gpu.get_peak()]
     for w, present in zip(("Wx", "Wy"), host.pml_fields()):
         if present:
             parts.append(gpu.get_pml(w).reshape(-1))
@@ -99,13 +107,24 @@ def checkpoint_read(gpu, host, name: str | Path, number: int | None = None) -> i
     nn = host.nF * host.ny * host.nx
     a = np.fromfile(f"{name}F.ckpt{number}", dtype=np.float64)
     pml = [w for w, present in zip(("Wx", "Wy"), host.pml_fields()) if present]
-    if a.size != (2 + len(pml)) * nn:
-        raise ValueError(f"{name}F.ckpt{number}: {a.size} values, expected {(2 + len(pml)) * nn}")
+    nU = 2 if host.mode == 2 else 1
+    plane = host.ny * host.nx
+    extra = (2 * nU if host.displacement else 0) + (2 if host.peak else 0)
+    if a.size != (2 + len(pml)) * nn + extra * plane:
+        raise ValueError(f"{name}F.ckpt{number}: {a.size} values, expected {(2 + len(pml)) * nn + extra * plane}")
     shape = (host.nF, host.ny, host.nx)
     gpu.set_fields(a[:nn].reshape(shape), a[nn:2 * nn].reshape(shape))
+    off = 2 * nn
+    if host.displacement:
+        U = np.stack([a[off + 2 * l * plane:off + (2 * l + 1) * plane] for l in range(nU)])
+        DU = np.stack([a[off + (2 * l + 1) * plane:off + (2 * l + 2) * plane] for l in range(nU)])
+        gpu.set_displacement(U.reshape(nU, host.ny, host.nx), DU.reshape(nU, host.ny, host.nx))
+        off += 2 * nU * plane
+    if host.peak:
+        gpu.set_peak(a[off:off + plane].reshape(host.ny, host.nx), a[off + plane:off + 2 * plane].reshape(host.ny, host.nx))
+        off += 2 * plane
     for k, w in enumerate(pml):
-        gpu.set_pml(w, a[(2 + k) * nn:(3 + k) * nn].reshape(shape))
-    nU = 2 if host.mode == 2 else 1
+        gpu.set_pml(w, a[off + k * nn:off + (k + 1) * nn].reshape(shape))
     for b in range(host.nblocks):
         for s in range(4):
             mgx, pgx, mgy, pgy = host.block_limits(b)

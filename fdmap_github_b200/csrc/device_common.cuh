@@ -62,6 +62,8 @@ struct DevBlock {
   const double* gforce;                // tsunami forcing: amp*exp(-(x/sigma)^2/2 - (y/sigma)^2/2) per node, or NULL
   const double* frc_old;               // forcing from file: frames at the step's start and end,
   const double* frc_new;               //   nF planes each (NULL when no forcing file)
+  double *U, *DU, *Utap;               // body displacement, its rate, its stage-1 value: nU planes (displacement = T)
+  double *pgv, *pga;                   // peak ground velocity / acceleration planes (peak = T)
   int tile_begin;                      // first stencil tile of this block
   int tiles_x;
   long long march_unit_begin;          // first row-group unit of this block (march kernel)
@@ -164,6 +166,7 @@ struct StageArgs {
   double C;      // RK C(stage-1): stage time = t0 + C*dt
   int tap;       // stage 1 with outputs open: interface kernels write their output snapshot
   double t0, dt; // step start and length (when ts == nullptr)
+  int first;     // stage 1 (update_fields_peak)
 };
 
 // Stage time t0 + C*dt with t0 = t_start + (n-1)*dt, rounded exactly as the

@@ -63,6 +63,7 @@ struct fdmap_gpu {
   bool dissipation = false;  // some block has Cdiss > 0 (tiled interior kernel)
   bool pml = false;  // some block has a perfectly matched layer (tiled interior kernel)
   bool forcing = false;  // tsunami forcing or forcing from file (tiled interior kernel)
+  bool extras = false;   // body displacement or peak motion tracked (tiled interior kernel)
   std::FILE* frc_file = nullptr;  // forcing frames, one (nx,ny,nF) frame per step
   std::vector<double> frc_host;   // the frame being loaded
   bool body_on_device = false;  // body built by build_body (fdmap_desc.body)

@@ -580,6 +580,21 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       B.frc_new = fn;
       h->forcing = true;
     }
+    B.U = B.DU = B.Utap = B.pgv = B.pga = nullptr;
+    if (d->displacement) {
+      // U = 0, DU = 1e40 (fields.f90:183-186)
+      const int nU = d->mode == 2 ? 2 : 1;
+      if ((rc = h->alloc_planes(&B.U, nU, g.plane)) || (rc = h->alloc_planes(&B.DU, nU, g.plane)) ||
+          (rc = h->alloc_planes(&B.Utap, nU, g.plane)))
+        return rc;
+      std::vector<double> big((size_t)nU * g.plane, 1e40);
+      CUDA_TRY(cudaMemcpy(B.DU, big.data(), big.size() * sizeof(double), cudaMemcpyHostToDevice));
+      h->extras = true;
+    }
+    if (d->peak) {
+      if ((rc = h->alloc_planes(&B.pgv, 1, g.plane)) || (rc = h->alloc_planes(&B.pga, 1, g.plane))) return rc;
+      h->extras = true;
+    }
     B.rinv_b = 1.0 / fb.rho;
     for (int s = 1; s <= op.pI; ++s) {
       B.coef[s][0] = op.DI[s] / fb.rho;
@@ -737,7 +752,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   {
     const char* ek = getenv("FDMAP_STENCIL");
     // dissipative blocks need J at the neighbours, which the march ring does not carry
-    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation && !h->pml && !h->forcing;
+    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation && !h->pml && !h->forcing && !h->extras;
     if (h->use_march && (rc = march_dispatch(h, nullptr))) return rc;
     // fused stage launches need every interface-side node to sit on one interface only
     bool junction = false;
@@ -796,6 +811,7 @@ int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, con
     a.C = h->rk.C[s];
     a.t0 = t0;
     a.dt = dt;
+    a.first = s == 0 ? 1 : 0;
     a.ts = ts;
     a.in = cur;
     a.out = 1 - cur;
@@ -1018,6 +1034,74 @@ int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out) {
   }
   CUDA_TRY(cudaMemcpyAsync(out, h->d_global, (size_t)NN * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+
+namespace {
+// planes `which` of every block (body displacement U / DU, nU planes; peak pgv / pga, 1 plane)
+// between the host's global layout and the device
+int body_planes(fdmap_gpu* h, int which, double* out, const double* in) {
+  const int nU = h->mode == 2 ? 2 : 1;
+  const int np = which <= 1 ? nU : 1;
+  const long long NN = (long long)h->nx_g * h->ny_g;
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    double* const planes[4] = {B.U, B.DU, B.pgv, B.pga};
+    if (!planes[which])
+      return set_err(FDMAP_ERR_INVALID_ARG, which <= 1 ? "the domain does not track the body displacement"
+                                                       : "the domain does not track peak motion");
+  }
+  CUDA_TRY(cudaSetDevice(h->device));
+  if (in) CUDA_TRY(cudaMemcpyAsync(h->d_global, in, (size_t)NN * np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    double* const planes[4] = {B.U, B.DU, B.pgv, B.pga};
+    const BlockGeom& g = h->geom[b];
+    dim3 grid((g.pitch + 255) / 256, g.ny);
+    if (in)
+      scatter_block<<<grid, 256, 0, h->stream>>>(h->d_global, planes[which], h->nx_g, NN, g.mgx, g.mgy, g.nx, g.ny,
+                                                 g.pitch, g.plane, np);
+    else
+      gather_block<<<grid, 256, 0, h->stream>>>(planes[which], h->d_global, h->nx_g, NN, g.mgx, g.mgy, g.nx, g.ny,
+                                                g.pitch, g.plane, np);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (out)
+    CUDA_TRY(cudaMemcpyAsync(out, h->d_global, (size_t)NN * np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
+}
+}  // namespace
+
+int fdmap_gpu_get_displacement(fdmap_gpu* h, double* U, double* DU) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  int rc = FDMAP_OK;
+  if (U && (rc = body_planes(h, 0, U, nullptr))) return rc;
+  if (DU && (rc = body_planes(h, 1, DU, nullptr))) return rc;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_displacement(fdmap_gpu* h, const double* U, const double* DU) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  int rc = FDMAP_OK;
+  if (U && (rc = body_planes(h, 0, nullptr, U))) return rc;
+  if (DU && (rc = body_planes(h, 1, nullptr, DU))) return rc;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_peak(fdmap_gpu* h, double* pgv, double* pga) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  int rc = FDMAP_OK;
+  if (pgv && (rc = body_planes(h, 2, pgv, nullptr))) return rc;
+  if (pga && (rc = body_planes(h, 3, pga, nullptr))) return rc;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_peak(fdmap_gpu* h, const double* pgv, const double* pga) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  int rc = FDMAP_OK;
+  if (pgv && (rc = body_planes(h, 2, nullptr, pgv))) return rc;
+  if (pga && (rc = body_planes(h, 3, nullptr, pga))) return rc;
   return FDMAP_OK;
 }
 

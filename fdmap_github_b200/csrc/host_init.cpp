@@ -536,10 +536,10 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
   if (get_bool(dl, "operator_split", false)) fail(FDMAP_ERR_UNSUPPORTED, "operator_split=T is not supported");
   if (get_bool(dl, "acoustic_gravity_waves", false) || get_bool(dl, "basal_traction_plane_stress", false))
     fail(FDMAP_ERR_UNSUPPORTED, "acoustic gravity / basal traction terms are not supported");
-  // body displacement (set_rates_displacement), peak motion (update_fields_peak)
-  // and the boundary energy balance (set_rates_energy) are not tracked
-  for (const char* flag : {"displacement", "peak", "energy_balance"})
-    if (get_bool(dl, flag, false)) fail(FDMAP_ERR_UNSUPPORTED, std::string(flag) + "=T is not supported");
+  // the energy balance (energy_block, set_rates_energy) is not tracked
+  if (get_bool(dl, "energy_balance", false)) fail(FDMAP_ERR_UNSUPPORTED, "energy_balance=T is not supported");
+  d.displacement = get_bool(dl, "displacement", false) ? 1 : 0;
+  d.peak = get_bool(dl, "peak", false) ? 1 : 0;
   std::vector<int> nx_list = get_int_list(dl, "nx_list"), ny_list = get_int_list(dl, "ny_list");
   if (mode != 2 && mode != 3) fail(FDMAP_ERR_INVALID_ARG, "mode must be 2 or 3");
   int method;
@@ -1209,6 +1209,13 @@ extern "C" int fdmap_host_info(const fdmap_domain* dom, int* ints, double* dbls)
   if (dbls) {
     dbls[0] = d.t0; dbls[1] = d.dt; dbls[2] = d.CFL; dbls[3] = d.hmin; dbls[4] = d.hmax;
   }
+  return FDMAP_OK;
+}
+
+extern "C" int fdmap_host_body_flags(const fdmap_domain* dom, int* flags) {
+  if (!dom || !flags) return FDMAP_ERR_INVALID_ARG;
+  flags[0] = dom->desc.displacement;
+  flags[1] = dom->desc.peak;
   return FDMAP_OK;
 }
 

@@ -66,7 +66,10 @@ __global__ void output_gather_kernel(const __grid_constant__ DevDomain D, const 
                                       : S.Fhat[(long long)it.ffield * S.n + elem_off[e]];
   } else {
     const DevBlock& B = D.blk[elem_b[e]];
-    v = B.F[cur][(long long)it.index * B.plane + elem_off[e]];
+    const int f = it.index;
+    if (f < FDMAP_OUT_BODY_U) v = B.F[cur][(long long)f * B.plane + elem_off[e]];
+    else if (f < FDMAP_OUT_BODY_PGV) v = B.Utap[(long long)(f - FDMAP_OUT_BODY_U) * B.plane + elem_off[e]];
+    else v = (f == FDMAP_OUT_BODY_PGV ? B.pgv : B.pga)[elem_off[e]];
   }
   ring[it.ring0 + (rec % R) * it.size + (e - it.elem0)] = (float)v;
 }
@@ -301,7 +304,11 @@ int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, in
     it.d.ffield = field;
     for (int k = mx; k <= px; k += sx) { it.eb.push_back(0); it.eoff.push_back(k - 1); }
   } else if (kind == FDMAP_OUT_BODY) {
-    if (field < 0 || field >= h->nF) return set_err(FDMAP_ERR_INVALID_ARG, "output: bad body field");
+    const int nU = h->mode == 2 ? 2 : 1;
+    const bool ok = (field >= 0 && field < h->nF) ||
+                    (field >= FDMAP_OUT_BODY_U && field < FDMAP_OUT_BODY_U + nU && h->hdom.blk[0].Utap) ||
+                    ((field == FDMAP_OUT_BODY_PGV || field == FDMAP_OUT_BODY_PGA) && h->hdom.blk[0].pgv);
+    if (!ok) return set_err(FDMAP_ERR_INVALID_ARG, "output: bad body field (or displacement / peak not tracked)");
     if (mx < 1 || px > h->nx_g || mx > px || my < 1 || py > h->ny_g || my > py)
       return set_err(FDMAP_ERR_INVALID_ARG, "output: body indices out of range");
     it.d.index = field;

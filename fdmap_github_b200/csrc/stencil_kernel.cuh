@@ -318,6 +318,41 @@ __device__ __forceinline__ void body_forces(const DevDomain& D, const DevBlock& 
   }
 }
 
+// body displacement and peak motion of one node, after its rates are complete:
+// DU <- A*DU + F(1:nU), U <- U + Bdt*DU (scale_rates_interior,
+// set_rates_displacement, update_fields_interior, fields.f90:1060-1258), the
+// stage-1 U kept for the output; in stage 1 pgv <- max(pgv, |v|),
+// pga <- max(pga, |dv/dt|) (update_fields_peak, fields.f90:1136-1164)
+template <int MODE>
+__device__ __forceinline__ void body_extras(const DevBlock& B, long long c, const double* Fc, const double* acc,
+                                            const StageArgs& a) {
+  if (B.DU) {
+    constexpr int NU = MODE == 2 ? 2 : 1;
+#pragma unroll
+    for (int l = 0; l < NU; ++l) {
+      const long long q = l * B.plane + c;
+      const double u = B.U[q];
+      double du = a.A != 0.0 ? a.A * B.DU[q] : 0.0;
+      du = du + Fc[l];
+      B.DU[q] = du;
+      if (a.tap && B.Utap) B.Utap[q] = u;
+      if (a.update) B.U[q] = u + a.Bdt * du;
+    }
+  }
+  if (B.pgv && a.first) {
+    double v, dv;
+    if (MODE == 2) {
+      v = sqrt(Fc[0] * Fc[0] + Fc[1] * Fc[1]);
+      dv = sqrt(acc[0] * acc[0] + acc[1] * acc[1]);
+    } else {
+      v = fabs(Fc[0]);
+      dv = fabs(acc[0]);
+    }
+    B.pgv[c] = fmax(B.pgv[c], v);
+    B.pga[c] = fmax(B.pga[c], dv);
+  }
+}
+
 __device__ __forceinline__ bool interior_node(const DevDomain& D, const DevBlock& B, int i, int j) {
   return i >= D.nbst && i <= B.nx - 1 - D.nbst && j >= D.nbst && j <= B.ny - 1 - D.nbst;
 }
@@ -530,6 +565,7 @@ __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock&
   if (!pml) closure_rates<MODE, PI_>(D, B, Fin, i, j, m, B.Ji[c], acc);
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
   body_forces<MODE>(D, B, i, j, stage_time(a), a, acc);
+  body_extras<MODE>(B, c, Fc, acc, a);
 #pragma unroll
   for (int l = 0; l < NF; ++l) B.DF[l * plane + c] = acc[l];
   if (a.update) {
@@ -734,6 +770,7 @@ __global__ void __launch_bounds__(TX* TY) stencil_kernel(const DevDomain* __rest
 
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
   body_forces<MODE>(D, B, i, j, stage_time(a), a, acc);
+  body_extras<MODE>(B, c, Fc, acc, a);
 
   double* __restrict__ DF = B.DF;
 #pragma unroll

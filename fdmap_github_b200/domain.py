@@ -40,6 +40,9 @@ class HostDomain:
         (self.mode, self.nF, self.nx, self.ny, self.nblocks, self.nifaces, self.nt, self.rk_order, self.fd_method,
          het) = list(ints)
         self.heterogeneous = bool(het)
+        fl = (C.c_int * 2)()
+        check_host(lib().fdmap_host_body_flags(self._h, fl), "fdmap_host_body_flags")
+        self.displacement, self.peak = bool(fl[0]), bool(fl[1])
         (self.t0, self.dt, self.CFL, self.hmin, self.hmax) = list(dbls)
 
     @property
@@ -186,6 +189,29 @@ class GpuDomain:
         out = np.empty((self.ny, self.nx))
         check_gpu(lib().fdmap_gpu_get_metric(self._g, native.METRIC_INDEX[name], dptr(out)), "fdmap_gpu_get_metric")
         return out
+
+    def get_displacement(self):
+        """Body displacement U and its rate DU (domain_list displacement = T), each (nU, ny, nx)."""
+        nU = 2 if self.host.mode == 2 else 1
+        U, DU = np.empty((nU, self.ny, self.nx)), np.empty((nU, self.ny, self.nx))
+        check_gpu(lib().fdmap_gpu_get_displacement(self._g, dptr(U), dptr(DU)), "fdmap_gpu_get_displacement")
+        return U, DU
+
+    def set_displacement(self, U=None, DU=None) -> None:
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        DU = None if DU is None else np.ascontiguousarray(DU, dtype=np.float64)
+        check_gpu(lib().fdmap_gpu_set_displacement(self._g, dptr(U), dptr(DU)), "fdmap_gpu_set_displacement")
+
+    def get_peak(self):
+        """Peak ground velocity and acceleration (domain_list peak = T), each (ny, nx)."""
+        pgv, pga = np.empty((self.ny, self.nx)), np.empty((self.ny, self.nx))
+        check_gpu(lib().fdmap_gpu_get_peak(self._g, dptr(pgv), dptr(pga)), "fdmap_gpu_get_peak")
+        return pgv, pga
+
+    def set_peak(self, pgv=None, pga=None) -> None:
+        pgv = None if pgv is None else np.ascontiguousarray(pgv, dtype=np.float64)
+        pga = None if pga is None else np.ascontiguousarray(pga, dtype=np.float64)
+        check_gpu(lib().fdmap_gpu_set_peak(self._g, dptr(pgv), dptr(pga)), "fdmap_gpu_set_peak")
 
     def get_side_displacement(self, b: int, s: int):
         """Boundary displacement U and its rate DU of block b, side s: each (nU, n)."""

@@ -46,6 +46,7 @@ SIGNATURES = {
     "fdmap_host_free": (None, [_VP]),
     "fdmap_host_info": (C.c_int, [_VP, C.POINTER(C.c_int), _DP]),
     "fdmap_host_iface_n": (C.c_int, [_VP, C.c_int]),
+    "fdmap_host_body_flags": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "fdmap_host_block_limits": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
     "fdmap_host_block_pml": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), _DP]),
     "fdmap_host_block_cdiss": (C.c_double, [_VP, C.c_int]),
@@ -74,6 +75,10 @@ SIGNATURES = {
     "fdmap_gpu_get_side_impedance": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_get_pml": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_get_side_displacement": (C.c_int, [_VP, C.c_int, C.c_int, _DP, _DP]),
+    "fdmap_gpu_get_displacement": (C.c_int, [_VP, _DP, _DP]),
+    "fdmap_gpu_set_displacement": (C.c_int, [_VP, _DP, _DP]),
+    "fdmap_gpu_get_peak": (C.c_int, [_VP, _DP, _DP]),
+    "fdmap_gpu_set_peak": (C.c_int, [_VP, _DP, _DP]),
     "fdmap_gpu_set_side_displacement": (C.c_int, [_VP, C.c_int, C.c_int, _DP, _DP]),
     "fdmap_gpu_set_pml": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_fault_max_noalloc": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),

@@ -24,6 +24,8 @@ import numpy as np
 from .native import FAULT_INDEX
 
 OUT_FAULT, OUT_BODY, OUT_SIDE, OUT_SIDE_U = 0, 1, 2, 8
+# body displacement and peak motion (get_field, domain.f90:551-557)
+BODY_EXTRA = {"ux": 16, "uz": 16, "uy": 17, "pgv": 24, "pga": 25}
 # bndX locations (get_field, domain.f90:763-860): the hat variables by position
 # (vx or vz the first, vy the second, sxx, sxy, syy the third to fifth) and the
 # boundary displacement; x, y are static
@@ -172,9 +174,13 @@ def configure_outputs(gpu, host, text: str, prefix: str | Path, ring_steps: int 
                     arr = host.array(f)[0]
                     static.append((bn, arr[my - 1:py:sy, mx - 1:px:sx], nmin, nmax))
                     continue
-                if f not in BODY_FIELDS[mode]:
+                if f in BODY_FIELDS[mode]:
+                    fld = BODY_FIELDS[mode].index(f)
+                elif f in BODY_EXTRA and not (mode == 3 and f == "uy"):
+                    fld = BODY_EXTRA[f]
+                else:
                     raise ValueError(f"output field {f!r} is not a mode {mode} body field")
-                gpu.output_add(bn, OUT_BODY, -1, BODY_FIELDS[mode].index(f), mx, px, sx, my, py, sy,
+                gpu.output_add(bn, OUT_BODY, -1, fld, mx, px, sx, my, py, sy,
                                nmin=nmin, nmax=nmax, stride=it.stride)
                 names.append(bn)
     # static fields: written once, as the reference does at its first output step

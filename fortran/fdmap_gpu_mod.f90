@@ -87,6 +87,7 @@ module fdmap_gpu_mod
      integer(c_int) :: nt
      real(c_double) :: hmin, hmax
      type(c_ptr) :: body          ! fdmap_body_t, or c_null_ptr: body arrays given by the host
+     integer(c_int) :: displacement, peak  ! domain_list displacement, peak (F%displacement, F%peak)
   end type fdmap_desc_t
 
   ! on-device initialisation (fdmap_desc.h: fdmap_perturb, fdmap_block_body, fdmap_body)
@@ -203,6 +204,26 @@ module fdmap_gpu_mod
        integer(c_int), value :: which
        real(c_double), intent(in) :: in(*)
      end function fdmap_gpu_set_pml
+
+     integer(c_int) function fdmap_gpu_get_displacement(h, U, DU) bind(C, name='fdmap_gpu_get_displacement')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, U, DU              ! (nx, ny, nU) each, or c_null_ptr
+     end function fdmap_gpu_get_displacement
+
+     integer(c_int) function fdmap_gpu_set_displacement(h, U, DU) bind(C, name='fdmap_gpu_set_displacement')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, U, DU
+     end function fdmap_gpu_set_displacement
+
+     integer(c_int) function fdmap_gpu_get_peak(h, pgv, pga) bind(C, name='fdmap_gpu_get_peak')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, pgv, pga           ! (nx, ny) each, or c_null_ptr
+     end function fdmap_gpu_get_peak
+
+     integer(c_int) function fdmap_gpu_set_peak(h, pgv, pga) bind(C, name='fdmap_gpu_set_peak')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h, pgv, pga
+     end function fdmap_gpu_set_peak
 
      integer(c_int) function fdmap_gpu_get_side_displacement(h, b, s, U, DU) &
           bind(C, name='fdmap_gpu_get_side_displacement')

@@ -262,6 +262,11 @@ typedef struct fdmap_desc {
   /* non-NULL: body built on the device (t0 is final; dt, CFL, nt, hmin, hmax
    * are finished by the engine, fdmap_gpu_time_params) */
   const fdmap_body* body;
+  /* domain_list displacement: body displacement U (nx,ny,nU) integrated from
+   * the velocities (set_rates_displacement, fields.f90:1245-1258); peak: peak
+   * ground velocity and acceleration pgv, pga (nx,ny) updated in stage 1
+   * (update_fields_peak, fields.f90:1136-1164) */
+  int displacement, peak;
 } fdmap_desc;
 
 #ifdef __cplusplus

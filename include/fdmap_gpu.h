@@ -92,6 +92,15 @@ int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out);
 int fdmap_gpu_get_pml(fdmap_gpu* h, int which, double* out);
 int fdmap_gpu_set_pml(fdmap_gpu* h, int which, const double* in);
 
+/* Body displacement U(nx,ny,nU) and its rate DU (F%U, F%DU; domain_list
+ * displacement = T) and peak ground velocity / acceleration pgv, pga (nx,ny;
+ * peak = T), global layout; any pointer may be NULL.  FDMAP_ERR_INVALID_ARG
+ * when the domain does not track them. */
+int fdmap_gpu_get_displacement(fdmap_gpu* h, double* U, double* DU);
+int fdmap_gpu_set_displacement(fdmap_gpu* h, const double* U, const double* DU);
+int fdmap_gpu_get_peak(fdmap_gpu* h, double* pgv, double* pga);
+int fdmap_gpu_set_peak(fdmap_gpu* h, const double* pgv, const double* pga);
+
 /* Boundary displacement U(n,nU) and its rate DU(n,nU) of side s (0..3 =
  * L,R,B,T) of block b (bndF%U, bndF%DU; nU = 2 in mode II, 1 in mode III):
  * integrated from the side's hat velocities every stage as the reference
@@ -118,7 +127,9 @@ int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
  * open_output_file names and lays out its files (output.f90:916-987).
  *   FDMAP_OUT_FAULT: `index` = interface, `field` = FDMAP_FAULT_*,
  *                    nodes mx..px (1-based along the interface) step sx;
- *   FDMAP_OUT_BODY:  `field` = body field component (0..nF-1), global
+ *   FDMAP_OUT_BODY:  `field` = body field component (0..nF-1), or
+ *                    FDMAP_OUT_BODY_U + c (displacement component c),
+ *                    FDMAP_OUT_BODY_PGV / _PGA (peak motion), global
  *                    nodes mx..px step sx by my..py step sy;
  *   FDMAP_OUT_SIDE:  `index` = 4*block + side (0..3 = L,R,B,T), `field` =
  *                    hat variable component 0..nF-1 or FDMAP_OUT_SIDE_U + c
@@ -128,7 +139,8 @@ int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
  * Items are added before fdmap_gpu_output_open; fdmap_gpu_output_flush
  * writes everything recorded so far, fdmap_gpu_output_close flushes and
  * releases the rings. */
-enum { FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1, FDMAP_OUT_SIDE = 2, FDMAP_OUT_SIDE_U = 8 };
+enum { FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1, FDMAP_OUT_SIDE = 2, FDMAP_OUT_SIDE_U = 8, FDMAP_OUT_BODY_U = 16,
+       FDMAP_OUT_BODY_PGV = 24, FDMAP_OUT_BODY_PGA = 25 };
 int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, int field, int mx, int px, int sx,
                          int my, int py, int sy, long long nmin, long long nmax, int stride);
 int fdmap_gpu_output_open(fdmap_gpu* h, const char* prefix, int ring_steps);

@@ -35,6 +35,7 @@ def lib() -> C.CDLL:
         L.oracle_get_fhat.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         L.oracle_get_pml.argtypes = [C.c_void_p, C.c_int, _DP]
         L.oracle_get_side_u.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP, _DP]
+        L.oracle_get_body_extras.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP]
         L.oracle_newton_failures.restype = C.c_longlong
         L.oracle_newton_failures.argtypes = [C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
@@ -90,6 +91,21 @@ class OracleDomain:
         out = np.empty(n * self.nF)
         lib().oracle_get_fhat(self._o, b, s, _p(out))
         return out.reshape(self.nF, n)
+
+    def get_displacement(self):
+        """Body displacement U and its rate DU, each (nU, ny, nx)."""
+        nU = 2 if self.host.mode == 2 else 1
+        U, DU = np.empty((nU, self.ny, self.nx)), np.empty((nU, self.ny, self.nx))
+        if lib().oracle_get_body_extras(self._o, _p(U), _p(DU), None, None):
+            raise RuntimeError("the domain does not track the body displacement")
+        return U, DU
+
+    def get_peak(self):
+        """Peak ground velocity and acceleration, each (ny, nx)."""
+        pgv, pga = np.empty((self.ny, self.nx)), np.empty((self.ny, self.nx))
+        if lib().oracle_get_body_extras(self._o, None, None, _p(pgv), _p(pga)):
+            raise RuntimeError("the domain does not track peak motion")
+        return pgv, pga
 
     def get_side_u(self, b: int, s: int):
         """Boundary displacement U and its rate DU of block b, side s: each (nU, n)."""

@@ -178,6 +178,8 @@ struct oracle_domain {
   vec F, DF, x, y, xq, xr, yq, yr, J, Ji;
   vec rho, G, M, gamma, nu;
   vec Wx, DWx, Wy, DWy;  // PML fields (nx,ny,nF), allocated when some block has pmlx / pmly (fields.f90:203-210)
+  vec U, DU;             // body displacement and its rate (nx,ny,nU), displacement = T (fields.f90:183-186)
+  vec pgv, pga;          // peak ground velocity / acceleration (nx,ny), peak = T (fields.f90:187-190)
   fdmap_source src;
   // forcing from file (source.f90:12-14): the frames of the current step and its window
   std::FILE* frc = nullptr;
@@ -1397,6 +1399,10 @@ void point_source(oracle_domain& D, const Blk& B, double t, double pi) {
 void set_rates_all(oracle_domain& D) {
   for (auto& B : D.blk) set_rates_SAT(D, B);
   for (auto& B : D.blk) set_rates(D, B);
+  // set_rates_displacement (fields.f90:1245-1258): DU += F(:, :, 1:nU)
+  if (!D.U.empty()) {
+    for (size_t q = 0; q < D.DU.size(); ++q) D.DU[q] = D.DU[q] + D.F[q];  // U(:,:,l) pairs with F(:,:,l)
+  }
   for (auto& B : D.blk) set_source(D, B, D.t);
   // set_rates_boundary (fields.f90:1261-1276): DU += Fhat(:, 1:nU) on every side
   const int nU = D.mode == 2 ? 2 : 1;
@@ -1418,6 +1424,7 @@ void scale_rates_all(oracle_domain& D, double A) {
     for (double& v : *W) v = A * v;
   for (auto& I : D.ifc)
     if (I.coupling == FDMAP_COUPLING_FRICTION) scale_rates_friction(I.fr, A);
+  for (double& v : D.DU) v = A * v;  // scale_rates_interior: body displacement rates
   // scale_rates_boundary (fields.f90:1083-1097): boundary displacement rates
   for (auto& B : D.blk)
     for (auto& S : B.side)
@@ -1433,6 +1440,7 @@ void update_fields_all(oracle_domain& D, double Bdt) {
   for (size_t q = 0; q < D.Wy.size(); ++q) D.Wy[q] = D.Wy[q] + Bdt * D.DWy[q];
   for (auto& I : D.ifc)
     if (I.coupling == FDMAP_COUPLING_FRICTION) update_fields_friction(I.fr, Bdt);
+  for (size_t q = 0; q < D.U.size(); ++q) D.U[q] = D.U[q] + Bdt * D.DU[q];  // update_fields_interior
   // update_fields_boundary (fields.f90:1189-1204)
   for (auto& B : D.blk)
     for (auto& S : B.side)
@@ -1469,6 +1477,15 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
     o->gamma = copyv(d->gamma, NN); o->nu = copyv(d->nu, NN);
   }
   o->src = d->src;
+  if (d->displacement) {
+    const size_t nU = d->mode == 2 ? 2 : 1;
+    o->U.assign(NN * nU, 0.0);
+    o->DU.assign(NN * nU, 1e40);
+  }
+  if (d->peak) {
+    o->pgv.assign(NN, 0.0);
+    o->pga.assign(NN, 0.0);
+  }
   if (d->src.forcing_filename) {
     // init_forcing_from_file (source.f90:409-448): frame 0 into the new frame
     o->frc = std::fopen(d->src.forcing_filename, "rb");
@@ -1570,6 +1587,19 @@ int oracle_time_step(oracle_domain* o, double t0, double dt, int final_step) {
     prepare_edges(D);
     enforce_edge_conditions(D, D.rk.B[stage - 1] * dt);
     set_rates_all(D);
+    if (stage == 1 && !D.pgv.empty()) {
+      // update_fields_peak (fields.f90:1136-1164), stage 1 only
+      const size_t NN = (size_t)D.nx * D.ny;
+      for (size_t g = 0; g < NN; ++g) {
+        if (D.mode == 2) {
+          D.pgv[g] = std::max(D.pgv[g], std::sqrt(D.F[g] * D.F[g] + D.F[g + NN] * D.F[g + NN]));
+          D.pga[g] = std::max(D.pga[g], std::sqrt(D.DF[g] * D.DF[g] + D.DF[g + NN] * D.DF[g + NN]));
+        } else {
+          D.pgv[g] = std::max(D.pgv[g], std::fabs(D.F[g]));
+          D.pga[g] = std::max(D.pga[g], std::fabs(D.DF[g]));
+        }
+      }
+    }
     if (final_step) return FDMAP_OK;
     D.t = t0 + D.rk.C[stage] * dt;
     update_fields_all(D, D.rk.B[stage - 1] * dt);
@@ -1617,6 +1647,18 @@ int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out) {
 }
 
 long long oracle_newton_failures(const oracle_domain* o) { return o ? o->newton_fail : -1; }
+
+// body displacement U, DU (nx,ny,nU) and peak motion pgv, pga (nx,ny); any may be NULL, -1 when absent
+int oracle_get_body_extras(const oracle_domain* o, double* U, double* DU, double* pgv, double* pga) {
+  if (!o) return -1;
+  if ((U || DU) && o->U.empty()) return -1;
+  if ((pgv || pga) && o->pgv.empty()) return -1;
+  if (U) std::copy(o->U.begin(), o->U.end(), U);
+  if (DU) std::copy(o->DU.begin(), o->DU.end(), DU);
+  if (pgv) std::copy(o->pgv.begin(), o->pgv.end(), pgv);
+  if (pga) std::copy(o->pga.begin(), o->pga.end(), pga);
+  return 0;
+}
 
 // boundary displacement U and its rate DU of side s of block b, (n, nU) each (either may be NULL)
 int oracle_get_side_u(const oracle_domain* o, int b, int s, double* U, double* DU) {

@@ -59,6 +59,10 @@ int oracle_get_fault(const oracle_domain* o, int iface, int field, double* out);
 /* Hat variables of side s (0..3) of block b: (n, nF). */
 int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out);
 
+/* Body displacement U, DU (nx, ny, nU) and peak motion pgv, pga (nx, ny);
+ * any pointer may be NULL; -1 when the domain does not track them. */
+int oracle_get_body_extras(const oracle_domain* o, double* U, double* DU, double* pgv, double* pga);
+
 /* Boundary displacement U and rate DU of side s (0..3) of block b: (n, nU) each. */
 int oracle_get_side_u(const oracle_domain* o, int b, int s, double* U, double* DU);
 
