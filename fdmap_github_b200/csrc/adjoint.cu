@@ -113,7 +113,8 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// 3-D FP64 map over `nplanes` planes of the block layout, box {bx, by, bz}
+// 3-D FP64 map over `nplanes` planes of the block layout, box {bx, by, bz};
+// halo boxes start off the 256-byte lines, so no L2 promotion (sector fetches)
 int adj_encode(EncodeTiledFn enc, CUtensorMap* map, const double* base, const BlockGeom& g, long long nplanes, int bx,
                int by, int bz) {
   cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
@@ -121,7 +122,7 @@ int adj_encode(EncodeTiledFn enc, CUtensorMap* map, const double* base, const Bl
   cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double*>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_err(FDMAP_ERR_CUDA, "adjoint tensor map (" + std::to_string((int)r) + ")");
   return FDMAP_OK;

@@ -120,14 +120,19 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// 3-D FP64 tensor map over `nplanes` consecutive planes of a block array
+// 3-D FP64 tensor map over `nplanes` consecutive planes of a block array,
+// nx columns wide (the pitch padding reads as zeros without touching memory).
+// No L2 promotion: boxes with halo columns start 16 bytes before a 256-byte
+// line, and promotion would pull a whole line at each end of every row for
+// those 16 bytes; fetched by sector, the halos cost what they hold.
 int encode_map(EncodeTiledFn enc, CUtensorMap* map, double* base, const BlockGeom& g, int nplanes, int box_x, int box_z) {
-  cuuint64_t dims[3] = {(cuuint64_t)g.pitch, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
+  cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
   cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8};
   cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)MR, (cuuint32_t)box_z};
   cuuint32_t estr[3] = {1, 1, 1};
+  const CUtensorMapL2promotion promo = CU_TENSOR_MAP_L2_PROMOTION_NONE;
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return set_err(FDMAP_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
   return FDMAP_OK;
 }
