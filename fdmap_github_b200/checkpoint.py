@@ -22,9 +22,9 @@ run: native-endian float64, Fortran column-major arrays, no headers.
                                   Nreg, DNreg          (friction.f90:491-552)
   <name>.ckpt                     the number of the last checkpoint written
 
-The engine does not track the boundary energy (energy_balance is off), so E
-and DE are written as the reference leaves them then, 0 and 1e40, and ignored
-on reading.  A resume needs F, DF, the boundary displacement and the friction
+The boundary energies are written as the reference leaves them (E = 0; DE =
+1e40, or 0 once a step has run with energy_balance on) and ignored on
+reading.  A resume needs F, DF, the boundary displacement and the friction
 fields; edge values and hat variables are recomputed in stage 1 of the next
 step, exactly as the reference recomputes them after checkpoint_read.
 """
@@ -82,7 +82,11 @@ def checkpoint_write(gpu, host, name: str | Path, number: int) -> list[Path]:
                 parts += [Fe[l], Fh[l], F0[l]]
             for l in range(U.shape[0]):
                 parts += [U[l], DU[l]]
-            parts += [np.zeros(n), np.full(n, 1e40)]  # boundary energy E, DE (not tracked)
+            # boundary energy E and its rate DE: E stays 0 (the reference's boundary flux
+            # is a stub); DE keeps its 1e40 start value unless the energy balance is on,
+            # where every stage scales it by A (0 in the first stage)
+            de = np.zeros(n) if (host.energy_balance and number > 0) else np.full(n, 1e40)
+            parts += [np.zeros(n), de]
             p = Path(f"{name}block{b + 1}{SIDES[s]}.ckpt{number}")
             np.concatenate(parts).astype(np.float64).tofile(p)
             files.append(p)

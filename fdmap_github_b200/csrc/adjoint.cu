@@ -337,7 +337,7 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
   if (!d) return set_err(FDMAP_ERR_INVALID_ARG, "null descriptor");
   if (d->mode != 3 || d->nblocks != 1 || d->nifaces != 0 || !d->heterogeneous)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers one heterogeneous mode III block without interfaces");
-  if (d->displacement || d->peak)
+  if (d->displacement || d->peak || d->energy_balance)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint does not track displacement or peak motion");
   if (d->src.gauss_forcing || d->src.forcing_filename)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers the point source only");

@@ -64,6 +64,7 @@ struct DevBlock {
   const double* frc_new;               //   nF planes each (NULL when no forcing file)
   double *U, *DU, *Utap;               // body displacement, its rate, its stage-1 value: nU planes (displacement = T)
   double *pgv, *pga;                   // peak ground velocity / acceleration planes (peak = T)
+  const double *Hx, *Hy;               // diagonal SBP norm along i and j (energy_balance = T)
   int tile_begin;                      // first stencil tile of this block
   int tiles_x;
   long long march_unit_begin;          // first row-group unit of this block (march kernel)
@@ -123,6 +124,7 @@ struct DevDomain {
   int seg_start[4 * MAX_BLOCKS + MAX_IFACES + 1];
   fdmap_source src;
   unsigned long long* status;  // [0] Newton failures, [1] nonfinite flags
+  const double* energy;        // [nblocks + 1] stage-1 mechanical energy (energy_balance = T), or NULL
 };
 
 // TMA descriptors of every block, passed by value as a __grid_constant__ parameter

@@ -64,6 +64,8 @@ struct fdmap_gpu {
   bool pml = false;  // some block has a perfectly matched layer (tiled interior kernel)
   bool forcing = false;  // tsunami forcing or forcing from file (tiled interior kernel)
   bool extras = false;   // body displacement or peak motion tracked (tiled interior kernel)
+  double* d_energy = nullptr;  // [nblocks + 1] stage-1 energies (energy_balance = T)
+  double* d_epart = nullptr;   // their partial sums
   std::FILE* frc_file = nullptr;  // forcing frames, one (nx,ny,nF) frame per step
   std::vector<double> frc_host;   // the frame being loaded
   bool body_on_device = false;  // body built by build_body (fdmap_desc.body)
@@ -196,6 +198,11 @@ struct BatchPlan {
   int closure_ctas, closure_tpb;
   int edge_ctas, edge_tpb;
 };
+// Stage-1 mechanical energy of every block into h->d_energy (energy.cu), from
+// the fields of buffer `cur`.
+int launch_energy(fdmap_gpu* h, int cur);
+int energy_scratch_size(int nblocks);
+
 // Builds the body of a domain whose descriptor carries fdmap_desc.body
 // (body_init.cu) into the already allocated block planes and side arrays, and
 // finishes set_dt into h->tp / h->tp_nt and each block's scaled Cdiss.

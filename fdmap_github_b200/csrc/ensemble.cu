@@ -208,6 +208,8 @@ int fdmap_gpu_ensemble_create(const fdmap_desc* const* descs, int ninst, int dev
     for (int s = 0; s < h->rk.nstage; ++s)
       if (h->rk.A[s] != p->rk.A[s] || h->rk.B[s] != p->rk.B[s] || h->rk.C[s] != p->rk.C[s])
         return fail(set_err(FDMAP_ERR_INVALID_ARG, "ensemble instances must share the RK table"));
+    if (h->d_energy)
+      return fail(set_err(FDMAP_ERR_UNSUPPORTED, "ensembles do not track the energy balance"));
     if (!h->use_march)
       return fail(set_err(FDMAP_ERR_UNSUPPORTED, "ensembles need the marching interior kernel (homogeneous mode II or any mode III)"));
     if (h->cur != 0) return fail(set_err(FDMAP_ERR_INVALID_ARG, "instance buffer state"));

@@ -510,10 +510,22 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     B.Cdiss = fb.Cdiss;  // on-device body: scaled by build_body once dt is known
     B.J = nullptr;
     const double cdiss_in = d->body ? d->body->blocks[b].Cdiss : fb.Cdiss;
-    if (cdiss_in > 0.0) {  // the dissipation term weights neighbours by J itself
+    if (cdiss_in > 0.0 || d->energy_balance) {  // dissipation and the energy weight nodes by J itself
       if ((rc = h->alloc_planes(&B.J, 1, g.plane))) return rc;
       if (!d->body && (rc = h->upload_plane(B.J, d->J, g))) return rc;
-      h->dissipation = true;
+      if (cdiss_in > 0.0) h->dissipation = true;
+    }
+    B.Hx = B.Hy = nullptr;
+    if (d->energy_balance) {
+      // diagonal norm with unit spacing (Hnorm, fd.f90:14-39)
+      std::vector<double> hx(g.nx, 1.0), hy(g.ny, 1.0);
+      for (int k = 0; k < op.nbst; ++k) {
+        hx[k] = op.HL[k]; hx[g.nx - 1 - k] = op.HL[k];
+        hy[k] = op.HL[k]; hy[g.ny - 1 - k] = op.HL[k];
+      }
+      double *dx = nullptr, *dy = nullptr;
+      if ((rc = h->upload(&dx, hx.data(), hx.size())) || (rc = h->upload(&dy, hy.data(), hy.size()))) return rc;
+      B.Hx = dx; B.Hy = dy;
     }
     B.pml = 0; B.pml_kappa = 0.0; B.pml_h = nullptr; B.pml_s = nullptr;
     B.Wx = B.DWx = B.Wy = B.DWy = nullptr;
@@ -784,6 +796,15 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   }
   CUDA_TRY(cudaMemset(h->d_status, 0, 4 * sizeof(unsigned long long)));
   D.status = h->d_status;
+  D.energy = nullptr;
+  if (d->energy_balance) {
+    if ((rc = h->alloc(&h->d_energy, (size_t)d->nblocks + 1)) ||
+        (rc = h->alloc(&h->d_epart, (size_t)energy_scratch_size(d->nblocks))))
+      return rc;
+    std::vector<double> big((size_t)d->nblocks + 1, 1e40);  // BF%Etot = 1d40 until the first stage 1
+    CUDA_TRY(cudaMemcpy(h->d_energy, big.data(), big.size() * sizeof(double), cudaMemcpyHostToDevice));
+    D.energy = h->d_energy;
+  }
   if ((rc = h->alloc(&h->ddom, 1))) return rc;
   CUDA_TRY(cudaMemcpy(h->ddom, &D, sizeof(DevDomain), cudaMemcpyHostToDevice));
 
@@ -824,6 +845,7 @@ int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, con
     a.update = final_step ? 0 : 1;
     int rc = launch_stage(h, a);
     if (rc) return rc;
+    if (s == 0 && h->d_energy && (rc = launch_energy(h, cur0))) return rc;
     if (s == 0 && outputs && (rc = output_gather(h, ts, n, cur0))) return rc;
     if (final_step) return FDMAP_OK;
     cur = 1 - cur;
@@ -1077,6 +1099,15 @@ int body_planes(fdmap_gpu* h, int which, double* out, const double* in) {
   return FDMAP_OK;
 }
 }  // namespace
+
+int fdmap_gpu_get_energy(fdmap_gpu* h, double* E) {
+  if (!h || !E) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  if (!h->d_energy) return set_err(FDMAP_ERR_INVALID_ARG, "the domain does not track the energy");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemcpy(E, h->d_energy, (size_t)(h->hdom.nblocks + 1) * sizeof(double), cudaMemcpyDeviceToHost));
+  return FDMAP_OK;
+}
 
 int fdmap_gpu_get_displacement(fdmap_gpu* h, double* U, double* DU) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");

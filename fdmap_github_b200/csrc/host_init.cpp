@@ -536,8 +536,7 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
   if (get_bool(dl, "operator_split", false)) fail(FDMAP_ERR_UNSUPPORTED, "operator_split=T is not supported");
   if (get_bool(dl, "acoustic_gravity_waves", false) || get_bool(dl, "basal_traction_plane_stress", false))
     fail(FDMAP_ERR_UNSUPPORTED, "acoustic gravity / basal traction terms are not supported");
-  // the energy balance (energy_block, set_rates_energy) is not tracked
-  if (get_bool(dl, "energy_balance", false)) fail(FDMAP_ERR_UNSUPPORTED, "energy_balance=T is not supported");
+  d.energy_balance = get_bool(dl, "energy_balance", false) ? 1 : 0;
   d.displacement = get_bool(dl, "displacement", false) ? 1 : 0;
   d.peak = get_bool(dl, "peak", false) ? 1 : 0;
   std::vector<int> nx_list = get_int_list(dl, "nx_list"), ny_list = get_int_list(dl, "ny_list");
@@ -735,6 +734,9 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
       dom.nu[g] = 0.5 * (dom.M[g] - 2.0 * dom.G[g]) / (dom.M[g] - dom.G[g]);
     }
   }
+  // energy_block weights with the block's homogeneous constants (energy.f90:67-90)
+  if (d.energy_balance && any_het)
+    fail(FDMAP_ERR_UNSUPPORTED, "energy_balance=T with a heterogeneous medium is not supported");
   for (auto& B : dom.bin) {
     if (B.cs == 0.0 && !B.heterogeneous) fail(FDMAP_ERR_INVALID_ARG, "Must specify S-wave speed");
     if (B.cp == 0.0) B.cp = std::sqrt(3.0) * B.cs;
@@ -1216,6 +1218,7 @@ extern "C" int fdmap_host_body_flags(const fdmap_domain* dom, int* flags) {
   if (!dom || !flags) return FDMAP_ERR_INVALID_ARG;
   flags[0] = dom->desc.displacement;
   flags[1] = dom->desc.peak;
+  flags[2] = dom->desc.energy_balance;
   return FDMAP_OK;
 }
 

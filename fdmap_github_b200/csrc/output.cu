@@ -60,6 +60,8 @@ __global__ void output_gather_kernel(const __grid_constant__ DevDomain D, const 
   if (it.kind == FDMAP_OUT_FAULT) {
     const DevIface& I = D.ifc[it.index];
     v = I.fr.st_out[(long long)it.ffield * I.n + elem_off[e]];
+  } else if (it.kind == FDMAP_OUT_ENERGY) {
+    v = it.ffield == 0 ? D.energy[it.index] : 0.0;
   } else if (it.kind == FDMAP_OUT_SIDE) {
     const DevSide& S = D.blk[it.index >> 2].side[it.index & 3];
     v = it.ffield >= FDMAP_OUT_SIDE_U ? S.Utap[(long long)(it.ffield - FDMAP_OUT_SIDE_U) * S.n + elem_off[e]]
@@ -324,6 +326,14 @@ int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, in
         it.eb.push_back(b);
         it.eoff.push_back((long long)(j - g.mgy) * g.pitch + (i - g.mgx));
       }
+  } else if (kind == FDMAP_OUT_ENERGY) {
+    if (!h->d_energy) return set_err(FDMAP_ERR_INVALID_ARG, "output: the domain does not track the energy");
+    if (index < -1 || index >= h->hdom.nblocks || field < 0 || field > 1)
+      return set_err(FDMAP_ERR_INVALID_ARG, "output: bad energy item");
+    it.d.index = index < 0 ? h->hdom.nblocks : index;
+    it.d.ffield = field;
+    it.eb.push_back(0);
+    it.eoff.push_back(0);
   } else if (kind == FDMAP_OUT_SIDE) {
     const int b = index >> 2, s = index & 3;
     if (index < 0 || b >= h->hdom.nblocks) return set_err(FDMAP_ERR_INVALID_ARG, "output: side index out of range");

@@ -40,9 +40,9 @@ class HostDomain:
         (self.mode, self.nF, self.nx, self.ny, self.nblocks, self.nifaces, self.nt, self.rk_order, self.fd_method,
          het) = list(ints)
         self.heterogeneous = bool(het)
-        fl = (C.c_int * 2)()
+        fl = (C.c_int * 3)()
         check_host(lib().fdmap_host_body_flags(self._h, fl), "fdmap_host_body_flags")
-        self.displacement, self.peak = bool(fl[0]), bool(fl[1])
+        self.displacement, self.peak, self.energy_balance = bool(fl[0]), bool(fl[1]), bool(fl[2])
         (self.t0, self.dt, self.CFL, self.hmin, self.hmax) = list(dbls)
 
     @property
@@ -189,6 +189,12 @@ class GpuDomain:
         out = np.empty((self.ny, self.nx))
         check_gpu(lib().fdmap_gpu_get_metric(self._g, native.METRIC_INDEX[name], dptr(out)), "fdmap_gpu_get_metric")
         return out
+
+    def get_energy(self) -> np.ndarray:
+        """Mechanical energy of every block, then their sum, as of the last stage 1 (energy_balance = T)."""
+        E = np.empty(self.host.nblocks + 1)
+        check_gpu(lib().fdmap_gpu_get_energy(self._g, dptr(E)), "fdmap_gpu_get_energy")
+        return E
 
     def get_displacement(self):
         """Body displacement U and its rate DU (domain_list displacement = T), each (nU, ny, nx)."""

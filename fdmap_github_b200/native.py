@@ -75,6 +75,7 @@ SIGNATURES = {
     "fdmap_gpu_get_side_impedance": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_get_pml": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_get_side_displacement": (C.c_int, [_VP, C.c_int, C.c_int, _DP, _DP]),
+    "fdmap_gpu_get_energy": (C.c_int, [_VP, _DP]),
     "fdmap_gpu_get_displacement": (C.c_int, [_VP, _DP, _DP]),
     "fdmap_gpu_set_displacement": (C.c_int, [_VP, _DP, _DP]),
     "fdmap_gpu_get_peak": (C.c_int, [_VP, _DP, _DP]),

@@ -23,7 +23,10 @@ import numpy as np
 
 from .native import FAULT_INDEX
 
-OUT_FAULT, OUT_BODY, OUT_SIDE, OUT_SIDE_U = 0, 1, 2, 8
+OUT_FAULT, OUT_BODY, OUT_SIDE, OUT_ENERGY, OUT_SIDE_U = 0, 1, 2, 3, 8
+# Ebody / Eblock fields (get_field, domain.f90:517-523, 863-895): Etot, and the
+# dissipated energies and rates, zero in the reference (its boundary flux is a stub)
+ENERGY_ZERO = {"E", "EL", "ER", "EB", "ET", "DE", "DEL", "DER", "DEB", "DET"}
 # body displacement and peak motion (get_field, domain.f90:551-557)
 BODY_EXTRA = {"ux": 16, "uz": 16, "uy": 17, "pgv": 24, "pga": 25}
 # bndX locations (get_field, domain.f90:763-860): the hat variables by position
@@ -126,6 +129,17 @@ def configure_outputs(gpu, host, text: str, prefix: str | Path, ring_steps: int 
                         gpu.output_add(pn, OUT_FAULT, iface, FAULT_INDEX[f], q, q, 1, nmin=nmin, nmax=nmax,
                                        stride=it.stride)
                         names.append(pn)
+                continue
+            if loc == "Ebody" or loc.startswith("Eblock"):
+                idx = -1 if loc == "Ebody" else int(loc[6:]) - 1
+                if f == "Etot":
+                    fld = 0
+                elif f in ENERGY_ZERO and loc != "Ebody":
+                    fld = 1
+                else:
+                    raise ValueError(f"output field {f!r} is not available at {loc}")
+                gpu.output_add(nm, OUT_ENERGY, idx, fld, 1, 1, 1, nmin=nmin, nmax=nmax, stride=it.stride)
+                names.append(nm)
                 continue
             if loc.startswith("bnd"):
                 # bndXN: side X (L, R, B, T) of block N, every side node

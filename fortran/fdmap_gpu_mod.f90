@@ -88,6 +88,7 @@ module fdmap_gpu_mod
      real(c_double) :: hmin, hmax
      type(c_ptr) :: body          ! fdmap_body_t, or c_null_ptr: body arrays given by the host
      integer(c_int) :: displacement, peak  ! domain_list displacement, peak (F%displacement, F%peak)
+     integer(c_int) :: energy_balance      ! domain_list energy_balance (F%energy_balance)
   end type fdmap_desc_t
 
   ! on-device initialisation (fdmap_desc.h: fdmap_perturb, fdmap_block_body, fdmap_body)

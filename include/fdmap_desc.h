@@ -267,6 +267,11 @@ typedef struct fdmap_desc {
    * ground velocity and acceleration pgv, pga (nx,ny) updated in stage 1
    * (update_fields_peak, fields.f90:1136-1164) */
   int displacement, peak;
+  /* domain_list energy_balance: the mechanical energy of every block in stage
+   * 1 (energy_block, energy.f90:35-96); the boundary energy flux of the
+   * reference is a stub (energy_rates_boundary, energy.f90:219-236), so the
+   * dissipated energies stay zero */
+  int energy_balance;
 } fdmap_desc;
 
 #ifdef __cplusplus

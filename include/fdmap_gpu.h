@@ -92,6 +92,11 @@ int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out);
 int fdmap_gpu_get_pml(fdmap_gpu* h, int which, double* out);
 int fdmap_gpu_set_pml(fdmap_gpu* h, int which, const double* in);
 
+/* Mechanical energy E[nblocks + 1] of every block and their sum as of the
+ * last stage 1 (BF%Etot, F%Etot; domain_list energy_balance = T); 1e40
+ * before the first step, as the reference initialises it. */
+int fdmap_gpu_get_energy(fdmap_gpu* h, double* E);
+
 /* Body displacement U(nx,ny,nU) and its rate DU (F%U, F%DU; domain_list
  * displacement = T) and peak ground velocity / acceleration pgv, pga (nx,ny;
  * peak = T), global layout; any pointer may be NULL.  FDMAP_ERR_INVALID_ARG
@@ -135,12 +140,18 @@ int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
  *                    hat variable component 0..nF-1 or FDMAP_OUT_SIDE_U + c
  *                    for the boundary displacement component c (the bndX
  *                    locations, get_field, domain.f90:763-860), side nodes
- *                    mx..px (1-based along the side) step sx.
+ *                    mx..px (1-based along the side) step sx;
+ *   FDMAP_OUT_ENERGY: `index` = block (0-based) or -1 for the sum over
+ *                    blocks, `field` = 0 for the mechanical energy Etot, 1
+ *                    for the dissipated energies and their rates (E, EL..ET,
+ *                    DE, DEL..DET), which stay zero because the reference's
+ *                    boundary energy flux is a stub (energy.f90:219-236);
+ *                    one value per output step (Ebody / Eblock locations).
  * Items are added before fdmap_gpu_output_open; fdmap_gpu_output_flush
  * writes everything recorded so far, fdmap_gpu_output_close flushes and
  * releases the rings. */
-enum { FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1, FDMAP_OUT_SIDE = 2, FDMAP_OUT_SIDE_U = 8, FDMAP_OUT_BODY_U = 16,
-       FDMAP_OUT_BODY_PGV = 24, FDMAP_OUT_BODY_PGA = 25 };
+enum { FDMAP_OUT_FAULT = 0, FDMAP_OUT_BODY = 1, FDMAP_OUT_SIDE = 2, FDMAP_OUT_ENERGY = 3, FDMAP_OUT_SIDE_U = 8,
+       FDMAP_OUT_BODY_U = 16, FDMAP_OUT_BODY_PGV = 24, FDMAP_OUT_BODY_PGA = 25 };
 int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, int field, int mx, int px, int sx,
                          int my, int py, int sy, long long nmin, long long nmax, int stride);
 int fdmap_gpu_output_open(fdmap_gpu* h, const char* prefix, int ring_steps);

@@ -62,7 +62,7 @@ void fdmap_host_free(fdmap_domain* dom);
  * dbls[5]  = t0, dt, CFL, hmin, hmax */
 int fdmap_host_info(const fdmap_domain* dom, int* ints, double* dbls);
 
-/* Optional body fields: flags[2] = displacement, peak (domain_list). */
+/* Optional body fields: flags[3] = displacement, peak, energy_balance (domain_list). */
 int fdmap_host_body_flags(const fdmap_domain* dom, int* flags);
 
 /* Number of nodes p-m+1 of interface `iface` (0-based), or a negative code. */

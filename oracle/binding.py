@@ -36,6 +36,7 @@ def lib() -> C.CDLL:
         L.oracle_get_pml.argtypes = [C.c_void_p, C.c_int, _DP]
         L.oracle_get_side_u.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP, _DP]
         L.oracle_get_body_extras.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP]
+        L.oracle_get_energy.argtypes = [C.c_void_p, _DP]
         L.oracle_newton_failures.restype = C.c_longlong
         L.oracle_newton_failures.argtypes = [C.c_void_p]
         L.oracle_num_threads.restype = C.c_int
@@ -99,6 +100,13 @@ class OracleDomain:
         if lib().oracle_get_body_extras(self._o, _p(U), _p(DU), None, None):
             raise RuntimeError("the domain does not track the body displacement")
         return U, DU
+
+    def get_energy(self) -> np.ndarray:
+        """Mechanical energy of every block, then their sum (energy_balance = T)."""
+        E = np.empty(self.host.nblocks + 1)
+        if lib().oracle_get_energy(self._o, _p(E)):
+            raise RuntimeError("the domain does not track the energy")
+        return E
 
     def get_peak(self):
         """Peak ground velocity and acceleration, each (ny, nx)."""

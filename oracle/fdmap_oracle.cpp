@@ -30,6 +30,7 @@ struct Ops {
   double DL[6][9];  // DL(s,r) at [r][s]
   double AI[4];     // AI(s), s = 0..pI (artificial dissipation, symmetric)
   double AL[6][9];  // AL(s,r) at [r][s]; AR(-s,-r) = AL(s,r) (fd_coeff.f90:244)
+  double HL[6];     // diagonal norm near the boundary, HR(-i) = HL(i) (fd_coeff.f90:79-245)
 };
 
 bool make_ops(int method, Ops* o) {
@@ -37,6 +38,7 @@ bool make_ops(int method, Ops* o) {
   if (method == FDMAP_SBP2) {
     o->nbnd = 2; o->nbst = 1; o->pI = 1;
     o->DI[1] = 0.5;
+    o->HL[0] = 0.5;
     o->DL[0][0] = -1.0; o->DL[0][1] = 1.0;
     o->AI[0] = -1.0; o->AI[1] = 0.5;
     o->AL[0][0] = -1.0; o->AL[0][1] = 1.0;
@@ -45,6 +47,10 @@ bool make_ops(int method, Ops* o) {
   if (method == FDMAP_SBP4) {
     o->nbnd = 6; o->nbst = 4; o->pI = 2;
     o->DI[1] = 0.666666666666667; o->DI[2] = -0.083333333333333;
+    {
+      const double hl[4] = {0.354166666666667, 1.229166666666667, 0.895833333333333, 1.020833333333333};
+      for (int r = 0; r < 4; ++r) o->HL[r] = hl[r];
+    }
     double t[4][6] = {{-1.411764705882353, 1.735294117647059, -0.235294117647059, -0.088235294117647, 0.0, 0.0},
                       {-0.5, 0.0, 0.5, 0.0, 0.0, 0.0},
                       {0.093023255813953, -0.686046511627907, 0.0, 0.686046511627907, -0.093023255813953, 0.0},
@@ -61,6 +67,11 @@ bool make_ops(int method, Ops* o) {
   if (method == FDMAP_SBP6) {
     o->nbnd = 9; o->nbst = 6; o->pI = 3;
     o->DI[1] = 0.75; o->DI[2] = -0.15; o->DI[3] = 0.016666666666667;
+    {
+      const double hl[6] = {0.315949074074074, 1.390393518518518, 0.627546296296296,
+                            1.240509259259259, 0.911689814814815, 1.013912037037037};
+      for (int r = 0; r < 6; ++r) o->HL[r] = hl[r];
+    }
     double t[6][9] = {
         {-1.582533518939116, 2.033378678700676, -0.141512858744873, -0.450398306578272, 0.104488069284042, 0.036577936277544, 0, 0, 0},
         {-0.462059195631158, 0.0, 0.287258622978251, 0.258816087376832, -0.069112065532624, -0.014903449191300, 0, 0, 0},
@@ -180,6 +191,8 @@ struct oracle_domain {
   vec Wx, DWx, Wy, DWy;  // PML fields (nx,ny,nF), allocated when some block has pmlx / pmly (fields.f90:203-210)
   vec U, DU;             // body displacement and its rate (nx,ny,nU), displacement = T (fields.f90:183-186)
   vec pgv, pga;          // peak ground velocity / acceleration (nx,ny), peak = T (fields.f90:187-190)
+  bool energy = false;   // energy_balance = T: stage-1 mechanical energy of every block (energy.f90:9-96)
+  std::vector<double> Etot;  // per block, then the sum over blocks
   fdmap_source src;
   // forcing from file (source.f90:12-14): the frames of the current step and its window
   std::FILE* frc = nullptr;
@@ -1304,6 +1317,51 @@ void singular_source(int i, int i0, double h, double a, double& d) {
 // set_source (source.f90:147-252) for one block; point source and gravity
 void point_source(oracle_domain& D, const Blk& B, double t, double pi);
 
+// diagonal SBP norm with unit spacing over a block's n nodes (Hnorm, fd.f90:14-39)
+double hnorm(const Ops& op, int n, int k) {
+  if (k < op.nbst) return op.HL[k];
+  if (k > n - 1 - op.nbst) return op.HL[n - 1 - k];
+  return 1.0;
+}
+
+// energy_block / energy_interior (energy.f90:9-96): the block's homogeneous
+// material, the step-start fields, the Jacobian and the norm in both directions
+void energy_interior(oracle_domain& D) {
+  const size_t NN = (size_t)D.nx * D.ny;
+  const vec& F = D.F;
+  double Esum = 0.0;
+  for (int b = 0; b < D.nblocks; ++b) {
+    const Blk& B = D.blk[b];
+    const int nxb = B.pgx - B.mgx + 1, nyb = B.pgy - B.mgy + 1;
+    double E = 0.0;
+    if (D.mode == 2) {
+      const double lambda = B.M - 2.0 * B.G;
+      const double v1 = 0.5 * B.rho, v2 = 0.5 * B.G, v3 = 0.25 * B.G;
+      const double v4 = -0.25 * B.G * (lambda / (3.0 * lambda + 2.0 * B.G));
+      for (int j = B.mgy; j <= B.pgy; ++j)
+        for (int i = B.mgx; i <= B.pgx; ++i) {
+          const size_t g = G2(D, i, j);
+          const double f1 = F[g], f2 = F[g + NN], f3 = F[g + 2 * NN], f4 = F[g + 3 * NN], f5 = F[g + 4 * NN],
+                       f6 = F[g + 5 * NN];
+          E = E + hnorm(D.op, nxb, i - B.mgx) * hnorm(D.op, nyb, j - B.mgy) * D.J[g] *
+                      (v1 * (f1 * f1 + f2 * f2) + v2 * (f4 * f4) + v3 * (f3 * f3 + f5 * f5 + f6 * f6) +
+                       v4 * ((f3 + f5 + f6) * (f3 + f5 + f6)));
+        }
+    } else {
+      for (int j = B.mgy; j <= B.pgy; ++j)
+        for (int i = B.mgx; i <= B.pgx; ++i) {
+          const size_t g = G2(D, i, j);
+          const double f1 = F[g], f2 = F[g + NN], f3 = F[g + 2 * NN];
+          E = E + 0.5 * D.J[g] * (B.rho * (f1 * f1) + (f2 * f2 + f3 * f3) / B.G) * hnorm(D.op, nxb, i - B.mgx) *
+                      hnorm(D.op, nyb, j - B.mgy);
+        }
+    }
+    D.Etot[b] = E;
+    Esum = Esum + E;
+  }
+  D.Etot[D.nblocks] = Esum;
+}
+
 void set_source(oracle_domain& D, const Blk& B, double t) {
   const fdmap_source& S = D.src;
   size_t NN = (size_t)D.nx * D.ny;
@@ -1486,6 +1544,8 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
     o->pgv.assign(NN, 0.0);
     o->pga.assign(NN, 0.0);
   }
+  o->energy = d->energy_balance != 0;
+  o->Etot.assign((size_t)d->nblocks + 1, 1e40);  // BF%Etot = 1d40 until the first stage 1
   if (d->src.forcing_filename) {
     // init_forcing_from_file (source.f90:409-448): frame 0 into the new frame
     o->frc = std::fopen(d->src.forcing_filename, "rb");
@@ -1587,6 +1647,7 @@ int oracle_time_step(oracle_domain* o, double t0, double dt, int final_step) {
     prepare_edges(D);
     enforce_edge_conditions(D, D.rk.B[stage - 1] * dt);
     set_rates_all(D);
+    if (stage == 1 && D.energy) energy_interior(D);
     if (stage == 1 && !D.pgv.empty()) {
       // update_fields_peak (fields.f90:1136-1164), stage 1 only
       const size_t NN = (size_t)D.nx * D.ny;
@@ -1666,6 +1727,13 @@ int oracle_get_side_u(const oracle_domain* o, int b, int s, double* U, double* D
   const Side& S = o->blk[b].side[s];
   if (U) std::copy(S.U.begin(), S.U.end(), U);
   if (DU) std::copy(S.DU.begin(), S.DU.end(), DU);
+  return 0;
+}
+
+// mechanical energy of every block and their sum, as of the last stage 1 (energy_balance = T)
+int oracle_get_energy(const oracle_domain* o, double* E) {
+  if (!o || !E || !o->energy) return -1;
+  std::copy(o->Etot.begin(), o->Etot.end(), E);
   return 0;
 }
 

@@ -63,6 +63,10 @@ int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out);
  * any pointer may be NULL; -1 when the domain does not track them. */
 int oracle_get_body_extras(const oracle_domain* o, double* U, double* DU, double* pgv, double* pga);
 
+/* Mechanical energy E[nblocks + 1] (every block, then the sum) of the last
+ * stage 1 with energy_balance = T; -1 when the domain does not track it. */
+int oracle_get_energy(const oracle_domain* o, double* E);
+
 /* Boundary displacement U and rate DU of side s (0..3) of block b: (n, nU) each. */
 int oracle_get_side_u(const oracle_domain* o, int b, int s, double* U, double* DU);
 

@@ -76,12 +76,9 @@ def test_rejects_unsupported_features():
     assert e.value.code == -6
     with pytest.raises(FdmapError):
         init_domain(problems.antiplane_pulse(n=21, L=2.0, nt=3).replace("absorbing", "bogus", 1))
-    with pytest.raises(FdmapError, match="energy_balance"):
-        init_domain(problems.antiplane_pulse(n=21, L=2.0, nt=3).replace("&domain_list mode=3",
-                                                                        "&domain_list mode=3, energy_balance=T"))
-    h = init_domain(problems.antiplane_pulse(n=21, L=2.0, nt=3).replace("&domain_list mode=3",
-                                                                        "&domain_list mode=3, displacement=T, peak=T"))
-    assert h.displacement and h.peak
+    h = init_domain(problems.antiplane_pulse(n=21, L=2.0, nt=3).replace(
+        "&domain_list mode=3", "&domain_list mode=3, displacement=T, peak=T, energy_balance=T"))
+    assert h.displacement and h.peak and h.energy_balance
 
 
 def test_missing_block_marker():
