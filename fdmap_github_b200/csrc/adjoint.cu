@@ -1,8 +1,15 @@
 // Forward/backward pair for gradients of a receiver-seismogram misfit with
 // respect to the density and shear-modulus fields of a heterogeneous mode III
-// block (SBP-SAT wave solve, LS-RK time stepping).  The reference has no
+// domain (SBP-SAT wave solve, LS-RK time stepping) and, with frictional
+// interfaces, the shear prestress of every fault node.  The reference has no
 // adjoint; the forward pass is the engine's own time step (time_step_LS,
 // time_step.f90:71-167), so the misfit is that of the production path.
+//
+// One block without interfaces takes the tiled path (adj_stage_tma beside
+// adj_band_kernel); several blocks or interfaces take the general path: every
+// block's nodes by adj_block_kernel, then the fault nodes by adj_fault_kernel
+// (adjoint_fault.cuh), with the state variable of each fault node stored
+// beside the fields at every stage and the fault registers in every checkpoint.
 //
 //   forward : steps 1..nt-1 as replayed graphs; vz sampled at the receivers at
 //             every step start (n = 1..nt, the reference's stage-1 output
@@ -23,6 +30,7 @@
 #include <string>
 #include <vector>
 
+#include "adjoint_fault.cuh"
 #include "adjoint_kernel.cuh"
 #include "engine.h"
 #include "fdmap_gpu.h"
@@ -57,7 +65,25 @@ struct fdmap_adjoint {
   double* qp[2] = {nullptr, nullptr};
   double* grho = nullptr;
   double* gG = nullptr;
-  double* geo[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<double*> geo;          // edge geometry factors, 4 sides per block
+  // general path (several blocks or interfaces)
+  bool general = false;
+  int nb = 1;
+  long long boff[MAX_BLOCKS] = {};   // block offsets in the concatenated 3-plane layout
+  long long goff[MAX_BLOCKS] = {};   // and in the concatenated gradient planes
+  long long total = 0;               // 3-plane layout doubles of all blocks
+  long long gtotal = 0;              // gradient-plane doubles of all blocks
+  int nfault = 0;                    // fault nodes of all interfaces
+  std::vector<AdjIfaceInfo> info_host;
+  AdjIfaceInfo* info = nullptr;
+  std::vector<long long> st_off;     // fault-register offset of each frictional interface in a checkpoint
+  long long st_total = 0;
+  double* init_st = nullptr;
+  double* psib = nullptr;            // Psibar, qbar'_Psi, dJ/dS0 per fault node
+  double* qpsib = nullptr;
+  double* gS0 = nullptr;
+  const double** recp[2] = {nullptr, nullptr};  // per receiver: vz in F[parity]
+  std::vector<std::pair<int, long long>> rec_gen;  // (block, local index) per receiver
   double* traces = nullptr;          // N*nrec
   double* resid = nullptr;           // N*nrec
   int trace_alloc = 0;
@@ -65,10 +91,12 @@ struct fdmap_adjoint {
   bool have_resid = false;
   // graphs: forward step (by F parity), recompute step (by F parity), adjoint step (by ubar parity)
   cudaGraphExec_t g_fwd[2] = {nullptr, nullptr}, g_rec[2] = {nullptr, nullptr}, g_adj[2] = {nullptr, nullptr};
-  double graph_dt = -1.0;
+  double graph_dt = -1.0, graph_t0 = 0.0;
   std::vector<void*> mem;
 
   long long stride() const { return 3 * h->hdom.blk[0].plane; }
+  long long slot_stride() const { return general ? total + nfault : stride(); }
+  long long ckpt_stride() const { return general ? total + st_total : stride(); }
   void free_graphs() {
     for (auto* set : {g_fwd, g_rec, g_adj})
       for (int q = 0; q < 2; ++q)
@@ -185,17 +213,27 @@ int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p, int q) {
 // forward stage sequence of one step from buffer `cur` (the engine's time_step_LS body)
 int forward_step_stages(fdmap_adjoint* a, int cur, double dt, bool stash) {
   fdmap_gpu* h = a->h;
-  const DevBlock& B = h->hdom.blk[0];
+  const long long slot = a->slot_stride();
   for (int s = 0; s < h->rk.nstage; ++s) {
     if (stash) {
       // the stage only reads F[cur]; the copy of it runs beside the stage and
       // joins before the next stage overwrites that buffer
       if (s > 0) CUDA_TRY(cudaStreamWaitEvent(h->stream, a->ev_cjoin, 0));
+      if (a->nfault > 0) {
+        // the stage updates Psi in place: its copy goes first, on the stage's stream
+        adj_stash_psi<<<(a->nfault + 127) / 128, 128, 0, h->stream>>>(
+            h->hdom, a->info, (int)a->info_host.size(), a->nfault, a->store, slot, a->total, &a->clock->rel, s,
+            h->rk.nstage);
+        CUDA_TRY(cudaGetLastError());
+      }
       CUDA_TRY(cudaEventRecord(a->ev_cfork, h->stream));
       CUDA_TRY(cudaStreamWaitEvent(a->copy, a->ev_cfork, 0));
-      adj_stash<<<296, 256, 0, a->copy>>>(B.F[cur], a->store, a->stride(), &a->clock->rel, s, h->rk.nstage,
-                                          a->stride());
-      CUDA_TRY(cudaGetLastError());
+      for (int b = 0; b < a->nb; ++b) {
+        const DevBlock& B = h->hdom.blk[b];
+        adj_stash<<<296, 256, 0, a->copy>>>(B.F[cur], a->store + a->boff[b], slot, &a->clock->rel, s, h->rk.nstage,
+                                            3 * B.plane);
+        CUDA_TRY(cudaGetLastError());
+      }
       CUDA_TRY(cudaEventRecord(a->ev_cjoin, a->copy));
     }
     StageArgs st{};
@@ -230,6 +268,65 @@ int capture(fdmap_adjoint* a, cudaGraphExec_t* out, const std::function<int()>& 
   return rc;
 }
 
+// one adjoint stage of the general path: every block, then the fault nodes
+int gen_stage_launch(fdmap_adjoint* a, int s, double dt, int q) {
+  fdmap_gpu* h = a->h;
+  for (int b = 0; b < a->nb; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    AdjStage p{};
+    p.A = h->rk.A[s];
+    p.Bdt = h->rk.B[s] * dt;
+    p.s = s;
+    p.nstage = h->rk.nstage;
+    p.ub_in = a->ub[q] + a->boff[b];
+    p.qp_in = a->qp[q] + a->boff[b];
+    p.ub_out = a->ub[1 - q] + a->boff[b];
+    p.qp_out = a->qp[1 - q] + a->boff[b];
+    p.store = a->store + a->boff[b];
+    p.stride = a->slot_stride();
+    p.rel = &a->clock->rel;
+    p.grho = a->grho + a->goff[b];
+    p.gG = a->gG + a->goff[b];
+    p.blk = b;
+    const int grid = (int)(((long long)B.nx * B.ny + 127) / 128);
+    if (h->pI == 1) adj_block_kernel<1><<<grid, 128, 0, h->stream>>>(h->hdom, p);
+    else if (h->pI == 2) adj_block_kernel<2><<<grid, 128, 0, h->stream>>>(h->hdom, p);
+    else adj_block_kernel<3><<<grid, 128, 0, h->stream>>>(h->hdom, p);
+    CUDA_TRY(cudaGetLastError());
+  }
+  if (a->nfault == 0) return FDMAP_OK;
+  AdjFaultArgs f{};
+  f.A = h->rk.A[s];
+  f.Bdt = h->rk.B[s] * dt;
+  f.C = h->rk.C[s];
+  f.t_start = a->t_start;
+  f.dt = dt;
+  f.s = s;
+  f.nstage = h->rk.nstage;
+  f.ub_in = a->ub[q];
+  f.qp_in = a->qp[q];
+  f.ub_out = a->ub[1 - q];
+  f.store = a->store;
+  f.slot_stride = a->slot_stride();
+  f.psi_off = a->total;
+  f.ck = a->clock;
+  f.psib = a->psib;
+  f.qpsib = a->qpsib;
+  f.grho = a->grho;
+  f.gG = a->gG;
+  f.gS0 = a->gS0;
+  f.info = a->info;
+  f.nifc = (int)a->info_host.size();
+  f.nfault = a->nfault;
+  for (int b = 0; b < a->nb; ++b) {
+    f.boff[b] = a->boff[b];
+    f.goff[b] = a->goff[b];
+  }
+  adj_fault_kernel<<<(a->nfault + 63) / 64, 64, 0, h->stream>>>(h->hdom, f);
+  CUDA_TRY(cudaGetLastError());
+  return FDMAP_OK;
+}
+
 int build_graphs(fdmap_adjoint* a, double dt) {
   a->free_graphs();
   fdmap_gpu* h = a->h;
@@ -242,7 +339,12 @@ int build_graphs(fdmap_adjoint* a, double dt) {
       int r = forward_step_stages(a, c, dt, false);
       if (r) return r;
       const int last = (h->rk.nstage & 1) ? 1 - c : c;  // buffer holding the new state
-      adj_sample_advance<<<1, 128, 0, h->stream>>>(B.F[last], a->rec, a->nrec, h->d_time, a->traces, a->trace_alloc);
+      if (a->general)
+        adj_sample_advance_ptr<<<1, 128, 0, h->stream>>>(a->recp[last], a->nrec, h->d_time, a->traces,
+                                                         a->trace_alloc);
+      else
+        adj_sample_advance<<<1, 128, 0, h->stream>>>(B.F[last], a->rec, a->nrec, h->d_time, a->traces,
+                                                     a->trace_alloc);
       return (int)FDMAP_OK;
     });
     if (rc) break;
@@ -257,7 +359,12 @@ int build_graphs(fdmap_adjoint* a, double dt) {
     // adjoint step: stages in reverse from ubar parity c, then the residual at this step start
     rc = capture(a, &a->g_adj[c], [&]() -> int {
       int q = c;
-      for (int s = h->rk.nstage - 1; s >= 0; --s) {
+      for (int s = h->rk.nstage - 1; s >= 0 && a->general; --s) {
+        int r = gen_stage_launch(a, s, dt, q);
+        if (r) return r;
+        q = 1 - q;
+      }
+      for (int s = h->rk.nstage - 1; s >= 0 && !a->general; --s) {
         AdjStage p{};
         p.A = h->rk.A[s];
         p.Bdt = h->rk.B[s] * dt;
@@ -287,14 +394,14 @@ int build_graphs(fdmap_adjoint* a, double dt) {
 }
 
 // global (nx, ny) plane -> device block plane and back
-int to_block(fdmap_adjoint* a, double* dst, const double* src) {
+int to_block(fdmap_adjoint* a, double* dst, const double* src, int b = 0) {
   fdmap_gpu* h = a->h;
-  return h->upload_plane(dst, src, h->geom[0]);
+  return h->upload_plane(dst, src, h->geom[b]);
 }
 
-int from_block(fdmap_adjoint* a, double* dst, const double* src) {
+int from_block(fdmap_adjoint* a, double* dst, const double* src, int b = 0) {
   fdmap_gpu* h = a->h;
-  const BlockGeom& g = h->geom[0];
+  const BlockGeom& g = h->geom[b];
   std::vector<double> tmp((size_t)g.plane);
   CUDA_TRY(cudaMemcpy(tmp.data(), src, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost));
   for (int j = 0; j < g.ny; ++j)
@@ -316,11 +423,41 @@ int ensure_trace_buffers(fdmap_adjoint* a, int N) {
   return FDMAP_OK;
 }
 
+// fields of every block into F[0] (and, given `st`, the fault registers)
+// from a checkpoint layout: blocks at boff, fault registers after them
+int restore_state(fdmap_adjoint* a, const double* src, const double* st) {
+  fdmap_gpu* h = a->h;
+  for (int b = 0; b < a->nb; ++b)
+    CUDA_TRY(cudaMemcpyAsync(h->hdom.blk[b].F[0], src + a->boff[b], 3 * h->hdom.blk[b].plane * sizeof(double),
+                             cudaMemcpyDeviceToDevice, h->stream));
+  for (size_t i = 0; i < a->st_off.size(); ++i) {
+    if (a->st_off[i] < 0) continue;
+    const double* from = st ? st + (a->st_off[i] - a->total) : src + a->st_off[i];
+    CUDA_TRY(cudaMemcpyAsync(h->hdom.ifc[i].fr.st, from, (size_t)FDMAP_FAULT_NFIELDS * h->hdom.ifc[i].n * sizeof(double),
+                             cudaMemcpyDeviceToDevice, h->stream));
+  }
+  return FDMAP_OK;
+}
+
+int save_state(fdmap_adjoint* a, double* dst) {
+  fdmap_gpu* h = a->h;
+  for (int b = 0; b < a->nb; ++b)
+    CUDA_TRY(cudaMemcpyAsync(dst + a->boff[b], h->hdom.blk[b].F[h->cur], 3 * h->hdom.blk[b].plane * sizeof(double),
+                             cudaMemcpyDeviceToDevice, h->stream));
+  for (size_t i = 0; i < a->st_off.size(); ++i) {
+    if (a->st_off[i] < 0) continue;
+    CUDA_TRY(cudaMemcpyAsync(dst + a->st_off[i], h->hdom.ifc[i].fr.st,
+                             (size_t)FDMAP_FAULT_NFIELDS * h->hdom.ifc[i].n * sizeof(double), cudaMemcpyDeviceToDevice,
+                             h->stream));
+  }
+  return FDMAP_OK;
+}
+
 int ensure_checkpoints(fdmap_adjoint* a, int nck) {
   if (nck <= a->nckpt_alloc) return FDMAP_OK;
   a->release(a->ckpt);
   a->ckpt = nullptr;
-  int rc = a->alloc(&a->ckpt, (size_t)nck * a->stride());
+  int rc = a->alloc(&a->ckpt, (size_t)nck * a->ckpt_stride());
   if (rc) return rc;
   a->nckpt_alloc = nck;
   return FDMAP_OK;
@@ -335,18 +472,40 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
   if (!out) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint pointer");
   *out = nullptr;
   if (!d) return set_err(FDMAP_ERR_INVALID_ARG, "null descriptor");
-  if (d->mode != 3 || d->nblocks != 1 || d->nifaces != 0 || !d->heterogeneous)
-    return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers one heterogeneous mode III block without interfaces");
+  if (d->mode != 3 || !d->heterogeneous)
+    return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers heterogeneous mode III domains");
   if (d->displacement || d->peak || d->energy_balance)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint does not track displacement or peak motion");
   if (d->src.gauss_forcing || d->src.forcing_filename)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers the point source only");
   if (d->body)  // the edge-impedance derivatives are formed from the host's metric arrays
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint needs the body arrays on the host");
-  for (int s = 0; s < 4; ++s) {
-    int bc = d->blocks[0].side[s].bc;
-    if (bc != FDMAP_BC_ABSORBING && bc != FDMAP_BC_FREE && bc != FDMAP_BC_RIGID)
-      return set_err(FDMAP_ERR_UNSUPPORTED, "adjoint sides must be absorbing, free or rigid");
+  for (int b = 0; b < d->nblocks; ++b)
+    for (int s = 0; s < 4; ++s) {
+      const int bc = d->blocks[b].side[s].bc;
+      if (bc == FDMAP_BC_NONE) {
+        // an interface side must be covered by interfaces over its whole length
+        const int len = s < 2 ? d->blocks[b].pgy - d->blocks[b].mgy + 1 : d->blocks[b].pgx - d->blocks[b].mgx + 1;
+        int cov = 0;
+        for (int i = 0; i < d->nifaces; ++i) {
+          const fdmap_iface& fi = d->ifaces[i];
+          const int sm = fi.direction == 0 ? 1 : 3, sp = fi.direction == 0 ? 0 : 2;
+          if ((fi.iblockm == b && sm == s) || (fi.iblockp == b && sp == s)) cov += fi.p - fi.m + 1;
+        }
+        if (cov != len) return set_err(FDMAP_ERR_UNSUPPORTED, "adjoint: a side without a boundary condition is not an interface");
+      } else if (bc != FDMAP_BC_ABSORBING && bc != FDMAP_BC_FREE && bc != FDMAP_BC_RIGID) {
+        return set_err(FDMAP_ERR_UNSUPPORTED, "adjoint sides must be absorbing, free or rigid");
+      }
+    }
+  for (int i = 0; i < d->nifaces; ++i) {
+    const fdmap_iface& fi = d->ifaces[i];
+    if (fi.coupling == FDMAP_COUPLING_LOCKED) continue;
+    const fdmap_friction& fr = fi.fr;
+    // the smooth laws: the slip-weakening kink has no derivative
+    if (fr.law == FDMAP_FR_SW)
+      return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers locked and rate-and-state interfaces, not slip weakening");
+    if (fr.force || fr.reg)
+      return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint does not cover forced rupture or regularised normal stress");
   }
   if (nrec < 1 || !rec_i || !rec_j) return set_err(FDMAP_ERR_INVALID_ARG, "receivers required");
   if (checkpoint_every < 1) return set_err(FDMAP_ERR_INVALID_ARG, "checkpoint interval must be positive");
@@ -363,11 +522,34 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
   fdmap_gpu* h = a->h;
   a->K = checkpoint_every;
   a->nrec = nrec;
+  a->general = d->nblocks > 1 || d->nifaces > 0;
+  a->nb = d->nblocks;
   const BlockGeom& g = h->geom[0];
   const int nbnd = h->hdom.nbnd;
-  if (g.nx < 2 * nbnd + 1 || g.ny < 2 * nbnd + 1)
-    return fail(set_err(FDMAP_ERR_UNSUPPORTED, "block too small for the adjoint band decomposition"));
+  for (int b = 0; b < a->nb; ++b) {
+    const BlockGeom& gb = h->geom[b];
+    if (gb.nx < 2 * nbnd + 1 || gb.ny < 2 * nbnd + 1)
+      return fail(set_err(FDMAP_ERR_UNSUPPORTED, "block too small for the adjoint band decomposition"));
+    a->boff[b] = a->total;
+    a->goff[b] = a->gtotal;
+    a->total += 3 * gb.plane;
+    a->gtotal += gb.plane;
+  }
   a->nband = 2LL * nbnd * g.nx + 2LL * nbnd * (g.ny - 2 * nbnd);
+  for (int i = 0; i < d->nifaces; ++i) {
+    const fdmap_iface& fi = d->ifaces[i];
+    const int n = fi.p - fi.m + 1;
+    a->info_host.push_back(AdjIfaceInfo{i, a->nfault, nullptr, nullptr});
+    a->nfault += n;
+    if (fi.coupling == FDMAP_COUPLING_LOCKED) {
+      a->st_off.push_back(-1);
+    } else {
+      a->st_off.push_back(a->total + a->st_total);
+      a->st_total += (long long)FDMAP_FAULT_NFIELDS * n;
+      // the background shear stress term is always read, so the prestress can be set
+      h->hdom.ifc[i].fr.has_bsS0 = 1;
+    }
+  }
   {
     int lo = 0, hi = 0;
     if (cudaDeviceGetStreamPriorityRange(&lo, &hi) != cudaSuccess ||
@@ -380,16 +562,35 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
       return fail(set_err(FDMAP_ERR_CUDA, "adjoint stream setup"));
   }
   for (int r = 0; r < nrec; ++r) {
-    int i = rec_i[r] - g.mgx, j = rec_j[r] - g.mgy;
-    if (i < 0 || i >= g.nx || j < 0 || j >= g.ny) return fail(set_err(FDMAP_ERR_INVALID_ARG, "receiver outside the block"));
-    a->rec_host.push_back((long long)j * g.pitch + i);
+    int b = 0;
+    while (b < a->nb && !(rec_i[r] >= h->geom[b].mgx && rec_i[r] < h->geom[b].mgx + h->geom[b].nx &&
+                          rec_j[r] >= h->geom[b].mgy && rec_j[r] < h->geom[b].mgy + h->geom[b].ny))
+      ++b;
+    if (b == a->nb) return fail(set_err(FDMAP_ERR_INVALID_ARG, "receiver outside the domain"));
+    const BlockGeom& gb = h->geom[b];
+    const long long local = (long long)(rec_j[r] - gb.mgy) * gb.pitch + (rec_i[r] - gb.mgx);
+    a->rec_host.push_back(a->boff[b] + local);  // vz of the node in the concatenated layout
+    a->rec_gen.push_back({b, local});
   }
-  const long long S = a->stride();
+  const long long S = a->total;
   if ((rc = a->alloc(&a->rec, nrec)) || (rc = a->alloc(&a->init_F, S)) || (rc = a->alloc(&a->init_DF, S)) ||
-      (rc = a->alloc(&a->store, (size_t)a->K * h->rk.nstage * S)) || (rc = a->alloc(&a->ub[0], S)) ||
+      (rc = a->alloc(&a->store, (size_t)a->K * h->rk.nstage * a->slot_stride())) || (rc = a->alloc(&a->ub[0], S)) ||
       (rc = a->alloc(&a->ub[1], S)) || (rc = a->alloc(&a->qp[0], S)) || (rc = a->alloc(&a->qp[1], S)) ||
-      (rc = a->alloc(&a->grho, g.plane)) || (rc = a->alloc(&a->gG, g.plane)) || (rc = a->alloc(&a->clock, 1)))
+      (rc = a->alloc(&a->grho, a->gtotal)) || (rc = a->alloc(&a->gG, a->gtotal)) || (rc = a->alloc(&a->clock, 1)))
     return fail(rc);
+  if (a->general) {
+    if ((rc = a->alloc(&a->init_st, std::max<long long>(a->st_total, 1))) ||
+        (rc = a->alloc(&a->psib, std::max(a->nfault, 1))) || (rc = a->alloc(&a->qpsib, std::max(a->nfault, 1))) ||
+        (rc = a->alloc(&a->gS0, std::max(a->nfault, 1))) || (rc = a->alloc(&a->recp[0], nrec)) ||
+        (rc = a->alloc(&a->recp[1], nrec)))
+      return fail(rc);
+    for (int c = 0; c < 2; ++c) {
+      std::vector<const double*> ptr(nrec);
+      for (int r = 0; r < nrec; ++r) ptr[r] = h->hdom.blk[a->rec_gen[r].first].F[c] + a->rec_gen[r].second;
+      if (cudaMemcpy(a->recp[c], ptr.data(), nrec * sizeof(double*), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(set_err(FDMAP_ERR_CUDA, "receiver upload"));
+    }
+  }
   if (cudaMemcpy(a->rec, a->rec_host.data(), nrec * sizeof(long long), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(set_err(FDMAP_ERR_CUDA, "receiver upload"));
   {
@@ -415,33 +616,57 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
         cudaMemcpy(a->rlist, rlist.data(), rlist.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(set_err(FDMAP_ERR_CUDA, "receiver upload"));
   }
-  const DevBlock& B = h->hdom.blk[0];
-  if (cudaMemcpy(a->init_F, B.F[h->cur], S * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess ||
-      cudaMemcpy(a->init_DF, B.DF, S * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess)
-    return fail(set_err(FDMAP_ERR_CUDA, "initial state copy"));
+  for (int b = 0; b < a->nb; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    if (cudaMemcpy(a->init_F + a->boff[b], B.F[h->cur], 3 * B.plane * sizeof(double), cudaMemcpyDeviceToDevice) !=
+            cudaSuccess ||
+        cudaMemcpy(a->init_DF + a->boff[b], B.DF, 3 * B.plane * sizeof(double), cudaMemcpyDeviceToDevice) !=
+            cudaSuccess)
+      return fail(set_err(FDMAP_ERR_CUDA, "initial state copy"));
+  }
+  for (int i = 0; i < d->nifaces; ++i)
+    if (a->st_off[i] >= 0 &&
+        cudaMemcpy(a->init_st + (a->st_off[i] - a->total), h->hdom.ifc[i].fr.st,
+                   (size_t)FDMAP_FAULT_NFIELDS * h->hdom.ifc[i].n * sizeof(double), cudaMemcpyDeviceToDevice) != cudaSuccess)
+      return fail(set_err(FDMAP_ERR_CUDA, "initial fault state copy"));
   // edge geometry factors H00i*|grad|/J (init_edges, domain.f90:1349-1459)
   SbpOperator op;
   sbp_operator(d->fd_method, &op);
-  const fdmap_block& fb = d->blocks[0];
-  for (int s = 0; s < 4; ++s) {
-    const int n = (s < 2) ? g.ny : g.nx;
-    std::vector<double> geo(n);
-    for (int k = 0; k < n; ++k) {
-      int i, j;
-      if (s == 0) { i = fb.mgx; j = fb.mgy + k; }
-      else if (s == 1) { i = fb.pgx; j = fb.mgy + k; }
-      else if (s == 2) { i = fb.mgx + k; j = fb.mgy; }
-      else { i = fb.mgx + k; j = fb.pgy; }
-      const size_t q = (size_t)(i - 1) + (size_t)d->nx * (size_t)(j - 1);
-      const double mag = (s < 2) ? std::sqrt(d->xr[q] * d->xr[q] + d->yr[q] * d->yr[q])
-                                 : std::sqrt(d->xq[q] * d->xq[q] + d->yq[q] * d->yq[q]);
-      geo[k] = op.H00i * mag / d->J[q];
+  a->geo.assign(4 * a->nb, nullptr);
+  for (int b = 0; b < a->nb; ++b) {
+    const fdmap_block& fb = d->blocks[b];
+    const BlockGeom& gb = h->geom[b];
+    for (int s = 0; s < 4; ++s) {
+      const int n = (s < 2) ? gb.ny : gb.nx;
+      std::vector<double> geo(n);
+      for (int k = 0; k < n; ++k) {
+        int i, j;
+        if (s == 0) { i = fb.mgx; j = fb.mgy + k; }
+        else if (s == 1) { i = fb.pgx; j = fb.mgy + k; }
+        else if (s == 2) { i = fb.mgx + k; j = fb.mgy; }
+        else { i = fb.mgx + k; j = fb.pgy; }
+        const size_t q = (size_t)(i - 1) + (size_t)d->nx * (size_t)(j - 1);
+        const double mag = (s < 2) ? std::sqrt(d->xr[q] * d->xr[q] + d->yr[q] * d->yr[q])
+                                   : std::sqrt(d->xq[q] * d->xq[q] + d->yq[q] * d->yq[q]);
+        geo[k] = op.H00i * mag / d->J[q];
+      }
+      if ((rc = a->alloc(&a->geo[4 * b + s], n))) return fail(rc);
+      if (cudaMemcpy(a->geo[4 * b + s], geo.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(set_err(FDMAP_ERR_CUDA, "geometry upload"));
     }
-    if ((rc = a->alloc(&a->geo[s], n))) return fail(rc);
-    if (cudaMemcpy(a->geo[s], geo.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
-      return fail(set_err(FDMAP_ERR_CUDA, "geometry upload"));
   }
-  if ((rc = adj_maps(a))) return fail(rc);
+  if (a->general && !a->info_host.empty()) {
+    for (auto& inf : a->info_host) {
+      const DevIface& I = h->hdom.ifc[inf.iface];
+      inf.geom = a->geo[4 * I.im + (I.direction == 0 ? 1 : 3)];
+      inf.geop = a->geo[4 * I.ip + (I.direction == 0 ? 0 : 2)];
+    }
+    if ((rc = a->alloc(&a->info, a->info_host.size()))) return fail(rc);
+    if (cudaMemcpy(a->info, a->info_host.data(), a->info_host.size() * sizeof(AdjIfaceInfo), cudaMemcpyHostToDevice) !=
+        cudaSuccess)
+      return fail(set_err(FDMAP_ERR_CUDA, "interface table upload"));
+  }
+  if (!a->general && (rc = adj_maps(a))) return fail(rc);
   *out = a;
   return FDMAP_OK;
 }
@@ -454,15 +679,27 @@ int fdmap_gpu_adjoint_set_material(fdmap_adjoint* a, const double* rho, const do
   const BlockGeom& g = h->geom[0];
   for (size_t q = 0; q < (size_t)h->nx_g * h->ny_g; ++q)
     if (!(rho[q] > 0.0) || !(G[q] > 0.0)) return set_err(FDMAP_ERR_INVALID_ARG, "density and shear modulus must be positive");
-  DevBlock& B = h->hdom.blk[0];
   int rc;
-  if ((rc = to_block(a, B.rho, rho))) return rc;
-  if ((rc = to_block(a, B.G, G))) return rc;
-  for (int s = 0; s < 4; ++s) {
-    const DevSide& S = B.side[s];
-    adj_edge_material<<<(S.n + 127) / 128, 128, 0, h->stream>>>(S, B.rho, B.G, a->geo[s], s, g.nx, g.ny, g.pitch);
+  for (int b = 0; b < a->nb; ++b) {
+    DevBlock& B = h->hdom.blk[b];
+    const BlockGeom& gb = h->geom[b];
+    if ((rc = to_block(a, B.rho, rho, b))) return rc;
+    if ((rc = to_block(a, B.G, G, b))) return rc;
+    for (int s = 0; s < 4; ++s) {
+      const DevSide& S = B.side[s];
+      adj_edge_material<<<(S.n + 127) / 128, 128, 0, h->stream>>>(S, B.rho, B.G, a->geo[4 * b + s], s, gb.nx, gb.ny,
+                                                                  gb.pitch);
+      CUDA_TRY(cudaGetLastError());
+    }
+  }
+  for (auto& inf : a->info_host) {
+    const DevIface& I = h->hdom.ifc[inf.iface];
+    const DevSide& Sm = h->hdom.blk[I.im].side[I.direction == 0 ? 1 : 3];
+    const DevSide& Sp = h->hdom.blk[I.ip].side[I.direction == 0 ? 0 : 2];
+    adj_iface_material<<<(I.n + 127) / 128, 128, 0, h->stream>>>(I, Sm, Sp);
     CUDA_TRY(cudaGetLastError());
   }
+  (void)g;
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   return FDMAP_OK;
 }
@@ -481,23 +718,27 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
   a->t_start = t_start;
   a->dt = dt;
   a->have_resid = false;
-  if (a->graph_dt != dt || !a->g_fwd[0]) {
+  if (a->graph_dt != dt || a->graph_t0 != t_start || !a->g_fwd[0]) {
     if ((rc = build_graphs(a, dt))) return rc;
+    a->graph_t0 = t_start;
   }
   // reset to the initial state
   DevBlock& B = h->hdom.blk[0];
-  const long long S = a->stride();
   h->cur = 0;
-  CUDA_TRY(cudaMemcpyAsync(B.F[0], a->init_F, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-  CUDA_TRY(cudaMemcpyAsync(B.DF, a->init_DF, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+  if ((rc = restore_state(a, a->init_F, a->init_st))) return rc;
+  for (int b = 0; b < a->nb; ++b)
+    CUDA_TRY(cudaMemcpyAsync(h->hdom.blk[b].DF, a->init_DF + a->boff[b], 3 * h->hdom.blk[b].plane * sizeof(double),
+                             cudaMemcpyDeviceToDevice, h->stream));
   set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, t_start, dt, 1);
   // sample 1: the initial state; each replayed step samples the state it produces
-  adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[0], a->rec, a->nrec, h->d_time, a->traces, nt);
+  if (a->general)
+    adj_sample_ptr<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(a->recp[0], a->nrec, h->d_time, a->traces, nt);
+  else
+    adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[0], a->rec, a->nrec, h->d_time, a->traces, nt);
   CUDA_TRY(cudaGetLastError());
   for (int n = 1; n <= nt - 1; ++n) {
-    if ((n - 1) % a->K == 0)
-      CUDA_TRY(cudaMemcpyAsync(a->ckpt + (size_t)((n - 1) / a->K) * S, B.F[h->cur], S * sizeof(double),
-                               cudaMemcpyDeviceToDevice, h->stream));
+    if ((n - 1) % a->K == 0 && (rc = save_state(a, a->ckpt + (size_t)((n - 1) / a->K) * a->ckpt_stride())))
+      return rc;
     CUDA_TRY(cudaGraphLaunch(a->g_fwd[h->cur], h->stream));
     if (h->rk.nstage & 1) h->cur = 1 - h->cur;
   }
@@ -524,16 +765,20 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
   if (!a->have_resid) return set_err(FDMAP_ERR_INVALID_ARG, "backward needs a forward run with data");
   fdmap_gpu* h = a->h;
   CUDA_TRY(cudaSetDevice(h->device));
-  DevBlock& B = h->hdom.blk[0];
-  const long long S = a->stride();
+  const long long S = a->total;
   const int N = a->N;
-  const size_t plane_bytes = (size_t)B.plane * sizeof(double);
+  const size_t plane_bytes = (size_t)a->gtotal * sizeof(double);
   for (int q = 0; q < 2; ++q) {
     CUDA_TRY(cudaMemsetAsync(a->ub[q], 0, S * sizeof(double), h->stream));
     CUDA_TRY(cudaMemsetAsync(a->qp[q], 0, S * sizeof(double), h->stream));
   }
   CUDA_TRY(cudaMemsetAsync(a->grho, 0, plane_bytes, h->stream));
   CUDA_TRY(cudaMemsetAsync(a->gG, 0, plane_bytes, h->stream));
+  if (a->nfault > 0) {
+    CUDA_TRY(cudaMemsetAsync(a->psib, 0, a->nfault * sizeof(double), h->stream));
+    CUDA_TRY(cudaMemsetAsync(a->qpsib, 0, a->nfault * sizeof(double), h->stream));
+    CUDA_TRY(cudaMemsetAsync(a->gS0, 0, a->nfault * sizeof(double), h->stream));
+  }
   // dJ/dU^N at the receivers
   AdjClock ck{0, N};
   CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
@@ -545,7 +790,8 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int n0 = seg * a->K + 1, n1 = std::min(n0 + a->K, N);  // steps n0 .. n1-1
     h->cur = 0;
-    CUDA_TRY(cudaMemcpyAsync(B.F[0], a->ckpt + (size_t)seg * S, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    int rc = restore_state(a, a->ckpt + (size_t)seg * a->ckpt_stride(), nullptr);
+    if (rc) return rc;
     set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, a->t_start, a->dt, n0);
     ck.rel = 0;
     ck.n = N;  // unused while recomputing
@@ -563,9 +809,53 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
     }
   }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
-  int rc;
-  if (grad_rho && (rc = from_block(a, grad_rho, a->grho))) return rc;
-  if (grad_G && (rc = from_block(a, grad_G, a->gG))) return rc;
+  for (int b = 0; b < a->nb; ++b) {
+    int rc;
+    if (grad_rho && (rc = from_block(a, grad_rho, a->grho + a->goff[b], b))) return rc;
+    if (grad_G && (rc = from_block(a, grad_G, a->gG + a->goff[b], b))) return rc;
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_adjoint_fault_size(const fdmap_adjoint* a) { return a ? a->nfault : 0; }
+
+int fdmap_gpu_adjoint_set_prestress(fdmap_adjoint* a, const double* S0) {
+  if (!a || !S0) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  fdmap_gpu* h = a->h;
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (const auto& inf : a->info_host) {
+    const DevIface& I = h->hdom.ifc[inf.iface];
+    if (I.coupling == FDMAP_COUPLING_LOCKED) continue;
+    CUDA_TRY(cudaMemcpy(I.fr.par + (size_t)PAR_BSS0 * I.n, S0 + inf.start, I.n * sizeof(double),
+                        cudaMemcpyHostToDevice));
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_adjoint_get_prestress(fdmap_adjoint* a, double* S0) {
+  if (!a || !S0) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  fdmap_gpu* h = a->h;
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  for (const auto& inf : a->info_host) {
+    const DevIface& I = h->hdom.ifc[inf.iface];
+    if (I.coupling == FDMAP_COUPLING_LOCKED) {
+      std::fill(S0 + inf.start, S0 + inf.start + I.n, 0.0);
+      continue;
+    }
+    CUDA_TRY(cudaMemcpy(S0 + inf.start, I.fr.par + (size_t)PAR_BSS0 * I.n, I.n * sizeof(double),
+                        cudaMemcpyDeviceToHost));
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_adjoint_prestress_gradient(fdmap_adjoint* a, double* grad_S0) {
+  if (!a || !grad_S0) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  if (a->nfault == 0) return FDMAP_OK;
+  CUDA_TRY(cudaSetDevice(a->h->device));
+  CUDA_TRY(cudaStreamSynchronize(a->h->stream));
+  CUDA_TRY(cudaMemcpy(grad_S0, a->gS0, a->nfault * sizeof(double), cudaMemcpyDeviceToHost));
   return FDMAP_OK;
 }
 

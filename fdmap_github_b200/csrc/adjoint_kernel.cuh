@@ -37,6 +37,7 @@ struct AdjStage {
   const long long* rel;           // device: step index within the recomputed segment
   double* grho;                   // dJ/drho, dJ/dG (1 plane each), accumulated
   double* gG;
+  int blk;                        // block whose nodes this stage covers
 };
 
 // SAT of one outer side at an edge node in mode III (set_bc_mode3 + SAT_term):
@@ -93,7 +94,7 @@ template <int PI_>
 __device__ __forceinline__ void adj_node_part(const DevDomain& D, const AdjStage& p, int i, int j, int part,
                                               double* acc, double* phi, double& grho, double& gG) {
   constexpr int nbnd = nbnd_of(PI_);
-  const DevBlock& B = D.blk[0];
+  const DevBlock& B = D.blk[p.blk];
   const int nx = B.nx, ny = B.ny, nbst = D.nbst;
   const long long pitch = B.pitch, plane = B.plane;
   const long long c = (long long)j * pitch + i;
@@ -188,6 +189,7 @@ __device__ __forceinline__ void adj_node_part(const DevDomain& D, const AdjStage
   const double rho = B.rho[c], G = B.G[c];
   auto side = [&](int sd, int k) {
     const DevSide& S = B.side[sd];
+    if (S.bc == FDMAP_BC_NONE) return;  // interface side: the fault adjoint's
     const double us[3] = {ust[c], ust[plane + c], ust[2 * plane + c]};
     const double F0[3] = {S.F0[k], S.F0[k + S.n], S.F0[k + 2 * S.n]};
     sat_adjoint(S.bc, S.M[k], S.M[k + 3 * S.n], S.nrm[k], S.nrm[k + S.n], lam, us, F0, rho, G, acc, &grho, &gG);

@@ -425,8 +425,10 @@ class GpuEnsemble:
 
 class GpuAdjoint:
     """Forward/backward pair (fdmap_gpu_adjoint_*): receiver misfit of a
-    heterogeneous mode III block and its gradient with respect to the density
-    and shear-modulus fields, by the discrete adjoint with checkpoints."""
+    heterogeneous mode III domain and its gradient with respect to the density
+    and shear-modulus fields and, on locked or rate-and-state interfaces, the
+    shear prestress of every fault node, by the discrete adjoint with
+    checkpoints."""
 
     def __init__(self, host: HostDomain, receivers, checkpoint_every: int = 45, device: int = 0):
         self.host = host
@@ -471,6 +473,30 @@ class GpuAdjoint:
         F = np.empty((h.nF, h.ny, h.nx))
         check_gpu(lib().fdmap_gpu_adjoint_fields(self._a, dptr(F)), "fdmap_gpu_adjoint_fields")
         return F
+
+    @property
+    def fault_size(self) -> int:
+        """Fault nodes of all interfaces, concatenated in interface order."""
+        return int(lib().fdmap_gpu_adjoint_fault_size(self._a))
+
+    def set_prestress(self, S0: np.ndarray) -> None:
+        """Background shear stress of every fault node (the stress_file S0 term)."""
+        s = np.ascontiguousarray(S0, dtype=np.float64).reshape(-1)
+        if s.size != self.fault_size:
+            raise ValueError(f"prestress needs {self.fault_size} values, got {s.size}")
+        check_gpu(lib().fdmap_gpu_adjoint_set_prestress(self._a, dptr(s)), "fdmap_gpu_adjoint_set_prestress")
+
+    def get_prestress(self) -> np.ndarray:
+        s = np.empty(self.fault_size)
+        check_gpu(lib().fdmap_gpu_adjoint_get_prestress(self._a, dptr(s)), "fdmap_gpu_adjoint_get_prestress")
+        return s
+
+    def prestress_gradient(self) -> np.ndarray:
+        """dJ/dS0 per fault node from the last backward pass."""
+        g = np.empty(self.fault_size)
+        check_gpu(lib().fdmap_gpu_adjoint_prestress_gradient(self._a, dptr(g)),
+                  "fdmap_gpu_adjoint_prestress_gradient")
+        return g
 
     def close(self) -> None:
         if self._a:

@@ -257,6 +257,57 @@ def heterogeneous_ricker(outdir: str | Path, n: int = 801, h: float = 0.02, nt: 
 """
 
 
+def heterogeneous_rs_fault(outdir: str | Path, n: int = 41, h: float = 0.25, nt: int = 41, rk: int = 4,
+                           cfl: float = 0.5, fd: str = "SBP4", law: str = "RAL", seed: int = 0, std: float = 0.05,
+                           corr: float = 1.0, coupling: str = "friction") -> str:
+    """Mode III rupture on a rate-and-state fault y = 0 between two
+    heterogeneous blocks of n x (n//2 + 1) nodes: density and shear modulus
+    are seeded Gaussian random fields (relative std `std`, correlation length
+    `corr` km) about 2.67 g/cm^3 and 32 GPa over the global grid, and a
+    Gaussian shear load nucleates slip at the centre."""
+    out = Path(outdir)
+    out.mkdir(parents=True, exist_ok=True)
+    rng = np.random.default_rng(seed)
+    m = n // 2 + 1
+    L, W = (n - 1) * h, (m - 1) * h
+
+    def grf(shape):
+        w = rng.standard_normal(shape)
+        kx = np.fft.fftfreq(shape[0], d=h)[:, None]
+        ky = np.fft.fftfreq(shape[1], d=h)[None, :]
+        filt = np.exp(-0.5 * (2 * np.pi) ** 2 * (kx ** 2 + ky ** 2) * (corr / 2) ** 2)
+        g = np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
+        return g / g.std()
+
+    # global grid: block 1 rows 1..m, block 2 rows m+1..2m; arrays (nx, ny), i fastest on disk
+    rho = 2.67 * (1.0 + std * grf((n, 2 * m)))
+    G = 32.0 * (1.0 + std * grf((n, 2 * m)))
+    cs = np.sqrt(G / rho)
+    _write(out / "medium.dat", rho.T, cs.T, np.sqrt(3.0) * cs.T)
+    g1 = f"nx={n}, ny={m}, LB={_f(-L / 2)},{_f(-W)}, LT={_f(-L / 2)},0d0, RB={_f(L / 2)},{_f(-W)}, RT={_f(L / 2)},0d0"
+    g2 = f"nx={n}, ny={m}, LB={_f(-L / 2)},0d0, LT={_f(-L / 2)},{_f(W)}, RB={_f(L / 2)},0d0, RT={_f(L / 2)},{_f(W)}"
+    mat = "&material_list heterogeneous=T, filename='medium.dat', rho=2.67d0, cs=3.464d0 /"
+    fields = "&fields_list syy0=-100d0, syz0=58d0 /"
+    friction = (f"&friction_list friction_law='{law}', rs%a=0.01d0, rs%b=0.014d0, rs%V0=1d-6, rs%f0=0.6d0, "
+                "rs%L=0.05d0, rs%fw=0.2d0, rs%Vw=0.1d0, Psi0=0.6d0, ld%shape='gaussian', ld%R=1.5d0, "
+                "ld%S=20d0, ld%x0=0d0, ld%y0=0d0, ld%T=0d0 /\n") if coupling == "friction" else ""
+    return f"""&problem_list name='heterogeneous_rs_fault', nt={nt}, CFL={_f(cfl)}, RKorder={rk} /
+&domain_list mode=3, FDmethod='{fd}', nblocks_x=1, nblocks_y=2 /
+!---BLOCK1---
+&grid_list {g1} /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='absorbing', bcT='none' /
+{mat}
+{fields}
+!---BLOCK2---
+&grid_list {g2} /
+&boundaries_list bcL='absorbing', bcR='absorbing', bcB='none', bcT='free' /
+{mat}
+{fields}
+!---IFACE1---
+&interface_list coupling='{coupling}', direction='y' /
+{friction}"""
+
+
 def von_karman_1d(n: int, h: float, hurst: float, corr: float, seed: int) -> np.ndarray:
     """Seeded 1-D von Karman random field on n points of spacing h: power
     spectral density proportional to (1 + (k a)^2)^-(H + 1/2) with k the

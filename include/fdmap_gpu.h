@@ -227,13 +227,18 @@ void fdmap_gpu_ensemble_destroy(fdmap_ensemble* e);
  *   J = 1/2 sum_{n=1..nt} sum_r (vz(x_r, t_n) - data[n-1][r])^2
  * (vz sampled at every step start, where the reference writes its output,
  * time_step.f90:129) with respect to the density rho(x) and shear modulus
- * G(x) of one heterogeneous mode III block with absorbing / free / rigid
- * sides and no interfaces.  The forward pass is fdmap_gpu_time_step itself;
- * the backward pass is the discrete adjoint of those LS-RK stages
- * (SBP-SAT rates and the edge impedances Zs = rho*cs, Ks = cs*H00i*|grad|/J
- * with cs = sqrt(G/rho)), with the fields checkpointed every
- * `checkpoint_every` steps and each segment recomputed once.  The reference
- * has no adjoint; there is no routine this replaces.
+ * G(x) of a heterogeneous mode III domain (absorbing / free / rigid sides,
+ * blocks coupled by locked or rate-and-state interfaces) and to the shear
+ * prestress S0 of every fault node.  The forward pass is fdmap_gpu_time_step
+ * itself; the backward pass is the discrete adjoint of those LS-RK stages
+ * (SBP-SAT rates, the edge impedances Zs = rho*cs, Ks = cs*H00i*|grad|/J with
+ * cs = sqrt(G/rho), and the interface solve of interfaces.f90:676-1012 /
+ * friction.f90:593-828 with its Newton root differentiated implicitly and the
+ * state variable's own RK adjoint), with the fields and fault registers
+ * checkpointed every `checkpoint_every` steps and each segment recomputed
+ * once.  Slip-weakening, forced rupture and regularised normal stress are
+ * refused (FDMAP_ERR_UNSUPPORTED).  The reference has no adjoint; there is no
+ * routine this replaces.
  * ---------------------------------------------------------------------- */
 typedef struct fdmap_adjoint fdmap_adjoint;
 
@@ -258,6 +263,18 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
 
 /* Body fields F(nx,ny,3) after the last forward pass. */
 int fdmap_gpu_adjoint_fields(fdmap_adjoint* a, double* F);
+
+/* Fault nodes of all interfaces, concatenated in interface order: the length
+ * of the prestress arrays below (nodes of locked interfaces read as 0). */
+int fdmap_gpu_adjoint_fault_size(const fdmap_adjoint* a);
+
+/* Background shear stress of the fault nodes (friction_list stress_file S0,
+ * load_stress, friction.f90:1317-1374): set and read back. */
+int fdmap_gpu_adjoint_set_prestress(fdmap_adjoint* a, const double* S0);
+int fdmap_gpu_adjoint_get_prestress(fdmap_adjoint* a, double* S0);
+
+/* dJ/dS0 per fault node from the last fdmap_gpu_adjoint_backward. */
+int fdmap_gpu_adjoint_prestress_gradient(fdmap_adjoint* a, double* grad_S0);
 
 void fdmap_gpu_adjoint_destroy(fdmap_adjoint* a);
 

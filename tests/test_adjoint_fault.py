@@ -1,0 +1,169 @@
+"""Forward/backward pair across a rate-and-state fault: two heterogeneous mode
+III blocks coupled by a frictional (or locked) interface.  The discrete-adjoint
+gradient of the receiver misfit with respect to rho(x), G(x) and the shear
+prestress S0 of every fault node against central finite differences of the
+forward misfit in random directions (h = 1e-6 relative), on the engine's own
+forward path (interfaces.f90:676-1012, friction.f90:593-828 for the solve)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from fdmap_github_b200 import FdmapError, GpuAdjoint, GpuDomain, init_domain, problems
+
+S0_SCALE = 58.0  # shear stress level of the problem: prestress directions are relative to it
+
+
+def _setup(tmp_path, law="RAL", coupling="friction", nt=41, K=7, fd="SBP4", seed=1):
+    text = problems.heterogeneous_rs_fault(tmp_path, n=41, h=0.25, nt=nt, law=law, fd=fd, seed=seed,
+                                           coupling=coupling)
+    if coupling == "locked":  # a point force below the interface drives the locked problem
+        text += ("&source_list x0=0.37d0, y0=-1.61d0, Fz=1d0, source_time_function='Ricker', "
+                 "t_center=0.3d0, t_duration=0.25d0 /\n")
+    h = init_domain(text, tmp_path)
+    cols = np.linspace(3, h.nx - 2, 6).round().astype(int)
+    rec = [(int(i), h.ny) for i in cols] + [(int(i), 1) for i in cols[::2]]  # top and bottom rows
+    return h, rec, GpuAdjoint(h, rec, checkpoint_every=K)
+
+
+def _material(h):
+    return h.array("rho")[0].copy(), h.array("G")[0].copy()
+
+
+def _data(adj, h):
+    """Traces of a perturbed model: a smooth 5 % material bump and a shear
+    prestress bump of 2 on the fault."""
+    rho, G = _material(h)
+    y, x = np.meshgrid(np.linspace(0, 1, h.ny), np.linspace(0, 1, h.nx), indexing="ij")
+    bump = np.exp(-((x - 0.4) ** 2 + (y - 0.6) ** 2) / 0.02)
+    adj.set_material(rho * (1 + 0.05 * bump), G * (1 - 0.05 * bump))
+    nf = adj.fault_size
+    s = np.linspace(-1, 1, nf)
+    adj.set_prestress(2.0 * np.exp(-((s - 0.2) / 0.3) ** 2))
+    d, _ = adj.forward()
+    adj.set_material(rho, G)
+    adj.set_prestress(np.zeros(nf))
+    return d
+
+
+def test_adjoint_rejects_slip_weakening(tmp_path):
+    text = problems.heterogeneous_rs_fault(tmp_path, n=21, h=0.5, nt=5, law="SW")
+    text = text.replace("rs%a=0.01d0", "sw%fs=0.68d0, sw%fd=0.52d0, sw%Dc=0.2d0, rs%a=0.01d0")
+    h = init_domain(text, tmp_path)
+    with pytest.raises(FdmapError) as e:
+        GpuAdjoint(h, [(5, h.ny)])
+    assert e.value.code == -6
+
+
+def test_adjoint_rejects_forced_rupture(tmp_path):
+    text = problems.heterogeneous_rs_fault(tmp_path, n=21, h=0.5, nt=5)
+    text = text.replace("ld%T=0d0 /", "ld%T=0d0, force=T, kn%fd=0.52d0 /")
+    h = init_domain(text, tmp_path)
+    with pytest.raises(FdmapError) as e:
+        GpuAdjoint(h, [(5, h.ny)])
+    assert e.value.code == -6
+
+
+@pytest.mark.gpu
+def test_forward_traces_are_the_engine_run(require_gpu, tmp_path):
+    h, rec, adj = _setup(tmp_path, nt=31)
+    tr, _ = adj.forward()
+    g = GpuDomain(h)
+    for n in range(1, h.nt + 1):
+        F, _ = g.get_fields()
+        vz = np.array([F[0, j - 1, i - 1] for i, j in rec])
+        assert np.array_equal(vz, tr[n - 1]), f"sample {n}"
+        if n < h.nt:
+            g.time_step_LS(h.t0 + (n - 1) * h.dt, h.dt)
+    assert np.array_equal(adj.fields(), g.get_fields()[0])
+    assert np.abs(g.get_fault(0, "V")).max() > 1.0  # the fault ruptures in the window
+    g.close()
+
+
+def _fd_check(adj, h, data, rng, ndir, what=("rho", "G", "S0")):
+    rho, G = _material(h)
+    nf = adj.fault_size
+    _, J0 = adj.forward(data=data)
+    assert J0 > 0
+    g_rho, g_G = adj.backward()
+    g_S0 = adj.prestress_gradient()
+    assert np.all(np.isfinite(g_rho)) and np.all(np.isfinite(g_G)) and np.all(np.isfinite(g_S0))
+    eps = 1e-6
+    worst = 0.0
+    for _ in range(ndir):
+        d_rho = rng.uniform(-1, 1, rho.shape) if "rho" in what else np.zeros_like(rho)
+        d_G = rng.uniform(-1, 1, G.shape) if "G" in what else np.zeros_like(G)
+        d_S0 = rng.uniform(-1, 1, nf) if "S0" in what else np.zeros(nf)
+        pred = float(np.sum(g_rho * rho * d_rho) + np.sum(g_G * G * d_G) + np.sum(g_S0 * S0_SCALE * d_S0))
+        Js = []
+        for sgn in (1, -1):
+            adj.set_material(rho * (1 + sgn * eps * d_rho), G * (1 + sgn * eps * d_G))
+            adj.set_prestress(sgn * eps * S0_SCALE * d_S0)
+            Js.append(adj.forward(data=data)[1])
+        fd_val = (Js[0] - Js[1]) / (2 * eps)
+        worst = max(worst, abs(fd_val - pred) / abs(fd_val))
+    adj.set_material(rho, G)
+    adj.set_prestress(np.zeros(nf))
+    return worst, (g_rho, g_G, g_S0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("law", ["RAL", "RSL", "RFL"])
+def test_gradient_vs_central_differences(require_gpu, tmp_path, law):
+    rng = np.random.default_rng(17)
+    h, rec, adj = _setup(tmp_path, law=law)
+    data = _data(adj, h)
+    ndir = 16 if law == "RAL" else 6
+    worst, (g_rho, g_G, g_S0) = _fd_check(adj, h, data, rng, ndir)
+    assert np.any(g_S0 != 0.0)
+    assert worst <= 1e-6, f"{law}: adjoint vs central differences, worst relative error {worst:.3e}"
+
+
+@pytest.mark.gpu
+def test_prestress_gradient_alone_vs_central_differences(require_gpu, tmp_path):
+    """Directions in the prestress only: the part of the gradient that runs
+    entirely through the implicit derivative of the friction solve."""
+    rng = np.random.default_rng(23)
+    h, rec, adj = _setup(tmp_path)
+    data = _data(adj, h)
+    worst, _ = _fd_check(adj, h, data, rng, 6, what=("S0",))
+    assert worst <= 1e-6, f"prestress: worst relative error {worst:.3e}"
+
+
+@pytest.mark.gpu
+def test_locked_interface_gradient(require_gpu, tmp_path):
+    rng = np.random.default_rng(29)
+    h, rec, adj = _setup(tmp_path, coupling="locked")
+    rho, G = _material(h)
+    y, x = np.meshgrid(np.linspace(0, 1, h.ny), np.linspace(0, 1, h.nx), indexing="ij")
+    adj.set_material(rho * (1 + 0.05 * np.exp(-((x - 0.4) ** 2 + (y - 0.6) ** 2) / 0.02)), G)
+    data, _ = adj.forward()
+    adj.set_material(rho, G)
+    worst, _ = _fd_check(adj, h, data, rng, 4, what=("rho", "G"))
+    assert worst <= 1e-6
+
+
+@pytest.mark.gpu
+def test_gradient_independent_of_checkpoint_interval(require_gpu, tmp_path):
+    h, rec, a7 = _setup(tmp_path, K=7)
+    data = _data(a7, h)
+    a7.forward(data=data)
+    g7 = a7.backward() + (a7.prestress_gradient(),)
+    a80 = GpuAdjoint(h, rec, checkpoint_every=80)
+    a80.set_material(*_material(h))  # same edge impedances as a7 (set_material path)
+    a80.forward(data=data)
+    g80 = a80.backward() + (a80.prestress_gradient(),)
+    for x, y in zip(g7, g80):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+def test_fault_nodes_carry_material_gradient(require_gpu, tmp_path):
+    """The interface impedances depend on rho and G at both edge nodes."""
+    h, rec, adj = _setup(tmp_path)
+    data = _data(adj, h)
+    adj.forward(data=data)
+    g_rho, g_G = adj.backward()
+    m = h.ny // 2
+    for row in (m - 1, m):  # edge rows of the two blocks
+        assert np.any(g_G[row] != 0.0) and np.any(g_rho[row] != 0.0)
