@@ -226,6 +226,12 @@ module fdmap_gpu_mod
        type(c_ptr), value :: h, pgv, pga
      end function fdmap_gpu_set_peak
 
+     integer(c_int) function fdmap_gpu_get_energy(h, E) bind(C, name='fdmap_gpu_get_energy')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), intent(out) :: E(*)         ! (nblocks + 1): Ebody, then Eblock per block
+     end function fdmap_gpu_get_energy
+
      integer(c_int) function fdmap_gpu_get_side_displacement(h, b, s, U, DU) &
           bind(C, name='fdmap_gpu_get_side_displacement')
        import :: c_int, c_ptr
@@ -369,6 +375,30 @@ module fdmap_gpu_mod
        type(c_ptr), value :: a
        real(c_double), intent(out) :: grad_rho(*), grad_G(*)
      end function fdmap_gpu_adjoint_backward
+
+     integer(c_int) function fdmap_gpu_adjoint_fault_size(a) bind(C, name='fdmap_gpu_adjoint_fault_size')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: a
+     end function fdmap_gpu_adjoint_fault_size
+
+     integer(c_int) function fdmap_gpu_adjoint_set_prestress(a, S0) bind(C, name='fdmap_gpu_adjoint_set_prestress')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a
+       real(c_double), intent(in) :: S0(*)           ! fault nodes of all interfaces, in interface order
+     end function fdmap_gpu_adjoint_set_prestress
+
+     integer(c_int) function fdmap_gpu_adjoint_get_prestress(a, S0) bind(C, name='fdmap_gpu_adjoint_get_prestress')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a
+       real(c_double), intent(out) :: S0(*)
+     end function fdmap_gpu_adjoint_get_prestress
+
+     integer(c_int) function fdmap_gpu_adjoint_prestress_gradient(a, grad_S0) &
+          bind(C, name='fdmap_gpu_adjoint_prestress_gradient')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a
+       real(c_double), intent(out) :: grad_S0(*)
+     end function fdmap_gpu_adjoint_prestress_gradient
 
      subroutine fdmap_gpu_adjoint_destroy(a) bind(C, name='fdmap_gpu_adjoint_destroy')
        import :: c_ptr
