@@ -476,6 +476,9 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers heterogeneous mode III domains");
   if (d->displacement || d->peak || d->energy_balance)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint does not track displacement or peak motion");
+  for (int b = 0; b < d->nblocks; ++b)
+    if (d->blocks[b].Cdiss > 0.0)
+      return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint does not cover artificial dissipation");
   if (d->src.gauss_forcing || d->src.forcing_filename)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers the point source only");
   if (d->body)  // the edge-impedance derivatives are formed from the host's metric arrays

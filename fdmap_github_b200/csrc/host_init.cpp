@@ -902,9 +902,9 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
     fb.pmlx = B.pmlx ? 1 : 0; fb.pmly = B.pmly ? 1 : 0;
     fb.pml_n = B.pml_n; fb.pml_sigma = B.pml_sigma; fb.pml_kappa = B.pml_kappa;
     fb.pml_mx = B.pml_mx; fb.pml_px = B.pml_px; fb.pml_my = B.pml_my; fb.pml_py = B.pml_py;
-    // the PML rates use the block's homogeneous material (rates.f90:2024-2044)
-    if (mode == 2 && (B.pmlx || B.pmly) && B.Cdiss == 0.0 && B.heterogeneous)
-      fail(FDMAP_ERR_UNSUPPORTED, "a perfectly matched layer in a heterogeneous block is not supported");
+    // a PML block of a heterogeneous medium runs the PML rates with the
+    // block's homogeneous material, as set_rates does (time_step.f90:354-420
+    // come before the heterogeneous branch); szz keeps the node's nu (486-490)
     for (int q = 0; q < 9; ++q) fb.F0[q] = B.F0v[q];
     for (int s = 0; s < 4; ++s) {
       fdmap_side& fs = fb.side[s];
@@ -949,9 +949,6 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
     }
     cmax = std::sqrt(cs * cs + cp * cp);
   }
-  for (int b = 0; b < nblocks; ++b)
-    if (dom.bin[b].Cdiss > 0.0 && dom.bin[b].heterogeneous)
-      fail(FDMAP_ERR_UNSUPPORTED, "artificial dissipation in a heterogeneous block is not supported");
   d.t0 = t0;
   if (dev_body) {
     // finished by fdmap_host_set_spacing once the device has reduced hmin, hmax

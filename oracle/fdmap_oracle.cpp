@@ -1139,9 +1139,12 @@ void rates_boundary_pml(oracle_domain& D, const Blk& B, int mx, int px, int my, 
 
 // ---------------------------------------------------------------------------
 // Rates with artificial dissipation (set_rates_dissipation, time_step.f90:555-751;
-// rates_dissipation_*_mode2/3, rates.f90:939-2021), homogeneous blocks.
+// rates_dissipation_*_mode2/3, rates.f90:939-2021; in a heterogeneous medium
+// rates_h_dissipation_*, rates_heterogeneous.f90:920-1997).
 // ---------------------------------------------------------------------------
-// interior (rates.f90:939-999 mode III, 1397-1482 mode II)
+// interior (rates.f90:939-999 mode III, 1397-1482 mode II; heterogeneous
+// rates_heterogeneous.f90:920-978, 1376-1458: the node's rho, G, M scale the
+// rate bracket; mode III as (T*DI(s)/rho)*Ji, mode II as (DI(s)/rho*T + d(s)*S)*Ji)
 void rates_dissipation_interior(Ctx& c, const Blk& B, int mx, int px, int my, int py) {
   oracle_domain& D = *c.D;
   const Ops& op = D.op;
@@ -1166,11 +1169,22 @@ void rates_dissipation_interior(Ctx& c, const Blk& B, int mx, int px, int my, in
           add_flux(c, rd, true, -1, g, qm, gmm, T, first);
           add_flux(c, rd, false, +1, g, rp, gmm, T, first);
           add_flux(c, rd, false, -1, g, rm, gmm, T, first);
-          double a = rd.coef == 0 ? op.DI[s] / B.rho : (rd.coef == 1 ? op.DI[s] * B.G : op.DI[s] * B.M);
           size_t off = c.NN * r;
           double S = D.J[qp] * D.F[qp + off] + D.J[qm] * D.F[qm + off] + D.J[rp] * D.F[rp + off] +
                      D.J[rm] * D.F[rm + off];
           double Ji = D.Ji[g];
+          if (D.het) {
+            const double m = mat(c, B, g, rd.coef);
+            if (D.mode == 3) {
+              const double Tm = rd.coef == 0 ? T * op.DI[s] / m : T * op.DI[s] * m;
+              D.DF[g + off] = D.DF[g + off] + Tm * Ji + dco[s] * Ji * S;
+            } else {
+              const double a = rd.coef == 0 ? op.DI[s] / m : op.DI[s] * m;
+              D.DF[g + off] = D.DF[g + off] + (a * T + dco[s] * S) * Ji;
+            }
+            continue;
+          }
+          double a = rd.coef == 0 ? op.DI[s] / B.rho : (rd.coef == 1 ? op.DI[s] * B.G : op.DI[s] * B.M);
           if (D.mode == 3) D.DF[g + off] = D.DF[g + off] + T * a * Ji + dco[s] * Ji * S;
           else D.DF[g + off] = D.DF[g + off] + (a * T + dco[s] * S) * Ji;
         }

@@ -81,12 +81,14 @@ def test_dissipation_takes_precedence():
     assert not np.any(o1.get_pml("Wx"))
 
 
-def test_heterogeneous_layer_rejected(tmp_path):
+def test_heterogeneous_layer_accepted(tmp_path):
+    """A layer in a heterogeneous block runs the homogeneous PML rates with the
+    block material (time_step.f90:354-420); tests/test_heterogeneous_variants.py
+    checks the arithmetic."""
     text = problems.heterogeneous_ricker(tmp_path, n=31, h=0.1, nt=5)
     text = text.replace("mode=3", "mode=2") + "&pml_list pmlx=T /\n"
-    with pytest.raises(FdmapError) as e:
-        init_domain(text, tmp_path)
-    assert e.value.code == -6
+    h = init_domain(text, tmp_path)
+    assert h.block_pml(0)["pmlx"]
 
 
 # ---------------------------------------------------------------- GPU
