@@ -412,12 +412,12 @@ int validate(const fdmap_desc* d) {
     int nx = B.pgx - B.mgx + 1, ny = B.pgy - B.mgy + 1;
     if (B.mgx < 1 || B.mgy < 1 || B.pgx > d->nx || B.pgy > d->ny)
       return set_err(FDMAP_ERR_INVALID_ARG, "block index limits outside the domain");
-    if (!dev_body && B.Cdiss > 0.0 && (!d->J || d->heterogeneous))
-      return set_err(d->J ? FDMAP_ERR_UNSUPPORTED : FDMAP_ERR_INVALID_ARG,
-                     d->J ? "artificial dissipation in heterogeneous blocks is not supported"
-                          : "artificial dissipation needs the Jacobian array J");
+    // in a heterogeneous medium the dissipative rates scale by the node's
+    // material (rates_h_dissipation_*) and the PML rates keep the block's
+    // homogeneous material (time_step.f90:354-420): both kernels cover that
+    if (!dev_body && B.Cdiss > 0.0 && !d->J)
+      return set_err(FDMAP_ERR_INVALID_ARG, "artificial dissipation needs the Jacobian array J");
     if (d->mode == 2 && (B.pmlx || B.pmly) && B.Cdiss == 0.0 && !(dev_body && d->body->blocks[b].Cdiss > 0.0)) {
-      if (d->heterogeneous) return set_err(FDMAP_ERR_UNSUPPORTED, "a perfectly matched layer needs homogeneous blocks");
       if (dev_body) return set_err(FDMAP_ERR_UNSUPPORTED, "a perfectly matched layer needs the body arrays on the host");
       if (B.pml_n > 0.0 && (!d->x || !d->y)) return set_err(FDMAP_ERR_INVALID_ARG, "the PML profile needs x and y");
     }
