@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "body_formulas.h"
+#include "pml_formula.h"
 #include "engine.h"
 
 namespace fdmap {
@@ -117,6 +118,30 @@ __global__ void metrics_kernel(BodyBlock B, BodyOp op, unsigned long long* hminm
   }
 }
 
+// PML damping planes sx, sy from the grid (pml_damping, rates.f90:2065-2068)
+__global__ void pml_damping_kernel(BodyBlock B, double* damp, double sigma, double n, double mx, double px, double my,
+                                   double py) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (i >= B.nx || j >= B.ny) return;
+  const long long o = (long long)j * B.pitch + i;
+  damp[o] = pml_damping(sigma, n, mx, px, B.x[o]);
+  damp[B.plane + o] = pml_damping(sigma, n, my, py, B.y[o]);
+}
+
+// hxi = Ji*yr, hyi = Ji*xq at the first node of each PML region (q, r: 0 minus
+// end, 1 plus end, 2 interior), one thread per region
+__global__ void pml_regions_kernel(BodyBlock B, double* hh, int nbst) {
+  const int k = threadIdx.x;
+  if (k >= 9) return;
+  const int q = k / 3, r = k % 3;
+  const int qi = q == 0 ? 0 : (q == 1 ? B.nx - nbst : nbst);
+  const int rj = r == 0 ? 0 : (r == 1 ? B.ny - nbst : nbst);
+  const long long o = (long long)rj * B.pitch + qi;
+  hh[2 * k] = B.Ji[o] * B.yr[o];
+  hh[2 * k + 1] = B.Ji[o] * B.xq[o];
+}
+
 // edge impedances (Zs, Zp, gamma, Ks, Kp) of the nodes of one side
 __global__ void side_impedance_kernel(BodyBlock B, BodySide S, double H00i) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -202,6 +227,13 @@ int build_body(fdmap_gpu* h, const fdmap_desc* d, const SbpOperator& sop) {
     CUDA_TRY(cudaGetLastError());
     metrics_kernel<<<grid, 128, 0, h->stream>>>(B, op, hmm);
     CUDA_TRY(cudaGetLastError());
+    if (D.pml) {
+      pml_damping_kernel<<<grid, 128, 0, h->stream>>>(B, const_cast<double*>(D.pml_s), fb.pml_sigma, fb.pml_n,
+                                                      fb.pml_mx, fb.pml_px, fb.pml_my, fb.pml_py);
+      CUDA_TRY(cudaGetLastError());
+      pml_regions_kernel<<<1, 32, 0, h->stream>>>(B, const_cast<double*>(D.pml_h), op.nbst);
+      CUDA_TRY(cudaGetLastError());
+    }
     for (int s = 0; s < 4; ++s) {
       const fdmap_side& fs = fb.side[s];
       BodySide S{};

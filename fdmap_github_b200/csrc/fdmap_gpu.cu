@@ -15,6 +15,7 @@
 
 #include "edge_kernel.cuh"
 #include "engine.h"
+#include "pml_formula.h"
 #include "march_kernel.cuh"
 #include "sbp_tables.h"
 #include "stencil_kernel.cuh"
@@ -418,8 +419,8 @@ int validate(const fdmap_desc* d) {
     if (!dev_body && B.Cdiss > 0.0 && !d->J)
       return set_err(FDMAP_ERR_INVALID_ARG, "artificial dissipation needs the Jacobian array J");
     if (d->mode == 2 && (B.pmlx || B.pmly) && B.Cdiss == 0.0 && !(dev_body && d->body->blocks[b].Cdiss > 0.0)) {
-      if (dev_body) return set_err(FDMAP_ERR_UNSUPPORTED, "a perfectly matched layer needs the body arrays on the host");
-      if (B.pml_n > 0.0 && (!d->x || !d->y)) return set_err(FDMAP_ERR_INVALID_ARG, "the PML profile needs x and y");
+      if (!dev_body && B.pml_n > 0.0 && (!d->x || !d->y))
+        return set_err(FDMAP_ERR_INVALID_ARG, "the PML profile needs x and y");
     }
     if (nx < 2 * op.nbst || ny < 2 * op.nbst || nx < op.nbnd || ny < op.nbnd)
       return set_err(FDMAP_ERR_UNSUPPORTED, "block too small for the SBP boundary closures");
@@ -537,36 +538,36 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
         return rc;
       if (fb.pmly && ((rc = h->alloc_planes(&B.Wy, nF, g.plane)) || (rc = h->alloc_planes(&B.DWy, nF, g.plane))))
         return rc;
-      // damping at every node (rates.f90:2065-2068), evaluated once here
-      std::vector<double> damp(2 * (size_t)g.plane, 0.0);
-      for (int j = 0; j < g.ny; ++j)
-        for (int i = 0; i < g.nx; ++i) {
-          double sx = fb.pml_sigma, sy = fb.pml_sigma;
-          if (fb.pml_n > 0.0) {
-            const size_t q = (size_t)(g.mgx - 1 + i) + (size_t)d->nx * (size_t)(g.mgy - 1 + j);
-            const double x = d->x[q], y = d->y[q];
-            sx = fb.pml_sigma * std::pow(std::fabs(std::max(0.0, std::max(fb.pml_mx - x, x - fb.pml_px))), fb.pml_n);
-            sy = fb.pml_sigma * std::pow(std::fabs(std::max(0.0, std::max(fb.pml_my - y, y - fb.pml_py))), fb.pml_n);
-          }
-          damp[(size_t)j * g.pitch + i] = sx;
-          damp[(size_t)g.plane + (size_t)j * g.pitch + i] = sy;
-        }
+      // damping at every node (rates.f90:2065-2068), evaluated once: here from
+      // the host grid, or by build_body from the device grid
       double* ds = nullptr;
       if ((rc = h->alloc_planes(&ds, 2, g.plane))) return rc;
-      CUDA_TRY(cudaMemcpy(ds, damp.data(), damp.size() * sizeof(double), cudaMemcpyHostToDevice));
-      B.pml_s = ds;
-      // hxi = Ji*yr, hyi = Ji*xq at the first node of each region: q and r
-      // index 0 = minus-end strip, 1 = plus-end strip, 2 = interior
-      double hh[18];
-      const int qi[3] = {0, g.nx - op.nbst, op.nbst}, rj[3] = {0, g.ny - op.nbst, op.nbst};
-      for (int q = 0; q < 3; ++q)
-        for (int r = 0; r < 3; ++r) {
-          const size_t k = (size_t)(g.mgx - 1 + qi[q]) + (size_t)d->nx * (size_t)(g.mgy - 1 + rj[r]);
-          hh[(q * 3 + r) * 2] = d->Ji[k] * d->yr[k];
-          hh[(q * 3 + r) * 2 + 1] = d->Ji[k] * d->xq[k];
-        }
       double* dh = nullptr;
-      if ((rc = h->upload(&dh, hh, 18))) return rc;
+      if ((rc = h->alloc(&dh, 18))) return rc;
+      if (!d->body) {
+        std::vector<double> damp(2 * (size_t)g.plane, 0.0);
+        for (int j = 0; j < g.ny; ++j)
+          for (int i = 0; i < g.nx; ++i) {
+            const size_t q = (size_t)(g.mgx - 1 + i) + (size_t)d->nx * (size_t)(g.mgy - 1 + j);
+            const bool prof = fb.pml_n > 0.0;
+            damp[(size_t)j * g.pitch + i] = pml_damping(fb.pml_sigma, fb.pml_n, fb.pml_mx, fb.pml_px, prof ? d->x[q] : 0.0);
+            damp[(size_t)g.plane + (size_t)j * g.pitch + i] =
+                pml_damping(fb.pml_sigma, fb.pml_n, fb.pml_my, fb.pml_py, prof ? d->y[q] : 0.0);
+          }
+        CUDA_TRY(cudaMemcpy(ds, damp.data(), damp.size() * sizeof(double), cudaMemcpyHostToDevice));
+        // hxi = Ji*yr, hyi = Ji*xq at the first node of each region: q and r
+        // index 0 = minus-end strip, 1 = plus-end strip, 2 = interior
+        double hh[18];
+        const int qi[3] = {0, g.nx - op.nbst, op.nbst}, rj[3] = {0, g.ny - op.nbst, op.nbst};
+        for (int q = 0; q < 3; ++q)
+          for (int r = 0; r < 3; ++r) {
+            const size_t k = (size_t)(g.mgx - 1 + qi[q]) + (size_t)d->nx * (size_t)(g.mgy - 1 + rj[r]);
+            hh[(q * 3 + r) * 2] = d->Ji[k] * d->yr[k];
+            hh[(q * 3 + r) * 2 + 1] = d->Ji[k] * d->xq[k];
+          }
+        CUDA_TRY(cudaMemcpy(dh, hh, sizeof(hh), cudaMemcpyHostToDevice));
+      }
+      B.pml_s = ds;
       B.pml_h = dh;
       h->pml = true;
     }

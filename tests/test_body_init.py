@@ -44,12 +44,14 @@ def _cases(tmp_path):
         ("skewed6", _skewed("SBP6", 53, 41), None, True),
         ("skewed2", _skewed("SBP2", 37, 29), None, True),
         ("cdiss", _skewed(cdiss="0.3d0"), None, True),
+        # perfectly matched layer: damping profile pow() on the device grid
+        ("pml", problems.pml_pulse(n=61, L=6.0, nt=21, width=1.5, bc="free"), None, True),
     ]
 
 
 # ---------------------------------------------------------------- host side (CPU)
 
-@pytest.mark.parametrize("k", range(8))
+@pytest.mark.parametrize("k", range(9))
 def test_deferred_host_init_matches_full(tmp_path, k):
     name, text, base, _ = _cases(tmp_path)[k]
     full = init_domain(text, base)
@@ -119,7 +121,7 @@ def _assert_fields(a, b, exp_shapes, what):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("k", range(8))
+@pytest.mark.parametrize("k", range(9))
 def test_device_body_matches_host_body(require_gpu, tmp_path, k):
     name, text, base, exp_shapes = _cases(tmp_path)[k]
     full = init_domain(text, base)
@@ -159,6 +161,10 @@ def test_device_body_matches_host_body(require_gpu, tmp_path, k):
         assert np.abs(Fd - Ff).max() <= 1e-13 * scale, name
     else:
         assert np.array_equal(Fd, Ff), f"{name}: fields after {nsteps} steps"
+    if name == "pml":
+        for w in ("Wx", "Wy"):
+            a, b = gd.get_pml(w), gf.get_pml(w)
+            assert np.abs(b).max() > 0 and np.abs(a - b).max() <= 1e-13 * np.abs(b).max(), f"pml {w}"
     for i in range(full.nifaces):
         if full.iface_info(i)[3] == 1:
             for f in ("V", "S", "N", "D", "Psi"):
