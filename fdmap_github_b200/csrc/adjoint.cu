@@ -481,8 +481,6 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
       return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint does not cover artificial dissipation");
   if (d->src.gauss_forcing || d->src.forcing_filename)
     return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint covers the point source only");
-  if (d->body)  // the edge-impedance derivatives are formed from the host's metric arrays
-    return set_err(FDMAP_ERR_UNSUPPORTED, "the adjoint needs the body arrays on the host");
   for (int b = 0; b < d->nblocks; ++b)
     for (int s = 0; s < 4; ++s) {
       const int bc = d->blocks[b].side[s].bc;
@@ -641,6 +639,14 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
     const BlockGeom& gb = h->geom[b];
     for (int s = 0; s < 4; ++s) {
       const int n = (s < 2) ? gb.ny : gb.nx;
+      if ((rc = a->alloc(&a->geo[4 * b + s], n))) return fail(rc);
+      if (d->body) {
+        // body built on the device: the factors come from its metric planes
+        adj_edge_geometry<<<(n + 127) / 128, 128, 0, h->stream>>>(h->hdom.blk[b], s, n, op.H00i, a->geo[4 * b + s]);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess)
+          return fail(set_err(FDMAP_ERR_CUDA, "edge geometry"));
+        continue;
+      }
       std::vector<double> geo(n);
       for (int k = 0; k < n; ++k) {
         int i, j;
@@ -653,7 +659,6 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
                                    : std::sqrt(d->xq[q] * d->xq[q] + d->yq[q] * d->yq[q]);
         geo[k] = op.H00i * mag / d->J[q];
       }
-      if ((rc = a->alloc(&a->geo[4 * b + s], n))) return fail(rc);
       if (cudaMemcpy(a->geo[4 * b + s], geo.data(), n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(set_err(FDMAP_ERR_CUDA, "geometry upload"));
     }
@@ -821,6 +826,11 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
 }
 
 int fdmap_gpu_adjoint_fault_size(const fdmap_adjoint* a) { return a ? a->nfault : 0; }
+
+int fdmap_gpu_adjoint_time_params(fdmap_adjoint* a, double* params, int* nt) {
+  if (!a) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint");
+  return fdmap_gpu_time_params(a->h, params, nt);
+}
 
 int fdmap_gpu_adjoint_set_prestress(fdmap_adjoint* a, const double* S0) {
   if (!a || !S0) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");

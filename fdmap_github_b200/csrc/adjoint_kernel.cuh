@@ -292,6 +292,20 @@ __global__ void adj_edge_material(DevSide S, const double* __restrict__ rho, con
   S.M[k + 3 * S.n] = cs * geo[k];
 }
 
+// edge geometry factor H00i*|grad|/J of side `side` from the device metric
+// planes, with J formed as the device-built body forms it (side_impedance_kernel)
+__global__ void adj_edge_geometry(DevBlock B, int side, int n, double H00i, double* geo) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int i, j;
+  side_node_local(side, k, B.nx, B.ny, i, j);
+  const long long o = (long long)j * B.pitch + i;
+  const double xq = B.xq[o], xr = B.xr[o], yq = B.yq[o], yr = B.yr[o];
+  const double J = xq * yr - xr * yq;
+  const double mag = side < 2 ? sqrt(xr * xr + yr * yr) : sqrt(xq * xq + yq * yq);
+  geo[k] = H00i * mag / J;
+}
+
 // vz at the receivers of state u for sample n = ts->n (1-based)
 __global__ void adj_sample(const double* __restrict__ u, const long long* __restrict__ rec, int nrec,
                            const TimeState* ts, double* traces, int nsamples) {

@@ -441,6 +441,11 @@ class GpuAdjoint:
         check_gpu(lib().fdmap_gpu_adjoint_create(host.desc, device, self.nrec, ri.ctypes.data_as(ip),
                                                  rj.ctypes.data_as(ip), checkpoint_every, C.byref(self._a)),
                   "fdmap_gpu_adjoint_create")
+        if host.spacing_pending:  # body built on the device: the time step follows its spacings
+            p = (C.c_double * 5)()
+            nt = C.c_int(0)
+            check_gpu(lib().fdmap_gpu_adjoint_time_params(self._a, p, C.byref(nt)), "fdmap_gpu_adjoint_time_params")
+            host.set_spacing(p[3], p[4])
 
     def set_material(self, rho: np.ndarray, G: np.ndarray) -> None:
         r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)

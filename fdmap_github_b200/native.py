@@ -113,6 +113,7 @@ SIGNATURES = {
     "fdmap_gpu_adjoint_backward": (C.c_int, [_VP, _DP, _DP]),
     "fdmap_gpu_adjoint_fields": (C.c_int, [_VP, _DP]),
     "fdmap_gpu_adjoint_fault_size": (C.c_int, [_VP]),
+    "fdmap_gpu_adjoint_time_params": (C.c_int, [_VP, _DP, C.POINTER(C.c_int)]),
     "fdmap_gpu_adjoint_set_prestress": (C.c_int, [_VP, _DP]),
     "fdmap_gpu_adjoint_get_prestress": (C.c_int, [_VP, _DP]),
     "fdmap_gpu_adjoint_prestress_gradient": (C.c_int, [_VP, _DP]),

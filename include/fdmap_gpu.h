@@ -264,6 +264,10 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
 /* Body fields F(nx,ny,3) after the last forward pass. */
 int fdmap_gpu_adjoint_fields(fdmap_adjoint* a, double* F);
 
+/* Time parameters of the adjoint's domain, as fdmap_gpu_time_params (with
+ * the body built on the device, the spacings the device reduced). */
+int fdmap_gpu_adjoint_time_params(fdmap_adjoint* a, double* params, int* nt);
+
 /* Fault nodes of all interfaces, concatenated in interface order: the length
  * of the prestress arrays below (nodes of locked interfaces read as 0). */
 int fdmap_gpu_adjoint_fault_size(const fdmap_adjoint* a);

@@ -99,3 +99,27 @@ def test_boundary_nodes_carry_gradient(require_gpu, tmp_path):
     adj.forward(data=data)
     g_rho, g_G = adj.backward()
     assert np.any(g_G[-1, :] != 0.0) and np.any(g_rho[-1, :] != 0.0)
+
+
+def test_device_built_body(require_gpu, tmp_path):
+    """With the body built on the device the edge geometry factors come from
+    the device metric planes: traces, misfit and gradients equal those of the
+    adjoint over the host-built body."""
+    text = problems.heterogeneous_ricker(tmp_path, n=61, h=0.1, nt=41, seed=3, f_peak=1.0)
+    full = init_domain(text, tmp_path)
+    dev = init_domain(text, tmp_path, body_on_device=True)
+    rec = [(i, 61) for i in (5, 20, 40, 57)]
+    af = GpuAdjoint(full, rec, checkpoint_every=7)
+    ad = GpuAdjoint(dev, rec, checkpoint_every=7)
+    assert (dev.dt, dev.nt) == (full.dt, full.nt)
+    rho, G = _material(full)
+    y, x = np.meshgrid(np.linspace(0, 1, full.ny), np.linspace(0, 1, full.nx), indexing="ij")
+    af.set_material(rho * (1 + 0.05 * np.exp(-((x - 0.4) ** 2 + (y - 0.7) ** 2) / 0.02)), G)
+    data, _ = af.forward()
+    for a in (af, ad):
+        a.set_material(rho, G)
+    tf, Jf = af.forward(data=data)
+    td, Jd = ad.forward(data=data)
+    assert np.array_equal(tf, td) and Jf == Jd and Jf > 0
+    for p, q in zip(af.backward(), ad.backward()):
+        assert np.array_equal(p, q)

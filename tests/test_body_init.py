@@ -11,7 +11,7 @@ import math
 import numpy as np
 import pytest
 
-from fdmap_github_b200 import FdmapError, GpuAdjoint, GpuDomain, GpuEnsemble, init_domain, problems
+from fdmap_github_b200 import FdmapError, GpuDomain, GpuEnsemble, init_domain, problems
 
 SKEWED = """&problem_list name='skew', nt=21, CFL=0.4d0, RKorder=4 /
 &domain_list mode=2, FDmethod='{fd}', nblocks_x=1, nblocks_y=1 /
@@ -101,13 +101,6 @@ def test_init_ex_rejects_unknown_flags():
     text = problems.antiplane_pulse(n=21, L=2.0, nt=3).encode()
     assert lib().fdmap_host_init_ex(text, None, 6, C.byref(h)) == -1
     assert not h
-
-
-def test_adjoint_needs_host_body(tmp_path):
-    h = init_domain(problems.heterogeneous_ricker(tmp_path, n=31, h=0.1, nt=5), tmp_path, body_on_device=True)
-    with pytest.raises(FdmapError) as e:
-        GpuAdjoint(h, [(5, 31)])
-    assert e.value.code == -6
 
 
 # ---------------------------------------------------------------- device side
