@@ -684,7 +684,6 @@ int fdmap_gpu_adjoint_set_material(fdmap_adjoint* a, const double* rho, const do
   fdmap_gpu* h = a->h;
   CUDA_TRY(cudaSetDevice(h->device));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
-  const BlockGeom& g = h->geom[0];
   for (size_t q = 0; q < (size_t)h->nx_g * h->ny_g; ++q)
     if (!(rho[q] > 0.0) || !(G[q] > 0.0)) return set_err(FDMAP_ERR_INVALID_ARG, "density and shear modulus must be positive");
   int rc;
@@ -707,7 +706,6 @@ int fdmap_gpu_adjoint_set_material(fdmap_adjoint* a, const double* rho, const do
     adj_iface_material<<<(I.n + 127) / 128, 128, 0, h->stream>>>(I, Sm, Sp);
     CUDA_TRY(cudaGetLastError());
   }
-  (void)g;
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   return FDMAP_OK;
 }
