@@ -5,11 +5,11 @@
 // adjoint; the forward pass is the engine's own time step (time_step_LS,
 // time_step.f90:71-167), so the misfit is that of the production path.
 //
-// One block without interfaces takes the tiled path (adj_stage_tma beside
-// adj_band_kernel); several blocks or interfaces take the general path: every
-// block's nodes by adj_block_kernel, then the fault nodes by adj_fault_kernel
-// (adjoint_fault.cuh), with the state variable of each fault node stored
-// beside the fields at every stage and the fault registers in every checkpoint.
+// Every block's stage runs as interior tiles (adj_stage_tma) beside its band
+// (adj_band_kernel).  Several blocks or interfaces take the general path:
+// after the blocks, the fault nodes run through adj_fault_kernel
+// (adjoint_fault.cuh); the state variable of each fault node is stored beside
+// the fields at every stage and the fault registers in every checkpoint.
 //
 //   forward : steps 1..nt-1 as replayed graphs; vz sampled at the receivers at
 //             every step start (n = 1..nt, the reference's stage-1 output
@@ -50,12 +50,12 @@ struct fdmap_adjoint {
   long long* node = nullptr;
   int* rstart = nullptr;
   int* rlist = nullptr;
-  long long nband = 0;                // nodes within nbnd of a side
+  std::vector<long long> nband;       // per block: nodes within nbnd of a side
   cudaStream_t side = nullptr;        // band kernel beside the interior adjoint kernel (high priority)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaStream_t copy = nullptr;        // stage-input copies beside the recomputed stage
   cudaEvent_t ev_cfork = nullptr, ev_cjoin = nullptr;
-  AdjMaps maps{};                     // TMA descriptors of the interior adjoint tiles
+  std::vector<AdjMaps> maps;          // per block: TMA descriptors of the interior adjoint tiles
   double* init_F = nullptr;          // initial fields (3 planes)
   double* init_DF = nullptr;
   double* ckpt = nullptr;            // checkpoints, 3 planes each
@@ -79,8 +79,8 @@ struct fdmap_adjoint {
   std::vector<long long> st_off;     // fault-register offset of each frictional interface in a checkpoint
   long long st_total = 0;
   double* init_st = nullptr;
-  double* psib = nullptr;            // Psibar, qbar'_Psi, dJ/dS0 per fault node
-  double* qpsib = nullptr;
+  double* psib[2] = {nullptr, nullptr};   // Psibar, qbar'_Psi per fault node (ubar parity)
+  double* qpsib[2] = {nullptr, nullptr};
   double* gS0 = nullptr;
   const double** recp[2] = {nullptr, nullptr};  // per receiver: vz in F[parity]
   std::vector<std::pair<int, long long>> rec_gen;  // (block, local index) per receiver
@@ -95,7 +95,9 @@ struct fdmap_adjoint {
   std::vector<void*> mem;
 
   long long stride() const { return 3 * h->hdom.blk[0].plane; }
-  long long slot_stride() const { return general ? total + nfault : stride(); }
+  // a stage slot: every block's 3 planes, then Psi of the fault nodes padded
+  // to an even count (the 4-D store map needs 16-byte slot strides)
+  long long slot_stride() const { return general ? total + ((nfault + 1) & ~1) : stride(); }
   long long ckpt_stride() const { return general ? total + st_total : stride(); }
   void free_graphs() {
     for (auto* set : {g_fwd, g_rec, g_adj})
@@ -156,24 +158,45 @@ int adj_encode(EncodeTiledFn enc, CUtensorMap* map, const double* base, const Bl
   return FDMAP_OK;
 }
 
+// 4-D FP64 map over the stage store of one block: (x, y, plane 0..2, slot),
+// slots `slot_stride` doubles apart; box {bx, by, 3, 1}
+int adj_encode_store(EncodeTiledFn enc, CUtensorMap* map, const double* base, const BlockGeom& g, long long slot_stride,
+                     long long nslots, int bx, int by) {
+  cuuint64_t dims[4] = {(cuuint64_t)g.pitch, (cuuint64_t)g.ny, 3, (cuuint64_t)nslots};
+  cuuint64_t strides[3] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8, (cuuint64_t)slot_stride * 8};
+  cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 3, 1};
+  cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return set_err(FDMAP_ERR_CUDA, "adjoint store tensor map (" + std::to_string((int)r) + ")");
+  return FDMAP_OK;
+}
+
 template <int PI_>
 int adj_maps_for(fdmap_adjoint* a) {
   using T = AdjTile<PI_>;
   fdmap_gpu* h = a->h;
-  const BlockGeom& g = h->geom[0];
   void* fn = nullptr;
   cudaDriverEntryPointQueryResult qr;
   CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr));
   if (!fn || qr != cudaDriverEntryPointSuccess) return set_err(FDMAP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
   EncodeTiledFn enc = (EncodeTiledFn)fn;
   int rc;
-  for (int q = 0; q < 2; ++q) {
-    if ((rc = adj_encode(enc, &a->maps.ub[q], a->ub[q], g, 3, T::WX, T::WY, 3))) return rc;
-    if ((rc = adj_encode(enc, &a->maps.qp[q], a->qp[q], g, 3, T::WX, T::WY, 3))) return rc;
+  a->maps.assign(a->nb, AdjMaps{});
+  for (int b = 0; b < a->nb; ++b) {
+    const BlockGeom& g = h->geom[b];
+    AdjMaps& m = a->maps[b];
+    for (int q = 0; q < 2; ++q) {
+      if ((rc = adj_encode(enc, &m.ub[q], a->ub[q] + a->boff[b], g, 3, T::WX, T::WY, 3))) return rc;
+      if ((rc = adj_encode(enc, &m.qp[q], a->qp[q] + a->boff[b], g, 3, T::WX, T::WY, 3))) return rc;
+    }
+    if ((rc = adj_encode_store(enc, &m.st, a->store + a->boff[b], g, a->slot_stride(), (long long)a->K * h->rk.nstage,
+                               T::WX, T::WY)))
+      return rc;
+    if ((rc = adj_encode(enc, &m.met, h->met_base[b], g, 5, T::WX, T::WY, 5))) return rc;
+    if ((rc = adj_encode(enc, &m.het, h->het_base[b], g, 2, T::WX, T::WY, 2))) return rc;
   }
-  if ((rc = adj_encode(enc, &a->maps.st, a->store, g, 3LL * a->K * h->rk.nstage, T::WX, T::WY, 3))) return rc;
-  if ((rc = adj_encode(enc, &a->maps.met, h->met_base[0], g, 5, T::WX, T::WY, 5))) return rc;
-  if ((rc = adj_encode(enc, &a->maps.het, h->het_base[0], g, 2, T::WX, T::WY, 2))) return rc;
   CUDA_TRY(cudaFuncSetAttribute(adj_stage_tma<PI_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM + 128));
   return FDMAP_OK;
 }
@@ -183,30 +206,48 @@ int adj_maps(fdmap_adjoint* a) {
   return pI == 1 ? adj_maps_for<1>(a) : (pI == 2 ? adj_maps_for<2>(a) : adj_maps_for<3>(a));
 }
 
-// interior tiles on the main stream, the band on a side stream (disjoint
-// nodes, same inputs), joined before the next stage; q = ubar / qbar' parity
-int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p, int q) {
+// one block's adjoint stage: interior tiles on the main stream, the band on
+// the side stream (disjoint nodes, same inputs); the caller forks and joins
+int adj_block_launch(fdmap_adjoint* a, const AdjStage& p, int q) {
   fdmap_gpu* h = a->h;
-  const DevBlock& B = h->hdom.blk[0];
+  const int b = p.blk;
+  const DevBlock& B = h->hdom.blk[b];
   dim3 blk(ATX * ATY), grid((B.nx + ATX - 1) / ATX, (B.ny + ATY - 1) / ATY);
-  const int bgrid = (int)((a->nband + BAND_NODES - 1) / BAND_NODES);
-  CUDA_TRY(cudaEventRecord(a->ev_fork, h->stream));
-  CUDA_TRY(cudaStreamWaitEvent(a->side, a->ev_fork, 0));
+  const long long nb = a->nband[b];
+  const int bgrid = (int)((nb + BAND_NODES - 1) / BAND_NODES);
+  const AdjMaps& m = a->maps[b];
   // the latency-bound band kernel goes first, at high priority, so its few CTAs
   // are placed before the interior tiles fill the SMs
   if (h->pI == 1) {
-    adj_band_kernel<1><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, a->nband);
-    adj_stage_tma<1><<<grid, blk, AdjTile<1>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
+    adj_band_kernel<1><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, nb);
+    adj_stage_tma<1><<<grid, blk, AdjTile<1>::SMEM + 128, h->stream>>>(h->hdom, p, m, q);
   } else if (h->pI == 2) {
-    adj_band_kernel<2><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, a->nband);
-    adj_stage_tma<2><<<grid, blk, AdjTile<2>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
+    adj_band_kernel<2><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, nb);
+    adj_stage_tma<2><<<grid, blk, AdjTile<2>::SMEM + 128, h->stream>>>(h->hdom, p, m, q);
   } else {
-    adj_band_kernel<3><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, a->nband);
-    adj_stage_tma<3><<<grid, blk, AdjTile<3>::SMEM + 128, h->stream>>>(h->hdom, p, a->maps, q);
+    adj_band_kernel<3><<<bgrid, 2 * BAND_NODES, 0, a->side>>>(h->hdom, p, nb);
+    adj_stage_tma<3><<<grid, blk, AdjTile<3>::SMEM + 128, h->stream>>>(h->hdom, p, m, q);
   }
   CUDA_TRY(cudaGetLastError());
+  return FDMAP_OK;
+}
+
+int adj_fork(fdmap_adjoint* a) {
+  CUDA_TRY(cudaEventRecord(a->ev_fork, a->h->stream));
+  CUDA_TRY(cudaStreamWaitEvent(a->side, a->ev_fork, 0));
+  return FDMAP_OK;
+}
+
+int adj_join(fdmap_adjoint* a) {
   CUDA_TRY(cudaEventRecord(a->ev_join, a->side));
-  CUDA_TRY(cudaStreamWaitEvent(h->stream, a->ev_join, 0));
+  CUDA_TRY(cudaStreamWaitEvent(a->h->stream, a->ev_join, 0));
+  return FDMAP_OK;
+}
+
+// single block: interior tiles and band, joined before the next stage; q = ubar / qbar' parity
+int adj_stage_launch(fdmap_adjoint* a, const AdjStage& p, int q) {
+  int rc;
+  if ((rc = adj_fork(a)) || (rc = adj_block_launch(a, p, q)) || (rc = adj_join(a))) return rc;
   return FDMAP_OK;
 }
 
@@ -268,11 +309,13 @@ int capture(fdmap_adjoint* a, cudaGraphExec_t* out, const std::function<int()>& 
   return rc;
 }
 
-// one adjoint stage of the general path: every block, then the fault nodes
+// one adjoint stage of the general path: every block (tiles and band), then
+// the fault nodes
 int gen_stage_launch(fdmap_adjoint* a, int s, double dt, int q) {
   fdmap_gpu* h = a->h;
+  int rc = adj_fork(a);
+  if (rc) return rc;
   for (int b = 0; b < a->nb; ++b) {
-    const DevBlock& B = h->hdom.blk[b];
     AdjStage p{};
     p.A = h->rk.A[s];
     p.Bdt = h->rk.B[s] * dt;
@@ -288,13 +331,9 @@ int gen_stage_launch(fdmap_adjoint* a, int s, double dt, int q) {
     p.grho = a->grho + a->goff[b];
     p.gG = a->gG + a->goff[b];
     p.blk = b;
-    const int grid = (int)(((long long)B.nx * B.ny + 127) / 128);
-    if (h->pI == 1) adj_block_kernel<1><<<grid, 128, 0, h->stream>>>(h->hdom, p);
-    else if (h->pI == 2) adj_block_kernel<2><<<grid, 128, 0, h->stream>>>(h->hdom, p);
-    else adj_block_kernel<3><<<grid, 128, 0, h->stream>>>(h->hdom, p);
-    CUDA_TRY(cudaGetLastError());
+    if ((rc = adj_block_launch(a, p, q))) return rc;
   }
-  if (a->nfault == 0) return FDMAP_OK;
+  if (a->nfault == 0) return adj_join(a);
   AdjFaultArgs f{};
   f.A = h->rk.A[s];
   f.Bdt = h->rk.B[s] * dt;
@@ -310,8 +349,10 @@ int gen_stage_launch(fdmap_adjoint* a, int s, double dt, int q) {
   f.slot_stride = a->slot_stride();
   f.psi_off = a->total;
   f.ck = a->clock;
-  f.psib = a->psib;
-  f.qpsib = a->qpsib;
+  f.psib_in = a->psib[q];
+  f.qpsib_in = a->qpsib[q];
+  f.psib_out = a->psib[1 - q];
+  f.qpsib_out = a->qpsib[1 - q];
   f.grho = a->grho;
   f.gG = a->gG;
   f.gS0 = a->gS0;
@@ -322,9 +363,12 @@ int gen_stage_launch(fdmap_adjoint* a, int s, double dt, int q) {
     f.boff[b] = a->boff[b];
     f.goff[b] = a->goff[b];
   }
-  adj_fault_kernel<<<(a->nfault + 63) / 64, 64, 0, h->stream>>>(h->hdom, f);
+  // on the side stream after the band kernels: the fault nodes write only
+  // edge nodes, which no interior tile touches
+  const long long thr = (long long)a->nfault * FAULT_LANES;
+  adj_fault_kernel<<<(int)((thr + 127) / 128), 128, 0, a->side>>>(h->hdom, f);
   CUDA_TRY(cudaGetLastError());
-  return FDMAP_OK;
+  return adj_join(a);
 }
 
 int build_graphs(fdmap_adjoint* a, double dt) {
@@ -536,7 +580,8 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
     a->total += 3 * gb.plane;
     a->gtotal += gb.plane;
   }
-  a->nband = 2LL * nbnd * g.nx + 2LL * nbnd * (g.ny - 2 * nbnd);
+  for (int b = 0; b < a->nb; ++b)
+    a->nband.push_back(2LL * nbnd * h->geom[b].nx + 2LL * nbnd * (h->geom[b].ny - 2 * nbnd));
   for (int i = 0; i < d->nifaces; ++i) {
     const fdmap_iface& fi = d->ifaces[i];
     const int n = fi.p - fi.m + 1;
@@ -581,7 +626,8 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
     return fail(rc);
   if (a->general) {
     if ((rc = a->alloc(&a->init_st, std::max<long long>(a->st_total, 1))) ||
-        (rc = a->alloc(&a->psib, std::max(a->nfault, 1))) || (rc = a->alloc(&a->qpsib, std::max(a->nfault, 1))) ||
+        (rc = a->alloc(&a->psib[0], std::max(a->nfault, 1))) || (rc = a->alloc(&a->qpsib[0], std::max(a->nfault, 1))) ||
+        (rc = a->alloc(&a->psib[1], std::max(a->nfault, 1))) || (rc = a->alloc(&a->qpsib[1], std::max(a->nfault, 1))) ||
         (rc = a->alloc(&a->gS0, std::max(a->nfault, 1))) || (rc = a->alloc(&a->recp[0], nrec)) ||
         (rc = a->alloc(&a->recp[1], nrec)))
       return fail(rc);
@@ -674,7 +720,7 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
         cudaSuccess)
       return fail(set_err(FDMAP_ERR_CUDA, "interface table upload"));
   }
-  if (!a->general && (rc = adj_maps(a))) return fail(rc);
+  if ((rc = adj_maps(a))) return fail(rc);
   *out = a;
   return FDMAP_OK;
 }
@@ -781,8 +827,10 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
   CUDA_TRY(cudaMemsetAsync(a->grho, 0, plane_bytes, h->stream));
   CUDA_TRY(cudaMemsetAsync(a->gG, 0, plane_bytes, h->stream));
   if (a->nfault > 0) {
-    CUDA_TRY(cudaMemsetAsync(a->psib, 0, a->nfault * sizeof(double), h->stream));
-    CUDA_TRY(cudaMemsetAsync(a->qpsib, 0, a->nfault * sizeof(double), h->stream));
+    for (int q = 0; q < 2; ++q) {
+      CUDA_TRY(cudaMemsetAsync(a->psib[q], 0, a->nfault * sizeof(double), h->stream));
+      CUDA_TRY(cudaMemsetAsync(a->qpsib[q], 0, a->nfault * sizeof(double), h->stream));
+    }
     CUDA_TRY(cudaMemsetAsync(a->gS0, 0, a->nfault * sizeof(double), h->stream));
   }
   // dJ/dU^N at the receivers

@@ -241,8 +241,10 @@ struct AdjFaultArgs {
   const double* store;            // stage inputs: slot (rel*nstage + s), slot_stride doubles each
   long long slot_stride, psi_off; // Psi of the fault nodes at psi_off within a slot
   const AdjClock* ck;
-  double* psib;                   // Psibar, qbar'_Psi per fault node
-  double* qpsib;
+  const double* psib_in;          // Psibar, qbar'_Psi per fault node (ping-pong with the stage)
+  const double* qpsib_in;
+  double* psib_out;
+  double* qpsib_out;
   double* grho;                   // gradient planes of all blocks (concatenated)
   double* gG;
   double* gS0;                    // dJ/dS0 per fault node
@@ -252,10 +254,15 @@ struct AdjFaultArgs {
   long long goff[MAX_BLOCKS];     // block offsets in the gradient planes
 };
 
-// one thread per fault node, after every block's adjoint stage
-__global__ void __launch_bounds__(64) adj_fault_kernel(const __grid_constant__ DevDomain D, AdjFaultArgs p) {
-  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (tid >= p.nfault) return;
+// FAULT_LANES threads per fault node, lane j forms the adjoint of input j
+// (lanes past FX_N idle); after the band kernels of every block, beside the
+// interior tiles (fault nodes touch only edge nodes, which are band nodes)
+constexpr int FAULT_LANES = 16;
+
+__global__ void __launch_bounds__(128) adj_fault_kernel(const __grid_constant__ DevDomain D, AdjFaultArgs p) {
+  const long long gt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int tid = (int)(gt / FAULT_LANES), lane = (int)(gt % FAULT_LANES);
+  if (tid >= p.nfault || lane >= FX_N) return;
   int q = 0;
   while (q + 1 < p.nifc && tid >= p.info[q + 1].start) ++q;
   const AdjIfaceInfo& inf = p.info[q];
@@ -327,77 +334,34 @@ __global__ void __launch_bounds__(64) adj_fault_kernel(const __grid_constant__ D
   }
   double psib = 0.0, qs_psi = 0.0;
   if (c.friction) {
-    psib = p.psib[tid];
-    qs_psi = p.qpsib[tid] + p.Bdt * psib;
+    psib = p.psib_in[tid];
+    qs_psi = p.qpsib_in[tid] + p.Bdt * psib;
   }
   yb[FY_PSI] = qs_psi;
+  // the Newton root from the values, then this lane's tangent
   double V0 = 0.0;
   Dn y[FY_N];
-  fault_map3(I.fr, n, k, c, x, true, V0, y);
-  double xb[FX_N];
-  for (int j = 0; j < FX_N; ++j) {
-    xb[j] = 0.0;
-    if (!c.friction && (j == FX_PSI || j == FX_S0)) continue;
-    x[j].d = 1.0;
+  const bool active = c.friction || (lane != FX_PSI && lane != FX_S0);
+  double xb = 0.0;
+  if (active) {
+    fault_map3(I.fr, n, k, c, x, true, V0, y);
+    x[lane].d = 1.0;
     fault_map3(I.fr, n, k, c, x, false, V0, y);
-    x[j].d = 0.0;
-    double s = 0.0;
 #pragma unroll
-    for (int o = 0; o < FY_N; ++o) s += yb[o] * y[o].d;
-    xb[j] = s;
+    for (int o = 0; o < FY_N; ++o) xb += yb[o] * y[o].d;
   }
-#pragma unroll
-  for (int l = 0; l < 3; ++l) {
-    p.ub_out[om + l * Bm.plane] += xb[FX_UM + l];
-    p.ub_out[op + l * Bp.plane] += xb[FX_UP + l];
-  }
-  p.grho[p.goff[im] + cm] += xb[FX_RHOM];
-  p.gG[p.goff[im] + cm] += xb[FX_GM];
-  p.grho[p.goff[ip] + cp] += xb[FX_RHOP];
-  p.gG[p.goff[ip] + cp] += xb[FX_GP];
-  if (c.friction) {
-    p.psib[tid] = psib + xb[FX_PSI];
-    p.qpsib[tid] = p.A * qs_psi;
-    p.gS0[tid] += xb[FX_S0];
-  }
-}
-
-// every node of block p.blk: both directions in one thread (the general
-// multi-block path; the single-block path tiles the interior with TMA)
-template <int PI_>
-__global__ void __launch_bounds__(128) adj_block_kernel(const __grid_constant__ DevDomain D, AdjStage p) {
-  const DevBlock& B = D.blk[p.blk];
-  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= (long long)B.nx * B.ny) return;
-  const int j = (int)(q / B.nx), i = (int)(q % B.nx);
-  double acc[3], phi[3], grho, gG, acc1[3], phi1[3], grho1, gG1;
-  adj_node_part<PI_>(D, p, i, j, 0, acc, phi, grho, gG);
-  adj_node_part<PI_>(D, p, i, j, 1, acc1, phi1, grho1, gG1);
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    acc[f] += acc1[f];
-    phi[f] += phi1[f];
-  }
-  grho += grho1;
-  gG += gG1;
-  const long long plane = B.plane;
-  const long long c = (long long)j * B.pitch + i;
-  double lam[3], ubc[3];
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    ubc[f] = p.ub_in[f * plane + c];
-    lam[f] = p.qp_in[f * plane + c] + p.Bdt * ubc[f];
-  }
-  const double Ji = B.Ji[c], rinv = 1.0 / B.rho[c];
-  grho -= lam[0] * (phi[0] * Ji) * (rinv * rinv);
-  gG += lam[1] * (phi[1] * Ji) + lam[2] * (phi[2] * Ji);
-  p.grho[c] += grho;
-  p.gG[c] += gG;
-#pragma unroll
-  for (int f = 0; f < 3; ++f) {
-    p.ub_out[f * plane + c] = ubc[f] + acc[f];
-    p.qp_out[f * plane + c] = p.A * lam[f];
-  }
+  // every lane owns the elements it writes
+  if (lane < FX_UP) p.ub_out[om + (lane - FX_UM) * Bm.plane] += xb;
+  else if (lane < FX_PSI) p.ub_out[op + (lane - FX_UP) * Bp.plane] += xb;
+  else if (lane == FX_PSI) {
+    p.psib_out[tid] = psib + xb;
+    p.qpsib_out[tid] = p.A * qs_psi;
+  } else if (lane == FX_S0) {
+    if (c.friction) p.gS0[tid] += xb;
+  } else if (lane == FX_RHOM) p.grho[p.goff[im] + cm] += xb;
+  else if (lane == FX_GM) p.gG[p.goff[im] + cm] += xb;
+  else if (lane == FX_RHOP) p.grho[p.goff[ip] + cp] += xb;
+  else p.gG[p.goff[ip] + cp] += xb;
 }
 
 // Psi of every frictional fault node -> its place in stage slot (rel*nstage + s)

@@ -205,6 +205,15 @@ __device__ __forceinline__ void adj_node_part(const DevDomain& D, const AdjStage
 
 constexpr int ATX = 32, ATY = 8;
 
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, int x, int y, int z, int w,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+      ::"r"(smem_u32(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(w),
+      "r"(smem_u32(bar))
+      : "memory");
+}
+
 
 // nodes within nbnd of a side use closure rows somewhere in their gather or
 // their own rates: the band handled by adj_band_kernel
@@ -238,7 +247,7 @@ __global__ void __launch_bounds__(2 * BAND_NODES) adj_band_kernel(const __grid_c
   const int part = threadIdx.x / BAND_NODES, slot = threadIdx.x % BAND_NODES;
   const long long q = (long long)blockIdx.x * BAND_NODES + slot;
   const bool valid = q < nband;
-  const DevBlock& B = D.blk[0];
+  const DevBlock& B = D.blk[p.blk];
   int i = 0, j = 0;
   double acc[3], phi[3], grho = 0.0, gG = 0.0;
   if (valid) {
@@ -346,7 +355,7 @@ __global__ void adj_forward_advance(TimeState* ts, AdjClock* ck) {
 struct AdjMaps {
   CUtensorMap ub[2];  // ubar buffers, box {WX, WY, 3}
   CUtensorMap qp[2];  // qbar' buffers, box {WX, WY, 3}
-  CUtensorMap st;     // stage-input store (3 planes per slot), box {WX, WY, 3}
+  CUtensorMap st;     // stage-input store: 4-D (x, y, plane, slot), box {WX, WY, 3, 1}
   CUtensorMap met;    // yr, xr, yq, xq, Ji, box {WX, WY, 5}
   CUtensorMap het;    // rho, G, box {WX, WY, 2}
 };
@@ -374,7 +383,7 @@ __global__ void __launch_bounds__(ATX* ATY) adj_stage_tma(const __grid_constant_
   extern __shared__ unsigned char adj_smem_raw[];
   double* sm = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(adj_smem_raw) + 127) & ~uintptr_t(127));
   __shared__ unsigned long long bar;
-  const DevBlock& B = D.blk[0];
+  const DevBlock& B = D.blk[p.blk];
   const int nx = B.nx, ny = B.ny;
   const int i0 = blockIdx.x * ATX, j0 = blockIdx.y * ATY;
   const int tx = threadIdx.x % ATX, ty = threadIdx.x / ATX;
@@ -386,11 +395,11 @@ __global__ void __launch_bounds__(ATX* ATY) adj_stage_tma(const __grid_constant_
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fence_proxy_async();
     const int x = i0 - T::HX, y = j0 - T::HY;
-    const int slot = (int)((*p.rel) * p.nstage + p.s) * 3;
+    const int slot = (int)((*p.rel) * p.nstage + p.s);
     mbar_arrive_tx(&bar, T::BYTES);
     tma_load_3d(&P(T::QP, 0, 0, 0), &maps.qp[q], x, y, 0, &bar);
     tma_load_3d(&P(T::UB, 0, 0, 0), &maps.ub[q], x, y, 0, &bar);
-    tma_load_3d(&P(T::ST, 0, 0, 0), &maps.st, x, y, slot, &bar);
+    tma_load_4d(&P(T::ST, 0, 0, 0), &maps.st, x, y, 0, slot, &bar);
     tma_load_3d(&P(T::MET, 0, 0, 0), &maps.met, x, y, 0, &bar);
     tma_load_3d(&P(T::HET, 0, 0, 0), &maps.het, x, y, 0, &bar);
   }
