@@ -376,6 +376,13 @@ module fdmap_gpu_mod
        real(c_double), intent(out) :: grad_rho(*), grad_G(*)
      end function fdmap_gpu_adjoint_backward
 
+     integer(c_int) function fdmap_gpu_adjoint_time_params(a, params, nt) bind(C, name='fdmap_gpu_adjoint_time_params')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: a
+       real(c_double), intent(out) :: params(5)     ! t0, dt, CFL, hmin, hmax
+       integer(c_int), intent(out) :: nt
+     end function fdmap_gpu_adjoint_time_params
+
      integer(c_int) function fdmap_gpu_adjoint_fault_size(a) bind(C, name='fdmap_gpu_adjoint_fault_size')
        import :: c_int, c_ptr
        type(c_ptr), value :: a
