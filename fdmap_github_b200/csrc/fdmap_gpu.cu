@@ -68,6 +68,22 @@ __global__ void gather_block(const double* __restrict__ src, double* __restrict_
 }
 // end of a replayed step: advance the device step clock
 __global__ void advance_step(TimeState* ts) { ts->n += 1; }
+
+// non-finite values among nF planes of nx x ny nodes (row pitch, plane
+// stride), added to *count once per warp
+__global__ void count_nonfinite_block(const double* __restrict__ F, int nx, int ny, long long pitch, long long plane,
+                                      int nF, unsigned long long* count) {
+  const long long n = (long long)nF * ny * nx;
+  unsigned c = 0;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(t % nx);
+    const long long r = t / nx;
+    const int j = (int)(r % ny), l = (int)(r / ny);
+    if (!isfinite(F[l * plane + (long long)j * pitch + i])) ++c;
+  }
+  for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
+}
 // start of a replayed sequence: set the step clock (by value, no host buffer to keep alive)
 __global__ void set_step_clock(TimeState* ts, double t_start, double dt, long long n) {
   ts->t_start = t_start;
@@ -1255,7 +1271,37 @@ int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures) {
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   CUDA_TRY(cudaMemcpy(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost));
   if (newton_failures) *newton_failures = (long long)st[0];
+  if (st[1] & 2ull) return set_err(FDMAP_ERR_TIMEOUT, "a bounded device wait gave up");
   return st[0] ? FDMAP_ERR_NEWTON_NOCONV : FDMAP_OK;
+}
+
+int fdmap_gpu_check_finite(fdmap_gpu* h, long long* count) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  unsigned long long* d_count = h->d_status + 2;  // scratch word of the status block
+  CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), h->stream));
+  for (int b = 0; b < h->hdom.nblocks; ++b) {
+    const DevBlock& B = h->hdom.blk[b];
+    const long long n = (long long)h->nF * B.ny * B.nx;
+    count_nonfinite_block<<<(int)std::min<long long>((n + 255) / 256, 4 * 148), 256, 0, h->stream>>>(
+        B.F[h->cur], B.nx, B.ny, B.pitch, B.plane, h->nF, d_count);
+    CUDA_TRY(cudaGetLastError());
+  }
+  for (int i = 0; i < h->hdom.nifaces; ++i) {
+    const DevIface& I = h->hdom.ifc[i];
+    if (I.coupling != FDMAP_COUPLING_FRICTION) continue;
+    const int fields[3] = {ST_V, ST_S, ST_PSI};
+    for (int f : fields) {
+      count_nonfinite_block<<<(I.n + 255) / 256, 256, 0, h->stream>>>(I.fr.st + (size_t)f * I.n, I.n, 1, I.n, I.n, 1,
+                                                                      d_count);
+      CUDA_TRY(cudaGetLastError());
+    }
+  }
+  unsigned long long c = 0;
+  CUDA_TRY(cudaMemcpyAsync(&c, d_count, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (count) *count = (long long)c;
+  return c ? set_err(FDMAP_ERR_NONFINITE, std::to_string(c) + " non-finite values") : FDMAP_OK;
 }
 
 int fdmap_gpu_set_stream(fdmap_gpu* h, void* stream) {

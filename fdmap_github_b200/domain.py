@@ -319,6 +319,15 @@ class GpuDomain:
         lib().fdmap_gpu_status(self._g, C.byref(n))
         return n.value
 
+    def nonfinite_count(self) -> int:
+        """Non-finite values in the body fields and the fault V, S, Psi
+        (fdmap_gpu_check_finite, which returns FDMAP_ERR_NONFINITE when any)."""
+        n = C.c_longlong()
+        rc = lib().fdmap_gpu_check_finite(self._g, C.byref(n))
+        if rc not in (0, -3):
+            check_gpu(rc, "fdmap_gpu_check_finite")
+        return n.value
+
     def launch_count(self) -> int:
         return lib().fdmap_gpu_launch_count(self._g)
 

@@ -70,6 +70,7 @@ SIGNATURES = {
     "fdmap_gpu_set_fault": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_get_fhat": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_status": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_check_finite": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
     "fdmap_gpu_time_params": (C.c_int, [_VP, _DP, C.POINTER(C.c_int)]),
     "fdmap_gpu_get_metric": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_get_side_impedance": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),

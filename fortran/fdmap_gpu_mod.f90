@@ -178,6 +178,12 @@ module fdmap_gpu_mod
        integer(c_long_long), intent(out) :: newton_failures
      end function fdmap_gpu_status
 
+     integer(c_int) function fdmap_gpu_check_finite(h, count) bind(C, name='fdmap_gpu_check_finite')
+       import :: c_int, c_ptr, c_long_long
+       type(c_ptr), value :: h
+       integer(c_long_long), intent(out) :: count   ! returns FDMAP_ERR_NONFINITE (-3) when count > 0
+     end function fdmap_gpu_check_finite
+
      integer(c_int) function fdmap_gpu_time_params(h, params, nt) bind(C, name='fdmap_gpu_time_params')
        import :: c_int, c_ptr, c_double
        type(c_ptr), value :: h

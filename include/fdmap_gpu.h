@@ -118,8 +118,17 @@ int fdmap_gpu_set_side_displacement(fdmap_gpu* h, int b, int s, const double* U,
  * of block b as the engine holds them (init_edges, domain.f90:1349-1459). */
 int fdmap_gpu_get_side_impedance(fdmap_gpu* h, int b, int s, double* out);
 
-/* Device status: Newton failures so far (the reference stops on the first). */
+/* Device status: Newton failures so far (the reference stops on the first,
+ * friction.f90:1012-1036).  Returns FDMAP_ERR_TIMEOUT if a bounded device wait
+ * (a TMA pipeline barrier) gave up, else FDMAP_ERR_NEWTON_NOCONV if the
+ * solver failed somewhere, else FDMAP_OK. */
 int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
+
+/* Counts the non-finite values (NaN, +-Inf) in the current body fields of
+ * every block and in the slip rate, shear stress and state of every
+ * frictional interface, on the device; FDMAP_ERR_NONFINITE if there are any.
+ * count may be NULL. */
+int fdmap_gpu_check_finite(fdmap_gpu* h, long long* count);
 
 /* ------------------------------------------------------------------------
  * Device-side output (write_output, output.f90:990-1060).  An item samples
