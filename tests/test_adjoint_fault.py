@@ -191,3 +191,14 @@ def test_fault_nodes_carry_material_gradient(require_gpu, tmp_path):
     m = h.ny // 2
     for row in (m - 1, m):  # edge rows of the two blocks
         assert np.any(g_G[row] != 0.0) and np.any(g_rho[row] != 0.0)
+
+
+def test_adjoint_rejects_dissipation(tmp_path):
+    """The backward pass has no dissipative terms, so a dissipative block is refused."""
+    text = problems.heterogeneous_ricker(tmp_path, n=31, h=0.1, nt=5)
+    text = text.replace("&material_list heterogeneous=T", "&operator_list Cdiss=0.2d0 /\n&material_list heterogeneous=T")
+    h = init_domain(text, tmp_path)
+    assert h.block_cdiss(0) > 0
+    with pytest.raises(FdmapError) as e:
+        GpuAdjoint(h, [(5, 31)])
+    assert e.value.code == -6
