@@ -78,6 +78,45 @@ def test_uniform_medium_dissipation_is_the_homogeneous_dissipation(tmp_path, mod
     np.testing.assert_allclose(Fa, Fb, rtol=0, atol=1e-12 * np.abs(Fb).max())
 
 
+def _sbp4_norm(n):
+    """Diagonal SBP4 norm with unit spacing (boundary weights 17/48, 59/48,
+    43/48, 49/48, interior 1)."""
+    w = np.ones(n)
+    hl = [17 / 48, 59 / 48, 43 / 48, 49 / 48]
+    w[:4] = hl
+    w[-4:] = hl[::-1]
+    return w
+
+
+@pytest.mark.parametrize("cdiss", [0.0, 0.4])
+def test_heterogeneous_energy_does_not_grow(tmp_path, cdiss):
+    """SBP-SAT energy of a heterogeneous mode III medium with absorbing sides,
+    E = 1/2 sum H J (rho vz^2 + (sxz^2 + syz^2)/G), never grows from step to
+    step, with or without the dissipative rates."""
+    from oracle.binding import OracleDomain
+
+    h = init_domain(_diss_text(tmp_path, 41, 3, cdiss=cdiss, seed=4), tmp_path)
+    o = OracleDomain(h)
+    rho, G, J = h.array("rho")[0], h.array("G")[0], h.array("J")[0]
+    W = np.outer(_sbp4_norm(h.ny), _sbp4_norm(h.nx)) * J
+    E = []
+    for n in range(1, 61):
+        F = o.get_fields()[0]
+        E.append(0.5 * np.sum(W * (rho * F[0] ** 2 + (F[1] ** 2 + F[2] ** 2) / G)))
+        o.run(n, n, nt=1 << 30)
+    E = np.array(E)
+    assert E[0] > 0
+    assert np.all(np.diff(E) <= 1e-13 * E[0])
+    if cdiss > 0:
+        # the dissipative rates remove energy the plain rates keep
+        h0 = init_domain(_diss_text(tmp_path, 41, 3, cdiss=0.0, seed=4), tmp_path)
+        o0 = OracleDomain(h0)
+        o0.run(1, 59, nt=1 << 30)
+        F0 = o0.get_fields()[0]
+        E0 = 0.5 * np.sum(W * (rho * F0[0] ** 2 + (F0[1] ** 2 + F0[2] ** 2) / G))
+        assert E[-1] < E0
+
+
 def test_dissipation_damps_a_heterogeneous_medium(tmp_path):
     """The dissipative rates remove energy that the plain rates keep."""
     _, o_d = _oracle(_diss_text(tmp_path, 41, 3, seed=4, cdiss=0.6), tmp_path, 40)
