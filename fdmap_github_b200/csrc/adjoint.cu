@@ -95,9 +95,11 @@ struct fdmap_adjoint {
   std::vector<void*> mem;
 
   long long stride() const { return 3 * h->hdom.blk[0].plane; }
-  // a stage slot: every block's 3 planes, then Psi of the fault nodes padded
-  // to an even count (the 4-D store map needs 16-byte slot strides)
-  long long slot_stride() const { return general ? total + ((nfault + 1) & ~1) : stride(); }
+  // a stage slot: every block's 3 planes, then Psi and the converged slip rate
+  // of the fault nodes, each padded to an even count (the 4-D store map needs
+  // 16-byte slot strides)
+  long long fault_pad() const { return (nfault + 1) & ~1; }
+  long long slot_stride() const { return general ? total + 2 * fault_pad() : stride(); }
   long long ckpt_stride() const { return general ? total + st_total : stride(); }
   void free_graphs() {
     for (auto* set : {g_fwd, g_rec, g_adj})
@@ -263,8 +265,8 @@ int forward_step_stages(fdmap_adjoint* a, int cur, double dt, bool stash) {
       if (a->nfault > 0) {
         // the stage updates Psi in place: its copy goes first, on the stage's stream
         adj_stash_psi<<<(a->nfault + 127) / 128, 128, 0, h->stream>>>(
-            h->hdom, a->info, (int)a->info_host.size(), a->nfault, a->store, slot, a->total, &a->clock->rel, s,
-            h->rk.nstage);
+            h->hdom, a->info, (int)a->info_host.size(), a->nfault, a->store, slot, a->total, a->total + a->fault_pad(),
+            &a->clock->rel, s, h->rk.nstage, 1);
         CUDA_TRY(cudaGetLastError());
       }
       CUDA_TRY(cudaEventRecord(a->ev_cfork, h->stream));
@@ -289,6 +291,13 @@ int forward_step_stages(fdmap_adjoint* a, int cur, double dt, bool stash) {
     int rc = engine_stage(h, st);
     if (rc) return rc;
     cur = 1 - cur;
+  }
+  if (stash && a->nfault > 0) {
+    // the slip rate the last stage converged to
+    adj_stash_psi<<<(a->nfault + 127) / 128, 128, 0, h->stream>>>(
+        h->hdom, a->info, (int)a->info_host.size(), a->nfault, a->store, slot, a->total, a->total + a->fault_pad(),
+        &a->clock->rel, h->rk.nstage - 1, h->rk.nstage, 0);
+    CUDA_TRY(cudaGetLastError());
   }
   if (stash) CUDA_TRY(cudaStreamWaitEvent(h->stream, a->ev_cjoin, 0));
   return FDMAP_OK;
@@ -348,6 +357,7 @@ int gen_stage_launch(fdmap_adjoint* a, int s, double dt, int q) {
   f.store = a->store;
   f.slot_stride = a->slot_stride();
   f.psi_off = a->total;
+  f.v_off = a->total + a->fault_pad();
   f.ck = a->clock;
   f.psib_in = a->psib[q];
   f.qpsib_in = a->qpsib[q];

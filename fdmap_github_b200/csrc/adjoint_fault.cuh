@@ -240,6 +240,7 @@ struct AdjFaultArgs {
   double* ub_out;                 // written by the block kernels, the interface terms are added
   const double* store;            // stage inputs: slot (rel*nstage + s), slot_stride doubles each
   long long slot_stride, psi_off; // Psi of the fault nodes at psi_off within a slot
+  long long v_off;                // the stage's converged slip rate at v_off
   const AdjClock* ck;
   const double* psib_in;          // Psibar, qbar'_Psi per fault node (ping-pong with the stage)
   const double* qpsib_in;
@@ -338,13 +339,13 @@ __global__ void __launch_bounds__(128) adj_fault_kernel(const __grid_constant__ 
     qs_psi = p.qpsib_in[tid] + p.Bdt * psib;
   }
   yb[FY_PSI] = qs_psi;
-  // the Newton root from the values, then this lane's tangent
-  double V0 = 0.0;
+  // the root the forward's Newton solve converged to in this stage, then this
+  // lane's tangent through one Newton step from it
+  double V0 = c.friction ? p.store[slot + p.v_off + tid] : 0.0;
   Dn y[FY_N];
   const bool active = c.friction || (lane != FX_PSI && lane != FX_S0);
   double xb = 0.0;
   if (active) {
-    fault_map3(I.fr, n, k, c, x, true, V0, y);
     x[lane].d = 1.0;
     fault_map3(I.fr, n, k, c, x, false, V0, y);
 #pragma unroll
@@ -365,17 +366,27 @@ __global__ void __launch_bounds__(128) adj_fault_kernel(const __grid_constant__ 
 }
 
 // Psi of every frictional fault node -> its place in stage slot (rel*nstage + s)
+// With psi: Psi before stage s into slot (rel*nstage + s), and the slip rate
+// the previous stage converged to into slot (rel*nstage + s - 1) when s > 0.
+// Without psi (after the last stage): only that stage's slip rate, slot
+// (rel*nstage + s).  Nodes of locked interfaces store 0.
 __global__ void adj_stash_psi(const __grid_constant__ DevDomain D, const AdjIfaceInfo* info, int nifc, int nfault,
-                              double* store, long long slot_stride, long long psi_off, const long long* rel, int s,
-                              int nstage) {
+                              double* store, long long slot_stride, long long psi_off, long long v_off,
+                              const long long* rel, int s, int nstage, int psi) {
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= nfault) return;
   int q = 0;
   while (q + 1 < nifc && tid >= info[q + 1].start) ++q;
   const DevIface& I = D.ifc[info[q].iface];
   const int k = tid - info[q].start;
-  store[((*rel) * nstage + s) * slot_stride + psi_off + tid] =
-      I.coupling == FDMAP_COUPLING_LOCKED ? 0.0 : I.fr.st[ST_PSI * I.n + k];
+  const bool locked = I.coupling == FDMAP_COUPLING_LOCKED;
+  const long long base = (*rel) * nstage;
+  if (psi) {
+    store[(base + s) * slot_stride + psi_off + tid] = locked ? 0.0 : I.fr.st[ST_PSI * I.n + k];
+    if (s > 0) store[(base + s - 1) * slot_stride + v_off + tid] = locked ? 0.0 : I.fr.st[ST_V * I.n + k];
+  } else {
+    store[(base + s) * slot_stride + v_off + tid] = locked ? 0.0 : I.fr.st[ST_V * I.n + k];
+  }
 }
 
 // vz at the receivers (one pointer per receiver into the state) for sample ts->n
