@@ -404,7 +404,12 @@ __global__ void __launch_bounds__(ATX* ATY) adj_stage_tma(const __grid_constant_
     tma_load_3d(&P(T::HET, 0, 0, 0), &maps.het, x, y, 0, &bar);
   }
   __syncthreads();
-  mbar_wait_bounded(&bar, 0, D.status);
+  if (__syncthreads_or(!mbar_wait_bounded(&bar, 0, D.status))) {
+    // the tile never arrived: no compute; wait once more for the copies before leaving
+    if (threadIdx.x == 0) mbar_wait_bounded(&bar, 0, D.status);
+    __syncthreads();
+    return;
+  }
   const int X0 = tx + T::HX, Y0 = ty + T::HY;
   const bool mine = adj_node_interior(i0 + tx, j0 + ty, nx, ny, nbnd);
   double lam[3], ubc[3];

@@ -123,7 +123,9 @@ struct DevDomain {
   int seg_b[4 * MAX_BLOCKS + MAX_IFACES];      // side (BC)
   int seg_start[4 * MAX_BLOCKS + MAX_IFACES + 1];
   fdmap_source src;
-  unsigned long long* status;  // [0] Newton failures, [1] nonfinite flags
+  unsigned long long* status;  // [0] Newton failures (first attempt), [1] flags (bit 1: a bounded wait gave up),
+                               // [2] scratch of fdmap_gpu_check_finite, [3] Newton retries that failed too
+  int newton_imax;             // Newton iteration limit (friction.f90:924 imax = 99; lowered only by tests)
   const double* energy;        // [nblocks + 1] stage-1 mechanical energy (energy_balance = T), or NULL
 };
 

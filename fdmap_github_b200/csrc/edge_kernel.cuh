@@ -89,9 +89,10 @@ __device__ __forceinline__ void d_strength(int law, const DRS& rs, double V, dou
 }
 
 // newton_solver (friction.f90:909-1038): bracketed Newton with log-bisection.
-// Returns true on failure (imax iterations without meeting atolR).
-static __device__ bool d_newton(int law, const DRS& rs, double& V, double& S, double Slock, double N, double eta, double Psi) {
-  const int imax = 99;
+// Returns true on failure (imax iterations without meeting atolR).  imax is
+// the reference's 99 (friction.f90:924) unless the host lowered it.
+static __device__ bool d_newton(int law, const DRS& rs, double& V, double& S, double Slock, double N, double eta, double Psi,
+                                int imax = 99) {
   const double atolR = 2.220446049250313e-16 * 1e4;
   double Vmin = fmin(0.0, Slock / eta);
   double Vmax = fmax(0.0, Slock / eta);
@@ -176,7 +177,7 @@ struct NodeState {
 
 static __device__ void d_solve_friction(const DevFriction& FR, int n, int k, NodeState& st, double S0, double N0, double phip,
                                  double phis, double eta, double x, double y, double t, double dt,
-                                 unsigned long long* status) {
+                                 unsigned long long* status, int imax) {
   d_load_stress(FR, n, k, x, y, t, st.S0, st.N0);
   st.S0 = st.S0 + S0;
   st.N0 = st.N0 + N0;
@@ -219,8 +220,11 @@ static __device__ void d_solve_friction(const DevFriction& FR, int n, int k, Nod
   }
   DRS rs{FR.par[PAR_A * n + k], FR.par[PAR_B * n + k], FR.par[PAR_V0 * n + k], FR.par[PAR_F0 * n + k],
          FR.par[PAR_L * n + k], FR.par[PAR_FW * n + k], FR.par[PAR_VW * n + k]};
-  if (d_newton(FR.law, rs, st.V, st.S, Slock, st.Nreg, eta, st.Psi)) {
+  if (d_newton(FR.law, rs, st.V, st.S, Slock, st.Nreg, eta, st.Psi, imax)) {
+    // the reference warns and retries from the failed iterate V, S
+    // (friction.f90:789-790); a second failure is where it stops (friction.f90:1014)
     atomicAdd(&status[0], 1ull);
+    if (d_newton(FR.law, rs, st.V, st.S, Slock, st.Nreg, eta, st.Psi, imax)) atomicAdd(&status[3], 1ull);
   }
   if (FR.force) {
     if (Sk < fabs(st.S)) { st.S = fsign(Sk, Slock); st.V = (Slock - st.S) / eta; }
@@ -383,7 +387,7 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
       double phip = etap * (rp[4] * Zpip + rm[4] * Zpim + rp[1] - rm[1]);
       double S0 = r0p[3];
       double N0 = -r0p[4] - p;
-      d_solve_friction(FR, n, k, ns, S0, N0, phip, phis, etas, x, y, stage_time(a), a.Bdt, D.status);
+      d_solve_friction(FR, n, k, ns, S0, N0, phip, phis, etas, x, y, stage_time(a), a.Bdt, D.status, D.newton_imax);
       double snn = -(ns.N - ns.N0) / (1.0 - FR.skempton);
       double vnp = rp[1] + Zpip * (rp[4] - snn);
       double vnm = rm[1] - Zpim * (rm[4] - snn);
@@ -410,7 +414,7 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
       double stt, snt, snn;
       xy2nt_mat(Bp.F0v[3], Bp.F0v[4], Bp.F0v[6], stt, snt, snn, n0, n1);
       double N0 = -snn - p;
-      d_solve_friction(FR, n, k, ns, S0, N0, 0.0, phis, etas, x, y, stage_time(a), a.Bdt, D.status);
+      d_solve_friction(FR, n, k, ns, S0, N0, 0.0, phis, etas, x, y, stage_time(a), a.Bdt, D.status, D.newton_imax);
       double snz = ns.S - ns.S0;
       double vzp = rp[0] + Zsip * (rp[2] - snz);
       double vzm = rm[0] - Zsim * (rm[2] - snz);

@@ -84,6 +84,21 @@ __global__ void count_nonfinite_block(const double* __restrict__ F, int nx, int 
   for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
   if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, (unsigned long long)c);
 }
+// Test kernel for the bounded wait: one CTA waits on a fresh mbarrier that no
+// copy or arrival will ever complete, with a short limit, so the wait gives
+// up and reports FDMAP_ERR_TIMEOUT through the status word.
+__global__ void wait_timeout_probe(unsigned long long* status, unsigned long long limit_ns) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  const bool ok = mbar_wait_bounded(&bar, 0, status, limit_ns);
+  __syncthreads();
+  if (threadIdx.x == 0 && ok) atomicOr(&status[1], 4ull);  // would mean a phase completed with no arrival
+}
+
 // start of a replayed sequence: set the step clock (by value, no host buffer to keep alive)
 __global__ void set_step_clock(TimeState* ts, double t_start, double dt, long long n) {
   ts->t_start = t_start;
@@ -813,6 +828,7 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   }
   CUDA_TRY(cudaMemset(h->d_status, 0, 4 * sizeof(unsigned long long)));
   D.status = h->d_status;
+  D.newton_imax = 99;  // friction.f90:924
   D.energy = nullptr;
   if (d->energy_balance) {
     if ((rc = h->alloc(&h->d_energy, (size_t)d->nblocks + 1)) ||
@@ -1265,14 +1281,55 @@ int fdmap_gpu_get_fhat(fdmap_gpu* h, int b, int s, double* out) {
 }
 
 int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures) {
+  long long counts[2] = {0, 0};
+  const int rc = fdmap_gpu_newton_counts(h, counts);
+  if (newton_failures) *newton_failures = counts[0];
+  return rc;
+}
+
+int fdmap_gpu_newton_counts(fdmap_gpu* h, long long* counts) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
   CUDA_TRY(cudaSetDevice(h->device));
   unsigned long long st[4];
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   CUDA_TRY(cudaMemcpy(st, h->d_status, sizeof(st), cudaMemcpyDeviceToHost));
-  if (newton_failures) *newton_failures = (long long)st[0];
+  if (counts) {
+    counts[0] = (long long)st[0];
+    counts[1] = (long long)st[3];
+  }
   if (st[1] & 2ull) return set_err(FDMAP_ERR_TIMEOUT, "a bounded device wait gave up");
-  return st[0] ? FDMAP_ERR_NEWTON_NOCONV : FDMAP_OK;
+  if (st[3]) return set_err(FDMAP_ERR_NEWTON_NOCONV, std::to_string(st[3]) + " Newton solves failed twice");
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_clear_status(fdmap_gpu* h) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  CUDA_TRY(cudaMemset(h->d_status, 0, 4 * sizeof(unsigned long long)));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_newton_limit(fdmap_gpu* h, int imax) {
+  if (!h || imax < 1 || imax > 99) return set_err(FDMAP_ERR_INVALID_ARG, "Newton iteration limit must be 1..99");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->hdom.newton_imax = imax;
+  CUDA_TRY(cudaMemcpy(h->ddom, &h->hdom, sizeof(DevDomain), cudaMemcpyHostToDevice));
+  // the step graphs carry the domain by value: capture them again
+  for (auto& ge : h->step_graph)
+    if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  h->graph_dt = 0.0;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_test_wait_timeout(fdmap_gpu* h, double limit_s) {
+  if (!h || !(limit_s > 0.0) || limit_s > 10.0) return set_err(FDMAP_ERR_INVALID_ARG, "limit must be in (0, 10] s");
+  CUDA_TRY(cudaSetDevice(h->device));
+  wait_timeout_probe<<<1, 32, 0, h->stream>>>(h->d_status, (unsigned long long)(limit_s * 1e9));
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return FDMAP_OK;
 }
 
 int fdmap_gpu_check_finite(fdmap_gpu* h, long long* count) {

@@ -2,20 +2,26 @@
 // (fused scale + SAT + SBP rates + szz + sources + RK update), organised for
 // HBM streaming on sm_100a.
 //
-// Work: every block is cut into strips of W = 64 columns; the strip-rows of
-// all blocks form one sequence of row groups (R = 4 rows) that is split into
+// Work: every block is cut into strips of MW = 128 columns; the strip-rows of
+// all blocks form one sequence of row groups (MR = 4 rows) that is split into
 // equal contiguous ranges, one per resident CTA (grid = SMs x CTAs per SM), so
 // every CTA streams the same amount of data and consecutive CTAs hold
 // vertically adjacent rows (their halo rows are shared through L2).
 //
-// Data movement: the rows a CTA needs -- fields used by the rates and the
-// metric terms -- arrive in a shared-memory ring of NS = 2R + 2H row slots
-// through 1-D TMA bulk copies (cp.async.bulk ... mbarrier::complete_tx) issued
-// by one thread two row groups ahead; each slot has its own mbarrier.
-// Neighbours along i come from the slot's halo columns, neighbours along j
-// from the adjacent slots.  Per-node data that no neighbour needs (rates DF,
-// szz, 1/J, heterogeneous material) is read by the owning thread with plain
-// coalesced loads one row group ahead.
+// Data movement: each row group arrives through 3-D tiled TMA boxes
+// (cp.async.bulk.tensor.3d ... mbarrier::complete_tx, no multicast) issued by
+// one thread ahead of use, into two shared-memory rings with one mbarrier per
+// slot:
+//  - the neighbour ring (NGS = 4 slots: groups g-1, g, g+1 resident, g+2 in
+//    flight) holds what the stencil reads at neighbours: the rate fields and
+//    yr, xr with PI halo columns ({WH, MR, NR} and {WH, MR, 2} boxes), and
+//    yq, xq, Ji ({MW, MR, 3});
+//  - the centre ring (NCS = 2 slots) holds what only the node itself reads:
+//    DF (skipped in a stage whose A is 0), szz and heterogeneous material.
+// Neighbours along i come from a slot's halo columns, neighbours along j from
+// the adjacent slots.  Boxes past the block edges are zero-filled by TMA.
+// Every wait is bounded in time; a CTA whose wait gives up stops computing,
+// drains its copies in flight and leaves (status word -> FDMAP_ERR_TIMEOUT).
 #pragma once
 
 #include <cuda.h>
@@ -143,13 +149,34 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// Bounded wait: gives up after ~2^28 polls (seconds) and records the event in
-// the status word instead of spinning forever.
-__device__ __forceinline__ void mbar_wait_bounded(unsigned long long* bar, unsigned parity, unsigned long long* status) {
-  for (unsigned it = 0; it < (1u << 28); ++it)
-    if (mbar_try_wait(bar, parity)) return;
-  atomicOr(&status[1], 2ull);
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
+
+// Longest a TMA pipeline wait may take before the kernel gives up (a normal
+// row-group delivery takes microseconds).
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+// Bounded wait on the phase `parity` of an mbarrier: polls until the phase
+// completes or `limit_ns` of %globaltimer time has passed.  On giving up it
+// records the event in status[1] (bit 1, read back as FDMAP_ERR_TIMEOUT) and
+// returns false; the caller then stops using the slot's data.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, unsigned long long* status,
+                                                  unsigned long long limit_ns = kWaitLimitNs) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer_ns();
+  for (;;) {
+#pragma unroll 1
+    for (int k = 0; k < 32; ++k)
+      if (mbar_try_wait(bar, parity)) return true;
+    if (globaltimer_ns() - t0 > limit_ns) break;
+  }
+  atomicOr(&status[1], 2ull);
+  return false;
+}
+
 
 // Row-group unit u -> (block, strip, first row)
 struct UnitPos {
@@ -241,7 +268,9 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
     }
     __syncthreads();
 
+    int nb_next = gmin, c_next = 0;  // next neighbour / centre group to be filled (thread 0)
     auto fill_nb = [&](int k) {  // neighbour group k -> slot (k - gmin) % NGS
+      nb_next = k + 1;
       const int sl = (k - gmin) % NGS;
       unsigned char* g = smem + (size_t)sl * L::GSLOT;
       const int row = jr0 + k * MR;
@@ -251,6 +280,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
       tma_load_3d(g + L::MC_OFF, &tmi.MC[b], i0, row, 2, &nbar[sl]);
     };
     auto fill_c = [&](int k) {  // centre group k -> slot k % NCS
+      c_next = k + 1;
       const int sl = k % NCS;
       unsigned char* g = smem + (size_t)NGS * L::GSLOT + (size_t)sl * L::CSLOT;
       const int row = jr0 + k * MR;
@@ -280,12 +310,20 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
     const bool forces = D.src.use_gravity || (D.src.use_singular && B.src_ok);
     const double t_stage = forces ? stage_time(a) : 0.0;
     const int i = i0 + cx;
+    int aborted_at = -1;
     for (int g = 0; g < ngroups; ++g) {
       // wait for groups g-1, g, g+1 (neighbours) and centre group g
       // neighbour group k lives in slot (k - gmin) % NGS as that slot's fill (k - gmin) / NGS
+      bool ok = true;
       for (int k = max(gmin, g - 1); k <= min(gmax, g + 1); ++k)
-        mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status);
-      mbar_wait_bounded(&cbar[g % NCS], (unsigned)((g / NCS) & 1), D.status);
+        ok = mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status) && ok;
+      ok = mbar_wait_bounded(&cbar[g % NCS], (unsigned)((g / NCS) & 1), D.status) && ok;
+      // a wait that gave up anywhere in the CTA: no compute or store from
+      // these slots, no further copies; the CTA drains and leaves
+      if (__syncthreads_or(!ok)) {
+        aborted_at = g;
+        break;
+      }
       const int j = jr0 + g * MR + ry;
       if (j < jr1 && i >= nbst && i <= nx - 1 - nbst && j >= nbst && j <= ny - 1 - nbst) {
         const long long c = (long long)j * pitch + i;
@@ -374,6 +412,18 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
         if (g - 1 >= gmin && g - 1 + NGS <= gmax) fill_nb(g - 1 + NGS);
         if (g + NCS < ngroups) fill_c(g + NCS);
       }
+    }
+    if (aborted_at >= 0) {
+      // wait (bounded again) for every copy this CTA may still have in
+      // flight into its shared memory, then end the CTA
+      if (tid == 0) {
+        const int g = aborted_at;
+        for (int k = max(gmin, g - 1); k < nb_next; ++k)
+          mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status);
+        for (int k = g; k < c_next; ++k) mbar_wait_bounded(&cbar[k % NCS], (unsigned)((k / NCS) & 1), D.status);
+      }
+      __syncthreads();
+      return;
     }
     __syncthreads();
     u = seg_end;

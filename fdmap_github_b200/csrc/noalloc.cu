@@ -15,8 +15,13 @@
 //  - at most NOALLOC_MAX_PARTIALS CTAs of NOALLOC_PER_CTA nodes each, i.e.
 //    faults of up to 1,048,576 nodes; longer ones are rejected
 //    (FDMAP_ERR_UNSUPPORTED) before anything is launched;
-//  - the completion counter must be zero when a call starts.  It is zero when
-//    the module loads, and the last CTA of every call resets it to zero;
+//  - the completion counter must be zero when a call starts: every call
+//    clears it with cudaMemsetAsync on its stream before the launch (a memset
+//    allocates nothing), so a counter left over by an earlier call that never
+//    finished cannot make a CTA mistake itself for the last one;
+//  - a NaN anywhere in the field makes the result NaN (the maximum does not
+//    skip it the way fmax would), so a blown-up slip rate is not reported as
+//    a finite maximum;
 //  - the partials need no initial value: each CTA writes its own slot before
 //    it counts itself done;
 //  - the scratch is shared by every handle on a device: two calls that overlap
@@ -75,15 +80,17 @@ int scratch_for(int device, ScratchPtrs* out) {
   return FDMAP_OK;
 }
 
+// maximum that propagates NaN: a NaN operand wins (fmax would drop it)
+__device__ __forceinline__ double max_nan(double a, double b) { return (b != b || b > a) ? b : a; }
+
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  for (int o = 16; o > 0; o >>= 1) v = max_nan(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
 // max |x[0..n)|: each CTA reduces NOALLOC_PER_CTA nodes into partials[cta];
-// the last CTA to finish folds the partials into partials[NOALLOC_MAX_PARTIALS]
-// and puts the counter back to zero.
+// the last CTA to finish folds the partials into partials[NOALLOC_MAX_PARTIALS].
 __global__ void __launch_bounds__(NOALLOC_THREADS) fault_absmax_kernel(const double* __restrict__ x, int n,
                                                                        double* partials, unsigned int* done) {
   __shared__ double warp_part[NOALLOC_THREADS / 32];
@@ -93,7 +100,7 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) fault_absmax_kernel(const dou
 #pragma unroll
   for (int q = 0; q < NOALLOC_PER_THREAD; ++q) {
     const int k = base + q * NOALLOC_THREADS;
-    if (k < n) m = fmax(m, fabs(x[k]));
+    if (k < n) m = max_nan(m, fabs(x[k]));
   }
   m = warp_max(m);
   if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = m;
@@ -113,15 +120,14 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) fault_absmax_kernel(const dou
   __threadfence();
   double v = 0.0;
   for (int c = threadIdx.x; c < (int)gridDim.x; c += NOALLOC_THREADS)
-    v = fmax(v, ((volatile double*)partials)[c]);
+    v = max_nan(v, ((volatile double*)partials)[c]);
   v = warp_max(v);
   if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x == 0) {
     double r = 0.0;
-    for (int w = 0; w < NOALLOC_THREADS / 32; ++w) r = fmax(r, warp_part[w]);
+    for (int w = 0; w < NOALLOC_THREADS / 32; ++w) r = max_nan(r, warp_part[w]);
     partials[NOALLOC_MAX_PARTIALS] = r;
-    *done = 0u;  // the next call starts from zero
   }
 }
 
@@ -146,6 +152,7 @@ extern "C" int fdmap_gpu_fault_max_noalloc(fdmap_gpu* h, int iface, int field, d
     return FDMAP_OK;
   }
   const double* x = I.fr.st + (size_t)field * n;
+  CUDA_TRY(cudaMemsetAsync(sp.done, 0, sizeof(unsigned int), h->stream));
   fault_absmax_kernel<<<(int)ctas, NOALLOC_THREADS, 0, h->stream>>>(x, n, sp.partials, sp.done);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaMemcpyAsync(out, sp.partials + NOALLOC_MAX_PARTIALS, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

@@ -315,9 +315,27 @@ class GpuDomain:
         return out.value
 
     def newton_failures(self) -> int:
-        n = C.c_longlong()
-        lib().fdmap_gpu_status(self._g, C.byref(n))
-        return n.value
+        """Friction solves whose first Newton attempt failed (the reference's warnings)."""
+        return self.newton_counts()[0]
+
+    def newton_counts(self) -> tuple[int, int]:
+        """(first-attempt Newton failures, retries that failed too -- where the reference stops)."""
+        c = (C.c_longlong * 2)()
+        rc = lib().fdmap_gpu_newton_counts(self._g, c)
+        if rc not in (0, -4, -5):
+            check_gpu(rc, "fdmap_gpu_newton_counts")
+        return int(c[0]), int(c[1])
+
+    def status(self) -> int:
+        """fdmap_gpu_status: 0, FDMAP_ERR_NEWTON_NOCONV (-4) or FDMAP_ERR_TIMEOUT (-5)."""
+        return lib().fdmap_gpu_status(self._g, None)
+
+    def clear_status(self) -> None:
+        check_gpu(lib().fdmap_gpu_clear_status(self._g), "fdmap_gpu_clear_status")
+
+    def set_newton_limit(self, imax: int) -> None:
+        """Lower the Newton iteration limit (imax = 99 in the reference) to provoke failures."""
+        check_gpu(lib().fdmap_gpu_set_newton_limit(self._g, int(imax)), "fdmap_gpu_set_newton_limit")
 
     def nonfinite_count(self) -> int:
         """Non-finite values in the body fields and the fault V, S, Psi

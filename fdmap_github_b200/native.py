@@ -71,6 +71,10 @@ SIGNATURES = {
     "fdmap_gpu_get_fhat": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),
     "fdmap_gpu_status": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
     "fdmap_gpu_check_finite": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_newton_counts": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_clear_status": (C.c_int, [_VP]),
+    "fdmap_gpu_set_newton_limit": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_test_wait_timeout": (C.c_int, [_VP, C.c_double]),
     "fdmap_gpu_time_params": (C.c_int, [_VP, _DP, C.POINTER(C.c_int)]),
     "fdmap_gpu_get_metric": (C.c_int, [_VP, C.c_int, _DP]),
     "fdmap_gpu_get_side_impedance": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),

@@ -118,11 +118,32 @@ int fdmap_gpu_set_side_displacement(fdmap_gpu* h, int b, int s, const double* U,
  * of block b as the engine holds them (init_edges, domain.f90:1349-1459). */
 int fdmap_gpu_get_side_impedance(fdmap_gpu* h, int b, int s, double* out);
 
-/* Device status: Newton failures so far (the reference stops on the first,
- * friction.f90:1012-1036).  Returns FDMAP_ERR_TIMEOUT if a bounded device wait
- * (a TMA pipeline barrier) gave up, else FDMAP_ERR_NEWTON_NOCONV if the
- * solver failed somewhere, else FDMAP_OK. */
+/* Device status.  *newton_failures: friction solves whose first Newton
+ * attempt failed so far (the reference warns and retries from the failed
+ * iterate, friction.f90:789-790, 1012-1036).  Returns FDMAP_ERR_TIMEOUT if a
+ * bounded device wait (a TMA pipeline barrier) gave up, else
+ * FDMAP_ERR_NEWTON_NOCONV if some retry failed as well (where the reference
+ * calls stop, friction.f90:1014), else FDMAP_OK. */
 int fdmap_gpu_status(fdmap_gpu* h, long long* newton_failures);
+
+/* counts[0]: first-attempt Newton failures, counts[1]: retries that failed
+ * too.  Return value as fdmap_gpu_status. */
+int fdmap_gpu_newton_counts(fdmap_gpu* h, long long* counts);
+
+/* Resets the status words (failure counts, timeout flag) to zero. */
+int fdmap_gpu_clear_status(fdmap_gpu* h);
+
+/* Iteration limit of every Newton solve, 1..99 (the reference's parameter
+ * imax = 99, friction.f90:924, is the default).  A driver or test lowers it
+ * to provoke solver failures on purpose (fault injection from the host). */
+int fdmap_gpu_set_newton_limit(fdmap_gpu* h, int imax);
+
+/* Self-test of the bounded device wait: launches one CTA that waits on an
+ * mbarrier nothing will complete, for at most limit_s seconds (0 < limit_s
+ * <= 10).  Afterwards fdmap_gpu_status reports FDMAP_ERR_TIMEOUT, exactly as
+ * after a TMA pipeline wait that gave up; the context stays usable.  No
+ * reference counterpart. */
+int fdmap_gpu_test_wait_timeout(fdmap_gpu* h, double limit_s);
 
 /* Counts the non-finite values (NaN, +-Inf) in the current body fields of
  * every block and in the slip rate, shear stress and state of every
@@ -173,8 +194,9 @@ int fdmap_gpu_output_close(fdmap_gpu* h);
  * drivers that check the fault every step and cannot allocate inside their
  * time loop.  Its scratch is a static device array shared by all handles of a
  * device, so calls on one device must not overlap; faults longer than
- * 1,048,576 nodes are rejected (FDMAP_ERR_UNSUPPORTED).  The first call on a
- * device looks up that scratch and should come before any stream capture. */
+ * 1,048,576 nodes are rejected (FDMAP_ERR_UNSUPPORTED).  A NaN anywhere in
+ * the field gives NaN.  The first call on a device looks up that scratch and
+ * should come before any stream capture. */
 int fdmap_gpu_fault_max_noalloc(fdmap_gpu* h, int iface, int field, double* out);
 
 /* Kernel launches issued by the last fdmap_gpu_run / time_step call. */

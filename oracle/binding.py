@@ -39,6 +39,9 @@ def lib() -> C.CDLL:
         L.oracle_get_energy.argtypes = [C.c_void_p, _DP]
         L.oracle_newton_failures.restype = C.c_longlong
         L.oracle_newton_failures.argtypes = [C.c_void_p]
+        L.oracle_newton_stops.restype = C.c_longlong
+        L.oracle_newton_stops.argtypes = [C.c_void_p]
+        L.oracle_set_newton_limit.argtypes = [C.c_void_p, C.c_int]
         L.oracle_num_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -132,6 +135,14 @@ class OracleDomain:
 
     def newton_failures(self) -> int:
         return lib().oracle_newton_failures(self._o)
+
+    def newton_counts(self) -> tuple[int, int]:
+        """(first-attempt Newton failures, retries that failed too)."""
+        return lib().oracle_newton_failures(self._o), lib().oracle_newton_stops(self._o)
+
+    def set_newton_limit(self, imax: int) -> None:
+        if lib().oracle_set_newton_limit(self._o, int(imax)) != 0:
+            raise ValueError("bad Newton iteration limit")
 
     def close(self) -> None:
         if self._o:

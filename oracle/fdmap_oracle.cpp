@@ -202,7 +202,9 @@ struct oracle_domain {
     if (frc) std::fclose(frc);
   }
   double t;
-  long long newton_fail;
+  long long newton_fail;   // solves whose first Newton attempt failed (the reference's warning)
+  long long newton_stop;   // solves whose retry failed too (the reference stops there)
+  int newton_imax = 99;    // friction.f90:924 imax
 };
 
 namespace {
@@ -357,9 +359,10 @@ void estimate_V(int law, const RS& rs, double& V, double Slock, double N, double
   else if (law != FDMAP_FR_RSF) V = 2.0 * rs.V0 * std::exp(-Psi / rs.a) * std::sinh(SaN);
 }
 
-// newton_solver (friction.f90:909-1038); returns fail
-bool newton_solver(int law, const RS& rs, double& V, double& S, double Slock, double N, double eta, double Psi) {
-  const int imax = 99;
+// newton_solver (friction.f90:909-1038); returns fail.  imax is the
+// reference's parameter 99 unless a test lowers it (oracle_set_newton_limit).
+bool newton_solver(int law, const RS& rs, double& V, double& S, double Slock, double N, double eta, double Psi,
+                   int imax) {
   const double rtolV = 0.0, atolV = 0.0, atolR = 2.220446049250313e-16 * 1e4;
   double Vmin = std::min(0.0, Slock / eta);
   double Vmax = std::max(0.0, Slock / eta);
@@ -441,12 +444,13 @@ void solve_friction(oracle_domain& Dm, Fric& FR, int k, double S0, double N0, do
     return;
   }
   RS rs{FR.a[k], FR.b[k], FR.V0[k], FR.f0[k], FR.L[k], FR.fw[k], FR.Vw[k]};
-  bool fail = newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi);
+  bool fail = newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi, Dm.newton_imax);
   if (fail) {
-    // the reference retries with diagnostics and stops on a second failure
-    // (friction.f90:790, 1014); the oracle counts the event instead
+    // the reference warns, then retries from the failed iterate V, S
+    // (friction.f90:789-790) and stops on a second failure (friction.f90:1014);
+    // the oracle counts both events instead
     Dm.newton_fail++;
-    newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi);
+    if (newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi, Dm.newton_imax)) Dm.newton_stop++;
   }
   if (FR.force) {
     if (Sk < std::fabs(S)) { S = fsign(Sk, Slock); V = (Slock - S) / eta; }
@@ -1535,6 +1539,7 @@ oracle_domain* oracle_create(const fdmap_desc* d) {
   o->nifaces = d->nifaces;
   o->het = d->heterogeneous;
   o->newton_fail = 0;
+  o->newton_stop = 0;
   o->t = d->t0;
   if (!make_ops(d->fd_method, &o->op) || !make_rk(d->rk_order, &o->rk)) { delete o; return nullptr; }
   size_t NN = (size_t)d->nx * d->ny;
@@ -1722,6 +1727,14 @@ int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out) {
 }
 
 long long oracle_newton_failures(const oracle_domain* o) { return o ? o->newton_fail : -1; }
+
+long long oracle_newton_stops(const oracle_domain* o) { return o ? o->newton_stop : -1; }
+
+int oracle_set_newton_limit(oracle_domain* o, int imax) {
+  if (!o || imax < 1) return FDMAP_ERR_INVALID_ARG;
+  o->newton_imax = imax;
+  return FDMAP_OK;
+}
 
 // body displacement U, DU (nx,ny,nU) and peak motion pgv, pga (nx,ny); any may be NULL, -1 when absent
 int oracle_get_body_extras(const oracle_domain* o, double* U, double* DU, double* pgv, double* pga) {

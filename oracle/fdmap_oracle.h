@@ -73,8 +73,17 @@ int oracle_get_side_u(const oracle_domain* o, int b, int s, double* U, double* D
 /* PML field Wx (which = 0) or Wy (which = 1), (nx, ny, nF); zeros where none. */
 int oracle_get_pml(const oracle_domain* o, int which, double* out);
 
-/* Number of Newton failures seen so far (the reference warns and retries). */
+/* Number of Newton failures seen so far (the reference warns and retries
+ * from the failed iterate, friction.f90:789-790). */
 long long oracle_newton_failures(const oracle_domain* o);
+
+/* Number of solves whose retry failed as well (the reference stops there,
+ * friction.f90:1014). */
+long long oracle_newton_stops(const oracle_domain* o);
+
+/* Iteration limit of every Newton solve (the reference's imax = 99,
+ * friction.f90:924).  A test lowers it to force failures on the host. */
+int oracle_set_newton_limit(oracle_domain* o, int imax);
 
 /* Number of OpenMP threads the oracle uses (1 when built without OpenMP). */
 int oracle_num_threads(void);
