@@ -19,7 +19,8 @@ one full low-storage RK4 time step (5 stages) over all 2,564,802 nodes.
 
 Multi-GPU: one replica per rank (weak scaling), no data-path collective.
 `--impl reference` times the CPU restatement of the reference (the Fortran/MPI
-reference cannot be built in this image) on the host cores.
+reference cannot be built in this image) on the host cores, on the same
+workload, steps and warm-up; both arms print the same `config`.
 """
 from __future__ import annotations
 
@@ -49,7 +50,25 @@ UNIT = "node-updates/s"
 # (compulsory reads and writes of one stage):
 #   mode II: F 6 read + 6 write, DF 5 read + 6 write, metrics xq,xr,yq,yr,Ji 5 read
 #   mode III: F 3+3, DF 3+3, metrics 5;  heterogeneous adds rho,G (III) / 5 arrays (II)
+# A stage whose RK coefficient A is 0 (the first) does not read DF: NR_DF
+# fewer doubles per node (DF6 is never read: rates_szz overwrites it).
 BYTES_PER_NODE_STAGE = {(2, False): 28 * 8, (2, True): 33 * 8, (3, False): 17 * 8, (3, True): 19 * 8}
+NR_DF = {2: 5, 3: 3}
+RK_STAGES = {1: 1, 2: 2, 3: 3, 4: 5}
+
+
+def bytes_per_node_update(mode: int, het: bool, rk_order: int) -> int:
+    """Algorithmic bytes of one node over one full step (all stages; DF unread in stage 1)."""
+    return RK_STAGES[rk_order] * BYTES_PER_NODE_STAGE[(mode, het)] - NR_DF[mode] * 8
+
+
+def shared_config(info: dict, host) -> dict:
+    """The workload as both arms report it (identical dicts): shapes, step
+    count of the full run, and how the inputs relate to the 126 MB L2."""
+    state = host.nx * host.ny * (2 * host.nF + 5) * 8  # F, DF and the five metric planes
+    l2 = (f"inputs larger than L2 (state {state / 1e9:.2f} GB > 126 MB), no flush needed" if state > 126e6
+          else f"state {state / 1e6:.1f} MB fits in L2: latency bound, roofline fraction not meaningful")
+    return {**info, "rk_stages_per_step": RK_STAGES[host.rk_order], "nt_reference": host.nt, "l2": l2}
 
 
 def workload(name: str, tmpdir: Path):
@@ -196,9 +215,6 @@ def run_gpu(args) -> None:
     # ---- device-resident throughput (value)
     g = GpuDomain(host, device=local)
     lib_set_stream(g, stream)
-    state_bytes = g.device_bytes()
-    l2_note = (f"inputs larger than L2 (device state {state_bytes / 1e9:.2f} GB > 126 MB)" if state_bytes > 126e6
-               else f"device state {state_bytes / 1e6:.1f} MB fits in L2: latency bound, roofline fraction not meaningful")
     nt_inf = 1 << 30
     g.run(1, args.warmup, nt=nt_inf)
     g.synchronize()
@@ -230,25 +246,39 @@ def run_gpu(args) -> None:
     stencil_ms = kms[0] / max(kn[0], 1)
     closure_ms = kms[1] / max(kn[1], 1)
     edge_ms = kms[2] / max(kn[2], 1)
+    nst = RK_STAGES[host.rk_order]
     bps = BYTES_PER_NODE_STAGE[(host.mode, het)]
-    alg_bytes = bps * interior_nodes(host)
+    n_int = interior_nodes(host)
+    # mean algorithmic bytes of one interior-kernel launch over the step's
+    # stages: every stage reads F, metrics and DF, except stage 1 (A = 0)
+    stage_bytes = [n_int * (bps - (NR_DF[host.mode] * 8 if q == 0 else 0)) for q in range(nst)]
+    alg_bytes = sum(stage_bytes) / nst
     achieved = alg_bytes / (stencil_ms * 1e-3) / 1e9
     peaks = measured_peaks()
+    # the whole step (every node, every stage, all kernels) against the same peak
+    step_bytes = nodes * bytes_per_node_update(host.mode, het, host.rk_order)
+    step_gbs = step_bytes / (ms_max / args.steps * 1e-3) / 1e9
+    survey_bytes = nodes * RK_STAGES[host.rk_order] * (BYTES_PER_NODE_STAGE[(host.mode, het)] - 5 * 8)
     newton_fail = g.newton_failures()
     g.close()
 
-    # ---- end to end through the public API with host buffers
+    # ---- end to end through the public API with host buffers: every timed
+    # repetition starts a fresh run from the initial state held in pinned
+    # host memory (fields and the 18 fault fields uploaded), runs the steps
+    # with the fault time series written through the device-side output, and
+    # reads the final fields back into pinned memory.  DF is not uploaded:
+    # the first stage multiplies it by A(1) = 0 and never reads it.
     g2 = GpuDomain(host, device=local, init_edges=False)
     lib_set_stream(g2, stream)
-    F0 = np.ascontiguousarray(host.array("F"))
-    DF0 = np.ascontiguousarray(host.array("DF"))
-    pin_F = torch.from_numpy(F0).pin_memory()
-    pin_DF = torch.from_numpy(DF0).pin_memory()
-    pin_out = torch.empty(F0.shape, dtype=torch.float64).pin_memory()  # the step's result, read back
     nf = info.get("fault_nodes", 0)
-    # fault time series of every step (slip, slip rate, shear stress, rupture
-    # time) through the device-side output: gathered into the device ring at
-    # the reference's stage-1 output point, drained to float32 files
+    # the fault registers as the descriptor gives them, before the initial edge solve
+    fault0 = {f: torch.from_numpy(g2.get_fault(0, f)).pin_memory().numpy() for f in FAULT_INDEX} if nf else {}
+    lib().fdmap_gpu_init_edges(g2._g, host.t0)
+    g2.run(1, args.warmup, nt=nt_inf)  # captures the step graphs (set-up, untimed)
+    g2.synchronize()
+    F0 = np.ascontiguousarray(host.array("F"))
+    pin_F = torch.from_numpy(F0).pin_memory()
+    pin_out = torch.empty(F0.shape, dtype=torch.float64).pin_memory()  # the run's result, read back
     out_dir = Path(tempfile.mkdtemp(prefix=f"fdmap_bench_out_r{rank}_"))
     if nf:
         for f in ("D", "V", "S", "trup"):
@@ -259,7 +289,9 @@ def run_gpu(args) -> None:
     t0 = time.perf_counter()
     e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
-    g2.set_fields(pin_F.numpy(), pin_DF.numpy())
+    g2.set_fields(pin_F.numpy(), None)
+    for f, v in fault0.items():
+        g2.set_fault(0, f, v)
     lib().fdmap_gpu_init_edges(g2._g, host.t0)
     g2.run(1, args.steps, nt=nt_inf)
     if nf:
@@ -272,7 +304,7 @@ def run_gpu(args) -> None:
     e_ms = max(e_start.elapsed_time(e_stop), (time.perf_counter() - t0) * 1e3)
     e_ms = barrier_max(e_ms, world)
     e2e = world * nodes * args.steps / (e_ms * 1e-3)
-    h2d = (F0.nbytes + DF0.nbytes) / args.steps
+    h2d = (F0.nbytes + sum(v.nbytes for v in fault0.values())) / args.steps
     d2h = (4 * nf * 4) + F0.nbytes / args.steps
     if nf:
         g2.output_close()
@@ -288,15 +320,21 @@ def run_gpu(args) -> None:
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {**info, "parallelism": f"replicas{world}", "rk_stages_per_step": 5,
-                       "l2": l2_note, "nt_reference": host.nt},
+            "config": shared_config(info, host),
+            "parallelism": f"replicas{world}",
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload),
                          "kernel": "march_kernel", "alg_bytes_per_launch": alg_bytes,
+                         "alg_bytes_per_stage_launch": stage_bytes,
                          "mean_launch_ms": stencil_ms, "closure_kernel_mean_ms": closure_ms,
                          "interface_kernel_mean_ms": edge_ms,
-                         "peak_source": peaks["source"]},
+                         "peak_source": peaks["source"],
+                         "step_level": {"achieved": step_gbs, "frac": step_gbs / peaks["hbm_gbs"],
+                                        "bytes_per_node_update": bytes_per_node_update(host.mode, het,
+                                                                                       host.rk_order),
+                                        "frac_without_metric_reads": survey_bytes / step_bytes * step_gbs
+                                        / peaks["hbm_gbs"]}},
             "clocks": ck,
             "gpu_launches": launches,
             "newton_failures": newton_fail,
@@ -348,29 +386,36 @@ def cpu_baseline(host, args, seconds: float = 15.0) -> dict:
 
 
 def run_reference(args) -> None:
+    """The CPU arm: the oracle (C++ restatement of the reference's time step;
+    the Fortran/MPI reference cannot be built in this image) on the host
+    cores, on the same workload, steps and warm-up as the GPU arm.  Its domain
+    is set up by the host initialisation built on its own
+    (oracle/_build/libhost_init.so), so no library of the GPU package loads."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     tmp = Path(tempfile.mkdtemp(prefix="fdmap_bench_ref_"))
     text, base, info = workload(args.workload, tmp)
-    host = init_domain(text, base)
-    from oracle.binding import OracleDomain, num_threads
+    from oracle.binding import OracleDomain, init_domain_cpu, num_threads
 
+    host = init_domain_cpu(text, base)
     o = OracleDomain(host)
     nodes = host.nx * host.ny
-    o.run(1, min(args.warmup, 1), nt=1 << 30)
+    nt_inf = 1 << 30
+    o.run(1, args.warmup, nt=nt_inf)
     t0 = time.perf_counter()
-    steps = max(1, min(args.steps, 8))
-    o.run(2, 1 + steps, nt=1 << 30)
+    o.run(args.warmup + 1, args.warmup + args.steps, nt=nt_inf)
     el = time.perf_counter() - t0
-    v = nodes * steps / el
-    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": 1,
-            "ms_per_step": el / steps * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {**info, "parallelism": "host threads"},
+    v = nodes * args.steps / el
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": shared_config(info, host),
+            "parallelism": f"host threads ({num_threads()})",
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": num_threads(), "kind": "port",
-                             "sample": f"{steps} LS-RK4 steps of the full workload on the host cores"},
+                             "sample": f"{args.steps} full LS-RK4 steps (after {args.warmup} warm-up steps) of the "
+                                       f"same {host.nx}x{host.ny}-node workload ({el:.1f} s)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -25,23 +25,27 @@ from .native import FAULT_INDEX, check_gpu, check_host, dptr, lib
 class HostDomain:
     """An initialised FDMAP domain held in host memory (the Fortran driver's state)."""
 
-    def __init__(self, input_text: str, base_dir: str | Path | None = None, body_on_device: bool = False):
+    def __init__(self, input_text: str, base_dir: str | Path | None = None, body_on_device: bool = False,
+                 native_lib=None):
+        # the fdmap_host_* entry points: the engine library, or the same
+        # restatement built on its own (a CPU-only caller)
+        self._L = native_lib if native_lib is not None else lib()
         self._h = C.c_void_p()
         base = str(base_dir).encode() if base_dir is not None else None
         self.body_on_device = bool(body_on_device)
         flags = native.INIT_BODY_ON_DEVICE if self.body_on_device else 0
-        check_host(lib().fdmap_host_init_ex(input_text.encode(), base, flags, C.byref(self._h)), "init_domain")
+        check_host(self._L.fdmap_host_init_ex(input_text.encode(), base, flags, C.byref(self._h)), "init_domain", self._L)
         self._info()
 
     def _info(self) -> None:
         ints = (C.c_int * 10)()
         dbls = (C.c_double * 5)()
-        check_host(lib().fdmap_host_info(self._h, ints, dbls), "fdmap_host_info")
+        check_host(self._L.fdmap_host_info(self._h, ints, dbls), "fdmap_host_info", self._L)
         (self.mode, self.nF, self.nx, self.ny, self.nblocks, self.nifaces, self.nt, self.rk_order, self.fd_method,
          het) = list(ints)
         self.heterogeneous = bool(het)
         fl = (C.c_int * 3)()
-        check_host(lib().fdmap_host_body_flags(self._h, fl), "fdmap_host_body_flags")
+        check_host(self._L.fdmap_host_body_flags(self._h, fl), "fdmap_host_body_flags", self._L)
         self.displacement, self.peak, self.energy_balance = bool(fl[0]), bool(fl[1]), bool(fl[2])
         (self.t0, self.dt, self.CFL, self.hmin, self.hmax) = list(dbls)
 
@@ -53,7 +57,7 @@ class HostDomain:
 
     def set_spacing(self, hmin: float, hmax: float) -> None:
         """Finish set_dt from the grid spacings the device reduced (fdmap_host_set_spacing)."""
-        check_host(lib().fdmap_host_set_spacing(self._h, hmin, hmax), "fdmap_host_set_spacing")
+        check_host(self._L.fdmap_host_set_spacing(self._h, hmin, hmax), "fdmap_host_set_spacing", self._L)
         self._info()
 
     @property
@@ -62,12 +66,12 @@ class HostDomain:
 
     @property
     def desc(self) -> C.c_void_p:
-        return C.c_void_p(lib().fdmap_host_desc(self._h))
+        return C.c_void_p(self._L.fdmap_host_desc(self._h))
 
     def array(self, name: str) -> np.ndarray:
         """View of a body array ("F", "DF", "x", "y", "xq", ...), shape (k, ny, nx)."""
         n = C.c_longlong()
-        p = lib().fdmap_host_array(self._h, name.encode(), C.byref(n))
+        p = self._L.fdmap_host_array(self._h, name.encode(), C.byref(n))
         if not p:
             raise KeyError(name)
         a = np.ctypeslib.as_array(p, shape=(n.value,))
@@ -75,22 +79,22 @@ class HostDomain:
         return a.reshape(k, self.ny, self.nx)
 
     def iface_n(self, iface: int) -> int:
-        n = lib().fdmap_host_iface_n(self._h, iface)
+        n = self._L.fdmap_host_iface_n(self._h, iface)
         if n < 0:
-            check_host(n, "fdmap_host_iface_n")
+            check_host(n, "fdmap_host_iface_n", self._L)
         return n
 
     def iface_info(self, iface: int) -> tuple[int, int, int, int]:
         """(direction 0='x' / 1='y', m, p, coupling) of interface `iface`."""
         info = (C.c_int * 4)()
-        check_host(lib().fdmap_host_iface_info(self._h, iface, info), "fdmap_host_iface_info")
+        check_host(self._L.fdmap_host_iface_info(self._h, iface, info), "fdmap_host_iface_info", self._L)
         return tuple(info)
 
     def iface_xy(self, iface: int) -> tuple[np.ndarray, np.ndarray]:
         n = self.iface_n(iface)
         out = []
         for w in (0, 1):
-            p = lib().fdmap_host_iface_xy(self._h, iface, w)
+            p = self._L.fdmap_host_iface_xy(self._h, iface, w)
             out.append(np.ctypeslib.as_array(p, shape=(n,)).copy() if p else np.zeros(n))
         return out[0], out[1]
 
@@ -98,7 +102,7 @@ class HostDomain:
         """Side array of block b, side s (0..3 = L, R, B, T): "F0" -> (nF, n), "M" -> (5, n), "normal" -> (2, n),
         "x" / "y" -> (1, n)."""
         n = C.c_longlong()
-        p = lib().fdmap_host_side_array(self._h, b, s, name.encode(), C.byref(n))
+        p = self._L.fdmap_host_side_array(self._h, b, s, name.encode(), C.byref(n))
         if not p:
             raise KeyError(name)
         a = np.ctypeslib.as_array(p, shape=(n.value,)).copy()
@@ -108,16 +112,16 @@ class HostDomain:
 
     def block_cdiss(self, b: int) -> float:
         """Artificial dissipation coefficient of block b, scaled by CFL/dt (0 = none)."""
-        v = lib().fdmap_host_block_cdiss(self._h, b)
+        v = self._L.fdmap_host_block_cdiss(self._h, b)
         if v < 0:
-            check_host(int(v), "fdmap_host_block_cdiss")
+            check_host(int(v), "fdmap_host_block_cdiss", self._L)
         return v
 
     def block_pml(self, b: int) -> dict:
         """pml_list of block b: pmlx, pmly, n, sigma, kappa, mx, px, my, py."""
         fl = (C.c_int * 2)()
         pr = (C.c_double * 7)()
-        check_host(lib().fdmap_host_block_pml(self._h, b, fl, pr), "fdmap_host_block_pml")
+        check_host(self._L.fdmap_host_block_pml(self._h, b, fl, pr), "fdmap_host_block_pml", self._L)
         keys = ("n", "sigma", "kappa", "mx", "px", "my", "py")
         return {"pmlx": bool(fl[0]), "pmly": bool(fl[1]), **dict(zip(keys, list(pr)))}
 
@@ -128,12 +132,12 @@ class HostDomain:
 
     def block_limits(self, b: int) -> tuple[int, int, int, int]:
         lim = (C.c_int * 4)()
-        check_host(lib().fdmap_host_block_limits(self._h, b, lim), "fdmap_host_block_limits")
+        check_host(self._L.fdmap_host_block_limits(self._h, b, lim), "fdmap_host_block_limits", self._L)
         return tuple(lim)
 
     def close(self) -> None:
         if self._h:
-            lib().fdmap_host_free(self._h)
+            self._L.fdmap_host_free(self._h)
             self._h = C.c_void_p()
 
     def __del__(self):

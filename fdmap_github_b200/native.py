@@ -162,9 +162,9 @@ def dptr(a) -> C.POINTER(C.c_double):
     return a.ctypes.data_as(_DP)
 
 
-def check_host(rc: int, where: str) -> None:
+def check_host(rc: int, where: str, L=None) -> None:
     if rc != 0:
-        raise FdmapError(rc, where, lib().fdmap_host_last_error().decode())
+        raise FdmapError(rc, where, (L if L is not None else lib()).fdmap_host_last_error().decode())
 
 
 def check_gpu(rc: int, where: str) -> None:

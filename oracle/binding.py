@@ -9,7 +9,7 @@ import ctypes as C
 
 import numpy as np
 
-from .build import LIB, build_oracle
+from .build import HOST_LIB, LIB, build_oracle
 
 FAULT_FIELDS = ["D", "Psi", "DPsi", "trup", "V", "O", "S", "N", "S0", "N0",
                 "Ds", "Dn", "DDs", "DDn", "W", "DW", "Nreg", "DNreg"]
@@ -45,6 +45,35 @@ def lib() -> C.CDLL:
         L.oracle_num_threads.restype = C.c_int
         _lib = L
     return _lib
+
+
+_host_lib = None
+
+
+def host_lib() -> C.CDLL:
+    """The host initialisation (fdmap_host_*) built on its own into
+    oracle/_build/libhost_init.so: the CPU arm's init_domain, which loads no
+    library of the GPU package."""
+    global _host_lib
+    if _host_lib is None:
+        build_oracle()
+        from fdmap_github_b200.native import SIGNATURES
+
+        L = C.CDLL(str(HOST_LIB))
+        for name, (res, args) in SIGNATURES.items():
+            if name.startswith("fdmap_host_"):
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+        _host_lib = L
+    return _host_lib
+
+
+def init_domain_cpu(input_text: str, base_dir=None):
+    """init_domain through libhost_init.so (same restatement, same descriptor)."""
+    from fdmap_github_b200.domain import HostDomain
+
+    return HostDomain(input_text, base_dir, native_lib=host_lib())
 
 
 def _p(a):

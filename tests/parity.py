@@ -50,13 +50,19 @@ def assert_fields_close(Fg, Fo, rtol=FIELD_RTOL, what="F"):
     return errs
 
 
-def assert_fault_close(gpu, orc, iface=0, rtol=FAULT_RTOL, dt=None, fields=("V", "S", "N", "D", "Psi")):
+def fault_errors(gpu, orc, iface=0, fields=("V", "S", "N", "D", "Psi")) -> dict:
+    """Norm-wise relative error of each fault field (GPU against oracle)."""
     out = {}
     for f in fields:
         g, o = gpu.get_fault(iface, f), orc.get_fault(iface, f)
-        e = rel_err(g, o)
-        out[f] = e
         assert np.all(np.isfinite(g)), f"fault {f}: non-finite"
+        out[f] = rel_err(g, o)
+    return out
+
+
+def assert_fault_close(gpu, orc, iface=0, rtol=FAULT_RTOL, dt=None, fields=("V", "S", "N", "D", "Psi")):
+    out = fault_errors(gpu, orc, iface, fields)
+    for f, e in out.items():
         assert e <= rtol, f"fault {f}: relative error {e} exceeds {rtol}"
     tg, to = gpu.get_fault(iface, "trup"), orc.get_fault(iface, "trup")
     mismatch = np.count_nonzero(tg != to)

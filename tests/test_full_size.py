@@ -1,0 +1,68 @@
+"""GPU against the oracle on the benchmarked configurations at their full
+grid sizes:
+
+  rupture     two blocks of 1601 x 801 nodes (dx 25 m), slip-weakening fault
+              of 1601 nodes, LS-RK4 at CFL 0.5 (the bench workload)
+  roughfault  two curvilinear blocks of 2001 x 1001 nodes on a seeded fractal
+              fault of 2001 nodes, flash-heating rate-and-state (RFL)
+
+By default a few hundred steps of each (the oracle needs about a minute on the
+GPU box's host cores).  With FDMAP_FULL_LENGTH=1 the whole runs, 4000 and 6000
+steps (nt = 4001 and 6001 loop indices, the last one the reference's
+output-only index), are compared instead.  Every case prints one line
+`FULLSIZE {json}` with the per-field and fault errors."""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from fdmap_github_b200 import GpuDomain, init_domain, problems
+from tests.parity import FAULT_RTOL, FIELD_RTOL, assert_fields_close, fault_errors, field_errors
+
+pytestmark = pytest.mark.gpu
+
+FULL = os.environ.get("FDMAP_FULL_LENGTH") == "1"
+
+
+def _compare(name, h, n_last, fault_fields=("V", "S", "N", "D", "Psi")):
+    from oracle.binding import OracleDomain
+
+    g, o = GpuDomain(h), OracleDomain(h)
+    g.run(1, n_last)
+    o.run(1, n_last)
+    Fg, Fo = g.get_fields()[0], o.get_fields()[0]
+    ferr = field_errors(Fg, Fo)
+    flt = fault_errors(g, o, fields=fault_fields)
+    tg, to = g.get_fault(0, "trup"), o.get_fault(0, "trup")
+    rec = {"case": name, "nx": h.nx, "ny": h.ny, "loop_indices": n_last, "field_rel_err": ferr,
+           "fault_rel_err": flt, "trup_mismatch_nodes": int(np.count_nonzero(tg != to)),
+           "max_slip_rate": float(np.abs(o.get_fault(0, "V")).max()),
+           "newton": [g.newton_failures(), o.newton_failures()]}
+    print("FULLSIZE " + json.dumps(rec), flush=True)
+    assert_fields_close(Fg, Fo, what=name)
+    for f, e in flt.items():
+        assert e <= FAULT_RTOL, f"{name}: fault {f} relative error {e}"
+    assert rec["trup_mismatch_nodes"] <= max(2, tg.size // 500)
+    g.close()
+    o.close()
+    return rec
+
+
+def test_rupture_full_grid(require_gpu):
+    h = init_domain(problems.rupture_sw())
+    assert (h.nx, h.ny) == (1601, 1602)
+    rec = _compare("rupture 2x1601x801", h, h.nt if FULL else 300, ("V", "S", "N", "D"))
+    assert rec["max_slip_rate"] > 0.1  # the patch has nucleated
+
+
+def test_roughfault_full_grid(require_gpu, tmp_path):
+    h = init_domain(problems.rough_fault_rs(tmp_path), tmp_path)
+    assert (h.nx, h.ny) == (2001, 2002)
+    _compare("roughfault 2x2001x1001", h, h.nt if FULL else 200)
+
+
+def test_field_tolerance_is_the_stated_one():
+    assert FIELD_RTOL == 1e-10

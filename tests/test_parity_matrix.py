@@ -18,9 +18,12 @@ def _f(x: float) -> str:
 
 
 def fault_text(mode=2, law="SW", direction="y", ld="gaussian", bc="absorbing", fd="SBP4", n=41, h=0.25,
-               friction_extra="", extra_blocks="", nt=31) -> str:
+               friction_extra="", extra_blocks="", nt=31, coupling="friction") -> str:
     """Two blocks of n x (n//2 + 1) nodes (direction 'y': stacked, fault y = 0;
-    'x': side by side, fault x = 0) with a frictional interface."""
+    'x': side by side, fault x = 0) with a frictional interface, or with
+    coupling='locked' a welded interface (locked_interface_mode2/3,
+    interfaces.f90:676-772) crossed by a Gaussian velocity pulse that starts
+    in block 1 one km from it."""
     m = n // 2 + 1
     L, W = (n - 1) * h, (m - 1) * h
     if direction == "y":
@@ -46,6 +49,10 @@ def fault_text(mode=2, law="SW", direction="y", ld="gaussian", bc="absorbing", f
         params = ""
     else:
         params = "rs%a=0.01d0, rs%b=0.014d0, rs%V0=1d-6, rs%f0=0.6d0, rs%L=0.05d0, rs%fw=0.2d0, rs%Vw=0.1d0, Psi0=0.6d0,"
+    if coupling == "locked":
+        x0, y0 = ("0.5d0", "-1d0") if direction == "y" else ("-1d0", "0.5d0")
+        v = "P5%vx=1d0, P5%vy=0.5d0" if mode == 2 else "P5%vz=1d0"
+        stress += f", P5%shape='gaussian', P5%x0={x0}, P5%y0={y0}, P5%Lx=0.6d0, P5%Ly=0.6d0, {v}"
     blk = f"&material_list rho=2.67d0, cs=3.464d0, cp=6d0 /\n&fields_list {stress} /\n"
     return f"""&problem_list name='matrix', nt={nt}, CFL=0.5d0, RKorder=4 /
 &domain_list mode={mode}, FDmethod='{fd}', {dom} /
@@ -56,10 +63,10 @@ def fault_text(mode=2, law="SW", direction="y", ld="gaussian", bc="absorbing", f
 &grid_list {g2} /
 &boundaries_list {b2} /
 {blk}{extra_blocks}!---IFACE1---
-&interface_list coupling='friction', direction='{direction}' /
-&friction_list friction_law='{law}', {params} {ldline}
+&interface_list coupling='{coupling}', direction='{direction}' /
+""" + ("" if coupling == "locked" else f"""&friction_list friction_law='{law}', {params} {ldline}
   rup_field='V', rup_threshold=1d-3 {friction_extra} /
-"""
+""")
 
 
 CASES = {
@@ -119,6 +126,52 @@ def test_every_case_initialises_and_runs_on_the_oracle():
         o.run(1, 3)
         F = o.get_fields()[0]
         assert np.all(np.isfinite(F)), name
+
+
+# welded interfaces in both modes and both directions (interfaces.f90:676-772)
+LOCKED = {
+    "locked-II-y": dict(coupling="locked"),
+    "locked-II-x": dict(coupling="locked", direction="x"),
+    "locked-III-y": dict(coupling="locked", mode=3),
+    "locked-III-x": dict(coupling="locked", mode=3, direction="x"),
+}
+
+
+def test_locked_cases_initialise_and_run_on_the_oracle():
+    from oracle.binding import OracleDomain
+
+    for name, kw in LOCKED.items():
+        h = init_domain(fault_text(**kw))
+        assert h.iface_info(0)[3] == 0, name  # FDMAP_COUPLING_LOCKED
+        o = OracleDomain(h)
+        o.run(1, 3)
+        assert np.all(np.isfinite(o.get_fields()[0])), name
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(LOCKED))
+def test_locked_gpu_vs_oracle(require_gpu, name):
+    """The pulse crosses the welded interface: fields and the hat variables of
+    both interface sides against the oracle."""
+    from oracle.binding import OracleDomain
+
+    from tests.parity import rel_err
+
+    h = init_domain(fault_text(**LOCKED[name]))
+    g, o = GpuDomain(h), OracleDomain(h)
+    g.run(1, 30)
+    o.run(1, 30)
+    Fo = o.get_fields()[0]
+    assert_fields_close(g.get_fields()[0], Fo, what=name)
+    sides = ((0, 3), (1, 2)) if LOCKED[name].get("direction", "y") == "y" else ((0, 1), (1, 0))
+    for b, sd in sides:
+        e = rel_err(g.get_fhat(b, sd), o.get_fhat(b, sd))
+        assert e <= 1e-10, f"{name}: hat variables of block {b} side {sd}: {e}"
+    # the pulse reached block 2 through the interface
+    n_half = h.ny // 2 if LOCKED[name].get("direction", "y") == "y" else None
+    v2 = Fo[0, n_half:, :] if n_half else Fo[0, :, h.nx // 2:]
+    assert np.abs(v2).max() > 1e-3
+    g.close()
 
 
 @pytest.mark.gpu
