@@ -43,6 +43,12 @@ def lib() -> C.CDLL:
         L.oracle_newton_stops.argtypes = [C.c_void_p]
         L.oracle_set_newton_limit.argtypes = [C.c_void_p, C.c_int]
         L.oracle_num_threads.restype = C.c_int
+        L.oracle_set_tap.argtypes = [C.c_void_p, C.c_int]
+        L.oracle_get_fault_tap.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
+        L.oracle_set_fault.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
+        L.oracle_set_side_u.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP, _DP]
+        L.oracle_set_body_extras.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP]
+        L.oracle_set_pml.argtypes = [C.c_void_p, C.c_int, _DP]
         _lib = L
     return _lib
 
@@ -118,6 +124,43 @@ class OracleDomain:
             raise RuntimeError(f"oracle_get_fault failed ({rc})")
         return out
 
+    def set_fault(self, iface: int, field: str, values) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if lib().oracle_set_fault(self._o, iface, FAULT_FIELDS.index(field), _p(v)) != 0:
+            raise RuntimeError("oracle_set_fault failed")
+
+    def set_tap(self, on: bool = True) -> None:
+        """Keep each step's stage-1 fault fields (the reference's output point)."""
+        lib().oracle_set_tap(self._o, int(on))
+
+    def get_fault_tap(self, iface: int, field: str) -> np.ndarray:
+        out = np.empty(self.host.iface_n(iface))
+        if lib().oracle_get_fault_tap(self._o, iface, FAULT_FIELDS.index(field), _p(out)) != 0:
+            raise RuntimeError("no stage-1 fault fields kept (set_tap first)")
+        return out
+
+    def set_side_displacement(self, b: int, s: int, U=None, DU=None) -> None:
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        DU = None if DU is None else np.ascontiguousarray(DU, dtype=np.float64)
+        lib().oracle_set_side_u(self._o, b, s, _p(U), _p(DU))
+
+    def set_displacement(self, U=None, DU=None) -> None:
+        U = None if U is None else np.ascontiguousarray(U, dtype=np.float64)
+        DU = None if DU is None else np.ascontiguousarray(DU, dtype=np.float64)
+        if lib().oracle_set_body_extras(self._o, _p(U), _p(DU), None, None):
+            raise RuntimeError("the domain does not track the body displacement")
+
+    def set_peak(self, pgv=None, pga=None) -> None:
+        pgv = None if pgv is None else np.ascontiguousarray(pgv, dtype=np.float64)
+        pga = None if pga is None else np.ascontiguousarray(pga, dtype=np.float64)
+        if lib().oracle_set_body_extras(self._o, None, None, _p(pgv), _p(pga)):
+            raise RuntimeError("the domain does not track peak motion")
+
+    def set_pml(self, which: str, W) -> None:
+        v = np.ascontiguousarray(W, dtype=np.float64)
+        if lib().oracle_set_pml(self._o, {"Wx": 0, "Wy": 1}[which], _p(v)):
+            raise RuntimeError("the domain has no such PML field")
+
     def get_fhat(self, b: int, s: int) -> np.ndarray:
         mgx, pgx, mgy, pgy = self.host.block_limits(b)
         n = (pgy - mgy + 1) if s < 2 else (pgx - mgx + 1)
@@ -155,6 +198,10 @@ class OracleDomain:
         U, DU = np.empty(n * nU), np.empty(n * nU)
         lib().oracle_get_side_u(self._o, b, s, _p(U), _p(DU))
         return U.reshape(nU, n), DU.reshape(nU, n)
+
+    def get_side_displacement(self, b: int, s: int):
+        """As get_side_u (the name GpuDomain uses)."""
+        return self.get_side_u(b, s)
 
     def get_pml(self, which: str) -> np.ndarray:
         """PML field "Wx" or "Wy", shape (nF, ny, nx); zeros where the domain has none."""

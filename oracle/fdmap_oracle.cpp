@@ -172,6 +172,7 @@ struct Fric {
   double ld_S, ld_N, ld_T, ld_R, ld_x0, ld_y0, tp_p0;
   vec a, b, V0, f0, L, fw, Vw, c0, fs, fd, Dc, bsS0, bsN0;
   vec st[FDMAP_FAULT_NFIELDS];
+  vec tap[FDMAP_FAULT_NFIELDS];  // the fields at stage 1's output point of the last step (tap on)
 };
 
 struct Ifc {
@@ -205,6 +206,7 @@ struct oracle_domain {
   long long newton_fail;   // solves whose first Newton attempt failed (the reference's warning)
   long long newton_stop;   // solves whose retry failed too (the reference stops there)
   int newton_imax = 99;    // friction.f90:924 imax
+  bool tap = false;        // keep each step's stage-1 fault fields (write_output's view, time_step.f90:129)
 };
 
 namespace {
@@ -1666,6 +1668,10 @@ int oracle_time_step(oracle_domain* o, double t0, double dt, int final_step) {
     prepare_edges(D);
     enforce_edge_conditions(D, D.rk.B[stage - 1] * dt);
     set_rates_all(D);
+    if (stage == 1 && D.tap)
+      for (auto& I : D.ifc)
+        if (I.coupling == FDMAP_COUPLING_FRICTION)
+          for (int f = 0; f < FDMAP_FAULT_NFIELDS; ++f) I.fr.tap[f] = I.fr.st[f];
     if (stage == 1 && D.energy) energy_interior(D);
     if (stage == 1 && !D.pgv.empty()) {
       // update_fields_peak (fields.f90:1136-1164), stage 1 only
@@ -1729,6 +1735,60 @@ int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out) {
 long long oracle_newton_failures(const oracle_domain* o) { return o ? o->newton_fail : -1; }
 
 long long oracle_newton_stops(const oracle_domain* o) { return o ? o->newton_stop : -1; }
+
+int oracle_set_tap(oracle_domain* o, int on) {
+  if (!o) return FDMAP_ERR_INVALID_ARG;
+  o->tap = on != 0;
+  return FDMAP_OK;
+}
+
+int oracle_get_fault_tap(const oracle_domain* o, int iface, int field, double* out) {
+  if (!o || iface < 0 || iface >= o->nifaces || field < 0 || field >= FDMAP_FAULT_NFIELDS || !out)
+    return FDMAP_ERR_INVALID_ARG;
+  const Ifc& I = o->ifc[iface];
+  if (I.coupling != FDMAP_COUPLING_FRICTION || I.fr.tap[field].empty()) return FDMAP_ERR_INVALID_ARG;
+  std::memcpy(out, I.fr.tap[field].data(), I.fr.tap[field].size() * sizeof(double));
+  return FDMAP_OK;
+}
+
+int oracle_set_fault(oracle_domain* o, int iface, int field, const double* in) {
+  if (!o || iface < 0 || iface >= o->nifaces || field < 0 || field >= FDMAP_FAULT_NFIELDS || !in)
+    return FDMAP_ERR_INVALID_ARG;
+  Ifc& I = o->ifc[iface];
+  if (I.coupling != FDMAP_COUPLING_FRICTION) return FDMAP_ERR_INVALID_ARG;
+  std::memcpy(I.fr.st[field].data(), in, I.fr.st[field].size() * sizeof(double));
+  return FDMAP_OK;
+}
+
+// boundary displacement U and its rate DU of side s of block b, (n, nU) each (either may be NULL)
+int oracle_set_side_u(oracle_domain* o, int b, int s, const double* U, const double* DU) {
+  if (!o || b < 0 || b >= o->nblocks || s < 0 || s > 3) return -1;
+  Side& S = o->blk[b].side[s];
+  if (U) std::copy(U, U + S.U.size(), S.U.begin());
+  if (DU) std::copy(DU, DU + S.DU.size(), S.DU.begin());
+  return 0;
+}
+
+// body displacement U, DU (nx,ny,nU) and peak motion pgv, pga (nx,ny); any may be NULL, -1 when absent
+int oracle_set_body_extras(oracle_domain* o, const double* U, const double* DU, const double* pgv, const double* pga) {
+  if (!o) return -1;
+  if ((U || DU) && o->U.empty()) return -1;
+  if ((pgv || pga) && o->pgv.empty()) return -1;
+  if (U) std::copy(U, U + o->U.size(), o->U.begin());
+  if (DU) std::copy(DU, DU + o->DU.size(), o->DU.begin());
+  if (pgv) std::copy(pgv, pgv + o->pgv.size(), o->pgv.begin());
+  if (pga) std::copy(pga, pga + o->pga.size(), o->pga.begin());
+  return 0;
+}
+
+// PML field Wx (which = 0) or Wy (1) from the global (nx,ny,nF) layout; -1 when the domain has none
+int oracle_set_pml(oracle_domain* o, int which, const double* in) {
+  if (!o || !in || which < 0 || which > 1) return -1;
+  vec& W = which == 0 ? o->Wx : o->Wy;
+  if (W.empty()) return -1;
+  std::copy(in, in + W.size(), W.begin());
+  return 0;
+}
 
 int oracle_set_newton_limit(oracle_domain* o, int imax) {
   if (!o || imax < 1) return FDMAP_ERR_INVALID_ARG;

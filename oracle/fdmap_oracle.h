@@ -85,6 +85,21 @@ long long oracle_newton_stops(const oracle_domain* o);
  * friction.f90:924).  A test lowers it to force failures on the host. */
 int oracle_set_newton_limit(oracle_domain* o, int imax);
 
+/* With tap on, every step keeps the 18 fault fields as they stand at the
+ * reference's output point (stage 1, after the interface solve and the
+ * rates, before the update; time_step.f90:129); read them back per field. */
+int oracle_set_tap(oracle_domain* o, int on);
+int oracle_get_fault_tap(const oracle_domain* o, int iface, int field, double* out);
+
+/* Setters for resuming from a checkpoint: a fault field, a side's boundary
+ * displacement U, DU (n, nU), the body displacement U, DU (nx, ny, nU) and
+ * peak motion pgv, pga (nx, ny), the PML field Wx (which = 0) or Wy (1). */
+int oracle_set_fault(oracle_domain* o, int iface, int field, const double* in);
+int oracle_set_side_u(oracle_domain* o, int b, int s, const double* U, const double* DU);
+int oracle_set_body_extras(oracle_domain* o, const double* U, const double* DU, const double* pgv,
+                           const double* pga);
+int oracle_set_pml(oracle_domain* o, int which, const double* in);
+
 /* Number of OpenMP threads the oracle uses (1 when built without OpenMP). */
 int oracle_num_threads(void);
 

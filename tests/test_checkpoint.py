@@ -69,3 +69,51 @@ def test_resume_with_pml_is_bitwise(require_gpu, tmp_path):
     assert np.array_equal(a.get_pml("Wx"), b.get_pml("Wx"))
     sizes = {p.name: p.stat().st_size // 8 for p in files}
     assert sizes["pmlF.ckpt25"] == 4 * h.nF * h.nx * h.ny
+
+
+@pytest.mark.gpu
+def test_oracle_resumes_from_gpu_checkpoint(require_gpu, tmp_path):
+    """The engine writes the checkpoint files; the oracle reads them (the same
+    reader, through the oracle's setters), continues, and lands where its own
+    uninterrupted run does."""
+    from oracle.binding import OracleDomain
+
+    from tests.parity import assert_fault_close, assert_fields_close
+
+    h = init_domain(problems.rupture_sw(nx=61, ny=31, h=0.4, nt=200))
+    g = GpuDomain(h)
+    g.run(1, 15)
+    name = tmp_path / "rup"
+    checkpoint_write(g, h, name, 15)
+    b = OracleDomain(h)
+    assert checkpoint_read(b, h, name) == 15
+    b.run(16, 40)
+    a = OracleDomain(h)
+    a.run(1, 40)
+    assert_fields_close(b.get_fields()[0], a.get_fields()[0], what="resumed F")
+    assert_fault_close(b, a, dt=h.dt)
+    for blk in range(2):
+        for s in range(4):
+            Ub, _ = b.get_side_u(blk, s)
+            Ua, _ = a.get_side_u(blk, s)
+            assert np.max(np.abs(Ub - Ua)) <= 1e-10 * max(np.abs(Ua).max(), 1e-30), (blk, s)
+    assert a.get_fault(0, "D").max() > 0.1
+
+
+def test_oracle_checkpoint_round_trip(tmp_path):
+    """The checkpoint writer and reader on the oracle alone (no GPU): resume
+    is bit for bit, with the boundary displacement and the fault registers."""
+    from oracle.binding import OracleDomain
+
+    h = init_domain(problems.rupture_sw(nx=41, ny=21, h=0.5, nt=100))
+    a = OracleDomain(h)
+    a.run(1, 10)
+    checkpoint_write(a, h, tmp_path / "o", 10)
+    a.run(11, 20)
+    b = OracleDomain(h)
+    assert checkpoint_read(b, h, tmp_path / "o") == 10
+    b.run(11, 20)
+    assert np.array_equal(a.get_fields()[0], b.get_fields()[0])
+    for f in FAULT_FIELDS:
+        assert np.array_equal(a.get_fault(0, f), b.get_fault(0, f)), f
+    assert np.array_equal(a.get_side_u(0, 3)[0], b.get_side_u(0, 3)[0])

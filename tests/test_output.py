@@ -195,3 +195,57 @@ def test_boundary_outputs_match_stage1_state(require_gpu, tmp_path):
             np.testing.assert_array_equal(lvy[(step - 1) // 3], p.get_fhat(1, 2)[1].astype(np.float32))
         p.time_step_LS(t0, h.dt)
     assert np.abs(lux).max() > 0  # the fault side of the upper block moves
+
+
+def test_oracle_writer_layout(tmp_path):
+    """The oracle's own writer (a restatement of write_output) on the same
+    list: item expansion, time windows and strides give the expected sizes."""
+    from oracle.binding import OracleDomain
+    from oracle.output_writer import OracleOutputs
+
+    text = _problem()
+    h = init_domain(text)
+    w = OracleOutputs(OracleDomain(h), h, text, tmp_path / "o")
+    w.run(1, 30)
+    nf = h.iface_n(0)
+    size = lambda stem, ext=".dat": (tmp_path / f"o_{stem}{ext}").stat().st_size // 4  # noqa: E731
+    assert size("I_V") == 30 * nf and size("I_V", ".t") == 30
+    assert size("B_vx") == 8 * h.nx * h.ny  # D%n = 0, 4, ..., 28
+    assert size("P_vy") == 30 and size("G_15_V") == 15 and size("G_25_V") == 15
+    assert sorted(s for s in w.stems if s.startswith("G_")) == ["G_15_V", "G_25_V", "G_5_V"]
+
+
+@pytest.mark.gpu
+def test_outputs_match_oracle_files(require_gpu, tmp_path):
+    """Every file the engine writes against the file the oracle's writer
+    writes for the same item: same size and times bit for bit, and float32
+    values equal except where the FP64 states, which agree to 1e-10, round
+    to neighbouring float32 numbers."""
+    from oracle.binding import OracleDomain
+    from oracle.output_writer import OracleOutputs
+
+    text = _problem()
+    h = init_domain(text)
+    g = GpuDomain(h)
+    configure_outputs(g, h, text, tmp_path / "g", ring_steps=7)
+    g.run(1, 30, nt=h.nt)
+    g.output_close()
+    w = OracleOutputs(OracleDomain(h), h, text, tmp_path / "o")
+    w.run(1, 30)
+    assert len(w.stems) == 8
+    differing = 0
+    for stem in w.stems:
+        for ext in (".t", ".dat"):
+            a = (tmp_path / f"g_{stem}{ext}").read_bytes()
+            b = (tmp_path / f"o_{stem}{ext}").read_bytes()
+            assert len(a) == len(b), f"{stem}{ext}: {len(a)} bytes against the oracle's {len(b)}"
+            if ext == ".t":
+                assert a == b, f"{stem}.t differs"
+                continue
+            x, y = np.frombuffer(a, np.float32), np.frombuffer(b, np.float32)
+            bad = x != y
+            differing += int(bad.sum())
+            if bad.any():
+                tol = 1e-10 * float(np.abs(y).max()) + np.spacing(np.abs(y[bad])).astype(np.float64)
+                assert np.all(np.abs(x[bad].astype(np.float64) - y[bad]) <= tol), f"{stem}.dat"
+    assert differing <= 4, f"{differing} float32 values differ"
