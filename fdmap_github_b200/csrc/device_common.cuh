@@ -97,6 +97,13 @@ struct DevIface {
   double* nhat;    // (n,2)
   double *x, *y;   // (n)
   DevFriction fr;
+  // Block-aligned partition (a side's block lives on another GPU): the edge
+  // values of that side arrive each stage in rem_m / rem_p ([l*n + k], the
+  // nF fields of the interface nodes); the local side's edge values are
+  // packed into `send` for the peer.  All NULL in an unpartitioned domain.
+  const double* rem_m;
+  const double* rem_p;
+  double* send;
 };
 
 // Device layout of every field array: PADL doubles of front padding (so that

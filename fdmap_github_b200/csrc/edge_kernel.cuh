@@ -310,12 +310,26 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
   side_node_local(I.direction == 0 ? 1 : 3, km, Bm.nx, Bm.ny, im_, jm_);
   side_node_local(I.direction == 0 ? 0 : 2, kp, Bp.nx, Bp.ny, ip_, jp_);
   double Fm[6], Fp[6], F0m[6], F0p[6];
-  const double* fm = Bm.F[a.in] + (long long)jm_ * Bm.pitch + im_;
-  const double* fp = Bp.F[a.in] + (long long)jp_ * Bp.pitch + ip_;
+  // edge values: the block's own row, or (partitioned domain) the values
+  // the peer GPU sent for this stage
+  if (I.rem_m) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fm[l] = I.rem_m[l * I.n + k];
+  } else {
+    const double* fm = Bm.F[a.in] + (long long)jm_ * Bm.pitch + im_;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fm[l] = fm[l * Bm.plane];
+  }
+  if (I.rem_p) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fp[l] = I.rem_p[l * I.n + k];
+  } else {
+    const double* fp = Bp.F[a.in] + (long long)jp_ * Bp.pitch + ip_;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) Fp[l] = fp[l * Bp.plane];
+  }
 #pragma unroll
   for (int l = 0; l < NF; ++l) {
-    Fm[l] = fm[l * Bm.plane];
-    Fp[l] = fp[l * Bp.plane];
     F0m[l] = Sm.F0[km + Sm.n * l];
     F0p[l] = Sp.F0[kp + Sp.n * l];
   }
@@ -471,6 +485,24 @@ __device__ void d_iface_node(const DevDomain& D, const DevIface& I, int k, const
 #pragma unroll
     for (int l = 0; l < NF; ++l) { Fhm_out[l] = Fhm[l]; Fhp_out[l] = Fhp[l]; }
   }
+}
+
+// Partitioned domain: the local side's edge values of every interface whose
+// other side lives on another GPU, packed as [l*n + k] for the peer.
+template <int MODE>
+__global__ void __launch_bounds__(128) pack_edges(const __grid_constant__ DevDomain D, int in, int iface) {
+  constexpr int NF = MODE == 2 ? 6 : 3;
+  const DevIface& I = D.ifc[iface];
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= I.n || !I.send) return;
+  const bool local_m = I.rem_p != nullptr;  // the minus side is this GPU's
+  const DevBlock& B = D.blk[local_m ? I.im : I.ip];
+  const int side = local_m ? (I.direction == 0 ? 1 : 3) : (I.direction == 0 ? 0 : 2);
+  int i, j;
+  side_node_local(side, (local_m ? I.offm : I.offp) + k, B.nx, B.ny, i, j);
+  const double* f = B.F[in] + (long long)j * B.pitch + i;
+#pragma unroll
+  for (int l = 0; l < NF; ++l) I.send[l * I.n + k] = f[l * B.plane];
 }
 
 // One thread per interface node: the locked / frictional solve of this stage,

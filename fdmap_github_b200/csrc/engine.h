@@ -95,6 +95,16 @@ struct fdmap_gpu {
   bool overlap = false;
   cudaStream_t side_stream = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // block-aligned partition (fdmap_gpu_create_part): the blocks this handle
+  // steps; the other blocks' body arrays live on peer GPUs
+  std::vector<char> owned;
+  std::vector<int> part_ifaces;       // interfaces with exactly one side here
+  fdmap_exchange_fn exchange = nullptr;
+  void* exchange_user = nullptr;
+  long long xstage = 0;               // stages issued (selects the send slot)
+  cudaEvent_t ev_packed = nullptr;    // the stage's edge values are packed
+  bool owns(int b) const { return owned.empty() || owned[(size_t)b] != 0; }
+  bool partitioned() const { return !owned.empty(); }
   // per-kernel event timing (fdmap_gpu_profile)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -169,6 +179,7 @@ struct fdmap_gpu {
     if (side_stream) cudaStreamDestroy(side_stream);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    if (ev_packed) cudaEventDestroy(ev_packed);
     output_destroy(this);
     delete tmaps;
     for (auto& ge : step_graph)

@@ -182,6 +182,7 @@ int march_maps(fdmap_gpu* h) {
   std::memset(h->tmaps, 0, sizeof(TmapSet));
   int rc;
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const BlockGeom& g = h->geom[b];
     DevBlock& B = h->hdom.blk[b];
     for (int q = 0; q < 2; ++q) {
@@ -358,18 +359,52 @@ int launch_boundary(fdmap_gpu* h, const StageArgs& a) {
   return FDMAP_OK;
 }
 
-int launch_stage(fdmap_gpu* h, const StageArgs& a) {
-  if (h->overlap && !h->profiling && !h->fused) {
-    // fork: the interior march is issued first on the (high-priority) main
-    // stream so its persistent CTAs take the SMs; edge + closure follow on
-    // the side stream and fill the registers the march leaves free; join.
+bool stage_overlaps(const fdmap_gpu* h) { return h->overlap && !h->profiling && !h->fused; }
+
+// stream of the stage's boundary work (interface solves, closure strips)
+cudaStream_t boundary_stream(const fdmap_gpu* h) { return stage_overlaps(h) ? h->side_stream : h->stream; }
+
+// Partitioned domain: the edge values of this stage's input buffer for every
+// interface with one side on a peer GPU, into the stage's send slot.
+int pack_partition_edges(fdmap_gpu* h, const StageArgs& a, cudaStream_t s) {
+  for (int k : h->part_ifaces) {
+    DevDomain& D = h->hdom;
+    DevIface& I = D.ifc[k];
+    double* slot0 = I.send;
+    I.send = slot0 + (size_t)(h->xstage & 1) * h->nF * I.n;
+    const int nb = (I.n + 127) / 128;
+    if (h->mode == 2) pack_edges<2><<<nb, 128, 0, s>>>(D, a.in, k);
+    else pack_edges<3><<<nb, 128, 0, s>>>(D, a.in, k);
+    I.send = slot0;
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+  }
+  CUDA_TRY(cudaEventRecord(h->ev_packed, s));
+  return FDMAP_OK;
+}
+
+// First half of a stage: with overlap, fork and issue the interior march on
+// the (high-priority) main stream, so its persistent CTAs take the SMs; then
+// the partition's edge values are packed on the boundary stream.
+int stage_begin(fdmap_gpu* h, const StageArgs& a) {
+  if (stage_overlaps(h)) {
     CUDA_TRY(cudaEventRecord(h->ev_fork, h->stream));
     CUDA_TRY(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
     int rc = launch_interior(h, a);
     if (rc) return rc;
+  }
+  if (!h->part_ifaces.empty()) return pack_partition_edges(h, a, boundary_stream(h));
+  return FDMAP_OK;
+}
+
+// Second half, after the peers' edge values have been queued on the boundary
+// stream: edge + closure on the side stream (filling the registers the march
+// leaves free) and join; or, serialised, boundary work then the interior.
+int stage_end(fdmap_gpu* h, const StageArgs& a) {
+  if (stage_overlaps(h)) {
     cudaStream_t main_stream = h->stream;
     h->stream = h->side_stream;
-    rc = launch_boundary(h, a);
+    int rc = launch_boundary(h, a);
     h->stream = main_stream;
     if (rc) return rc;
     CUDA_TRY(cudaEventRecord(h->ev_join, h->side_stream));
@@ -389,6 +424,20 @@ int launch_stage(fdmap_gpu* h, const StageArgs& a) {
   return launch_interior(h, a);
 }
 
+// One stage of a single handle: with a partition, the caller's exchange
+// callback queues the transfer of the peers' edge values between the halves.
+int launch_stage(fdmap_gpu* h, const StageArgs& a) {
+  int rc = stage_begin(h, a);
+  if (rc) return rc;
+  if (!h->part_ifaces.empty()) {
+    if (!h->exchange) return set_err(FDMAP_ERR_INVALID_ARG, "partitioned domain without an exchange callback");
+    rc = h->exchange(h->exchange_user, h->xstage, (void*)boundary_stream(h));
+    if (rc) return set_err(FDMAP_ERR_CUDA, "edge exchange callback failed (" + std::to_string(rc) + ")");
+  }
+  h->xstage++;
+  return stage_end(h, a);
+}
+
 // reads the next forcing frame into the blocks' new-frame planes (values past
 // the end of the file read as zero)
 int forcing_read_frame(fdmap_gpu* h) {
@@ -400,6 +449,7 @@ int forcing_read_frame(fdmap_gpu* h) {
   CUDA_TRY(cudaMemcpyAsync(h->d_global, h->frc_host.data(), h->frc_host.size() * sizeof(double),
                            cudaMemcpyHostToDevice, h->stream));
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const BlockGeom& g = h->geom[b];
     dim3 grid((g.pitch + 255) / 256, g.ny);
     scatter_block<<<grid, 256, 0, h->stream>>>(h->d_global, const_cast<double*>(h->hdom.blk[b].frc_new), h->nx_g, NN,
@@ -415,6 +465,7 @@ int forcing_read_frame(fdmap_gpu* h) {
 int forcing_load(fdmap_gpu* h) {
   if (!h->frc_file) return FDMAP_OK;
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const DevBlock& B = h->hdom.blk[b];
     CUDA_TRY(cudaMemcpyAsync(const_cast<double*>(B.frc_old), B.frc_new, (size_t)h->nF * B.plane * sizeof(double),
                              cudaMemcpyDeviceToDevice, h->stream));
@@ -514,135 +565,140 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     g.plane = ((long long)g.pitch * g.ny + PADTAIL + 31) / 32 * 32;
     B.nx = g.nx; B.ny = g.ny; B.pitch = g.pitch; B.plane = g.plane;
     int rc;
-    for (int q = 0; q < 2; ++q)
-      if ((rc = h->alloc_planes(&B.F[q], nF, g.plane))) return rc;
-    if ((rc = h->alloc_planes(&B.DF, nF, g.plane))) return rc;
-    // metric terms as 5 consecutive planes yr, xr, yq, xq, Ji (one TMA tensor)
-    double* met_base = nullptr;
-    if ((rc = h->alloc_planes(&met_base, 5, g.plane))) return rc;
-    double** met[5] = {&B.yr, &B.xr, &B.yq, &B.xq, &B.Ji};
-    const double* msrc[5] = {d->yr, d->xr, d->yq, d->xq, d->Ji};
-    for (int q = 0; q < 5; ++q) {
-      *met[q] = met_base + (size_t)q * g.plane;
-      if (!d->body && (rc = h->upload_plane(*met[q], msrc[q], g))) return rc;
-    }
-    h->met_base[b] = met_base;
-    if (d->heterogeneous) {
-      double* het_base = nullptr;
-      if ((rc = h->alloc_planes(&het_base, 5, g.plane))) return rc;
-      double** hm[5] = {&B.rho, &B.G, &B.M, &B.gamma, &B.nu};
-      const double* hs[5] = {d->rho, d->G, d->M, d->gamma, d->nu};
+    // a block another GPU owns (block-aligned partition): no body arrays
+    // here, only its side arrays, which the interface solve writes
+    const bool own = h->owns(b);
+    if (own) {
+      for (int q = 0; q < 2; ++q)
+        if ((rc = h->alloc_planes(&B.F[q], nF, g.plane))) return rc;
+      if ((rc = h->alloc_planes(&B.DF, nF, g.plane))) return rc;
+      // metric terms as 5 consecutive planes yr, xr, yq, xq, Ji (one TMA tensor)
+      double* met_base = nullptr;
+      if ((rc = h->alloc_planes(&met_base, 5, g.plane))) return rc;
+      double** met[5] = {&B.yr, &B.xr, &B.yq, &B.xq, &B.Ji};
+      const double* msrc[5] = {d->yr, d->xr, d->yq, d->xq, d->Ji};
       for (int q = 0; q < 5; ++q) {
-        *hm[q] = het_base + (size_t)q * g.plane;
-        if (hs[q] && (rc = h->upload_plane(*hm[q], hs[q], g))) return rc;
+        *met[q] = met_base + (size_t)q * g.plane;
+        if (!d->body && (rc = h->upload_plane(*met[q], msrc[q], g))) return rc;
       }
-      h->het_base[b] = het_base;
-    }
-    B.rho_b = fb.rho; B.G_b = fb.G; B.M_b = fb.M; B.gamma_b = fb.gamma; B.nu_b = fb.nu;
-    B.Cdiss = fb.Cdiss;  // on-device body: scaled by build_body once dt is known
-    B.J = nullptr;
-    const double cdiss_in = d->body ? d->body->blocks[b].Cdiss : fb.Cdiss;
-    if (cdiss_in > 0.0 || d->energy_balance) {  // dissipation and the energy weight nodes by J itself
-      if ((rc = h->alloc_planes(&B.J, 1, g.plane))) return rc;
-      if (!d->body && (rc = h->upload_plane(B.J, d->J, g))) return rc;
-      if (cdiss_in > 0.0) h->dissipation = true;
-    }
-    B.Hx = B.Hy = nullptr;
-    if (d->energy_balance) {
-      // diagonal norm with unit spacing (Hnorm, fd.f90:14-39)
-      std::vector<double> hx(g.nx, 1.0), hy(g.ny, 1.0);
-      for (int k = 0; k < op.nbst; ++k) {
-        hx[k] = op.HL[k]; hx[g.nx - 1 - k] = op.HL[k];
-        hy[k] = op.HL[k]; hy[g.ny - 1 - k] = op.HL[k];
+      h->met_base[b] = met_base;
+      if (d->heterogeneous) {
+        double* het_base = nullptr;
+        if ((rc = h->alloc_planes(&het_base, 5, g.plane))) return rc;
+        double** hm[5] = {&B.rho, &B.G, &B.M, &B.gamma, &B.nu};
+        const double* hs[5] = {d->rho, d->G, d->M, d->gamma, d->nu};
+        for (int q = 0; q < 5; ++q) {
+          *hm[q] = het_base + (size_t)q * g.plane;
+          if (hs[q] && (rc = h->upload_plane(*hm[q], hs[q], g))) return rc;
+        }
+        h->het_base[b] = het_base;
       }
-      double *dx = nullptr, *dy = nullptr;
-      if ((rc = h->upload(&dx, hx.data(), hx.size())) || (rc = h->upload(&dy, hy.data(), hy.size()))) return rc;
-      B.Hx = dx; B.Hy = dy;
-    }
-    B.pml = 0; B.pml_kappa = 0.0; B.pml_h = nullptr; B.pml_s = nullptr;
-    B.Wx = B.DWx = B.Wy = B.DWy = nullptr;
-    if (d->mode == 2 && (fb.pmlx || fb.pmly) && cdiss_in == 0.0) {
-      // perfectly matched layer (set_rates PML branch, time_step.f90:354-420)
-      B.pml = (fb.pmlx ? 1 : 0) | (fb.pmly ? 2 : 0);
-      B.pml_kappa = fb.pml_kappa;
-      if (fb.pmlx && ((rc = h->alloc_planes(&B.Wx, nF, g.plane)) || (rc = h->alloc_planes(&B.DWx, nF, g.plane))))
-        return rc;
-      if (fb.pmly && ((rc = h->alloc_planes(&B.Wy, nF, g.plane)) || (rc = h->alloc_planes(&B.DWy, nF, g.plane))))
-        return rc;
-      // damping at every node (rates.f90:2065-2068), evaluated once: here from
-      // the host grid, or by build_body from the device grid
-      double* ds = nullptr;
-      if ((rc = h->alloc_planes(&ds, 2, g.plane))) return rc;
-      double* dh = nullptr;
-      if ((rc = h->alloc(&dh, 18))) return rc;
-      if (!d->body) {
-        std::vector<double> damp(2 * (size_t)g.plane, 0.0);
+      B.rho_b = fb.rho; B.G_b = fb.G; B.M_b = fb.M; B.gamma_b = fb.gamma; B.nu_b = fb.nu;
+      B.Cdiss = fb.Cdiss;  // on-device body: scaled by build_body once dt is known
+      B.J = nullptr;
+      const double cdiss_in = d->body ? d->body->blocks[b].Cdiss : fb.Cdiss;
+      if (cdiss_in > 0.0 || d->energy_balance) {  // dissipation and the energy weight nodes by J itself
+        if ((rc = h->alloc_planes(&B.J, 1, g.plane))) return rc;
+        if (!d->body && (rc = h->upload_plane(B.J, d->J, g))) return rc;
+        if (cdiss_in > 0.0) h->dissipation = true;
+      }
+      B.Hx = B.Hy = nullptr;
+      if (d->energy_balance) {
+        // diagonal norm with unit spacing (Hnorm, fd.f90:14-39)
+        std::vector<double> hx(g.nx, 1.0), hy(g.ny, 1.0);
+        for (int k = 0; k < op.nbst; ++k) {
+          hx[k] = op.HL[k]; hx[g.nx - 1 - k] = op.HL[k];
+          hy[k] = op.HL[k]; hy[g.ny - 1 - k] = op.HL[k];
+        }
+        double *dx = nullptr, *dy = nullptr;
+        if ((rc = h->upload(&dx, hx.data(), hx.size())) || (rc = h->upload(&dy, hy.data(), hy.size()))) return rc;
+        B.Hx = dx; B.Hy = dy;
+      }
+      B.pml = 0; B.pml_kappa = 0.0; B.pml_h = nullptr; B.pml_s = nullptr;
+      B.Wx = B.DWx = B.Wy = B.DWy = nullptr;
+      if (d->mode == 2 && (fb.pmlx || fb.pmly) && cdiss_in == 0.0) {
+        // perfectly matched layer (set_rates PML branch, time_step.f90:354-420)
+        B.pml = (fb.pmlx ? 1 : 0) | (fb.pmly ? 2 : 0);
+        B.pml_kappa = fb.pml_kappa;
+        if (fb.pmlx && ((rc = h->alloc_planes(&B.Wx, nF, g.plane)) || (rc = h->alloc_planes(&B.DWx, nF, g.plane))))
+          return rc;
+        if (fb.pmly && ((rc = h->alloc_planes(&B.Wy, nF, g.plane)) || (rc = h->alloc_planes(&B.DWy, nF, g.plane))))
+          return rc;
+        // damping at every node (rates.f90:2065-2068), evaluated once: here from
+        // the host grid, or by build_body from the device grid
+        double* ds = nullptr;
+        if ((rc = h->alloc_planes(&ds, 2, g.plane))) return rc;
+        double* dh = nullptr;
+        if ((rc = h->alloc(&dh, 18))) return rc;
+        if (!d->body) {
+          std::vector<double> damp(2 * (size_t)g.plane, 0.0);
+          for (int j = 0; j < g.ny; ++j)
+            for (int i = 0; i < g.nx; ++i) {
+              const size_t q = (size_t)(g.mgx - 1 + i) + (size_t)d->nx * (size_t)(g.mgy - 1 + j);
+              const bool prof = fb.pml_n > 0.0;
+              damp[(size_t)j * g.pitch + i] = pml_damping(fb.pml_sigma, fb.pml_n, fb.pml_mx, fb.pml_px, prof ? d->x[q] : 0.0);
+              damp[(size_t)g.plane + (size_t)j * g.pitch + i] =
+                  pml_damping(fb.pml_sigma, fb.pml_n, fb.pml_my, fb.pml_py, prof ? d->y[q] : 0.0);
+            }
+          CUDA_TRY(cudaMemcpy(ds, damp.data(), damp.size() * sizeof(double), cudaMemcpyHostToDevice));
+          // hxi = Ji*yr, hyi = Ji*xq at the first node of each region: q and r
+          // index 0 = minus-end strip, 1 = plus-end strip, 2 = interior
+          double hh[18];
+          const int qi[3] = {0, g.nx - op.nbst, op.nbst}, rj[3] = {0, g.ny - op.nbst, op.nbst};
+          for (int q = 0; q < 3; ++q)
+            for (int r = 0; r < 3; ++r) {
+              const size_t k = (size_t)(g.mgx - 1 + qi[q]) + (size_t)d->nx * (size_t)(g.mgy - 1 + rj[r]);
+              hh[(q * 3 + r) * 2] = d->Ji[k] * d->yr[k];
+              hh[(q * 3 + r) * 2 + 1] = d->Ji[k] * d->xq[k];
+            }
+          CUDA_TRY(cudaMemcpy(dh, hh, sizeof(hh), cudaMemcpyHostToDevice));
+        }
+        B.pml_s = ds;
+        B.pml_h = dh;
+        h->pml = true;
+      }
+      B.gforce = nullptr; B.frc_old = nullptr; B.frc_new = nullptr;
+      if (d->src.gauss_forcing && d->mode == 3) {
+        // spatial factor amp*exp(-(x/sigma)^2/2 - (y/sigma)^2/2) of the tsunami forcing (source.f90:308)
+        const fdmap_source& S = d->src;
+        std::vector<double> gf((size_t)g.plane, 0.0);
         for (int j = 0; j < g.ny; ++j)
           for (int i = 0; i < g.nx; ++i) {
             const size_t q = (size_t)(g.mgx - 1 + i) + (size_t)d->nx * (size_t)(g.mgy - 1 + j);
-            const bool prof = fb.pml_n > 0.0;
-            damp[(size_t)j * g.pitch + i] = pml_damping(fb.pml_sigma, fb.pml_n, fb.pml_mx, fb.pml_px, prof ? d->x[q] : 0.0);
-            damp[(size_t)g.plane + (size_t)j * g.pitch + i] =
-                pml_damping(fb.pml_sigma, fb.pml_n, fb.pml_my, fb.pml_py, prof ? d->y[q] : 0.0);
+            const double x = d->x[q], y = d->y[q];
+            gf[(size_t)j * g.pitch + i] =
+                S.gauss_amp * std::exp(-0.5 * ((x / S.gauss_sigma) * (x / S.gauss_sigma)) -
+                                       0.5 * ((y / S.gauss_sigma) * (y / S.gauss_sigma)));
           }
-        CUDA_TRY(cudaMemcpy(ds, damp.data(), damp.size() * sizeof(double), cudaMemcpyHostToDevice));
-        // hxi = Ji*yr, hyi = Ji*xq at the first node of each region: q and r
-        // index 0 = minus-end strip, 1 = plus-end strip, 2 = interior
-        double hh[18];
-        const int qi[3] = {0, g.nx - op.nbst, op.nbst}, rj[3] = {0, g.ny - op.nbst, op.nbst};
-        for (int q = 0; q < 3; ++q)
-          for (int r = 0; r < 3; ++r) {
-            const size_t k = (size_t)(g.mgx - 1 + qi[q]) + (size_t)d->nx * (size_t)(g.mgy - 1 + rj[r]);
-            hh[(q * 3 + r) * 2] = d->Ji[k] * d->yr[k];
-            hh[(q * 3 + r) * 2 + 1] = d->Ji[k] * d->xq[k];
-          }
-        CUDA_TRY(cudaMemcpy(dh, hh, sizeof(hh), cudaMemcpyHostToDevice));
+        double* dg = nullptr;
+        if ((rc = h->alloc_planes(&dg, 1, g.plane))) return rc;
+        CUDA_TRY(cudaMemcpy(dg, gf.data(), gf.size() * sizeof(double), cudaMemcpyHostToDevice));
+        B.gforce = dg;
+        h->forcing = true;
       }
-      B.pml_s = ds;
-      B.pml_h = dh;
-      h->pml = true;
-    }
-    B.gforce = nullptr; B.frc_old = nullptr; B.frc_new = nullptr;
-    if (d->src.gauss_forcing && d->mode == 3) {
-      // spatial factor amp*exp(-(x/sigma)^2/2 - (y/sigma)^2/2) of the tsunami forcing (source.f90:308)
-      const fdmap_source& S = d->src;
-      std::vector<double> gf((size_t)g.plane, 0.0);
-      for (int j = 0; j < g.ny; ++j)
-        for (int i = 0; i < g.nx; ++i) {
-          const size_t q = (size_t)(g.mgx - 1 + i) + (size_t)d->nx * (size_t)(g.mgy - 1 + j);
-          const double x = d->x[q], y = d->y[q];
-          gf[(size_t)j * g.pitch + i] =
-              S.gauss_amp * std::exp(-0.5 * ((x / S.gauss_sigma) * (x / S.gauss_sigma)) -
-                                     0.5 * ((y / S.gauss_sigma) * (y / S.gauss_sigma)));
-        }
-      double* dg = nullptr;
-      if ((rc = h->alloc_planes(&dg, 1, g.plane))) return rc;
-      CUDA_TRY(cudaMemcpy(dg, gf.data(), gf.size() * sizeof(double), cudaMemcpyHostToDevice));
-      B.gforce = dg;
-      h->forcing = true;
-    }
-    if (d->src.forcing_filename) {
-      double* fo = nullptr;
-      double* fn = nullptr;
-      if ((rc = h->alloc_planes(&fo, nF, g.plane)) || (rc = h->alloc_planes(&fn, nF, g.plane))) return rc;
-      B.frc_old = fo;
-      B.frc_new = fn;
-      h->forcing = true;
-    }
-    B.U = B.DU = B.Utap = B.pgv = B.pga = nullptr;
-    if (d->displacement) {
-      // U = 0, DU = 1e40 (fields.f90:183-186)
-      const int nU = d->mode == 2 ? 2 : 1;
-      if ((rc = h->alloc_planes(&B.U, nU, g.plane)) || (rc = h->alloc_planes(&B.DU, nU, g.plane)) ||
-          (rc = h->alloc_planes(&B.Utap, nU, g.plane)))
-        return rc;
-      std::vector<double> big((size_t)nU * g.plane, 1e40);
-      CUDA_TRY(cudaMemcpy(B.DU, big.data(), big.size() * sizeof(double), cudaMemcpyHostToDevice));
-      h->extras = true;
-    }
-    if (d->peak) {
-      if ((rc = h->alloc_planes(&B.pgv, 1, g.plane)) || (rc = h->alloc_planes(&B.pga, 1, g.plane))) return rc;
-      h->extras = true;
+      if (d->src.forcing_filename) {
+        double* fo = nullptr;
+        double* fn = nullptr;
+        if ((rc = h->alloc_planes(&fo, nF, g.plane)) || (rc = h->alloc_planes(&fn, nF, g.plane))) return rc;
+        B.frc_old = fo;
+        B.frc_new = fn;
+        h->forcing = true;
+      }
+      B.U = B.DU = B.Utap = B.pgv = B.pga = nullptr;
+      if (d->displacement) {
+        // U = 0, DU = 1e40 (fields.f90:183-186)
+        const int nU = d->mode == 2 ? 2 : 1;
+        if ((rc = h->alloc_planes(&B.U, nU, g.plane)) || (rc = h->alloc_planes(&B.DU, nU, g.plane)) ||
+            (rc = h->alloc_planes(&B.Utap, nU, g.plane)))
+          return rc;
+        std::vector<double> big((size_t)nU * g.plane, 1e40);
+        CUDA_TRY(cudaMemcpy(B.DU, big.data(), big.size() * sizeof(double), cudaMemcpyHostToDevice));
+        h->extras = true;
+      }
+      if (d->peak) {
+        if ((rc = h->alloc_planes(&B.pgv, 1, g.plane)) || (rc = h->alloc_planes(&B.pga, 1, g.plane))) return rc;
+        h->extras = true;
+      }
     }
     B.rinv_b = 1.0 / fb.rho;
     for (int s = 1; s <= op.pI; ++s) {
@@ -682,12 +738,12 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       source_weights(fb.src_hx, fb.src_ax, B.src_wx);
       source_weights(fb.src_hy, fb.src_ay, B.src_wy);
     }
-    B.tiles_x = (g.nx + TX - 1) / TX;
-    int tiles_y = (g.ny + TY - 1) / TY;
+    B.tiles_x = own ? (g.nx + TX - 1) / TX : 0;
+    int tiles_y = own ? (g.ny + TY - 1) / TY : 0;
     B.tile_begin = tiles;
     tiles += B.tiles_x * tiles_y;
     B.march_unit_begin = h->march_units;
-    h->march_units += (long long)((g.nx + MW - 1) / MW) * ((g.ny + MR - 1) / MR);
+    if (own) h->march_units += (long long)((g.nx + MW - 1) / MW) * ((g.ny + MR - 1) / MR);
   }
   h->total_tiles = tiles;
   h->body_on_device = d->body != nullptr;
@@ -747,6 +803,18 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
       }
       if ((rc = h->upload(&I.icoef, ic.data(), ic.size()))) return rc;
     }
+    I.rem_m = I.rem_p = nullptr;
+    I.send = nullptr;
+    if (h->owns(fi.iblockm) != h->owns(fi.iblockp)) {
+      // one side on this GPU, the other on a peer: receive buffer for the
+      // peer's edge values, two send slots (alternating stages) for ours
+      double *rem = nullptr, *snd = nullptr;
+      if ((rc = h->alloc(&rem, (size_t)nF * I.n)) || (rc = h->alloc(&snd, 2 * (size_t)nF * I.n))) return rc;
+      CUDA_TRY(cudaMemset(rem, 0, (size_t)nF * I.n * sizeof(double)));
+      (h->owns(fi.iblockm) ? I.rem_p : I.rem_m) = rem;
+      I.send = snd;
+      h->part_ifaces.push_back(k);
+    }
     if ((rc = h->upload(&I.nhat, fi.nhat, 2 * (size_t)I.n))) return rc;
     if ((rc = h->upload(&I.x, fi.x, (size_t)I.n))) return rc;
     if ((rc = h->upload(&I.y, fi.y, (size_t)I.n))) return rc;
@@ -778,6 +846,8 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   // interface work segments; closure strips per block
   int nseg = 0, start = 0;
   for (int k = 0; k < d->nifaces; ++k) {
+    // an interface between two blocks of other GPUs is solved there
+    if (!h->owns(D.ifc[k].im) && !h->owns(D.ifc[k].ip)) continue;
     D.seg_kind[nseg] = 1; D.seg_a[nseg] = k; D.seg_b[nseg] = 0; D.seg_start[nseg] = start;
     start += D.ifc[k].n;
     ++nseg;
@@ -786,8 +856,9 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     long long cs = 0;
     for (int b = 0; b < d->nblocks; ++b) {
       const BlockGeom& g = h->geom[b];
-      long long strip[4] = {(long long)op.nbst * g.nx, (long long)op.nbst * g.nx,
-                            (long long)(g.ny - 2 * op.nbst) * op.nbst, (long long)(g.ny - 2 * op.nbst) * op.nbst};
+      const long long w = h->owns(b) ? 1 : 0;
+      long long strip[4] = {w * op.nbst * g.nx, w * op.nbst * g.nx, w * (g.ny - 2 * op.nbst) * op.nbst,
+                            w * (g.ny - 2 * op.nbst) * op.nbst};
       for (int q = 0; q < 4; ++q) { D.cstart[4 * b + q] = cs; cs += strip[q]; }
     }
     D.cstart[4 * d->nblocks] = cs;
@@ -923,11 +994,23 @@ int build_step_graphs(fdmap_gpu* h, double dt) {
 
 extern "C" {
 
-int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu** out) {
+}  // extern "C"
+
+namespace {
+
+int create_impl(const fdmap_desc* d, int device, int init_edges, const int* owned, fdmap_gpu** out) {
   if (!out) return set_err(FDMAP_ERR_INVALID_ARG, "null handle pointer");
   *out = nullptr;
   int rc = validate(d);
   if (rc) return rc;
+  if (owned) {
+    int nown = 0;
+    for (int b = 0; b < d->nblocks; ++b) nown += owned[b] != 0;
+    if (nown == 0) return set_err(FDMAP_ERR_INVALID_ARG, "a partition must own at least one block");
+    if (d->body) return set_err(FDMAP_ERR_UNSUPPORTED, "a partitioned domain needs the body built on the host");
+    if (d->energy_balance || d->src.forcing_filename)
+      return set_err(FDMAP_ERR_UNSUPPORTED, "energy balance and forcing files are not available on a partition");
+  }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return set_err(FDMAP_ERR_CUDA, "no CUDA device available");
@@ -945,7 +1028,21 @@ int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu*
     return set_err(FDMAP_ERR_CUDA, "cannot initialise device");
   }
   h->stream = h->own_stream;
+  if (owned) {
+    h->owned.assign(owned, owned + d->nblocks);
+    for (auto& o : h->owned) o = o != 0;
+    if (cudaEventCreateWithFlags(&h->ev_packed, cudaEventDisableTiming) != cudaSuccess) {
+      delete h;
+      return set_err(FDMAP_ERR_CUDA, "cannot create events");
+    }
+  }
   rc = build(h, d);
+  if (rc == FDMAP_OK && h->partitioned()) {
+    // the edge exchange is a host callback (or a group step): no step graphs,
+    // and interface solves stay apart from the closure strips
+    h->use_graphs = false;
+    h->fused = 0;
+  }
   if (rc == FDMAP_OK && init_edges) rc = fdmap_gpu_init_edges(h, d->t0);
   if (rc == FDMAP_OK) rc = fdmap_gpu_synchronize(h);
   if (rc) {
@@ -958,12 +1055,170 @@ int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu*
   return FDMAP_OK;
 }
 
+StageArgs init_edge_args(const fdmap_gpu* h, double t) {
+  StageArgs a{};
+  a.A = 0.0; a.Bdt = 0.0; a.t = t; a.in = h->cur; a.out = 1 - h->cur; a.scale = 0; a.update = 0;
+  return a;
+}
+
+// the stage arguments of every stage of one step from buffer `cur`
+std::vector<StageArgs> step_args(const fdmap_gpu* h, int cur, double t0, double dt, bool final_step) {
+  std::vector<StageArgs> v;
+  for (int s = 0; s < h->rk.nstage; ++s) {
+    StageArgs a{};
+    a.A = h->rk.A[s];
+    a.Bdt = h->rk.B[s] * dt;
+    a.t = t0 + h->rk.C[s] * dt;
+    a.C = h->rk.C[s];
+    a.t0 = t0;
+    a.dt = dt;
+    a.first = s == 0 ? 1 : 0;
+    a.in = cur;
+    a.out = 1 - cur;
+    a.scale = 1;
+    a.update = final_step ? 0 : 1;
+    v.push_back(a);
+    if (final_step) break;
+    cur = 1 - cur;
+  }
+  return v;
+}
+
+// Group of partitions driven from one host thread (one handle per GPU, or
+// several on one GPU): after every handle has packed its edge values for the
+// stage, each handle's boundary stream waits for its peers' pack and copies
+// their values into its receive buffers (peer-to-peer between GPUs), then
+// finishes the stage.  Send slots alternate between stages, so a pack never
+// overwrites a slot a peer may still be reading.
+int group_exchange(fdmap_gpu* const* hs, int n, bool main_stream) {
+  for (int i = 0; i < n; ++i) {
+    fdmap_gpu* h = hs[i];
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaStream_t bs = main_stream ? h->stream : boundary_stream(h);
+    for (int k : h->part_ifaces) {
+      const DevIface& I = h->hdom.ifc[k];
+      const int rb = h->owns(I.im) ? I.ip : I.im;  // the block on a peer
+      fdmap_gpu* p = nullptr;
+      for (int j = 0; j < n; ++j)
+        if (j != i && hs[j]->owns(rb) && hs[j]->partitioned()) p = hs[j];
+      if (!p) return set_err(FDMAP_ERR_INVALID_ARG, "no handle of the group owns block " + std::to_string(rb));
+      const DevIface& P = p->hdom.ifc[k];
+      const size_t cnt = (size_t)h->nF * I.n;
+      const double* src = P.send + (size_t)(p->xstage & 1) * cnt;
+      double* dst = const_cast<double*>(I.rem_m ? I.rem_m : I.rem_p);
+      CUDA_TRY(cudaStreamWaitEvent(bs, p->ev_packed, 0));
+      if (p->device == h->device) CUDA_TRY(cudaMemcpyAsync(dst, src, cnt * sizeof(double), cudaMemcpyDeviceToDevice, bs));
+      else CUDA_TRY(cudaMemcpyPeerAsync(dst, h->device, src, p->device, cnt * sizeof(double), bs));
+    }
+  }
+  return FDMAP_OK;
+}
+
+int check_group(fdmap_gpu* const* hs, int n) {
+  if (!hs || n < 1) return set_err(FDMAP_ERR_INVALID_ARG, "empty group");
+  for (int i = 0; i < n; ++i)
+    if (!hs[i] || !hs[i]->partitioned()) return set_err(FDMAP_ERR_INVALID_ARG, "group members must be partitions");
+  return FDMAP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdmap_gpu_create(const fdmap_desc* d, int device, int init_edges, fdmap_gpu** out) {
+  return create_impl(d, device, init_edges, nullptr, out);
+}
+
 int fdmap_gpu_init_edges(fdmap_gpu* h, double t) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
   CUDA_TRY(cudaSetDevice(h->device));
-  StageArgs a{};
-  a.A = 0.0; a.Bdt = 0.0; a.t = t; a.in = h->cur; a.out = 1 - h->cur; a.scale = 0; a.update = 0;
+  const StageArgs a = init_edge_args(h, t);
+  if (!h->part_ifaces.empty()) {
+    // the peers' edge values first, through the exchange callback
+    if (!h->exchange) return set_err(FDMAP_ERR_INVALID_ARG, "partitioned domain without an exchange callback");
+    int rc = pack_partition_edges(h, a, h->stream);
+    if (rc) return rc;
+    rc = h->exchange(h->exchange_user, h->xstage, (void*)h->stream);
+    if (rc) return set_err(FDMAP_ERR_CUDA, "edge exchange callback failed (" + std::to_string(rc) + ")");
+    h->xstage++;
+  }
   return launch_edges(h, a);
+}
+
+int fdmap_gpu_create_part(const fdmap_desc* d, int device, const int* owned, fdmap_gpu** out) {
+  if (!owned) return set_err(FDMAP_ERR_INVALID_ARG, "null ownership list");
+  return create_impl(d, device, 0, owned, out);
+}
+
+int fdmap_gpu_part_interfaces(fdmap_gpu* h, int* ifaces, int max) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  const int n = (int)h->part_ifaces.size();
+  for (int q = 0; q < n && q < max && ifaces; ++q) ifaces[q] = h->part_ifaces[(size_t)q];
+  return n;
+}
+
+int fdmap_gpu_part_buffers(fdmap_gpu* h, int iface, long long stage, double** send, double** recv, long long* count) {
+  if (!h || iface < 0 || iface >= h->hdom.nifaces) return set_err(FDMAP_ERR_INVALID_ARG, "bad part_buffers arguments");
+  const DevIface& I = h->hdom.ifc[iface];
+  if (!I.send) return set_err(FDMAP_ERR_INVALID_ARG, "interface has no side on a peer GPU");
+  const size_t cnt = (size_t)h->nF * I.n;
+  if (send) *send = I.send + (size_t)(stage & 1) * cnt;
+  if (recv) *recv = const_cast<double*>(I.rem_m ? I.rem_m : I.rem_p);
+  if (count) *count = (long long)cnt;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_exchange(fdmap_gpu* h, fdmap_exchange_fn fn, void* user) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  h->exchange = fn;
+  h->exchange_user = user;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_group_init_edges(fdmap_gpu* const* hs, int n, double t) {
+  int rc = check_group(hs, n);
+  if (rc) return rc;
+  for (int i = 0; i < n; ++i) {
+    CUDA_TRY(cudaSetDevice(hs[i]->device));
+    if ((rc = pack_partition_edges(hs[i], init_edge_args(hs[i], t), hs[i]->stream))) return rc;
+  }
+  if ((rc = group_exchange(hs, n, true))) return rc;
+  for (int i = 0; i < n; ++i) {
+    hs[i]->xstage++;
+    CUDA_TRY(cudaSetDevice(hs[i]->device));
+    if ((rc = launch_edges(hs[i], init_edge_args(hs[i], t)))) return rc;
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_group_time_step(fdmap_gpu* const* hs, int n, double t0, double dt, int final_step) {
+  int rc = check_group(hs, n);
+  if (rc) return rc;
+  std::vector<std::vector<StageArgs>> args;
+  for (int i = 0; i < n; ++i) args.push_back(step_args(hs[i], hs[i]->cur, t0, dt, final_step != 0));
+  for (size_t s = 0; s < args[0].size(); ++s) {
+    for (int i = 0; i < n; ++i) {
+      CUDA_TRY(cudaSetDevice(hs[i]->device));
+      if ((rc = stage_begin(hs[i], args[(size_t)i][s]))) return rc;
+    }
+    if ((rc = group_exchange(hs, n, false))) return rc;
+    for (int i = 0; i < n; ++i) {
+      hs[i]->xstage++;
+      CUDA_TRY(cudaSetDevice(hs[i]->device));
+      if ((rc = stage_end(hs[i], args[(size_t)i][s]))) return rc;
+    }
+  }
+  for (int i = 0; i < n; ++i)
+    if (!final_step && (hs[i]->rk.nstage & 1)) hs[i]->cur = 1 - hs[i]->cur;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_group_run(fdmap_gpu* const* hs, int n, double t_start, double dt, int n_first, int n_last, int nt) {
+  for (int k = n_first; k <= n_last; ++k) {
+    int rc = fdmap_gpu_group_time_step(hs, n, t_start + (double)(k - 1) * dt, dt, k == nt);
+    if (rc) return rc;
+  }
+  return FDMAP_OK;
 }
 
 int fdmap_gpu_time_step(fdmap_gpu* h, double t0, double dt, int final_step) {
@@ -1028,6 +1283,7 @@ int fdmap_gpu_get_fields(fdmap_gpu* h, double* F, double* DF) {
     if (!dst) continue;
     // padded block planes -> one contiguous global array on the device -> one copy
     for (int b = 0; b < h->hdom.nblocks; ++b) {
+      if (!h->owns(b)) continue;  // body on a peer GPU
       const BlockGeom& g = h->geom[b];
       const double* src = which == 0 ? h->hdom.blk[b].F[h->cur] : h->hdom.blk[b].DF;
       dim3 grid((g.nx + 255) / 256, g.ny);
@@ -1052,6 +1308,7 @@ int fdmap_gpu_set_fields(fdmap_gpu* h, const double* F, const double* DF) {
     // one copy of the global array, then scattered into the padded block planes
     CUDA_TRY(cudaMemcpyAsync(h->d_global, src, (size_t)NN * nF * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     for (int b = 0; b < h->hdom.nblocks; ++b) {
+      if (!h->owns(b)) continue;  // body on a peer GPU
       const BlockGeom& g = h->geom[b];
       double* dst = which == 0 ? h->hdom.blk[b].F[h->cur] : h->hdom.blk[b].DF;
       dim3 grid((g.pitch + 255) / 256, g.ny);
@@ -1077,6 +1334,7 @@ int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out) {
     return set_err(FDMAP_ERR_INVALID_ARG, "bad get_metric arguments");
   CUDA_TRY(cudaSetDevice(h->device));
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const DevBlock& B = h->hdom.blk[b];
     const double* planes[6] = {B.xq, B.xr, B.yq, B.yr, B.Ji, B.J};
     if (!planes[which]) return set_err(FDMAP_ERR_INVALID_ARG, "the Jacobian plane is kept for dissipative blocks only");
@@ -1084,6 +1342,7 @@ int fdmap_gpu_get_metric(fdmap_gpu* h, int which, double* out) {
   const long long NN = (long long)h->nx_g * h->ny_g;
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const DevBlock& B = h->hdom.blk[b];
     const double* planes[6] = {B.xq, B.xr, B.yq, B.yr, B.Ji, B.J};
     const BlockGeom& g = h->geom[b];
@@ -1105,6 +1364,7 @@ int body_planes(fdmap_gpu* h, int which, double* out, const double* in) {
   const int np = which <= 1 ? nU : 1;
   const long long NN = (long long)h->nx_g * h->ny_g;
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const DevBlock& B = h->hdom.blk[b];
     double* const planes[4] = {B.U, B.DU, B.pgv, B.pga};
     if (!planes[which])
@@ -1114,6 +1374,7 @@ int body_planes(fdmap_gpu* h, int which, double* out, const double* in) {
   CUDA_TRY(cudaSetDevice(h->device));
   if (in) CUDA_TRY(cudaMemcpyAsync(h->d_global, in, (size_t)NN * np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const DevBlock& B = h->hdom.blk[b];
     double* const planes[4] = {B.U, B.DU, B.pgv, B.pga};
     const BlockGeom& g = h->geom[b];
@@ -1182,6 +1443,7 @@ int fdmap_gpu_get_pml(fdmap_gpu* h, int which, double* out) {
   const long long NN = (long long)h->nx_g * h->ny_g;
   CUDA_TRY(cudaMemsetAsync(h->d_global, 0, (size_t)NN * nF * sizeof(double), h->stream));
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const double* W = which == 0 ? h->hdom.blk[b].Wx : h->hdom.blk[b].Wy;
     if (!W) continue;
     const BlockGeom& g = h->geom[b];
@@ -1202,6 +1464,7 @@ int fdmap_gpu_set_pml(fdmap_gpu* h, int which, const double* in) {
   const long long NN = (long long)h->nx_g * h->ny_g;
   CUDA_TRY(cudaMemcpyAsync(h->d_global, in, (size_t)NN * nF * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     double* W = which == 0 ? h->hdom.blk[b].Wx : h->hdom.blk[b].Wy;
     if (!W) continue;
     const BlockGeom& g = h->geom[b];
@@ -1338,6 +1601,7 @@ int fdmap_gpu_check_finite(fdmap_gpu* h, long long* count) {
   unsigned long long* d_count = h->d_status + 2;  // scratch word of the status block
   CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(unsigned long long), h->stream));
   for (int b = 0; b < h->hdom.nblocks; ++b) {
+    if (!h->owns(b)) continue;  // body on a peer GPU
     const DevBlock& B = h->hdom.blk[b];
     const long long n = (long long)h->nF * B.ny * B.nx;
     count_nonfinite_block<<<(int)std::min<long long>((n + 255) / 256, 4 * 148), 256, 0, h->stream>>>(

@@ -1231,6 +1231,13 @@ extern "C" int fdmap_host_iface_info(const fdmap_domain* dom, int iface, int* in
   return FDMAP_OK;
 }
 
+extern "C" int fdmap_host_iface_blocks(const fdmap_domain* dom, int iface, int* blocks) {
+  if (!dom || !blocks || iface < 0 || iface >= dom->desc.nifaces) return FDMAP_ERR_INVALID_ARG;
+  const fdmap_iface& I = dom->desc.ifaces[iface];
+  blocks[0] = I.iblockm; blocks[1] = I.iblockp;
+  return FDMAP_OK;
+}
+
 extern "C" const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface, int which) {
   if (!dom || iface < 0 || iface >= dom->desc.nifaces) return nullptr;
   const fdmap_iface& I = dom->desc.ifaces[iface];

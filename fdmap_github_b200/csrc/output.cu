@@ -355,6 +355,7 @@ int fdmap_gpu_output_add(fdmap_gpu* h, const char* name, int kind, int index, in
 
 int fdmap_gpu_output_open(fdmap_gpu* h, const char* prefix, int ring_steps) {
   if (!h || !prefix) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  if (h->partitioned()) return set_err(FDMAP_ERR_UNSUPPORTED, "device-side output is not available on a partition");
   if (!h->out || h->out->items.empty()) return set_err(FDMAP_ERR_INVALID_ARG, "no output items");
   if (h->out->open) return set_err(FDMAP_ERR_INVALID_ARG, "outputs already open");
   if (ring_steps < 1) return set_err(FDMAP_ERR_INVALID_ARG, "ring must hold at least one step");

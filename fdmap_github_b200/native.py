@@ -52,6 +52,7 @@ SIGNATURES = {
     "fdmap_host_block_cdiss": (C.c_double, [_VP, C.c_int]),
     "fdmap_host_iface_info": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
     "fdmap_host_iface_xy": (_DP, [_VP, C.c_int, C.c_int]),
+    "fdmap_host_iface_blocks": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int)]),
     "fdmap_host_side_array": (_DP, [_VP, C.c_int, C.c_int, C.c_char_p, C.POINTER(C.c_longlong)]),
     "fdmap_host_array": (_DP, [_VP, C.c_char_p, C.POINTER(C.c_longlong)]),
     "fdmap_host_last_error": (C.c_char_p, []),
@@ -93,6 +94,15 @@ SIGNATURES = {
     "fdmap_gpu_output_open": (C.c_int, [_VP, C.c_char_p, C.c_int]),
     "fdmap_gpu_output_flush": (C.c_int, [_VP]),
     "fdmap_gpu_output_close": (C.c_int, [_VP]),
+    "fdmap_gpu_create_part": (C.c_int, [_VP, C.c_int, C.POINTER(C.c_int), C.POINTER(_VP)]),
+    "fdmap_gpu_part_interfaces": (C.c_int, [_VP, C.POINTER(C.c_int), C.c_int]),
+    "fdmap_gpu_part_buffers": (C.c_int, [_VP, C.c_int, C.c_longlong, C.POINTER(_DP), C.POINTER(_DP),
+                                         C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_set_exchange": (C.c_int, [_VP, _VP, _VP]),
+    "fdmap_gpu_group_init_edges": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_double]),
+    "fdmap_gpu_group_time_step": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_double, C.c_double, C.c_int]),
+    "fdmap_gpu_group_run": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                      C.c_int]),
     "fdmap_gpu_launch_count": (C.c_longlong, [_VP]),
     "fdmap_gpu_device_bytes": (C.c_longlong, [_VP]),
     "fdmap_gpu_destroy": (None, [_VP]),

@@ -199,6 +199,52 @@ int fdmap_gpu_output_close(fdmap_gpu* h);
  * should come before any stream capture. */
 int fdmap_gpu_fault_max_noalloc(fdmap_gpu* h, int iface, int field, double* out);
 
+/* ------------------------------------------------------------------------
+ * Block-aligned partition over several GPUs.  Replaces the reference's
+ * exchange of interface edge rows between processes (exchange_edge,
+ * mpi_routines2d.f90:168-208, called from domain.f90:1179-1322): each GPU
+ * holds and steps the blocks it owns; an interface whose two sides live on
+ * different GPUs is solved on both, redundantly and identically, from the
+ * local side's edge values and the peer's, which arrive every stage.  Blocks
+ * never share grid nodes, so no halo rows are exchanged.
+ *
+ * fdmap_gpu_create_part: owned[b] != 0 for the blocks this GPU steps.  The
+ * other blocks' body arrays are not allocated.  No initial edge solve is run
+ * (it needs the peers' values): call fdmap_gpu_init_edges (callback) or
+ * fdmap_gpu_group_init_edges (group) once every partition exists.
+ * Outputs, energy balance, forcing files and a body built on the device are
+ * refused (FDMAP_ERR_UNSUPPORTED) on a partition.
+ * ---------------------------------------------------------------------- */
+int fdmap_gpu_create_part(const fdmap_desc* d, int device, const int* owned, fdmap_gpu** h);
+
+/* Interfaces with exactly one side on this GPU (written to ifaces[0..max)); returns their count. */
+int fdmap_gpu_part_interfaces(fdmap_gpu* h, int* ifaces, int max);
+
+/* Device buffers of interface `iface` for exchange number `stage`: *send
+ * holds this GPU's side's edge values, *recv receives the peer's, both
+ * count = nF * (p - m + 1) doubles laid out [l*n + k] (field l, interface
+ * node k). */
+int fdmap_gpu_part_buffers(fdmap_gpu* h, int iface, long long stage, double** send, double** recv,
+                           long long* count);
+
+/* Exchange callback, called by the host once per stage (and by
+ * fdmap_gpu_init_edges) after this GPU's edge values have been packed into
+ * the send buffers, with the exchange number and the cudaStream_t on which
+ * the interface solve of the stage follows.  It queues (on that stream, or
+ * otherwise completes before returning) the transfer of every send buffer to
+ * the peer and of the peer's values into the receive buffers -- NCCL
+ * ncclSend / ncclRecv in a group, MPI, or a device copy -- and returns 0. */
+typedef int (*fdmap_exchange_fn)(void* user, long long stage, void* stream);
+int fdmap_gpu_set_exchange(fdmap_gpu* h, fdmap_exchange_fn fn, void* user);
+
+/* The partitions of one domain driven by one host thread (one handle per
+ * GPU, or several on one GPU): every stage, after all of them have packed
+ * their edge values, each copies its peers' values peer to peer on its
+ * boundary stream and finishes the stage. */
+int fdmap_gpu_group_init_edges(fdmap_gpu* const* hs, int n, double t);
+int fdmap_gpu_group_time_step(fdmap_gpu* const* hs, int n, double t0, double dt, int final_step);
+int fdmap_gpu_group_run(fdmap_gpu* const* hs, int n, double t_start, double dt, int n_first, int n_last, int nt);
+
 /* Kernel launches issued by the last fdmap_gpu_run / time_step call. */
 long long fdmap_gpu_launch_count(fdmap_gpu* h);
 

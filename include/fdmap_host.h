@@ -72,6 +72,10 @@ int fdmap_host_iface_n(const fdmap_domain* dom, int iface);
  * indices along the interface), coupling. */
 int fdmap_host_iface_info(const fdmap_domain* dom, int iface, int* info);
 
+/* Blocks on the minus and plus side of interface `iface`: blocks[2], 0-based
+ * (interface_list iblockm / iblockp, interfaces.f90:26-135). */
+int fdmap_host_iface_blocks(const fdmap_domain* dom, int iface, int* blocks);
+
 /* Interface geometry: x[n], y[n] of interface `iface` (NULL if absent). */
 const double* fdmap_host_iface_xy(const fdmap_domain* dom, int iface, int which);
 

@@ -49,6 +49,10 @@ def lib() -> C.CDLL:
         L.oracle_set_side_u.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP, _DP]
         L.oracle_set_body_extras.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP]
         L.oracle_set_pml.argtypes = [C.c_void_p, C.c_int, _DP]
+        L.oracle_set_owned.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+        L.oracle_set_exchange.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.oracle_get_iface_edge.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
+        L.oracle_set_iface_edge.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         _lib = L
     return _lib
 
@@ -99,12 +103,14 @@ class OracleDomain:
             lib().oracle_init_edges(self._o, host.t0)
 
     def time_step_LS(self, t0: float, dt: float, final_step: bool = False) -> None:
-        lib().oracle_time_step(self._o, t0, dt, int(final_step))
+        if lib().oracle_time_step(self._o, t0, dt, int(final_step)) != 0:
+            raise RuntimeError("oracle_time_step failed")
 
     def run(self, n_first: int, n_last: int, t_start=None, dt=None, nt=None) -> None:
         h = self.host
-        lib().oracle_run(self._o, h.t0 if t_start is None else t_start, h.dt if dt is None else dt,
-                         n_first, n_last, h.nt if nt is None else nt)
+        if lib().oracle_run(self._o, h.t0 if t_start is None else t_start, h.dt if dt is None else dt,
+                            n_first, n_last, h.nt if nt is None else nt) != 0:
+            raise RuntimeError("oracle_run failed")
 
     def get_fields(self, want_F: bool = True, want_DF: bool = False):
         F = np.empty((self.nF, self.ny, self.nx)) if want_F else None
@@ -234,3 +240,48 @@ class OracleDomain:
 
 def num_threads() -> int:
     return lib().oracle_num_threads()
+
+
+ORACLE_EXCHANGE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_longlong)
+
+
+class OraclePartition(OracleDomain):
+    """One rank's part of a block-aligned partition on the CPU oracle: the
+    other ranks' blocks are NaN here, and every stage the interface edge
+    values are exchanged with the peers through torch.distributed (gloo),
+    by the same exchange_edges the GPU partitions use."""
+
+    def __init__(self, host, plan, rank: int, group=None):
+        super().__init__(host, init_edges=False)
+        self.plan, self.rank, self.group = plan, rank, group
+        owned = (C.c_int * host.nblocks)(*plan.owned(rank))
+        lib().oracle_set_owned(self._o, owned)
+        self.pairs = plan.pairs(rank)
+        self.errors = []
+        self._cb = ORACLE_EXCHANGE(self._exchange)
+        lib().oracle_set_exchange(self._o, C.cast(self._cb, C.c_void_p), None)
+        if lib().oracle_init_edges(self._o, host.t0) != 0:
+            raise RuntimeError("initial edge exchange failed: " + "; ".join(self.errors))
+
+    def _exchange(self, user, stage) -> int:
+        try:
+            import torch
+
+            from fdmap_github_b200.partition import exchange_edges
+
+            send, recv = [], []
+            for k, side, _ in self.pairs:
+                n = self.host.iface_n(k)
+                buf = np.empty(self.nF * n)
+                lib().oracle_get_iface_edge(self._o, k, side, _p(buf))
+                send.append(torch.from_numpy(buf))
+                recv.append(torch.empty(self.nF * n, dtype=torch.float64))
+            exchange_edges(self.pairs, send, recv, self.group)
+            for (k, side, _), r in zip(self.pairs, recv):
+                v = np.ascontiguousarray(r.numpy())
+                lib().oracle_set_iface_edge(self._o, k, 1 - side, _p(v))
+            return 0
+        except Exception as e:  # noqa: BLE001  (reported as a failed step)
+            self.errors.append(repr(e))
+            return 1
+

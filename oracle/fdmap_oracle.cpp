@@ -207,6 +207,12 @@ struct oracle_domain {
   long long newton_stop;   // solves whose retry failed too (the reference stops there)
   int newton_imax = 99;    // friction.f90:924 imax
   bool tap = false;        // keep each step's stage-1 fault fields (write_output's view, time_step.f90:129)
+  // block-aligned partition: blocks this rank steps (empty: all) and the
+  // exchange of interface edge values, called after prepare_edges
+  std::vector<char> owned;
+  int (*exchange)(void*, long long) = nullptr;
+  void* exchange_user = nullptr;
+  long long xstage = 0;
 };
 
 namespace {
@@ -1525,6 +1531,24 @@ void update_fields_all(oracle_domain& D, double Bdt) {
       for (size_t q = 0; q < S.U.size(); ++q) S.U[q] = S.U[q] + Bdt * S.DU[q];
 }
 
+// exchange_edge (mpi_routines2d.f90:168-208) for a partitioned run: the
+// caller's callback replaces the edge values of every interface side that
+// lives on another rank with that rank's values (oracle_set_iface_edge)
+int exchange_edges(oracle_domain& D) {
+  if (D.owned.empty()) return FDMAP_OK;
+  if (!D.exchange) return FDMAP_ERR_INVALID_ARG;
+  const int rc = D.exchange(D.exchange_user, D.xstage);
+  D.xstage++;
+  return rc ? FDMAP_ERR_IO : FDMAP_OK;
+}
+
+// side and side-local offset of interface I's minus (side 0) or plus (side 1) nodes
+Side& iface_side(oracle_domain& D, const Ifc& I, int side, int& off) {
+  Blk& B = D.blk[side == 0 ? I.im : I.ip];
+  off = I.m - (I.direction == 0 ? B.mgy : B.mgx);
+  return B.side[side == 0 ? (I.direction == 0 ? 1 : 3) : (I.direction == 0 ? 0 : 2)];
+}
+
 }  // namespace
 
 extern "C" {
@@ -1654,6 +1678,7 @@ int oracle_init_edges(oracle_domain* o, double t) {
   if (!o) return FDMAP_ERR_INVALID_ARG;
   o->t = t;
   prepare_edges(*o);
+  if (int rc = exchange_edges(*o)) return rc;
   enforce_edge_conditions(*o, 0.0);
   return FDMAP_OK;
 }
@@ -1666,6 +1691,7 @@ int oracle_time_step(oracle_domain* o, double t0, double dt, int final_step) {
   for (int stage = 1; stage <= D.rk.nstage; ++stage) {
     scale_rates_all(D, D.rk.A[stage - 1]);
     prepare_edges(D);
+    if (int rc = exchange_edges(D)) return rc;
     enforce_edge_conditions(D, D.rk.B[stage - 1] * dt);
     set_rates_all(D);
     if (stage == 1 && D.tap)
@@ -1735,6 +1761,55 @@ int oracle_get_fhat(const oracle_domain* o, int b, int s, double* out) {
 long long oracle_newton_failures(const oracle_domain* o) { return o ? o->newton_fail : -1; }
 
 long long oracle_newton_stops(const oracle_domain* o) { return o ? o->newton_stop : -1; }
+
+int oracle_set_owned(oracle_domain* o, const int* owned) {
+  if (!o || !owned) return FDMAP_ERR_INVALID_ARG;
+  o->owned.assign(owned, owned + o->nblocks);
+  // the other ranks' blocks hold NaN here: any read of them that is not an
+  // exchanged edge value spreads NaN into the result
+  const size_t NN = (size_t)o->nx * o->ny;
+  const double nan = std::nan("");
+  for (int b = 0; b < o->nblocks; ++b) {
+    if (owned[b]) continue;
+    const Blk& B = o->blk[b];
+    for (int l = 0; l < o->nF; ++l)
+      for (int j = B.mgy; j <= B.pgy; ++j)
+        for (int i = B.mgx; i <= B.pgx; ++i) {
+          o->F[G2(*o, i, j) + NN * l] = nan;
+          o->DF[G2(*o, i, j) + NN * l] = nan;
+        }
+  }
+  return FDMAP_OK;
+}
+
+int oracle_set_exchange(oracle_domain* o, int (*fn)(void*, long long), void* user) {
+  if (!o) return FDMAP_ERR_INVALID_ARG;
+  o->exchange = fn;
+  o->exchange_user = user;
+  return FDMAP_OK;
+}
+
+int oracle_get_iface_edge(oracle_domain* o, int iface, int side, double* out) {
+  if (!o || iface < 0 || iface >= o->nifaces || side < 0 || side > 1 || !out) return FDMAP_ERR_INVALID_ARG;
+  const Ifc& I = o->ifc[iface];
+  int off = 0;
+  const Side& S = iface_side(*o, I, side, off);
+  const int n = I.p - I.m + 1;
+  for (int l = 0; l < o->nF; ++l)
+    for (int k = 0; k < n; ++k) out[(size_t)l * n + k] = S.F[off + k + (size_t)S.n * l];
+  return FDMAP_OK;
+}
+
+int oracle_set_iface_edge(oracle_domain* o, int iface, int side, const double* in) {
+  if (!o || iface < 0 || iface >= o->nifaces || side < 0 || side > 1 || !in) return FDMAP_ERR_INVALID_ARG;
+  const Ifc& I = o->ifc[iface];
+  int off = 0;
+  Side& S = iface_side(*o, I, side, off);
+  const int n = I.p - I.m + 1;
+  for (int l = 0; l < o->nF; ++l)
+    for (int k = 0; k < n; ++k) S.F[off + k + (size_t)S.n * l] = in[(size_t)l * n + k];
+  return FDMAP_OK;
+}
 
 int oracle_set_tap(oracle_domain* o, int on) {
   if (!o) return FDMAP_ERR_INVALID_ARG;

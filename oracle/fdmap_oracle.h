@@ -100,6 +100,18 @@ int oracle_set_body_extras(oracle_domain* o, const double* U, const double* DU, 
                            const double* pga);
 int oracle_set_pml(oracle_domain* o, int which, const double* in);
 
+/* Block-aligned partition (the reference's exchange_edge between processes,
+ * mpi_routines2d.f90:168-208): owned[b] != 0 for the blocks this rank steps;
+ * the others are filled with NaN.  Every stage (and the initial edge solve),
+ * after the edge values are gathered, `fn(user, exchange_number)` runs; it
+ * reads this rank's side of every interface cut by the partition
+ * (oracle_get_iface_edge, side 0 = minus, 1 = plus; [l*n + k]) and writes
+ * the peer's side (oracle_set_iface_edge), and returns 0. */
+int oracle_set_owned(oracle_domain* o, const int* owned);
+int oracle_set_exchange(oracle_domain* o, int (*fn)(void*, long long), void* user);
+int oracle_get_iface_edge(oracle_domain* o, int iface, int side, double* out);
+int oracle_set_iface_edge(oracle_domain* o, int iface, int side, const double* in);
+
 /* Number of OpenMP threads the oracle uses (1 when built without OpenMP). */
 int oracle_num_threads(void);
 
