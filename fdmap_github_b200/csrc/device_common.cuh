@@ -145,6 +145,7 @@ struct TmapSet {
   CUtensorMap MH[MAX_BLOCKS];      // yr, xr, box {WH, MR, 2}
   CUtensorMap MC[MAX_BLOCKS];      // yq, xq, Ji, box {MW, MR, 3}
   CUtensorMap HT[MAX_BLOCKS];      // heterogeneous material, box {MW, MR, NH}
+  CUtensorMap JH[MAX_BLOCKS];      // Jacobian of dissipative blocks, box {WH, MR, 1}
 };
 
 // Batched launches: CTAs [begin[k], begin[k+1]) serve instance k.  Returns

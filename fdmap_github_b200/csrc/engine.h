@@ -47,6 +47,7 @@ struct fdmap_gpu {
   DevDomain hdom{};
   DevDomain* ddom = nullptr;
   std::vector<void*> allocs;
+  std::vector<size_t> alloc_sizes;  // bytes of each allocation (state snapshots for the autotuner)
   long long bytes = 0;
   int cur = 0;
   int mode = 2, nF = 6, pI = 2, het = 0;
@@ -60,6 +61,8 @@ struct fdmap_gpu {
   long long march_units = 0;
   int march_grid = 0;
   int use_march = 1;
+  int march_shape = 0;      // tile shape of the march (shape_mw / shape_mr)
+  bool march_ext = false;   // the march variant with dissipation, PML, forcing and body extras
   bool dissipation = false;  // some block has Cdiss > 0 (tiled interior kernel)
   bool pml = false;  // some block has a perfectly matched layer (tiled interior kernel)
   bool forcing = false;  // tsunami forcing or forcing from file (tiled interior kernel)
@@ -120,6 +123,7 @@ struct fdmap_gpu {
     cudaError_t e = cudaMalloc(&q, bytes_);
     if (e != cudaSuccess) return set_err(FDMAP_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
     allocs.push_back(q);
+    alloc_sizes.push_back(bytes_);
     bytes += (long long)bytes_;
     *p = (T*)q;
     return FDMAP_OK;
@@ -223,6 +227,26 @@ int build_body(fdmap_gpu* h, const fdmap_desc* d, const SbpOperator& op);
 int engine_stage(fdmap_gpu* h, const StageArgs& a);
 
 int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+
+// The interior march for tile shape 0..2 (march_s<N>.cu): configure sets the
+// unit decomposition, tensor maps and grid for that shape (FDMAP_ERR_UNSUPPORTED
+// when the shape cannot serve the handle's variant); launch issues one stage.
+int march_configure_s0(fdmap_gpu* h);
+int march_configure_s1(fdmap_gpu* h);
+int march_configure_s2(fdmap_gpu* h);
+int march_launch_s0(fdmap_gpu* h, const StageArgs& a);
+int march_launch_s1(fdmap_gpu* h, const StageArgs& a);
+int march_launch_s2(fdmap_gpu* h, const StageArgs& a);
+int march_batch_s0(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+int march_batch_s1(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+int march_batch_s2(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+// configure for `shape` and publish the domain (device copy, step graphs dropped)
+int march_set_shape(fdmap_gpu* h, int shape);
+
+// Copy of every device allocation of a handle (its whole state), to put the
+// state back after timing runs; `out` receives the copies (freed by restore).
+int state_snapshot(fdmap_gpu* h, std::vector<void*>& out, cudaStream_t s);
+int state_restore(fdmap_gpu* h, std::vector<void*>& saved, cudaStream_t s);
 int batch_closure(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 int batch_edges(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 

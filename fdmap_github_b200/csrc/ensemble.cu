@@ -20,6 +20,7 @@
 
 #include "engine.h"
 #include "fdmap_gpu.h"
+#include "march_kernel.cuh"
 
 using namespace fdmap;
 
@@ -165,6 +166,53 @@ int ens_build_graphs(fdmap_ensemble* e, double dt) {
   return rc;
 }
 
+// per-instance device descriptors and tensor maps and the prefix of march
+// units over instances, for the instances' current march tile shape
+int ens_fill_plan(fdmap_ensemble* e) {
+  const int ninst = e->ninst;
+  std::vector<DevDomain> doms(ninst);
+  std::vector<TmapSet> maps(ninst);
+  std::vector<long long> ub(ninst + 1, 0);
+  long long units = 0;
+  int grid = 0;
+  for (int k = 0; k < ninst; ++k) {
+    fdmap_gpu* h = e->inst[k];
+    if (h->march_shape != e->proto->march_shape)
+      return set_err(FDMAP_ERR_INVALID_ARG, "ensemble instances must share the march tile shape");
+    doms[k] = h->hdom;
+    maps[k] = *h->tmaps;
+    ub[k] = units;
+    units += h->march_units;
+    grid = std::max(grid, h->march_grid);
+  }
+  ub[ninst] = units;
+  CUDA_TRY(cudaMemcpy(e->d_doms, doms.data(), sizeof(DevDomain) * ninst, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(e->d_tmaps, maps.data(), sizeof(TmapSet) * ninst, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(e->d_unit_begin, ub.data(), sizeof(long long) * (ninst + 1), cudaMemcpyHostToDevice));
+  e->plan.units = units;
+  // CTAs per SM as the shape allows (the ring fills shared memory), never more CTAs than units
+  e->plan.march_grid = (int)std::min<long long>(grid, units);
+  e->free_graphs();
+  return FDMAP_OK;
+}
+
+// every instance to march tile `tile`, then the plan (FDMAP_ERR_UNSUPPORTED,
+// with the previous tile restored, if some instance cannot take it)
+int ens_set_tile(fdmap_ensemble* e, int tile) {
+  const int keep = e->proto->march_shape;
+  int rc = FDMAP_OK;
+  for (fdmap_gpu* h : e->inst)
+    if ((rc = march_set_shape(h, tile))) break;
+  if (rc) {
+    const std::string msg = g_err;
+    for (fdmap_gpu* h : e->inst) march_set_shape(h, keep);
+    ens_fill_plan(e);
+    g_err = msg;
+    return rc;
+  }
+  return ens_fill_plan(e);
+}
+
 int ens_check_cur(fdmap_ensemble* e) {
   for (fdmap_gpu* h : e->inst)
     if (h->cur != e->cur) return set_err(FDMAP_ERR_INVALID_ARG, "an instance was stepped outside its ensemble");
@@ -223,32 +271,16 @@ int fdmap_gpu_ensemble_create(const fdmap_desc* const* descs, int ninst, int dev
         CUDA_TRY(cudaStreamCreateWithPriority(&e->side, cudaStreamNonBlocking, lo));
         CUDA_TRY(cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming));
         CUDA_TRY(cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming));
-        // per-instance device descriptors and tensor maps, unit prefix
-        std::vector<DevDomain> doms(ninst);
-        std::vector<TmapSet> maps(ninst);
-        std::vector<long long> ub(ninst + 1, 0);
-        long long units = 0;
-        int grid = 0;
         for (int k = 0; k < ninst; ++k) {
-          fdmap_gpu* h = e->inst[k];
-          doms[k] = h->hdom;
-          maps[k] = *h->tmaps;
-          ub[k] = units;
-          units += h->march_units;
-          grid = std::max(grid, h->march_grid);
-          e->closure_threads.push_back(h->closure_threads);
-          e->edge_threads.push_back(h->edge_threads);
+          e->closure_threads.push_back(e->inst[k]->closure_threads);
+          e->edge_threads.push_back(e->inst[k]->edge_threads);
         }
-        ub[ninst] = units;
         CUDA_TRY(cudaMalloc(&e->d_doms, sizeof(DevDomain) * ninst));
         CUDA_TRY(cudaMalloc(&e->d_tmaps, sizeof(TmapSet) * ninst));
         CUDA_TRY(cudaMalloc(&e->d_unit_begin, sizeof(long long) * (ninst + 1)));
         CUDA_TRY(cudaMalloc(&e->d_closure_begin, sizeof(int) * (ninst + 1)));
         CUDA_TRY(cudaMalloc(&e->d_edge_begin, sizeof(int) * (ninst + 1)));
         CUDA_TRY(cudaMalloc(&e->d_time, sizeof(TimeState)));
-        CUDA_TRY(cudaMemcpy(e->d_doms, doms.data(), sizeof(DevDomain) * ninst, cudaMemcpyHostToDevice));
-        CUDA_TRY(cudaMemcpy(e->d_tmaps, maps.data(), sizeof(TmapSet) * ninst, cudaMemcpyHostToDevice));
-        CUDA_TRY(cudaMemcpy(e->d_unit_begin, ub.data(), sizeof(long long) * (ninst + 1), cudaMemcpyHostToDevice));
         CUDA_TRY(cudaMemset(e->d_time, 0, sizeof(TimeState)));
         e->plan.doms = e->d_doms;
         e->plan.tmaps = e->d_tmaps;
@@ -256,15 +288,12 @@ int fdmap_gpu_ensemble_create(const fdmap_desc* const* descs, int ninst, int dev
         e->plan.closure_cta_begin = e->d_closure_begin;
         e->plan.edge_cta_begin = e->d_edge_begin;
         e->plan.ninst = ninst;
-        e->plan.units = units;
-        // one CTA per SM (the ring fills shared memory), never more CTAs than units
-        e->plan.march_grid = (int)std::min<long long>(grid, units);
         // instances read and write through the ensemble stream
         for (fdmap_gpu* h : e->inst) {
           CUDA_TRY(cudaStreamSynchronize(h->stream));
           h->stream = e->stream;
         }
-        return FDMAP_OK;
+        return ens_fill_plan(e);
       }()))
     return fail(rc);
   if ((rc = apply_shapes(e, 128, 64, 1))) return fail(rc);
@@ -341,68 +370,69 @@ int fdmap_gpu_ensemble_get_shape(fdmap_ensemble* e, int* shape) {
   return FDMAP_OK;
 }
 
-// Autotuner: times `steps` graph-replayed steps (best of two repetitions) for every launch shape
-// (closure block size x interface block size x boundary/interior overlap),
-// keeps the fastest and leaves it applied.  The instances' state is saved
-// before and restored after, so tuning does not advance the ensemble.
+// Autotuner: times `steps` graph-replayed steps (best of two repetitions),
+// first for every march tile shape (strip width x rows per group) the
+// instances can take, then on the fastest tile for every launch shape of the
+// boundary kernels (closure block size x interface block size x
+// boundary/interior overlap); keeps the fastest and leaves it applied.  Every
+// instance's device state is saved before and restored after, so tuning does
+// not advance the ensemble.
 int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_shape, double* best_ms) {
   if (!e) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble");
   if (steps < 1) return set_err(FDMAP_ERR_INVALID_ARG, "steps must be positive");
   CUDA_TRY(cudaSetDevice(e->device));
   int rc = ens_check_cur(e);
   if (rc) return rc;
-  // snapshot of every instance's state (both F buffers, DF, fault state) on the device
-  struct Saved { void* dst; const void* src; size_t bytes; };
-  std::vector<Saved> saved;
-  std::vector<void*> bufs;
-  auto cleanup = [&]() { for (void* b : bufs) cudaFree(b); };
-  auto snap = [&](const void* src, size_t bytes) -> int {
-    void* d = nullptr;
-    if (cudaMalloc(&d, bytes) != cudaSuccess) return set_err(FDMAP_ERR_NOMEM, "no device memory for the tuning snapshot");
-    bufs.push_back(d);
-    saved.push_back({d, src, bytes});
-    CUDA_TRY(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, e->stream));
-    return FDMAP_OK;
+  // snapshot of every instance's whole device state
+  std::vector<std::vector<void*>> saved(e->inst.size());
+  for (size_t k = 0; k < e->inst.size() && rc == FDMAP_OK; ++k) rc = state_snapshot(e->inst[k], saved[k], e->stream);
+  auto cleanup = [&]() {
+    for (auto& v : saved) {
+      for (void* p : v) cudaFree(p);
+      v.clear();
+    }
   };
-  for (fdmap_gpu* h : e->inst) {
-    for (int b = 0; b < h->hdom.nblocks && rc == FDMAP_OK; ++b) {
-      const DevBlock& B = h->hdom.blk[b];
-      const size_t bytes = (size_t)B.plane * h->nF * sizeof(double);
-      for (int q = 0; q < 2 && rc == FDMAP_OK; ++q) rc = snap(B.F[q], bytes);
-      if (rc == FDMAP_OK) rc = snap(B.DF, bytes);
-    }
-    for (int k = 0; k < h->hdom.nifaces && rc == FDMAP_OK; ++k) {
-      const DevIface& I = h->hdom.ifc[k];
-      if (I.fr.st) rc = snap(I.fr.st, (size_t)FDMAP_FAULT_NFIELDS * I.n * sizeof(double));
-    }
-    if (rc) break;
-  }
   if (rc) { cleanup(); return rc; }
   const int cur0 = e->cur;
   const int ctpb[3] = {64, 128, 256}, etpb[3] = {32, 64, 128};
-  int best[3] = {e->plan.closure_tpb, e->plan.edge_tpb, e->overlap};
+  int best[4] = {e->plan.closure_tpb, e->plan.edge_tpb, e->overlap, e->proto->march_shape};
   float best_t = -1.f;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
+  // warm-up step (also builds the graphs), then two timed repetitions; the faster counts
+  auto time_shape = [&](float& ms) -> int {
+    int r = fdmap_gpu_ensemble_run(e, 0.0, dt, 1, 1, 1 << 30);
+    if (r) return r;
+    ms = -1.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaEventRecord(t0, e->stream);
+      if ((r = fdmap_gpu_ensemble_run(e, 0.0, dt, 2, 1 + steps, 1 << 30))) return r;
+      cudaEventRecord(t1, e->stream);
+      if (cudaEventSynchronize(t1) != cudaSuccess) return set_err(FDMAP_ERR_CUDA, "tuning run failed");
+      float m = 0.f;
+      cudaEventElapsedTime(&m, t0, t1);
+      if (ms < 0.f || m < ms) ms = m;
+    }
+    return FDMAP_OK;
+  };
+  // 1. the march tile shape, with the boundary launch shapes as they are
+  for (int tile = 0; tile < MARCH_SHAPES && rc == FDMAP_OK; ++tile) {
+    rc = ens_set_tile(e, tile);
+    if (rc == FDMAP_ERR_UNSUPPORTED) { rc = FDMAP_OK; continue; }
+    float ms = 0.f;
+    if (rc || (rc = time_shape(ms))) break;
+    if (best_t < 0.f || ms < best_t) { best_t = ms; best[3] = tile; }
+  }
+  // 2. closure and interface block sizes and the overlap, on the best tile
+  if (rc == FDMAP_OK) rc = ens_set_tile(e, best[3]);
   for (int ov = 0; ov < 2 && rc == FDMAP_OK; ++ov)
     for (int ci = 0; ci < 3 && rc == FDMAP_OK; ++ci)
       for (int ei = 0; ei < 3 && rc == FDMAP_OK; ++ei) {
         if ((rc = apply_shapes(e, ctpb[ci], etpb[ei], ov))) break;
-        // warm-up step (also builds the graphs), then two timed repetitions; the faster counts
-        if ((rc = fdmap_gpu_ensemble_run(e, 0.0, dt, 1, 1, 1 << 30))) break;
-        float ms = -1.f;
-        for (int rep = 0; rep < 2 && rc == FDMAP_OK; ++rep) {
-          cudaEventRecord(t0, e->stream);
-          if ((rc = fdmap_gpu_ensemble_run(e, 0.0, dt, 2, 1 + steps, 1 << 30))) break;
-          cudaEventRecord(t1, e->stream);
-          if (cudaEventSynchronize(t1) != cudaSuccess) { rc = set_err(FDMAP_ERR_CUDA, "tuning run failed"); break; }
-          float m = 0.f;
-          cudaEventElapsedTime(&m, t0, t1);
-          if (ms < 0.f || m < ms) ms = m;
-        }
-        if (rc) break;
-        if (best_t < 0.f || ms < best_t) {
+        float ms = 0.f;
+        if ((rc = time_shape(ms))) break;
+        if (ms < best_t) {
           best_t = ms;
           best[0] = ctpb[ci]; best[1] = etpb[ei]; best[2] = ov;
         }
@@ -410,17 +440,31 @@ int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_s
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   // restore the state and the buffer parity
-  for (const Saved& s : saved)
-    if (cudaMemcpyAsync(const_cast<void*>(s.src), s.dst, s.bytes, cudaMemcpyDeviceToDevice, e->stream) != cudaSuccess && !rc)
-      rc = set_err(FDMAP_ERR_CUDA, "restoring the tuning snapshot failed");
-  if (cudaStreamSynchronize(e->stream) != cudaSuccess && !rc) rc = set_err(FDMAP_ERR_CUDA, "tuning restore failed");
+  for (size_t k = 0; k < e->inst.size(); ++k) {
+    const int rr = state_restore(e->inst[k], saved[k], e->stream);
+    if (rr && !rc) rc = rr;
+  }
   cleanup();
   e->cur = cur0;
   ens_sync_cur(e);
   if (rc) return rc;
+  if ((rc = ens_set_tile(e, best[3]))) return rc;
   if ((rc = apply_shapes(e, best[0], best[1], best[2]))) return rc;
   if (best_shape) { best_shape[0] = best[0]; best_shape[1] = best[1]; best_shape[2] = best[2]; }
   if (best_ms) *best_ms = best_t / steps;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_set_tile(fdmap_ensemble* e, int tile) {
+  if (!e || tile < 0 || tile >= MARCH_SHAPES) return set_err(FDMAP_ERR_INVALID_ARG, "tile must be 0, 1 or 2");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  return ens_set_tile(e, tile);
+}
+
+int fdmap_gpu_ensemble_get_tile(fdmap_ensemble* e, int* tile) {
+  if (!e || !tile) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
+  *tile = e->proto->march_shape;
   return FDMAP_OK;
 }
 

@@ -148,83 +148,6 @@ void launch_stencil_mode(fdmap_gpu* h, const StageArgs& a) {
   }
 }
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-// 3-D FP64 tensor map over `nplanes` consecutive planes of a block array,
-// nx columns wide (the pitch padding reads as zeros without touching memory).
-// No L2 promotion: boxes with halo columns start 16 bytes before a 256-byte
-// line, and promotion would pull a whole line at each end of every row for
-// those 16 bytes; fetched by sector, the halos cost what they hold.
-int encode_map(EncodeTiledFn enc, CUtensorMap* map, double* base, const BlockGeom& g, int nplanes, int box_x, int box_z) {
-  cuuint64_t dims[3] = {(cuuint64_t)g.nx, (cuuint64_t)g.ny, (cuuint64_t)nplanes};
-  cuuint64_t strides[2] = {(cuuint64_t)g.pitch * 8, (cuuint64_t)g.plane * 8};
-  cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)MR, (cuuint32_t)box_z};
-  cuuint32_t estr[3] = {1, 1, 1};
-  const CUtensorMapL2promotion promo = CU_TENSOR_MAP_L2_PROMOTION_NONE;
-  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_NONE, promo, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) return set_err(FDMAP_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
-  return FDMAP_OK;
-}
-
-template <int MODE, int PI_, bool HET>
-int march_maps(fdmap_gpu* h) {
-  using L = MarchLayout<MODE, PI_, HET>;
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult qr;
-  CUDA_TRY(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr));
-  if (!fn || qr != cudaDriverEntryPointSuccess) return set_err(FDMAP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-  EncodeTiledFn enc = (EncodeTiledFn)fn;
-  if (!h->tmaps) h->tmaps = new (std::nothrow) TmapSet();
-  if (!h->tmaps) return set_err(FDMAP_ERR_NOMEM, "out of host memory");
-  std::memset(h->tmaps, 0, sizeof(TmapSet));
-  int rc;
-  for (int b = 0; b < h->hdom.nblocks; ++b) {
-    if (!h->owns(b)) continue;  // body on a peer GPU
-    const BlockGeom& g = h->geom[b];
-    DevBlock& B = h->hdom.blk[b];
-    for (int q = 0; q < 2; ++q) {
-      if ((rc = encode_map(enc, &h->tmaps->F[b][q], B.F[q], g, h->nF, L::WH, L::NR))) return rc;
-      if ((rc = encode_map(enc, &h->tmaps->F6[b][q], B.F[q], g, h->nF, MW, 1))) return rc;
-    }
-    if ((rc = encode_map(enc, &h->tmaps->DF[b], B.DF, g, h->nF, MW, L::NR))) return rc;
-    if ((rc = encode_map(enc, &h->tmaps->MH[b], h->met_base[b], g, 5, L::WH, 2))) return rc;
-    if ((rc = encode_map(enc, &h->tmaps->MC[b], h->met_base[b], g, 5, MW, 3))) return rc;
-    if (HET && (rc = encode_map(enc, &h->tmaps->HT[b], h->het_base[b], g, 5, MW, L::NH))) return rc;
-  }
-  return FDMAP_OK;
-}
-
-template <int MODE, int PI_, bool HET>
-int march_setup(fdmap_gpu* h) {
-  size_t smem = MarchLayout<MODE, PI_, HET>::BYTES;
-  int optin = 0;
-  CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device));
-  if (smem > (size_t)optin) {  // the ring does not fit: this variant uses the tiled kernel
-    h->use_march = 0;
-    return FDMAP_OK;
-  }
-  int rc0 = march_maps<MODE, PI_, HET>(h);
-  if (rc0) return rc0;
-  auto k = march_kernel<MODE, PI_, HET>;
-  CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0, sms = 0;
-  CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, MTHREADS, smem));
-  CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device));
-  if (per_sm < 1) return set_err(FDMAP_ERR_CUDA, "march kernel does not fit on an SM");
-  long long g = (long long)sms * per_sm;
-  h->march_grid = (int)std::min<long long>(g, h->march_units);
-  return FDMAP_OK;
-}
-
-template <int MODE, int PI_, bool HET>
-void march_launch(fdmap_gpu* h, const StageArgs& a) {
-  MarchPlan plan{h->march_grid, h->march_units, nullptr, nullptr, 1};
-  march_kernel<MODE, PI_, HET><<<h->march_grid, MTHREADS, MarchLayout<MODE, PI_, HET>::BYTES, h->stream>>>(h->ddom, a, plan, *h->tmaps);
-}
-
 template <int MODE, bool HET, typename Fn>
 int dispatch_pi(int pI, Fn&& fn) {
   if (pI == 1) return fn(std::integral_constant<int, 1>{});
@@ -232,18 +155,21 @@ int dispatch_pi(int pI, Fn&& fn) {
   return fn(std::integral_constant<int, 3>{});
 }
 
-int march_dispatch(fdmap_gpu* h, const StageArgs* a) {
-  auto go = [&](auto mode_c, auto het_c) {
-    constexpr int MODE = decltype(mode_c)::value;
-    constexpr bool HET = decltype(het_c)::value;
-    return dispatch_pi<MODE, HET>(h->pI, [&](auto pi_c) {
-      constexpr int PI_ = decltype(pi_c)::value;
-      if (a) { march_launch<MODE, PI_, HET>(h, *a); return (int)FDMAP_OK; }
-      return march_setup<MODE, PI_, HET>(h);
-    });
-  };
-  if (h->mode == 2) return h->het ? go(std::integral_constant<int, 2>{}, std::true_type{}) : go(std::integral_constant<int, 2>{}, std::false_type{});
-  return h->het ? go(std::integral_constant<int, 3>{}, std::true_type{}) : go(std::integral_constant<int, 3>{}, std::false_type{});
+int march_dispatch(fdmap_gpu* h, const StageArgs& a) {
+  switch (h->march_shape) {
+    case 0: return march_launch_s0(h, a);
+    case 1: return march_launch_s1(h, a);
+    default: return march_launch_s2(h, a);
+  }
+}
+
+int march_configure(fdmap_gpu* h, int shape) {
+  switch (shape) {
+    case 0: return march_configure_s0(h);
+    case 1: return march_configure_s1(h);
+    case 2: return march_configure_s2(h);
+  }
+  return set_err(FDMAP_ERR_INVALID_ARG, "march tile shape must be 0, 1 or 2");
 }
 
 int launch_stage(fdmap_gpu* h, const StageArgs& a);
@@ -266,16 +192,56 @@ namespace fdmap {
 int engine_stage(fdmap_gpu* h, const StageArgs& a) { return launch_stage(h, a); }
 
 int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s) {
-  return dispatch_variant(proto, [&](auto mode_c, auto pi_c, auto het_c) {
-    constexpr int MODE = decltype(mode_c)::value;
-    constexpr int PI_ = decltype(pi_c)::value;
-    constexpr bool HET = decltype(het_c)::value;
-    MarchPlan plan{p.march_grid, p.units, p.tmaps, p.unit_begin, p.ninst};
-    march_kernel<MODE, PI_, HET><<<p.march_grid, MTHREADS, MarchLayout<MODE, PI_, HET>::BYTES, s>>>(p.doms, a, plan,
-                                                                                                    *proto->tmaps);
-    CUDA_TRY(cudaGetLastError());
-    return (int)FDMAP_OK;
-  });
+  switch (proto->march_shape) {
+    case 0: return march_batch_s0(proto, a, p, s);
+    case 1: return march_batch_s1(proto, a, p, s);
+    default: return march_batch_s2(proto, a, p, s);
+  }
+}
+
+int state_snapshot(fdmap_gpu* h, std::vector<void*>& out, cudaStream_t s) {
+  out.clear();
+  for (size_t q = 0; q < h->allocs.size(); ++q) {
+    void* d = nullptr;
+    if (cudaMalloc(&d, h->alloc_sizes[q]) != cudaSuccess) {
+      for (void* p : out) cudaFree(p);
+      out.clear();
+      return set_err(FDMAP_ERR_NOMEM, "no device memory for the tuning snapshot");
+    }
+    out.push_back(d);
+    CUDA_TRY(cudaMemcpyAsync(d, h->allocs[q], h->alloc_sizes[q], cudaMemcpyDeviceToDevice, s));
+  }
+  return FDMAP_OK;
+}
+
+int state_restore(fdmap_gpu* h, std::vector<void*>& saved, cudaStream_t s) {
+  int rc = FDMAP_OK;
+  for (size_t q = 0; q < saved.size() && q < h->allocs.size(); ++q)
+    if (cudaMemcpyAsync(h->allocs[q], saved[q], h->alloc_sizes[q], cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+      rc = set_err(FDMAP_ERR_CUDA, "restoring the tuning snapshot failed");
+  if (cudaStreamSynchronize(s) != cudaSuccess && !rc) rc = set_err(FDMAP_ERR_CUDA, "restoring the tuning snapshot failed");
+  for (void* p : saved) cudaFree(p);
+  saved.clear();
+  return rc;
+}
+
+int march_set_shape(fdmap_gpu* h, int shape) {
+  if (!h->use_march) return set_err(FDMAP_ERR_UNSUPPORTED, "the domain does not use the march kernel");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const int keep = h->march_shape;
+  int rc = march_configure(h, shape);
+  if (rc) {
+    std::string msg = g_err;
+    march_configure(h, keep);  // back to the shape in use
+    g_err = msg;
+    return rc;
+  }
+  CUDA_TRY(cudaMemcpy(h->ddom, &h->hdom, sizeof(DevDomain), cudaMemcpyHostToDevice));
+  for (auto& ge : h->step_graph)
+    if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  h->graph_dt = 0.0;
+  return FDMAP_OK;
 }
 
 int batch_closure(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s) {
@@ -339,7 +305,7 @@ void launch_boundary_mode(fdmap_gpu* h, const StageArgs& a) {
 int launch_interior(fdmap_gpu* h, const StageArgs& a) {
   ProfScope ps(h, 0);
   if (h->use_march) {
-    int rc = march_dispatch(h, &a);
+    int rc = march_dispatch(h, a);
     if (rc) return rc;
   } else if (h->mode == 2) launch_stencil_mode<2>(h, a);
   else launch_stencil_mode<3>(h, a);
@@ -742,8 +708,6 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     int tiles_y = own ? (g.ny + TY - 1) / TY : 0;
     B.tile_begin = tiles;
     tiles += B.tiles_x * tiles_y;
-    B.march_unit_begin = h->march_units;
-    if (own) h->march_units += (long long)((g.nx + MW - 1) / MW) * ((g.ny + MR - 1) / MR);
   }
   h->total_tiles = tiles;
   h->body_on_device = d->body != nullptr;
@@ -871,9 +835,17 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   int rc;
   {
     const char* ek = getenv("FDMAP_STENCIL");
-    // dissipative blocks need J at the neighbours, which the march ring does not carry
-    h->use_march = !(ek && std::string(ek) == "tile") && !h->dissipation && !h->pml && !h->forcing && !h->extras;
-    if (h->use_march && (rc = march_dispatch(h, nullptr))) return rc;
+    // the march serves every variant: dissipation (J halo rows in the ring),
+    // PML, forcing and body extras through its extras variant; the first
+    // tile shape whose rings fit is taken (the autotuner may change it)
+    h->march_ext = h->dissipation || h->pml || h->forcing || h->extras;
+    h->use_march = !(ek && std::string(ek) == "tile");
+    if (h->use_march) {
+      rc = FDMAP_ERR_UNSUPPORTED;
+      for (int sh = 0; sh < MARCH_SHAPES && rc == FDMAP_ERR_UNSUPPORTED; ++sh) rc = march_configure(h, sh);
+      if (rc == FDMAP_ERR_UNSUPPORTED) h->use_march = 0;  // no shape fits: the tiled interior kernel
+      else if (rc) return rc;
+    }
     // fused stage launches need every interface-side node to sit on one interface only
     bool junction = false;
     for (int b = 0; b < d->nblocks; ++b) {
@@ -1570,6 +1542,68 @@ int fdmap_gpu_clear_status(fdmap_gpu* h) {
   CUDA_TRY(cudaSetDevice(h->device));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   CUDA_TRY(cudaMemset(h->d_status, 0, 4 * sizeof(unsigned long long)));
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_tile(fdmap_gpu* h, int tile) {
+  if (!h || tile < 0 || tile >= MARCH_SHAPES) return set_err(FDMAP_ERR_INVALID_ARG, "tile must be 0, 1 or 2");
+  return march_set_shape(h, tile);
+}
+
+int fdmap_gpu_get_tile(fdmap_gpu* h, int* tile, int* mw, int* mr) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  if (!h->use_march) return set_err(FDMAP_ERR_UNSUPPORTED, "the domain uses the tiled interior kernel");
+  if (tile) *tile = h->march_shape;
+  if (mw) *mw = shape_mw(h->march_shape);
+  if (mr) *mr = shape_mr(h->march_shape);
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_tune(fdmap_gpu* h, double dt, int steps, int* best_tile, double* best_ms) {
+  if (!h || steps < 1) return set_err(FDMAP_ERR_INVALID_ARG, "bad tune arguments");
+  if (!h->use_march) return set_err(FDMAP_ERR_UNSUPPORTED, "the domain uses the tiled interior kernel");
+  if (h->partitioned()) return set_err(FDMAP_ERR_UNSUPPORTED, "a partition is not tuned on its own");
+  if (output_is_open(h)) return set_err(FDMAP_ERR_INVALID_ARG, "tune before opening the outputs");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  std::vector<void*> saved;
+  int rc = state_snapshot(h, saved, h->stream);
+  if (rc) return rc;
+  const int cur0 = h->cur, shape0 = h->march_shape;
+  const long long out0 = h->out_next_n;
+  int best = shape0;
+  float best_t = -1.f;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  for (int sh = 0; sh < MARCH_SHAPES && rc == FDMAP_OK; ++sh) {
+    rc = march_set_shape(h, sh);
+    if (rc == FDMAP_ERR_UNSUPPORTED) { rc = FDMAP_OK; continue; }
+    if (rc) break;
+    // warm-up step (captures the graphs), then two timed repetitions; the faster counts
+    if ((rc = fdmap_gpu_run(h, 0.0, dt, 1, 1, 1 << 30))) break;
+    float ms = -1.f;
+    for (int rep = 0; rep < 2 && rc == FDMAP_OK; ++rep) {
+      cudaEventRecord(t0, h->stream);
+      if ((rc = fdmap_gpu_run(h, 0.0, dt, 2, 1 + steps, 1 << 30))) break;
+      cudaEventRecord(t1, h->stream);
+      if (cudaEventSynchronize(t1) != cudaSuccess) { rc = set_err(FDMAP_ERR_CUDA, "tuning run failed"); break; }
+      float m = 0.f;
+      cudaEventElapsedTime(&m, t0, t1);
+      if (ms < 0.f || m < ms) ms = m;
+    }
+    if (rc == FDMAP_OK && (best_t < 0.f || ms < best_t)) { best_t = ms; best = sh; }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  const int rr = state_restore(h, saved, h->stream);
+  h->cur = cur0;
+  h->out_next_n = out0;
+  if (rc) { march_set_shape(h, shape0); return rc; }
+  if (rr) return rr;
+  if ((rc = march_set_shape(h, best))) return rc;
+  if (best_tile) *best_tile = best;
+  if (best_ms) *best_ms = best_t / steps;
   return FDMAP_OK;
 }
 

@@ -30,26 +30,38 @@
 
 namespace fdmap {
 
-constexpr int MW = 128;         // strip width (columns)
-constexpr int MR = 4;           // rows per row group
-constexpr int MTHREADS = MW * MR;
+// Tile shapes of the march: strip width MW (columns) x rows per row group MR.
+// The host picks one per domain (the first whose rings fit in shared memory,
+// or the autotuner's choice); the unit decomposition and the tensor-map boxes
+// follow it.
+constexpr int MARCH_SHAPES = 3;
+__host__ __device__ constexpr int shape_mw(int sh) { return sh == 2 ? 64 : 128; }
+__host__ __device__ constexpr int shape_mr(int sh) { return sh == 1 ? 2 : 4; }
 constexpr int NGS = 4;          // neighbour ring: row groups g-1, g, g+1 resident, g+2 in flight
 constexpr int NCS = 2;          // centre ring: group g resident, g+1 in flight
 
 __host__ __device__ constexpr int even_halo(int h) { return (h + 1) & ~1; }
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
-template <int MODE, int PI_, bool HET>
+// EXT: the variant for blocks with artificial dissipation (a J plane with
+// halo columns in every neighbour slot), a perfectly matched layer, source
+// forcing, body displacement or peak motion (node-local data read and
+// written by the node's own thread).
+template <int MODE, int PI_, bool HET, bool EXT, int SH>
 struct MarchLayout {
+  static constexpr int MW = shape_mw(SH);
+  static constexpr int MR = shape_mr(SH);
+  static constexpr int THREADS = MW * MR;
   static constexpr int NR = RDef<MODE>::NR;
   static constexpr int HP = even_halo(PI_);
   static constexpr int WH = MW + 2 * HP;                       // halo row length (doubles)
   static constexpr int NH = HET ? (MODE == 2 ? 5 : 2) : 0;     // heterogeneous material planes
-  // neighbour group slot: rate fields [NR][MR][WH], yr,xr [2][MR][WH], yq,xq,Ji [3][MR][MW]
+  // neighbour group slot: rate fields [NR][MR][WH], yr,xr [2][MR][WH], yq,xq,Ji [3][MR][MW], (EXT) J [MR][WH]
   static constexpr size_t F_OFF = 0;
   static constexpr size_t MH_OFF = align128(F_OFF + (size_t)NR * MR * WH * 8);
   static constexpr size_t MC_OFF = align128(MH_OFF + (size_t)2 * MR * WH * 8);
-  static constexpr size_t GSLOT = align128(MC_OFF + (size_t)3 * MR * MW * 8);
+  static constexpr size_t J_OFF = align128(MC_OFF + (size_t)3 * MR * MW * 8);
+  static constexpr size_t GSLOT = align128(J_OFF + (EXT ? (size_t)MR * WH * 8 : 0));
   // centre group slot: DF [NR][MR][MW], szz [1][MR][MW] (mode II), material [NH][MR][MW]
   static constexpr size_t DF_OFF = 0;
   static constexpr size_t F6_OFF = align128(DF_OFF + (size_t)NR * MR * MW * 8);
@@ -58,6 +70,7 @@ struct MarchLayout {
   static constexpr size_t BARS_OFF = NGS * GSLOT + NCS * CSLOT;
   static constexpr size_t BYTES = BARS_OFF + (NGS + NCS) * 8 + 128;  // + alignment slack
   static constexpr unsigned NB_BYTES = (unsigned)(((size_t)(NR + 2) * WH + 3 * MW) * MR * 8);
+  static constexpr unsigned J_BYTES = (unsigned)((size_t)MR * WH * 8);
 };
 
 struct MarchPlan {
@@ -178,36 +191,41 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 }
 
 
-// Row-group unit u -> (block, strip, first row)
+// Row-group unit u -> (block, strip, first row) for tiles of MW x MR
 struct UnitPos {
   int b, sx, j0;
 };
 
+template <int MR_>
 __device__ __forceinline__ UnitPos unit_pos(const DevDomain& D, long long u) {
   UnitPos p{0, 0, 0};
   int b = 0;
   while (b + 1 < D.nblocks && u >= D.blk[b + 1].march_unit_begin) ++b;
   const DevBlock& B = D.blk[b];
   long long local = u - B.march_unit_begin;
-  int groups = (B.ny + MR - 1) / MR;
+  int groups = (B.ny + MR_ - 1) / MR_;
   p.b = b;
   p.sx = (int)(local / groups);
-  p.j0 = (int)(local % groups) * MR;
+  p.j0 = (int)(local % groups) * MR_;
   return p;
 }
 
 // Register budget of the march kernel: 96 per thread (48K of the SM's 64K for
-// the 512-thread CTA) leaves room for one boundary CTA beside it, so the
+// a 512-thread CTA) leaves room for one boundary CTA beside it, so the
 // edge and closure kernels of the same stage run concurrently with the
-// interior march.  The SBP6 mode II variant needs more to avoid spills.
-template <int MODE, int PI_>
-constexpr int march_regs() { return (MODE == 2 && PI_ == 3) ? 128 : 96; }
+// interior march.  The SBP6 mode II variant and the extras variant of a
+// 256-thread shape take more to avoid spills.
+template <int MODE, int PI_, bool EXT, int SH>
+constexpr int march_regs() {
+  return ((MODE == 2 && PI_ == 3) || (EXT && shape_mw(SH) * shape_mr(SH) <= 256)) ? 128 : 96;
+}
 
-template <int MODE, int PI_, bool HET>
-__global__ void __maxnreg__((march_regs<MODE, PI_>()))
+template <int MODE, int PI_, bool HET, bool EXT, int SH>
+__global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
     march_kernel(const DevDomain* __restrict__ doms, StageArgs a, MarchPlan plan, const __grid_constant__ TmapSet tm) {
-  using L = MarchLayout<MODE, PI_, HET>;
+  using L = MarchLayout<MODE, PI_, HET, EXT, SH>;
   using RD = RDef<MODE>;
+  constexpr int MW = L::MW, MR = L::MR;
   constexpr int NR = RD::NR;
   constexpr int NF = MODE == 2 ? 6 : 3;
   constexpr int HP = L::HP;
@@ -244,7 +262,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
     const DevDomain& D = doms[inst];
     const TmapSet& tmi = plan.tms ? plan.tms[inst] : tm;
     // segment: consecutive row groups of one strip
-    const UnitPos p0 = unit_pos(D, u - base);
+    const UnitPos p0 = unit_pos<MR>(D, u - base);
     const int b = p0.b;
     const DevBlock& B = D.blk[b];
     const int groups = (B.ny + MR - 1) / MR;
@@ -261,6 +279,9 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
     const int gmax = ngroups - 1 + (jr1 < ny ? 1 : 0);
     const CUtensorMap* mF = &tmi.F[b][a.in];
     const CUtensorMap* mF6 = &tmi.F6[b][a.in];
+    // artificial dissipation of this block: J with halo columns in the neighbour ring
+    const bool diss = EXT && B.Cdiss > 0.0;
+    const unsigned nbytes = L::NB_BYTES + (diss ? L::J_BYTES : 0u);
 
     if (tid == 0) {
       for (int s = 0; s < NGS + NCS; ++s) mbar_init(&nbar[s], 1);
@@ -274,10 +295,11 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
       const int sl = (k - gmin) % NGS;
       unsigned char* g = smem + (size_t)sl * L::GSLOT;
       const int row = jr0 + k * MR;
-      mbar_arrive_tx(&nbar[sl], L::NB_BYTES);
+      mbar_arrive_tx(&nbar[sl], nbytes);
       tma_load_3d(g + L::F_OFF, mF, i0 - HP, row, 0, &nbar[sl]);
       tma_load_3d(g + L::MH_OFF, &tmi.MH[b], i0 - HP, row, 0, &nbar[sl]);
       tma_load_3d(g + L::MC_OFF, &tmi.MC[b], i0, row, 2, &nbar[sl]);
+      if (diss) tma_load_3d(g + L::J_OFF, &tmi.JH[b], i0 - HP, row, 0, &nbar[sl]);
     };
     auto fill_c = [&](int k) {  // centre group k -> slot k % NCS
       c_next = k + 1;
@@ -306,8 +328,10 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
     double* __restrict__ Fout = B.F[a.out];
 
     const int nbst = D.nbst;
-    // body forces of this block (point source / gravity), evaluated once per segment
-    const bool forces = D.src.use_gravity || (D.src.use_singular && B.src_ok);
+    // body forces of this block (point source / gravity; with EXT also the
+    // long-wave forcing and forcing from file), evaluated once per segment
+    const bool forces = D.src.use_gravity || (D.src.use_singular && B.src_ok) ||
+                        (EXT && (D.src.use_singular || B.gforce || B.frc_new));
     const double t_stage = forces ? stage_time(a) : 0.0;
     const int i = i0 + cx;
     int aborted_at = -1;
@@ -330,7 +354,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
         // row j lives in group g, row ry; rows j +- s in group g + (ry +- s) div MR
         auto nrow = [&](int dr, size_t off, int q, int width) -> const double* {
           int rr = ry + dr;
-          int k = g + (rr >= 0 ? rr / MR : -1);
+          int k = g + (rr >= 0 ? rr / MR : -((MR - 1 - rr) / MR));
           int r = rr - (k - g) * MR;
           return reinterpret_cast<const double*>(smem + (size_t)((k - gmin) % NGS) * L::GSLOT + off) + ((size_t)q * MR + r) * width;
         };
@@ -360,7 +384,20 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
           m.rho = rho_b; m.G = G_b; m.M = M_b; m.gamma = gamma_b; m.nu = nu_b;
         }
         m.rinv = HET ? 1.0 / m.rho : 0.0;
-        {
+        bool pml = false;
+        if constexpr (EXT && MODE == 2) {
+          if (B.pml) {
+            // Cartesian PML rates of the interior region (rates.f90:2089-2126)
+            // from the ring; szz at the neighbours through the cache
+            const double* Fin = B.F[a.in];
+            march_pml_interior<PI_>(D, B, c, a, acc, [&](int l, int dq, int dr) -> double {
+              if (l == 5) return Fin[5 * plane + c + dq + (long long)dr * pitch];
+              return dr == 0 ? nrow(0, L::F_OFF, l, WH)[cx + HP + dq] : nrow(dr, L::F_OFF, l, WH)[cx + HP];
+            });
+            pml = true;
+          }
+        }
+        if (!pml) {
           const double* hy = nrow(0, L::MH_OFF, 0, WH) + cx + HP;  // yr, centred on the node
           const double* hx = nrow(0, L::MH_OFF, 1, WH) + cx + HP;  // xr
           const double yrc = hy[0], xrc = hx[0];
@@ -395,9 +432,29 @@ __global__ void __maxnreg__((march_regs<MODE, PI_>()))
               acc[r] += sum * cfr * Ji;
             }
           }
+          if (EXT && diss) {
+            // artificial dissipation (rates_dissipation_interior_mode2/3,
+            // rates.f90:939-999, 1397-1482): 2*AI(0)*F + sum_s AI(s)*Ji*(J F at
+            // the four neighbours at distance s), in the tiled kernel's order
+            const double Cd = B.Cdiss;
+            const double* jr = nrow(0, L::J_OFF, 0, WH) + cx + HP;
+#pragma unroll
+            for (int l = 0; l < NR; ++l) {
+              const double* fr = nrow(0, L::F_OFF, l, WH) + cx + HP;
+              double sum = 2.0 * D.AI[0] * Cd * fr[0];
+#pragma unroll
+              for (int s = 1; s <= PI_; ++s)
+                sum += D.AI[s] * Cd * Ji *
+                       (jr[s] * fr[s] + jr[-s] * fr[-s] +
+                        nrow(s, L::J_OFF, 0, WH)[cx + HP] * nrow(s, L::F_OFF, l, WH)[cx + HP] +
+                        nrow(-s, L::J_OFF, 0, WH)[cx + HP] * nrow(-s, L::F_OFF, l, WH)[cx + HP]);
+              acc[l] += sum;
+            }
+          }
         }
         if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
         if (forces) body_forces<MODE>(D, B, i, j, t_stage, a, acc);
+        if (EXT) body_extras<MODE>(B, c, Fc, acc, a);
 #pragma unroll
         for (int l = 0; l < NF; ++l) DFp[l * plane + c] = acc[l];
         if (a.update) {

@@ -526,6 +526,91 @@ __device__ __forceinline__ void pml_rates(const DevDomain& D, const DevBlock& B,
   }
 }
 
+// The interior branch of pml_rates (rates.f90:2089-2126) for a node whose
+// neighbour values come from elsewhere (the march kernel's shared-memory
+// ring): F(l, dq, dr) is field l at (i + dq, j + dr).  Same arithmetic, in the
+// same order, as pml_rates for an interior node.
+template <int PI_, typename FieldAt>
+__device__ __forceinline__ void march_pml_interior(const DevDomain& D, const DevBlock& B, long long c,
+                                                   const StageArgs& a, double* acc, FieldAt F) {
+  constexpr int NF = 6;
+  const long long plane = B.plane;
+  const double hxi = B.pml_h[(2 * 3 + 2) * 2], hyi = B.pml_h[(2 * 3 + 2) * 2 + 1];
+  const double sx = B.pml_s[c], sy = B.pml_s[plane + c];
+  const double rho = B.rho_b, G = B.G_b, M = B.M_b, gamma = B.gamma_b;
+  const bool onx = B.pml & 1, ony = (B.pml >> 1) & 1;
+  const bool load = a.scale && a.A != 0.0;
+  double dwx[NF], dwy[NF];
+  if (onx) {
+    double w[NF];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      w[l] = B.Wx[l * plane + c];
+      dwx[l] = load ? a.A * B.DWx[l * plane + c] : 0.0;
+    }
+    acc[0] = acc[0] - w[2] / rho;
+    acc[1] = acc[1] - w[3] / rho;
+    acc[2] = acc[2] - w[0] * M;
+    acc[3] = acc[3] - w[1] * G;
+    acc[4] = acc[4] - w[0] * gamma * M;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] - (sx + B.pml_kappa) * w[l];
+  }
+  if (ony) {
+    double w[NF];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      w[l] = B.Wy[l * plane + c];
+      dwy[l] = load ? a.A * B.DWy[l * plane + c] : 0.0;
+    }
+    acc[0] = acc[0] - w[3] / rho;
+    acc[1] = acc[1] - w[4] / rho;
+    acc[2] = acc[2] - w[1] * gamma * M;
+    acc[3] = acc[3] - w[0] * G;
+    acc[4] = acc[4] - w[1] * M;
+#pragma unroll
+    for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] - (sy + B.pml_kappa) * w[l];
+  }
+#pragma unroll
+  for (int s = 1; s <= PI_; ++s) {
+    double dq[NF], dr[NF];
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      dq[l] = F(l, s, 0) - F(l, -s, 0);
+      dr[l] = F(l, 0, s) - F(l, 0, -s);
+    }
+    const double DIs = D.DI[s];
+    if (onx) {
+#pragma unroll
+      for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] + sx * hxi * dq[l] * DIs;
+    }
+    if (ony) {
+#pragma unroll
+      for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] + sy * hyi * dr[l] * DIs;
+    }
+    const double as = DIs / rho, bs = DIs * G, cs = DIs * M;
+    acc[0] = acc[0] + (hxi * dq[2] + hyi * dr[3]) * as;
+    acc[1] = acc[1] + (hxi * dq[3] + hyi * dr[4]) * as;
+    acc[2] = acc[2] + (hxi * dq[0] + hyi * dr[1] * gamma) * cs;
+    acc[3] = acc[3] + (hxi * dq[1] + hyi * dr[0]) * bs;
+    acc[4] = acc[4] + (hxi * dq[0] * gamma + hyi * dr[1]) * cs;
+  }
+  if (onx) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      B.DWx[l * plane + c] = dwx[l];
+      if (a.update) B.Wx[l * plane + c] = B.Wx[l * plane + c] + a.Bdt * dwx[l];
+    }
+  }
+  if (ony) {
+#pragma unroll
+    for (int l = 0; l < NF; ++l) {
+      B.DWy[l * plane + c] = dwy[l];
+      if (a.update) B.Wy[l * plane + c] = B.Wy[l * plane + c] + a.Bdt * dwy[l];
+    }
+  }
+}
+
 // Whole stage for one node of the SBP closure strips: scale, SAT (sides in the
 // reference's order L, R, B, T), one-sided closure rates (rates_boundary_mode2/3),
 // szz, sources, update.  Side `iside` takes the caller's hat variables.

@@ -337,6 +337,22 @@ class GpuDomain:
     def clear_status(self) -> None:
         check_gpu(lib().fdmap_gpu_clear_status(self._g), "fdmap_gpu_clear_status")
 
+    def tile(self) -> tuple[int, int, int]:
+        """(tile shape, strip width, rows per row group) of the interior march."""
+        t, w, r = C.c_int(), C.c_int(), C.c_int()
+        check_gpu(lib().fdmap_gpu_get_tile(self._g, C.byref(t), C.byref(w), C.byref(r)), "fdmap_gpu_get_tile")
+        return t.value, w.value, r.value
+
+    def set_tile(self, tile: int) -> None:
+        check_gpu(lib().fdmap_gpu_set_tile(self._g, int(tile)), "fdmap_gpu_set_tile")
+
+    def tune(self, steps: int = 5, dt: float | None = None) -> tuple[int, float]:
+        """Autotune the march tile shape; returns (tile, ms per step).  The state is left as it was."""
+        t, ms = C.c_int(), C.c_double()
+        check_gpu(lib().fdmap_gpu_tune(self._g, self.host.dt if dt is None else dt, steps, C.byref(t), C.byref(ms)),
+                  "fdmap_gpu_tune")
+        return t.value, ms.value
+
     def set_newton_limit(self, imax: int) -> None:
         """Lower the Newton iteration limit (imax = 99 in the reference) to provoke failures."""
         check_gpu(lib().fdmap_gpu_set_newton_limit(self._g, int(imax)), "fdmap_gpu_set_newton_limit")
@@ -436,6 +452,16 @@ class GpuEnsemble:
         check_gpu(lib().fdmap_gpu_ensemble_tune(self._e, self.dt if dt is None else dt, steps, s,
                                                 C.byref(ms)), "fdmap_gpu_ensemble_tune")
         return tuple(s), ms.value
+
+    @property
+    def tile(self) -> int:
+        t = C.c_int()
+        check_gpu(lib().fdmap_gpu_ensemble_get_tile(self._e, C.byref(t)), "fdmap_gpu_ensemble_get_tile")
+        return t.value
+
+    @tile.setter
+    def tile(self, v: int) -> None:
+        check_gpu(lib().fdmap_gpu_ensemble_set_tile(self._e, int(v)), "fdmap_gpu_ensemble_set_tile")
 
     def launch_count(self) -> int:
         return lib().fdmap_gpu_ensemble_launch_count(self._e)

@@ -75,6 +75,9 @@ SIGNATURES = {
     "fdmap_gpu_newton_counts": (C.c_int, [_VP, C.POINTER(C.c_longlong)]),
     "fdmap_gpu_clear_status": (C.c_int, [_VP]),
     "fdmap_gpu_set_newton_limit": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_set_tile": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_get_tile": (C.c_int, [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "fdmap_gpu_tune": (C.c_int, [_VP, C.c_double, C.c_int, C.POINTER(C.c_int), _DP]),
     "fdmap_gpu_test_wait_timeout": (C.c_int, [_VP, C.c_double]),
     "fdmap_gpu_time_params": (C.c_int, [_VP, _DP, C.POINTER(C.c_int)]),
     "fdmap_gpu_get_metric": (C.c_int, [_VP, C.c_int, _DP]),
@@ -118,6 +121,8 @@ SIGNATURES = {
     "fdmap_gpu_ensemble_set_shape": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "fdmap_gpu_ensemble_get_shape": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "fdmap_gpu_ensemble_tune": (C.c_int, [_VP, C.c_double, C.c_int, C.POINTER(C.c_int), _DP]),
+    "fdmap_gpu_ensemble_set_tile": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_ensemble_get_tile": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "fdmap_gpu_ensemble_launch_count": (C.c_longlong, [_VP]),
     "fdmap_gpu_ensemble_destroy": (None, [_VP]),
     # fdmap_gpu.h: forward/backward pair

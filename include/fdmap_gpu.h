@@ -133,6 +133,23 @@ int fdmap_gpu_newton_counts(fdmap_gpu* h, long long* counts);
 /* Resets the status words (failure counts, timeout flag) to zero. */
 int fdmap_gpu_clear_status(fdmap_gpu* h);
 
+/* Tile shape of the interior march kernel: 0 = 128 columns x 4 rows per row
+ * group, 1 = 128 x 2, 2 = 64 x 4.  The engine starts with the first shape
+ * whose shared-memory rings fit the domain's variant (a heterogeneous mode II
+ * medium or the extras of dissipation, PML, forcing and body displacement
+ * need the smaller rings).  set_tile returns FDMAP_ERR_UNSUPPORTED for a
+ * shape that cannot serve the domain; get_tile fills any non-NULL pointer
+ * with the shape and its width / rows. */
+int fdmap_gpu_set_tile(fdmap_gpu* h, int tile);
+int fdmap_gpu_get_tile(fdmap_gpu* h, int* tile, int* mw, int* mr);
+
+/* Autotuner of a single domain: times `steps` steps (CUDA graphs, best of two
+ * repetitions) with every tile shape the domain can take, keeps the fastest
+ * and returns it (best_tile, best_ms per step; either may be NULL).  The whole
+ * device state is copied before and put back after, so tuning does not
+ * advance the run.  Call it before opening outputs. */
+int fdmap_gpu_tune(fdmap_gpu* h, double dt, int steps, int* best_tile, double* best_ms);
+
 /* Iteration limit of every Newton solve, 1..99 (the reference's parameter
  * imax = 99, friction.f90:924, is the default).  A driver or test lowers it
  * to provoke solver failures on purpose (fault injection from the host). */
@@ -291,10 +308,17 @@ int fdmap_gpu_ensemble_synchronize(fdmap_ensemble* e);
 int fdmap_gpu_ensemble_set_shape(fdmap_ensemble* e, const int* shape);
 int fdmap_gpu_ensemble_get_shape(fdmap_ensemble* e, int* shape);
 
-/* Autotuner: times `steps` replayed steps of every launch shape, applies the
- * fastest and returns it (best_shape[3], best_ms per step; either may be
- * NULL).  The ensemble's state is restored afterwards. */
+/* Autotuner: times `steps` replayed steps of every march tile shape the
+ * instances can take, then, on the fastest tile, of every launch shape;
+ * applies the fastest and returns it (best_shape[3], best_ms per step;
+ * either may be NULL; the tile through fdmap_gpu_ensemble_get_tile).  The
+ * ensemble's state is restored afterwards. */
 int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_shape, double* best_ms);
+
+/* March tile shape of every instance (0: 128 columns x 4 rows per row
+ * group, 1: 128 x 2, 2: 64 x 4); the autotuner picks it first. */
+int fdmap_gpu_ensemble_set_tile(fdmap_ensemble* e, int tile);
+int fdmap_gpu_ensemble_get_tile(fdmap_ensemble* e, int* tile);
 
 long long fdmap_gpu_ensemble_launch_count(fdmap_ensemble* e);
 void fdmap_gpu_ensemble_destroy(fdmap_ensemble* e);
