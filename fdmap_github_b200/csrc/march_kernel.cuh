@@ -2,11 +2,13 @@
 // (fused scale + SAT + SBP rates + szz + sources + RK update), organised for
 // HBM streaming on sm_100a.
 //
-// Work: every block is cut into strips of MW = 128 columns; the strip-rows of
-// all blocks form one sequence of row groups (MR = 4 rows) that is split into
-// equal contiguous ranges, one per resident CTA (grid = SMs x CTAs per SM), so
+// Work: every block is cut into strips of MW columns; the strip-rows of all
+// blocks form one sequence of row groups (MR rows) that is split into equal
+// contiguous ranges, one per resident CTA (grid = SMs x CTAs per SM), so
 // every CTA streams the same amount of data and consecutive CTAs hold
-// vertically adjacent rows (their halo rows are shared through L2).
+// vertically adjacent rows (their halo rows are shared through L2).  The tile
+// MW x MR is a template parameter (128 x 4, 128 x 2 or 64 x 4), chosen per
+// domain by the host or the autotuner; one CTA has MW x MR threads.
 //
 // Data movement: each row group arrives through 3-D tiled TMA boxes
 // (cp.async.bulk.tensor.3d ... mbarrier::complete_tx, no multicast) issued by
