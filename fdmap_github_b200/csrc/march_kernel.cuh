@@ -14,11 +14,11 @@
 // (cp.async.bulk.tensor.3d ... mbarrier::complete_tx, no multicast) issued by
 // one thread ahead of use, into two shared-memory rings with one mbarrier per
 // slot:
-//  - the neighbour ring (NGS = 4 slots: groups g-1, g, g+1 resident, g+2 in
-//    flight) holds what the stencil reads at neighbours: the rate fields and
+//  - the neighbour ring (NGS slots: groups g-1, g, g+1 resident, the next
+//    ones in flight) holds what the stencil reads at neighbours: the rate fields and
 //    yr, xr with PI halo columns ({WH, MR, NR} and {WH, MR, 2} boxes), and
 //    yq, xq, Ji ({MW, MR, 3});
-//  - the centre ring (NCS = 2 slots) holds what only the node itself reads:
+//  - the centre ring (NCS slots) holds what only the node itself reads:
 //    DF (skipped in a stage whose A is 0), szz and heterogeneous material.
 // Neighbours along i come from a slot's halo columns, neighbours along j from
 // the adjacent slots.  Boxes past the block edges are zero-filled by TMA.
@@ -39,8 +39,12 @@ namespace fdmap {
 constexpr int MARCH_SHAPES = 3;
 __host__ __device__ constexpr int shape_mw(int sh) { return sh == 2 ? 64 : 128; }
 __host__ __device__ constexpr int shape_mr(int sh) { return sh == 1 ? 2 : 4; }
-constexpr int NGS = 4;          // neighbour ring: row groups g-1, g, g+1 resident, g+2 in flight
-constexpr int NCS = 2;          // centre ring: group g resident, g+1 in flight
+// Ring depths: the neighbour ring holds groups g-1, g, g+1 and prefetches
+// the rest; the centre ring holds group g and prefetches the rest.  Thin
+// row groups get deeper rings, so about as many rows are in flight as with
+// 4-row groups.
+__host__ __device__ constexpr int shape_ngs(int sh) { return shape_mr(sh) == 2 ? 6 : 4; }
+__host__ __device__ constexpr int shape_ncs(int sh) { return shape_mr(sh) == 2 ? 3 : 2; }
 
 __host__ __device__ constexpr int even_halo(int h) { return (h + 1) & ~1; }
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
@@ -54,6 +58,8 @@ struct MarchLayout {
   static constexpr int MW = shape_mw(SH);
   static constexpr int MR = shape_mr(SH);
   static constexpr int THREADS = MW * MR;
+  static constexpr int NGS = shape_ngs(SH);
+  static constexpr int NCS = shape_ncs(SH);
   static constexpr int NR = RDef<MODE>::NR;
   static constexpr int HP = even_halo(PI_);
   static constexpr int WH = MW + 2 * HP;                       // halo row length (doubles)
@@ -232,6 +238,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
   constexpr int NF = MODE == 2 ? 6 : 3;
   constexpr int HP = L::HP;
   constexpr int WH = L::WH;
+  constexpr int NGS = L::NGS, NCS = L::NCS;
   extern __shared__ unsigned char smem_dyn[];
   unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_dyn) + 127) & ~uintptr_t(127));
   unsigned long long* nbar = reinterpret_cast<unsigned long long*>(smem + L::BARS_OFF);
