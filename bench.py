@@ -40,7 +40,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-from fdmap_github_b200 import GpuDomain, init_domain, problems  # noqa: E402
+from fdmap_github_b200 import FdmapError, GpuDomain, init_domain, problems  # noqa: E402
 from fdmap_github_b200.native import FAULT_INDEX  # noqa: E402
 
 METRIC = "FP64 node-updates/s"
@@ -57,9 +57,33 @@ NR_DF = {2: 5, 3: 3}
 RK_STAGES = {1: 1, 2: 2, 3: 3, 4: 5}
 
 
-def bytes_per_node_update(mode: int, het: bool, rk_order: int) -> int:
+def extra_bytes_per_node_stage(host) -> tuple[int, int]:
+    """(bytes in every stage, bytes not read in stage 1) a node moves for the
+    domain's extras: the Jacobian of dissipative blocks (1 read); per PML
+    layer W read + written and DW read + written (nF planes each, DW unread
+    when A = 0) and the two damping planes; body displacement U, DU (nU
+    planes each, read + written; DU unread when A = 0)."""
+    nF, every, first_skip = host.nF, 0, 0
+    if any(host.block_cdiss(b) > 0 for b in range(host.nblocks)):
+        every += 8
+    px, py = host.pml_fields()
+    if px or py:
+        every += 2 * 8
+        for on in (px, py):
+            if on:
+                every += 4 * nF * 8
+                first_skip += nF * 8
+    if host.displacement:
+        nU = 2 if host.mode == 2 else 1
+        every += 4 * nU * 8
+        first_skip += nU * 8
+    return every, first_skip
+
+
+def bytes_per_node_update(mode: int, het: bool, rk_order: int, host=None) -> int:
     """Algorithmic bytes of one node over one full step (all stages; DF unread in stage 1)."""
-    return RK_STAGES[rk_order] * BYTES_PER_NODE_STAGE[(mode, het)] - NR_DF[mode] * 8
+    ex, skip = extra_bytes_per_node_stage(host) if host is not None else (0, 0)
+    return RK_STAGES[rk_order] * (BYTES_PER_NODE_STAGE[(mode, het)] + ex) - NR_DF[mode] * 8 - skip
 
 
 def shared_config(info: dict, host) -> dict:
@@ -81,6 +105,14 @@ def workload(name: str, tmpdir: Path):
         text = problems.rough_fault_rs(tmpdir)
         return text, tmpdir, {"workload": "mode II rate-and-state (RFL) rough fault, 2 curvilinear blocks x 2001x1001",
                               "nodes": 2001 * 2002, "fault_nodes": 2001}
+    if name == "rupture_cdiss":
+        return problems.rupture_sw(cdiss=0.3), None, {
+            "workload": "mode II slip-weakening rupture, 2 blocks x 1601x801, dx 25 m, artificial dissipation "
+                        "Cdiss 0.3, LS-RK4 CFL 0.5", "nodes": 1601 * 1602, "fault_nodes": 1601}
+    if name == "pml":
+        return problems.pml_pulse(n=2001, L=40.0, width=3.0, nt=4001), None, {
+            "workload": "mode II P-SV pulse, 1 block 2001x2001 (dx 20 m) with a 3 km perfectly matched layer "
+                        "(Wx and Wy on every node), LS-RK4 CFL 0.5", "nodes": 2001 * 2001}
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -216,6 +248,12 @@ def run_gpu(args) -> None:
     g = GpuDomain(host, device=local)
     lib_set_stream(g, stream)
     nt_inf = 1 << 30
+    # the autotuner picks the march tile (the state is left as it was)
+    try:
+        tile, tune_ms = g.tune(steps=3)
+        tile_info = dict(zip(("tile", "strip_width", "rows_per_group"), g.tile()), tuned_ms_per_step=tune_ms)
+    except FdmapError:
+        tile, tile_info = None, {"tile": None, "kernel": "tiled interior kernel"}
     g.run(1, args.warmup, nt=nt_inf)
     g.synchronize()
     barrier(world)
@@ -251,12 +289,13 @@ def run_gpu(args) -> None:
     n_int = interior_nodes(host)
     # mean algorithmic bytes of one interior-kernel launch over the step's
     # stages: every stage reads F, metrics and DF, except stage 1 (A = 0)
-    stage_bytes = [n_int * (bps - (NR_DF[host.mode] * 8 if q == 0 else 0)) for q in range(nst)]
+    ex, skip = extra_bytes_per_node_stage(host)
+    stage_bytes = [n_int * (bps + ex - ((NR_DF[host.mode] * 8 + skip) if q == 0 else 0)) for q in range(nst)]
     alg_bytes = sum(stage_bytes) / nst
     achieved = alg_bytes / (stencil_ms * 1e-3) / 1e9
     peaks = measured_peaks()
     # the whole step (every node, every stage, all kernels) against the same peak
-    step_bytes = nodes * bytes_per_node_update(host.mode, het, host.rk_order)
+    step_bytes = nodes * bytes_per_node_update(host.mode, het, host.rk_order, host)
     step_gbs = step_bytes / (ms_max / args.steps * 1e-3) / 1e9
     survey_bytes = nodes * RK_STAGES[host.rk_order] * (BYTES_PER_NODE_STAGE[(host.mode, het)] - 5 * 8)
     newton_fail = g.newton_failures()
@@ -270,6 +309,8 @@ def run_gpu(args) -> None:
     # the first stage multiplies it by A(1) = 0 and never reads it.
     g2 = GpuDomain(host, device=local, init_edges=False)
     lib_set_stream(g2, stream)
+    if tile is not None:
+        g2.set_tile(tile)
     nf = info.get("fault_nodes", 0)
     # the fault registers as the descriptor gives them, before the initial edge solve
     fault0 = {f: torch.from_numpy(g2.get_fault(0, f)).pin_memory().numpy() for f in FAULT_INDEX} if nf else {}
@@ -332,9 +373,10 @@ def run_gpu(args) -> None:
                          "peak_source": peaks["source"],
                          "step_level": {"achieved": step_gbs, "frac": step_gbs / peaks["hbm_gbs"],
                                         "bytes_per_node_update": bytes_per_node_update(host.mode, het,
-                                                                                       host.rk_order),
+                                                                                       host.rk_order, host),
                                         "frac_without_metric_reads": survey_bytes / step_bytes * step_gbs
                                         / peaks["hbm_gbs"]}},
+            "march_tile": tile_info,
             "clocks": ck,
             "gpu_launches": launches,
             "newton_failures": newton_fail,
@@ -447,6 +489,7 @@ def run_ensemble(args) -> None:
     ens.synchronize()
     t_create = time.perf_counter() - t_create
     shape, tune_ms = ens.tune(steps=5, dt=dt)
+    tile = ens.tile
     ens.run(1, args.warmup, dt=dt, nt=1 << 30)
     ens.synchronize()
     barrier(world)
@@ -462,6 +505,7 @@ def run_ensemble(args) -> None:
     seq = 0.0
     for h in hosts:
         g = GpuDomain(h, device=local)
+        g.tune(steps=2, dt=dt)  # each plain run with its own best tile, as the ensemble has its own
         g.run(1, args.warmup, dt=dt, nt=1 << 30)
         g.synchronize()
         t0 = time.perf_counter()
@@ -488,6 +532,7 @@ def run_ensemble(args) -> None:
                 "config": {"workload": f"{n} mode II rate-and-state instances (RFL), 2 blocks each of "
                                        "401x401 / 801x401 / 801x801 / 1601x801 (seeded), von Karman prestress",
                            "instances": n, "nodes": nodes, "run_steps": run_steps, "shape": list(shape),
+                           "march_tile": tile,
                            "tuned_ms_per_step": tune_ms},
                 "node_updates_per_s": world * nodes / per_step,
                 "sequential_plain": {"runs_per_s": n / (seq / args.steps * run_steps),
@@ -655,7 +700,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--workload", default="rupture",
-                    choices=["rupture", "pulse", "roughfault", "ensemble", "adjoint", "adjoint_fault"])
+                    choices=["rupture", "pulse", "roughfault", "rupture_cdiss", "pml", "ensemble", "adjoint",
+                             "adjoint_fault"])
     ap.add_argument("--instances", type=int, default=64, help="ensemble workload: number of instances")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
