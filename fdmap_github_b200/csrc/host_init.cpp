@@ -734,9 +734,8 @@ void build(fdmap_domain& dom, const std::string& text, const std::string& base, 
       dom.nu[g] = 0.5 * (dom.M[g] - 2.0 * dom.G[g]) / (dom.M[g] - dom.G[g]);
     }
   }
-  // energy_block weights with the block's homogeneous constants (energy.f90:67-90)
-  if (d.energy_balance && any_het)
-    fail(FDMAP_ERR_UNSUPPORTED, "energy_balance=T with a heterogeneous medium is not supported");
+  // energy_block weights every block, heterogeneous ones too, with the
+  // block's material_list constants (M%rho, M%G, M%lambda; energy.f90:67-90)
   for (auto& B : dom.bin) {
     if (B.cs == 0.0 && !B.heterogeneous) fail(FDMAP_ERR_INVALID_ARG, "Must specify S-wave speed");
     if (B.cp == 0.0) B.cp = std::sqrt(3.0) * B.cs;

@@ -74,19 +74,36 @@ def test_mode2_energy_is_the_reference_quadrature():
     assert abs(o.get_energy()[-1] - np.sum(W * dens)) <= 1e-12 * o.get_energy()[-1]
 
 
-def test_energy_rejected_where_not_tracked(tmp_path):
+def test_heterogeneous_energy_uses_the_block_constants(tmp_path):
+    """In a heterogeneous medium energy_block still weights with the block's
+    material_list constants M%rho, M%G (energy.f90:67-90), not the node's."""
+    from oracle.binding import OracleDomain
+
     het = problems.heterogeneous_ricker(tmp_path, n=31, h=0.1, nt=5)
-    with pytest.raises(FdmapError):
-        init_domain(_energy(het, 3), tmp_path)
+    h = init_domain(_energy(het, 3), tmp_path)
+    assert h.heterogeneous and h.energy_balance
+    o = OracleDomain(h)
+    o.run(1, 3)
+    F = o.get_fields()[0]
+    o.time_step_LS(h.t0 + 3 * h.dt, h.dt, True)
+    # the quadrature of energy_block with the block constants rho = 2.67, G = rho*cs^2
+    hl = np.array([0.354166666666667, 1.229166666666667, 0.895833333333333, 1.020833333333333])
+    W = np.outer(_hnorm(h.ny, hl), _hnorm(h.nx, hl)) / h.array("Ji")[0]
+    rho, cs = 2.67, 3.464
+    G = rho * cs * cs
+    E = float(np.sum(0.5 * W * (rho * F[0] ** 2 + (F[1] ** 2 + F[2] ** 2) / G)))
+    assert abs(o.get_energy()[-1] - E) <= 1e-12 * abs(E)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case", ["rupture", "pulse"])
-def test_gpu_energy_vs_oracle(require_gpu, case):
+@pytest.mark.parametrize("case", ["rupture", "pulse", "heterogeneous"])
+def test_gpu_energy_vs_oracle(require_gpu, case, tmp_path):
     from oracle.binding import OracleDomain
 
     if case == "rupture":
         h = init_domain(_energy(problems.rupture_sw(nx=61, ny=31, h=0.4, nt=100), 2))
+    elif case == "heterogeneous":
+        h = init_domain(_energy(problems.heterogeneous_ricker(tmp_path, n=61, h=0.05, nt=100), 3), tmp_path)
     else:
         h = init_domain(_energy(problems.antiplane_pulse(n=61, L=6.0, nt=100), 3))
     g, o = GpuDomain(h), OracleDomain(h)
