@@ -15,7 +15,7 @@
 ! Every routine returns 0 or a negative FDMAP_ERR_* code; none aborts.
 module fdmap_gpu_mod
 
-  use, intrinsic :: iso_c_binding, only : c_int, c_double, c_ptr, c_char, c_long_long, c_null_ptr
+  use, intrinsic :: iso_c_binding, only : c_int, c_double, c_ptr, c_char, c_long_long, c_null_ptr, c_funptr
 
   implicit none
 
@@ -177,6 +177,90 @@ module fdmap_gpu_mod
        type(c_ptr), value :: h
        integer(c_long_long), intent(out) :: newton_failures
      end function fdmap_gpu_status
+
+     integer(c_int) function fdmap_gpu_newton_counts(h, counts) bind(C, name='fdmap_gpu_newton_counts')
+       import :: c_int, c_ptr, c_long_long
+       type(c_ptr), value :: h
+       integer(c_long_long), intent(out) :: counts(2)   ! first-attempt failures, failed retries
+     end function fdmap_gpu_newton_counts
+
+     integer(c_int) function fdmap_gpu_clear_status(h) bind(C, name='fdmap_gpu_clear_status')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function fdmap_gpu_clear_status
+
+     integer(c_int) function fdmap_gpu_set_newton_limit(h, imax) bind(C, name='fdmap_gpu_set_newton_limit')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: imax
+     end function fdmap_gpu_set_newton_limit
+
+     integer(c_int) function fdmap_gpu_test_wait_timeout(h, limit_s) bind(C, name='fdmap_gpu_test_wait_timeout')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: limit_s
+     end function fdmap_gpu_test_wait_timeout
+
+     integer(c_int) function fdmap_gpu_set_tile(h, tile) bind(C, name='fdmap_gpu_set_tile')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: tile
+     end function fdmap_gpu_set_tile
+
+     integer(c_int) function fdmap_gpu_get_tile(h, tile, mw, mr) bind(C, name='fdmap_gpu_get_tile')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), intent(out) :: tile, mw, mr
+     end function fdmap_gpu_get_tile
+
+     integer(c_int) function fdmap_gpu_tune(h, dt, steps, tile, ms) bind(C, name='fdmap_gpu_tune')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: h
+       real(c_double), value :: dt
+       integer(c_int), value :: steps
+       integer(c_int), intent(out) :: tile
+       real(c_double), intent(out) :: ms
+     end function fdmap_gpu_tune
+
+     integer(c_int) function fdmap_gpu_create_part(d, device, owned, h) bind(C, name='fdmap_gpu_create_part')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: d
+       integer(c_int), value :: device
+       integer(c_int), intent(in) :: owned(*)   ! 1 for every block this GPU steps
+       type(c_ptr), intent(out) :: h
+     end function fdmap_gpu_create_part
+
+     integer(c_int) function fdmap_gpu_part_buffers(h, iface, stage, send, recv, count) &
+          bind(C, name='fdmap_gpu_part_buffers')
+       import :: c_int, c_ptr, c_long_long
+       type(c_ptr), value :: h
+       integer(c_int), value :: iface
+       integer(c_long_long), value :: stage
+       type(c_ptr), intent(out) :: send, recv     ! device pointers
+       integer(c_long_long), intent(out) :: count
+     end function fdmap_gpu_part_buffers
+
+     integer(c_int) function fdmap_gpu_set_exchange(h, fn, user) bind(C, name='fdmap_gpu_set_exchange')
+       import :: c_int, c_ptr, c_funptr
+       type(c_ptr), value :: h
+       type(c_funptr), value :: fn     ! integer(c_int) function(user, stage, stream) bind(C)
+       type(c_ptr), value :: user
+     end function fdmap_gpu_set_exchange
+
+     integer(c_int) function fdmap_gpu_group_init_edges(hs, n, t) bind(C, name='fdmap_gpu_group_init_edges')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), intent(in) :: hs(*)
+       integer(c_int), value :: n
+       real(c_double), value :: t
+     end function fdmap_gpu_group_init_edges
+
+     integer(c_int) function fdmap_gpu_group_run(hs, n, t_start, dt, n_first, n_last, nt) &
+          bind(C, name='fdmap_gpu_group_run')
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), intent(in) :: hs(*)
+       integer(c_int), value :: n, n_first, n_last, nt
+       real(c_double), value :: t_start, dt
+     end function fdmap_gpu_group_run
 
      integer(c_int) function fdmap_gpu_check_finite(h, count) bind(C, name='fdmap_gpu_check_finite')
        import :: c_int, c_ptr, c_long_long
