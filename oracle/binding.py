@@ -42,6 +42,7 @@ def lib() -> C.CDLL:
         L.oracle_newton_stops.restype = C.c_longlong
         L.oracle_newton_stops.argtypes = [C.c_void_p]
         L.oracle_set_newton_limit.argtypes = [C.c_void_p, C.c_int]
+        L.oracle_set_newton_tolerance.argtypes = [C.c_void_p, C.c_double]
         L.oracle_num_threads.restype = C.c_int
         L.oracle_set_tap.argtypes = [C.c_void_p, C.c_int]
         L.oracle_get_fault_tap.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
@@ -221,6 +222,11 @@ class OracleDomain:
     def newton_counts(self) -> tuple[int, int]:
         """(first-attempt Newton failures, retries that failed too)."""
         return lib().oracle_newton_failures(self._o), lib().oracle_newton_stops(self._o)
+
+    def set_newton_tolerance(self, scale: float) -> None:
+        """Newton residual tolerance = scale x the reference's atolR."""
+        if lib().oracle_set_newton_tolerance(self._o, float(scale)) != 0:
+            raise ValueError("bad tolerance scale")
 
     def set_newton_limit(self, imax: int) -> None:
         if lib().oracle_set_newton_limit(self._o, int(imax)) != 0:

@@ -206,6 +206,7 @@ struct oracle_domain {
   long long newton_fail;   // solves whose first Newton attempt failed (the reference's warning)
   long long newton_stop;   // solves whose retry failed too (the reference stops there)
   int newton_imax = 99;    // friction.f90:924 imax
+  double newton_tol_scale = 1.0;  // atolR = 1e4*eps times this (a test of the result's sensitivity to atolR)
   bool tap = false;        // keep each step's stage-1 fault fields (write_output's view, time_step.f90:129)
   // block-aligned partition: blocks this rank steps (empty: all) and the
   // exchange of interface edge values, called after prepare_edges
@@ -370,8 +371,8 @@ void estimate_V(int law, const RS& rs, double& V, double Slock, double N, double
 // newton_solver (friction.f90:909-1038); returns fail.  imax is the
 // reference's parameter 99 unless a test lowers it (oracle_set_newton_limit).
 bool newton_solver(int law, const RS& rs, double& V, double& S, double Slock, double N, double eta, double Psi,
-                   int imax) {
-  const double rtolV = 0.0, atolV = 0.0, atolR = 2.220446049250313e-16 * 1e4;
+                   int imax, double tol_scale = 1.0) {
+  const double rtolV = 0.0, atolV = 0.0, atolR = 2.220446049250313e-16 * 1e4 * tol_scale;
   double Vmin = std::min(0.0, Slock / eta);
   double Vmax = std::max(0.0, Slock / eta);
   estimate_V(law, rs, V, Slock, N, Psi);
@@ -452,13 +453,13 @@ void solve_friction(oracle_domain& Dm, Fric& FR, int k, double S0, double N0, do
     return;
   }
   RS rs{FR.a[k], FR.b[k], FR.V0[k], FR.f0[k], FR.L[k], FR.fw[k], FR.Vw[k]};
-  bool fail = newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi, Dm.newton_imax);
+  bool fail = newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi, Dm.newton_imax, Dm.newton_tol_scale);
   if (fail) {
     // the reference warns, then retries from the failed iterate V, S
     // (friction.f90:789-790) and stops on a second failure (friction.f90:1014);
     // the oracle counts both events instead
     Dm.newton_fail++;
-    if (newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi, Dm.newton_imax)) Dm.newton_stop++;
+    if (newton_solver(FR.law, rs, V, S, Slock, Nreg, eta, Psi, Dm.newton_imax, Dm.newton_tol_scale)) Dm.newton_stop++;
   }
   if (FR.force) {
     if (Sk < std::fabs(S)) { S = fsign(Sk, Slock); V = (Slock - S) / eta; }
@@ -1863,6 +1864,12 @@ int oracle_set_pml(oracle_domain* o, int which, const double* in) {
   if (W.empty()) return -1;
   std::copy(in, in + W.size(), W.begin());
   return 0;
+}
+
+int oracle_set_newton_tolerance(oracle_domain* o, double scale) {
+  if (!o || !(scale > 0.0)) return FDMAP_ERR_INVALID_ARG;
+  o->newton_tol_scale = scale;
+  return FDMAP_OK;
 }
 
 int oracle_set_newton_limit(oracle_domain* o, int imax) {

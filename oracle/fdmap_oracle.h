@@ -81,6 +81,11 @@ long long oracle_newton_failures(const oracle_domain* o);
  * friction.f90:1014). */
 long long oracle_newton_stops(const oracle_domain* o);
 
+/* Newton residual tolerance as a multiple of the reference's atolR = 1e4*eps
+ * (friction.f90:931).  A test runs the oracle at another multiple to measure
+ * how far the result moves within the solver's own tolerance. */
+int oracle_set_newton_tolerance(oracle_domain* o, double scale);
+
 /* Iteration limit of every Newton solve (the reference's imax = 99,
  * friction.f90:924).  A test lowers it to force failures on the host. */
 int oracle_set_newton_limit(oracle_domain* o, int imax);

@@ -8,7 +8,7 @@ import pytest
 
 from fdmap_github_b200 import GpuDomain, GpuEnsemble, init_domain, problems
 from fdmap_github_b200.native import FAULT_FIELDS
-from tests.parity import assert_fault_close, assert_fields_close
+from tests.parity import assert_law_parity
 
 
 def _instances(tmp_path, sizes, nt=41):
@@ -70,8 +70,7 @@ def test_ensemble_instance_vs_oracle(require_gpu, tmp_path):
     ens.run(1, 25, dt=dt)
     o = OracleDomain(hosts[1])
     o.run(1, 25, dt=dt)
-    assert_fields_close(ens[1].get_fields()[0], o.get_fields()[0])
-    assert_fault_close(ens[1], o, dt=dt)
+    assert_law_parity(ens[1], o, "RFL", hosts[1], 25, dt=dt)
     ens.close()
 
 

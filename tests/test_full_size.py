@@ -10,7 +10,10 @@ By default a few hundred steps of each (the oracle needs about a minute on the
 GPU box's host cores).  With FDMAP_FULL_LENGTH=1 the whole runs, 4000 and 6000
 steps (nt = 4001 and 6001 loop indices, the last one the reference's
 output-only index), are compared instead.  Every case prints one line
-`FULLSIZE {json}` with the per-field and fault errors."""
+`FULLSIZE {json}` with the per-field and fault errors and the tolerances
+they were held to (tests/parity.py: 1e-10 for the slip-weakening rupture; for
+the rate-and-state run the spread of the oracle's own answer when its Newton
+tolerance is halved, measured in the same test)."""
 from __future__ import annotations
 
 import json
@@ -20,14 +23,14 @@ import numpy as np
 import pytest
 
 from fdmap_github_b200 import GpuDomain, init_domain, problems
-from tests.parity import FAULT_RTOL, FIELD_RTOL, assert_fields_close, fault_errors, field_errors
+from tests.parity import FIELD_RTOL, assert_fault_close, assert_fields_close, fault_errors, field_errors, law_tolerances
 
 pytestmark = pytest.mark.gpu
 
 FULL = os.environ.get("FDMAP_FULL_LENGTH") == "1"
 
 
-def _compare(name, h, n_last, fault_fields=("V", "S", "N", "D", "Psi")):
+def _compare(name, h, n_last, law, fault_fields=("V", "S", "N", "D", "Psi")):
     from oracle.binding import OracleDomain
 
     g, o = GpuDomain(h), OracleDomain(h)
@@ -37,15 +40,16 @@ def _compare(name, h, n_last, fault_fields=("V", "S", "N", "D", "Psi")):
     ferr = field_errors(Fg, Fo)
     flt = fault_errors(g, o, fields=fault_fields)
     tg, to = g.get_fault(0, "trup"), o.get_fault(0, "trup")
+    # explicit solves: 1e-10; rate-and-state: the spread within the reference's solver tolerance
+    ftol, qtol = law_tolerances(law, h, n_last, fault_fields)
     rec = {"case": name, "nx": h.nx, "ny": h.ny, "loop_indices": n_last, "field_rel_err": ferr,
-           "fault_rel_err": flt, "trup_mismatch_nodes": int(np.count_nonzero(tg != to)),
+           "fault_rel_err": flt, "field_tolerance": ftol, "fault_tolerance": qtol,
+           "trup_mismatch_nodes": int(np.count_nonzero(tg != to)),
            "max_slip_rate": float(np.abs(o.get_fault(0, "V")).max()),
            "newton": [g.newton_failures(), o.newton_failures()]}
     print("FULLSIZE " + json.dumps(rec), flush=True)
-    assert_fields_close(Fg, Fo, what=name)
-    for f, e in flt.items():
-        assert e <= FAULT_RTOL, f"{name}: fault {f} relative error {e}"
-    assert rec["trup_mismatch_nodes"] <= max(2, tg.size // 500)
+    assert_fields_close(Fg, Fo, rtol=ftol, what=name)
+    assert_fault_close(g, o, rtol=qtol, dt=h.dt, fields=fault_fields)
     g.close()
     o.close()
     return rec
@@ -54,14 +58,14 @@ def _compare(name, h, n_last, fault_fields=("V", "S", "N", "D", "Psi")):
 def test_rupture_full_grid(require_gpu):
     h = init_domain(problems.rupture_sw())
     assert (h.nx, h.ny) == (1601, 1602)
-    rec = _compare("rupture 2x1601x801", h, h.nt if FULL else 300, ("V", "S", "N", "D"))
+    rec = _compare("rupture 2x1601x801", h, h.nt if FULL else 300, "SW", ("V", "S", "N", "D"))
     assert rec["max_slip_rate"] > 0.1  # the patch has nucleated
 
 
 def test_roughfault_full_grid(require_gpu, tmp_path):
     h = init_domain(problems.rough_fault_rs(tmp_path), tmp_path)
     assert (h.nx, h.ny) == (2001, 2002)
-    _compare("roughfault 2x2001x1001", h, h.nt if FULL else 200)
+    _compare("roughfault 2x2001x1001", h, h.nt if FULL else 200, "RFL")
 
 
 def test_field_tolerance_is_the_stated_one():

@@ -6,7 +6,7 @@ import pytest
 
 from fdmap_github_b200 import GpuDomain, init_domain, problems
 from oracle.binding import OracleDomain
-from tests.parity import assert_fault_close, assert_fields_close, field_errors, rel_err
+from tests.parity import assert_fault_close, assert_fields_close, assert_law_parity, field_errors, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -117,8 +117,7 @@ def test_rough_fault_rate_state(require_gpu, tmp_path):
     h, g, o = _pair(text, tmp_path)
     g.run(1, h.nt)
     o.run(1, h.nt)
-    assert_fields_close(g.get_fields()[0], o.get_fields()[0])
-    assert_fault_close(g, o, dt=h.dt, fields=("V", "S", "N", "D", "Psi"))
+    assert_law_parity(g, o, "RFL", h, h.nt, dt=h.dt)
     assert g.newton_failures() == 0 and o.newton_failures() == 0
 
 

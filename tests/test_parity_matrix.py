@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from fdmap_github_b200 import GpuDomain, init_domain
-from tests.parity import assert_fault_close, assert_fields_close
+from tests.parity import assert_fields_close, assert_law_parity
 
 
 def _f(x: float) -> str:
@@ -184,8 +184,32 @@ def test_gpu_vs_oracle(require_gpu, name):
     steps = 30
     g.run(1, steps)
     o.run(1, steps)
-    assert_fields_close(g.get_fields()[0], o.get_fields()[0], what=name)
-    assert_fault_close(g, o, dt=h.dt)
+    law = CASES[name].get("law", "SW")
+    assert_law_parity(g, o, law, h, steps, dt=h.dt, what=name)
     assert g.newton_failures() == o.newton_failures() == 0
     assert np.abs(o.get_fault(0, "V")).max() > 1e-3, f"{name}: the fault should slip"
+    g.close()
+
+
+# 200 steps of every law whose Newton solves all converge there (the
+# log-strength law 'FL' fails its retries on this rupture after ~100 steps,
+# where the reference would stop, friction.f90:1014)
+LONG = ["SW", "SL", "RSL", "RFL", "RSF", "RAL", "III-RAL", "x-RFL", "lock-window"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", LONG)
+def test_gpu_vs_oracle_200_steps(require_gpu, name):
+    """Longer runs: the rate-and-state laws are held to the spread of the
+    reference's own answer within its Newton tolerance (tests/parity.py),
+    the explicit laws to 1e-10."""
+    from oracle.binding import OracleDomain
+
+    h = init_domain(fault_text(**CASES[name], nt=201))
+    g, o = GpuDomain(h), OracleDomain(h)
+    g.run(1, 200)
+    o.run(1, 200)
+    law = CASES[name].get("law", "SW")
+    assert_law_parity(g, o, law, h, 200, dt=h.dt, what=name)
+    assert g.newton_counts() == o.newton_counts()
     g.close()
