@@ -228,18 +228,21 @@ int engine_stage(fdmap_gpu* h, const StageArgs& a);
 
 int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 
-// The interior march for tile shape 0..2 (march_s<N>.cu): configure sets the
+// The interior march for tile shape 0..3 (march_s<N>.cu): configure sets the
 // unit decomposition, tensor maps and grid for that shape (FDMAP_ERR_UNSUPPORTED
 // when the shape cannot serve the handle's variant); launch issues one stage.
 int march_configure_s0(fdmap_gpu* h);
 int march_configure_s1(fdmap_gpu* h);
 int march_configure_s2(fdmap_gpu* h);
+int march_configure_s3(fdmap_gpu* h);
 int march_launch_s0(fdmap_gpu* h, const StageArgs& a);
 int march_launch_s1(fdmap_gpu* h, const StageArgs& a);
 int march_launch_s2(fdmap_gpu* h, const StageArgs& a);
+int march_launch_s3(fdmap_gpu* h, const StageArgs& a);
 int march_batch_s0(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 int march_batch_s1(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 int march_batch_s2(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
+int march_batch_s3(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 // configure for `shape` and publish the domain (device copy, step graphs dropped)
 int march_set_shape(fdmap_gpu* h, int shape);
 

@@ -456,7 +456,7 @@ int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_s
 }
 
 int fdmap_gpu_ensemble_set_tile(fdmap_ensemble* e, int tile) {
-  if (!e || tile < 0 || tile >= MARCH_SHAPES) return set_err(FDMAP_ERR_INVALID_ARG, "tile must be 0, 1 or 2");
+  if (!e || tile < 0 || tile >= MARCH_SHAPES) return set_err(FDMAP_ERR_INVALID_ARG, "tile must be 0..3");
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
   return ens_set_tile(e, tile);

@@ -159,7 +159,8 @@ int march_dispatch(fdmap_gpu* h, const StageArgs& a) {
   switch (h->march_shape) {
     case 0: return march_launch_s0(h, a);
     case 1: return march_launch_s1(h, a);
-    default: return march_launch_s2(h, a);
+    case 2: return march_launch_s2(h, a);
+    default: return march_launch_s3(h, a);
   }
 }
 
@@ -168,8 +169,9 @@ int march_configure(fdmap_gpu* h, int shape) {
     case 0: return march_configure_s0(h);
     case 1: return march_configure_s1(h);
     case 2: return march_configure_s2(h);
+    case 3: return march_configure_s3(h);
   }
-  return set_err(FDMAP_ERR_INVALID_ARG, "march tile shape must be 0, 1 or 2");
+  return set_err(FDMAP_ERR_INVALID_ARG, "march tile shape must be 0..3");
 }
 
 int launch_stage(fdmap_gpu* h, const StageArgs& a);
@@ -195,7 +197,8 @@ int batch_march(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, 
   switch (proto->march_shape) {
     case 0: return march_batch_s0(proto, a, p, s);
     case 1: return march_batch_s1(proto, a, p, s);
-    default: return march_batch_s2(proto, a, p, s);
+    case 2: return march_batch_s2(proto, a, p, s);
+    default: return march_batch_s3(proto, a, p, s);
   }
 }
 
@@ -1546,7 +1549,7 @@ int fdmap_gpu_clear_status(fdmap_gpu* h) {
 }
 
 int fdmap_gpu_set_tile(fdmap_gpu* h, int tile) {
-  if (!h || tile < 0 || tile >= MARCH_SHAPES) return set_err(FDMAP_ERR_INVALID_ARG, "tile must be 0, 1 or 2");
+  if (!h || tile < 0 || tile >= MARCH_SHAPES) return set_err(FDMAP_ERR_INVALID_ARG, "tile must be 0..3");
   return march_set_shape(h, tile);
 }
 

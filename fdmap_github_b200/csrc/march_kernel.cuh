@@ -7,8 +7,9 @@
 // contiguous ranges, one per resident CTA (grid = SMs x CTAs per SM), so
 // every CTA streams the same amount of data and consecutive CTAs hold
 // vertically adjacent rows (their halo rows are shared through L2).  The tile
-// MW x MR is a template parameter (128 x 4, 128 x 2 or 64 x 4), chosen per
-// domain by the host or the autotuner; one CTA has MW x MR threads.
+// MW x MR is a template parameter (128 x 4, 128 x 2 with deep rings, 64 x 4,
+// 128 x 2 with shallow rings and two CTAs per SM), chosen per domain by the
+// host or the autotuner; one CTA has MW x MR threads.
 //
 // Data movement: each row group arrives through 3-D tiled TMA boxes
 // (cp.async.bulk.tensor.3d ... mbarrier::complete_tx, no multicast) issued by
@@ -36,15 +37,16 @@ namespace fdmap {
 // The host picks one per domain (the first whose rings fit in shared memory,
 // or the autotuner's choice); the unit decomposition and the tensor-map boxes
 // follow it.
-constexpr int MARCH_SHAPES = 3;
+constexpr int MARCH_SHAPES = 4;
 __host__ __device__ constexpr int shape_mw(int sh) { return sh == 2 ? 64 : 128; }
-__host__ __device__ constexpr int shape_mr(int sh) { return sh == 1 ? 2 : 4; }
+__host__ __device__ constexpr int shape_mr(int sh) { return (sh == 1 || sh == 3) ? 2 : 4; }
 // Ring depths: the neighbour ring holds groups g-1, g, g+1 and prefetches
-// the rest; the centre ring holds group g and prefetches the rest.  Thin
-// row groups get deeper rings, so about as many rows are in flight as with
-// 4-row groups.
-__host__ __device__ constexpr int shape_ngs(int sh) { return shape_mr(sh) == 2 ? 6 : 4; }
-__host__ __device__ constexpr int shape_ncs(int sh) { return shape_mr(sh) == 2 ? 3 : 2; }
+// the rest; the centre ring holds group g and prefetches the rest.  Shape 1
+// (2-row groups) gets deeper rings, so about as many rows are in flight per
+// CTA as with 4-row groups; shape 3 (also 2-row groups) keeps the shallow
+// rings, small enough for two CTAs per SM.
+__host__ __device__ constexpr int shape_ngs(int sh) { return sh == 1 ? 6 : 4; }
+__host__ __device__ constexpr int shape_ncs(int sh) { return sh == 1 ? 3 : 2; }
 
 __host__ __device__ constexpr int even_halo(int h) { return (h + 1) & ~1; }
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }

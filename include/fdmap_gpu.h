@@ -134,7 +134,8 @@ int fdmap_gpu_newton_counts(fdmap_gpu* h, long long* counts);
 int fdmap_gpu_clear_status(fdmap_gpu* h);
 
 /* Tile shape of the interior march kernel: 0 = 128 columns x 4 rows per row
- * group, 1 = 128 x 2, 2 = 64 x 4.  The engine starts with the first shape
+ * group, 1 = 128 x 2 with deep prefetch rings, 2 = 64 x 4, 3 = 128 x 2 with
+ * shallow rings and two CTAs per SM.  The engine starts with the first shape
  * whose shared-memory rings fit the domain's variant (a heterogeneous mode II
  * medium or the extras of dissipation, PML, forcing and body displacement
  * need the smaller rings).  set_tile returns FDMAP_ERR_UNSUPPORTED for a
@@ -315,8 +316,8 @@ int fdmap_gpu_ensemble_get_shape(fdmap_ensemble* e, int* shape);
  * ensemble's state is restored afterwards. */
 int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_shape, double* best_ms);
 
-/* March tile shape of every instance (0: 128 columns x 4 rows per row
- * group, 1: 128 x 2, 2: 64 x 4); the autotuner picks it first. */
+/* March tile shape of every instance (as fdmap_gpu_set_tile, 0..3); the
+ * autotuner picks it first. */
 int fdmap_gpu_ensemble_set_tile(fdmap_ensemble* e, int tile);
 int fdmap_gpu_ensemble_get_tile(fdmap_ensemble* e, int* tile);
 
