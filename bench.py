@@ -329,17 +329,22 @@ def run_gpu(args) -> None:
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_up, e_run = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
     g2.set_fields(pin_F.numpy(), None)
     for f, v in fault0.items():
         g2.set_fault(0, f, v)
+    e_up.record(stream)
     lib().fdmap_gpu_init_edges(g2._g, host.t0)
     g2.run(1, args.steps, nt=nt_inf)
     if nf:
         g2.output_flush()
+    e_run.record(stream)
     rc = lib().fdmap_gpu_get_fields(g2._g, C.cast(pin_out.data_ptr(), C.POINTER(C.c_double)), None)
     e_stop.record(stream)
     e_stop.synchronize()
+    e_parts = {"upload_ms": e_start.elapsed_time(e_up), "steps_and_output_ms": e_up.elapsed_time(e_run),
+               "download_ms": e_run.elapsed_time(e_stop)}
     if rc:
         raise RuntimeError(f"fdmap_gpu_get_fields failed ({rc})")
     e_ms = max(e_start.elapsed_time(e_stop), (time.perf_counter() - t0) * 1e3)
@@ -363,7 +368,8 @@ def run_gpu(args) -> None:
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": shared_config(info, host),
             "parallelism": f"replicas{world}",
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms": e_ms, **e_parts},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload),
                          "kernel": "march_kernel", "alg_bytes_per_launch": alg_bytes,
