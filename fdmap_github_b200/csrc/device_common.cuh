@@ -112,7 +112,17 @@ struct DevIface {
 constexpr int PADL = 32;
 constexpr int PADTAIL = 192;
 
+// Timeline of the stage kernels (fdmap_gpu_trace): one record of three words
+// per CTA, (kind | SM << 8 | CTA << 16, start ns, end ns) on %globaltimer
+enum { TRACE_MARCH = 1, TRACE_CLOSURE = 2, TRACE_EDGE = 3, TRACE_TILED = 4 };
+struct TraceBuf {
+  unsigned long long* rec;  // NULL: tracing off
+  unsigned int* n;
+  unsigned int cap;
+};
+
 struct DevDomain {
+  TraceBuf trace;
   int mode, nF, nblocks, nifaces, het;
   int nbst, nbnd, pI;
   double DI[4];     // DI[s], s = 1..pI (fd_coeff.f90)
@@ -244,5 +254,24 @@ __device__ __forceinline__ void rot3_nt2xy(double* F, double n0, double n1, doub
 }
 
 __device__ __forceinline__ double fsign(double a, double b) { return copysign(fabs(a), b); }
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// one timeline record for the calling CTA (call from one thread)
+__device__ __forceinline__ void trace_record(const TraceBuf& T, int kind, unsigned long long t0) {
+  if (!T.rec) return;
+  unsigned sm;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+  const unsigned k = atomicAdd(T.n, 1u);
+  if (k >= T.cap) return;
+  unsigned long long* r = T.rec + 3 * (size_t)k;
+  r[0] = (unsigned long long)kind | ((unsigned long long)sm << 8) | ((unsigned long long)blockIdx.x << 16);
+  r[1] = t0;
+  r[2] = globaltimer_ns();
+}
 
 }  // namespace fdmap

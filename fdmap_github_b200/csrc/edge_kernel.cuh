@@ -509,11 +509,13 @@ __global__ void __launch_bounds__(128) pack_edges(const __grid_constant__ DevDom
 // hat variables of both sides, and the fault register life cycle.
 template <int MODE>
 __global__ void __launch_bounds__(64) edge_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
+  const unsigned long long t_in = (threadIdx.x == 0 && D.trace.rec) ? globaltimer_ns() : 0ull;
   int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.seg_start[D.nseg]) return;
   int sg = 0;
   while (tid >= D.seg_start[sg + 1]) ++sg;
   d_iface_node<MODE>(D, D.ifc[D.seg_a[sg]], tid - D.seg_start[sg], a);
+  if (threadIdx.x == 0) trace_record(D.trace, TRACE_EDGE, t_in);
 }
 
 // Interface nodes of a batch of independent instances in one launch.

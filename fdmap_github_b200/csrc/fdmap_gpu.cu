@@ -1548,6 +1548,43 @@ int fdmap_gpu_clear_status(fdmap_gpu* h) {
   return FDMAP_OK;
 }
 
+int fdmap_gpu_trace(fdmap_gpu* h, int capacity) {
+  if (!h || capacity < 0) return set_err(FDMAP_ERR_INVALID_ARG, "bad trace arguments");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  TraceBuf& T = h->hdom.trace;
+  if (capacity > 0 && (unsigned)capacity > T.cap) {
+    unsigned long long* rec = nullptr;
+    unsigned int* n = nullptr;
+    int rc;
+    if ((rc = h->alloc(&rec, (size_t)capacity * 3)) || (rc = h->alloc(&n, 1))) return rc;
+    T.rec = rec;
+    T.n = n;
+    T.cap = (unsigned)capacity;
+  }
+  if (capacity == 0) T.rec = nullptr;  // off (the buffers stay with the handle)
+  if (T.n) CUDA_TRY(cudaMemset(T.n, 0, sizeof(unsigned int)));
+  CUDA_TRY(cudaMemcpy(h->ddom, &h->hdom, sizeof(DevDomain), cudaMemcpyHostToDevice));
+  for (auto& ge : h->step_graph)  // the graphs carry the domain by value
+    if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  h->graph_dt = 0.0;
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_trace_read(fdmap_gpu* h, unsigned long long* records, int max) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  const TraceBuf& T = h->hdom.trace;
+  if (!T.n) return 0;
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  unsigned int n = 0;
+  CUDA_TRY(cudaMemcpy(&n, T.n, sizeof(n), cudaMemcpyDeviceToHost));
+  n = std::min<unsigned>(n, T.cap);
+  const int k = std::min<int>((int)n, max);
+  if (records && k > 0) CUDA_TRY(cudaMemcpy(records, T.rec, (size_t)k * 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  return (int)n;
+}
+
 int fdmap_gpu_set_tile(fdmap_gpu* h, int tile) {
   if (!h || tile < 0 || tile >= MARCH_SHAPES) return set_err(FDMAP_ERR_INVALID_ARG, "tile must be 0..3");
   return march_set_shape(h, tile);

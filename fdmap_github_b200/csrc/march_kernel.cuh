@@ -172,12 +172,6 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
 // Longest a TMA pipeline wait may take before the kernel gives up (a normal
 // row-group delivery takes microseconds).
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
@@ -248,6 +242,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
 
   const int tid = threadIdx.x;
   const int cx = tid % MW, ry = tid / MW;
+  const unsigned long long t_in = (tid == 0 && doms[0].trace.rec) ? globaltimer_ns() : 0ull;
   const long long ubeg = plan.units * blockIdx.x / gridDim.x;
   const long long uend = plan.units * (blockIdx.x + 1) / gridDim.x;
   const bool load_df = a.scale && a.A != 0.0;  // A = 0 (first stage): A*DF = 0, DF is not read
@@ -496,6 +491,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
     __syncthreads();
     u = seg_end;
   }
+  if (tid == 0) trace_record(doms[0].trace, TRACE_MARCH, t_in);
 }
 
 }  // namespace fdmap

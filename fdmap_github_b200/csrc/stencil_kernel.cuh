@@ -687,11 +687,13 @@ __device__ __forceinline__ bool on_interface_side(const DevBlock& B, int i, int 
 // Boundary kernel: every node within nbst of a block edge (the SBP closure strips).
 template <int MODE, int PI_, bool HET>
 __global__ void __launch_bounds__(128) closure_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
+  const unsigned long long t_in = (threadIdx.x == 0 && D.trace.rec) ? globaltimer_ns() : 0ull;
   long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.cstart[4 * D.nblocks]) return;
   int i, j;
   const int b = closure_item(D, tid, i, j);
   closure_node<MODE, PI_, HET>(D, D.blk[b], i, j, a, -1, nullptr);
+  if (threadIdx.x == 0) trace_record(D.trace, TRACE_CLOSURE, t_in);
 }
 
 // Closure strips of a batch of independent instances in one launch.

@@ -353,6 +353,20 @@ class GpuDomain:
                   "fdmap_gpu_tune")
         return t.value, ms.value
 
+    def trace(self, capacity: int) -> None:
+        """Record one timeline entry per CTA of the stage kernels (0 switches it off)."""
+        check_gpu(lib().fdmap_gpu_trace(self._g, int(capacity)), "fdmap_gpu_trace")
+
+    def trace_records(self) -> np.ndarray:
+        """(n, 5) int64 array: kind (1 march, 2 closure, 3 interface), SM, CTA, start ns, end ns."""
+        n = lib().fdmap_gpu_trace_read(self._g, None, 0)
+        if n < 0:
+            check_gpu(n, "fdmap_gpu_trace_read")
+        buf = (C.c_ulonglong * (3 * max(n, 1)))()
+        lib().fdmap_gpu_trace_read(self._g, buf, n)
+        a = np.ctypeslib.as_array(buf)[:3 * n].reshape(n, 3).astype(np.int64)
+        return np.stack([a[:, 0] & 0xFF, (a[:, 0] >> 8) & 0xFF, a[:, 0] >> 16, a[:, 1], a[:, 2]], axis=1)
+
     def set_newton_limit(self, imax: int) -> None:
         """Lower the Newton iteration limit (imax = 99 in the reference) to provoke failures."""
         check_gpu(lib().fdmap_gpu_set_newton_limit(self._g, int(imax)), "fdmap_gpu_set_newton_limit")

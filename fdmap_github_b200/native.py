@@ -106,6 +106,8 @@ SIGNATURES = {
     "fdmap_gpu_group_time_step": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_double, C.c_double, C.c_int]),
     "fdmap_gpu_group_run": (C.c_int, [C.POINTER(_VP), C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
                                       C.c_int]),
+    "fdmap_gpu_trace": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_trace_read": (C.c_int, [_VP, C.POINTER(C.c_ulonglong), C.c_int]),
     "fdmap_gpu_launch_count": (C.c_longlong, [_VP]),
     "fdmap_gpu_device_bytes": (C.c_longlong, [_VP]),
     "fdmap_gpu_destroy": (None, [_VP]),

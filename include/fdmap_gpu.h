@@ -263,6 +263,16 @@ int fdmap_gpu_group_init_edges(fdmap_gpu* const* hs, int n, double t);
 int fdmap_gpu_group_time_step(fdmap_gpu* const* hs, int n, double t0, double dt, int final_step);
 int fdmap_gpu_group_run(fdmap_gpu* const* hs, int n, double t_start, double dt, int n_first, int n_last, int nt);
 
+/* Kernel timeline: with capacity > 0 every CTA of the stage kernels
+ * (interior march, closure, interface) appends one record of three words --
+ * kind (1 march, 2 closure, 3 interface) | SM << 8 | CTA << 16, start and end
+ * in ns of the device's global timer -- until `capacity` records are taken;
+ * 0 switches it off.  Enabling clears the records.  fdmap_gpu_trace_read
+ * copies up to `max` records and returns how many were taken.  No reference
+ * counterpart (the reference times whole steps, main.f90:202-253). */
+int fdmap_gpu_trace(fdmap_gpu* h, int capacity);
+int fdmap_gpu_trace_read(fdmap_gpu* h, unsigned long long* records, int max);
+
 /* Kernel launches issued by the last fdmap_gpu_run / time_step call. */
 long long fdmap_gpu_launch_count(fdmap_gpu* h);
 
