@@ -232,7 +232,7 @@ def test_outputs_match_oracle_files(require_gpu, tmp_path):
     g.output_close()
     w = OracleOutputs(OracleDomain(h), h, text, tmp_path / "o")
     w.run(1, 30)
-    assert len(w.stems) == 8
+    assert len(w.stems) == 10  # I: D V S trup, B: vx sxy, P: vy, G: V at nodes 5, 15, 25
     differing = 0
     for stem in w.stems:
         for ext in (".t", ".dat"):
