@@ -62,7 +62,7 @@ struct fdmap_gpu {
   int march_grid = 0;
   int use_march = 1;
   int march_shape = 0;      // tile shape of the march (shape_mw / shape_mr)
-  bool march_ext = false;   // the march variant with dissipation, PML, forcing and body extras
+  int march_ext = 0;        // march variant: 0 plain, 1 dissipation / forcing / body extras, 2 PML (+ forcing, extras)
   bool dissipation = false;  // some block has Cdiss > 0 (tiled interior kernel)
   bool pml = false;  // some block has a perfectly matched layer (tiled interior kernel)
   bool forcing = false;  // tsunami forcing or forcing from file (tiled interior kernel)
@@ -105,6 +105,7 @@ struct fdmap_gpu {
   fdmap_exchange_fn exchange = nullptr;
   void* exchange_user = nullptr;
   long long xstage = 0;               // stages issued (selects the send slot)
+  unsigned long long* trace_rec = nullptr;  // timeline records (fdmap_gpu_trace), kept while tracing is off
   cudaEvent_t ev_packed = nullptr;    // the stage's edge values are packed
   bool owns(int b) const { return owned.empty() || owned[(size_t)b] != 0; }
   bool partitioned() const { return !owned.empty(); }

@@ -271,18 +271,44 @@ int batch_edges(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, 
 
 namespace {
 
+// 64-thread closure CTAs: at about 170 registers a thread, two warps fit in
+// the registers a 512-thread march CTA leaves free on its SM
+constexpr int CLOSURE_TPB = 64;
+
 template <int MODE>
 void launch_closure_mode(fdmap_gpu* h, const StageArgs& a) {
-  int nb = (int)((h->closure_threads + 127) / 128);
+  const int t = CLOSURE_TPB;
+  int nb = (int)((h->closure_threads + t - 1) / t);
   if (h->het) {
-    if (h->pI == 1) closure_kernel<MODE, 1, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
-    else if (h->pI == 2) closure_kernel<MODE, 2, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
-    else closure_kernel<MODE, 3, true><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    if (h->pI == 1) closure_kernel<MODE, 1, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+    else if (h->pI == 2) closure_kernel<MODE, 2, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+    else closure_kernel<MODE, 3, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
   } else {
-    if (h->pI == 1) closure_kernel<MODE, 1, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
-    else if (h->pI == 2) closure_kernel<MODE, 2, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
-    else closure_kernel<MODE, 3, false><<<nb, 128, 0, h->stream>>>(h->hdom, a);
+    if (h->pI == 1) closure_kernel<MODE, 1, false><<<nb, t, 0, h->stream>>>(h->hdom, a);
+    else if (h->pI == 2) closure_kernel<MODE, 2, false><<<nb, t, 0, h->stream>>>(h->hdom, a);
+    else closure_kernel<MODE, 3, false><<<nb, t, 0, h->stream>>>(h->hdom, a);
   }
+}
+
+// The boundary kernels run beside the persistent march CTAs, which configure
+// their SMs for the largest shared-memory carveout; a kernel launched with
+// another carveout preference is not placed on an SM configured otherwise, so
+// without this the boundary CTAs would wait for the march CTAs to retire.
+template <int MODE>
+int boundary_carveout_mode() {
+  const void* ks[] = {
+      (const void*)edge_kernel<MODE>, (const void*)edge_kernel_batch<MODE>, (const void*)pack_edges<MODE>,
+      (const void*)closure_kernel<MODE, 1, false>, (const void*)closure_kernel<MODE, 2, false>,
+      (const void*)closure_kernel<MODE, 3, false>, (const void*)closure_kernel<MODE, 1, true>,
+      (const void*)closure_kernel<MODE, 2, true>, (const void*)closure_kernel<MODE, 3, true>,
+      (const void*)closure_kernel_batch<MODE, 1, false>, (const void*)closure_kernel_batch<MODE, 2, false>,
+      (const void*)closure_kernel_batch<MODE, 3, false>, (const void*)closure_kernel_batch<MODE, 1, true>,
+      (const void*)closure_kernel_batch<MODE, 2, true>, (const void*)closure_kernel_batch<MODE, 3, true>,
+  };
+  for (const void* k : ks)
+    CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
+  return FDMAP_OK;
 }
 
 template <int MODE>
@@ -841,13 +867,20 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     // the march serves every variant: dissipation (J halo rows in the ring),
     // PML, forcing and body extras through its extras variant; the first
     // tile shape whose rings fit is taken (the autotuner may change it)
-    h->march_ext = h->dissipation || h->pml || h->forcing || h->extras;
-    h->use_march = !(ek && std::string(ek) == "tile");
+    // (a domain with both dissipative and PML blocks keeps the tiled kernel)
+    h->march_ext = h->pml ? 2 : ((h->dissipation || h->forcing || h->extras) ? 1 : 0);
+    h->use_march = !(ek && std::string(ek) == "tile") && !(h->pml && h->dissipation);
     if (h->use_march) {
       rc = FDMAP_ERR_UNSUPPORTED;
       for (int sh = 0; sh < MARCH_SHAPES && rc == FDMAP_ERR_UNSUPPORTED; ++sh) rc = march_configure(h, sh);
       if (rc == FDMAP_ERR_UNSUPPORTED) h->use_march = 0;  // no shape fits: the tiled interior kernel
       else if (rc) return rc;
+    }
+    // boundary kernels on the march's carveout (FDMAP_CARVEOUT=default leaves the driver's choice)
+    const char* ec = getenv("FDMAP_CARVEOUT");
+    if (h->use_march && !(ec && std::string(ec) == "default")) {
+      rc = h->mode == 2 ? boundary_carveout_mode<2>() : boundary_carveout_mode<3>();
+      if (rc) return rc;
     }
     // fused stage launches need every interface-side node to sit on one interface only
     bool junction = false;
@@ -1558,12 +1591,16 @@ int fdmap_gpu_trace(fdmap_gpu* h, int capacity) {
     unsigned int* n = nullptr;
     int rc;
     if ((rc = h->alloc(&rec, (size_t)capacity * 3)) || (rc = h->alloc(&n, 1))) return rc;
-    T.rec = rec;
+    h->trace_rec = rec;
     T.n = n;
     T.cap = (unsigned)capacity;
   }
-  if (capacity == 0) T.rec = nullptr;  // off (the buffers stay with the handle)
-  if (T.n) CUDA_TRY(cudaMemset(T.n, 0, sizeof(unsigned int)));
+  if (capacity == 0) {
+    T.rec = nullptr;  // off; the records taken so far stay readable
+  } else {
+    T.rec = h->trace_rec;
+    CUDA_TRY(cudaMemset(T.n, 0, sizeof(unsigned int)));
+  }
   CUDA_TRY(cudaMemcpy(h->ddom, &h->hdom, sizeof(DevDomain), cudaMemcpyHostToDevice));
   for (auto& ge : h->step_graph)  // the graphs carry the domain by value
     if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
@@ -1575,13 +1612,14 @@ int fdmap_gpu_trace_read(fdmap_gpu* h, unsigned long long* records, int max) {
   if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
   const TraceBuf& T = h->hdom.trace;
   if (!T.n) return 0;
+  const unsigned long long* rec = h->trace_rec;
   CUDA_TRY(cudaSetDevice(h->device));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   unsigned int n = 0;
   CUDA_TRY(cudaMemcpy(&n, T.n, sizeof(n), cudaMemcpyDeviceToHost));
   n = std::min<unsigned>(n, T.cap);
   const int k = std::min<int>((int)n, max);
-  if (records && k > 0) CUDA_TRY(cudaMemcpy(records, T.rec, (size_t)k * 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+  if (records && k > 0) CUDA_TRY(cudaMemcpy(records, rec, (size_t)k * 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
   return (int)n;
 }
 

@@ -2,7 +2,7 @@
 // decomposition of the handle's blocks, the TMA tensor maps whose boxes
 // follow the shape, the launch configuration, and the launches (single
 // domain and batched instances).  Each march_s<SH>.cu instantiates it for
-// one shape, so the variants of the three shapes compile in parallel.
+// one shape, so the variants of the four shapes compile in parallel.
 #pragma once
 
 #include <cuda.h>
@@ -42,7 +42,7 @@ inline int encode_map(EncodeTiledFn enc, CUtensorMap* map, const double* base, c
   return FDMAP_OK;
 }
 
-template <int MODE, int PI_, bool HET, bool EXT, int SH>
+template <int MODE, int PI_, bool HET, int EXT, int SH>
 int maps(fdmap_gpu* h) {
   using L = MarchLayout<MODE, PI_, HET, EXT, SH>;
   void* fn = nullptr;
@@ -66,7 +66,9 @@ int maps(fdmap_gpu* h) {
     if ((rc = encode_map(enc, &h->tmaps->MH[b], h->met_base[b], g, 5, L::WH, L::MR, 2))) return rc;
     if ((rc = encode_map(enc, &h->tmaps->MC[b], h->met_base[b], g, 5, L::MW, L::MR, 3))) return rc;
     if (HET && (rc = encode_map(enc, &h->tmaps->HT[b], h->het_base[b], g, 5, L::MW, L::MR, L::NH))) return rc;
-    if (EXT && B.J && B.Cdiss > 0.0 && (rc = encode_map(enc, &h->tmaps->JH[b], B.J, g, 1, L::WH, L::MR, 1))) return rc;
+    if (EXT == MARCH_DISS && B.J && B.Cdiss > 0.0 &&
+        (rc = encode_map(enc, &h->tmaps->JH[b], B.J, g, 1, L::WH, L::MR, 1)))
+      return rc;
   }
   return FDMAP_OK;
 }
@@ -74,7 +76,7 @@ int maps(fdmap_gpu* h) {
 // FDMAP_ERR_UNSUPPORTED when the shape cannot serve the variant (its rings do
 // not fit in shared memory, or a row group is thinner than the stencil's
 // half-width, so rows j +- PI would lie outside the three resident groups)
-template <int MODE, int PI_, bool HET, bool EXT, int SH>
+template <int MODE, int PI_, bool HET, int EXT, int SH>
 int configure(fdmap_gpu* h) {
   using L = MarchLayout<MODE, PI_, HET, EXT, SH>;
   if (PI_ > L::MR) return set_err(FDMAP_ERR_UNSUPPORTED, "row groups thinner than the stencil");
@@ -102,7 +104,7 @@ int configure(fdmap_gpu* h) {
   return FDMAP_OK;
 }
 
-template <int MODE, int PI_, bool HET, bool EXT, int SH>
+template <int MODE, int PI_, bool HET, int EXT, int SH>
 int launch(fdmap_gpu* h, const StageArgs& a) {
   using L = MarchLayout<MODE, PI_, HET, EXT, SH>;
   MarchPlan plan{h->march_grid, h->march_units, nullptr, nullptr, 1};
@@ -111,7 +113,7 @@ int launch(fdmap_gpu* h, const StageArgs& a) {
   return FDMAP_OK;
 }
 
-template <int MODE, int PI_, bool HET, bool EXT, int SH>
+template <int MODE, int PI_, bool HET, int EXT, int SH>
 int launch_batch(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s) {
   using L = MarchLayout<MODE, PI_, HET, EXT, SH>;
   MarchPlan plan{p.march_grid, p.units, p.tmaps, p.unit_begin, p.ninst};
@@ -132,7 +134,9 @@ int dispatch(const fdmap_gpu* h, Fn&& fn) {
     return set_err(FDMAP_ERR_UNSUPPORTED, "row groups thinner than the stencil");
   };
   auto with_ext = [&](auto mode_c, auto het_c) -> int {
-    return h->march_ext ? with_pi(mode_c, het_c, std::true_type{}) : with_pi(mode_c, het_c, std::false_type{});
+    if (h->march_ext == MARCH_DISS) return with_pi(mode_c, het_c, std::integral_constant<int, MARCH_DISS>{});
+    if (h->march_ext == MARCH_PML) return with_pi(mode_c, het_c, std::integral_constant<int, MARCH_PML>{});
+    return with_pi(mode_c, het_c, std::integral_constant<int, MARCH_PLAIN>{});
   };
   auto with_het = [&](auto mode_c) -> int {
     return h->het ? with_ext(mode_c, std::true_type{}) : with_ext(mode_c, std::false_type{});

@@ -51,11 +51,15 @@ __host__ __device__ constexpr int shape_ncs(int sh) { return sh == 1 ? 3 : 2; }
 __host__ __device__ constexpr int even_halo(int h) { return (h + 1) & ~1; }
 __host__ __device__ constexpr size_t align128(size_t b) { return (b + 127) / 128 * 128; }
 
-// EXT: the variant for blocks with artificial dissipation (a J plane with
-// halo columns in every neighbour slot), a perfectly matched layer, source
-// forcing, body displacement or peak motion (node-local data read and
-// written by the node's own thread).
-template <int MODE, int PI_, bool HET, bool EXT, int SH>
+// EXT: 0 the plain variant; 1 the variant for artificial dissipation (a J
+// plane with halo columns in every neighbour slot), source forcing, body
+// displacement and peak motion; 2 the variant for a perfectly matched layer
+// (with forcing and body extras).  Forcing, displacement, peak motion and the
+// PML's auxiliary fields are node-local: read and written by the node's own
+// thread.
+enum { MARCH_PLAIN = 0, MARCH_DISS = 1, MARCH_PML = 2 };
+
+template <int MODE, int PI_, bool HET, int EXT, int SH>
 struct MarchLayout {
   static constexpr int MW = shape_mw(SH);
   static constexpr int MR = shape_mr(SH);
@@ -71,7 +75,7 @@ struct MarchLayout {
   static constexpr size_t MH_OFF = align128(F_OFF + (size_t)NR * MR * WH * 8);
   static constexpr size_t MC_OFF = align128(MH_OFF + (size_t)2 * MR * WH * 8);
   static constexpr size_t J_OFF = align128(MC_OFF + (size_t)3 * MR * MW * 8);
-  static constexpr size_t GSLOT = align128(J_OFF + (EXT ? (size_t)MR * WH * 8 : 0));
+  static constexpr size_t GSLOT = align128(J_OFF + (EXT == MARCH_DISS ? (size_t)MR * WH * 8 : 0));
   // centre group slot: DF [NR][MR][MW], szz [1][MR][MW] (mode II), material [NH][MR][MW]
   static constexpr size_t DF_OFF = 0;
   static constexpr size_t F6_OFF = align128(DF_OFF + (size_t)NR * MR * MW * 8);
@@ -219,12 +223,12 @@ __device__ __forceinline__ UnitPos unit_pos(const DevDomain& D, long long u) {
 // edge and closure kernels of the same stage run concurrently with the
 // interior march.  The SBP6 mode II variant and the extras variant of a
 // 256-thread shape take more to avoid spills.
-template <int MODE, int PI_, bool EXT, int SH>
+template <int MODE, int PI_, int EXT, int SH>
 constexpr int march_regs() {
   return ((MODE == 2 && PI_ == 3) || (EXT && shape_mw(SH) * shape_mr(SH) <= 256)) ? 128 : 96;
 }
 
-template <int MODE, int PI_, bool HET, bool EXT, int SH>
+template <int MODE, int PI_, bool HET, int EXT, int SH>
 __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
     march_kernel(const DevDomain* __restrict__ doms, StageArgs a, MarchPlan plan, const __grid_constant__ TmapSet tm) {
   using L = MarchLayout<MODE, PI_, HET, EXT, SH>;
@@ -286,7 +290,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
     const CUtensorMap* mF = &tmi.F[b][a.in];
     const CUtensorMap* mF6 = &tmi.F6[b][a.in];
     // artificial dissipation of this block: J with halo columns in the neighbour ring
-    const bool diss = EXT && B.Cdiss > 0.0;
+    const bool diss = EXT == MARCH_DISS && B.Cdiss > 0.0;
     const unsigned nbytes = L::NB_BYTES + (diss ? L::J_BYTES : 0u);
 
     if (tid == 0) {
@@ -337,7 +341,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
     // body forces of this block (point source / gravity; with EXT also the
     // long-wave forcing and forcing from file), evaluated once per segment
     const bool forces = D.src.use_gravity || (D.src.use_singular && B.src_ok) ||
-                        (EXT && (D.src.use_singular || B.gforce || B.frc_new));
+                        (EXT != MARCH_PLAIN && (D.src.use_singular || B.gforce || B.frc_new));
     const double t_stage = forces ? stage_time(a) : 0.0;
     const int i = i0 + cx;
     int aborted_at = -1;
@@ -391,7 +395,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
         }
         m.rinv = HET ? 1.0 / m.rho : 0.0;
         bool pml = false;
-        if constexpr (EXT && MODE == 2) {
+        if constexpr (EXT == MARCH_PML && MODE == 2) {
           if (B.pml) {
             // Cartesian PML rates of the interior region (rates.f90:2089-2126)
             // from the ring; szz at the neighbours through the cache
@@ -403,7 +407,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
             pml = true;
           }
         }
-        if (!pml) {
+        if (!pml && !diss) {
           const double* hy = nrow(0, L::MH_OFF, 0, WH) + cx + HP;  // yr, centred on the node
           const double* hx = nrow(0, L::MH_OFF, 1, WH) + cx + HP;  // xr
           const double yrc = hy[0], xrc = hx[0];
@@ -438,29 +442,69 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
               acc[r] += sum * cfr * Ji;
             }
           }
-          if (EXT && diss) {
-            // artificial dissipation (rates_dissipation_interior_mode2/3,
-            // rates.f90:939-999, 1397-1482): 2*AI(0)*F + sum_s AI(s)*Ji*(J F at
-            // the four neighbours at distance s), in the tiled kernel's order
-            const double Cd = B.Cdiss;
-            const double* jr = nrow(0, L::J_OFF, 0, WH) + cx + HP;
+        }
+        if (EXT == MARCH_DISS && !pml && diss) {
+          // split-form rates and artificial dissipation together
+          // (rates_dissipation_interior_mode2/3, rates.f90:939-999,
+          // 1397-1482): the neighbour values of every field are read from the
+          // ring once per s and serve both; the dissipation sum is
+          // 2*AI(0)*F + sum_s AI(s)*Ji*(J F at the four neighbours at distance
+          // s), added after the rates, in the tiled kernel's order
+          const double Cd = B.Cdiss;
+          double dsum[NR];
+#pragma unroll
+          for (int l = 0; l < NR; ++l) dsum[l] = 2.0 * D.AI[0] * Cd * nrow(0, L::F_OFF, l, WH)[cx + HP];
+          const double* hy = nrow(0, L::MH_OFF, 0, WH) + cx + HP;
+          const double* hx = nrow(0, L::MH_OFF, 1, WH) + cx + HP;
+          const double* jr = nrow(0, L::J_OFF, 0, WH) + cx + HP;
+          const double yrc = hy[0], xrc = hx[0];
+          const double yqc = nrow(0, L::MC_OFF, 0, MW)[cx], xqc = nrow(0, L::MC_OFF, 1, MW)[cx];
+#pragma unroll
+          for (int s = 1; s <= PI_; ++s) {
+            const double Yrp = 0.5 * (hy[s] + yrc), Xrp = 0.5 * (hx[s] + xrc);
+            const double Yrm = 0.5 * (hy[-s] + yrc), Xrm = 0.5 * (hx[-s] + xrc);
+            const double Yqp = 0.5 * (nrow(s, L::MC_OFF, 0, MW)[cx] + yqc), Xqp = 0.5 * (nrow(s, L::MC_OFF, 1, MW)[cx] + xqc);
+            const double Yqm = 0.5 * (nrow(-s, L::MC_OFF, 0, MW)[cx] + yqc), Xqm = 0.5 * (nrow(-s, L::MC_OFF, 1, MW)[cx] + xqc);
+            double fqp[NR], fqm[NR], frp[NR], frm[NR];
 #pragma unroll
             for (int l = 0; l < NR; ++l) {
               const double* fr = nrow(0, L::F_OFF, l, WH) + cx + HP;
-              double sum = 2.0 * D.AI[0] * Cd * fr[0];
-#pragma unroll
-              for (int s = 1; s <= PI_; ++s)
-                sum += D.AI[s] * Cd * Ji *
-                       (jr[s] * fr[s] + jr[-s] * fr[-s] +
-                        nrow(s, L::J_OFF, 0, WH)[cx + HP] * nrow(s, L::F_OFF, l, WH)[cx + HP] +
-                        nrow(-s, L::J_OFF, 0, WH)[cx + HP] * nrow(-s, L::F_OFF, l, WH)[cx + HP]);
-              acc[l] += sum;
+              fqp[l] = fr[s];
+              fqm[l] = fr[-s];
+              frp[l] = nrow(s, L::F_OFF, l, WH)[cx + HP];
+              frm[l] = nrow(-s, L::F_OFF, l, WH)[cx + HP];
             }
+            const double w = HET ? D.DI[s] : 0.0;
+#pragma unroll
+            for (int r = 0; r < NR; ++r) {
+              double sum = 0.0;
+              if (RD::fa(r) >= 0) {
+                const int f = RD::fa(r);
+                double t = Yrp * fqp[f] - Yrm * fqm[f] - Yqp * frp[f] + Yqm * frm[f];
+                if (RD::ga(r)) t *= m.gamma;
+                sum += t;
+              }
+              if (RD::fb(r) >= 0) {
+                const int f = RD::fb(r);
+                double t = -Xrp * fqp[f] + Xrm * fqm[f] + Xqp * frp[f] - Xqm * frm[f];
+                if (RD::gb(r)) t *= m.gamma;
+                sum += t;
+              }
+              const double cfr = HET ? mat_coef(m, RD::coef(r), w) : cf[s][RD::coef(r)];
+              acc[r] += sum * cfr * Ji;
+            }
+            const double jqp = jr[s], jqm = jr[-s];
+            const double jrp = nrow(s, L::J_OFF, 0, WH)[cx + HP], jrm = nrow(-s, L::J_OFF, 0, WH)[cx + HP];
+#pragma unroll
+            for (int l = 0; l < NR; ++l)
+              dsum[l] += D.AI[s] * Cd * Ji * (jqp * fqp[l] + jqm * fqm[l] + jrp * frp[l] + jrm * frm[l]);
           }
+#pragma unroll
+          for (int l = 0; l < NR; ++l) acc[l] += dsum[l];
         }
         if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
         if (forces) body_forces<MODE>(D, B, i, j, t_stage, a, acc);
-        if (EXT) body_extras<MODE>(B, c, Fc, acc, a);
+        if (EXT != MARCH_PLAIN) body_extras<MODE>(B, c, Fc, acc, a);
 #pragma unroll
         for (int l = 0; l < NF; ++l) DFp[l * plane + c] = acc[l];
         if (a.update) {

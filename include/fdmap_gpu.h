@@ -267,7 +267,8 @@ int fdmap_gpu_group_run(fdmap_gpu* const* hs, int n, double t_start, double dt, 
  * (interior march, closure, interface) appends one record of three words --
  * kind (1 march, 2 closure, 3 interface) | SM << 8 | CTA << 16, start and end
  * in ns of the device's global timer -- until `capacity` records are taken;
- * 0 switches it off.  Enabling clears the records.  fdmap_gpu_trace_read
+ * 0 switches it off and keeps the records taken.  Enabling clears them.
+ * fdmap_gpu_trace_read
  * copies up to `max` records and returns how many were taken.  No reference
  * counterpart (the reference times whole steps, main.f90:202-253). */
 int fdmap_gpu_trace(fdmap_gpu* h, int capacity);
