@@ -277,13 +277,18 @@ def run_gpu(args) -> None:
 
     lib().fdmap_gpu_profile(g._g, 1)
     g.run(args.warmup + args.steps + 1, args.warmup + 2 * args.steps, nt=nt_inf)
-    kms = (C.c_double * 3)()
-    kn = (C.c_longlong * 3)()
-    lib().fdmap_gpu_profile_read(g._g, kms, kn)
+    kms = (C.c_double * 5)()
+    kn = (C.c_longlong * 5)()
+    lib().fdmap_gpu_profile_read_kinds(g._g, 5, kms, kn)
     lib().fdmap_gpu_profile(g._g, 0)
     stencil_ms = kms[0] / max(kn[0], 1)
     closure_ms = kms[1] / max(kn[1], 1)
     edge_ms = kms[2] / max(kn[2], 1)
+    pair_ms = kms[3] / max(kn[3], 1)
+    band_ms = kms[4] / max(kn[4], 1)
+    prof_kinds = {k: {"launches": int(kn[i]), "mean_ms": kms[i] / max(kn[i], 1)}
+                  for i, k in enumerate(("march", "closure", "interface", "pair_march", "band")) if kn[i]}
+    pairs = bool(g.pairs)
     nst = RK_STAGES[host.rk_order]
     bps = BYTES_PER_NODE_STAGE[(host.mode, het)]
     n_int = interior_nodes(host)
@@ -383,6 +388,8 @@ def run_gpu(args) -> None:
                                         "frac_without_metric_reads": survey_bytes / step_bytes * step_gbs
                                         / peaks["hbm_gbs"]}},
             "march_tile": tile_info,
+            "two_stage_passes": pairs,
+            "kernels_serialised": prof_kinds,
             "clocks": ck,
             "gpu_launches": launches,
             "newton_failures": newton_fail,

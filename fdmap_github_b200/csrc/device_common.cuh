@@ -40,8 +40,10 @@ struct DevSide {
 struct DevBlock {
   int nx, ny, pitch;
   long long plane;
-  double* F[2];
+  double* F[3];                        // F[0], F[1] ping-pong; F[2] the first stage's values near the
+                                       // block edges in a two-stage pass (NULL when pairs are off)
   double* DF;
+  double* DFalt;                       // second rate buffer of two-stage passes (NULL when pairs are off)
   double *xq, *xr, *yq, *yr, *Ji;      // (pitch, ny)
   double *rho, *G, *M, *gamma, *nu;    // heterogeneous only
   double rho_b, G_b, M_b, gamma_b, nu_b;
@@ -68,6 +70,7 @@ struct DevBlock {
   int tile_begin;                      // first stencil tile of this block
   int tiles_x;
   long long march_unit_begin;          // first row-group unit of this block (march kernel)
+  long long pair_unit_begin;           // first row-group unit of this block (two-stage march)
 };
 
 // per-interface friction storage: st[f*n + k] for the 18 FDMAP_FAULT_* fields,
@@ -112,9 +115,18 @@ struct DevIface {
 constexpr int PADL = 32;
 constexpr int PADTAIL = 192;
 
+// Register cap of the boundary kernels (interface solves, closure strips).
+// They run on a side stream beside a resident interior kernel, and a warp
+// takes its registers from one of the SM's four sub-partitions (16K
+// registers each), not from the SM as a whole: beside a march CTA of 512
+// threads at 96 registers (12K per sub-partition) only a warp of at most 128
+// registers a thread fits.  Uncapped (166 and 196 registers) they waited for
+// the interior kernel to finish.
+constexpr int BOUNDARY_REGS = 128;
+
 // Timeline of the stage kernels (fdmap_gpu_trace): one record of three words
 // per CTA, (kind | SM << 8 | CTA << 16, start ns, end ns) on %globaltimer
-enum { TRACE_MARCH = 1, TRACE_CLOSURE = 2, TRACE_EDGE = 3, TRACE_TILED = 4 };
+enum { TRACE_MARCH = 1, TRACE_CLOSURE = 2, TRACE_EDGE = 3, TRACE_TILED = 4, TRACE_PAIR = 5, TRACE_BAND = 6 };
 struct TraceBuf {
   unsigned long long* rec;  // NULL: tracing off
   unsigned int* n;
@@ -133,6 +145,9 @@ struct DevDomain {
   DevIface ifc[MAX_IFACES];
   // closure strips of every block (bottom, top, left, right): thread offsets
   long long cstart[4 * MAX_BLOCKS + 1];
+  // edge bands of width nbw = nbst + pI (second stage of a two-stage pass), same order
+  long long bstart[4 * MAX_BLOCKS + 1];
+  int nbw;
   // interface work segments (one thread per interface node)
   int nseg;
   int seg_kind[4 * MAX_BLOCKS + MAX_IFACES];   // 0 = BC side, 1 = interface
@@ -189,6 +204,7 @@ struct StageArgs {
   int tap;       // stage 1 with outputs open: interface kernels write their output snapshot
   double t0, dt; // step start and length (when ts == nullptr)
   int first;     // stage 1 (update_fields_peak)
+  int dfr, dfw;  // rate buffer read (scaled by A) and written: 0 DF, 1 DFalt (two-stage passes)
 };
 
 // Stage time t0 + C*dt with t0 = t_start + (n-1)*dt, rounded exactly as the

@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(128) pack_edges(const __grid_constant__ DevDom
 // One thread per interface node: the locked / frictional solve of this stage,
 // hat variables of both sides, and the fault register life cycle.
 template <int MODE>
-__global__ void __launch_bounds__(64) edge_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
+__global__ void __maxnreg__(BOUNDARY_REGS) edge_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
   const unsigned long long t_in = (threadIdx.x == 0 && D.trace.rec) ? globaltimer_ns() : 0ull;
   int tid = blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.seg_start[D.nseg]) return;
@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(64) edge_kernel(const __grid_constant__ DevDom
 
 // Interface nodes of a batch of independent instances in one launch.
 template <int MODE>
-__global__ void __launch_bounds__(128)
+__global__ void __maxnreg__(BOUNDARY_REGS)
     edge_kernel_batch(const DevDomain* __restrict__ doms, const int* __restrict__ cta_begin, int ninst, StageArgs a) {
   const int k = batch_instance(cta_begin, ninst, blockIdx.x);
   const DevDomain& D = doms[k];

@@ -32,9 +32,11 @@ struct BlockGeom {
 };
 
 struct OutputState;  // device-side output (output.cu)
+struct TmapPair;     // tensor maps of the two-stage march (march_pair.cuh)
 void output_destroy(fdmap_gpu* h);
 
 __global__ void advance_step(TimeState* ts);
+void pair_free(fdmap_gpu* h);  // releases the two-stage march's host-side maps (march_pair.cu)
 __global__ void set_step_clock(TimeState* ts, double t_start, double dt, long long n);
 
 }  // namespace fdmap
@@ -75,6 +77,15 @@ struct fdmap_gpu {
   double tp[5] = {0, 0, 0, 0, 0};  // t0, dt, CFL, hmin, hmax (set_dt)
   int tp_nt = 0;
   int fused = 0;  // boundary kernel handles interface solves and closure strips in one launch
+  // two-stage passes (march_pair.cuh): stages 2k+1, 2k+2 of a step in one
+  // interior pass; available for homogeneous plain domains (pair_ok), used
+  // when also enabled (use_pairs)
+  bool pair_ok = false;
+  bool use_pairs = false;
+  TmapPair* tmaps_pair = nullptr;
+  long long pair_units = 0;
+  int pair_grid = 0;
+  long long band_threads = 0;
   // CUDA graphs of one full step, one per starting F buffer, replayed by fdmap_gpu_run
   TimeState* d_time = nullptr;
   cudaGraphExec_t step_graph[2] = {nullptr, nullptr};
@@ -113,8 +124,9 @@ struct fdmap_gpu {
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;  // kind, (start, stop)
-  double prof_ms[3] = {0, 0, 0};
-  long long prof_n[3] = {0, 0, 0};
+  // kinds: 0 interior march, 1 closure strips, 2 interface solves, 3 two-stage march, 4 band
+  double prof_ms[5] = {0, 0, 0, 0, 0};
+  long long prof_n[5] = {0, 0, 0, 0, 0};
 
   template <typename T>
   int alloc(T** p, size_t count) {
@@ -187,6 +199,7 @@ struct fdmap_gpu {
     if (ev_packed) cudaEventDestroy(ev_packed);
     output_destroy(this);
     delete tmaps;
+    pair_free(this);
     for (auto& ge : step_graph)
       if (ge) cudaGraphExecDestroy(ge);
   }
@@ -246,6 +259,17 @@ int march_batch_s2(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& 
 int march_batch_s3(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, cudaStream_t s);
 // configure for `shape` and publish the domain (device copy, step graphs dropped)
 int march_set_shape(fdmap_gpu* h, int shape);
+
+// Two-stage passes (march_pair.cu).  pair_configure checks whether the
+// handle's domain can use them (homogeneous material, plain split form, SBP2
+// or SBP4, blocks wider than two bands), allocates the scratch field buffer
+// F[2] and the second rate buffer, builds the band table and the tensor maps,
+// and sets h->pair_ok; it leaves the handle unchanged when the domain does
+// not qualify.  pair_launch issues the interior pass of stages a0, a1;
+// band_launch the band kernel of the second stage.
+int pair_configure(fdmap_gpu* h);
+int pair_launch(fdmap_gpu* h, const StageArgs& a0, const StageArgs& a1, int dfr, int dfw);
+int band_launch(fdmap_gpu* h, const StageArgs& a);
 
 // Copy of every device allocation of a handle (its whole state), to put the
 // state back after timing runs; `out` receives the copies (freed by restore).

@@ -271,8 +271,8 @@ int batch_edges(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p, 
 
 namespace {
 
-// 64-thread closure CTAs: at about 170 registers a thread, two warps fit in
-// the registers a 512-thread march CTA leaves free on its SM
+// 64-thread closure CTAs (two warps, capped at BOUNDARY_REGS registers a
+// thread) fit beside a resident march CTA
 constexpr int CLOSURE_TPB = 64;
 
 template <int MODE>
@@ -917,6 +917,11 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
     CUDA_TRY(cudaMemcpy(h->d_energy, big.data(), big.size() * sizeof(double), cudaMemcpyHostToDevice));
     D.energy = h->d_energy;
   }
+  // two-stage passes where the domain allows them (FDMAP_PAIRS=0 keeps stage by stage)
+  if (h->rk.A[0] == 0.0) {
+    const char* ep = getenv("FDMAP_PAIRS");
+    if (!(ep && std::string(ep) == "0") && (rc = pair_configure(h))) return rc;
+  }
   if ((rc = h->alloc(&h->ddom, 1))) return rc;
   CUDA_TRY(cudaMemcpy(h->ddom, &D, sizeof(DevDomain), cudaMemcpyHostToDevice));
 
@@ -934,13 +939,70 @@ int build(fdmap_gpu* h, const fdmap_desc* d) {
   return fdmap_gpu_set_fields(h, d->F, d->DF);
 }
 
+// Two consecutive stages a0, a1 (F[a0.in] -> F[a1.out]) as one interior pass
+// (march_pair.cuh).  Beside the pass, on the side stream: the interface solve
+// and closure strips of the first stage (writing the scratch buffer F[2]),
+// then the interface solve of the second stage from F[2]; after both, the
+// band kernel does the second stage near the block edges.  Rates go from
+// buffer dfr to buffer dfw.  `gather`: a0 is stage 1 with outputs open; the
+// output gather runs between the first stage's closure strips and the second
+// stage's interface solve, while the hat variables are still stage 1's (the
+// body fields it samples, F[a0.in], are not written by the pair).
+int launch_pair(fdmap_gpu* h, const StageArgs& a0, const StageArgs& a1, int dfr, int dfw, bool gather,
+                long long n) {
+  StageArgs c0 = a0;  // first stage at the closure strips: into the scratch buffer
+  c0.out = 2;
+  c0.dfr = dfr;
+  c0.dfw = dfw;
+  StageArgs e1 = a1;  // second stage's interface solve and band: from the scratch buffer
+  e1.in = 2;
+  e1.dfr = dfw;
+  e1.dfw = dfw;
+  const bool ov = h->overlap && !h->profiling;
+  if (ov) {
+    CUDA_TRY(cudaEventRecord(h->ev_fork, h->stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+  }
+  {
+    ProfScope ps(h, 3);
+    int rc = pair_launch(h, a0, a1, dfr, dfw);
+    if (rc) return rc;
+    h->launches++;
+  }
+  cudaStream_t main_stream = h->stream;
+  if (ov) h->stream = h->side_stream;
+  int rc = launch_boundary(h, c0);
+  if (rc == FDMAP_OK && gather) rc = output_gather(h, a0.ts, n, a0.in);
+  if (rc == FDMAP_OK) rc = launch_edges(h, e1);
+  h->stream = main_stream;
+  if (rc) return rc;
+  if (ov) {
+    CUDA_TRY(cudaEventRecord(h->ev_join, h->side_stream));
+    CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+  }
+  ProfScope pb(h, 4);
+  if ((rc = band_launch(h, e1))) return rc;
+  h->launches++;
+  return FDMAP_OK;
+}
+
+// F buffer swaps of one (non-final) step: one per stage, or one per pass
+// when stages run in two-stage passes
+int step_swaps(const fdmap_gpu* h) {
+  return h->use_pairs ? h->rk.nstage / 2 + (h->rk.nstage & 1) : h->rk.nstage;
+}
+
 // all stages of one step starting from buffer `cur`; final = stage 1 only.
 // With outputs open, stage 1 taps the interface state and the output gather
-// follows it (step index from the device clock `ts`, else `n`).
+// follows it (step index from the device clock `ts`, else `n`).  With
+// two-stage passes, stages (1,2), (3,4), ... run as pairs and an odd last
+// stage alone; the pairs' rate buffers alternate so that the last pair
+// writes DF and the step ends with its rates in DF, as stage by stage.
 int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, const TimeState* ts, long long n = 0) {
   const bool outputs = output_is_open(h);
   const int cur0 = cur;
-  for (int s = 0; s < h->rk.nstage; ++s) {
+  const int npairs = (h->use_pairs && !final_step) ? h->rk.nstage / 2 : 0;
+  auto args = [&](int s, int in) {
     StageArgs a{};
     a.tap = (s == 0 && outputs) ? 1 : 0;
     a.A = h->rk.A[s];
@@ -951,14 +1013,28 @@ int issue_step(fdmap_gpu* h, int cur, double t0, double dt, bool final_step, con
     a.dt = dt;
     a.first = s == 0 ? 1 : 0;
     a.ts = ts;
-    a.in = cur;
-    a.out = 1 - cur;
+    a.in = in;
+    a.out = 1 - in;
     a.scale = 1;
     a.update = final_step ? 0 : 1;
-    int rc = launch_stage(h, a);
-    if (rc) return rc;
-    if (s == 0 && h->d_energy && (rc = launch_energy(h, cur0))) return rc;
-    if (s == 0 && outputs && (rc = output_gather(h, ts, n, cur0))) return rc;
+    return a;
+  };
+  for (int s = 0; s < h->rk.nstage; ++s) {
+    int rc;
+    const StageArgs a = args(s, cur);
+    if (s < 2 * npairs) {
+      const int p = s / 2;
+      const int dfw = ((npairs - 1 - p) & 1) ? 1 : 0;
+      const int dfr = p == 0 ? 0 : 1 - dfw;  // the first pair reads no rates (A(1) = 0)
+      StageArgs a1 = args(s + 1, cur);
+      a1.out = 1 - cur;
+      if ((rc = launch_pair(h, a, a1, dfr, dfw, a.first && outputs, n))) return rc;
+      ++s;
+    } else {
+      if ((rc = launch_stage(h, a))) return rc;
+      if (a.first && h->d_energy && (rc = launch_energy(h, cur0))) return rc;
+      if (a.first && outputs && (rc = output_gather(h, ts, n, cur0))) return rc;
+    }
     if (final_step) return FDMAP_OK;
     cur = 1 - cur;
   }
@@ -1238,7 +1314,7 @@ int fdmap_gpu_time_step(fdmap_gpu* h, double t0, double dt, int final_step) {
   rc = issue_step(h, h->cur, t0, dt, final_step != 0, nullptr, h->out_next_n);
   if (rc) return rc;
   h->out_next_n += 1;
-  if (!final_step && (h->rk.nstage & 1)) h->cur = 1 - h->cur;
+  if (!final_step && (step_swaps(h) & 1)) h->cur = 1 - h->cur;
   return FDMAP_OK;
 }
 
@@ -1261,7 +1337,7 @@ int fdmap_gpu_run(fdmap_gpu* h, double t_start, double dt, int n_first, int n_la
       if ((rc = forcing_load(h))) return rc;
       CUDA_TRY(cudaGraphLaunch(h->step_graph[h->cur], h->stream));
       h->launches += h->graph_launches;
-      if (h->rk.nstage & 1) h->cur = 1 - h->cur;
+      if (step_swaps(h) & 1) h->cur = 1 - h->cur;
     }
     n_first = n_graph_last + 1;
   }
@@ -1750,8 +1826,38 @@ int fdmap_gpu_profile(fdmap_gpu* h, int enable) {
   CUDA_TRY(cudaSetDevice(h->device));
   h->drain_events();
   h->profiling = enable != 0;
-  for (int k = 0; k < 3; ++k) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
+  for (int k = 0; k < 5; ++k) { h->prof_ms[k] = 0.0; h->prof_n[k] = 0; }
   return FDMAP_OK;
+}
+
+int fdmap_gpu_profile_read_kinds(fdmap_gpu* h, int n, double* ms, long long* count) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  if (n < 0 || n > 5) return set_err(FDMAP_ERR_INVALID_ARG, "at most 5 kernel kinds");
+  CUDA_TRY(cudaSetDevice(h->device));
+  h->drain_events();
+  for (int k = 0; k < n; ++k) {
+    if (ms) ms[k] = h->prof_ms[k];
+    if (count) count[k] = h->prof_n[k];
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_set_pairs(fdmap_gpu* h, int enable) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  if (enable && !h->pair_ok) return set_err(FDMAP_ERR_UNSUPPORTED, "the domain cannot run two-stage passes");
+  CUDA_TRY(cudaSetDevice(h->device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (h->use_pairs != (enable != 0)) {
+    h->use_pairs = enable != 0;
+    for (auto& ge : h->step_graph)
+      if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_get_pairs(fdmap_gpu* h) {
+  if (!h) return set_err(FDMAP_ERR_INVALID_ARG, "null handle");
+  return h->use_pairs ? 1 : 0;
 }
 
 int fdmap_gpu_profile_read(fdmap_gpu* h, double* ms, long long* count) {

@@ -29,6 +29,8 @@
 
 #include <cuda.h>
 
+#include <type_traits>
+
 #include "stencil_kernel.cuh"
 
 namespace fdmap {
@@ -359,16 +361,29 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
         break;
       }
       const int j = jr0 + g * MR + ry;
-      if (j < jr1 && i >= nbst && i <= nx - 1 - nbst && j >= nbst && j <= ny - 1 - nbst) {
+      // this iteration's neighbour slots, groups g-1, g, g+1 (a group outside
+      // the CTA's range gets slot 0: no node that is computed reads it)
+      const unsigned char* gq[3];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int k = g - 1 + q;
+        gq[q] = smem + (size_t)((k >= gmin ? k - gmin : 0) % NGS) * L::GSLOT;
+      }
+      const unsigned char* cslot = smem + (size_t)NGS * L::GSLOT + (size_t)(g % NCS) * L::CSLOT;
+      // the node's work with its row in the group as a compile-time constant
+      // (ry is warp-uniform), so that every ring address is a slot pointer
+      // plus a constant
+      auto node = [&](auto ryc) {
+        constexpr int RY = decltype(ryc)::value;
         const long long c = (long long)j * pitch + i;
-        // row j lives in group g, row ry; rows j +- s in group g + (ry +- s) div MR
+        // row j lives in group g, row RY; rows j +- s in group g + (RY +- s) div MR
         auto nrow = [&](int dr, size_t off, int q, int width) -> const double* {
-          int rr = ry + dr;
-          int k = g + (rr >= 0 ? rr / MR : -((MR - 1 - rr) / MR));
-          int r = rr - (k - g) * MR;
-          return reinterpret_cast<const double*>(smem + (size_t)((k - gmin) % NGS) * L::GSLOT + off) + ((size_t)q * MR + r) * width;
+          const int rr = RY + dr;
+          const int go = rr >= 0 ? rr / MR : -((MR - 1 - rr) / MR);
+          const int r = rr - go * MR;
+          return reinterpret_cast<const double*>(gq[1 + go] + off) + ((size_t)q * MR + r) * width;
         };
-        const unsigned char* cslot = smem + (size_t)NGS * L::GSLOT + (size_t)(g % NCS) * L::CSLOT;
+        constexpr int ry = RY;
         double acc[NF];
         if (load_df) {
           const double* dfc = reinterpret_cast<const double*>(cslot + L::DF_OFF) + (size_t)ry * MW + cx;
@@ -408,40 +423,12 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
           }
         }
         if (!pml && !diss) {
-          const double* hy = nrow(0, L::MH_OFF, 0, WH) + cx + HP;  // yr, centred on the node
-          const double* hx = nrow(0, L::MH_OFF, 1, WH) + cx + HP;  // xr
-          const double yrc = hy[0], xrc = hx[0];
-          const double yqc = nrow(0, L::MC_OFF, 0, MW)[cx], xqc = nrow(0, L::MC_OFF, 1, MW)[cx];
-#pragma unroll
-          for (int s = 1; s <= PI_; ++s) {
-            const double Yrp = 0.5 * (hy[s] + yrc), Xrp = 0.5 * (hx[s] + xrc);
-            const double Yrm = 0.5 * (hy[-s] + yrc), Xrm = 0.5 * (hx[-s] + xrc);
-            const double Yqp = 0.5 * (nrow(s, L::MC_OFF, 0, MW)[cx] + yqc), Xqp = 0.5 * (nrow(s, L::MC_OFF, 1, MW)[cx] + xqc);
-            const double Yqm = 0.5 * (nrow(-s, L::MC_OFF, 0, MW)[cx] + yqc), Xqm = 0.5 * (nrow(-s, L::MC_OFF, 1, MW)[cx] + xqc);
-            const double w = HET ? D.DI[s] : 0.0;
-#pragma unroll
-            for (int r = 0; r < NR; ++r) {
-              double sum = 0.0;
-              if (RD::fa(r) >= 0) {
-                const int f = RD::fa(r);
-                const double* fr = nrow(0, L::F_OFF, f, WH) + cx + HP;
-                double t = Yrp * fr[s] - Yrm * fr[-s] - Yqp * nrow(s, L::F_OFF, f, WH)[cx + HP] +
-                           Yqm * nrow(-s, L::F_OFF, f, WH)[cx + HP];
-                if (RD::ga(r)) t *= m.gamma;
-                sum += t;
-              }
-              if (RD::fb(r) >= 0) {
-                const int f = RD::fb(r);
-                const double* fr = nrow(0, L::F_OFF, f, WH) + cx + HP;
-                double t = -Xrp * fr[s] + Xrm * fr[-s] + Xqp * nrow(s, L::F_OFF, f, WH)[cx + HP] -
-                           Xqm * nrow(-s, L::F_OFF, f, WH)[cx + HP];
-                if (RD::gb(r)) t *= m.gamma;
-                sum += t;
-              }
-              const double cfr = HET ? mat_coef(m, RD::coef(r), w) : cf[s][RD::coef(r)];
-              acc[r] += sum * cfr * Ji;
-            }
-          }
+          split_rates<MODE, PI_, HET>(
+              acc, m, cf, D.DI, Ji,
+              [&](int l, int s) { return nrow(0, L::F_OFF, l, WH)[cx + HP + s]; },
+              [&](int l, int s) { return nrow(s, L::F_OFF, l, WH)[cx + HP]; },
+              [&](int k, int s) { return nrow(0, L::MH_OFF, k, WH)[cx + HP + s]; },
+              [&](int k, int s) { return nrow(s, L::MC_OFF, k, MW)[cx]; });
         }
         if (EXT == MARCH_DISS && !pml && diss) {
           // split-form rates and artificial dissipation together
@@ -510,6 +497,18 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
         if (a.update) {
 #pragma unroll
           for (int l = 0; l < NF; ++l) Fout[l * plane + c] = Fc[l] + a.Bdt * acc[l];
+        }
+      };
+      if (j < jr1 && i >= nbst && i <= nx - 1 - nbst && j >= nbst && j <= ny - 1 - nbst) {
+        if constexpr (MR == 2) {
+          if (ry == 0) node(std::integral_constant<int, 0>{});
+          else node(std::integral_constant<int, 1>{});
+        } else {
+          static_assert(MR == 4, "row groups of 2 or 4 rows");
+          if (ry == 0) node(std::integral_constant<int, 0>{});
+          else if (ry == 1) node(std::integral_constant<int, 1>{});
+          else if (ry == 2) node(std::integral_constant<int, 2>{});
+          else node(std::integral_constant<int, 3>{});
         }
       }
       __syncthreads();

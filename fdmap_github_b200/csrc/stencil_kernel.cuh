@@ -49,6 +49,49 @@ __device__ __forceinline__ double mat_coef(const NodeMat& m, int kind, double w)
   return kind == 0 ? w * m.rinv : (kind == 1 ? w * m.G : w * m.M);
 }
 
+// Split-form rates of one interior node (rates_interior_mode2/3,
+// rates.f90:8-56, 384-450; heterogeneous media rates_heterogeneous.f90), added
+// to acc.  Every interior kernel that reads its neighbourhood from a
+// shared-memory ring or from global memory calls this one routine, so the
+// same inputs give the same bits whichever kernel computes the node.
+// Accessors (s = +-1 .. +-PI, 0 the node itself):
+//   fq(l, s) field l at column offset s,   fr(l, s) field l at row offset s;
+//   mq(0, s) yr, mq(1, s) xr at column offset s;
+//   mr(0, s) yq, mr(1, s) xq at row offset s.
+template <int MODE, int PI_, bool HET, class FQ, class FR, class MQ, class MRr>
+__device__ __forceinline__ void split_rates(double* acc, const NodeMat& m, const double (&cf)[PI_ + 1][3],
+                                            const double* DI, double Ji, FQ&& fq, FR&& fr, MQ&& mq, MRr&& mr) {
+  using RD = RDef<MODE>;
+  const double yrc = mq(0, 0), xrc = mq(1, 0);
+  const double yqc = mr(0, 0), xqc = mr(1, 0);
+#pragma unroll
+  for (int s = 1; s <= PI_; ++s) {
+    const double Yrp = 0.5 * (mq(0, s) + yrc), Xrp = 0.5 * (mq(1, s) + xrc);
+    const double Yrm = 0.5 * (mq(0, -s) + yrc), Xrm = 0.5 * (mq(1, -s) + xrc);
+    const double Yqp = 0.5 * (mr(0, s) + yqc), Xqp = 0.5 * (mr(1, s) + xqc);
+    const double Yqm = 0.5 * (mr(0, -s) + yqc), Xqm = 0.5 * (mr(1, -s) + xqc);
+    const double w = HET ? DI[s] : 0.0;
+#pragma unroll
+    for (int r = 0; r < RD::NR; ++r) {
+      double sum = 0.0;
+      if (RD::fa(r) >= 0) {
+        const int f = RD::fa(r);
+        double t = Yrp * fq(f, s) - Yrm * fq(f, -s) - Yqp * fr(f, s) + Yqm * fr(f, -s);
+        if (RD::ga(r)) t *= m.gamma;
+        sum += t;
+      }
+      if (RD::fb(r) >= 0) {
+        const int f = RD::fb(r);
+        double t = -Xrp * fq(f, s) + Xrm * fq(f, -s) + Xqp * fr(f, s) - Xqm * fr(f, -s);
+        if (RD::gb(r)) t *= m.gamma;
+        sum += t;
+      }
+      const double cfr = HET ? mat_coef(m, RD::coef(r), w) : cf[s][RD::coef(r)];
+      acc[r] += sum * cfr * Ji;
+    }
+  }
+}
+
 // flux of rate r at point k: q direction +t1 - t2 (Yr, Xr), r direction -t1 + t2 (Yq, Xq);
 // r is a compile-time constant after unrolling, so the table lookups fold away
 template <int MODE>
@@ -622,10 +665,11 @@ __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock&
   const long long pitch = B.pitch, plane = B.plane;
   const long long c = (long long)j * pitch + i;
   const double* __restrict__ Fin = B.F[a.in];
+  const double* __restrict__ DFr = a.dfr ? B.DFalt : B.DF;
   double acc[NF];
   const bool load_df = a.scale && a.A != 0.0;
 #pragma unroll
-  for (int l = 0; l < NF; ++l) acc[l] = load_df ? a.A * B.DF[l * plane + c] : 0.0;
+  for (int l = 0; l < NF; ++l) acc[l] = load_df ? a.A * DFr[l * plane + c] : 0.0;
   if (MODE == 2) acc[5] = 0.0;
   double Fc[NF];
 #pragma unroll
@@ -651,8 +695,9 @@ __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock&
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
   body_forces<MODE>(D, B, i, j, stage_time(a), a, acc);
   body_extras<MODE>(B, c, Fc, acc, a);
+  double* __restrict__ DFw = a.dfw ? B.DFalt : B.DF;
 #pragma unroll
-  for (int l = 0; l < NF; ++l) B.DF[l * plane + c] = acc[l];
+  for (int l = 0; l < NF; ++l) DFw[l * plane + c] = acc[l];
   if (a.update) {
     double* __restrict__ Fout = B.F[a.out];
 #pragma unroll
@@ -686,7 +731,7 @@ __device__ __forceinline__ bool on_interface_side(const DevBlock& B, int i, int 
 
 // Boundary kernel: every node within nbst of a block edge (the SBP closure strips).
 template <int MODE, int PI_, bool HET>
-__global__ void __launch_bounds__(128) closure_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
+__global__ void __maxnreg__(BOUNDARY_REGS) closure_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
   const unsigned long long t_in = (threadIdx.x == 0 && D.trace.rec) ? globaltimer_ns() : 0ull;
   long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.cstart[4 * D.nblocks]) return;
@@ -698,7 +743,7 @@ __global__ void __launch_bounds__(128) closure_kernel(const __grid_constant__ De
 
 // Closure strips of a batch of independent instances in one launch.
 template <int MODE, int PI_, bool HET>
-__global__ void __launch_bounds__(256)
+__global__ void __maxnreg__(BOUNDARY_REGS)
     closure_kernel_batch(const DevDomain* __restrict__ doms, const int* __restrict__ cta_begin, int ninst, StageArgs a) {
   const int k = batch_instance(cta_begin, ninst, blockIdx.x);
   const DevDomain& D = doms[k];

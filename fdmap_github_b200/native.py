@@ -65,6 +65,9 @@ SIGNATURES = {
     "fdmap_gpu_set_stream": (C.c_int, [_VP, _VP]),
     "fdmap_gpu_profile": (C.c_int, [_VP, C.c_int]),
     "fdmap_gpu_profile_read": (C.c_int, [_VP, _DP, C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_profile_read_kinds": (C.c_int, [_VP, C.c_int, _DP, C.POINTER(C.c_longlong)]),
+    "fdmap_gpu_set_pairs": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_get_pairs": (C.c_int, [_VP]),
     "fdmap_gpu_get_fields": (C.c_int, [_VP, _DP, _DP]),
     "fdmap_gpu_set_fields": (C.c_int, [_VP, _DP, _DP]),
     "fdmap_gpu_get_fault": (C.c_int, [_VP, C.c_int, C.c_int, _DP]),

@@ -58,6 +58,9 @@ int fdmap_gpu_set_stream(fdmap_gpu* h, void* stream);
  * stencil kernel, [1] the boundary-closure kernel, [2] the interface kernel. */
 int fdmap_gpu_profile(fdmap_gpu* h, int enable);
 int fdmap_gpu_profile_read(fdmap_gpu* h, double* ms, long long* count);
+/* The same for up to n (<= 5) kernel kinds: [0..2] as above, [3] the
+ * two-stage interior pass, [4] the band kernel of its second stage. */
+int fdmap_gpu_profile_read_kinds(fdmap_gpu* h, int n, double* ms, long long* count);
 
 /* Body fields F(nx,ny,nF) and rates DF(nx,ny,nF) in FDMAP's global
  * column-major layout; either pointer may be NULL.  Blocks the host. */
@@ -150,6 +153,20 @@ int fdmap_gpu_get_tile(fdmap_gpu* h, int* tile, int* mw, int* mr);
  * device state is copied before and put back after, so tuning does not
  * advance the run.  Call it before opening outputs. */
 int fdmap_gpu_tune(fdmap_gpu* h, double dt, int steps, int* best_tile, double* best_ms);
+
+/* Two-stage passes (no routine of the reference: an execution schedule of
+ * time_step_LS, time_step.f90:96-165).  Stages (1,2), (3,4), ... of a step
+ * run as one interior pass over HBM each, with the boundary work of both
+ * stages beside it and the second stage near the block edges after it; the
+ * arithmetic of every node is the stage-by-stage arithmetic, so results are
+ * bit-identical either way.  Available for homogeneous blocks without
+ * dissipation, PML, forcing, displacement, peak motion or energy tracking,
+ * SBP2 or SBP4, unpartitioned, and on by default there (FDMAP_PAIRS=0 turns
+ * it off at creation).  set_pairs returns FDMAP_ERR_UNSUPPORTED when asked to
+ * enable them on a domain that cannot take them; get_pairs returns 1 (in
+ * use), 0 (not in use) or a negative error code. */
+int fdmap_gpu_set_pairs(fdmap_gpu* h, int enable);
+int fdmap_gpu_get_pairs(fdmap_gpu* h);
 
 /* Iteration limit of every Newton solve, 1..99 (the reference's parameter
  * imax = 99, friction.f90:924, is the default).  A driver or test lowers it
