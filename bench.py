@@ -80,6 +80,38 @@ def extra_bytes_per_node_stage(host) -> tuple[int, int]:
     return every, first_skip
 
 
+PI_OF = {2: 1, 4: 2, 6: 3}
+NBST_OF = {2: 1, 4: 4, 6: 6}
+
+
+def nodes_at_least(host, k: int) -> int:
+    """Nodes at distance >= k from their block's nearest edge, summed over blocks."""
+    n = 0
+    for b in range(host.nblocks):
+        mgx, pgx, mgy, pgy = host.block_limits(b)
+        nx, ny = pgx - mgx + 1, pgy - mgy + 1
+        n += max(nx - 2 * k, 0) * max(ny - 2 * k, 0)
+    return n
+
+
+def pair_bytes(host, reads_rates: bool) -> int:
+    """Algorithmic bytes of one two-stage interior pass (march_pair.cuh): at
+    every interior node (distance >= nbst from the edges) the stage input is
+    read once -- the NR rate fields, szz (mode II), the five metric planes and,
+    when the first stage's A is not 0, the NR input rates; at nodes >= nbst + PI
+    the pass writes the second stage's fields and rates (2 NF planes); nearer
+    the edges it writes the first stage's fields (nbst .. nbst + 2 PI) and
+    rates (nbst .. nbst + PI) for the band kernel."""
+    nr, nf = (5, 6) if host.mode == 2 else (3, 3)
+    nbst, pi = NBST_OF[host.fd_method], PI_OF[host.fd_method]
+    n_int = nodes_at_least(host, nbst)
+    reads = n_int * (nr + (1 if host.mode == 2 else 0) + 5 + (nr if reads_rates else 0))
+    writes = (nodes_at_least(host, nbst + pi) * 2 * nf
+              + (n_int - nodes_at_least(host, nbst + 2 * pi)) * nf
+              + (n_int - nodes_at_least(host, nbst + pi)) * nf)
+    return 8 * (reads + writes)
+
+
 def bytes_per_node_update(mode: int, het: bool, rk_order: int, host=None) -> int:
     """Algorithmic bytes of one node over one full step (all stages; DF unread in stage 1)."""
     ex, skip = extra_bytes_per_node_stage(host) if host is not None else (0, 0)
@@ -189,13 +221,13 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profiled_traffic(config_key: str):
-    """DRAM bytes per interior-kernel launch from the committed ncu summary, if any."""
-    p = ROOT / "profiles" / "march_kernel_rupture_2x1601x801.md"
-    if not p.exists():
-        return None
-    m = re.search(rf"traffic_bytes_per_launch\[{config_key}\]\s*=\s*([0-9.eE+]+)", p.read_text())
-    return float(m.group(1)) if m else None
+def profiled_traffic(config_key: str, kernel: str = "march_kernel"):
+    """DRAM bytes per launch of `kernel` from the committed ncu summaries, if any."""
+    for p in sorted((ROOT / "profiles").glob("*.md")):
+        m = re.search(rf"traffic_bytes_per_launch\[{config_key}:{kernel}\]\s*=\s*([0-9.eE+]+)", p.read_text())
+        if m:
+            return float(m.group(1))
+    return None
 
 
 def dist_setup():
@@ -288,7 +320,7 @@ def run_gpu(args) -> None:
     band_ms = kms[4] / max(kn[4], 1)
     prof_kinds = {k: {"launches": int(kn[i]), "mean_ms": kms[i] / max(kn[i], 1)}
                   for i, k in enumerate(("march", "closure", "interface", "pair_march", "band")) if kn[i]}
-    pairs = bool(g.pairs)
+    pairs = bool(g.two_stage)
     nst = RK_STAGES[host.rk_order]
     bps = BYTES_PER_NODE_STAGE[(host.mode, het)]
     n_int = interior_nodes(host)
@@ -297,11 +329,33 @@ def run_gpu(args) -> None:
     ex, skip = extra_bytes_per_node_stage(host)
     stage_bytes = [n_int * (bps + ex - ((NR_DF[host.mode] * 8 + skip) if q == 0 else 0)) for q in range(nst)]
     alg_bytes = sum(stage_bytes) / nst
-    achieved = alg_bytes / (stencil_ms * 1e-3) / 1e9
     peaks = measured_peaks()
-    # the whole step (every node, every stage, all kernels) against the same peak
+    # stage by stage, every stage moves the whole state (stage_bytes); with
+    # two-stage passes, stages (1,2) and (3,4) are one pass each and only the
+    # last stage of an odd count runs alone
+    npairs = nst // 2 if pairs else 0
+    pass_bytes = [pair_bytes(host, q > 0) for q in range(npairs)]
+    single_bytes = stage_bytes[2 * npairs:]
+    if pairs:
+        kernel, mean_ms = "march_pair_kernel", pair_ms
+        launch_bytes = sum(pass_bytes) / npairs
+    else:
+        kernel, mean_ms = "march_kernel", stencil_ms
+        launch_bytes = alg_bytes
+    achieved = launch_bytes / (mean_ms * 1e-3) / 1e9
+    march_bytes = (sum(single_bytes) / len(single_bytes)) if single_bytes else alg_bytes
+    march_gbs = march_bytes / (stencil_ms * 1e-3) / 1e9 if kn[0] else None
+    # the whole step against the same peak: the schedule's own algorithmic
+    # bytes (interior passes and stages, plus the closure strips' stage-by-
+    # stage bytes), and the stage-by-stage bytes of every node (the work the
+    # step does, counted as one pass per stage)
+    n_edge = nodes - n_int
+    sched_bytes = sum(pass_bytes) + sum(single_bytes) + n_edge * bytes_per_node_update(host.mode, het,
+                                                                                      host.rk_order, host)
+    step_s = ms_max / args.steps * 1e-3
     step_bytes = nodes * bytes_per_node_update(host.mode, het, host.rk_order, host)
-    step_gbs = step_bytes / (ms_max / args.steps * 1e-3) / 1e9
+    step_gbs = sched_bytes / step_s / 1e9
+    unfused_gbs = step_bytes / step_s / 1e9
     survey_bytes = nodes * RK_STAGES[host.rk_order] * (BYTES_PER_NODE_STAGE[(host.mode, het)] - 5 * 8)
     newton_fail = g.newton_failures()
     g.close()
@@ -376,16 +430,23 @@ def run_gpu(args) -> None:
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms": e_ms, **e_parts},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload),
-                         "kernel": "march_kernel", "alg_bytes_per_launch": alg_bytes,
+                         "frac": achieved / peaks["hbm_gbs"], "traffic": profiled_traffic(args.workload, kernel),
+                         "kernel": kernel, "alg_bytes_per_launch": launch_bytes,
+                         "alg_bytes_per_pass_launch": pass_bytes,
                          "alg_bytes_per_stage_launch": stage_bytes,
-                         "mean_launch_ms": stencil_ms, "closure_kernel_mean_ms": closure_ms,
-                         "interface_kernel_mean_ms": edge_ms,
+                         "mean_launch_ms": mean_ms,
+                         "march_kernel": {"mean_launch_ms": stencil_ms if kn[0] else None, "achieved": march_gbs,
+                                          "frac": march_gbs / peaks["hbm_gbs"] if march_gbs else None},
+                         "closure_kernel_mean_ms": closure_ms, "interface_kernel_mean_ms": edge_ms,
+                         "band_kernel_mean_ms": band_ms if kn[4] else None,
                          "peak_source": peaks["source"],
                          "step_level": {"achieved": step_gbs, "frac": step_gbs / peaks["hbm_gbs"],
-                                        "bytes_per_node_update": bytes_per_node_update(host.mode, het,
-                                                                                       host.rk_order, host),
-                                        "frac_without_metric_reads": survey_bytes / step_bytes * step_gbs
+                                        "bytes_per_step": sched_bytes,
+                                        "stage_by_stage_bytes_per_node_update": bytes_per_node_update(
+                                            host.mode, het, host.rk_order, host),
+                                        "effective_stage_by_stage": unfused_gbs,
+                                        "effective_frac": unfused_gbs / peaks["hbm_gbs"],
+                                        "frac_without_metric_reads": survey_bytes / step_bytes * unfused_gbs
                                         / peaks["hbm_gbs"]}},
             "march_tile": tile_info,
             "two_stage_passes": pairs,

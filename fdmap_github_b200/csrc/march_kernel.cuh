@@ -201,6 +201,11 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 }
 
 
+// A row index given at run time or as a compile-time constant
+__device__ __forceinline__ int row_value(int r) { return r; }
+template <int V>
+__device__ __forceinline__ constexpr int row_value(std::integral_constant<int, V>) { return V; }
+
 // Row-group unit u -> (block, strip, first row) for tiles of MW x MR
 struct UnitPos {
   int b, sx, j0;
@@ -346,6 +351,10 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
                         (EXT != MARCH_PLAIN && (D.src.use_singular || B.gforce || B.frc_new));
     const double t_stage = forces ? stage_time(a) : 0.0;
     const int i = i0 + cx;
+    PmlSeg pseg{};
+    if constexpr (EXT == MARCH_PML && MODE == 2) {
+      if (B.pml) pseg = pml_segment<PI_>(D, B);
+    }
     int aborted_at = -1;
     for (int g = 0; g < ngroups; ++g) {
       // wait for groups g-1, g, g+1 (neighbours) and centre group g
@@ -374,7 +383,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
       // (ry is warp-uniform), so that every ring address is a slot pointer
       // plus a constant
       auto node = [&](auto ryc) {
-        constexpr int RY = decltype(ryc)::value;
+        const int RY = row_value(ryc);  // a compile-time constant, or the thread's row (PML variant)
         const long long c = (long long)j * pitch + i;
         // row j lives in group g, row RY; rows j +- s in group g + (RY +- s) div MR
         auto nrow = [&](int dr, size_t off, int q, int width) -> const double* {
@@ -383,7 +392,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
           const int r = rr - go * MR;
           return reinterpret_cast<const double*>(gq[1 + go] + off) + ((size_t)q * MR + r) * width;
         };
-        constexpr int ry = RY;
+        const int ry = RY;
         double acc[NF];
         if (load_df) {
           const double* dfc = reinterpret_cast<const double*>(cslot + L::DF_OFF) + (size_t)ry * MW + cx;
@@ -415,7 +424,7 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
             // Cartesian PML rates of the interior region (rates.f90:2089-2126)
             // from the ring; szz at the neighbours through the cache
             const double* Fin = B.F[a.in];
-            march_pml_interior<PI_>(D, B, c, a, acc, [&](int l, int dq, int dr) -> double {
+            march_pml_interior<PI_>(pseg, B, c, a, acc, [&](int l, int dq, int dr) -> double {
               if (l == 5) return Fin[5 * plane + c + dq + (long long)dr * pitch];
               return dr == 0 ? nrow(0, L::F_OFF, l, WH)[cx + HP + dq] : nrow(dr, L::F_OFF, l, WH)[cx + HP];
             });
@@ -500,7 +509,9 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
         }
       };
       if (j < jr1 && i >= nbst && i <= nx - 1 - nbst && j >= nbst && j <= ny - 1 - nbst) {
-        if constexpr (MR == 2) {
+        if constexpr (EXT == MARCH_PML) {
+          node(ry);  // one body: the PML variant is large, and copies per row strain the instruction cache
+        } else if constexpr (MR == 2) {
           if (ry == 0) node(std::integral_constant<int, 0>{});
           else node(std::integral_constant<int, 1>{});
         } else {

@@ -38,12 +38,15 @@
 //   - input ring (6 slots): the rate fields and yr, xr, yq, xq, Ji of a row
 //     group, {128 + 2 PI, 2, NR} and {128 + 2 PI, 2, 5};
 //   - centre ring (3 slots): the stage-s input rates (A != 0) and szz;
-//   - stage-s ring (3 slots): the rate fields after stage s, read by stage
-//     s+1 at the neighbours; each thread keeps its own node's stage-s fields
-//     and rates in registers for stage s+1 one iteration later.
-// Stage s runs one row group ahead of stage s+1.  Every mbarrier wait is
-// bounded in time; a CTA whose wait gives up stops, drains its copies and
-// leaves (status word -> FDMAP_ERR_TIMEOUT).
+//   - stage-s ring (4 slots): the rate fields after stage s, read by stage
+//     s+1 at the neighbours; each thread keeps its own node's stage-s rates
+//     and szz in registers for stage s+1 two iterations later.
+// Stage s runs two row groups ahead of stage s+1, so within one iteration
+// the two stages touch disjoint data and one barrier per iteration suffices;
+// a ring slot is refilled after that barrier, once every thread has left the
+// iteration that last read it.  Every mbarrier wait is bounded in time; a CTA
+// whose wait gives up stops, drains its copies and leaves (status word ->
+// FDMAP_ERR_TIMEOUT).
 #pragma once
 
 #include "march_kernel.cuh"
@@ -57,7 +60,7 @@ struct PairLayout {
   static constexpr int MR = 2;                // rows of a row group
   static constexpr int THREADS = MWX * MR;
   static constexpr int WB = MWX + 2 * PI_;    // box width: columns i0 - 2 PI .. i0 + MWC + 2 PI - 1
-  static constexpr int NGS = 6, NCS = 3, N1S = 3;
+  static constexpr int NGS = 6, NCS = 3, N1S = 4;
   static constexpr int NR = RDef<MODE>::NR;
   // input slot: rate fields [NR][MR][WB], yr, xr, yq, xq, Ji [5][MR][WB]
   static constexpr size_t F_OFF = 0;
@@ -74,7 +77,7 @@ struct PairLayout {
   static constexpr size_t BARS_OFF = S1_BASE + (size_t)N1S * S1SLOT;
   static constexpr size_t BYTES = BARS_OFF + (NGS + NCS) * 8 + 128;  // + alignment slack
   static constexpr unsigned NB_BYTES = (unsigned)((size_t)(NR + 5) * MR * WB * 8);
-  static_assert(PI_ <= MR, "stage s runs one row group ahead: PI rows must fit in one group");
+  static_assert(PI_ <= MR, "PI rows must fit in one row group");
 };
 
 // TMA descriptors of the two-stage march, every box {WB, MR, planes}
@@ -219,35 +222,50 @@ __global__ void __maxnreg__(168)
     // pointer of the iteration plus a constant)
     auto goff = [](int rr) { return rr >= 0 ? rr / MR : -((MR - 1 - rr) / MR); };
 
-    double pdf[NF], pf[NF];  // this thread's node, stage s: rates and fields (from the previous iteration)
+    // this thread's node, stage s, from the last two iterations (its rates
+    // and szz; the other fields are in the stage-s ring): [0] group t-2, [1] t-1
+    double hdf[2][NF], hf6[2];
 #pragma unroll
-    for (int l = 0; l < NF; ++l) { pdf[l] = 0.0; pf[l] = 0.0; }
-    double cdf[NF], cfl[NF];
+    for (int q = 0; q < 2; ++q) {
+      hf6[q] = 0.0;
+#pragma unroll
+      for (int l = 0; l < NF; ++l) hdf[q][l] = 0.0;
+    }
     int aborted_at = -1;
-    for (int t = ks0; t <= ks1 + 1; ++t) {
+    // iteration t: stage s at row group t, stage s+1 at row group t-2, one
+    // barrier; the second stage reads only what earlier iterations wrote, so
+    // the two are independent within an iteration
+    for (int t = ks0; t <= ngroups + 1; ++t) {
       bool ok = true;
-      // input groups t-2 .. t+1 (stage s at t needs t-1..t+1, stage s+1 at t-1 needs t-2..t)
-      for (int k = max(gmin, t - 2); k <= min(gmax, t + 1); ++k)
+      // input groups t-3 .. t+1 (stage s at t needs t-1..t+1, stage s+1 at t-2 needs t-3..t-1)
+      for (int k = max(gmin, t - 3); k <= min(gmax, t + 1); ++k)
         ok = mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status) && ok;
       if (t <= ks1) ok = mbar_wait_bounded(&cbar[(t - ks0) % NCS], (unsigned)(((t - ks0) / NCS) & 1), D.status) && ok;
       if (__syncthreads_or(!ok)) {
         aborted_at = t;
         break;
       }
+      // every thread is past iteration t-1: input group t-4 and centre group
+      // t-1 are free; their slots take groups t+2
+      if (tid == 0) {
+        fence_proxy_async();
+        if (t - 4 >= gmin && t + 2 <= gmax) fill_nb(t + 2);
+        if (t - 1 >= ks0 && t + 2 <= ks1) fill_c(t + 2);
+      }
       // this iteration's slots, offset by this thread's box column: input
-      // groups t-2 .. t+1, stage-s groups t-2 .. t, the centre group t (a
+      // groups t-3 .. t+1, stage-s groups t-3 .. t, the centre group t (a
       // group outside the CTA's range gets slot 0: no node that is computed
       // reads it)
-      const double* gp[4];
+      const double* gp[5];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int k = t - 2 + q;
+      for (int q = 0; q < 5; ++q) {
+        const int k = t - 3 + q;
         gp[q] = reinterpret_cast<const double*>(smem + (size_t)((k >= gmin ? k - gmin : 0) % NGS) * L::GSLOT) + pc;
       }
-      double* sp[3];
+      double* sp[4];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int k = t - 2 + q;
+      for (int q = 0; q < 4; ++q) {
+        const int k = t - 3 + q;
         sp[q] = reinterpret_cast<double*>(smem + L::S1_BASE + (size_t)((k >= ks0 ? k - ks0 : 0) % N1S) * L::S1SLOT) + cx;
       }
       const double* cp =
@@ -256,71 +274,25 @@ __global__ void __maxnreg__(168)
                     SO = (int)(L::F6_OFF / 8);
       const int js = jr0 + t * MR + ry;
       const bool s_on = t <= ks1 && i >= nbst && i <= nx - 1 - nbst && js >= nbst && js <= ny - 1 - nbst;
-      const int k1 = t - 1;
-      const int j1 = jr0 + k1 * MR + ry;
-      const bool s1_on = k1 >= 0 && core && j1 < jr1 && edge_distance(i, j1, nx, ny) >= nbst + PI_;
+      const int k2 = t - 2;
+      const int j2 = jr0 + k2 * MR + ry;
+      const bool s2_on = k2 >= 0 && core && j2 < jr1 && edge_distance(i, j2, nx, ny) >= nbst + PI_;
+      double cdf[NF], cf6 = 0.0;
+#pragma unroll
+      for (int l = 0; l < NF; ++l) cdf[l] = 0.0;
       // the row within the group is warp-uniform: one body per row value
-      // ---- stage s at row group t (interior nodes of the extended tile)
-      auto stage_s = [&](auto ryc) {
+      auto body = [&](auto ryc) {
         constexpr int RY = decltype(ryc)::value;
-#pragma unroll
-        for (int l = 0; l < NF; ++l) { cdf[l] = 0.0; cfl[l] = 0.0; }
-        if (s_on) {
+        // ---- stage s+1 at row group t-2 (core nodes at least nbst + PI from every edge)
+        if (s2_on) {
           double acc[NF];
-          if (load_df) {
 #pragma unroll
-            for (int l = 0; l < NR; ++l) acc[l] = a0.A * cp[DO + (l * MR + RY) * WB];
-          } else {
-#pragma unroll
-            for (int l = 0; l < NR; ++l) acc[l] = 0.0;
-          }
+          for (int l = 0; l < NR; ++l) acc[l] = a1.A != 0.0 ? a1.A * hdf[0][l] : 0.0;
           if (MODE == 2) acc[5] = 0.0;
           double Fc[NF];
 #pragma unroll
-          for (int l = 0; l < NR; ++l) Fc[l] = gp[2][FO + (l * MR + RY) * WB];
-          if (MODE == 2) Fc[5] = cp[SO + RY * WB];
-          const double Ji = gp[2][MO + (4 * MR + RY) * WB];
-          split_rates<MODE, PI_, false>(
-              acc, m, cf, D.DI, Ji, [&](int l, int s) { return gp[2][FO + (l * MR + RY) * WB + s]; },
-              [&](int l, int s) {
-                const int go = goff(RY + s);
-                return gp[2 + go][FO + (l * MR + (RY + s - go * MR)) * WB];
-              },
-              [&](int k, int s) { return gp[2][MO + (k * MR + RY) * WB + s]; },
-              [&](int k, int s) {
-                const int go = goff(RY + s);
-                return gp[2 + go][MO + ((2 + k) * MR + (RY + s - go * MR)) * WB];
-              });
-          if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-          if (forces) body_forces<MODE>(D, B, i, js, t0s, a0, acc);
-#pragma unroll
-          for (int l = 0; l < NF; ++l) {
-            cdf[l] = acc[l];
-            cfl[l] = Fc[l] + a0.Bdt * acc[l];
-          }
-#pragma unroll
-          for (int l = 0; l < NR; ++l) sp[2][(l * MR + RY) * MWX] = cfl[l];
-          // values the band kernel reads: stage s within nbst + 2 PI of an edge
-          const int d = edge_distance(i, js, nx, ny);
-          if (core && js >= jr0 && js < jr1 && d < nbst + 2 * PI_) {
-            const long long c = (long long)js * pitch + i;
-#pragma unroll
-            for (int l = 0; l < NF; ++l) Fband[l * plane + c] = cfl[l];
-            if (d < nbst + PI_) {
-#pragma unroll
-              for (int l = 0; l < NF; ++l) DFw[l * plane + c] = cdf[l];
-            }
-          }
-        }
-      };
-      // ---- stage s+1 at row group t - 1 (core nodes at least nbst + PI from every edge)
-      auto stage_s1 = [&](auto ryc) {
-        constexpr int RY = decltype(ryc)::value;
-        if (s1_on) {
-          double acc[NF];
-#pragma unroll
-          for (int l = 0; l < NR; ++l) acc[l] = a1.A != 0.0 ? a1.A * pdf[l] : 0.0;
-          if (MODE == 2) acc[5] = 0.0;
+          for (int l = 0; l < NR; ++l) Fc[l] = sp[1][(l * MR + RY) * MWX];
+          if (MODE == 2) Fc[5] = hf6[0];
           const double Ji = gp[1][MO + (4 * MR + RY) * WB];
           split_rates<MODE, PI_, false>(
               acc, m, cf, D.DI, Ji, [&](int l, int s) { return sp[1][(l * MR + RY) * MWX + s]; },
@@ -334,35 +306,77 @@ __global__ void __maxnreg__(168)
                 return gp[1 + go][MO + ((2 + k) * MR + (RY + s - go * MR)) * WB];
               });
           if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-          if (forces) body_forces<MODE>(D, B, i, j1, t1s, a1, acc);
-          const long long c = (long long)j1 * pitch + i;
+          if (forces) body_forces<MODE>(D, B, i, j2, t1s, a1, acc);
+          const long long c = (long long)j2 * pitch + i;
 #pragma unroll
           for (int l = 0; l < NF; ++l) DFw[l * plane + c] = acc[l];
 #pragma unroll
-          for (int l = 0; l < NF; ++l) Fout[l * plane + c] = pf[l] + a1.Bdt * acc[l];
+          for (int l = 0; l < NF; ++l) Fout[l * plane + c] = Fc[l] + a1.Bdt * acc[l];
+        }
+        // ---- stage s at row group t (interior nodes of the extended tile)
+        if (s_on) {
+          double acc[NF];
+          if (load_df) {
+#pragma unroll
+            for (int l = 0; l < NR; ++l) acc[l] = a0.A * cp[DO + (l * MR + RY) * WB];
+          } else {
+#pragma unroll
+            for (int l = 0; l < NR; ++l) acc[l] = 0.0;
+          }
+          if (MODE == 2) acc[5] = 0.0;
+          double Fc[NF];
+#pragma unroll
+          for (int l = 0; l < NR; ++l) Fc[l] = gp[3][FO + (l * MR + RY) * WB];
+          if (MODE == 2) Fc[5] = cp[SO + RY * WB];
+          const double Ji = gp[3][MO + (4 * MR + RY) * WB];
+          split_rates<MODE, PI_, false>(
+              acc, m, cf, D.DI, Ji, [&](int l, int s) { return gp[3][FO + (l * MR + RY) * WB + s]; },
+              [&](int l, int s) {
+                const int go = goff(RY + s);
+                return gp[3 + go][FO + (l * MR + (RY + s - go * MR)) * WB];
+              },
+              [&](int k, int s) { return gp[3][MO + (k * MR + RY) * WB + s]; },
+              [&](int k, int s) {
+                const int go = goff(RY + s);
+                return gp[3 + go][MO + ((2 + k) * MR + (RY + s - go * MR)) * WB];
+              });
+          if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
+          if (forces) body_forces<MODE>(D, B, i, js, t0s, a0, acc);
+          double F1[NF];
+#pragma unroll
+          for (int l = 0; l < NF; ++l) {
+            cdf[l] = acc[l];
+            F1[l] = Fc[l] + a0.Bdt * acc[l];
+          }
+          if (MODE == 2) cf6 = F1[5];
+#pragma unroll
+          for (int l = 0; l < NR; ++l) sp[3][(l * MR + RY) * MWX] = F1[l];
+          // values the band kernel reads: stage s within nbst + 2 PI of an edge
+          const int d = edge_distance(i, js, nx, ny);
+          if (core && js >= jr0 && js < jr1 && d < nbst + 2 * PI_) {
+            const long long c = (long long)js * pitch + i;
+#pragma unroll
+            for (int l = 0; l < NF; ++l) Fband[l * plane + c] = F1[l];
+            if (d < nbst + PI_) {
+#pragma unroll
+              for (int l = 0; l < NF; ++l) DFw[l * plane + c] = cdf[l];
+            }
+          }
         }
       };
-      if (ry == 0) stage_s(std::integral_constant<int, 0>{});
-      else stage_s(std::integral_constant<int, 1>{});
-      __syncthreads();
-      if (ry == 0) stage_s1(std::integral_constant<int, 0>{});
-      else stage_s1(std::integral_constant<int, 1>{});
+      if (ry == 0) body(std::integral_constant<int, 0>{});
+      else body(std::integral_constant<int, 1>{});
 #pragma unroll
-      for (int l = 0; l < NF; ++l) { pdf[l] = cdf[l]; pf[l] = cfl[l]; }
-      __syncthreads();
-      // input group t-2 is no longer needed: its slot takes t-2+NGS; centre slot of t takes t+NCS
-      if (tid == 0) {
-        fence_proxy_async();
-        if (t - 2 >= gmin && t - 2 + NGS <= gmax) fill_nb(t - 2 + NGS);
-        if (t <= ks1 && t + NCS <= ks1) fill_c(t + NCS);
-      }
+      for (int l = 0; l < NF; ++l) { hdf[0][l] = hdf[1][l]; hdf[1][l] = cdf[l]; }
+      hf6[0] = hf6[1];
+      hf6[1] = cf6;
     }
     if (aborted_at >= 0) {
       // wait (bounded again) for every copy this CTA may still have in flight
       // into its shared memory, then end the CTA
       if (tid == 0) {
         const int t = aborted_at;
-        for (int k = max(gmin, t - 2); k < nb_next; ++k)
+        for (int k = max(gmin, t - 3); k < nb_next; ++k)
           mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status);
         for (int k = max(ks0, t); k < c_next; ++k)
           mbar_wait_bounded(&cbar[(k - ks0) % NCS], (unsigned)(((k - ks0) / NCS) & 1), D.status);

@@ -569,19 +569,47 @@ __device__ __forceinline__ void pml_rates(const DevDomain& D, const DevBlock& B,
   }
 }
 
+// Per-block constants of the PML interior, read once per march segment
+// instead of once per node.
+struct PmlSeg {
+  double hxi, hyi, kappa, rho, G, M, gamma;
+  double DI[4], as[4], bs[4], cs[4];  // DI(s), DI(s)/rho, DI(s)*G, DI(s)*M
+  bool onx, ony;
+};
+
+template <int PI_>
+__device__ __forceinline__ PmlSeg pml_segment(const DevDomain& D, const DevBlock& B) {
+  PmlSeg P;
+  P.hxi = B.pml_h[(2 * 3 + 2) * 2];
+  P.hyi = B.pml_h[(2 * 3 + 2) * 2 + 1];
+  P.kappa = B.pml_kappa;
+  P.rho = B.rho_b; P.G = B.G_b; P.M = B.M_b; P.gamma = B.gamma_b;
+  P.onx = B.pml & 1;
+  P.ony = (B.pml >> 1) & 1;
+#pragma unroll
+  for (int s = 1; s <= PI_; ++s) {
+    P.DI[s] = D.DI[s];
+    P.as[s] = P.DI[s] / P.rho;
+    P.bs[s] = P.DI[s] * P.G;
+    P.cs[s] = P.DI[s] * P.M;
+  }
+  return P;
+}
+
 // The interior branch of pml_rates (rates.f90:2089-2126) for a node whose
 // neighbour values come from elsewhere (the march kernel's shared-memory
 // ring): F(l, dq, dr) is field l at (i + dq, j + dr).  Same arithmetic, in the
-// same order, as pml_rates for an interior node.
+// same order, as pml_rates for an interior node; the block constants come
+// from pml_segment.
 template <int PI_, typename FieldAt>
-__device__ __forceinline__ void march_pml_interior(const DevDomain& D, const DevBlock& B, long long c,
+__device__ __forceinline__ void march_pml_interior(const PmlSeg& P, const DevBlock& B, long long c,
                                                    const StageArgs& a, double* acc, FieldAt F) {
   constexpr int NF = 6;
   const long long plane = B.plane;
-  const double hxi = B.pml_h[(2 * 3 + 2) * 2], hyi = B.pml_h[(2 * 3 + 2) * 2 + 1];
+  const double hxi = P.hxi, hyi = P.hyi;
   const double sx = B.pml_s[c], sy = B.pml_s[plane + c];
-  const double rho = B.rho_b, G = B.G_b, M = B.M_b, gamma = B.gamma_b;
-  const bool onx = B.pml & 1, ony = (B.pml >> 1) & 1;
+  const double rho = P.rho, G = P.G, M = P.M, gamma = P.gamma;
+  const bool onx = P.onx, ony = P.ony;
   const bool load = a.scale && a.A != 0.0;
   double dwx[NF], dwy[NF];
   if (onx) {
@@ -597,7 +625,7 @@ __device__ __forceinline__ void march_pml_interior(const DevDomain& D, const Dev
     acc[3] = acc[3] - w[1] * G;
     acc[4] = acc[4] - w[0] * gamma * M;
 #pragma unroll
-    for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] - (sx + B.pml_kappa) * w[l];
+    for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] - (sx + P.kappa) * w[l];
   }
   if (ony) {
     double w[NF];
@@ -612,7 +640,7 @@ __device__ __forceinline__ void march_pml_interior(const DevDomain& D, const Dev
     acc[3] = acc[3] - w[0] * G;
     acc[4] = acc[4] - w[1] * M;
 #pragma unroll
-    for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] - (sy + B.pml_kappa) * w[l];
+    for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] - (sy + P.kappa) * w[l];
   }
 #pragma unroll
   for (int s = 1; s <= PI_; ++s) {
@@ -622,7 +650,7 @@ __device__ __forceinline__ void march_pml_interior(const DevDomain& D, const Dev
       dq[l] = F(l, s, 0) - F(l, -s, 0);
       dr[l] = F(l, 0, s) - F(l, 0, -s);
     }
-    const double DIs = D.DI[s];
+    const double DIs = P.DI[s];
     if (onx) {
 #pragma unroll
       for (int l = 0; l < NF; ++l) dwx[l] = dwx[l] + sx * hxi * dq[l] * DIs;
@@ -631,7 +659,7 @@ __device__ __forceinline__ void march_pml_interior(const DevDomain& D, const Dev
 #pragma unroll
       for (int l = 0; l < NF; ++l) dwy[l] = dwy[l] + sy * hyi * dr[l] * DIs;
     }
-    const double as = DIs / rho, bs = DIs * G, cs = DIs * M;
+    const double as = P.as[s], bs = P.bs[s], cs = P.cs[s];
     acc[0] = acc[0] + (hxi * dq[2] + hyi * dr[3]) * as;
     acc[1] = acc[1] + (hxi * dq[3] + hyi * dr[4]) * as;
     acc[2] = acc[2] + (hxi * dq[0] + hyi * dr[1] * gamma) * cs;

@@ -347,14 +347,14 @@ class GpuDomain:
         check_gpu(lib().fdmap_gpu_set_tile(self._g, int(tile)), "fdmap_gpu_set_tile")
 
     @property
-    def pairs(self) -> bool:
+    def two_stage(self) -> bool:
         """True when stages run in two-stage interior passes (march_pair.cuh)."""
         r = lib().fdmap_gpu_get_pairs(self._g)
         check_gpu(min(r, 0), "fdmap_gpu_get_pairs")
         return r == 1
 
-    @pairs.setter
-    def pairs(self, on: bool) -> None:
+    @two_stage.setter
+    def two_stage(self, on: bool) -> None:
         check_gpu(lib().fdmap_gpu_set_pairs(self._g, 1 if on else 0), "fdmap_gpu_set_pairs")
 
     def tune(self, steps: int = 5, dt: float | None = None) -> tuple[int, float]:

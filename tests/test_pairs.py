@@ -62,9 +62,9 @@ CASES = {
 def test_pairs_equal_stage_by_stage(require_gpu, case):
     h = init_domain(CASES[case]())
     g1, g0 = GpuDomain(h), GpuDomain(h)
-    assert g1.pairs, "the domain should take two-stage passes"
-    g0.pairs = False
-    assert not g0.pairs
+    assert g1.two_stage, "the domain should take two-stage passes"
+    g0.two_stage = False
+    assert not g0.two_stage
     n = h.nt - 1
     g1.run(1, n)
     g0.run(1, n)
@@ -97,11 +97,11 @@ def test_pairs_switch_mid_run(require_gpu):
     """Passes switched off and on between steps keep the run bit-identical."""
     h = init_domain(problems.rupture_sw(nx=161, ny=81, h=0.25, nt=61))
     a, b = GpuDomain(h), GpuDomain(h)
-    b.pairs = False
+    b.two_stage = False
     a.run(1, 10)
-    a.pairs = False
+    a.two_stage = False
     a.run(11, 17)
-    a.pairs = True
+    a.two_stage = True
     a.run(18, 30)
     b.run(1, 30)
     _same(_state(a, 1), _state(b, 1), "switched")
@@ -114,7 +114,7 @@ def test_pairs_with_outputs_open(require_gpu, tmp_path):
     outs = []
     for on in (True, False):
         g = GpuDomain(h)
-        g.pairs = on
+        g.two_stage = on
         g.output_add("V", 0, 0, FAULT_FIELDS.index("V"), 1, 161, 1, nmin=0, nmax=1 << 30, stride=1)
         g.output_add("S", 0, 0, FAULT_FIELDS.index("S"), 1, 161, 4, nmin=0, nmax=1 << 30, stride=2)
         g.output_add("vx", 1, 0, 0, 1, 161, 8, 1, 162, 8, nmin=0, nmax=1 << 30, stride=3)
@@ -136,7 +136,7 @@ def test_pairs_against_the_oracle(require_gpu):
 
     h = init_domain(problems.rupture_sw(nx=401, ny=201, h=0.1, nt=101))
     g, o = GpuDomain(h), OracleDomain(h)
-    assert g.pairs
+    assert g.two_stage
     g.run(1, 100)
     o.run(1, 100)
     assert_fields_close(g.get_fields()[0], o.get_fields()[0], what="pairs vs oracle")
@@ -150,9 +150,9 @@ def test_pairs_refused_where_they_do_not_apply(require_gpu, tmp_path):
                  problems.heterogeneous_ricker(tmp_path, n=61, h=0.1, nt=5)):
         h = init_domain(text, tmp_path)
         g = GpuDomain(h)
-        assert not g.pairs
+        assert not g.two_stage
         with pytest.raises(FdmapError) as e:
-            g.pairs = True
+            g.two_stage = True
         assert e.value.code == -6
         g.run(1, 3)
         g.close()

@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 def test_trace_records_every_stage_kernel(require_gpu):
     h = init_domain(problems.rupture_sw(nx=161, ny=81, h=0.25, nt=50))
     g = GpuDomain(h)
-    g.pairs = False  # stage by stage: one march launch per stage
+    g.two_stage = False  # stage by stage: one march launch per stage
     g.run(1, 3)
     g.trace(100000)
     g.run(4, 5)  # two steps, five stages each
@@ -36,7 +36,7 @@ def test_trace_records_two_stage_passes(require_gpu):
     the single fifth stage (1), and the closure and interface kernels."""
     h = init_domain(problems.rupture_sw(nx=161, ny=81, h=0.25, nt=50))
     g = GpuDomain(h)
-    assert g.pairs
+    assert g.two_stage
     g.run(1, 3)
     g.trace(100000)
     g.run(4, 5)
