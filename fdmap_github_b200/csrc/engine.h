@@ -271,6 +271,22 @@ int pair_configure(fdmap_gpu* h);
 int pair_launch(fdmap_gpu* h, const StageArgs& a0, const StageArgs& a1, int dfr, int dfw);
 int band_launch(fdmap_gpu* h, const StageArgs& a);
 
+// Two-stage passes over a batch of instances (ensemble.cu): the pass walks the
+// concatenated units of every instance, the band kernel the concatenated bands.
+struct PairBatch {
+  const DevDomain* doms;           // [ninst] device copies of each instance's domain
+  const TmapPair* tmaps;           // [ninst] device copies of each instance's pass tensor maps
+  const long long* unit_begin;     // [ninst+1] pass units, prefix over instances
+  const int* band_cta_begin;       // [ninst+1] band CTAs (128 threads), prefix over instances
+  int ninst;
+  long long units;
+  int grid;
+  int band_ctas;
+};
+int pair_batch(const fdmap_gpu* proto, const StageArgs& a0, const StageArgs& a1, int dfr, int dfw,
+               const PairBatch& p, cudaStream_t s);
+int band_batch(const fdmap_gpu* proto, const StageArgs& a, const PairBatch& p, cudaStream_t s);
+
 // Copy of every device allocation of a handle (its whole state), to put the
 // state back after timing runs; `out` receives the copies (freed by restore).
 int state_snapshot(fdmap_gpu* h, std::vector<void*>& out, cudaStream_t s);

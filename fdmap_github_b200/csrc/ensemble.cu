@@ -21,6 +21,7 @@
 #include "engine.h"
 #include "fdmap_gpu.h"
 #include "march_kernel.cuh"
+#include "march_pair.cuh"
 
 using namespace fdmap;
 
@@ -39,6 +40,13 @@ struct fdmap_ensemble {
   TimeState* d_time = nullptr;
   std::vector<long long> closure_threads, edge_threads;
   BatchPlan plan{};
+  // two-stage passes over every instance (all instances able to take them)
+  TmapPair* d_pmaps = nullptr;
+  long long* d_pair_begin = nullptr;
+  int* d_band_begin = nullptr;
+  PairBatch pplan{};
+  bool pair_ok = false;
+  bool pairs = false;
   int overlap = 1;
   int cur = 0;
   RkTable rk{};
@@ -61,6 +69,9 @@ struct fdmap_ensemble {
     cudaFree(d_unit_begin);
     cudaFree(d_closure_begin);
     cudaFree(d_edge_begin);
+    cudaFree(d_pmaps);
+    cudaFree(d_pair_begin);
+    cudaFree(d_band_begin);
     cudaFree(d_time);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
@@ -120,21 +131,74 @@ int ens_stage(fdmap_ensemble* e, const StageArgs& a) {
   return FDMAP_OK;
 }
 
-// all stages of one step of every instance (final step: stage 1 only)
+// Two stages a0, a1 of every instance as one interior pass (the single
+// domain's launch_pair over the batch): the pass beside the first stage's
+// interface solves and closure strips and the second stage's interface
+// solves, then the bands.
+int ens_pair(fdmap_ensemble* e, const StageArgs& a0, const StageArgs& a1, int dfr, int dfw) {
+  const BatchPlan& p = e->plan;
+  StageArgs c0 = a0;
+  c0.out = 2;
+  c0.dfr = dfr;
+  c0.dfw = dfw;
+  StageArgs e1 = a1;
+  e1.in = 2;
+  e1.dfr = dfw;
+  e1.dfw = dfw;
+  int rc;
+  cudaStream_t bs = e->overlap ? e->side : e->stream;
+  if (e->overlap) {
+    CUDA_TRY(cudaEventRecord(e->ev_fork, e->stream));
+    CUDA_TRY(cudaStreamWaitEvent(e->side, e->ev_fork, 0));
+  }
+  if ((rc = pair_batch(e->proto, a0, a1, dfr, dfw, e->pplan, e->stream))) return rc;
+  if ((rc = batch_edges(e->proto, c0, p, bs))) return rc;
+  if ((rc = batch_closure(e->proto, c0, p, bs))) return rc;
+  if ((rc = batch_edges(e->proto, e1, p, bs))) return rc;
+  if (e->overlap) {
+    CUDA_TRY(cudaEventRecord(e->ev_join, e->side));
+    CUDA_TRY(cudaStreamWaitEvent(e->stream, e->ev_join, 0));
+  }
+  if ((rc = band_batch(e->proto, e1, e->pplan, e->stream))) return rc;
+  e->launches += 2 * (p.edge_ctas ? 1 : 0) + (p.closure_ctas ? 1 : 0) + 1 + (e->pplan.band_ctas ? 1 : 0);
+  return FDMAP_OK;
+}
+
+// F buffer swaps of one (non-final) step: one per stage, or one per pass
+int ens_swaps(const fdmap_ensemble* e) {
+  return e->pairs ? e->rk.nstage / 2 + (e->rk.nstage & 1) : e->rk.nstage;
+}
+
+// all stages of one step of every instance (final step: stage 1 only); with
+// two-stage passes, stages (1,2), (3,4), ... as pairs and an odd last stage
+// alone, the rate buffers alternating as in the single domain's issue_step
 int ens_issue_step(fdmap_ensemble* e, int cur, double t0, double dt, bool final_step, const TimeState* ts) {
-  for (int s = 0; s < e->rk.nstage; ++s) {
+  const int npairs = (e->pairs && !final_step) ? e->rk.nstage / 2 : 0;
+  auto args = [&](int s, int in) {
     StageArgs a{};
     a.A = e->rk.A[s];
     a.Bdt = e->rk.B[s] * dt;
     a.t = t0 + e->rk.C[s] * dt;
     a.C = e->rk.C[s];
     a.ts = ts;
-    a.in = cur;
-    a.out = 1 - cur;
+    a.in = in;
+    a.out = 1 - in;
     a.scale = 1;
     a.update = final_step ? 0 : 1;
-    int rc = ens_stage(e, a);
-    if (rc) return rc;
+    return a;
+  };
+  for (int s = 0; s < e->rk.nstage; ++s) {
+    int rc;
+    const StageArgs a = args(s, cur);
+    if (s < 2 * npairs) {
+      const int p = s / 2;
+      const int dfw = ((npairs - 1 - p) & 1) ? 1 : 0;
+      const int dfr = p == 0 ? 0 : 1 - dfw;
+      if ((rc = ens_pair(e, a, args(s + 1, cur), dfr, dfw))) return rc;
+      ++s;
+    } else if ((rc = ens_stage(e, a))) {
+      return rc;
+    }
     if (final_step) return FDMAP_OK;
     cur = 1 - cur;
   }
@@ -192,6 +256,38 @@ int ens_fill_plan(fdmap_ensemble* e) {
   e->plan.units = units;
   // CTAs per SM as the shape allows (the ring fills shared memory), never more CTAs than units
   e->plan.march_grid = (int)std::min<long long>(grid, units);
+  // two-stage passes when every instance can take them
+  e->pair_ok = true;
+  for (fdmap_gpu* h : e->inst) e->pair_ok = e->pair_ok && h->pair_ok;
+  if (e->pair_ok) {
+    std::vector<TmapPair> pm(ninst);
+    std::vector<long long> pb(ninst + 1, 0);
+    std::vector<int> bb(ninst + 1, 0);
+    long long pu = 0;
+    int bc = 0, pgrid = 0;
+    for (int k = 0; k < ninst; ++k) {
+      fdmap_gpu* h = e->inst[k];
+      pm[k] = *h->tmaps_pair;
+      pb[k] = pu;
+      pu += h->pair_units;
+      bb[k] = bc;
+      bc += (int)((h->band_threads + 127) / 128);
+      pgrid = std::max(pgrid, h->pair_grid);
+    }
+    pb[ninst] = pu;
+    bb[ninst] = bc;
+    if (!e->d_pmaps) {
+      CUDA_TRY(cudaMalloc(&e->d_pmaps, sizeof(TmapPair) * ninst));
+      CUDA_TRY(cudaMalloc(&e->d_pair_begin, sizeof(long long) * (ninst + 1)));
+      CUDA_TRY(cudaMalloc(&e->d_band_begin, sizeof(int) * (ninst + 1)));
+    }
+    CUDA_TRY(cudaMemcpy(e->d_pmaps, pm.data(), sizeof(TmapPair) * ninst, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(e->d_pair_begin, pb.data(), sizeof(long long) * (ninst + 1), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(e->d_band_begin, bb.data(), sizeof(int) * (ninst + 1), cudaMemcpyHostToDevice));
+    e->pplan = PairBatch{e->d_doms, e->d_pmaps, e->d_pair_begin, e->d_band_begin, ninst, pu,
+                         (int)std::min<long long>(pgrid, pu), bc};
+  }
+  e->pairs = e->pair_ok && e->proto->use_pairs;
   e->free_graphs();
   return FDMAP_OK;
 }
@@ -316,7 +412,7 @@ int fdmap_gpu_ensemble_time_step(fdmap_ensemble* e, double t0, double dt, int fi
   int rc = ens_check_cur(e);
   if (rc) return rc;
   if ((rc = ens_issue_step(e, e->cur, t0, dt, final_step != 0, nullptr))) return rc;
-  if (!final_step && (e->rk.nstage & 1)) e->cur = 1 - e->cur;
+  if (!final_step && (ens_swaps(e) & 1)) e->cur = 1 - e->cur;
   ens_sync_cur(e);
   return FDMAP_OK;
 }
@@ -338,7 +434,7 @@ int fdmap_gpu_ensemble_run(fdmap_ensemble* e, double t_start, double dt, int n_f
     for (int n = n_first; n <= n_graph_last; ++n) {
       CUDA_TRY(cudaGraphLaunch(e->graph[e->cur], e->stream));
       e->launches += e->graph_launches;
-      if (e->rk.nstage & 1) e->cur = 1 - e->cur;
+      if (ens_swaps(e) & 1) e->cur = 1 - e->cur;
     }
     n_first = n_graph_last + 1;
   }
@@ -453,6 +549,23 @@ int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_s
   if (best_shape) { best_shape[0] = best[0]; best_shape[1] = best[1]; best_shape[2] = best[2]; }
   if (best_ms) *best_ms = best_t / steps;
   return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_set_pairs(fdmap_ensemble* e, int enable) {
+  if (!e) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble");
+  if (enable && !e->pair_ok) return set_err(FDMAP_ERR_UNSUPPORTED, "some instance cannot run two-stage passes");
+  CUDA_TRY(cudaSetDevice(e->device));
+  CUDA_TRY(cudaStreamSynchronize(e->stream));
+  if (e->pairs != (enable != 0)) {
+    e->pairs = enable != 0;
+    e->free_graphs();
+  }
+  return FDMAP_OK;
+}
+
+int fdmap_gpu_ensemble_get_pairs(fdmap_ensemble* e) {
+  if (!e) return set_err(FDMAP_ERR_INVALID_ARG, "null ensemble");
+  return e->pairs ? 1 : 0;
 }
 
 int fdmap_gpu_ensemble_set_tile(fdmap_ensemble* e, int tile) {

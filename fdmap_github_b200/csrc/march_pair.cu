@@ -151,4 +151,26 @@ int band_launch(fdmap_gpu* h, const StageArgs& a) {
   });
 }
 
+int pair_batch(const fdmap_gpu* proto, const StageArgs& a0, const StageArgs& a1, int dfr, int dfw,
+               const PairBatch& p, cudaStream_t s) {
+  return pair_dispatch(proto, [&](auto m, auto pi) -> int {
+    constexpr int MODE = decltype(m)::value, PI_ = decltype(pi)::value;
+    using L = PairLayout<MODE, PI_>;
+    PairPlan plan{p.units, p.tmaps, p.unit_begin, p.ninst, dfr, dfw};
+    march_pair_kernel<MODE, PI_><<<p.grid, L::THREADS, L::BYTES, s>>>(p.doms, a0, a1, plan, *proto->tmaps_pair);
+    CUDA_TRY(cudaGetLastError());
+    return FDMAP_OK;
+  });
+}
+
+int band_batch(const fdmap_gpu* proto, const StageArgs& a, const PairBatch& p, cudaStream_t s) {
+  if (p.band_ctas == 0) return FDMAP_OK;
+  return pair_dispatch(proto, [&](auto m, auto pi) -> int {
+    band_kernel_batch<decltype(m)::value, decltype(pi)::value><<<p.band_ctas, 128, 0, s>>>(p.doms, p.band_cta_begin,
+                                                                                           p.ninst, a);
+    CUDA_TRY(cudaGetLastError());
+    return FDMAP_OK;
+  });
+}
+
 }  // namespace fdmap

@@ -488,6 +488,17 @@ class GpuEnsemble:
     def tile(self, v: int) -> None:
         check_gpu(lib().fdmap_gpu_ensemble_set_tile(self._e, int(v)), "fdmap_gpu_ensemble_set_tile")
 
+    @property
+    def two_stage(self) -> bool:
+        """True when every instance steps in two-stage interior passes."""
+        r = lib().fdmap_gpu_ensemble_get_pairs(self._e)
+        check_gpu(min(r, 0), "fdmap_gpu_ensemble_get_pairs")
+        return r == 1
+
+    @two_stage.setter
+    def two_stage(self, on: bool) -> None:
+        check_gpu(lib().fdmap_gpu_ensemble_set_pairs(self._e, 1 if on else 0), "fdmap_gpu_ensemble_set_pairs")
+
     def launch_count(self) -> int:
         return lib().fdmap_gpu_ensemble_launch_count(self._e)
 

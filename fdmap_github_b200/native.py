@@ -127,6 +127,8 @@ SIGNATURES = {
     "fdmap_gpu_ensemble_get_shape": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "fdmap_gpu_ensemble_tune": (C.c_int, [_VP, C.c_double, C.c_int, C.POINTER(C.c_int), _DP]),
     "fdmap_gpu_ensemble_set_tile": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_ensemble_set_pairs": (C.c_int, [_VP, C.c_int]),
+    "fdmap_gpu_ensemble_get_pairs": (C.c_int, [_VP]),
     "fdmap_gpu_ensemble_get_tile": (C.c_int, [_VP, C.POINTER(C.c_int)]),
     "fdmap_gpu_ensemble_launch_count": (C.c_longlong, [_VP]),
     "fdmap_gpu_ensemble_destroy": (None, [_VP]),

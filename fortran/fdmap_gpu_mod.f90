@@ -222,6 +222,20 @@ module fdmap_gpu_mod
        real(c_double), intent(out) :: ms
      end function fdmap_gpu_tune
 
+     ! two-stage interior passes: stages (1,2), (3,4) of a step in one pass
+     ! each, bit-identical to stage by stage; on by default where the domain
+     ! allows them; get_pairs returns 1 (in use), 0 or a negative code
+     integer(c_int) function fdmap_gpu_set_pairs(h, enable) bind(C, name='fdmap_gpu_set_pairs')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+       integer(c_int), value :: enable
+     end function fdmap_gpu_set_pairs
+
+     integer(c_int) function fdmap_gpu_get_pairs(h) bind(C, name='fdmap_gpu_get_pairs')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: h
+     end function fdmap_gpu_get_pairs
+
      integer(c_int) function fdmap_gpu_create_part(d, device, owned, h) bind(C, name='fdmap_gpu_create_part')
        import :: c_int, c_ptr
        type(c_ptr), value :: d

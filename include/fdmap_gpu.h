@@ -344,6 +344,12 @@ int fdmap_gpu_ensemble_get_shape(fdmap_ensemble* e, int* shape);
  * ensemble's state is restored afterwards. */
 int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_shape, double* best_ms);
 
+/* Two-stage interior passes for every instance (as fdmap_gpu_set_pairs): on
+ * by default when every instance can take them; results are bit-identical
+ * either way.  get_pairs returns 1, 0 or a negative code. */
+int fdmap_gpu_ensemble_set_pairs(fdmap_ensemble* e, int enable);
+int fdmap_gpu_ensemble_get_pairs(fdmap_ensemble* e);
+
 /* March tile shape of every instance (as fdmap_gpu_set_tile, 0..3); the
  * autotuner picks it first. */
 int fdmap_gpu_ensemble_set_tile(fdmap_ensemble* e, int tile);

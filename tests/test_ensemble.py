@@ -103,3 +103,35 @@ def test_ensemble_tuner_and_shapes(require_gpu, tmp_path):
                 assert np.array_equal(a, b)
         e2.close()
     ens.close()
+
+
+@pytest.mark.gpu
+def test_ensemble_two_stage_passes_are_bit_identical(require_gpu, tmp_path):
+    """The batched two-stage passes (every instance's stages (1,2), (3,4) in
+    one pass) give the bits of the batched stage-by-stage run and of plain
+    stage-by-stage runs; the final step issued on top as well."""
+    sizes = [(81, 41), (161, 41), (131, 65)]
+    hosts = _instances(tmp_path, sizes)
+    ens, ens0 = GpuEnsemble(hosts), GpuEnsemble(hosts)
+    assert ens.two_stage
+    ens0.two_stage = False
+    assert not ens0.two_stage
+    dt = ens.dt
+    for e in (ens, ens0):
+        e.run(1, 25, dt=dt)
+        e.run(26, 26, dt=dt, nt=26)
+        e.synchronize()
+    for k, h in enumerate(hosts):
+        plain = GpuDomain(h)
+        plain.two_stage = False
+        plain.run(1, 25, dt=dt)
+        plain.run(26, 26, dt=dt, nt=26)
+        for other, what in ((ens0[k], "batched stage by stage"), (plain, "plain stage by stage")):
+            Fe, DFe = ens[k].get_fields(True, True)
+            Fo, DFo = other.get_fields(True, True)
+            assert np.array_equal(Fe, Fo) and np.array_equal(DFe, DFo), f"instance {k}: fields differ from the {what} run"
+            for f in FAULT_FIELDS:
+                assert np.array_equal(ens[k].get_fault(0, f), other.get_fault(0, f)), f"instance {k}: {f} ({what})"
+        plain.close()
+    ens.close()
+    ens0.close()
