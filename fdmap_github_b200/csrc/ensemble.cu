@@ -47,6 +47,7 @@ struct fdmap_ensemble {
   PairBatch pplan{};
   bool pair_ok = false;
   bool pairs = false;
+  bool pairs_wanted = true;  // the caller's (or the tuner's) choice; used when pair_ok
   int overlap = 1;
   int cur = 0;
   RkTable rk{};
@@ -287,7 +288,7 @@ int ens_fill_plan(fdmap_ensemble* e) {
     e->pplan = PairBatch{e->d_doms, e->d_pmaps, e->d_pair_begin, e->d_band_begin, ninst, pu,
                          (int)std::min<long long>(pgrid, pu), bc};
   }
-  e->pairs = e->pair_ok && e->proto->use_pairs;
+  e->pairs = e->pair_ok && e->pairs_wanted;
   e->free_graphs();
   return FDMAP_OK;
 }
@@ -512,16 +513,26 @@ int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_s
     }
     return FDMAP_OK;
   };
-  // 1. the march tile shape, with the boundary launch shapes as they are
-  for (int tile = 0; tile < MARCH_SHAPES && rc == FDMAP_OK; ++tile) {
+  // 1. the march tile shape, with two-stage passes on and off where every
+  // instance can take them, with the boundary launch shapes as they are
+  const bool pairs0 = e->pairs;
+  bool best_pairs = pairs0;
+  for (int k = 0; k < (e->pair_ok ? 2 : 1) * MARCH_SHAPES && rc == FDMAP_OK; ++k) {
+    const int tile = k % MARCH_SHAPES;
     rc = ens_set_tile(e, tile);
     if (rc == FDMAP_ERR_UNSUPPORTED) { rc = FDMAP_OK; continue; }
+    e->pairs = e->pair_ok ? k < MARCH_SHAPES : pairs0;  // after ens_set_tile, which resets it
+    e->free_graphs();
     float ms = 0.f;
     if (rc || (rc = time_shape(ms))) break;
-    if (best_t < 0.f || ms < best_t) { best_t = ms; best[3] = tile; }
+    if (best_t < 0.f || ms < best_t) { best_t = ms; best[3] = tile; best_pairs = e->pairs; }
   }
   // 2. closure and interface block sizes and the overlap, on the best tile
   if (rc == FDMAP_OK) rc = ens_set_tile(e, best[3]);
+  if (rc == FDMAP_OK) {
+    e->pairs = best_pairs;
+    e->free_graphs();
+  }
   for (int ov = 0; ov < 2 && rc == FDMAP_OK; ++ov)
     for (int ci = 0; ci < 3 && rc == FDMAP_OK; ++ci)
       for (int ei = 0; ei < 3 && rc == FDMAP_OK; ++ei) {
@@ -543,7 +554,12 @@ int fdmap_gpu_ensemble_tune(fdmap_ensemble* e, double dt, int steps, int* best_s
   cleanup();
   e->cur = cur0;
   ens_sync_cur(e);
-  if (rc) return rc;
+  if (rc) {
+    e->pairs = pairs0;
+    e->free_graphs();
+    return rc;
+  }
+  e->pairs_wanted = best_pairs;
   if ((rc = ens_set_tile(e, best[3]))) return rc;
   if ((rc = apply_shapes(e, best[0], best[1], best[2]))) return rc;
   if (best_shape) { best_shape[0] = best[0]; best_shape[1] = best[1]; best_shape[2] = best[2]; }
@@ -556,6 +572,7 @@ int fdmap_gpu_ensemble_set_pairs(fdmap_ensemble* e, int enable) {
   if (enable && !e->pair_ok) return set_err(FDMAP_ERR_UNSUPPORTED, "some instance cannot run two-stage passes");
   CUDA_TRY(cudaSetDevice(e->device));
   CUDA_TRY(cudaStreamSynchronize(e->stream));
+  e->pairs_wanted = enable != 0;
   if (e->pairs != (enable != 0)) {
     e->pairs = enable != 0;
     e->free_graphs();

@@ -1724,13 +1724,26 @@ int fdmap_gpu_tune(fdmap_gpu* h, double dt, int steps, int* best_tile, double* b
   int rc = state_snapshot(h, saved, h->stream);
   if (rc) return rc;
   const int cur0 = h->cur, shape0 = h->march_shape;
+  const bool pairs0 = h->use_pairs;
   const long long out0 = h->out_next_n;
   int best = shape0;
+  bool best_pairs = pairs0;
   float best_t = -1.f;
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
-  for (int sh = 0; sh < MARCH_SHAPES && rc == FDMAP_OK; ++sh) {
+  auto set_pairs = [&](bool on) {
+    if (h->use_pairs == on) return;
+    h->use_pairs = on;
+    for (auto& ge : h->step_graph)
+      if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+  };
+  // every tile shape, with two-stage passes on and off where the domain can
+  // take them (small, L2-resident domains step faster stage by stage)
+  for (int k = 0; k < (h->pair_ok ? 2 : 1) * MARCH_SHAPES && rc == FDMAP_OK; ++k) {
+    const int sh = k % MARCH_SHAPES;
+    const bool pv = h->pair_ok ? k < MARCH_SHAPES : pairs0;
+    set_pairs(pv);
     rc = march_set_shape(h, sh);
     if (rc == FDMAP_ERR_UNSUPPORTED) { rc = FDMAP_OK; continue; }
     if (rc) break;
@@ -1746,15 +1759,16 @@ int fdmap_gpu_tune(fdmap_gpu* h, double dt, int steps, int* best_tile, double* b
       cudaEventElapsedTime(&m, t0, t1);
       if (ms < 0.f || m < ms) ms = m;
     }
-    if (rc == FDMAP_OK && (best_t < 0.f || ms < best_t)) { best_t = ms; best = sh; }
+    if (rc == FDMAP_OK && (best_t < 0.f || ms < best_t)) { best_t = ms; best = sh; best_pairs = pv; }
   }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   const int rr = state_restore(h, saved, h->stream);
   h->cur = cur0;
   h->out_next_n = out0;
-  if (rc) { march_set_shape(h, shape0); return rc; }
+  if (rc) { set_pairs(pairs0); march_set_shape(h, shape0); return rc; }
   if (rr) return rr;
+  set_pairs(best_pairs);
   if ((rc = march_set_shape(h, best))) return rc;
   if (best_tile) *best_tile = best;
   if (best_ms) *best_ms = best_t / steps;

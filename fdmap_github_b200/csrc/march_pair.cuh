@@ -78,6 +78,7 @@ struct PairLayout {
   static constexpr size_t BYTES = BARS_OFF + (NGS + NCS) * 8 + 128;  // + alignment slack
   static constexpr unsigned NB_BYTES = (unsigned)((size_t)(NR + 5) * MR * WB * 8);
   static_assert(PI_ <= MR, "PI rows must fit in one row group");
+  static_assert((N1S & (N1S - 1)) == 0, "the stage-s ring index wraps by masking");
 };
 
 // TMA descriptors of the two-stage march, every box {WB, MR, planes}
@@ -235,12 +236,19 @@ __global__ void __maxnreg__(168)
     // iteration t: stage s at row group t, stage s+1 at row group t-2, one
     // barrier; the second stage reads only what earlier iterations wrote, so
     // the two are independent within an iteration
+    // ring slots of input group t-3, stage-s group t-3 and centre group t,
+    // advanced with t (a group outside the CTA's range maps to some slot: no
+    // node that is computed reads it)
+    int gi = ((ks0 - 3 - gmin) % NGS + NGS) % NGS;
+    int si = (ks0 - 3 - ks0) & (N1S - 1);
+    int ci = 0;
     for (int t = ks0; t <= ngroups + 1; ++t) {
       bool ok = true;
-      // input groups t-3 .. t+1 (stage s at t needs t-1..t+1, stage s+1 at t-2 needs t-3..t-1)
-      for (int k = max(gmin, t - 3); k <= min(gmax, t + 1); ++k)
+      // input groups t-3 .. t+1 (stage s at t needs t-1..t+1, stage s+1 at t-2
+      // needs t-3..t-1): all of them on the first iteration, then the new one
+      for (int k = (t == ks0 ? gmin : t + 1); k <= min(gmax, t + 1); ++k)
         ok = mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status) && ok;
-      if (t <= ks1) ok = mbar_wait_bounded(&cbar[(t - ks0) % NCS], (unsigned)(((t - ks0) / NCS) & 1), D.status) && ok;
+      if (t <= ks1) ok = mbar_wait_bounded(&cbar[ci], (unsigned)(((t - ks0) / NCS) & 1), D.status) && ok;
       if (__syncthreads_or(!ok)) {
         aborted_at = t;
         break;
@@ -259,17 +267,17 @@ __global__ void __maxnreg__(168)
       const double* gp[5];
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        const int k = t - 3 + q;
-        gp[q] = reinterpret_cast<const double*>(smem + (size_t)((k >= gmin ? k - gmin : 0) % NGS) * L::GSLOT) + pc;
+        const int sl = gi + q >= NGS ? gi + q - NGS : gi + q;
+        gp[q] = reinterpret_cast<const double*>(smem + (size_t)sl * L::GSLOT) + pc;
       }
       double* sp[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int k = t - 3 + q;
-        sp[q] = reinterpret_cast<double*>(smem + L::S1_BASE + (size_t)((k >= ks0 ? k - ks0 : 0) % N1S) * L::S1SLOT) + cx;
-      }
-      const double* cp =
-          reinterpret_cast<const double*>(smem + L::C_BASE + (size_t)((t >= ks0 ? t - ks0 : 0) % NCS) * L::CSLOT) + pc;
+      for (int q = 0; q < 4; ++q)
+        sp[q] = reinterpret_cast<double*>(smem + L::S1_BASE + (size_t)((si + q) & (N1S - 1)) * L::S1SLOT) + cx;
+      const double* cp = reinterpret_cast<const double*>(smem + L::C_BASE + (size_t)ci * L::CSLOT) + pc;
+      gi = gi + 1 == NGS ? 0 : gi + 1;
+      si = (si + 1) & (N1S - 1);
+      ci = ci + 1 == NCS ? 0 : ci + 1;
       constexpr int FO = (int)(L::F_OFF / 8), MO = (int)(L::M_OFF / 8), DO = (int)(L::DF_OFF / 8),
                     SO = (int)(L::F6_OFF / 8);
       const int js = jr0 + t * MR + ry;

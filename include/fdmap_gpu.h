@@ -148,10 +148,12 @@ int fdmap_gpu_set_tile(fdmap_gpu* h, int tile);
 int fdmap_gpu_get_tile(fdmap_gpu* h, int* tile, int* mw, int* mr);
 
 /* Autotuner of a single domain: times `steps` steps (CUDA graphs, best of two
- * repetitions) with every tile shape the domain can take, keeps the fastest
- * and returns it (best_tile, best_ms per step; either may be NULL).  The whole
- * device state is copied before and put back after, so tuning does not
- * advance the run.  Call it before opening outputs. */
+ * repetitions) with every tile shape the domain can take -- and, where the
+ * domain can take two-stage passes (fdmap_gpu_set_pairs), with the passes on
+ * and off -- keeps the fastest and returns its tile (best_tile, best_ms per
+ * step; either may be NULL; fdmap_gpu_get_pairs tells whether the passes were
+ * kept).  The whole device state is copied before and put back after, so
+ * tuning does not advance the run.  Call it before opening outputs. */
 int fdmap_gpu_tune(fdmap_gpu* h, double dt, int steps, int* best_tile, double* best_ms);
 
 /* Two-stage passes (no routine of the reference: an execution schedule of

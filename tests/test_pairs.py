@@ -156,3 +156,17 @@ def test_pairs_refused_where_they_do_not_apply(require_gpu, tmp_path):
         assert e.value.code == -6
         g.run(1, 3)
         g.close()
+
+
+def test_tuner_chooses_passes_and_keeps_the_bits(require_gpu):
+    """The autotuner times every tile with the passes on and off and keeps the
+    fastest; whatever it picks, the run is the untuned run bit for bit."""
+    for text in (problems.antiplane_pulse(n=201, L=10.0, nt=41), problems.rupture_sw(nx=321, ny=161, h=0.125, nt=41)):
+        h = init_domain(text)
+        g, ref = GpuDomain(h), GpuDomain(h)
+        tile, ms = g.tune(steps=3)
+        assert tile in (0, 1, 2, 3) and ms > 0.0
+        assert isinstance(g.two_stage, bool)
+        g.run(1, 30)
+        ref.run(1, 30)
+        _same(_state(g, h.nifaces), _state(ref, h.nifaces), f"tuned ({'passes' if g.two_stage else 'stage by stage'})")
