@@ -356,29 +356,40 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
       if (B.pml) pseg = pml_segment<PI_>(D, B);
     }
     int aborted_at = -1;
+    // ring slots of neighbour group g-1 and centre group g, advanced with g
+    // (a group outside the CTA's range maps to some slot: no node that is
+    // computed reads it)
+    int gi = ((-1 - gmin) % NGS + NGS) % NGS;
+    int ci = 0;
     for (int g = 0; g < ngroups; ++g) {
-      // wait for groups g-1, g, g+1 (neighbours) and centre group g
-      // neighbour group k lives in slot (k - gmin) % NGS as that slot's fill (k - gmin) / NGS
+      // wait for groups g-1, g, g+1 (neighbours; all of them on the first
+      // iteration, then the new one) and centre group g; neighbour group k
+      // lives in slot (k - gmin) % NGS as that slot's fill (k - gmin) / NGS
       bool ok = true;
-      for (int k = max(gmin, g - 1); k <= min(gmax, g + 1); ++k)
+      for (int k = (g == 0 ? max(gmin, g - 1) : g + 1); k <= min(gmax, g + 1); ++k)
         ok = mbar_wait_bounded(&nbar[(k - gmin) % NGS], (unsigned)(((k - gmin) / NGS) & 1), D.status) && ok;
-      ok = mbar_wait_bounded(&cbar[g % NCS], (unsigned)((g / NCS) & 1), D.status) && ok;
+      ok = mbar_wait_bounded(&cbar[ci], (unsigned)((g / NCS) & 1), D.status) && ok;
       // a wait that gave up anywhere in the CTA: no compute or store from
       // these slots, no further copies; the CTA drains and leaves
       if (__syncthreads_or(!ok)) {
         aborted_at = g;
         break;
       }
+      // every thread has left iteration g-1: neighbour group g-2 and centre
+      // group g-1 are no longer needed; their slots take g-2+NGS and g-1+NCS
+      if (tid == 0) {
+        fence_proxy_async();
+        if (g - 2 >= gmin && g - 2 + NGS <= gmax) fill_nb(g - 2 + NGS);
+        if (g >= 1 && g - 1 + NCS < ngroups) fill_c(g - 1 + NCS);
+      }
       const int j = jr0 + g * MR + ry;
-      // this iteration's neighbour slots, groups g-1, g, g+1 (a group outside
-      // the CTA's range gets slot 0: no node that is computed reads it)
+      // this iteration's neighbour slots, groups g-1, g, g+1
       const unsigned char* gq[3];
 #pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int k = g - 1 + q;
-        gq[q] = smem + (size_t)((k >= gmin ? k - gmin : 0) % NGS) * L::GSLOT;
-      }
-      const unsigned char* cslot = smem + (size_t)NGS * L::GSLOT + (size_t)(g % NCS) * L::CSLOT;
+      for (int q = 0; q < 3; ++q) gq[q] = smem + (size_t)(gi + q >= NGS ? gi + q - NGS : gi + q) * L::GSLOT;
+      const unsigned char* cslot = smem + (size_t)NGS * L::GSLOT + (size_t)ci * L::CSLOT;
+      gi = gi + 1 == NGS ? 0 : gi + 1;
+      ci = ci + 1 == NCS ? 0 : ci + 1;
       // the node's work with its row in the group as a compile-time constant
       // (ry is warp-uniform), so that every ring address is a slot pointer
       // plus a constant
@@ -521,13 +532,6 @@ __global__ void __maxnreg__((march_regs<MODE, PI_, EXT, SH>()))
           else if (ry == 2) node(std::integral_constant<int, 2>{});
           else node(std::integral_constant<int, 3>{});
         }
-      }
-      __syncthreads();
-      // group g-1 is no longer needed: its slot takes group g-1+NGS; centre slot g%NCS takes g+NCS
-      if (tid == 0) {
-        fence_proxy_async();
-        if (g - 1 >= gmin && g - 1 + NGS <= gmax) fill_nb(g - 1 + NGS);
-        if (g + NCS < ngroups) fill_c(g + NCS);
       }
     }
     if (aborted_at >= 0) {
