@@ -253,7 +253,12 @@ int batch_closure(const fdmap_gpu* proto, const StageArgs& a, const BatchPlan& p
     constexpr int MODE = decltype(mode_c)::value;
     constexpr int PI_ = decltype(pi_c)::value;
     constexpr bool HET = decltype(het_c)::value;
-    closure_kernel_batch<MODE, PI_, HET><<<p.closure_ctas, p.closure_tpb, 0, s>>>(p.doms, p.closure_cta_begin, p.ninst, a);
+    if (proto->march_ext == 0 && !proto->dissipation && !proto->pml && !proto->forcing && !proto->extras)
+      closure_kernel_batch<MODE, PI_, HET, true><<<p.closure_ctas, p.closure_tpb, 0, s>>>(p.doms, p.closure_cta_begin,
+                                                                                        p.ninst, a);
+    else
+      closure_kernel_batch<MODE, PI_, HET><<<p.closure_ctas, p.closure_tpb, 0, s>>>(p.doms, p.closure_cta_begin,
+                                                                                  p.ninst, a);
     CUDA_TRY(cudaGetLastError());
     return (int)FDMAP_OK;
   });
@@ -275,10 +280,26 @@ namespace {
 // thread) fit beside a resident march CTA
 constexpr int CLOSURE_TPB = 64;
 
+// a domain without PML, dissipation, forcing and body extras: the closure
+// kernel without those branches
+bool plain_domain(const fdmap_gpu* h) { return !h->dissipation && !h->pml && !h->forcing && !h->extras; }
+
 template <int MODE>
 void launch_closure_mode(fdmap_gpu* h, const StageArgs& a) {
   const int t = CLOSURE_TPB;
   int nb = (int)((h->closure_threads + t - 1) / t);
+  if (plain_domain(h)) {
+    if (h->het) {
+      if (h->pI == 1) closure_kernel<MODE, 1, true, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+      else if (h->pI == 2) closure_kernel<MODE, 2, true, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+      else closure_kernel<MODE, 3, true, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+    } else {
+      if (h->pI == 1) closure_kernel<MODE, 1, false, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+      else if (h->pI == 2) closure_kernel<MODE, 2, false, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+      else closure_kernel<MODE, 3, false, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
+    }
+    return;
+  }
   if (h->het) {
     if (h->pI == 1) closure_kernel<MODE, 1, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
     else if (h->pI == 2) closure_kernel<MODE, 2, true><<<nb, t, 0, h->stream>>>(h->hdom, a);
@@ -304,6 +325,12 @@ int boundary_carveout_mode() {
       (const void*)closure_kernel_batch<MODE, 1, false>, (const void*)closure_kernel_batch<MODE, 2, false>,
       (const void*)closure_kernel_batch<MODE, 3, false>, (const void*)closure_kernel_batch<MODE, 1, true>,
       (const void*)closure_kernel_batch<MODE, 2, true>, (const void*)closure_kernel_batch<MODE, 3, true>,
+      (const void*)closure_kernel<MODE, 1, false, true>, (const void*)closure_kernel<MODE, 2, false, true>,
+      (const void*)closure_kernel<MODE, 3, false, true>, (const void*)closure_kernel<MODE, 1, true, true>,
+      (const void*)closure_kernel<MODE, 2, true, true>, (const void*)closure_kernel<MODE, 3, true, true>,
+      (const void*)closure_kernel_batch<MODE, 1, false, true>, (const void*)closure_kernel_batch<MODE, 2, false, true>,
+      (const void*)closure_kernel_batch<MODE, 3, false, true>, (const void*)closure_kernel_batch<MODE, 1, true, true>,
+      (const void*)closure_kernel_batch<MODE, 2, true, true>, (const void*)closure_kernel_batch<MODE, 3, true, true>,
   };
   for (const void* k : ks)
     CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,

@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(128) band_kernel(const __grid_constant__ DevDo
     int i, j;
     const int b = band_item(D, tid, i, j);
     const DevBlock& B = D.blk[b];
-    if (edge_distance(i, j, B.nx, B.ny) < D.nbst) closure_node<MODE, PI_, false>(D, B, i, j, a, -1, nullptr);
+    if (edge_distance(i, j, B.nx, B.ny) < D.nbst) closure_node<MODE, PI_, false, true>(D, B, i, j, a, -1, nullptr);
     else interior_node_global<MODE, PI_>(D, B, i, j, a);
   }
   if (threadIdx.x == 0) trace_record(D.trace, TRACE_BAND, t_in);
@@ -488,7 +488,7 @@ __global__ void __launch_bounds__(128)
   int i, j;
   const int b = band_item(D, tid, i, j);
   const DevBlock& B = D.blk[b];
-  if (edge_distance(i, j, B.nx, B.ny) < D.nbst) closure_node<MODE, PI_, false>(D, B, i, j, a, -1, nullptr);
+  if (edge_distance(i, j, B.nx, B.ny) < D.nbst) closure_node<MODE, PI_, false, true>(D, B, i, j, a, -1, nullptr);
   else interior_node_global<MODE, PI_>(D, B, i, j, a);
 }
 

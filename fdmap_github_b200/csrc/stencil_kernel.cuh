@@ -115,7 +115,7 @@ __device__ __forceinline__ double flux(int r, double Ym, double Xm, const double
 // (rates_boundary_mode2/3 and the heterogeneous variants).
 __host__ __device__ constexpr int nbnd_of(int pI) { return pI == 1 ? 2 : (pI == 2 ? 6 : 9); }
 
-template <int MODE, int PI_>
+template <int MODE, int PI_, bool PLAIN = false>
 __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock& B, const double* __restrict__ Fin, int i, int j,
                               const NodeMat& m, double Ji, double* acc) {
   using RD = RDef<MODE>;
@@ -193,7 +193,7 @@ __device__ __forceinline__ void closure_rates(const DevDomain& D, const DevBlock
       qterm(c - s, D.DI[s], -1);
     }
   }
-  if (B.Cdiss > 0.0) {
+  if (!PLAIN && B.Cdiss > 0.0) {
     // artificial dissipation (rates_dissipation_boundary_mode2/3, rates.f90:1002-1394,
     // 1485-2021): J-weighted AL rows (AR mirrors AL without a sign change) in a
     // one-sided direction, AI in a central one, and AI(0)*F once per central direction
@@ -315,7 +315,9 @@ __device__ __forceinline__ double stf_amp(const fdmap_source& S, double t) {
 
 // body forces (set_source, source.f90:147-324) at block-local node (i, j):
 // gravity, the point source, tsunami forcing and forcing from file, in that order
-template <int MODE>
+// PLAIN: the domain has no long-wave forcing and no forcing file, so only
+// gravity and the point source are compiled in.
+template <int MODE, bool PLAIN = false>
 __device__ __forceinline__ void body_forces(const DevDomain& D, const DevBlock& B, int i, int j, double t,
                                             const StageArgs& a, double* acc) {
   if (D.src.use_gravity) {
@@ -342,6 +344,7 @@ __device__ __forceinline__ void body_forces(const DevDomain& D, const DevBlock& 
       }
     }
   }
+  if constexpr (PLAIN) return;
   const long long c = (long long)j * B.pitch + i;
   if (MODE == 3 && B.gforce) {
     // problem = 'Forcing' (source.f90:299-312); the spatial factor is per node
@@ -685,7 +688,10 @@ __device__ __forceinline__ void march_pml_interior(const PmlSeg& P, const DevBlo
 // Whole stage for one node of the SBP closure strips: scale, SAT (sides in the
 // reference's order L, R, B, T), one-sided closure rates (rates_boundary_mode2/3),
 // szz, sources, update.  Side `iside` takes the caller's hat variables.
-template <int MODE, int PI_, bool HET>
+// PLAIN: a domain without PML, dissipation, forcing, body displacement and
+// peak motion; those branches are compiled out (a smaller kernel, fewer
+// instruction-cache misses), the arithmetic is the same.
+template <int MODE, int PI_, bool HET, bool PLAIN = false>
 __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock& B, int i, int j, const StageArgs& a,
                                              int iside, const double* Fh_given) {
   constexpr int NF = MODE == 2 ? 6 : 3;
@@ -716,13 +722,14 @@ __device__ __forceinline__ void closure_node(const DevDomain& D, const DevBlock&
   }
   m.rinv = HET ? 1.0 / m.rho : B.rinv_b;
   bool pml = false;
-  if constexpr (MODE == 2) {
+  if constexpr (MODE == 2 && !PLAIN) {
     if (B.pml) { pml_rates<PI_>(D, B, Fin, i, j, a, acc); pml = true; }
   }
-  if (!pml) closure_rates<MODE, PI_>(D, B, Fin, i, j, m, B.Ji[c], acc);
+  if (!pml) closure_rates<MODE, PI_, PLAIN>(D, B, Fin, i, j, m, B.Ji[c], acc);
   if (MODE == 2) acc[5] = m.nu * (acc[2] + acc[4]);
-  body_forces<MODE>(D, B, i, j, stage_time(a), a, acc);
-  body_extras<MODE>(B, c, Fc, acc, a);
+  if (!PLAIN || D.src.use_gravity || D.src.use_singular)
+    body_forces<MODE, PLAIN>(D, B, i, j, stage_time(a), a, acc);
+  if constexpr (!PLAIN) body_extras<MODE>(B, c, Fc, acc, a);
   double* __restrict__ DFw = a.dfw ? B.DFalt : B.DF;
 #pragma unroll
   for (int l = 0; l < NF; ++l) DFw[l * plane + c] = acc[l];
@@ -758,19 +765,19 @@ __device__ __forceinline__ bool on_interface_side(const DevBlock& B, int i, int 
 }
 
 // Boundary kernel: every node within nbst of a block edge (the SBP closure strips).
-template <int MODE, int PI_, bool HET>
+template <int MODE, int PI_, bool HET, bool PLAIN = false>
 __global__ void __maxnreg__(BOUNDARY_REGS) closure_kernel(const __grid_constant__ DevDomain D, StageArgs a) {
   const unsigned long long t_in = (threadIdx.x == 0 && D.trace.rec) ? globaltimer_ns() : 0ull;
   long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (tid >= D.cstart[4 * D.nblocks]) return;
   int i, j;
   const int b = closure_item(D, tid, i, j);
-  closure_node<MODE, PI_, HET>(D, D.blk[b], i, j, a, -1, nullptr);
+  closure_node<MODE, PI_, HET, PLAIN>(D, D.blk[b], i, j, a, -1, nullptr);
   if (threadIdx.x == 0) trace_record(D.trace, TRACE_CLOSURE, t_in);
 }
 
 // Closure strips of a batch of independent instances in one launch.
-template <int MODE, int PI_, bool HET>
+template <int MODE, int PI_, bool HET, bool PLAIN = false>
 __global__ void __maxnreg__(BOUNDARY_REGS)
     closure_kernel_batch(const DevDomain* __restrict__ doms, const int* __restrict__ cta_begin, int ninst, StageArgs a) {
   const int k = batch_instance(cta_begin, ninst, blockIdx.x);
@@ -779,7 +786,7 @@ __global__ void __maxnreg__(BOUNDARY_REGS)
   if (tid >= D.cstart[4 * D.nblocks]) return;
   int i, j;
   const int b = closure_item(D, tid, i, j);
-  closure_node<MODE, PI_, HET>(D, D.blk[b], i, j, a, -1, nullptr);
+  closure_node<MODE, PI_, HET, PLAIN>(D, D.blk[b], i, j, a, -1, nullptr);
 }
 
 template <int MODE, int PI_, bool HET>

@@ -55,6 +55,9 @@ CASES = {
     "III-pulse": lambda: problems.antiplane_pulse(n=161, L=8.0, nt=41),
     "II-SW-RK3": lambda: problems.rupture_sw(nx=161, ny=81, h=0.25, nt=41, rk=3),
     "II-SW-RK2": lambda: problems.rupture_sw(nx=161, ny=81, h=0.25, nt=41, rk=2),
+    # a point force in the interior and in the band: the passes' body-force variant
+    "III-locked-source": lambda: fault_text(mode=3, coupling="locked", n=81, nt=41)
+    + "&source_list x0=0.37d0, y0=-1.61d0, Fz=1d0, source_time_function='Ricker', t_center=0.3d0, t_duration=0.25d0 /\n",
 }
 
 
