@@ -370,6 +370,8 @@ def run_gpu(args) -> None:
     lib_set_stream(g2, stream)
     if tile is not None:
         g2.set_tile(tile)
+    if g2.two_stage != pairs:
+        g2.two_stage = pairs  # the tuner's choice for the first handle
     nf = info.get("fault_nodes", 0)
     # the fault registers as the descriptor gives them, before the initial edge solve
     fault0 = {f: torch.from_numpy(g2.get_fault(0, f)).pin_memory().numpy() for f in FAULT_INDEX} if nf else {}
