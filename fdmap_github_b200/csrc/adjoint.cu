@@ -19,6 +19,12 @@
 //             every stage input stored, then reversed stage by stage with the
 //             discrete adjoint (adjoint_kernel.cuh), injecting the receiver
 //             residuals dJ/dU^n = vz - d at every step start.
+//   resident segments: with a store budget, the forward run with data keeps
+//             the stage inputs of its last R segments in device memory (the
+//             whole 2000-step trajectory of an 801 x 801 block is 157 GB),
+//             and the backward reverses those without recomputing them; the
+//             others are recomputed into one more segment store after them.
+//             The stored inputs are the recomputed ones bit for bit.
 // J = 1/2 sum_n sum_r (vz_r(U^n) - d_r^n)^2.
 #include <cuda_runtime.h>
 
@@ -60,7 +66,13 @@ struct fdmap_adjoint {
   double* init_DF = nullptr;
   double* ckpt = nullptr;            // checkpoints, 3 planes each
   int nckpt_alloc = 0;
-  double* store = nullptr;           // stage inputs of one segment: K*nstage slots of 3 planes
+  double* store = nullptr;           // stage inputs: store_segs segments of K*nstage slots
+  int store_segs = 1;                // segment stores allocated (the resident ones, then the recomputed one)
+  long long store_budget = 0;        // bytes for resident segments: 0 none, < 0 all free device memory
+  int plan_nseg = -1;                // segments and budget the present store was sized for
+  long long plan_budget = 0;
+  int plan_R = 0;                    // resident segments of that plan
+  int resident = 0;                  // last segments of the last forward with data held in the store
   double* ub[2] = {nullptr, nullptr};
   double* qp[2] = {nullptr, nullptr};
   double* grho = nullptr;
@@ -89,8 +101,10 @@ struct fdmap_adjoint {
   int trace_alloc = 0;
   AdjClock* clock = nullptr;
   bool have_resid = false;
-  // graphs: forward step (by F parity), recompute step (by F parity), adjoint step (by ubar parity)
-  cudaGraphExec_t g_fwd[2] = {nullptr, nullptr}, g_rec[2] = {nullptr, nullptr}, g_adj[2] = {nullptr, nullptr};
+  // graphs: forward step, forward step that also stores its stage inputs,
+  // recompute step (each by F parity), adjoint step (by ubar parity)
+  cudaGraphExec_t g_fwd[2] = {nullptr, nullptr}, g_fst[2] = {nullptr, nullptr}, g_rec[2] = {nullptr, nullptr},
+                  g_adj[2] = {nullptr, nullptr};
   double graph_dt = -1.0, graph_t0 = 0.0;
   std::vector<void*> mem;
 
@@ -101,8 +115,9 @@ struct fdmap_adjoint {
   long long fault_pad() const { return (nfault + 1) & ~1; }
   long long slot_stride() const { return general ? total + 2 * fault_pad() : stride(); }
   long long ckpt_stride() const { return general ? total + st_total : stride(); }
+  size_t segment_bytes() const { return (size_t)K * h->rk.nstage * slot_stride() * sizeof(double); }
   void free_graphs() {
-    for (auto* set : {g_fwd, g_rec, g_adj})
+    for (auto* set : {g_fwd, g_fst, g_rec, g_adj})
       for (int q = 0; q < 2; ++q)
         if (set[q]) { cudaGraphExecDestroy(set[q]); set[q] = nullptr; }
     graph_dt = -1.0;
@@ -193,8 +208,8 @@ int adj_maps_for(fdmap_adjoint* a) {
       if ((rc = adj_encode(enc, &m.ub[q], a->ub[q] + a->boff[b], g, 3, T::WX, T::WY, 3))) return rc;
       if ((rc = adj_encode(enc, &m.qp[q], a->qp[q] + a->boff[b], g, 3, T::WX, T::WY, 3))) return rc;
     }
-    if ((rc = adj_encode_store(enc, &m.st, a->store + a->boff[b], g, a->slot_stride(), (long long)a->K * h->rk.nstage,
-                               T::WX, T::WY)))
+    if ((rc = adj_encode_store(enc, &m.st, a->store + a->boff[b], g, a->slot_stride(),
+                               (long long)a->store_segs * a->K * h->rk.nstage, T::WX, T::WY)))
       return rc;
     if ((rc = adj_encode(enc, &m.met, h->met_base[b], g, 5, T::WX, T::WY, 5))) return rc;
     if ((rc = adj_encode(enc, &m.het, h->het_base[b], g, 2, T::WX, T::WY, 2))) return rc;
@@ -388,19 +403,23 @@ int build_graphs(fdmap_adjoint* a, double dt) {
   const DevBlock& B = h->hdom.blk[0];
   int rc = FDMAP_OK;
   for (int c = 0; c < 2 && rc == FDMAP_OK; ++c) {
-    // forward step: sample vz at the receivers at the step start, then the stages
-    rc = capture(a, &a->g_fwd[c], [&]() -> int {
-      int r = forward_step_stages(a, c, dt, false);
-      if (r) return r;
-      const int last = (h->rk.nstage & 1) ? 1 - c : c;  // buffer holding the new state
-      if (a->general)
-        adj_sample_advance_ptr<<<1, 128, 0, h->stream>>>(a->recp[last], a->nrec, h->d_time, a->traces,
-                                                         a->trace_alloc);
-      else
-        adj_sample_advance<<<1, 128, 0, h->stream>>>(B.F[last], a->rec, a->nrec, h->d_time, a->traces,
-                                                     a->trace_alloc);
-      return (int)FDMAP_OK;
-    });
+    // forward step: the stages, then vz at the receivers of the new state;
+    // the storing variant also puts every stage input into the store and
+    // advances the store's step index
+    for (int keep = 0; keep < 2 && rc == FDMAP_OK; ++keep)
+      rc = capture(a, keep ? &a->g_fst[c] : &a->g_fwd[c], [&]() -> int {
+        int r = forward_step_stages(a, c, dt, keep != 0);
+        if (r) return r;
+        const int last = (h->rk.nstage & 1) ? 1 - c : c;  // buffer holding the new state
+        AdjClock* ck = keep ? a->clock : nullptr;
+        if (a->general)
+          adj_sample_advance_ptr<<<1, 128, 0, h->stream>>>(a->recp[last], a->nrec, h->d_time, a->traces,
+                                                           a->trace_alloc, ck);
+        else
+          adj_sample_advance<<<1, 128, 0, h->stream>>>(B.F[last], a->rec, a->nrec, h->d_time, a->traces,
+                                                       a->trace_alloc, ck);
+        return (int)FDMAP_OK;
+      });
     if (rc) break;
     // recomputed step: every stage input goes to the segment store
     rc = capture(a, &a->g_rec[c], [&]() -> int {
@@ -504,6 +523,51 @@ int save_state(fdmap_adjoint* a, double* dst) {
                              (size_t)FDMAP_FAULT_NFIELDS * h->hdom.ifc[i].n * sizeof(double), cudaMemcpyDeviceToDevice,
                              h->stream));
   }
+  return FDMAP_OK;
+}
+
+// Size the stage store for a forward with data over `nseg` segments: R
+// resident segments (the last ones) as the budget and the free device memory
+// allow, less a 2 GiB margin, and one segment store more for recomputing the
+// others when R < nseg.  The plan is kept while nseg and the budget stay the
+// same, so repeated forward runs reuse the store, its maps and the graphs.
+int ensure_store(fdmap_adjoint* a, int nseg) {
+  if (a->plan_nseg == nseg && a->plan_budget == a->store_budget) return FDMAP_OK;
+  const size_t seg = a->segment_bytes();
+  int R = 0;
+  if (a->store_budget != 0) {
+    size_t freeb = 0, totalb = 0;
+    CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+    const size_t margin = (size_t)2 << 30;
+    const size_t have = freeb + (size_t)a->store_segs * seg;  // the present store is given back first
+    size_t avail = have > margin ? have - margin : 0;
+    if (a->store_budget > 0) avail = std::min(avail, (size_t)a->store_budget);
+    const long long fit = (long long)(avail / seg);
+    R = fit >= nseg ? nseg : (int)std::max(0LL, fit - 1);
+  }
+  const int segs = R < nseg ? R + 1 : R;
+  if (segs != a->store_segs) {
+    a->free_graphs();  // graphs and maps hold the store
+    CUDA_TRY(cudaStreamSynchronize(a->h->stream));
+    a->release(a->store);
+    a->store = nullptr;
+    a->resident = 0;
+    if (a->alloc(&a->store, (size_t)segs * seg / sizeof(double)) != FDMAP_OK) {
+      // fall back to checkpointing alone (and clear the failed allocation's error)
+      cudaGetLastError();
+      R = 0;
+      int rc = a->alloc(&a->store, seg / sizeof(double));
+      if (rc) return rc;
+      a->store_segs = 1;
+    } else {
+      a->store_segs = segs;
+    }
+    int rc = adj_maps(a);
+    if (rc) return rc;
+  }
+  a->plan_nseg = nseg;
+  a->plan_budget = a->store_budget;
+  a->plan_R = R;
   return FDMAP_OK;
 }
 
@@ -738,6 +802,7 @@ int fdmap_gpu_adjoint_create(const fdmap_desc* d, int device, int nrec, const in
 int fdmap_gpu_adjoint_set_material(fdmap_adjoint* a, const double* rho, const double* G) {
   if (!a || !rho || !G) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
   fdmap_gpu* h = a->h;
+  a->resident = 0;  // stored stage inputs belong to the old model: a backward recomputes
   CUDA_TRY(cudaSetDevice(h->device));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   for (size_t q = 0; q < (size_t)h->nx_g * h->ny_g; ++q)
@@ -776,6 +841,10 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
   if ((rc = ensure_trace_buffers(a, nt))) return rc;
   const int nck = (nt - 1 + a->K - 1) / a->K;
   if ((rc = ensure_checkpoints(a, nck))) return rc;
+  // a run with data precedes a backward: its last R segments keep their stage inputs
+  if (data && (rc = ensure_store(a, nck))) return rc;
+  const int R = data ? a->plan_R : 0;
+  a->resident = 0;
   a->N = nt;
   a->t_start = t_start;
   a->dt = dt;
@@ -798,10 +867,18 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
   else
     adj_sample<<<(a->nrec + 127) / 128, 128, 0, h->stream>>>(B.F[0], a->rec, a->nrec, h->d_time, a->traces, nt);
   CUDA_TRY(cudaGetLastError());
+  const int first = nck - R;  // first resident segment
   for (int n = 1; n <= nt - 1; ++n) {
-    if ((n - 1) % a->K == 0 && (rc = save_state(a, a->ckpt + (size_t)((n - 1) / a->K) * a->ckpt_stride())))
-      return rc;
-    CUDA_TRY(cudaGraphLaunch(a->g_fwd[h->cur], h->stream));
+    const int seg = (n - 1) / a->K;
+    if ((n - 1) % a->K == 0) {
+      if ((rc = save_state(a, a->ckpt + (size_t)seg * a->ckpt_stride()))) return rc;
+      if (R > 0 && seg == first) {
+        // resident segment r, step k: store step index r*K + k
+        AdjClock c0{0, nt};
+        CUDA_TRY(cudaMemcpyAsync(a->clock, &c0, sizeof(c0), cudaMemcpyHostToDevice, h->stream));
+      }
+    }
+    CUDA_TRY(cudaGraphLaunch(seg >= first ? a->g_fst[h->cur] : a->g_fwd[h->cur], h->stream));
     if (h->rk.nstage & 1) h->cur = 1 - h->cur;
   }
   std::vector<double> tr((size_t)nt * a->nrec);
@@ -818,6 +895,7 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
     if (misfit) *misfit = J;
     CUDA_TRY(cudaMemcpy(a->resid, tr.data(), tr.size() * sizeof(double), cudaMemcpyHostToDevice));
     a->have_resid = true;
+    a->resident = R;
   }
   return FDMAP_OK;
 }
@@ -851,20 +929,27 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
   CUDA_TRY(cudaGetLastError());
   int p = 0;  // ubar parity
   const int nseg = (N - 1 + a->K - 1) / a->K;
+  const int R = a->resident, first = nseg - R;
+  // recomputed segments go to the store after the resident ones
+  const long long rbase = (long long)R * a->K;
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int n0 = seg * a->K + 1, n1 = std::min(n0 + a->K, N);  // steps n0 .. n1-1
-    h->cur = 0;
-    int rc = restore_state(a, a->ckpt + (size_t)seg * a->ckpt_stride(), nullptr);
-    if (rc) return rc;
-    set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, a->t_start, a->dt, n0);
-    ck.rel = 0;
-    ck.n = N;  // unused while recomputing
-    CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
-    for (int n = n0; n < n1; ++n) {
-      CUDA_TRY(cudaGraphLaunch(a->g_rec[h->cur], h->stream));
-      if (h->rk.nstage & 1) h->cur = 1 - h->cur;
+    long long base = (long long)(seg - first) * a->K;
+    if (seg < first) {
+      h->cur = 0;
+      int rc = restore_state(a, a->ckpt + (size_t)seg * a->ckpt_stride(), nullptr);
+      if (rc) return rc;
+      set_step_clock<<<1, 1, 0, h->stream>>>(h->d_time, a->t_start, a->dt, n0);
+      ck.rel = rbase;
+      ck.n = N;  // unused while recomputing
+      CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
+      for (int n = n0; n < n1; ++n) {
+        CUDA_TRY(cudaGraphLaunch(a->g_rec[h->cur], h->stream));
+        if (h->rk.nstage & 1) h->cur = 1 - h->cur;
+      }
+      base = rbase;
     }
-    ck.rel = n1 - 1 - n0;
+    ck.rel = base + (n1 - 1 - n0);
     ck.n = n1 - 1;
     CUDA_TRY(cudaMemcpyAsync(a->clock, &ck, sizeof(ck), cudaMemcpyHostToDevice, h->stream));
     for (int n = n1 - 1; n >= n0; --n) {
@@ -883,6 +968,16 @@ int fdmap_gpu_adjoint_backward(fdmap_adjoint* a, double* grad_rho, double* grad_
 
 int fdmap_gpu_adjoint_fault_size(const fdmap_adjoint* a) { return a ? a->nfault : 0; }
 
+int fdmap_gpu_adjoint_set_store_budget(fdmap_adjoint* a, long long bytes) {
+  if (!a) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint");
+  a->store_budget = bytes < 0 ? -1 : bytes;
+  return FDMAP_OK;
+}
+
+long long fdmap_gpu_adjoint_segment_bytes(const fdmap_adjoint* a) { return a ? (long long)a->segment_bytes() : 0; }
+
+int fdmap_gpu_adjoint_resident_segments(const fdmap_adjoint* a) { return a ? a->resident : 0; }
+
 int fdmap_gpu_adjoint_time_params(fdmap_adjoint* a, double* params, int* nt) {
   if (!a) return set_err(FDMAP_ERR_INVALID_ARG, "null adjoint");
   return fdmap_gpu_time_params(a->h, params, nt);
@@ -891,6 +986,7 @@ int fdmap_gpu_adjoint_time_params(fdmap_adjoint* a, double* params, int* nt) {
 int fdmap_gpu_adjoint_set_prestress(fdmap_adjoint* a, const double* S0) {
   if (!a || !S0) return set_err(FDMAP_ERR_INVALID_ARG, "null argument");
   fdmap_gpu* h = a->h;
+  a->resident = 0;
   CUDA_TRY(cudaSetDevice(h->device));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   for (const auto& inf : a->info_host) {

@@ -494,14 +494,18 @@ __global__ void adj_inject(double* ub, const long long* __restrict__ node, const
   }
 }
 
-// end of a forward step: vz at the receivers of the new state (sample n+1), then n += 1
+// end of a forward step: vz at the receivers of the new state (sample n+1),
+// then n += 1 and, given the store clock, its step index += 1
 __global__ void adj_sample_advance(const double* __restrict__ u, const long long* __restrict__ rec, int nrec,
-                                   TimeState* ts, double* traces, int nsamples) {
+                                   TimeState* ts, double* traces, int nsamples, AdjClock* ck) {
   const long long n = ts->n + 1;
   for (int r = threadIdx.x; r < nrec; r += blockDim.x)
     if (n >= 1 && n <= nsamples) traces[(n - 1) * nrec + r] = u[rec[r]];
   __syncthreads();
-  if (threadIdx.x == 0) ts->n = n;
+  if (threadIdx.x == 0) {
+    ts->n = n;
+    if (ck) ck->rel += 1;
+  }
 }
 
 }  // namespace fdmap

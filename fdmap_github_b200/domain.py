@@ -523,7 +523,8 @@ class GpuAdjoint:
     shear prestress of every fault node, by the discrete adjoint with
     checkpoints."""
 
-    def __init__(self, host: HostDomain, receivers, checkpoint_every: int = 45, device: int = 0):
+    def __init__(self, host: HostDomain, receivers, checkpoint_every: int = 45, device: int = 0,
+                 store_budget: int = 0):
         self.host = host
         rec = np.asarray(receivers, dtype=np.int32).reshape(-1, 2)  # 1-based (i, j)
         self.nrec = rec.shape[0]
@@ -539,6 +540,26 @@ class GpuAdjoint:
             nt = C.c_int(0)
             check_gpu(lib().fdmap_gpu_adjoint_time_params(self._a, p, C.byref(nt)), "fdmap_gpu_adjoint_time_params")
             host.set_spacing(p[3], p[4])
+        if store_budget:
+            self.set_store_budget(store_budget)
+
+    def set_store_budget(self, nbytes: int) -> None:
+        """Device memory the forward pass with data may keep stage inputs in
+        (fdmap_gpu_adjoint_set_store_budget): its last segments stay resident
+        and the backward pass reverses them without recomputing; negative =
+        all free device memory, 0 = recompute every segment."""
+        check_gpu(lib().fdmap_gpu_adjoint_set_store_budget(self._a, int(nbytes)),
+                  "fdmap_gpu_adjoint_set_store_budget")
+
+    @property
+    def segment_bytes(self) -> int:
+        """Bytes of one segment's stage store."""
+        return int(lib().fdmap_gpu_adjoint_segment_bytes(self._a))
+
+    @property
+    def resident_segments(self) -> int:
+        """Segments of the last forward pass with data kept resident."""
+        return int(lib().fdmap_gpu_adjoint_resident_segments(self._a))
 
     def set_material(self, rho: np.ndarray, G: np.ndarray) -> None:
         r = np.ascontiguousarray(rho, dtype=np.float64).reshape(-1)

@@ -144,6 +144,9 @@ SIGNATURES = {
     "fdmap_gpu_adjoint_set_prestress": (C.c_int, [_VP, _DP]),
     "fdmap_gpu_adjoint_get_prestress": (C.c_int, [_VP, _DP]),
     "fdmap_gpu_adjoint_prestress_gradient": (C.c_int, [_VP, _DP]),
+    "fdmap_gpu_adjoint_set_store_budget": (C.c_int, [_VP, C.c_longlong]),
+    "fdmap_gpu_adjoint_segment_bytes": (C.c_longlong, [_VP]),
+    "fdmap_gpu_adjoint_resident_segments": (C.c_int, [_VP]),
     "fdmap_gpu_adjoint_destroy": (None, [_VP]),
 }
 

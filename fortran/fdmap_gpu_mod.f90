@@ -511,6 +511,25 @@ module fdmap_gpu_mod
        real(c_double), intent(out) :: grad_S0(*)
      end function fdmap_gpu_adjoint_prestress_gradient
 
+     integer(c_int) function fdmap_gpu_adjoint_set_store_budget(a, bytes) &
+          bind(C, name='fdmap_gpu_adjoint_set_store_budget')
+       import :: c_int, c_ptr, c_long_long
+       type(c_ptr), value :: a
+       integer(c_long_long), value :: bytes
+     end function fdmap_gpu_adjoint_set_store_budget
+
+     integer(c_long_long) function fdmap_gpu_adjoint_segment_bytes(a) &
+          bind(C, name='fdmap_gpu_adjoint_segment_bytes')
+       import :: c_long_long, c_ptr
+       type(c_ptr), value :: a
+     end function fdmap_gpu_adjoint_segment_bytes
+
+     integer(c_int) function fdmap_gpu_adjoint_resident_segments(a) &
+          bind(C, name='fdmap_gpu_adjoint_resident_segments')
+       import :: c_int, c_ptr
+       type(c_ptr), value :: a
+     end function fdmap_gpu_adjoint_resident_segments
+
      subroutine fdmap_gpu_adjoint_destroy(a) bind(C, name='fdmap_gpu_adjoint_destroy')
        import :: c_ptr
        type(c_ptr), value :: a

@@ -374,7 +374,7 @@ void fdmap_gpu_ensemble_destroy(fdmap_ensemble* e);
  * friction.f90:593-828 with its Newton root differentiated implicitly and the
  * state variable's own RK adjoint), with the fields and fault registers
  * checkpointed every `checkpoint_every` steps and each segment recomputed
- * once.  Slip-weakening, forced rupture and regularised normal stress are
+ * once, or kept resident (fdmap_gpu_adjoint_set_store_budget).  Slip-weakening, forced rupture and regularised normal stress are
  * refused (FDMAP_ERR_UNSUPPORTED).  The reference has no adjoint; there is no
  * routine this replaces.
  * ---------------------------------------------------------------------- */
@@ -417,6 +417,24 @@ int fdmap_gpu_adjoint_get_prestress(fdmap_adjoint* a, double* S0);
 
 /* dJ/dS0 per fault node from the last fdmap_gpu_adjoint_backward. */
 int fdmap_gpu_adjoint_prestress_gradient(fdmap_adjoint* a, double* grad_S0);
+
+/* Device memory (bytes) a forward pass with data may keep stage inputs in:
+ * the stage inputs of its last R segments (checkpoint intervals) stay
+ * resident, and the backward pass reverses those without recomputing them.
+ * R = the segments that fit in the budget and in the free device memory less
+ * 2 GiB, all of them or else one fewer than fit (a further segment store
+ * holds the recomputed ones).  0 (the default): every segment is recomputed;
+ * a negative budget: all free device memory.  Gradients do not depend on it
+ * (the stored inputs are the recomputed ones bit for bit).  The store is
+ * sized at the next forward pass with data; changing the material or the
+ * prestress drops the resident segments. */
+int fdmap_gpu_adjoint_set_store_budget(fdmap_adjoint* a, long long bytes);
+
+/* Bytes of one segment's stage store (checkpoint_every * stages slots). */
+long long fdmap_gpu_adjoint_segment_bytes(const fdmap_adjoint* a);
+
+/* Resident segments of the last forward pass with data (0 when none). */
+int fdmap_gpu_adjoint_resident_segments(const fdmap_adjoint* a);
 
 void fdmap_gpu_adjoint_destroy(fdmap_adjoint* a);
 

@@ -6,6 +6,7 @@ consumes the same fdmap_desc a HostDomain produces.
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -15,6 +16,29 @@ FAULT_FIELDS = ["D", "Psi", "DPsi", "trup", "V", "O", "S", "N", "S0", "N0",
                 "Ds", "Dn", "DDs", "DDn", "W", "DW", "Nreg", "DNreg"]
 
 _lib = None
+
+
+def usable_cpus() -> int:
+    """CPUs this process may use: its affinity mask, capped by the cgroup's
+    CPU quota (cgroup v2 cpu.max, v1 cfs quota/period), so that OpenMP does
+    not run more threads than a container is given time for."""
+    n = len(os.sched_getaffinity(0))
+    for quota_file, period_file in (("/sys/fs/cgroup/cpu.max", None),
+                                    ("/sys/fs/cgroup/cpu/cpu.cfs_quota_us", "/sys/fs/cgroup/cpu/cpu.cfs_period_us")):
+        try:
+            with open(quota_file) as f:
+                parts = f.read().split()
+            if period_file is None:
+                quota, period = parts[0], parts[1]
+            else:
+                with open(period_file) as f:
+                    quota, period = parts[0], f.read().split()[0]
+            if quota not in ("max", "-1") and int(period) > 0:
+                n = min(n, max(1, int(quota) // int(period)))
+            break
+        except (OSError, ValueError, IndexError):
+            continue
+    return max(1, n)
 
 
 def lib() -> C.CDLL:
@@ -44,6 +68,9 @@ def lib() -> C.CDLL:
         L.oracle_set_newton_limit.argtypes = [C.c_void_p, C.c_int]
         L.oracle_set_newton_tolerance.argtypes = [C.c_void_p, C.c_double]
         L.oracle_num_threads.restype = C.c_int
+        L.oracle_set_num_threads.argtypes = [C.c_int]
+        if "OMP_NUM_THREADS" not in os.environ:
+            L.oracle_set_num_threads(min(L.oracle_num_threads(), usable_cpus()))
         L.oracle_set_tap.argtypes = [C.c_void_p, C.c_int]
         L.oracle_get_fault_tap.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]
         L.oracle_set_fault.argtypes = [C.c_void_p, C.c_int, C.c_int, _DP]

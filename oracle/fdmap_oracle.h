@@ -117,8 +117,10 @@ int oracle_set_exchange(oracle_domain* o, int (*fn)(void*, long long), void* use
 int oracle_get_iface_edge(oracle_domain* o, int iface, int side, double* out);
 int oracle_set_iface_edge(oracle_domain* o, int iface, int side, const double* in);
 
-/* Number of OpenMP threads the oracle uses (1 when built without OpenMP). */
+/* Number of OpenMP threads the oracle uses (1 when built without OpenMP),
+ * and a cap on it (n > 0). */
 int oracle_num_threads(void);
+void oracle_set_num_threads(int n);
 
 #ifdef __cplusplus
 }

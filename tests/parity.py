@@ -73,30 +73,36 @@ def fault_errors(gpu, orc, iface=0, fields=("V", "S", "N", "D", "Psi")) -> dict:
     return out
 
 
-def solver_spread(host, n_last, fields=("V", "S", "N", "D", "Psi"), iface=0, **run_kw):
+def solver_spread(host, n_last, fields=("V", "S", "N", "D", "Psi"), iface=0, base=None, **run_kw):
     """How far the oracle's own result moves when its Newton residual
-    tolerance atolR is halved: (largest field error, {fault field: error})."""
+    tolerance atolR is halved: (largest field error, {fault field: error}).
+    `base`: an oracle already run over the same loop indices at the
+    reference's tolerance, used in place of a fresh run."""
     from oracle.binding import OracleDomain
 
-    a, b = OracleDomain(host), OracleDomain(host)
+    a = base
+    if a is None:
+        a = OracleDomain(host)
+        a.run(1, n_last, **run_kw)
+    b = OracleDomain(host)
     b.set_newton_tolerance(0.5)
-    a.run(1, n_last, **run_kw)
     b.run(1, n_last, **run_kw)
     fe = max(field_errors(b.get_fields()[0], a.get_fields()[0]))
     ft = fault_errors(b, a, iface, fields) if host.nifaces else {}
-    a.close()
+    if base is None:
+        a.close()
     b.close()
     return fe, ft
 
 
-def law_tolerances(law, host=None, n_last=None, fields=("V", "S", "N", "D", "Psi"), **run_kw):
+def law_tolerances(law, host=None, n_last=None, fields=("V", "S", "N", "D", "Psi"), base=None, **run_kw):
     """(field tolerance, {fault field: tolerance}) for a run with friction law
     `law`: 1e-10 for explicit interface solves; for rate-and-state laws
     SPREAD_FACTOR times the spread within the reference's solver tolerance
     (never below 1e-10)."""
     if law in EXPLICIT_LAWS:
         return FIELD_RTOL, {f: FAULT_RTOL for f in fields}
-    fe, ft = solver_spread(host, n_last, fields, **run_kw)
+    fe, ft = solver_spread(host, n_last, fields, base=base, **run_kw)
     return (max(FIELD_RTOL, SPREAD_FACTOR * fe), {f: max(FAULT_RTOL, SPREAD_FACTOR * ft[f]) for f in fields})
 
 

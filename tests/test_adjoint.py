@@ -90,6 +90,32 @@ def test_gradient_independent_of_checkpoint_interval(require_gpu, tmp_path):
         assert np.array_equal(x, y)
 
 
+def test_resident_segments_match_recompute(require_gpu, tmp_path):
+    """Stage inputs kept resident from the forward pass (every segment, some
+    of them, none) give the recomputed gradient bit for bit, also from a
+    second backward over the same forward; a material change drops them."""
+    rng = np.random.default_rng(5)
+    h, rec, a = _setup(tmp_path, K=7)  # 80 steps: 12 segments, the last of 3 steps
+    data = _data(a, h, rng)
+    tr0, J0 = a.forward(data=data)
+    ref = a.backward()
+    assert a.resident_segments == 0
+    seg = a.segment_bytes
+    assert seg >= 7 * 5 * 3 * 8 * h.ny * h.nx  # K steps x 5 stages x 3 padded planes
+    for budget, want in ((-1, 12), (4 * seg, 3), (seg, 0), (12 * seg, 12)):
+        a.set_store_budget(budget)
+        tr, J = a.forward(data=data)
+        assert np.array_equal(tr, tr0) and J == J0
+        assert a.resident_segments == want, budget
+        for _ in range(2):
+            for x, y in zip(ref, a.backward()):
+                assert np.array_equal(x, y), budget
+    a.set_material(*_material(h))
+    assert a.resident_segments == 0
+    for x, y in zip(ref, a.backward()):
+        assert np.array_equal(x, y)
+
+
 def test_boundary_nodes_carry_gradient(require_gpu, tmp_path):
     """The edge impedances depend on rho and G: boundary-node gradients are
     part of the FD-checked total and must not vanish."""

@@ -182,6 +182,25 @@ def test_gradient_independent_of_checkpoint_interval(require_gpu, tmp_path):
 
 
 @pytest.mark.gpu
+def test_resident_segments_match_recompute(require_gpu, tmp_path):
+    """Fields, state variable and slip rate of resident segments (all, or the
+    last two with the rest recomputed after them) give the recomputed
+    gradients in rho, G and S0 bit for bit."""
+    h, rec, a = _setup(tmp_path, K=7)  # 40 steps: 6 segments
+    data = _data(a, h)
+    a.forward(data=data)
+    ref = a.backward() + (a.prestress_gradient(),)
+    seg = a.segment_bytes
+    for budget, want in ((-1, 6), (3 * seg, 2)):
+        a.set_store_budget(budget)
+        a.forward(data=data)
+        assert a.resident_segments == want
+        for _ in range(2):
+            for x, y in zip(ref, a.backward() + (a.prestress_gradient(),)):
+                assert np.array_equal(x, y), budget
+
+
+@pytest.mark.gpu
 def test_fault_nodes_carry_material_gradient(require_gpu, tmp_path):
     """The interface impedances depend on rho and G at both edge nodes."""
     h, rec, adj = _setup(tmp_path)

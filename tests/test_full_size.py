@@ -41,7 +41,7 @@ def _compare(name, h, n_last, law, fault_fields=("V", "S", "N", "D", "Psi")):
     flt = fault_errors(g, o, fields=fault_fields)
     tg, to = g.get_fault(0, "trup"), o.get_fault(0, "trup")
     # explicit solves: 1e-10; rate-and-state: the spread within the reference's solver tolerance
-    ftol, qtol = law_tolerances(law, h, n_last, fault_fields)
+    ftol, qtol = law_tolerances(law, h, n_last, fault_fields, base=o)
     rec = {"case": name, "nx": h.nx, "ny": h.ny, "loop_indices": n_last, "field_rel_err": ferr,
            "fault_rel_err": flt, "field_tolerance": ftol, "fault_tolerance": qtol,
            "trup_mismatch_nodes": int(np.count_nonzero(tg != to)),
