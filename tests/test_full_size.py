@@ -6,10 +6,11 @@ grid sizes:
   roughfault  two curvilinear blocks of 2001 x 1001 nodes on a seeded fractal
               fault of 2001 nodes, flash-heating rate-and-state (RFL)
 
-By default a few hundred steps of each (the oracle needs about a minute on the
-GPU box's host cores).  With FDMAP_FULL_LENGTH=1 the whole runs, 4000 and 6000
-steps (nt = 4001 and 6001 loop indices, the last one the reference's
-output-only index), are compared instead.  Every case prints one line
+By default 300 steps of the rupture and 50 of the rough fault (about half a
+minute and two minutes of the oracle on 16 host cores; 200 rough-fault steps
+take ten, set FDMAP_ROUGH_STEPS to run them).  With FDMAP_FULL_LENGTH=1 the
+whole runs, 4000 and 6000 steps (nt = 4001 and 6001 loop indices, the last
+one the reference's output-only index), are compared instead.  Every case prints one line
 `FULLSIZE {json}` with the per-field and fault errors and the tolerances
 they were held to (tests/parity.py: 1e-10 for the slip-weakening rupture; for
 the rate-and-state run the spread of the oracle's own answer when its Newton
@@ -65,7 +66,8 @@ def test_rupture_full_grid(require_gpu):
 def test_roughfault_full_grid(require_gpu, tmp_path):
     h = init_domain(problems.rough_fault_rs(tmp_path), tmp_path)
     assert (h.nx, h.ny) == (2001, 2002)
-    _compare("roughfault 2x2001x1001", h, h.nt if FULL else 200, "RFL")
+    steps = int(os.environ.get("FDMAP_ROUGH_STEPS", "50"))
+    _compare("roughfault 2x2001x1001", h, h.nt if FULL else steps, "RFL")
 
 
 def test_field_tolerance_is_the_stated_one():
