@@ -551,13 +551,18 @@ int ensure_store(fdmap_adjoint* a, int nseg) {
     CUDA_TRY(cudaStreamSynchronize(a->h->stream));
     a->release(a->store);
     a->store = nullptr;
+    a->store_segs = 0;  // no store: the next forward with data sizes it again
     a->resident = 0;
     if (a->alloc(&a->store, (size_t)segs * seg / sizeof(double)) != FDMAP_OK) {
       // fall back to checkpointing alone (and clear the failed allocation's error)
       cudaGetLastError();
       R = 0;
       int rc = a->alloc(&a->store, seg / sizeof(double));
-      if (rc) return rc;
+      if (rc) {
+        cudaGetLastError();
+        a->plan_nseg = -1;
+        return rc;
+      }
       a->store_segs = 1;
     } else {
       a->store_segs = segs;
@@ -837,6 +842,9 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
   if (nt < 2) return set_err(FDMAP_ERR_INVALID_ARG, "nt must be at least 2");
   fdmap_gpu* h = a->h;
   CUDA_TRY(cudaSetDevice(h->device));
+  // until this run has finished, there is nothing to take a backward pass over
+  a->have_resid = false;
+  a->resident = 0;
   int rc;
   if ((rc = ensure_trace_buffers(a, nt))) return rc;
   const int nck = (nt - 1 + a->K - 1) / a->K;
@@ -844,11 +852,9 @@ int fdmap_gpu_adjoint_forward(fdmap_adjoint* a, double t_start, double dt, int n
   // a run with data precedes a backward: its last R segments keep their stage inputs
   if (data && (rc = ensure_store(a, nck))) return rc;
   const int R = data ? a->plan_R : 0;
-  a->resident = 0;
   a->N = nt;
   a->t_start = t_start;
   a->dt = dt;
-  a->have_resid = false;
   if (a->graph_dt != dt || a->graph_t0 != t_start || !a->g_fwd[0]) {
     if ((rc = build_graphs(a, dt))) return rc;
     a->graph_t0 = t_start;
